@@ -1,0 +1,308 @@
+/*
+ * vgpu.h -- C ABI of the B200-native DuckDB GPU execution path (libvgpu.so).
+ *
+ * Everything crosses this boundary as plain C: POD structs, raw pointers, sizes and integer status
+ * codes. No C++ types, no exceptions, no torch types. A failed call returns a status other than
+ * VGPU_OK and leaves a human-readable message in a thread-local buffer (vgpu_last_error()).
+ *
+ * The plan IR mirrors the reference engine boundary, cuda_engine/include/gpu_engine.hpp:
+ *   vgpu_op_type          <- GpuOpType            (gpu_engine.hpp:14-21)
+ *   vgpu_value_type       <- GpuValueType         (gpu_engine.hpp:29-38)
+ *   vgpu_hugeint          <- GpuHugeInt           (gpu_engine.hpp:40-47)
+ *   vgpu_expr             <- GpuExpr              (gpu_engine.hpp:56-80)
+ *   vgpu_aggregate_kind   <- GpuAggregateKind     (gpu_engine.hpp:85-92)
+ *   vgpu_aggregate        <- GpuAggregate         (gpu_engine.hpp:96-104)
+ *   vgpu_plan_node        <- GpuPlanNode          (gpu_engine.hpp:135-185), children by index
+ *   vgpu_column           <- GpuColumn            (gpu_engine.hpp:199-213)
+ *   vgpu_result           <- GpuExecutionResult   (gpu_engine.hpp:215-222)
+ *   vgpu_exec_options     <- GpuExecuteOptions    (gpu_engine.hpp:357-385)
+ */
+#ifndef VGPU_H_
+#define VGPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VGPU_ABI_VERSION 1
+
+typedef enum vgpu_status {
+	VGPU_OK = 0,
+	VGPU_ERR_INVALID_ARGUMENT = 1, /* malformed plan, null pointer, size mismatch */
+	VGPU_ERR_UNSUPPORTED = 2,      /* a shape this engine refuses cleanly (caller falls back to CPU) */
+	VGPU_ERR_CUDA = 3,             /* CUDA runtime / driver failure */
+	VGPU_ERR_OUT_OF_MEMORY = 4,    /* device budget exhausted or allocation failed */
+	VGPU_ERR_COMPILE = 5,          /* NVRTC rejected generated source */
+	VGPU_ERR_NOT_READY = 6,        /* non-blocking query: work not finished yet */
+	VGPU_ERR_TIMEOUT = 7,          /* a bounded wait gave up */
+	VGPU_ERR_REJECTED = 8,         /* admission control refused the request */
+	VGPU_ERR_INTERNAL = 9
+} vgpu_status;
+
+/* GpuOpType, same order (gpu_engine.hpp:14-21). */
+typedef enum vgpu_op_type {
+	VGPU_OP_SCAN = 0,
+	VGPU_OP_FILTER = 1,
+	VGPU_OP_PROJECTION = 2,
+	VGPU_OP_HASH_JOIN = 3,
+	VGPU_OP_GROUP_BY_AGGREGATE = 4,
+	VGPU_OP_CROSS_PRODUCT = 5
+} vgpu_op_type;
+
+/* GpuValueType, same order (gpu_engine.hpp:29-38). */
+typedef enum vgpu_value_type {
+	VGPU_INT16 = 0,
+	VGPU_INT32 = 1,
+	VGPU_INT64 = 2,
+	VGPU_FLOAT32 = 3,
+	VGPU_FLOAT64 = 4,
+	VGPU_BOOLEAN = 5,
+	VGPU_DICTIONARY_STRING = 6,
+	VGPU_HUGEINT = 7
+} vgpu_value_type;
+
+/* GpuHugeInt (gpu_engine.hpp:40-47): two's-complement 128-bit integer, little-endian halves. */
+typedef struct vgpu_hugeint {
+	uint64_t lower;
+	int64_t upper;
+} vgpu_hugeint;
+
+/* GpuAggregateKind, same order (gpu_engine.hpp:85-92). */
+typedef enum vgpu_aggregate_kind {
+	VGPU_AGG_COUNT_STAR = 0,
+	VGPU_AGG_COUNT = 1,
+	VGPU_AGG_SUM = 2,
+	VGPU_AGG_MIN = 3,
+	VGPU_AGG_MAX = 4,
+	VGPU_AGG_AVG = 5
+} vgpu_aggregate_kind;
+
+/* GpuExpr (gpu_engine.hpp:56-80). `source` is a CUDA statement that reads its inputs as
+ * ((const T*)inputs[i])[row] and writes ((T*)out)[idx], exactly the form the reference's
+ * expression translator emits (extension/src/expression_translator.cpp:311-315, 489-493). */
+typedef struct vgpu_expr {
+	const char *source;
+	const char *const *input_columns;
+	uint32_t n_input_columns;
+	uint32_t output_type; /* vgpu_value_type */
+} vgpu_expr;
+
+/* GpuAggregate (gpu_engine.hpp:96-104). input_column is NULL/empty for COUNT_STAR. */
+typedef struct vgpu_aggregate {
+	uint32_t kind;        /* vgpu_aggregate_kind */
+	uint32_t output_type; /* vgpu_value_type */
+	const char *input_column;
+} vgpu_aggregate;
+
+/* GpuPlanNode (gpu_engine.hpp:135-185) flattened: children are indices into vgpu_plan.nodes.
+ * Output naming follows the reference: PROJECTION emits "col<i>", GROUP_BY emits its key names then
+ * "agg_<i>", FILTER passes its child's columns through, joins emit `output_columns`. */
+typedef struct vgpu_plan_node {
+	uint32_t op; /* vgpu_op_type */
+	uint32_t n_children;
+	const uint32_t *children;
+	/* SCAN */
+	const char *catalog;
+	const char *schema;
+	const char *table;
+	const char *const *column_names;
+	uint32_t n_column_names;
+	/* FILTER / PROJECTION */
+	const vgpu_expr *expressions;
+	uint32_t n_expressions;
+	/* HASH_JOIN: build_keys name children[0] columns, probe_keys children[1] columns */
+	const char *const *build_keys;
+	uint32_t n_build_keys;
+	const char *const *probe_keys;
+	uint32_t n_probe_keys;
+	/* HASH_JOIN / CROSS_PRODUCT */
+	const char *const *output_columns;
+	uint32_t n_output_columns;
+	/* GROUP_BY_AGGREGATE */
+	const char *const *group_keys;
+	uint32_t n_group_keys;
+	const vgpu_aggregate *aggregates;
+	uint32_t n_aggregates;
+	/* cost-model inputs (advisory) */
+	uint64_t estimated_rows;
+	uint32_t estimated_row_width_bytes;
+} vgpu_plan_node;
+
+typedef struct vgpu_plan {
+	const vgpu_plan_node *nodes;
+	uint32_t n_nodes;
+	uint32_t root;
+} vgpu_plan;
+
+typedef enum vgpu_memory {
+	VGPU_MEM_HOST = 0,  /* pageable or pinned host memory */
+	VGPU_MEM_DEVICE = 1 /* device memory of the current device */
+} vgpu_memory;
+
+/* GpuColumn (gpu_engine.hpp:199-213). Validity: NULL = no nulls; otherwise an Arrow LSB-first
+ * bitmap (bit set = valid) living in the same memory space as `data`. */
+typedef struct vgpu_column {
+	const char *name;
+	uint32_t type;   /* vgpu_value_type */
+	uint32_t memory; /* vgpu_memory */
+	const void *data;
+	const uint8_t *validity;
+	uint64_t row_count;
+} vgpu_column;
+
+/* GpuExecuteOptions (gpu_engine.hpp:357-385) plus placement controls. */
+typedef struct vgpu_exec_options {
+	int32_t stage_scan_to_cache;         /* hand every SCAN column to the open cache staging slot */
+	int32_t serve_whole_scan_from_cache; /* read every SCAN leaf from the committed cache entry */
+	int64_t cache_chunk_index;           /* >=0: serve chunk i of the cache entry (row-independent plans) */
+	int32_t output_memory;               /* VGPU_MEM_HOST (default) or VGPU_MEM_DEVICE */
+	int32_t flags;                       /* VGPU_EXEC_* bits */
+	void *stream;                        /* cudaStream_t to run on; NULL = the engine's own stream */
+} vgpu_exec_options;
+
+#define VGPU_EXEC_NO_SYNC 1u /* device output only: return without synchronizing the stream */
+
+void vgpu_exec_options_init(vgpu_exec_options *options);
+
+typedef struct vgpu_result vgpu_result;
+
+/* GpuEngine::ExecutePlan (gpu_engine.hpp:389-402; cuda_engine/src/gpu_engine.cpp:37-74).
+ * SCAN leaves consume `inputs` positionally in traversal order, children[0] before children[1]
+ * (cuda_engine/src/gpu_executor_internal.hpp:97). Host inputs are read during the call only. */
+vgpu_status vgpu_execute_plan(const vgpu_plan *plan, const vgpu_column *inputs, size_t n_inputs,
+                              const vgpu_exec_options *options, vgpu_result **out);
+
+/* GpuExecutionResult::columns (gpu_engine.hpp:215-222). Column pointers stay valid until
+ * vgpu_result_free; their memory space is vgpu_exec_options.output_memory. */
+size_t vgpu_result_column_count(const vgpu_result *result);
+vgpu_status vgpu_result_get_column(const vgpu_result *result, size_t index, vgpu_column *out);
+void vgpu_result_free(vgpu_result *result);
+
+/* Thread-local message describing the last failed call on this thread ("" if none). */
+const char *vgpu_last_error(void);
+const char *vgpu_status_string(vgpu_status status);
+int vgpu_abi_version(void);
+
+/* ---- Device, streams and timing plumbing ---------------------------------------------------- */
+
+/* Device properties the engine sized itself against (device 0 unless vgpu_set_device was called). */
+typedef struct vgpu_device_info {
+	int32_t device;
+	int32_t sm_count;
+	int32_t cc_major;
+	int32_t cc_minor;
+	uint64_t total_memory;
+	uint64_t free_memory;
+	uint64_t l2_bytes;
+	uint64_t smem_per_block_optin;
+	char name[128];
+} vgpu_device_info;
+
+vgpu_status vgpu_set_device(int device);
+vgpu_status vgpu_get_device_info(vgpu_device_info *out);
+vgpu_status vgpu_synchronize(void *stream);
+
+/* Per-launch device timing of the engine's own kernels (CUDA events on the launching stream).
+ * While enabled, every launch records a start/stop event pair; vgpu_profile_collect synchronizes
+ * and returns (name, milliseconds, algorithmic bytes) per launch since the last collect. */
+typedef struct vgpu_kernel_timing {
+	char name[48];
+	float ms;
+	uint64_t bytes;
+	uint64_t rows;
+} vgpu_kernel_timing;
+
+vgpu_status vgpu_profile_enable(int enable);
+vgpu_status vgpu_profile_collect(vgpu_kernel_timing *out, size_t capacity, size_t *count);
+/* Number of engine kernels launched since process start (all streams). */
+uint64_t vgpu_launch_count(void);
+
+/* ---- Kernel cache (cuda_engine/include/code_generator.hpp:30-155, kernel_cache.hpp:29-66) ---- */
+
+/* SHA-256 of `n` bytes as 64 lowercase hex characters plus NUL (KernelCache::HashSource,
+ * cuda_engine/src/kernel_cache.cpp:20-146). `out` must hold 65 bytes. */
+void vgpu_sha256_hex(const void *data, size_t n, char *out);
+
+typedef struct vgpu_kernel_cache_stats {
+	uint64_t entries;
+	uint64_t hits;
+	uint64_t misses;
+	uint64_t disk_hits;
+	uint64_t compiles;
+	double compile_ms_total;
+} vgpu_kernel_cache_stats;
+
+vgpu_status vgpu_kernel_cache_stats_get(vgpu_kernel_cache_stats *out);
+/* Compiles `source` (a whole translation unit) with NVRTC for sm_100a without loading it. Usable on
+ * a machine without a GPU; returns VGPU_ERR_COMPILE with the NVRTC log on failure. */
+vgpu_status vgpu_nvrtc_compile_check(const char *source, size_t *cubin_bytes);
+/* Generates (but does not compile) the fused source the engine would build for `plan`; writes at
+ * most `capacity` bytes including the NUL and reports the full length in *length. */
+vgpu_status vgpu_generate_source(const vgpu_plan *plan, const vgpu_column *inputs, size_t n_inputs,
+                                 char *out, size_t capacity, size_t *length);
+
+/* ---- Cost model (cuda_engine/include/gpu_engine.hpp:187-348; src/gpu_cost_model.cpp) ------- */
+
+typedef struct vgpu_working_set {
+	uint64_t total_bytes; /* saturates at UINT64_MAX */
+	int32_t chunk_capped;
+	uint64_t largest_bytes;
+	char largest_operator[32];
+} vgpu_working_set;
+
+/* IsRowIndependent (gpu_engine.hpp:248) */
+int vgpu_is_row_independent(const vgpu_plan *plan);
+/* EstimateWorkingSet (gpu_engine.hpp:341), re-derived for this engine's own allocation sites. */
+vgpu_status vgpu_estimate_working_set(const vgpu_plan *plan, uint64_t max_chunk_rows, vgpu_working_set *out);
+
+/* ---- Device memory budget (cuda_engine/include/rmm_pool.hpp:32-141) -------------------------- */
+
+typedef struct vgpu_memory_stats {
+	uint64_t budget_bytes;
+	uint64_t in_use_bytes;
+	uint64_t peak_bytes;
+	uint64_t allocations;
+	uint64_t failed_allocations;
+} vgpu_memory_stats;
+
+/* 0 = derive from VECTOR_GPU_VRAM_FRACTION (default 0.85) of free memory at first use. */
+vgpu_status vgpu_memory_set_budget(uint64_t bytes);
+vgpu_status vgpu_memory_stats_get(vgpu_memory_stats *out);
+/* HasHeadroomFor (cuda_engine/src/rmm_pool.cpp:172-191) */
+int vgpu_memory_has_headroom(uint64_t bytes);
+
+/* ---- Device column cache (cuda_engine/include/gpu_column_cache.hpp:107-281) ------------------ */
+
+typedef struct vgpu_table_ref {
+	const char *catalog;
+	const char *schema;
+	const char *table;
+} vgpu_table_ref;
+
+/* EnsureInitialized: fraction of free device memory (VECTOR_GPU_CACHE_FRACTION / _MB override). */
+vgpu_status vgpu_cache_init(double fraction_of_vram);
+vgpu_status vgpu_cache_begin_staging(const vgpu_table_ref *table);
+/* StageChunk: copies (H2D or D2D) `chunk` into cache-owned device memory as the next chunk of the
+ * column. *accepted = 1 when staged, 0 when declined (no open slot, type mismatch, budget). */
+vgpu_status vgpu_cache_stage_chunk(const vgpu_table_ref *table, const vgpu_column *chunk, int *accepted);
+vgpu_status vgpu_cache_commit_staging(const vgpu_table_ref *table, uint64_t scanned_rows);
+vgpu_status vgpu_cache_abort_staging(const vgpu_table_ref *table);
+/* ReplayableChunkRows: writes up to `capacity` chunk row counts; *count = number of chunks (0 on miss). */
+vgpu_status vgpu_cache_replayable_chunk_rows(const vgpu_table_ref *table, const char *const *column_names,
+                                             size_t n_columns, uint64_t *rows, size_t capacity, size_t *count);
+/* TryGetChunk: borrow of the device buffer (valid until the next evicting call). */
+vgpu_status vgpu_cache_try_get_chunk(const vgpu_table_ref *table, const char *column_name, uint64_t chunk_index,
+                                     vgpu_column *out, int *found);
+vgpu_status vgpu_cache_invalidate_table(const vgpu_table_ref *table);
+vgpu_status vgpu_cache_invalidate_all(void);
+uint64_t vgpu_cache_current_bytes(void);
+uint64_t vgpu_cache_table_generation(const vgpu_table_ref *table);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* VGPU_H_ */

@@ -1,0 +1,97 @@
+"""Parity of the benchmark queries: the engine (C ABI) against the oracle on the same seeded tables.
+
+Integer, DECIMAL (exact 128-bit) and COUNT results must be bit-exact; DOUBLE sums and averages are
+order-dependent FP64 and must agree within 1e-12 relative (the tolerance the query contract states).
+"""
+import numpy as np
+import pytest
+
+from vectisdb_b200 import GpuEngine
+from vectisdb_b200 import workloads as W
+from vectisdb_b200.engine import hugeint_to_int
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-12
+
+
+def _run(wl):
+    r = GpuEngine.instance().execute_plan(wl.plan, wl.inputs)
+    assert r.success, r.error_message
+    return r.columns
+
+
+def _close(got, exp):
+    got = np.asarray(got, np.float64)
+    exp = np.asarray(exp, np.float64)
+    return np.all(np.abs(got - exp) <= REL * np.maximum(np.abs(exp), 1e-300))
+
+
+@pytest.mark.parametrize("n,k_card", [(1 << 16, 1024), (1_000_003, 1024), (1 << 20, 16), (300_000, 3000)])
+def test_c0_filter_group_by(n, k_card):
+    wl = W.c0(n=n, k_card=k_card)
+    cols = _run(wl)
+    k, s, c, mn, mx = [x.data for x in cols]
+    order = np.argsort(k)
+    exp = O.c0(wl.inputs[0].data, wl.inputs[1].data, wl.inputs[2].data, 0.5, 7)
+    assert np.array_equal(k[order], exp["k"])
+    assert np.array_equal(c[order], exp["count"])
+    assert np.array_equal(mn[order], exp["min"])
+    assert np.array_equal(mx[order], exp["max"])
+    assert _close(s[order], exp["sum"])
+
+
+@pytest.mark.parametrize("n", [1 << 14, 1 << 18, 3_000_001])
+def test_c1_high_cardinality_group_by(n):
+    wl = W.c1(n=n)
+    a, b, amt, v, ts = [c.data for c in wl.inputs]
+    cols = _run(wl)
+    ga, gb, gsum, gavg, gcnt, gmax = [c.data for c in cols]
+    order = np.lexsort((gb, ga))
+    exp = O.c1(a, b, amt, v, ts, wl.params["ts_gt"])
+    assert len(ga) == len(exp["a"])
+    assert np.array_equal(ga[order], exp["a"]) and np.array_equal(gb[order], exp["b"])
+    assert np.array_equal(gcnt[order], exp["count"])
+    assert np.array_equal(gmax[order], exp["max"])
+    gs = gsum[order]
+    assert np.array_equal(gs["lower"], exp["sum_lo"]) and np.array_equal(gs["upper"], exp["sum_hi"])
+    assert _close(gavg[order], exp["avg"])
+
+
+def test_c1_sum_is_exact_beyond_int64():
+    """SUM over BIGINT returns HUGEINT: sums that overflow 64 bits stay exact (DuckDB's DECIMAL(38,x))."""
+    from vectisdb_b200.engine import GpuAggregateKind as A, GpuValueType as T
+    from vectisdb_b200 import make_aggregate, make_column, make_group_by, make_scan
+    n = 1 << 16
+    k = np.arange(n) % 3
+    big = np.full(n, (1 << 62) + 12345, np.int64)
+    big[::5] = -(1 << 62) - 7
+    plan = make_group_by(["k"], [make_aggregate(A.SUM, "v", T.HUGEINT)], make_scan(["k", "v"]))
+    r = GpuEngine.instance().execute_plan(plan, [make_column("k", T.INT32, k), make_column("v", T.INT64, big)])
+    assert r.success, r.error_message
+    got = dict(zip(r.columns[0].data.tolist(), hugeint_to_int(r.columns[1].data)))
+    for key in range(3):
+        assert got[key] == int(big[k == key].astype(object).sum())
+
+
+@pytest.mark.parametrize("probe_n,build_n", [(1 << 16, 1 << 12), (1 << 20, 1 << 16)])
+def test_c2_join_group_by(probe_n, build_n):
+    wl = W.c2(probe_n=probe_n, build_n=build_n, miss_lo=build_n, miss_span=build_n)
+    pkey, x, bkey, g = [c.data for c in wl.inputs]
+    cols = _run(wl)
+    gg, gs = [c.data for c in cols]
+    order = np.argsort(gg)
+    exp = O.c2(bkey, g, pkey, x)
+    assert np.array_equal(gg[order], exp["g"])
+    assert _close(gs[order], exp["sum"])
+
+
+@pytest.mark.parametrize("side", [256, 1000, 4096])
+def test_c2b_filtered_cross_product(side):
+    wl = W.c2b(side=side)
+    a, b = [c.data for c in wl.inputs]
+    cols = _run(wl)
+    count, ea, eb = O.c2b(a, b, 13)
+    assert len(cols[0].data) == count
+    assert np.array_equal(cols[0].data, ea) and np.array_equal(cols[1].data, eb)  # left-major order

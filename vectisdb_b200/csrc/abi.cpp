@@ -1,0 +1,376 @@
+// abi.cpp -- the extern "C" boundary (include/vgpu.h). Every entry point catches everything: no C++
+// exception and no process abort ever crosses into the caller; failures become a status code plus a
+// thread-local message (the reference's success=false + error_message contract,
+// cuda_engine/src/gpu_engine.cpp:41-52).
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "column_cache.hpp"
+#include "cost_model.hpp"
+#include "executor.hpp"
+#include "plan.hpp"
+#include "runtime.hpp"
+
+namespace vgpu {
+std::string Sha256Hex(const void *data, size_t n);
+}
+
+using namespace vgpu;
+
+struct vgpu_result {
+	ExecResult exec;
+	std::vector<std::string> names;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <typename F> vgpu_status Guard(F &&f) {
+	try {
+		g_last_error.clear();
+		f();
+		return VGPU_OK;
+	} catch (const Error &e) {
+		g_last_error = e.what();
+		return e.status();
+	} catch (const std::bad_alloc &) {
+		g_last_error = "host allocation failed";
+		return VGPU_ERR_OUT_OF_MEMORY;
+	} catch (const std::exception &e) {
+		g_last_error = e.what();
+		return VGPU_ERR_INTERNAL;
+	} catch (...) {
+		g_last_error = "unknown internal error";
+		return VGPU_ERR_INTERNAL;
+	}
+}
+
+TableRef ToTable(const vgpu_table_ref *t) {
+	if (t == nullptr) Fail(VGPU_ERR_INVALID_ARGUMENT, "null table reference");
+	return TableRef {t->catalog ? t->catalog : "", t->schema ? t->schema : "", t->table ? t->table : ""};
+}
+
+} // namespace
+
+extern "C" {
+
+int vgpu_abi_version(void) {
+	return VGPU_ABI_VERSION;
+}
+
+const char *vgpu_last_error(void) {
+	return g_last_error.c_str();
+}
+
+const char *vgpu_status_string(vgpu_status status) {
+	switch (status) {
+	case VGPU_OK:
+		return "OK";
+	case VGPU_ERR_INVALID_ARGUMENT:
+		return "INVALID_ARGUMENT";
+	case VGPU_ERR_UNSUPPORTED:
+		return "UNSUPPORTED";
+	case VGPU_ERR_CUDA:
+		return "CUDA";
+	case VGPU_ERR_OUT_OF_MEMORY:
+		return "OUT_OF_MEMORY";
+	case VGPU_ERR_COMPILE:
+		return "COMPILE";
+	case VGPU_ERR_NOT_READY:
+		return "NOT_READY";
+	case VGPU_ERR_TIMEOUT:
+		return "TIMEOUT";
+	case VGPU_ERR_REJECTED:
+		return "REJECTED";
+	case VGPU_ERR_INTERNAL:
+		return "INTERNAL";
+	}
+	return "UNKNOWN";
+}
+
+void vgpu_exec_options_init(vgpu_exec_options *o) {
+	if (!o) return;
+	std::memset(o, 0, sizeof(*o));
+	o->cache_chunk_index = -1;
+	o->output_memory = VGPU_MEM_HOST;
+}
+
+vgpu_status vgpu_execute_plan(const vgpu_plan *plan, const vgpu_column *inputs, size_t n_inputs,
+                              const vgpu_exec_options *options, vgpu_result **out) {
+	return Guard([&] {
+		if (out == nullptr) Fail(VGPU_ERR_INVALID_ARGUMENT, "null result pointer");
+		*out = nullptr;
+		if (n_inputs > 0 && inputs == nullptr) Fail(VGPU_ERR_INVALID_ARGUMENT, "null inputs with nonzero count");
+		auto root = ConvertPlan(plan);
+		ExecOptions eo;
+		cudaStream_t stream = nullptr;
+		if (options) {
+			eo.stage_scan_to_cache = options->stage_scan_to_cache != 0;
+			eo.serve_whole_scan_from_cache = options->serve_whole_scan_from_cache != 0;
+			eo.cache_chunk_index = options->cache_chunk_index;
+			eo.output_on_device = options->output_memory == VGPU_MEM_DEVICE;
+			eo.no_sync = (options->flags & VGPU_EXEC_NO_SYNC) != 0;
+			stream = static_cast<cudaStream_t>(options->stream);
+			if (eo.serve_whole_scan_from_cache && eo.cache_chunk_index >= 0) {
+				Fail(VGPU_ERR_INVALID_ARGUMENT, "serve_whole_scan_from_cache and cache_chunk_index are exclusive");
+			}
+			if (eo.stage_scan_to_cache) {
+				Fail(VGPU_ERR_UNSUPPORTED, "stage_scan_to_cache: stage columns with vgpu_cache_stage_chunk");
+			}
+		}
+		if (stream == nullptr) stream = Runtime::Get().default_stream();
+		std::vector<vgpu_column> in(inputs, inputs + n_inputs);
+		auto *r = new vgpu_result();
+		try {
+			r->exec = ExecutePlan(*root, in, eo, stream);
+		} catch (...) {
+			delete r;
+			throw;
+		}
+		*out = r;
+	});
+}
+
+size_t vgpu_result_column_count(const vgpu_result *result) {
+	return result ? result->exec.columns.size() : 0;
+}
+
+vgpu_status vgpu_result_get_column(const vgpu_result *result, size_t index, vgpu_column *out) {
+	return Guard([&] {
+		if (!result || !out) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		if (index >= result->exec.columns.size()) Fail(VGPU_ERR_INVALID_ARGUMENT, "column index out of range");
+		const HostColumnOut &c = result->exec.columns[index];
+		out->name = c.name.c_str();
+		out->type = static_cast<uint32_t>(c.type);
+		out->row_count = c.rows;
+		if (c.device_data != nullptr) {
+			out->memory = VGPU_MEM_DEVICE;
+			out->data = c.device_data;
+			out->validity = c.device_validity;
+		} else {
+			out->memory = VGPU_MEM_HOST;
+			out->data = c.data.empty() ? nullptr : c.data.data();
+			out->validity = c.validity.empty() ? nullptr : c.validity.data();
+		}
+	});
+}
+
+void vgpu_result_free(vgpu_result *result) {
+	if (!result) return;
+	try {
+		for (void *p : result->exec.device_buffers) {
+			Runtime::Get().allocator().Free(p, result->exec.stream);
+		}
+	} catch (...) {
+	}
+	delete result;
+}
+
+vgpu_status vgpu_set_device(int device) {
+	return Guard([&] { Runtime::Get().SetDevice(device); });
+}
+
+vgpu_status vgpu_get_device_info(vgpu_device_info *out) {
+	return Guard([&] {
+		if (!out) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		const auto &p = Runtime::Get().props();
+		std::memset(out, 0, sizeof(*out));
+		out->device = p.device;
+		out->sm_count = p.sm_count;
+		out->cc_major = p.cc_major;
+		out->cc_minor = p.cc_minor;
+		out->total_memory = p.total_memory;
+		size_t free_b = 0, total_b = 0;
+		VGPU_CUDA(cudaMemGetInfo(&free_b, &total_b));
+		out->free_memory = free_b;
+		out->l2_bytes = p.l2_bytes;
+		out->smem_per_block_optin = p.smem_optin;
+		std::snprintf(out->name, sizeof(out->name), "%s", p.name.c_str());
+	});
+}
+
+vgpu_status vgpu_synchronize(void *stream) {
+	return Guard([&] {
+		cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : Runtime::Get().default_stream();
+		VGPU_CUDA(cudaStreamSynchronize(s));
+	});
+}
+
+vgpu_status vgpu_profile_enable(int enable) {
+	return Guard([&] { Runtime::Get().profiler().Enable(enable != 0); });
+}
+
+vgpu_status vgpu_profile_collect(vgpu_kernel_timing *out, size_t capacity, size_t *count) {
+	return Guard([&] {
+		auto v = Runtime::Get().profiler().Collect();
+		if (count) *count = v.size();
+		for (size_t i = 0; i < v.size() && i < capacity && out; i++) out[i] = v[i];
+	});
+}
+
+uint64_t vgpu_launch_count(void) {
+	return Runtime::Get().launches();
+}
+
+void vgpu_sha256_hex(const void *data, size_t n, char *out) {
+	if (!out) return;
+	std::string h = Sha256Hex(data, data ? n : 0);
+	std::memcpy(out, h.c_str(), 65);
+}
+
+vgpu_status vgpu_kernel_cache_stats_get(vgpu_kernel_cache_stats *out) {
+	return Guard([&] {
+		if (!out) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		*out = Runtime::Get().modules().Stats();
+	});
+}
+
+vgpu_status vgpu_nvrtc_compile_check(const char *source, size_t *cubin_bytes) {
+	return Guard([&] {
+		if (!source) Fail(VGPU_ERR_INVALID_ARGUMENT, "null source");
+		const char *arch = std::getenv("VGPU_NVRTC_ARCH");
+		auto cubin = CompileToCubin(source, arch ? arch : "sm_100a", nullptr);
+		if (cubin_bytes) *cubin_bytes = cubin.size();
+	});
+}
+
+vgpu_status vgpu_generate_source(const vgpu_plan *plan, const vgpu_column *inputs, size_t n_inputs, char *out,
+                                 size_t capacity, size_t *length) {
+	return Guard([&] {
+		auto root = ConvertPlan(plan);
+		std::vector<vgpu_column> in(inputs, inputs + n_inputs);
+		std::string src = GenerateSourceText(*root, in);
+		if (length) *length = src.size();
+		if (out && capacity > 0) {
+			size_t n = std::min(capacity - 1, src.size());
+			std::memcpy(out, src.data(), n);
+			out[n] = '\0';
+		}
+	});
+}
+
+int vgpu_is_row_independent(const vgpu_plan *plan) {
+	try {
+		auto root = ConvertPlan(plan);
+		return IsRowIndependent(*root) ? 1 : 0;
+	} catch (...) {
+		return 0;
+	}
+}
+
+vgpu_status vgpu_estimate_working_set(const vgpu_plan *plan, uint64_t max_chunk_rows, vgpu_working_set *out) {
+	return Guard([&] {
+		if (!out) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		auto root = ConvertPlan(plan);
+		*out = EstimateWorkingSet(*root, max_chunk_rows);
+	});
+}
+
+vgpu_status vgpu_memory_set_budget(uint64_t bytes) {
+	return Guard([&] {
+		Runtime::Get().EnsureDevice();
+		Runtime::Get().allocator().SetBudget(bytes);
+	});
+}
+
+vgpu_status vgpu_memory_stats_get(vgpu_memory_stats *out) {
+	return Guard([&] {
+		if (!out) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		Runtime::Get().EnsureDevice();
+		*out = Runtime::Get().allocator().Stats();
+	});
+}
+
+int vgpu_memory_has_headroom(uint64_t bytes) {
+	try {
+		Runtime::Get().EnsureDevice();
+		return Runtime::Get().allocator().HasHeadroom(bytes) ? 1 : 0;
+	} catch (...) {
+		return 0;
+	}
+}
+
+vgpu_status vgpu_cache_init(double fraction_of_vram) {
+	return Guard([&] { ColumnCache::Get().EnsureInitialized(fraction_of_vram); });
+}
+
+vgpu_status vgpu_cache_begin_staging(const vgpu_table_ref *table) {
+	return Guard([&] { ColumnCache::Get().BeginStaging(ToTable(table)); });
+}
+
+vgpu_status vgpu_cache_stage_chunk(const vgpu_table_ref *table, const vgpu_column *chunk, int *accepted) {
+	return Guard([&] {
+		if (!chunk) Fail(VGPU_ERR_INVALID_ARGUMENT, "null chunk");
+		bool ok = ColumnCache::Get().StageChunk(ToTable(table), *chunk);
+		if (accepted) *accepted = ok ? 1 : 0;
+	});
+}
+
+vgpu_status vgpu_cache_commit_staging(const vgpu_table_ref *table, uint64_t scanned_rows) {
+	return Guard([&] { ColumnCache::Get().CommitStaging(ToTable(table), scanned_rows); });
+}
+
+vgpu_status vgpu_cache_abort_staging(const vgpu_table_ref *table) {
+	return Guard([&] { ColumnCache::Get().AbortStaging(ToTable(table)); });
+}
+
+vgpu_status vgpu_cache_replayable_chunk_rows(const vgpu_table_ref *table, const char *const *column_names,
+                                             size_t n_columns, uint64_t *rows, size_t capacity, size_t *count) {
+	return Guard([&] {
+		std::vector<std::string> cols;
+		for (size_t i = 0; i < n_columns; i++) cols.emplace_back(column_names[i] ? column_names[i] : "");
+		auto v = ColumnCache::Get().ReplayableChunkRows(ToTable(table), cols);
+		if (count) *count = v.size();
+		for (size_t i = 0; i < v.size() && i < capacity && rows; i++) rows[i] = v[i];
+	});
+}
+
+vgpu_status vgpu_cache_try_get_chunk(const vgpu_table_ref *table, const char *column_name, uint64_t chunk_index,
+                                     vgpu_column *out, int *found) {
+	return Guard([&] {
+		if (!out || !column_name) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		DevColumn c;
+		bool ok = ColumnCache::Get().TryGetChunk(ToTable(table), column_name, chunk_index, c);
+		if (found) *found = ok ? 1 : 0;
+		if (ok) {
+			out->name = column_name;
+			out->type = static_cast<uint32_t>(c.type);
+			out->memory = VGPU_MEM_DEVICE;
+			out->data = c.data;
+			out->validity = nullptr; // internal byte masks are not an Arrow bitmap; not exposed
+			out->row_count = c.rows;
+		}
+	});
+}
+
+vgpu_status vgpu_cache_invalidate_table(const vgpu_table_ref *table) {
+	return Guard([&] { ColumnCache::Get().InvalidateTable(ToTable(table)); });
+}
+
+vgpu_status vgpu_cache_invalidate_all(void) {
+	return Guard([&] { ColumnCache::Get().InvalidateAll(); });
+}
+
+uint64_t vgpu_cache_current_bytes(void) {
+	try {
+		return ColumnCache::Get().CurrentBytes();
+	} catch (...) {
+		return 0;
+	}
+}
+
+uint64_t vgpu_cache_table_generation(const vgpu_table_ref *table) {
+	try {
+		return ColumnCache::Get().Generation(ToTable(table));
+	} catch (...) {
+		return 0;
+	}
+}
+
+} // extern "C"

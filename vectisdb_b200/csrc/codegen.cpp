@@ -1,0 +1,886 @@
+// codegen.cpp -- see codegen.hpp.
+#include "codegen.hpp"
+
+#include <algorithm>
+#include <map>
+#include <regex>
+#include <set>
+#include <sstream>
+
+namespace vgpu {
+
+size_t CTypeSize(const std::string &ctype) {
+	static const std::map<std::string, size_t> sizes = {
+	    {"bool", 1},          {"char", 1},          {"signed char", 1},         {"unsigned char", 1},
+	    {"short", 2},         {"unsigned short", 2}, {"int", 4},                {"unsigned int", 4},
+	    {"unsigned", 4},      {"float", 4},         {"long long", 8},           {"unsigned long long", 8},
+	    {"double", 8},        {"long", 8},          {"long long int", 8},       {"short int", 2}};
+	auto it = sizes.find(ctype);
+	return it == sizes.end() ? 0 : it->second;
+}
+
+namespace {
+
+std::string NormalizeCType(std::string t) {
+	// collapse internal whitespace
+	std::string out;
+	bool space = false;
+	for (char c : t) {
+		if (c == ' ' || c == '\t' || c == '\n') {
+			space = !out.empty();
+			continue;
+		}
+		if (space) {
+			out += ' ';
+			space = false;
+		}
+		out += c;
+	}
+	if (out == "long long int") {
+		out = "long long";
+	}
+	if (out == "short int") {
+		out = "short";
+	}
+	if (out == "unsigned") {
+		out = "unsigned int";
+	}
+	if (out == "long") {
+		out = "long long";
+	}
+	return out;
+}
+
+bool ContainsWord(const std::string &s, const std::string &word) {
+	size_t pos = 0;
+	while ((pos = s.find(word, pos)) != std::string::npos) {
+		bool left_ok = pos == 0 || !(std::isalnum(static_cast<unsigned char>(s[pos - 1])) || s[pos - 1] == '_');
+		size_t end = pos + word.size();
+		bool right_ok = end >= s.size() || !(std::isalnum(static_cast<unsigned char>(s[end])) || s[end] == '_');
+		if (left_ok && right_ok) {
+			return true;
+		}
+		pos = end;
+	}
+	return false;
+}
+
+} // namespace
+
+RewrittenExpr RewriteExpression(const std::string &source, size_t n_inputs) {
+	static const std::regex input_re(
+	    R"(\(\s*\(\s*const\s+([A-Za-z_][A-Za-z_0-9 ]*?)\s*\*\s*\)\s*inputs\s*\[\s*(\d+)\s*\]\s*\)\s*\[\s*row\s*\])");
+	static const std::regex output_re(R"(\(\s*\(\s*([A-Za-z_][A-Za-z_0-9 ]*?)\s*\*\s*\)\s*out\s*\)\s*\[\s*idx\s*\])");
+	RewrittenExpr rw;
+	rw.input_ctypes.assign(n_inputs, "");
+	std::string s;
+	{
+		std::string rest = source;
+		std::smatch m;
+		while (std::regex_search(rest, m, input_re)) {
+			size_t index = std::stoul(m[2].str());
+			if (index >= n_inputs) {
+				Fail(VGPU_ERR_INVALID_ARGUMENT, "expression reads inputs[" + std::to_string(index) + "] but lists only " +
+				                                    std::to_string(n_inputs) + " input columns");
+			}
+			std::string ctype = NormalizeCType(m[1].str());
+			if (!rw.input_ctypes[index].empty() && rw.input_ctypes[index] != ctype) {
+				Fail(VGPU_ERR_UNSUPPORTED, "expression reads inputs[" + std::to_string(index) + "] as two different types");
+			}
+			rw.input_ctypes[index] = ctype;
+			s += m.prefix().str();
+			s += "vgpu_in_" + std::to_string(index);
+			rest = m.suffix().str();
+		}
+		s += rest;
+	}
+	std::smatch m;
+	std::string out;
+	int writes = 0;
+	{
+		std::string rest = s;
+		while (std::regex_search(rest, m, output_re)) {
+			std::string ctype = NormalizeCType(m[1].str());
+			if (!rw.output_ctype.empty() && rw.output_ctype != ctype) {
+				Fail(VGPU_ERR_UNSUPPORTED, "expression writes out[] as two different types");
+			}
+			rw.output_ctype = ctype;
+			out += m.prefix().str();
+			out += "vgpu_out";
+			rest = m.suffix().str();
+			writes++;
+		}
+		out += rest;
+	}
+	if (writes == 0) {
+		Fail(VGPU_ERR_UNSUPPORTED, "expression source does not write ((T*)out)[idx]: " + source);
+	}
+	for (const char *word : {"inputs", "out", "row", "idx", "sel", "input_valid", "out_valid"}) {
+		if (ContainsWord(out, word)) {
+			Fail(VGPU_ERR_UNSUPPORTED, std::string("expression source uses '") + word +
+			                               "' outside the ((const T*)inputs[i])[row] / ((T*)out)[idx] forms: " +
+			                               source);
+		}
+	}
+	if (CTypeSize(rw.output_ctype) == 0) {
+		Fail(VGPU_ERR_UNSUPPORTED, "expression writes an unsupported C type '" + rw.output_ctype + "'");
+	}
+	for (auto &t : rw.input_ctypes) {
+		if (!t.empty() && CTypeSize(t) == 0) {
+			Fail(VGPU_ERR_UNSUPPORTED, "expression reads an unsupported C type '" + t + "'");
+		}
+	}
+	rw.statement = out;
+	return rw;
+}
+
+// ============================================================================================
+// PipelineCodegen
+
+PipelineCodegen::PipelineCodegen(const PipelineSpec &spec) : spec_(spec) {
+	for (auto &src : spec_.sources) {
+		if (src.type == ValueType::HUGEINT) {
+			Fail(VGPU_ERR_UNSUPPORTED, "column '" + src.name + "': HUGEINT columns cannot feed a fused pipeline");
+		}
+	}
+	Resolve();
+}
+
+int PipelineCodegen::FindVisible(const std::string &name) const {
+	for (size_t i = 0; i < visible_.size(); i++) {
+		if (visible_[i].name == name) {
+			return static_cast<int>(i);
+		}
+	}
+	return -1;
+}
+
+std::string PipelineCodegen::EmitExpression(const Expr &expr, const std::vector<PipeColumn> &cols, int k) {
+	RewrittenExpr rw = RewriteExpression(expr.source, expr.input_columns.size());
+	std::ostringstream o;
+	const char *out_c = CudaTypeName(expr.output_type);
+	if (expr.output_type == ValueType::HUGEINT) {
+		Fail(VGPU_ERR_UNSUPPORTED, "expressions producing HUGEINT are not supported");
+	}
+	if (CTypeSize(rw.output_ctype) != TypeSize(expr.output_type)) {
+		Fail(VGPU_ERR_UNSUPPORTED, "expression writes " + rw.output_ctype + " into a " + TypeName(expr.output_type) +
+		                               " result");
+	}
+	o << "\t\t" << out_c << " e" << k << ";\n\t\t{\n";
+	std::vector<std::string> valids;
+	for (size_t i = 0; i < expr.input_columns.size(); i++) {
+		if (rw.input_ctypes[i].empty()) {
+			continue;
+		}
+		const std::string &name = expr.input_columns[i];
+		const PipeColumn *col = nullptr;
+		for (auto &c : cols) {
+			if (c.name == name) {
+				col = &c;
+				break;
+			}
+		}
+		if (!col) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: expression input column '" + name + "' not found");
+		}
+		if (CTypeSize(rw.input_ctypes[i]) != TypeSize(col->type)) {
+			Fail(VGPU_ERR_UNSUPPORTED, "expression reads column '" + name + "' (" + TypeName(col->type) + ") as " +
+			                               rw.input_ctypes[i]);
+		}
+		o << "\t\t\tconst " << rw.input_ctypes[i] << " vgpu_in_" << i << " = vgpu_dev::reinterpret_value<"
+		  << rw.input_ctypes[i] << ", " << CudaTypeName(col->type) << ">(" << col->value << ");\n";
+		if (col->nullable) {
+			valids.push_back("(" + col->valid + ")");
+		}
+	}
+	o << "\t\t\t" << rw.output_ctype << " vgpu_out;\n";
+	o << "\t\t\t" << rw.statement << "\n";
+	o << "\t\t\te" << k << " = vgpu_dev::reinterpret_value<" << out_c << ", " << rw.output_ctype << ">(vgpu_out);\n";
+	o << "\t\t}\n";
+	o << "\t\tconst bool ev" << k << " = ";
+	if (valids.empty()) {
+		o << "true";
+	} else {
+		for (size_t i = 0; i < valids.size(); i++) {
+			o << (i ? " && " : "") << valids[i];
+		}
+	}
+	o << ";\n";
+	return o.str();
+}
+
+void PipelineCodegen::Resolve() {
+	std::vector<PipeColumn> cols;
+	for (size_t i = 0; i < spec_.sources.size(); i++) {
+		PipeColumn c;
+		c.name = spec_.sources[i].name;
+		c.type = spec_.sources[i].type;
+		c.source = static_cast<int>(i);
+		c.value = "s" + std::to_string(i) + "[r]";
+		c.nullable = spec_.sources[i].nullable;
+		c.valid = c.nullable ? "sv" + std::to_string(i) + "[r]" : "true";
+		cols.push_back(c);
+	}
+	chain_sources_.assign(spec_.sources.size(), false);
+	std::ostringstream code;
+	// Sources read by each visible column (transitively through projections).
+	std::vector<std::set<int>> deps(cols.size());
+	for (size_t i = 0; i < cols.size(); i++) {
+		deps[i].insert(static_cast<int>(i));
+	}
+	for (const PlanNode *node : spec_.chain) {
+		if (node->op == OpType::FILTER) {
+			for (auto &expr : node->expressions) {
+				if (expr.output_type != ValueType::BOOLEAN) {
+					Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: FILTER predicate did not evaluate to BOOLEAN");
+				}
+				int k = expr_count_++;
+				code << EmitExpression(expr, cols, k);
+				code << "\t\tkeep = keep && ev" << k << " && e" << k << ";\n";
+				for (auto &in : expr.input_columns) {
+					for (size_t c = 0; c < cols.size(); c++) {
+						if (cols[c].name == in) {
+							for (int s : deps[c]) {
+								chain_sources_[s] = true;
+							}
+							break;
+						}
+					}
+				}
+			}
+			if (!node->expressions.empty()) {
+				has_filter_ = true;
+			}
+		} else if (node->op == OpType::PROJECTION) {
+			std::vector<PipeColumn> next;
+			std::vector<std::set<int>> next_deps;
+			for (size_t i = 0; i < node->expressions.size(); i++) {
+				auto &expr = node->expressions[i];
+				int k = expr_count_++;
+				code << EmitExpression(expr, cols, k);
+				PipeColumn c;
+				c.name = "col" + std::to_string(i);
+				c.type = expr.output_type;
+				c.value = "e" + std::to_string(k);
+				c.valid = "ev" + std::to_string(k);
+				std::set<int> d;
+				bool nullable = false;
+				for (auto &in : expr.input_columns) {
+					for (size_t cc = 0; cc < cols.size(); cc++) {
+						if (cols[cc].name == in) {
+							d.insert(deps[cc].begin(), deps[cc].end());
+							nullable |= cols[cc].nullable;
+							break;
+						}
+					}
+				}
+				c.nullable = nullable;
+				if (!nullable) {
+					c.valid = "true";
+				}
+				next.push_back(c);
+				next_deps.push_back(d);
+			}
+			cols = std::move(next);
+			deps = std::move(next_deps);
+		} else {
+			Fail(VGPU_ERR_INTERNAL, "pipeline chain may hold only FILTER/PROJECTION nodes");
+		}
+	}
+	visible_ = cols;
+	chain_uses_.clear();
+	for (auto &d : deps) {
+		chain_uses_.emplace_back(d.begin(), d.end());
+	}
+	chain_code_ = code.str();
+}
+
+std::vector<bool> PipelineCodegen::NeededSources(const std::vector<int> &extra_columns) const {
+	std::vector<bool> needed = chain_sources_;
+	for (int c : extra_columns) {
+		for (int s : chain_uses_[c]) {
+			needed[s] = true;
+		}
+	}
+	return needed;
+}
+
+std::string PipelineCodegen::Prologue() const {
+	return "#include \"vgpu_device_lib.cuh\"\n"
+	       "using namespace vgpu_dev;\n"
+	       "__device__ __forceinline__ double __vgpu_radians(double d) { return d * 0.017453292519943295; }\n"
+	       "__device__ __forceinline__ double __vgpu_degrees(double r) { return r * 57.29577951308232; }\n";
+}
+
+std::string PipelineCodegen::LoadBlock(const Geometry &g, const std::vector<bool> &needed, bool chunked) const {
+	(void)chunked;
+	std::ostringstream o;
+	o << "\t\tconst u64 row0 = tile * (u64)" << g.tile() << " + (u64)threadIdx.x * " << g.items << ";\n";
+	if (spec_.cross) {
+		o << "\t\tu64 li[" << g.items << "], rj[" << g.items << "];\n";
+		o << "\t\t{ u64 i0 = row0 / m; u64 j0 = row0 - i0 * m;\n";
+		o << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items
+		  << "; ++r) { li[r] = i0; rj[r] = j0; if (++j0 == m) { j0 = 0; ++i0; } } }\n";
+	}
+	for (size_t i = 0; i < spec_.sources.size(); i++) {
+		if (!needed[i]) {
+			continue;
+		}
+		const auto &src = spec_.sources[i];
+		const char *t = CudaTypeName(src.type);
+		const int w = 2 + 2 * static_cast<int>(i);
+		o << "\t\t" << t << " s" << i << "[" << g.items << "];\n";
+		if (src.nullable) {
+			o << "\t\tbool sv" << i << "[" << g.items << "];\n";
+		}
+		if (!spec_.cross) {
+			o << "\t\tload_rows<" << t << ", " << g.items << ">((const " << t << "*)a.w[" << w << "], row0, n, s" << i
+			  << ");\n";
+			if (src.nullable) {
+				o << "\t\tload_valid<" << g.items << ">((const u8*)a.w[" << w + 1 << "], row0, n, sv" << i << ");\n";
+			}
+		} else {
+			const char *idx = src.side == 0 ? "li[r]" : "rj[r]";
+			o << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) {\n";
+			o << "\t\t\ts" << i << "[r] = (row0 + r < n) ? ((const " << t << "*)a.w[" << w << "])[" << idx << "] : ("
+			  << t << ")0;\n";
+			if (src.nullable) {
+				o << "\t\t\tsv" << i << "[r] = (row0 + r < n) ? (((const u8*)a.w[" << w + 1 << "])[" << idx
+				  << "] != 0) : false;\n";
+			}
+			o << "\t\t}\n";
+		}
+	}
+	return o.str();
+}
+
+namespace {
+
+const char *kKernelHead = "\tconst u64 n = a.w[0];\n\tconst u64 m = a.w[1];\n\t(void)m;\n";
+
+} // namespace
+
+std::string PipelineCodegen::EmitMaterialize(const std::vector<int> &outs, const Geometry &g) const {
+	std::ostringstream o;
+	o << Prologue();
+	const int cb = ConsumerBase();
+	std::vector<int> out_cols = outs;
+	auto needed = NeededSources(out_cols);
+	const std::string loads = LoadBlock(g, needed, false);
+	if (has_filter_) {
+		o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_mat_count(KArgs a) {\n"
+		  << kKernelHead << "\t__shared__ u32 scan_scratch[33];\n"
+		  << "\tu32 *tile_counts = (u32*)a.w[" << cb << "];\n"
+		  << "\tconst u64 ntiles = (n + " << g.tile() - 1 << ") / " << g.tile() << ";\n"
+		  << "\tfor (u64 tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n"
+		  << LoadBlock(g, NeededSources({}), false) << "\t\tu32 cnt = 0;\n"
+		  << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) {\n"
+		  << "\t\tconst u64 row = row0 + r; (void)row;\n\t\tbool keep = row < n;\n"
+		  << chain_code_ << "\t\tcnt += keep ? 1u : 0u;\n\t\t}\n"
+		  << "\t\tu32 total; block_exclusive_scan(cnt, scan_scratch, &total);\n"
+		  << "\t\tif (threadIdx.x == 0) tile_counts[tile] = total;\n\t}\n}\n\n";
+	}
+	o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_mat_write(KArgs a) {\n"
+	  << kKernelHead << "\t__shared__ u32 scan_scratch[33];\n"
+	  << "\tconst u32 *tile_offsets = (const u32*)a.w[" << cb << "]; (void)tile_offsets;\n"
+	  << "\tconst u64 ntiles = (n + " << g.tile() - 1 << ") / " << g.tile() << ";\n"
+	  << "\tfor (u64 tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n"
+	  << loads << "\t\tbool kv[" << g.items << "];\n";
+	for (size_t c = 0; c < out_cols.size(); c++) {
+		const auto &col = visible_[out_cols[c]];
+		o << "\t\t" << CudaTypeName(col.type) << " o" << c << "[" << g.items << "];\n";
+		if (col.nullable) {
+			o << "\t\tbool ov" << c << "[" << g.items << "];\n";
+		}
+	}
+	o << "\t\tu32 cnt = 0;\n\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) {\n"
+	  << "\t\tconst u64 row = row0 + r; (void)row;\n\t\tbool keep = row < n;\n"
+	  << chain_code_ << "\t\tkv[r] = keep;\n\t\tcnt += keep ? 1u : 0u;\n";
+	for (size_t c = 0; c < out_cols.size(); c++) {
+		const auto &col = visible_[out_cols[c]];
+		o << "\t\to" << c << "[r] = " << col.value << ";\n";
+		if (col.nullable) {
+			o << "\t\tov" << c << "[r] = " << col.valid << ";\n";
+		}
+	}
+	o << "\t\t}\n";
+	if (has_filter_) {
+		o << "\t\tu32 total; u32 pos = block_exclusive_scan(cnt, scan_scratch, &total) + tile_offsets[tile];\n";
+	} else {
+		o << "\t\tu64 pos = row0;\n";
+	}
+	o << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) {\n\t\t\tif (kv[r]) {\n";
+	for (size_t c = 0; c < out_cols.size(); c++) {
+		const auto &col = visible_[out_cols[c]];
+		int w = cb + 1 + 2 * static_cast<int>(c);
+		o << "\t\t\t\t((" << CudaTypeName(col.type) << "*)a.w[" << w << "])[pos] = o" << c << "[r];\n";
+		if (col.nullable) {
+			o << "\t\t\t\tif (a.w[" << w + 1 << "]) ((u8*)a.w[" << w + 1 << "])[pos] = ov" << c << "[r] ? 1 : 0;\n";
+		}
+	}
+	if (has_filter_) {
+		o << "\t\t\t\t++pos;\n\t\t\t}\n";
+	} else {
+		o << "\t\t\t}\n\t\t\t++pos;\n";
+	}
+	o << "\t\t}\n\t}\n}\n";
+	return o.str();
+}
+
+std::string PipelineCodegen::EmitStats(const std::vector<int> &columns, const Geometry &g) const {
+	std::ostringstream o;
+	o << Prologue();
+	const int cb = ConsumerBase();
+	auto needed = NeededSources(columns);
+	// Predicates are not applied: the bound must hold for every row the consumer could see, and a
+	// superset bound is still a valid one.
+	std::vector<bool> load_needed(spec_.sources.size(), false);
+	for (int c : columns) {
+		for (int s : chain_uses_[c]) {
+			load_needed[s] = true;
+		}
+	}
+	// The chain code may reference any source the chain touches; load those too.
+	for (size_t i = 0; i < load_needed.size(); i++) {
+		load_needed[i] = load_needed[i] || needed[i];
+	}
+	o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_stats(KArgs a) {\n" << kKernelHead;
+	for (size_t c = 0; c < columns.size(); c++) {
+		o << "\ti64 mn" << c << " = 0x7fffffffffffffffLL, mx" << c << " = (-0x7fffffffffffffffLL - 1);\n";
+	}
+	o << "\tconst u64 ntiles = (n + " << g.tile() - 1 << ") / " << g.tile() << ";\n"
+	  << "\tfor (u64 tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n"
+	  << LoadBlock(g, load_needed, false) << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) {\n"
+	  << "\t\tconst u64 row = row0 + r; (void)row;\n\t\tbool keep = row < n;\n"
+	  << chain_code_ << "\t\tif (row < n) {\n";
+	for (size_t c = 0; c < columns.size(); c++) {
+		const auto &col = visible_[columns[c]];
+		o << "\t\t\t{ const i64 x = (i64)(" << col.value << "); mn" << c << " = x < mn" << c << " ? x : mn" << c
+		  << "; mx" << c << " = x > mx" << c << " ? x : mx" << c << "; }\n";
+	}
+	o << "\t\t}\n\t\t}\n\t}\n";
+	for (size_t c = 0; c < columns.size(); c++) {
+		o << "\tfor (int off = 16; off > 0; off >>= 1) {\n"
+		  << "\t\ti64 a1 = __shfl_xor_sync(0xffffffffu, mn" << c << ", off); mn" << c << " = a1 < mn" << c << " ? a1 : mn"
+		  << c << ";\n"
+		  << "\t\ti64 b1 = __shfl_xor_sync(0xffffffffu, mx" << c << ", off); mx" << c << " = b1 > mx" << c << " ? b1 : mx"
+		  << c << ";\n\t}\n"
+		  << "\tif ((threadIdx.x & 31) == 0) { atomic_min_i64((i64*)a.w[" << cb + 2 * c << "], mn" << c
+		  << "); atomic_max_i64((i64*)a.w[" << cb + 2 * c + 1 << "], mx" << c << "); }\n";
+	}
+	o << "}\n";
+	return o.str();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Group-by
+
+namespace {
+
+struct Field {
+	std::string kind; // "cnt", "f64", "lo", "hi", "min", "max"
+	int agg = -1;
+};
+
+std::vector<Field> StateFields(const PipelineCodegen::GroupBySpec &gb) {
+	std::vector<Field> f;
+	f.push_back({"cnt", -1});
+	for (size_t i = 0; i < gb.aggs.size(); i++) {
+		auto &a = gb.aggs[i];
+		int ai = static_cast<int>(i);
+		switch (a.kind) {
+		case AggKind::COUNT_STAR:
+		case AggKind::COUNT:
+			break;
+		case AggKind::SUM:
+		case AggKind::AVG:
+			if (IsFloatType(a.input_type)) {
+				f.push_back({"f64", ai});
+			} else {
+				f.push_back({"lo", ai});
+				f.push_back({"hi", ai});
+			}
+			break;
+		case AggKind::MIN:
+			f.push_back({"min", ai});
+			break;
+		case AggKind::MAX:
+			f.push_back({"max", ai});
+			break;
+		}
+	}
+	return f;
+}
+
+int FieldIndex(const std::vector<Field> &fields, const std::string &kind, int agg) {
+	for (size_t i = 0; i < fields.size(); i++) {
+		if (fields[i].kind == kind && fields[i].agg == agg) {
+			return static_cast<int>(i);
+		}
+	}
+	return -1;
+}
+
+std::string InitValue(const Field &f) {
+	if (f.kind == "min") {
+		return "0x7fffffffffffffffull";
+	}
+	if (f.kind == "max") {
+		return "0x8000000000000000ull";
+	}
+	return "0ull"; // cnt, f64 (+0.0 bit pattern), lo, hi
+}
+
+// Update of table T (u64 arrays T_f at slot S) with the value expression `v` of aggregate field f.
+std::string UpdateCode(const std::vector<Field> &fields, const std::string &tab, const std::string &slot,
+                       const std::vector<std::string> &agg_values) {
+	std::ostringstream o;
+	for (size_t i = 0; i < fields.size(); i++) {
+		auto &f = fields[i];
+		std::string p = tab + std::to_string(i) + " + " + slot;
+		if (f.kind == "cnt") {
+			o << "\t\t\tatomicAdd(" << p << ", 1ull);\n";
+		} else if (f.kind == "f64") {
+			o << "\t\t\tatomicAdd((double*)(" << p << "), (double)(" << agg_values[f.agg] << "));\n";
+		} else if (f.kind == "lo") {
+			std::string phi = tab + std::to_string(i + 1) + " + " + slot;
+			o << "\t\t\tatomic_add_i128(" << p << ", (i64*)(" << phi << "), (i64)(" << agg_values[f.agg] << "));\n";
+		} else if (f.kind == "min") {
+			o << "\t\t\tatomic_min_i64((i64*)(" << p << "), (i64)(" << agg_values[f.agg] << "));\n";
+		} else if (f.kind == "max") {
+			o << "\t\t\tatomic_max_i64((i64*)(" << p << "), (i64)(" << agg_values[f.agg] << "));\n";
+		}
+	}
+	return o.str();
+}
+
+// Merge of source table slot into destination table slot (both u64 field arrays).
+std::string MergeCode(const std::vector<Field> &fields, const std::string &src, const std::string &ss,
+                      const std::string &dst, const std::string &ds) {
+	std::ostringstream o;
+	for (size_t i = 0; i < fields.size(); i++) {
+		auto &f = fields[i];
+		std::string ps = src + std::to_string(i) + "[" + ss + "]";
+		std::string pd = dst + std::to_string(i) + " + " + ds;
+		if (f.kind == "cnt") {
+			o << "\t\t\tatomicAdd(" << pd << ", " << ps << ");\n";
+		} else if (f.kind == "f64") {
+			o << "\t\t\tatomicAdd((double*)(" << pd << "), __longlong_as_double((i64)" << ps << "));\n";
+		} else if (f.kind == "lo") {
+			std::string ps_hi = src + std::to_string(i + 1) + "[" + ss + "]";
+			std::string pd_hi = dst + std::to_string(i + 1) + " + " + ds;
+			o << "\t\t\tatomic_add_i128_pair(" << pd << ", (i64*)(" << pd_hi << "), " << ps << ", (i64)" << ps_hi
+			  << ");\n";
+		} else if (f.kind == "min") {
+			o << "\t\t\tatomic_min_i64((i64*)(" << pd << "), (i64)" << ps << ");\n";
+		} else if (f.kind == "max") {
+			o << "\t\t\tatomic_max_i64((i64*)(" << pd << "), (i64)" << ps << ");\n";
+		}
+	}
+	return o.str();
+}
+
+// Writes the finalized outputs of one group from table T slot `s` to output row `pos`.
+// Outputs start at word `out_base`: keys first, then aggregates (HUGEINT outputs are 16 bytes/row).
+std::string FinalizeCode(const PipelineCodegen::GroupBySpec &gb, const std::vector<Field> &fields,
+                         const std::vector<PipeColumn> &visible, const std::string &tab, const std::string &s,
+                         const std::string &key, const std::string &pos, int out_base) {
+	std::ostringstream o;
+	int w = out_base;
+	for (auto &k : gb.keys) {
+		const auto &col = visible[k.column];
+		const char *t = CudaTypeName(col.type);
+		u_int64_t mask = k.bits >= 64 ? ~0ull : ((1ull << k.bits) - 1);
+		o << "\t\t\t((" << t << "*)a.w[" << w << "])[" << pos << "] = (" << t << ")((i64)((" << key << " >> " << k.shift
+		  << ") & 0x" << std::hex << mask << std::dec << "ull) + (" << k.min << "LL));\n";
+		w++;
+	}
+	const std::string cnt = tab + "0[" + s + "]";
+	for (size_t i = 0; i < gb.aggs.size(); i++) {
+		auto &a = gb.aggs[i];
+		int ai = static_cast<int>(i);
+		std::string out = "a.w[" + std::to_string(w) + "]";
+		switch (a.kind) {
+		case AggKind::COUNT_STAR:
+		case AggKind::COUNT:
+			o << "\t\t\t((i64*)" << out << ")[" << pos << "] = (i64)" << cnt << ";\n";
+			break;
+		case AggKind::SUM:
+		case AggKind::AVG: {
+			bool avg = a.kind == AggKind::AVG;
+			if (IsFloatType(a.input_type)) {
+				int f = FieldIndex(fields, "f64", ai);
+				std::string sum = "__longlong_as_double((i64)" + tab + std::to_string(f) + "[" + s + "])";
+				if (avg) {
+					o << "\t\t\t((double*)" << out << ")[" << pos << "] = " << sum << " / (double)" << cnt << ";\n";
+				} else {
+					o << "\t\t\t((double*)" << out << ")[" << pos << "] = " << sum << ";\n";
+				}
+			} else {
+				int f = FieldIndex(fields, "lo", ai);
+				std::string lo = tab + std::to_string(f) + "[" + s + "]";
+				std::string hi = "(i64)" + tab + std::to_string(f + 1) + "[" + s + "]";
+				if (avg) {
+					o << "\t\t\t((double*)" << out << ")[" << pos << "] = i128_to_double(" << lo << ", " << hi
+					  << ") / (double)" << cnt << ";\n";
+				} else if (a.output_type == ValueType::HUGEINT) {
+					o << "\t\t\t((u64*)" << out << ")[2 * (" << pos << ")] = " << lo << ";\n";
+					o << "\t\t\t((u64*)" << out << ")[2 * (" << pos << ") + 1] = (u64)" << hi << ";\n";
+				} else {
+					o << "\t\t\t((double*)" << out << ")[" << pos << "] = i128_to_double(" << lo << ", " << hi << ");\n";
+				}
+			}
+			break;
+		}
+		case AggKind::MIN:
+		case AggKind::MAX: {
+			int f = FieldIndex(fields, a.kind == AggKind::MIN ? "min" : "max", ai);
+			const char *t = CudaTypeName(a.output_type);
+			o << "\t\t\t((" << t << "*)" << out << ")[" << pos << "] = (" << t << ")(i64)" << tab << f << "[" << s << "];\n";
+			break;
+		}
+		}
+		w++;
+	}
+	return o.str();
+}
+
+} // namespace
+
+int PipelineCodegen::StateWords(const GroupBySpec &gb) {
+	return static_cast<int>(StateFields(gb).size());
+}
+
+std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned, const Geometry &g) const {
+	std::ostringstream o;
+	o << Prologue();
+	const int cb = ConsumerBase();
+	const auto fields = StateFields(gb);
+	const int F = static_cast<int>(fields.size());
+	// Columns the consumer reads: keys and aggregate inputs.
+	std::vector<int> used;
+	for (auto &k : gb.keys) {
+		used.push_back(k.column);
+	}
+	for (auto &a : gb.aggs) {
+		if (a.column >= 0) {
+			used.push_back(a.column);
+		}
+	}
+	auto needed = NeededSources(used);
+	// Distinct aggregate input columns (the values a partitioned scatter carries).
+	std::vector<int> value_cols;
+	for (auto &a : gb.aggs) {
+		if (a.column >= 0 && (a.kind != AggKind::COUNT && a.kind != AggKind::COUNT_STAR) &&
+		    std::find(value_cols.begin(), value_cols.end(), a.column) == value_cols.end()) {
+			value_cols.push_back(a.column);
+		}
+	}
+	std::ostringstream pack;
+	pack << "(0ull";
+	for (auto &k : gb.keys) {
+		pack << " | ((u64)((i64)(" << visible_[k.column].value << ") - (" << k.min << "LL)) << " << k.shift << ")";
+	}
+	pack << ")";
+	auto value_of = [&](int agg_index, bool from_partition) -> std::string {
+		const auto &a = gb.aggs[agg_index];
+		if (a.column < 0) {
+			return "0";
+		}
+		if (!from_partition) {
+			return visible_[a.column].value;
+		}
+		int vi = static_cast<int>(std::find(value_cols.begin(), value_cols.end(), a.column) - value_cols.begin());
+		return "((const " + std::string(CudaTypeName(visible_[a.column].type)) + "*)vin" + std::to_string(vi) + ")[i]";
+	};
+	std::vector<std::string> pipe_values, part_values;
+	for (size_t i = 0; i < gb.aggs.size(); i++) {
+		pipe_values.push_back(value_of(static_cast<int>(i), false));
+		part_values.push_back(value_of(static_cast<int>(i), true));
+	}
+	const std::string tile_loop_head = "\tconst u64 ntiles = (n + " + std::to_string(g.tile() - 1) + ") / " +
+	                                   std::to_string(g.tile()) + ";\n";
+	const std::string item_head = "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " + std::to_string(g.items) +
+	                              "; ++r) {\n\t\tconst u64 row = row0 + r; (void)row;\n\t\tbool keep = row < n;\n";
+	const int out_words = static_cast<int>(gb.keys.size() + gb.aggs.size());
+
+	if (!partitioned) {
+		// ---- direct: packed key is the slot of a dense table of `domain` groups ----
+		// args: cb+0 = D, cb+1+f = global field arrays, then (final) outputs, then count ptr.
+		o << "extern \"C\" __global__ void vgpu_gb_direct_init(KArgs a) {\n"
+		  << "\tconst u64 D = a.w[" << cb << "];\n"
+		  << "\tfor (u64 s = blockIdx.x * (u64)blockDim.x + threadIdx.x; s < D; s += (u64)gridDim.x * blockDim.x) {\n";
+		for (int f = 0; f < F; f++) {
+			o << "\t\t((u64*)a.w[" << cb + 1 + f << "])[s] = " << InitValue(fields[f]) << ";\n";
+		}
+		o << "\t}\n}\n\n";
+		o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_gb_direct(KArgs a) {\n"
+		  << kKernelHead << "\textern __shared__ __align__(16) u64 vgpu_smem[];\n"
+		  << "\tconst u64 D = a.w[" << cb << "];\n";
+		for (int f = 0; f < F; f++) {
+			o << "\tu64 *T" << f << " = vgpu_smem + " << f << " * D;\n";
+		}
+		o << "\tfor (u64 s = threadIdx.x; s < D; s += " << g.block << ") {\n";
+		for (int f = 0; f < F; f++) {
+			o << "\t\tT" << f << "[s] = " << InitValue(fields[f]) << ";\n";
+		}
+		o << "\t}\n\t__syncthreads();\n" << tile_loop_head
+		  << "\tfor (u64 tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n"
+		  << LoadBlock(g, needed, false) << item_head << chain_code_ << "\t\tif (keep) {\n"
+		  << "\t\t\tconst u64 slot = " << pack.str() << ";\n"
+		  << UpdateCode(fields, "T", "slot", pipe_values) << "\t\t}\n\t\t}\n\t}\n\t__syncthreads();\n";
+		for (int f = 0; f < F; f++) {
+			o << "\tu64 *G" << f << " = (u64*)a.w[" << cb + 1 + f << "];\n";
+		}
+		o << "\tfor (u64 s = threadIdx.x; s < D; s += " << g.block << ") {\n\t\tif (T0[s] != 0) {\n"
+		  << MergeCode(fields, "T", "s", "G", "s") << "\t\t}\n\t}\n}\n\n";
+		// final: one CTA compacts the non-empty groups in key order
+		o << "extern \"C\" __global__ void vgpu_gb_direct_final(KArgs a) {\n"
+		  << "\t__shared__ u32 scan_scratch[33];\n"
+		  << "\tconst u64 D = a.w[" << cb << "];\n";
+		for (int f = 0; f < F; f++) {
+			o << "\tconst u64 *G" << f << " = (const u64*)a.w[" << cb + 1 + f << "];\n";
+		}
+		o << "\tu64 base = 0;\n"
+		  << "\tfor (u64 c0 = 0; c0 < D; c0 += blockDim.x) {\n"
+		  << "\t\tconst u64 s = c0 + threadIdx.x;\n"
+		  << "\t\tconst bool live = s < D && G0[s] != 0;\n"
+		  << "\t\tu32 total; const u32 off = block_exclusive_scan(live ? 1u : 0u, scan_scratch, &total);\n"
+		  << "\t\tif (live) {\n\t\t\tconst u64 pos = base + off;\n\t\t\tconst u64 key = s;\n"
+		  << FinalizeCode(gb, fields, visible_, "G", "s", "key", "pos", cb + 1 + F) << "\t\t}\n"
+		  << "\t\tbase += total;\n\t}\n"
+		  << "\tif (threadIdx.x == 0) *(u64*)a.w[" << cb + 1 + F + out_words << "] = base;\n}\n";
+		return o.str();
+	}
+
+	// ---- partitioned: radix partition on the mixed key, then one hash table per partition ----
+	// part_count / part_scatter args: cb+0 = P, cb+1 = pbits, cb+2 = tiles per CTA,
+	//   cb+3 = counts/offsets (u32, [p * G + cta]), cb+4 = keys out (u64), cb+5+v = value columns out.
+	o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_gb_part_count(KArgs a) {\n"
+	  << kKernelHead << "\textern __shared__ __align__(16) u32 vgpu_hist[];\n"
+	  << "\tconst u32 P = (u32)a.w[" << cb << "]; const int pbits = (int)a.w[" << cb + 1 << "];\n"
+	  << "\tconst u64 tpc = a.w[" << cb + 2 << "];\n"
+	  << "\tfor (u32 p = threadIdx.x; p < P; p += " << g.block << ") vgpu_hist[p] = 0;\n\t__syncthreads();\n"
+	  << tile_loop_head
+	  << "\tconst u64 t_end = (blockIdx.x + 1) * tpc < ntiles ? (blockIdx.x + 1) * tpc : ntiles;\n"
+	  << "\tfor (u64 tile = blockIdx.x * tpc; tile < t_end; ++tile) {\n"
+	  << LoadBlock(g, needed, true) << item_head << chain_code_ << "\t\tif (keep) {\n"
+	  << "\t\t\tatomicAdd(&vgpu_hist[partition_of(" << pack.str() << ", pbits)], 1u);\n"
+	  << "\t\t}\n\t\t}\n\t}\n\t__syncthreads();\n"
+	  << "\tu32 *counts = (u32*)a.w[" << cb + 3 << "];\n"
+	  << "\tfor (u32 p = threadIdx.x; p < P; p += " << g.block << ") counts[(u64)p * gridDim.x + blockIdx.x] = vgpu_hist[p];\n}\n\n";
+
+	o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_gb_part_scatter(KArgs a) {\n"
+	  << kKernelHead << "\textern __shared__ __align__(16) u32 vgpu_cursor[];\n"
+	  << "\tconst u32 P = (u32)a.w[" << cb << "]; const int pbits = (int)a.w[" << cb + 1 << "];\n"
+	  << "\tconst u64 tpc = a.w[" << cb + 2 << "];\n"
+	  << "\tconst u32 *offsets = (const u32*)a.w[" << cb + 3 << "];\n"
+	  << "\tu64 *keys_out = (u64*)a.w[" << cb + 4 << "];\n"
+	  << "\tfor (u32 p = threadIdx.x; p < P; p += " << g.block
+	  << ") vgpu_cursor[p] = offsets[(u64)p * gridDim.x + blockIdx.x];\n\t__syncthreads();\n"
+	  << tile_loop_head
+	  << "\tconst u64 t_end = (blockIdx.x + 1) * tpc < ntiles ? (blockIdx.x + 1) * tpc : ntiles;\n"
+	  << "\tfor (u64 tile = blockIdx.x * tpc; tile < t_end; ++tile) {\n"
+	  << LoadBlock(g, needed, true) << item_head << chain_code_ << "\t\tif (keep) {\n"
+	  << "\t\t\tconst u64 key = " << pack.str() << ";\n"
+	  << "\t\t\tconst u32 pos = atomicAdd(&vgpu_cursor[partition_of(key, pbits)], 1u);\n"
+	  << "\t\t\tkeys_out[pos] = key;\n";
+	for (size_t v = 0; v < value_cols.size(); v++) {
+		const auto &col = visible_[value_cols[v]];
+		o << "\t\t\t((" << CudaTypeName(col.type) << "*)a.w[" << cb + 5 + v << "])[pos] = " << col.value << ";\n";
+	}
+	o << "\t\t}\n\t\t}\n\t}\n}\n\n";
+
+	// bucket: args cb+0 = P, cb+1 = C (smem table slots), cb+2 = offsets (u32 [p*G]), cb+3 = G,
+	//   cb+4 = total ptr (u32*), cb+5 = keys in, cb+6+v = value columns in, then
+	//   W = cb+6+V: work counter (u32*), W+1 overflow flags (u32 [P]), W+2 overflow count (u32*),
+	//   W+3 output count (u64*), W+4.. outputs. Global-table variant: W+4+outs = partition list (u32*),
+	//   +1 list length, +2 table base (u64*), +3 per-list-entry table offsets (u64*), +4 capacities (u32*).
+	const int V = static_cast<int>(value_cols.size());
+	const int W = cb + 6 + V;
+	const int OUT = W + 4;
+	o << "__device__ __forceinline__ void vgpu_bucket_process(const KArgs &a, u32 p, u64 *tab, u32 C, bool *overflow) {\n"
+	  << "\tconst u32 P = (u32)a.w[" << cb << "];\n"
+	  << "\tconst u32 *offsets = (const u32*)a.w[" << cb + 2 << "];\n"
+	  << "\tconst u64 G = a.w[" << cb + 3 << "];\n"
+	  << "\tconst u32 total_rows = *(const u32*)a.w[" << cb + 4 << "];\n"
+	  << "\tconst u64 *keys_in = (const u64*)a.w[" << cb + 5 << "];\n";
+	for (int v = 0; v < V; v++) {
+		o << "\tconst void *vin" << v << " = (const void*)a.w[" << cb + 6 + v << "];\n";
+	}
+	o << "\tconst u32 start = offsets[(u64)p * G];\n"
+	  << "\tconst u32 end = (p + 1 < P) ? offsets[(u64)(p + 1) * G] : total_rows;\n"
+	  << "\tu64 *K = tab;\n";
+	for (int f = 0; f < F; f++) {
+		o << "\tu64 *T" << f << " = tab + (u64)" << f + 1 << " * C;\n";
+	}
+	o << "\tfor (u32 s = threadIdx.x; s < C; s += blockDim.x) {\n\t\tK[s] = ~0ull;\n";
+	for (int f = 0; f < F; f++) {
+		o << "\t\tT" << f << "[s] = " << InitValue(fields[f]) << ";\n";
+	}
+	o << "\t}\n\t__syncthreads();\n"
+	  << "\tfor (u32 i = start + threadIdx.x; i < end; i += blockDim.x) {\n"
+	  << "\t\tconst u64 key = keys_in[i];\n"
+	  << "\t\tu32 slot = (u32)mix64(key) & (C - 1);\n"
+	  << "\t\tbool found = false;\n"
+	  << "\t\tfor (u32 probe = 0; probe < C; ++probe) {\n"
+	  << "\t\t\tconst u64 cur = K[slot];\n"
+	  << "\t\t\tif (cur == key) { found = true; break; }\n"
+	  << "\t\t\tif (cur == ~0ull) {\n"
+	  << "\t\t\t\tconst u64 prev = atomicCAS(&K[slot], ~0ull, key);\n"
+	  << "\t\t\t\tif (prev == ~0ull || prev == key) { found = true; break; }\n"
+	  << "\t\t\t}\n"
+	  << "\t\t\tslot = (slot + 1) & (C - 1);\n"
+	  << "\t\t}\n"
+	  << "\t\tif (!found) { *overflow = true; break; }\n"
+	  << "\t\t{\n"
+	  << UpdateCode(fields, "T", "slot", part_values) << "\t\t}\n\t}\n\t__syncthreads();\n"
+	  << "\tif (*overflow) return;\n"
+	  << "\t__shared__ u32 scan_scratch[33];\n\t__shared__ u64 out_base;\n"
+	  << "\t// count live slots, reserve one output range, then write in slot order\n"
+	  << "\tu32 live = 0;\n"
+	  << "\tfor (u32 s = threadIdx.x; s < C; s += blockDim.x) live += (K[s] != ~0ull) ? 1u : 0u;\n"
+	  << "\tu32 live_total; block_exclusive_scan(live, scan_scratch, &live_total);\n"
+	  << "\tif (threadIdx.x == 0) out_base = atomicAdd((unsigned long long*)a.w[" << W + 3
+	  << "], (unsigned long long)live_total);\n"
+	  << "\t__syncthreads();\n"
+	  << "\tu64 base = out_base;\n"
+	  << "\tfor (u32 c0 = 0; c0 < C; c0 += blockDim.x) {\n"
+	  << "\t\tconst u32 s = c0 + threadIdx.x;\n"
+	  << "\t\tconst bool is_live = s < C && K[s] != ~0ull;\n"
+	  << "\t\tu32 chunk_total; const u32 off = block_exclusive_scan(is_live ? 1u : 0u, scan_scratch, &chunk_total);\n"
+	  << "\t\tif (is_live) {\n\t\t\tconst u64 pos = base + off;\n\t\t\tconst u64 key = K[s];\n"
+	  << FinalizeCode(gb, fields, visible_, "T", "s", "key", "pos", OUT) << "\t\t}\n"
+	  << "\t\tbase += chunk_total;\n\t}\n\t__syncthreads();\n}\n\n";
+
+	o << "extern \"C\" __global__ void __launch_bounds__(512) vgpu_gb_bucket(KArgs a) {\n"
+	  << "\textern __shared__ __align__(16) u64 vgpu_tab[];\n"
+	  << "\t__shared__ u32 cur_p;\n\t__shared__ bool overflow;\n"
+	  << "\tconst u32 P = (u32)a.w[" << cb << "]; const u32 C = (u32)a.w[" << cb + 1 << "];\n"
+	  << "\twhile (true) {\n"
+	  << "\t\tif (threadIdx.x == 0) { cur_p = atomicAdd((u32*)a.w[" << W << "], 1u); overflow = false; }\n"
+	  << "\t\t__syncthreads();\n"
+	  << "\t\tconst u32 p = cur_p;\n"
+	  << "\t\tif (p >= P) break;\n"
+	  << "\t\tvgpu_bucket_process(a, p, vgpu_tab, C, &overflow);\n"
+	  << "\t\tif (threadIdx.x == 0 && overflow) { ((u32*)a.w[" << W + 1 << "])[p] = 1u; atomicAdd((u32*)a.w[" << W + 2
+	  << "], 1u); }\n"
+	  << "\t\t__syncthreads();\n\t}\n}\n\n";
+
+	const int L = OUT + out_words;
+	o << "extern \"C\" __global__ void __launch_bounds__(512) vgpu_gb_bucket_global(KArgs a) {\n"
+	  << "\t__shared__ bool overflow;\n"
+	  << "\tconst u32 *list = (const u32*)a.w[" << L << "];\n"
+	  << "\tconst u32 nlist = (u32)a.w[" << L + 1 << "];\n"
+	  << "\tu64 *tables = (u64*)a.w[" << L + 2 << "];\n"
+	  << "\tconst u64 *tab_off = (const u64*)a.w[" << L + 3 << "];\n"
+	  << "\tconst u32 *caps = (const u32*)a.w[" << L + 4 << "];\n"
+	  << "\tfor (u32 e = blockIdx.x; e < nlist; e += gridDim.x) {\n"
+	  << "\t\tif (threadIdx.x == 0) overflow = false;\n\t\t__syncthreads();\n"
+	  << "\t\tvgpu_bucket_process(a, list[e], tables + tab_off[e], caps[e], &overflow);\n"
+	  << "\t\tif (threadIdx.x == 0 && overflow) atomicAdd((u32*)a.w[" << W + 2 << "], 1u);\n"
+	  << "\t\t__syncthreads();\n\t}\n}\n";
+	return o.str();
+}
+
+} // namespace vgpu

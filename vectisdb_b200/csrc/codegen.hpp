@@ -1,0 +1,136 @@
+// codegen.hpp -- per-query CUDA source generation for NVRTC.
+//
+// A "pipeline" is a chain of FILTER/PROJECTION nodes over a source relation (scanned columns, a
+// materialized intermediate, or the virtual pair space of a CROSS_PRODUCT). The generator walks the
+// chain symbolically and emits ONE kernel body that loads each needed source column once (128-bit
+// coalesced loads, R consecutive rows per thread), evaluates every predicate and projection in
+// registers, and hands the surviving rows to a consumer: compaction into dense output columns, key
+// statistics, or a group-by (direct shared-memory tables or radix partitioning).
+//
+// Expression sources keep the reference's contract (cuda_engine/src/code_generator.cpp:269-310 and
+// extension/src/expression_translator.cpp:311-315): a statement reading ((const T*)inputs[i])[row] and
+// writing ((T*)out)[idx]. The generator rewrites those two access forms into register values.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "plan.hpp"
+
+namespace vgpu {
+
+struct SourceColumn {
+	std::string name;
+	ValueType type = ValueType::INT32;
+	bool nullable = false;
+	int side = 0; // CROSS_PRODUCT pipelines: 0 = left (row / m), 1 = right (row % m)
+};
+
+struct PipelineSpec {
+	std::vector<SourceColumn> sources;
+	bool cross = false;
+	std::vector<const PlanNode *> chain; // FILTER / PROJECTION nodes, bottom-up
+};
+
+struct PipeColumn {
+	std::string name;
+	ValueType type = ValueType::INT32;
+	int source = -1;    // >= 0: pass-through of that source column
+	std::string value;  // C expression for item r
+	std::string valid;  // C bool expression for item r ("true" when never NULL)
+	bool nullable = false;
+};
+
+//! Launch geometry of one generated kernel.
+struct Geometry {
+	int block = 256;
+	int items = 4; // consecutive rows per thread
+	int tile() const {
+		return block * items;
+	}
+};
+
+// KArgs word layout shared by every pipeline kernel:
+//   w[0] = rows (pairs n*m for CROSS), w[1] = right rows m (CROSS) else 0,
+//   w[2 + 2*i] = source i data pointer, w[3 + 2*i] = source i byte-validity pointer (or 0),
+//   w[ConsumerBase() + k] = consumer arguments documented per Emit* function.
+class PipelineCodegen {
+public:
+	explicit PipelineCodegen(const PipelineSpec &spec);
+
+	const std::vector<PipeColumn> &visible() const {
+		return visible_;
+	}
+	bool has_filter() const {
+		return has_filter_;
+	}
+	int FindVisible(const std::string &name) const;
+	int ConsumerBase() const {
+		return 2 + 2 * static_cast<int>(spec_.sources.size());
+	}
+
+	//! vgpu_mat_count(tile_counts u32* @+0) and vgpu_mat_write(tile_offsets u32* @+0,
+	//! then per output column c: data @+1+2c, byte-validity @+2+2c). Without a filter only
+	//! vgpu_mat_write exists and writes row-aligned.
+	std::string EmitMaterialize(const std::vector<int> &out_columns, const Geometry &g) const;
+
+	//! vgpu_stats: per column c, atomic min/max of the (integer) value over every row < n into
+	//! i64 mins @+2c and maxs @+2c+1 (pointers to device i64). Ignores predicates (a superset bound).
+	std::string EmitStats(const std::vector<int> &columns, const Geometry &g) const;
+
+	struct GroupKey {
+		int column;     // visible column index
+		int64_t min;    // value offset
+		int shift;      // bit position in the packed key
+		int bits;       // width
+	};
+	struct AggSpec {
+		AggKind kind;
+		int column = -1; // visible column (-1 for COUNT_STAR)
+		ValueType input_type = ValueType::INT64;
+		ValueType output_type = ValueType::INT64;
+	};
+	struct GroupBySpec {
+		std::vector<GroupKey> keys;
+		std::vector<AggSpec> aggs;
+		uint64_t domain = 1; // number of packed key values (direct strategy)
+		int partition_bits = 0;
+		int table_capacity = 4096; // bucket hash-table slots (partitioned strategy)
+	};
+
+	//! Group-by kernels (see executor for the argument layout), all in one translation unit:
+	//!  direct: vgpu_gb_direct_init, vgpu_gb_direct, vgpu_gb_direct_final
+	//!  partitioned: vgpu_gb_part_count, vgpu_gb_part_scatter, vgpu_gb_bucket
+	std::string EmitGroupBy(const GroupBySpec &gb, bool partitioned, const Geometry &g) const;
+
+	//! Bytes of per-group aggregate state (excluding the key), as laid out by EmitGroupBy.
+	static int StateWords(const GroupBySpec &gb);
+
+private:
+	void Resolve();
+	std::string EmitExpression(const Expr &expr, const std::vector<PipeColumn> &cols, int index);
+	std::string Prologue() const;
+	std::string LoadBlock(const Geometry &g, const std::vector<bool> &needed, bool chunked) const;
+	std::vector<bool> NeededSources(const std::vector<int> &extra_columns) const;
+
+	PipelineSpec spec_;
+	std::vector<PipeColumn> visible_;
+	bool has_filter_ = false;
+	std::string chain_code_;               // per-item code computing keep + expression values
+	std::vector<std::vector<int>> chain_uses_; // per expression: source columns it reads (transitively)
+	std::vector<bool> chain_sources_;      // sources read by the chain itself
+	int expr_count_ = 0;
+};
+
+//! Registers the reference access forms of an expression source: returns the rewritten statement or
+//! throws Error(VGPU_ERR_UNSUPPORTED) when the source uses inputs/out/row/idx any other way.
+struct RewrittenExpr {
+	std::string statement;                 // writes `vgpu_out`, reads `vgpu_in_<i>`
+	std::vector<std::string> input_ctypes; // C type each inputs[i] is read as ("" = unused)
+	std::string output_ctype;
+};
+RewrittenExpr RewriteExpression(const std::string &source, size_t n_inputs);
+
+size_t CTypeSize(const std::string &ctype);
+
+} // namespace vgpu

@@ -1,0 +1,78 @@
+// column_cache.hpp -- device-resident column cache: the reference's GpuColumnCache
+// (cuda_engine/include/gpu_column_cache.hpp:107-281, src/gpu_column_cache.cpp) re-built for a
+// resident-column B200: committed columns are ONE contiguous device buffer each (chunk boundaries are
+// kept as offsets, so chunk replay is a pointer offset and whole-column serving is zero-copy), and the
+// integer range of every column is computed once at commit so group-by key packing needs no pass.
+#pragma once
+
+#include <list>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "executor.hpp"
+#include "plan.hpp"
+
+namespace vgpu {
+
+class ColumnCache {
+public:
+	static ColumnCache &Get();
+
+	void EnsureInitialized(double fraction_of_vram);
+	void BeginStaging(const TableRef &table);
+	bool StageChunk(const TableRef &table, const vgpu_column &chunk);
+	void CommitStaging(const TableRef &table, uint64_t scanned_rows);
+	void AbortStaging(const TableRef &table);
+	std::vector<uint64_t> ReplayableChunkRows(const TableRef &table, const std::vector<std::string> &columns);
+	bool TryGetChunk(const TableRef &table, const std::string &column, uint64_t chunk, DevColumn &out);
+	//! Borrow of the whole committed column (zero-copy); false on a miss.
+	bool GetWhole(const TableRef &table, const std::string &column, DevColumn &out);
+	void InvalidateTable(const TableRef &table);
+	void InvalidateAll();
+	uint64_t CurrentBytes();
+	uint64_t Generation(const TableRef &table);
+
+private:
+	struct Chunk {
+		void *data = nullptr;
+		uint8_t *valid = nullptr;
+		uint64_t rows = 0;
+		uint64_t bytes = 0;
+	};
+	struct Staged {
+		std::vector<Chunk> chunks;
+		ValueType type = ValueType::INT32;
+		bool type_known = false;
+		bool failed = false;
+		uint64_t rows = 0;
+		uint64_t bytes = 0;
+	};
+	struct Entry {
+		DevColumn column; // contiguous data (+ byte validity), stats filled
+		std::vector<uint64_t> chunk_rows;
+		uint64_t bytes = 0;
+		std::list<std::string>::iterator lru;
+	};
+	static std::string Key(const TableRef &t, const std::string &column);
+	static std::string TableKey(const TableRef &t);
+	void EvictLocked(const std::string &key);
+	void EvictTableLocked(const TableRef &table);
+	void AbortLocked(const TableRef &table);
+	void FreeChunk(Chunk &c);
+	bool MakeRoomLocked(uint64_t bytes);
+
+	std::mutex mu_;
+	bool initialized_ = false;
+	uint64_t budget_ = 0;
+	uint64_t committed_ = 0;
+	uint64_t staged_ = 0;
+	std::list<std::string> lru_;
+	std::unordered_map<std::string, Entry> entries_;
+	std::unordered_map<std::string, std::unordered_map<std::string, Staged>> staging_;
+	std::unordered_map<std::string, std::vector<std::string>> table_columns_;
+	std::unordered_map<std::string, uint64_t> generation_;
+};
+
+} // namespace vgpu

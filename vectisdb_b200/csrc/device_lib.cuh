@@ -1,0 +1,245 @@
+// device_lib.cuh -- device-side building blocks shared by the precompiled kernels (nvcc) and the
+// per-query kernels generated at run time (NVRTC, where this file is handed over as an in-memory
+// header). It therefore uses no host or standard-library headers: builtin types and CUDA intrinsics
+// only.
+#pragma once
+
+namespace vgpu_dev {
+
+typedef unsigned long long u64;
+typedef long long i64;
+typedef unsigned int u32;
+typedef unsigned short u16;
+typedef unsigned char u8;
+
+// Argument block every generated kernel takes by value: pointers, sizes and bit-cast constants, one
+// 64-bit word each. Keeps the host side free of per-kernel struct layouts.
+struct KArgs {
+	u64 w[128];
+};
+
+// ---------------------------------------------------------------------------------------------
+// Bit casts
+
+template <typename T> __device__ __forceinline__ T from_bits(u64 b);
+template <> __device__ __forceinline__ bool from_bits<bool>(u64 b) { return (b & 0xffull) != 0; }
+template <> __device__ __forceinline__ signed char from_bits<signed char>(u64 b) { return (signed char)(b & 0xff); }
+template <> __device__ __forceinline__ unsigned char from_bits<unsigned char>(u64 b) { return (unsigned char)(b & 0xff); }
+template <> __device__ __forceinline__ char from_bits<char>(u64 b) { return (char)(b & 0xff); }
+template <> __device__ __forceinline__ short from_bits<short>(u64 b) { return (short)(u16)(b & 0xffff); }
+template <> __device__ __forceinline__ unsigned short from_bits<unsigned short>(u64 b) { return (u16)(b & 0xffff); }
+template <> __device__ __forceinline__ int from_bits<int>(u64 b) { return (int)(u32)b; }
+template <> __device__ __forceinline__ u32 from_bits<u32>(u64 b) { return (u32)b; }
+template <> __device__ __forceinline__ float from_bits<float>(u64 b) { return __int_as_float((int)(u32)b); }
+template <> __device__ __forceinline__ i64 from_bits<i64>(u64 b) { return (i64)b; }
+template <> __device__ __forceinline__ u64 from_bits<u64>(u64 b) { return b; }
+template <> __device__ __forceinline__ double from_bits<double>(u64 b) { return __longlong_as_double((i64)b); }
+
+template <typename T> __device__ __forceinline__ u64 to_bits(T v);
+template <> __device__ __forceinline__ u64 to_bits<bool>(bool v) { return v ? 1ull : 0ull; }
+template <> __device__ __forceinline__ u64 to_bits<signed char>(signed char v) { return (u64)(u8)v; }
+template <> __device__ __forceinline__ u64 to_bits<unsigned char>(unsigned char v) { return (u64)v; }
+template <> __device__ __forceinline__ u64 to_bits<char>(char v) { return (u64)(u8)v; }
+template <> __device__ __forceinline__ u64 to_bits<unsigned short>(unsigned short v) { return (u64)v; }
+template <> __device__ __forceinline__ u64 to_bits<short>(short v) { return (u64)(u16)v; }
+template <> __device__ __forceinline__ u64 to_bits<int>(int v) { return (u64)(u32)v; }
+template <> __device__ __forceinline__ u64 to_bits<u32>(u32 v) { return (u64)v; }
+template <> __device__ __forceinline__ u64 to_bits<float>(float v) { return (u64)(u32)__float_as_int(v); }
+template <> __device__ __forceinline__ u64 to_bits<i64>(i64 v) { return (u64)v; }
+template <> __device__ __forceinline__ u64 to_bits<u64>(u64 v) { return v; }
+template <> __device__ __forceinline__ u64 to_bits<double>(double v) { return (u64)__double_as_longlong(v); }
+
+// Reinterprets the storage of a value of type S as type T of the same size (the reference kernels read
+// a column through whatever pointer type the expression casts it to).
+template <typename T, typename S> __device__ __forceinline__ T reinterpret_value(S v) {
+	return from_bits<T>(to_bits<S>(v));
+}
+
+// ---------------------------------------------------------------------------------------------
+// Coalesced row loads: R consecutive rows of one column per thread, 128-bit vectors where the
+// address allows it, streaming cache policy (each input byte is read exactly once per launch).
+
+__device__ __forceinline__ uint4 ld_stream_v4(const void *p) {
+	uint4 r;
+	asm("ld.global.cs.v4.u32 {%0,%1,%2,%3}, [%4];"
+	             : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+	             : "l"(p));
+	return r;
+}
+__device__ __forceinline__ uint2 ld_stream_v2(const void *p) {
+	uint2 r;
+	asm("ld.global.cs.v2.u32 {%0,%1}, [%2];" : "=r"(r.x), "=r"(r.y) : "l"(p));
+	return r;
+}
+__device__ __forceinline__ u32 ld_stream_u32(const void *p) {
+	u32 r;
+	asm("ld.global.cs.u32 %0, [%1];" : "=r"(r) : "l"(p));
+	return r;
+}
+
+template <typename T> __device__ __forceinline__ T ld_scalar(const T *p) {
+	return *p;
+}
+
+// Extracts element `i` (of size sizeof(T)) from a little-endian array of 32-bit words.
+template <typename T> __device__ __forceinline__ T word_element(const u32 *words, int i) {
+	if (sizeof(T) == 8) {
+		u64 b = (u64)words[2 * i] | ((u64)words[2 * i + 1] << 32);
+		return from_bits<T>(b);
+	} else if (sizeof(T) == 4) {
+		return from_bits<T>((u64)words[i]);
+	} else if (sizeof(T) == 2) {
+		u32 w = words[i >> 1];
+		return from_bits<T>((u64)((w >> ((i & 1) * 16)) & 0xffffu));
+	} else {
+		u32 w = words[i >> 2];
+		return from_bits<T>((u64)((w >> ((i & 3) * 8)) & 0xffu));
+	}
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void load_rows(const T *__restrict__ base, u64 row0, u64 n, T (&out)[R]) {
+	constexpr int BYTES = (int)sizeof(T) * R;
+	const T *p = base + row0;
+	const u64 addr = (u64)p;
+	if (row0 + R <= n && (BYTES % 16 == 0) && (addr & 15ull) == 0) {
+		u32 words[BYTES / 4];
+#pragma unroll
+		for (int q = 0; q < BYTES / 16; ++q) {
+			uint4 v = ld_stream_v4(reinterpret_cast<const char *>(p) + 16 * q);
+			words[4 * q + 0] = v.x;
+			words[4 * q + 1] = v.y;
+			words[4 * q + 2] = v.z;
+			words[4 * q + 3] = v.w;
+		}
+#pragma unroll
+		for (int r = 0; r < R; ++r) out[r] = word_element<T>(words, r);
+	} else if (row0 + R <= n && BYTES == 8 && (addr & 7ull) == 0) {
+		u32 words[2];
+		uint2 v = ld_stream_v2(p);
+		words[0] = v.x;
+		words[1] = v.y;
+#pragma unroll
+		for (int r = 0; r < R; ++r) out[r] = word_element<T>(words, r);
+	} else {
+#pragma unroll
+		for (int r = 0; r < R; ++r) out[r] = (row0 + r < n) ? ld_scalar(p + r) : T();
+	}
+}
+
+// Byte-per-row validity (the engine's internal null mask layout). nullptr = all valid.
+template <int R>
+__device__ __forceinline__ void load_valid(const u8 *__restrict__ base, u64 row0, u64 n, bool (&out)[R]) {
+	if (base == nullptr) {
+#pragma unroll
+		for (int r = 0; r < R; ++r) out[r] = true;
+		return;
+	}
+#pragma unroll
+	for (int r = 0; r < R; ++r) out[r] = (row0 + r < n) ? (base[row0 + r] != 0) : false;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Block-wide exclusive scan of one u32 per thread (blockDim.x a multiple of 32, <= 1024).
+// `scratch` needs 33 words of shared memory. Returns the exclusive prefix; *total gets the sum.
+
+__device__ __forceinline__ u32 block_exclusive_scan(u32 v, u32 *scratch, u32 *total) {
+	const int lane = threadIdx.x & 31;
+	const int warp = threadIdx.x >> 5;
+	const int nwarps = blockDim.x >> 5;
+	u32 x = v;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		u32 y = __shfl_up_sync(0xffffffffu, x, o);
+		if (lane >= o) x += y;
+	}
+	if (lane == 31) scratch[warp] = x;
+	__syncthreads();
+	if (warp == 0) {
+		u32 w = (lane < nwarps) ? scratch[lane] : 0u;
+		u32 s = w;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			u32 y = __shfl_up_sync(0xffffffffu, s, o);
+			if (lane >= o) s += y;
+		}
+		if (lane < nwarps) scratch[lane] = s - w;
+		if (lane == 31) scratch[32] = s;
+	}
+	__syncthreads();
+	u32 result = scratch[warp] + x - v;
+	*total = scratch[32];
+	__syncthreads();
+	return result;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Atomics
+
+// Exact 128-bit accumulation from 64-bit atomics. Order-independent: every add's carry out of the
+// low word is computed against the value that add actually replaced, so the high word receives the
+// true total of carries whatever the interleaving.
+__device__ __forceinline__ void atomic_add_i128(u64 *lo, i64 *hi, i64 x) {
+	const u64 ux = (u64)x;
+	const u64 old = atomicAdd(lo, ux);
+	const u64 sum = old + ux;
+	i64 hi_add = (x < 0 ? -1 : 0) + (sum < old ? 1 : 0);
+	if (hi_add != 0) atomicAdd(reinterpret_cast<u64 *>(hi), (u64)hi_add);
+}
+
+// Same, adding an already-128-bit partial (lo, hi).
+__device__ __forceinline__ void atomic_add_i128_pair(u64 *lo, i64 *hi, u64 add_lo, i64 add_hi) {
+	const u64 old = atomicAdd(lo, add_lo);
+	const u64 sum = old + add_lo;
+	i64 hi_add = add_hi + (sum < old ? 1 : 0);
+	if (hi_add != 0) atomicAdd(reinterpret_cast<u64 *>(hi), (u64)hi_add);
+}
+
+__device__ __forceinline__ void atomic_min_i64(i64 *p, i64 v) { atomicMin(reinterpret_cast<long long *>(p), (long long)v); }
+__device__ __forceinline__ void atomic_max_i64(i64 *p, i64 v) { atomicMax(reinterpret_cast<long long *>(p), (long long)v); }
+
+// ---------------------------------------------------------------------------------------------
+// Hashing of packed group keys
+
+__device__ __forceinline__ u64 mix64(u64 k) {
+	k ^= k >> 33;
+	k *= 0xff51afd7ed558ccdull;
+	k ^= k >> 33;
+	k *= 0xc4ceb9fe1a85ec53ull;
+	k ^= k >> 33;
+	return k;
+}
+
+// Partition of a packed key: the top `bits` of the mixed key. Bucket-table slots use the low bits of
+// the same mix, so the two are independent.
+__device__ __forceinline__ u32 partition_of(u64 key, int bits) {
+	return bits == 0 ? 0u : (u32)(mix64(key) >> (64 - bits));
+}
+
+// ---------------------------------------------------------------------------------------------
+// int128 -> double, correctly rounded (round to nearest even), from the two's-complement halves.
+// The magnitude is normalised so its top bit is bit 127; the upper 64 bits, with every lower bit
+// folded into bit 0 as a sticky bit, convert exactly like the full value would (the rounding point
+// sits at bit 11 of that word), and the power-of-two rescale is exact.
+__device__ __forceinline__ double i128_to_double(u64 lo, i64 hi) {
+	const bool neg = hi < 0;
+	u64 mlo = lo, mhi = (u64)hi;
+	if (neg) {
+		mlo = ~mlo + 1ull;
+		mhi = ~mhi + (mlo == 0 ? 1ull : 0ull);
+	}
+	double mag;
+	if (mhi == 0) {
+		mag = (double)mlo;
+	} else {
+		const int s = __clzll((long long)mhi);
+		u64 top = s == 0 ? mhi : ((mhi << s) | (mlo >> (64 - s)));
+		const u64 rest = s == 0 ? mlo : (mlo << s);
+		if (rest != 0) top |= 1ull;
+		const double scale = __longlong_as_double((long long)((u64)(1023 + 64 - s) << 52));
+		mag = (double)top * scale;
+	}
+	return neg ? -mag : mag;
+}
+
+} // namespace vgpu_dev

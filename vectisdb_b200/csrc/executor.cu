@@ -1,0 +1,921 @@
+// executor.cu -- plan execution (see executor.hpp).
+//
+// Operator mapping to the reference engine (cuda_engine/src):
+//   SCAN                -> gpu_executor.cu:368-643   (H2D / cache serving; validity unpacked to bytes)
+//   FILTER/PROJECTION   -> gpu_executor.cu:645-746   (one fused NVRTC kernel per chain, stable compaction)
+//   GROUP_BY_AGGREGATE  -> operators/gpu_groupby.cu  (direct shared-memory tables when the packed key
+//                          domain is small, else radix partitioning + per-partition hash tables)
+//   HASH_JOIN           -> operators/gpu_hash_join.cu (sort-merge: LSD radix sort of the right side,
+//                          per-left-row search, load-balanced expansion, gathers)
+//   CROSS_PRODUCT       -> operators/gpu_cross_join.cu (left-major virtual pair space fed straight into
+//                          the fused pipeline, so a filter above it never materializes the n*m pairs)
+#include "executor.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <set>
+
+#include "column_cache.hpp"
+#include "kernels.hpp"
+
+namespace vgpu {
+
+namespace {
+
+constexpr uint64_t kMaxOutputRows = 1ull << 32; // same backstop as the reference's join/cross caps
+
+struct KArgsHost {
+	uint64_t w[128];
+	int used = 0;
+	KArgsHost() {
+		std::memset(w, 0, sizeof(w));
+	}
+	void Set(int i, uint64_t v) {
+		if (i >= 128) Fail(VGPU_ERR_UNSUPPORTED, "generated kernel needs more than 128 argument words");
+		w[i] = v;
+		used = std::max(used, i + 1);
+	}
+	void SetPtr(int i, const void *p) {
+		Set(i, reinterpret_cast<uint64_t>(p));
+	}
+};
+
+void LaunchGenerated(Module &m, const char *name, dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                     KArgsHost &args, uint64_t bytes, uint64_t rows) {
+	CUfunction f = m.Get(name);
+	LaunchScope scope(name, stream, bytes, rows);
+	void *params[] = {args.w};
+	Runtime::Get().LaunchModuleKernel(f, grid, block, smem, stream, params);
+}
+
+int BitsFor(uint64_t range) {
+	int b = 0;
+	while (b < 64 && (range >> b) != 0) {
+		b++;
+	}
+	return b;
+}
+
+uint64_t NextPow2(uint64_t x) {
+	uint64_t p = 1;
+	while (p < x) p <<= 1;
+	return p;
+}
+
+uint64_t FloorPow2(uint64_t x) {
+	uint64_t p = 1;
+	while ((p << 1) <= x) p <<= 1;
+	return p;
+}
+
+class Executor {
+public:
+	Executor(const std::vector<vgpu_column> &inputs, const ExecOptions &options, cudaStream_t stream, bool nulls_ok)
+	    : inputs_(inputs), options_(options), stream_(stream), arena_(stream), nulls_supported_(nulls_ok) {
+	}
+
+	Relation Exec(const PlanNode &node);
+	Arena &arena() {
+		return arena_;
+	}
+	std::string last_source;
+
+private:
+	struct PipelineInput {
+		PipelineSpec spec;
+		std::vector<DevColumn> sources; // parallel to spec.sources
+		uint64_t rows = 0;              // pairs for CROSS
+		uint64_t right_rows = 0;
+	};
+
+	Relation Scan(const PlanNode &node);
+	PipelineInput BuildPipeline(const PlanNode &top, std::vector<const PlanNode *> chain_top_down);
+	Relation Materialize(PipelineInput &pin, const std::vector<int> &out_cols, const std::vector<std::string> &names);
+	Relation RunChain(const PlanNode &node);
+	Relation GroupBy(const PlanNode &node);
+	Relation Join(const PlanNode &node);
+	Relation CrossProduct(const PlanNode &node);
+	void ComputeStats(PipelineInput &pin, PipelineCodegen &cg, const std::vector<int> &cols,
+	                  std::vector<std::pair<int64_t, int64_t>> &out);
+	void FillArgs(const PipelineInput &pin, KArgsHost &args);
+	uint64_t ReadU64(const void *dev);
+	uint32_t ReadU32(const void *dev);
+
+	const std::vector<vgpu_column> &inputs_;
+	ExecOptions options_;
+	cudaStream_t stream_;
+	Arena arena_;
+	size_t cursor_ = 0;
+	bool nulls_supported_;
+};
+
+uint64_t Executor::ReadU64(const void *dev) {
+	uint64_t v = 0;
+	VGPU_CUDA(cudaMemcpyAsync(&v, dev, sizeof(v), cudaMemcpyDeviceToHost, stream_));
+	VGPU_CUDA(cudaStreamSynchronize(stream_));
+	return v;
+}
+
+uint32_t Executor::ReadU32(const void *dev) {
+	uint32_t v = 0;
+	VGPU_CUDA(cudaMemcpyAsync(&v, dev, sizeof(v), cudaMemcpyDeviceToHost, stream_));
+	VGPU_CUDA(cudaStreamSynchronize(stream_));
+	return v;
+}
+
+// ---- SCAN ------------------------------------------------------------------------------------------
+
+Relation Executor::Scan(const PlanNode &node) {
+	Relation out;
+	if (options_.serve_whole_scan_from_cache || options_.cache_chunk_index >= 0) {
+		auto &cache = ColumnCache::Get();
+		for (auto &name : node.column_names) {
+			DevColumn col;
+			bool ok = options_.cache_chunk_index >= 0
+			              ? cache.TryGetChunk(node.table, name, static_cast<uint64_t>(options_.cache_chunk_index), col)
+			              : cache.GetWhole(node.table, name, col);
+			if (!ok) {
+				Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: column '" + name + "' of table '" + node.table.ToString() +
+				                                    "' was expected to be cache-resident but is no longer present -- "
+				                                    "retry the query");
+			}
+			if (col.valid != nullptr && !nulls_supported_) {
+				Fail(VGPU_ERR_UNSUPPORTED, "gpu_executor: cached column '" + name +
+				                               "' contains NULLs, which this operator does not model");
+			}
+			out.push_back(col);
+		}
+		return out;
+	}
+	for (size_t i = 0; i < node.column_names.size(); i++) {
+		if (cursor_ >= inputs_.size()) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: plan expects more scanned columns than were supplied");
+		}
+		const vgpu_column &in = inputs_[cursor_++];
+		if (!IsValidValueType(in.type)) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: input column type out of range");
+		}
+		DevColumn col;
+		col.name = in.name ? in.name : "";
+		col.type = static_cast<ValueType>(in.type);
+		col.rows = in.row_count;
+		if (in.validity != nullptr && !nulls_supported_) {
+			Fail(VGPU_ERR_UNSUPPORTED,
+			     "gpu_executor: column '" + col.name + "' contains NULLs, which this operator does not model");
+		}
+		const size_t bytes = static_cast<size_t>(in.row_count) * TypeSize(col.type);
+		if (bytes > 0 && in.data == nullptr) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: column '" + col.name + "' has rows but no data");
+		}
+		if (in.memory == VGPU_MEM_DEVICE) {
+			col.data = const_cast<void *>(in.data);
+			if (col.data == nullptr) {
+				col.data = arena_.Alloc(16);
+			}
+		} else {
+			col.data = arena_.Alloc(bytes);
+			if (bytes > 0) {
+				VGPU_CUDA(cudaMemcpyAsync(col.data, in.data, bytes, cudaMemcpyHostToDevice, stream_));
+			}
+		}
+		if (in.validity != nullptr && in.row_count > 0) {
+			const size_t vbytes = (in.row_count + 7) / 8;
+			const uint8_t *bitmap = in.validity;
+			if (in.memory != VGPU_MEM_DEVICE) {
+				uint8_t *dev_bitmap = arena_.AllocT<uint8_t>(vbytes);
+				VGPU_CUDA(cudaMemcpyAsync(dev_bitmap, in.validity, vbytes, cudaMemcpyHostToDevice, stream_));
+				bitmap = dev_bitmap;
+			}
+			col.valid = arena_.AllocT<uint8_t>(in.row_count);
+			kern::UnpackValidity(bitmap, col.valid, in.row_count, stream_);
+		}
+		out.push_back(col);
+	}
+	return out;
+}
+
+// ---- pipelines -------------------------------------------------------------------------------------
+
+void Executor::FillArgs(const PipelineInput &pin, KArgsHost &args) {
+	args.Set(0, pin.rows);
+	args.Set(1, pin.right_rows);
+	for (size_t i = 0; i < pin.sources.size(); i++) {
+		args.SetPtr(2 + 2 * static_cast<int>(i), pin.sources[i].data);
+		args.SetPtr(3 + 2 * static_cast<int>(i), pin.sources[i].valid);
+	}
+}
+
+Executor::PipelineInput Executor::BuildPipeline(const PlanNode &top, std::vector<const PlanNode *> chain) {
+	// `top` is the first non-FILTER/PROJECTION node below the chain.
+	PipelineInput pin;
+	std::reverse(chain.begin(), chain.end()); // bottom-up
+	pin.spec.chain = chain;
+	if (top.op == OpType::CROSS_PRODUCT) {
+		if (top.children.size() != 2) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: CROSS_PRODUCT expects exactly two children");
+		}
+		if (top.output_columns.empty()) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_cross_join: node has no output columns");
+		}
+		Relation left = Exec(*top.children[0]);
+		Relation right = Exec(*top.children[1]);
+		if (left.empty() || right.empty()) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_cross_join: both inputs must produce at least one column");
+		}
+		const uint64_t ln = left.front().rows, rn = right.front().rows;
+		for (auto &c : left) {
+			if (c.rows != ln) Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_cross_join: left input column '" + c.name + "' row count mismatch");
+		}
+		for (auto &c : right) {
+			if (c.rows != rn) Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_cross_join: right input column '" + c.name + "' row count mismatch");
+		}
+		for (auto &name : top.output_columns) {
+			const DevColumn *l = nullptr, *r = nullptr;
+			for (auto &c : left) if (c.name == name) { l = &c; break; }
+			for (auto &c : right) if (c.name == name) { r = &c; break; }
+			if (l && r) {
+				Fail(VGPU_ERR_UNSUPPORTED, "gpu_cross_join: output column '" + name + "' is ambiguous (present on both sides)");
+			}
+			if (!l && !r) {
+				Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_cross_join: output column '" + name + "' not found on either side");
+			}
+			SourceColumn sc;
+			sc.name = name;
+			sc.type = (l ? l : r)->type;
+			sc.nullable = (l ? l : r)->valid != nullptr;
+			sc.side = l ? 0 : 1;
+			pin.spec.sources.push_back(sc);
+			pin.sources.push_back(*(l ? l : r));
+		}
+		pin.spec.cross = true;
+		if (ln == 0 || rn == 0) {
+			pin.rows = 0;
+			pin.right_rows = std::max<uint64_t>(rn, 1);
+		} else {
+			if (ln > kMaxOutputRows / rn || ln * rn > kMaxOutputRows) {
+				Fail(VGPU_ERR_UNSUPPORTED, "gpu_cross_join: cross product of " + std::to_string(ln) + " x " +
+				                               std::to_string(rn) + " rows is too large for GPU execution");
+			}
+			pin.rows = ln * rn;
+			pin.right_rows = rn;
+		}
+		return pin;
+	}
+	Relation rel = top.op == OpType::SCAN ? Scan(top) : Exec(top);
+	uint64_t rows = rel.empty() ? 0 : rel.front().rows;
+	for (auto &c : rel) {
+		if (c.rows != rows) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: input column '" + c.name + "' row count mismatch");
+		}
+		SourceColumn sc;
+		sc.name = c.name;
+		sc.type = c.type;
+		sc.nullable = c.valid != nullptr;
+		pin.spec.sources.push_back(sc);
+		pin.sources.push_back(c);
+	}
+	pin.rows = rows;
+	return pin;
+}
+
+Relation Executor::Materialize(PipelineInput &pin, const std::vector<int> &out_cols,
+                               const std::vector<std::string> &names) {
+	PipelineCodegen cg(pin.spec);
+	Geometry g;
+	g.block = 256;
+	g.items = 4;
+	std::string src = cg.EmitMaterialize(out_cols, g);
+	last_source = src;
+	auto module = Runtime::Get().modules().GetOrCompile(src);
+	const uint64_t n = pin.rows;
+	const uint64_t ntiles = (n + g.tile() - 1) / g.tile();
+	const int sms = Runtime::Get().props().sm_count;
+	const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ntiles, uint64_t(sms) * 8)));
+	const int cb = cg.ConsumerBase();
+	uint64_t out_rows = n;
+	uint32_t *tile_offsets = nullptr;
+	if (cg.has_filter() && n > 0) {
+		uint32_t *tile_counts = arena_.AllocT<uint32_t>(ntiles);
+		uint32_t *total = arena_.AllocT<uint32_t>(1);
+		KArgsHost a;
+		FillArgs(pin, a);
+		a.SetPtr(cb, tile_counts);
+		uint64_t in_bytes = 0;
+		for (auto &s : pin.sources) in_bytes += s.rows * TypeSize(s.type);
+		LaunchGenerated(*module, "vgpu_mat_count", grid, g.block, 0, stream_, a, in_bytes, n);
+		kern::ExclusiveScanU32(tile_counts, tile_counts, ntiles, total, arena_);
+		out_rows = ReadU32(total);
+		tile_offsets = tile_counts;
+	}
+	Relation out;
+	KArgsHost a;
+	FillArgs(pin, a);
+	a.SetPtr(cb, tile_offsets);
+	for (size_t c = 0; c < out_cols.size(); c++) {
+		const auto &vc = cg.visible()[out_cols[c]];
+		DevColumn col;
+		col.name = names[c];
+		col.type = vc.type;
+		col.rows = out_rows;
+		col.data = arena_.Alloc(out_rows * TypeSize(vc.type));
+		if (vc.nullable) {
+			col.valid = arena_.AllocT<uint8_t>(out_rows);
+		}
+		if (vc.source >= 0 && pin.sources[vc.source].has_stats) {
+			col.has_stats = true;
+			col.min = pin.sources[vc.source].min;
+			col.max = pin.sources[vc.source].max;
+		}
+		a.SetPtr(cb + 1 + 2 * static_cast<int>(c), col.data);
+		a.SetPtr(cb + 2 + 2 * static_cast<int>(c), col.valid);
+		out.push_back(col);
+	}
+	if (n > 0 && (out_rows > 0 || !cg.has_filter())) {
+		LaunchGenerated(*module, "vgpu_mat_write", grid, g.block, 0, stream_, a, 0, n);
+	}
+	return out;
+}
+
+Relation Executor::RunChain(const PlanNode &node) {
+	std::vector<const PlanNode *> chain;
+	const PlanNode *cur = &node;
+	while (cur->op == OpType::FILTER || cur->op == OpType::PROJECTION) {
+		if (cur->children.size() != 1) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, std::string("gpu_executor: ") +
+			                                    (cur->op == OpType::FILTER ? "FILTER" : "PROJECTION") +
+			                                    " expects exactly one child");
+		}
+		chain.push_back(cur);
+		cur = cur->children[0].get();
+	}
+	PipelineInput pin = BuildPipeline(*cur, chain);
+	PipelineCodegen probe(pin.spec);
+	std::vector<int> outs;
+	std::vector<std::string> names;
+	for (size_t i = 0; i < probe.visible().size(); i++) {
+		outs.push_back(static_cast<int>(i));
+		names.push_back(probe.visible()[i].name);
+	}
+	return Materialize(pin, outs, names);
+}
+
+Relation Executor::CrossProduct(const PlanNode &node) {
+	PipelineInput pin = BuildPipeline(node, {});
+	std::vector<int> outs;
+	std::vector<std::string> names;
+	for (size_t i = 0; i < pin.spec.sources.size(); i++) {
+		outs.push_back(static_cast<int>(i));
+		names.push_back(pin.spec.sources[i].name);
+	}
+	return Materialize(pin, outs, names);
+}
+
+void Executor::ComputeStats(PipelineInput &pin, PipelineCodegen &cg, const std::vector<int> &cols,
+                            std::vector<std::pair<int64_t, int64_t>> &out) {
+	out.assign(cols.size(), {0, 0});
+	std::vector<int> missing;
+	std::vector<size_t> missing_pos;
+	for (size_t i = 0; i < cols.size(); i++) {
+		const auto &vc = cg.visible()[cols[i]];
+		if (vc.source >= 0 && pin.sources[vc.source].has_stats) {
+			out[i] = {pin.sources[vc.source].min, pin.sources[vc.source].max};
+		} else {
+			missing.push_back(cols[i]);
+			missing_pos.push_back(i);
+		}
+	}
+	if (missing.empty()) {
+		return;
+	}
+	Geometry g;
+	g.block = 256;
+	g.items = 4;
+	std::string src = cg.EmitStats(missing, g);
+	auto module = Runtime::Get().modules().GetOrCompile(src);
+	int64_t *mm = arena_.AllocT<int64_t>(2 * missing.size());
+	std::vector<int64_t> init(2 * missing.size());
+	for (size_t i = 0; i < missing.size(); i++) {
+		init[2 * i] = INT64_MAX;
+		init[2 * i + 1] = INT64_MIN;
+	}
+	VGPU_CUDA(cudaMemcpyAsync(mm, init.data(), init.size() * 8, cudaMemcpyHostToDevice, stream_));
+	KArgsHost a;
+	FillArgs(pin, a);
+	const int cb = cg.ConsumerBase();
+	for (size_t i = 0; i < missing.size(); i++) {
+		a.SetPtr(cb + 2 * static_cast<int>(i), mm + 2 * i);
+		a.SetPtr(cb + 2 * static_cast<int>(i) + 1, mm + 2 * i + 1);
+	}
+	const uint64_t ntiles = (pin.rows + g.tile() - 1) / g.tile();
+	const unsigned grid = static_cast<unsigned>(
+	    std::max<uint64_t>(1, std::min<uint64_t>(ntiles, uint64_t(Runtime::Get().props().sm_count) * 8)));
+	if (pin.rows > 0) {
+		LaunchGenerated(*module, "vgpu_stats", grid, g.block, 0, stream_, a, 0, pin.rows);
+	}
+	std::vector<int64_t> host(2 * missing.size());
+	VGPU_CUDA(cudaMemcpyAsync(host.data(), mm, host.size() * 8, cudaMemcpyDeviceToHost, stream_));
+	VGPU_CUDA(cudaStreamSynchronize(stream_));
+	for (size_t i = 0; i < missing.size(); i++) {
+		out[missing_pos[i]] = {host[2 * i], host[2 * i + 1]};
+	}
+}
+
+// ---- GROUP BY --------------------------------------------------------------------------------------
+
+Relation Executor::GroupBy(const PlanNode &node) {
+	if (node.children.size() != 1) {
+		Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: GROUP_BY_AGGREGATE expects exactly one child");
+	}
+	if (node.group_keys.empty() && node.aggregates.empty()) {
+		Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_groupby: node has neither group keys nor aggregates");
+	}
+	std::vector<const PlanNode *> chain;
+	const PlanNode *cur = node.children[0].get();
+	while (cur->op == OpType::FILTER || cur->op == OpType::PROJECTION) {
+		if (cur->children.size() != 1) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: FILTER/PROJECTION expects exactly one child");
+		}
+		chain.push_back(cur);
+		cur = cur->children[0].get();
+	}
+	PipelineInput pin = BuildPipeline(*cur, chain);
+	PipelineCodegen cg(pin.spec);
+	if (cg.visible().empty()) {
+		Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_groupby: input operator produced no columns to group");
+	}
+	auto find = [&](const std::string &name, const char *what) {
+		int c = cg.FindVisible(name);
+		if (c < 0) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, std::string("gpu_groupby: ") + what + " column '" + name + "' not found");
+		}
+		return c;
+	};
+	// Validation mirrors operators/gpu_groupby.cu:224-299 and :320-350.
+	std::vector<int> key_cols;
+	for (auto &k : node.group_keys) {
+		int c = find(k, "group key");
+		const ValueType t = cg.visible()[c].type;
+		if (!IsIntegerKeyType(t)) {
+			Fail(VGPU_ERR_UNSUPPORTED, "gpu_groupby: group key '" + k +
+			                               "' is not an integer/boolean column, which this GPU path requires");
+		}
+		key_cols.push_back(c);
+	}
+	PipelineCodegen::GroupBySpec gb;
+	for (auto &agg : node.aggregates) {
+		PipelineCodegen::AggSpec s;
+		s.kind = agg.kind;
+		s.output_type = agg.output_type;
+		if (agg.kind == AggKind::COUNT_STAR) {
+			if (agg.output_type != ValueType::INT64) Fail(VGPU_ERR_UNSUPPORTED, "gpu_groupby: COUNT(*) must produce INT64");
+			gb.aggs.push_back(s);
+			continue;
+		}
+		s.column = find(agg.input_column, "aggregate input");
+		s.input_type = cg.visible()[s.column].type;
+		const ValueType in = s.input_type;
+		switch (agg.kind) {
+		case AggKind::COUNT:
+			if (agg.output_type != ValueType::INT64) Fail(VGPU_ERR_UNSUPPORTED, "gpu_groupby: COUNT must produce INT64");
+			break;
+		case AggKind::SUM:
+			if (IsFloatType(in)) {
+				if (agg.output_type != ValueType::FLOAT64) {
+					Fail(VGPU_ERR_UNSUPPORTED, "gpu_groupby: SUM on this GPU path supports only FLOAT/DOUBLE input "
+					                           "producing DOUBLE");
+				}
+			} else if (in == ValueType::INT16 || in == ValueType::INT32 || in == ValueType::INT64) {
+				// DuckDB: SUM over INTEGER/BIGINT/DECIMAL(<=18) returns a 128-bit integer (exact).
+				if (agg.output_type != ValueType::HUGEINT) {
+					Fail(VGPU_ERR_UNSUPPORTED, "gpu_groupby: SUM over an integer column must produce HUGEINT");
+				}
+			} else {
+				Fail(VGPU_ERR_UNSUPPORTED, "gpu_groupby: SUM on this GPU path supports only FLOAT/DOUBLE input "
+				                           "producing DOUBLE");
+			}
+			break;
+		case AggKind::AVG:
+			if (agg.output_type != ValueType::FLOAT64) Fail(VGPU_ERR_UNSUPPORTED, "gpu_groupby: AVG must produce DOUBLE");
+			if (!(in == ValueType::INT16 || in == ValueType::INT32 || in == ValueType::INT64 || IsFloatType(in))) {
+				Fail(VGPU_ERR_UNSUPPORTED, "gpu_groupby: AVG supports numeric columns only");
+			}
+			break;
+		case AggKind::MIN:
+		case AggKind::MAX:
+			if (agg.output_type != in) {
+				Fail(VGPU_ERR_UNSUPPORTED, "gpu_groupby: MIN/MAX output type must match its input column type");
+			}
+			if (!IsIntegerKeyType(in)) {
+				Fail(VGPU_ERR_UNSUPPORTED, "gpu_groupby: MIN/MAX on this GPU path supports only integer/boolean columns");
+			}
+			break;
+		default:
+			break;
+		}
+		gb.aggs.push_back(s);
+	}
+	const uint64_t n = pin.rows;
+	auto empty_result = [&]() {
+		Relation out;
+		for (size_t i = 0; i < key_cols.size(); i++) {
+			DevColumn c;
+			c.name = node.group_keys[i];
+			c.type = cg.visible()[key_cols[i]].type;
+			c.rows = 0;
+			c.data = arena_.Alloc(0);
+			out.push_back(c);
+		}
+		for (size_t i = 0; i < node.aggregates.size(); i++) {
+			DevColumn c;
+			c.name = "agg_" + std::to_string(i);
+			c.type = node.aggregates[i].output_type;
+			c.rows = 0;
+			c.data = arena_.Alloc(0);
+			out.push_back(c);
+		}
+		return out;
+	};
+	const char *kEmptyGlobal = "gpu_groupby: global aggregate over an empty input needs NULL results, which this GPU "
+	                           "path cannot represent";
+	if (n == 0) {
+		if (node.group_keys.empty()) Fail(VGPU_ERR_UNSUPPORTED, kEmptyGlobal);
+		return empty_result();
+	}
+	// Key packing from the key ranges.
+	std::vector<std::pair<int64_t, int64_t>> ranges;
+	ComputeStats(pin, cg, key_cols, ranges);
+	int shift = 0;
+	for (size_t i = 0; i < key_cols.size(); i++) {
+		PipelineCodegen::GroupKey k;
+		k.column = key_cols[i];
+		k.min = ranges[i].first;
+		const uint64_t span = static_cast<uint64_t>(ranges[i].second) - static_cast<uint64_t>(ranges[i].first);
+		k.bits = BitsFor(span);
+		k.shift = shift;
+		shift += k.bits;
+		gb.keys.push_back(k);
+	}
+	if (shift > 63) {
+		Fail(VGPU_ERR_UNSUPPORTED, "gpu_groupby: the group key ranges need " + std::to_string(shift) +
+		                               " bits packed, more than the 63 this path supports");
+	}
+	const auto &props = Runtime::Get().props();
+	const int F = PipelineCodegen::StateWords(gb);
+	const uint64_t domain = 1ull << shift;
+	const uint64_t direct_smem = domain * static_cast<uint64_t>(F) * 8;
+	const bool direct = direct_smem <= 96 * 1024;
+	const int key_words = static_cast<int>(gb.keys.size());
+	const int out_words = key_words + static_cast<int>(gb.aggs.size());
+	gb.domain = domain;
+
+	// Output columns, sized for the largest possible group count.
+	const uint64_t cap_rows = direct ? domain : std::min<uint64_t>(domain, n);
+	Relation out;
+	for (size_t i = 0; i < key_cols.size(); i++) {
+		DevColumn c;
+		c.name = node.group_keys[i];
+		c.type = cg.visible()[key_cols[i]].type;
+		c.data = arena_.Alloc(cap_rows * TypeSize(c.type));
+		c.has_stats = true;
+		c.min = ranges[i].first;
+		c.max = ranges[i].second;
+		out.push_back(c);
+	}
+	for (size_t i = 0; i < node.aggregates.size(); i++) {
+		DevColumn c;
+		c.name = "agg_" + std::to_string(i);
+		c.type = node.aggregates[i].output_type;
+		c.data = arena_.Alloc(cap_rows * TypeSize(c.type));
+		out.push_back(c);
+	}
+	uint64_t in_bytes = 0;
+	for (auto &s : pin.sources) in_bytes += s.rows * TypeSize(s.type);
+	const int cb = cg.ConsumerBase();
+	uint64_t groups = 0;
+
+	if (direct) {
+		Geometry g;
+		g.block = 512;
+		g.items = 4;
+		std::string src = cg.EmitGroupBy(gb, false, g);
+		last_source = src;
+		auto module = Runtime::Get().modules().GetOrCompile(src);
+		uint64_t *fields = arena_.AllocT<uint64_t>(domain * F);
+		uint64_t *count = arena_.AllocT<uint64_t>(1);
+		KArgsHost a;
+		FillArgs(pin, a);
+		a.Set(cb, domain);
+		for (int f = 0; f < F; f++) a.SetPtr(cb + 1 + f, fields + domain * f);
+		for (int w = 0; w < out_words; w++) a.SetPtr(cb + 1 + F + w, out[w].data);
+		a.SetPtr(cb + 1 + F + out_words, count);
+		const unsigned init_grid = static_cast<unsigned>(std::min<uint64_t>((domain + 255) / 256, 1024));
+		LaunchGenerated(*module, "vgpu_gb_direct_init", init_grid, 256, 0, stream_, a, domain * F * 8, domain);
+		const size_t smem = static_cast<size_t>(direct_smem);
+		CUfunction f = module->Get("vgpu_gb_direct");
+		int occ = std::max(1, Runtime::Get().MaxActiveBlocks(f, g.block, smem));
+		const uint64_t ntiles = (n + g.tile() - 1) / g.tile();
+		const unsigned grid =
+		    static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ntiles, uint64_t(props.sm_count) * occ)));
+		LaunchGenerated(*module, "vgpu_gb_direct", grid, g.block, smem, stream_, a, in_bytes, n);
+		LaunchGenerated(*module, "vgpu_gb_direct_final", 1, 1024, 0, stream_, a, domain * F * 8, domain);
+		groups = ReadU64(count);
+	} else {
+		// Partitioned: table capacity from the shared-memory budget, partitions so each table runs at
+		// most half full on average.
+		const uint64_t smem_cap = std::min<uint64_t>(props.smem_optin > 4096 ? props.smem_optin - 4096 : 48 * 1024,
+		                                             200 * 1024);
+		const uint64_t C = std::max<uint64_t>(256, FloorPow2(smem_cap / ((1 + F) * 8)));
+		const uint64_t expected_groups = std::min<uint64_t>(domain, n);
+		uint64_t P = NextPow2(std::max<uint64_t>(1, (expected_groups + C / 2 - 1) / (C / 2)));
+		P = std::min<uint64_t>(P, 16384);
+		int pbits = BitsFor(P - 1);
+		if (P == 1) pbits = 0;
+		gb.partition_bits = pbits;
+		gb.table_capacity = static_cast<int>(C);
+		Geometry g;
+		g.block = 512;
+		g.items = 4;
+		std::string src = cg.EmitGroupBy(gb, true, g);
+		last_source = src;
+		auto module = Runtime::Get().modules().GetOrCompile(src);
+		CUfunction fcount = module->Get("vgpu_gb_part_count");
+		const size_t part_smem = P * 4;
+		int occ = std::max(1, Runtime::Get().MaxActiveBlocks(fcount, g.block, part_smem));
+		occ = std::min(occ, std::max(1, Runtime::Get().MaxActiveBlocks(module->Get("vgpu_gb_part_scatter"), g.block, part_smem)));
+		const uint64_t ntiles = (n + g.tile() - 1) / g.tile();
+		const uint64_t G = std::max<uint64_t>(1, std::min<uint64_t>(ntiles, uint64_t(props.sm_count) * occ));
+		const uint64_t tpc = (ntiles + G - 1) / G;
+		if (n >= (1ull << 32)) Fail(VGPU_ERR_UNSUPPORTED, "gpu_groupby: more than 2^32 input rows");
+		uint32_t *offsets = arena_.AllocT<uint32_t>(P * G);
+		uint32_t *total = arena_.AllocT<uint32_t>(1);
+		// value columns carried by the scatter (same order as EmitGroupBy's value_cols)
+		std::vector<int> value_cols;
+		for (auto &s : gb.aggs) {
+			if (s.column >= 0 && s.kind != AggKind::COUNT && s.kind != AggKind::COUNT_STAR &&
+			    std::find(value_cols.begin(), value_cols.end(), s.column) == value_cols.end()) {
+				value_cols.push_back(s.column);
+			}
+		}
+		KArgsHost a;
+		FillArgs(pin, a);
+		a.Set(cb, P);
+		a.Set(cb + 1, static_cast<uint64_t>(pbits));
+		a.Set(cb + 2, tpc);
+		a.SetPtr(cb + 3, offsets);
+		LaunchGenerated(*module, "vgpu_gb_part_count", static_cast<unsigned>(G), g.block, part_smem, stream_, a, in_bytes, n);
+		kern::ExclusiveScanU32(offsets, offsets, P * G, total, arena_);
+		uint64_t *keys_part = arena_.AllocT<uint64_t>(n);
+		std::vector<void *> vals_part;
+		for (int c : value_cols) vals_part.push_back(arena_.Alloc(n * TypeSize(cg.visible()[c].type)));
+		a.SetPtr(cb + 4, keys_part);
+		for (size_t v = 0; v < vals_part.size(); v++) a.SetPtr(cb + 5 + static_cast<int>(v), vals_part[v]);
+		LaunchGenerated(*module, "vgpu_gb_part_scatter", static_cast<unsigned>(G), g.block, part_smem, stream_, a, in_bytes, n);
+		// bucket tables
+		const int V = static_cast<int>(value_cols.size());
+		const int W = cb + 6 + V;
+		uint32_t *control = arena_.AllocT<uint32_t>(2 + P);
+		uint64_t *out_count = arena_.AllocT<uint64_t>(1);
+		VGPU_CUDA(cudaMemsetAsync(control, 0, (2 + P) * 4, stream_));
+		VGPU_CUDA(cudaMemsetAsync(out_count, 0, 8, stream_));
+		KArgsHost b;
+		FillArgs(pin, b);
+		b.Set(cb, P);
+		b.Set(cb + 1, C);
+		b.SetPtr(cb + 2, offsets);
+		b.Set(cb + 3, G);
+		b.SetPtr(cb + 4, total);
+		b.SetPtr(cb + 5, keys_part);
+		for (int v = 0; v < V; v++) b.SetPtr(cb + 6 + v, vals_part[v]);
+		b.SetPtr(W, control);           // work counter
+		b.SetPtr(W + 1, control + 2);   // overflow flags [P]
+		b.SetPtr(W + 2, control + 1);   // overflow count
+		b.SetPtr(W + 3, out_count);
+		for (int w = 0; w < out_words; w++) b.SetPtr(W + 4 + w, out[w].data);
+		const size_t bucket_smem = static_cast<size_t>((1 + F) * 8 * C);
+		CUfunction fb = module->Get("vgpu_gb_bucket");
+		int bocc = std::max(1, Runtime::Get().MaxActiveBlocks(fb, 512, bucket_smem));
+		const unsigned bgrid = static_cast<unsigned>(std::min<uint64_t>(P, uint64_t(props.sm_count) * bocc));
+		uint64_t part_bytes = n * 8;
+		for (int c : value_cols) part_bytes += n * TypeSize(cg.visible()[c].type);
+		LaunchGenerated(*module, "vgpu_gb_bucket", bgrid, 512, bucket_smem, stream_, b, part_bytes, n);
+		const uint32_t overflowed = ReadU32(control + 1);
+		if (overflowed > 0) {
+			// Partitions with more distinct keys than a shared-memory table holds: redo them with a
+			// global-memory table sized from the partition's row count.
+			std::vector<uint32_t> flags(P), offs(P * G);
+			uint32_t total_rows = ReadU32(total);
+			VGPU_CUDA(cudaMemcpyAsync(flags.data(), control + 2, P * 4, cudaMemcpyDeviceToHost, stream_));
+			VGPU_CUDA(cudaMemcpyAsync(offs.data(), offsets, P * G * 4, cudaMemcpyDeviceToHost, stream_));
+			VGPU_CUDA(cudaStreamSynchronize(stream_));
+			std::vector<uint32_t> list, caps;
+			std::vector<uint64_t> tab_off;
+			uint64_t words = 0;
+			for (uint64_t p = 0; p < P; p++) {
+				if (!flags[p]) continue;
+				const uint32_t start = offs[p * G];
+				const uint32_t end = p + 1 < P ? offs[(p + 1) * G] : total_rows;
+				const uint64_t cap = NextPow2(std::max<uint64_t>(64, 2ull * (end - start)));
+				list.push_back(static_cast<uint32_t>(p));
+				caps.push_back(static_cast<uint32_t>(cap));
+				tab_off.push_back(words);
+				words += cap * (1 + F);
+			}
+			uint64_t *tables = arena_.AllocT<uint64_t>(words);
+			uint32_t *d_list = arena_.AllocT<uint32_t>(list.size());
+			uint32_t *d_caps = arena_.AllocT<uint32_t>(caps.size());
+			uint64_t *d_off = arena_.AllocT<uint64_t>(tab_off.size());
+			VGPU_CUDA(cudaMemcpyAsync(d_list, list.data(), list.size() * 4, cudaMemcpyHostToDevice, stream_));
+			VGPU_CUDA(cudaMemcpyAsync(d_caps, caps.data(), caps.size() * 4, cudaMemcpyHostToDevice, stream_));
+			VGPU_CUDA(cudaMemcpyAsync(d_off, tab_off.data(), tab_off.size() * 8, cudaMemcpyHostToDevice, stream_));
+			VGPU_CUDA(cudaMemsetAsync(control + 1, 0, 4, stream_));
+			const int L = W + 4 + out_words;
+			b.SetPtr(L, d_list);
+			b.Set(L + 1, list.size());
+			b.SetPtr(L + 2, tables);
+			b.SetPtr(L + 3, d_off);
+			b.SetPtr(L + 4, d_caps);
+			LaunchGenerated(*module, "vgpu_gb_bucket_global",
+			                static_cast<unsigned>(std::min<uint64_t>(list.size(), uint64_t(props.sm_count) * 2)), 512, 0,
+			                stream_, b, 0, 0);
+			if (ReadU32(control + 1) != 0) {
+				Fail(VGPU_ERR_INTERNAL, "gpu_groupby: global-table fallback overflowed");
+			}
+		}
+		groups = ReadU64(out_count);
+	}
+	if (node.group_keys.empty() && groups == 0) {
+		Fail(VGPU_ERR_UNSUPPORTED, kEmptyGlobal);
+	}
+	for (auto &c : out) c.rows = groups;
+	return out;
+}
+
+// ---- HASH_JOIN (sort-merge) ------------------------------------------------------------------------
+
+Relation Executor::Join(const PlanNode &node) {
+	if (node.children.size() != 2) {
+		Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: HASH_JOIN expects exactly two children");
+	}
+	if (node.build_keys.size() != 1 || node.probe_keys.size() != 1) {
+		Fail(VGPU_ERR_UNSUPPORTED, "gpu_hash_join: this GPU path joins on exactly one equality key column");
+	}
+	if (node.output_columns.empty()) {
+		Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_hash_join: node has no output columns");
+	}
+	Relation left = Exec(*node.children[0]);
+	Relation right = Exec(*node.children[1]);
+	auto find = [](const Relation &rel, const std::string &name, const char *side) -> const DevColumn & {
+		for (auto &c : rel) {
+			if (c.name == name) return c;
+		}
+		Fail(VGPU_ERR_INVALID_ARGUMENT, std::string("gpu_hash_join: ") + side + " key column '" + name + "' not found");
+	};
+	const DevColumn &lk = find(left, node.build_keys[0], "left");
+	const DevColumn &rk = find(right, node.probe_keys[0], "right");
+	for (auto *k : {&lk, &rk}) {
+		if (!IsIntegerKeyType(k->type)) {
+			Fail(VGPU_ERR_UNSUPPORTED, std::string("gpu_hash_join: ") + (k == &lk ? "left" : "right") +
+			                               " join key is not an integer/boolean column, which this GPU path requires");
+		}
+	}
+	if (lk.type != rk.type) {
+		Fail(VGPU_ERR_UNSUPPORTED, "gpu_hash_join: join key columns must have the same type on both sides");
+	}
+	std::vector<const DevColumn *> sources;
+	std::vector<bool> from_left;
+	for (auto &name : node.output_columns) {
+		const DevColumn *l = nullptr, *r = nullptr;
+		for (auto &c : left) if (c.name == name) { l = &c; break; }
+		for (auto &c : right) if (c.name == name) { r = &c; break; }
+		if (l && r) Fail(VGPU_ERR_UNSUPPORTED, "gpu_hash_join: output column '" + name + "' is ambiguous (present on both sides)");
+		if (!l && !r) Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_hash_join: output column '" + name + "' not found on either side");
+		sources.push_back(l ? l : r);
+		from_left.push_back(l != nullptr);
+	}
+	const uint64_t ln = lk.rows, rn = rk.rows;
+	auto make_out = [&](uint64_t rows) {
+		Relation out;
+		for (size_t i = 0; i < sources.size(); i++) {
+			DevColumn c;
+			c.name = node.output_columns[i];
+			c.type = sources[i]->type;
+			c.rows = rows;
+			c.data = arena_.Alloc(rows * TypeSize(c.type));
+			c.has_stats = sources[i]->has_stats;
+			c.min = sources[i]->min;
+			c.max = sources[i]->max;
+			out.push_back(c);
+		}
+		return out;
+	};
+	if (ln == 0 || rn == 0) {
+		return make_out(0);
+	}
+	if (ln >= (1ull << 32) || rn >= (1ull << 32)) Fail(VGPU_ERR_UNSUPPORTED, "gpu_hash_join: side too large");
+	const size_t kw = TypeSize(lk.type);
+	uint64_t *lw = arena_.AllocT<uint64_t>(ln);
+	uint64_t *rw = arena_.AllocT<uint64_t>(rn);
+	kern::WidenKeys(lk.data, kw, ln, lw, stream_);
+	kern::WidenKeys(rk.data, kw, rn, rw, stream_);
+	uint64_t *mm = arena_.AllocT<uint64_t>(2);
+	kern::MinMaxU64(rw, rn, mm, stream_);
+	uint64_t host_mm[2];
+	VGPU_CUDA(cudaMemcpyAsync(host_mm, mm, 16, cudaMemcpyDeviceToHost, stream_));
+	VGPU_CUDA(cudaStreamSynchronize(stream_));
+	const uint64_t bias = host_mm[0];
+	const int bits = BitsFor(host_mm[1] - host_mm[0]);
+	kern::SubtractBias(rw, rn, bias, stream_);
+	uint32_t *perm = arena_.AllocT<uint32_t>(rn);
+	kern::Iota(perm, rn, stream_);
+	uint64_t *rw_alt = arena_.AllocT<uint64_t>(rn);
+	uint32_t *perm_alt = arena_.AllocT<uint32_t>(rn);
+	kern::RadixSortPairs(rw, perm, rw_alt, perm_alt, rn, bits, arena_);
+	arena_.FreeNow(rw_alt);
+	arena_.FreeNow(perm_alt);
+	uint64_t *lower = arena_.AllocT<uint64_t>(ln);
+	uint64_t *counts = arena_.AllocT<uint64_t>(ln);
+	kern::JoinSearch(lw, ln, rw, rn, bias, lower, counts, stream_);
+	uint64_t *total = arena_.AllocT<uint64_t>(1);
+	kern::ExclusiveScanU64(counts, counts, ln, total, arena_);
+	const uint64_t total_rows = ReadU64(total);
+	if (total_rows > kMaxOutputRows) {
+		Fail(VGPU_ERR_UNSUPPORTED, "gpu_hash_join: join result of " + std::to_string(total_rows) +
+		                               " rows is too large for GPU execution");
+	}
+	Relation out = make_out(total_rows);
+	if (total_rows == 0) return out;
+	uint32_t *out_left = arena_.AllocT<uint32_t>(total_rows);
+	uint32_t *out_right = arena_.AllocT<uint32_t>(total_rows);
+	kern::JoinExpand(counts, lower, ln, perm, total_rows, out_left, out_right, stream_);
+	for (size_t i = 0; i < sources.size(); i++) {
+		kern::Gather(sources[i]->data, TypeSize(sources[i]->type), from_left[i] ? out_left : out_right, total_rows,
+		             out[i].data, stream_);
+	}
+	return out;
+}
+
+Relation Executor::Exec(const PlanNode &node) {
+	switch (node.op) {
+	case OpType::SCAN:
+		return Scan(node);
+	case OpType::FILTER:
+	case OpType::PROJECTION:
+		return RunChain(node);
+	case OpType::GROUP_BY_AGGREGATE:
+		return GroupBy(node);
+	case OpType::HASH_JOIN:
+		return Join(node);
+	case OpType::CROSS_PRODUCT:
+		return CrossProduct(node);
+	}
+	Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: unknown GpuOpType value");
+}
+
+} // namespace
+
+ExecResult ExecutePlan(const PlanNode &plan, const std::vector<vgpu_column> &inputs, const ExecOptions &options,
+                       cudaStream_t stream) {
+	Runtime::Get().EnsureDevice();
+	Executor ex(inputs, options, stream, IsRowIndependent(plan));
+	Relation rel = ex.Exec(plan);
+	ExecResult result;
+	result.stream = stream;
+	for (auto &c : rel) {
+		HostColumnOut o;
+		o.name = c.name;
+		o.type = c.type;
+		o.rows = c.rows;
+		const size_t bytes = c.rows * TypeSize(c.type);
+		if (options.output_on_device) {
+			// Copy into buffers the result owns, so borrowed inputs/cache entries are never aliased.
+			void *d = Runtime::Get().allocator().Alloc(bytes, stream);
+			result.device_buffers.push_back(d);
+			if (bytes) VGPU_CUDA(cudaMemcpyAsync(d, c.data, bytes, cudaMemcpyDeviceToDevice, stream));
+			o.device_data = d;
+			if (c.valid) {
+				const size_t vb = (c.rows + 7) / 8;
+				uint8_t *bm = static_cast<uint8_t *>(Runtime::Get().allocator().Alloc(vb, stream));
+				result.device_buffers.push_back(bm);
+				kern::PackValidity(c.valid, bm, c.rows, stream);
+				o.device_validity = bm;
+			}
+		} else {
+			o.data.resize(bytes);
+			if (bytes) VGPU_CUDA(cudaMemcpyAsync(o.data.data(), c.data, bytes, cudaMemcpyDeviceToHost, stream));
+			if (c.valid && c.rows > 0) {
+				const size_t vb = (c.rows + 7) / 8;
+				uint8_t *bm = ex.arena().AllocT<uint8_t>(vb);
+				kern::PackValidity(c.valid, bm, c.rows, stream);
+				o.validity.resize(vb);
+				VGPU_CUDA(cudaMemcpyAsync(o.validity.data(), bm, vb, cudaMemcpyDeviceToHost, stream));
+			}
+		}
+		result.columns.push_back(std::move(o));
+	}
+	if (!(options.output_on_device && options.no_sync)) {
+		VGPU_CUDA(cudaStreamSynchronize(stream));
+	}
+	return result;
+}
+
+} // namespace vgpu

@@ -1,0 +1,525 @@
+// kernels.cu -- precompiled device primitives (see kernels.hpp).
+#include "kernels.hpp"
+
+#include <utility>
+
+#include "device_lib.cuh"
+
+namespace vgpu {
+namespace kern {
+
+using namespace vgpu_dev;
+
+namespace {
+
+constexpr int kScanBlock = 512;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanBlock * kScanItems;
+
+unsigned GridFor(uint64_t n, int block) {
+	uint64_t g = (n + block - 1) / block;
+	if (g == 0) {
+		g = 1;
+	}
+	const uint64_t cap = static_cast<uint64_t>(Runtime::Get().props().sm_count) * 32;
+	return static_cast<unsigned>(g < cap ? g : cap);
+}
+
+template <typename T> __device__ __forceinline__ T BlockScanExclusive(T v, T *scratch /*33*/, T *total) {
+	const int lane = threadIdx.x & 31;
+	const int warp = threadIdx.x >> 5;
+	const int nwarps = blockDim.x >> 5;
+	T x = v;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		T y = __shfl_up_sync(0xffffffffu, x, o);
+		if (lane >= o) x += y;
+	}
+	if (lane == 31) scratch[warp] = x;
+	__syncthreads();
+	if (warp == 0) {
+		T w = (lane < nwarps) ? scratch[lane] : T(0);
+		T s = w;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			T y = __shfl_up_sync(0xffffffffu, s, o);
+			if (lane >= o) s += y;
+		}
+		if (lane < nwarps) scratch[lane] = s - w;
+		if (lane == 31) scratch[32] = s;
+	}
+	__syncthreads();
+	T r = scratch[warp] + x - v;
+	*total = scratch[32];
+	__syncthreads();
+	return r;
+}
+
+template <typename T> __global__ void __launch_bounds__(kScanBlock) ScanTileSums(const T *in, uint64_t n, T *sums) {
+	__shared__ T scratch[33];
+	const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kScanTile + static_cast<uint64_t>(threadIdx.x) * kScanItems;
+	T local = 0;
+#pragma unroll
+	for (int i = 0; i < kScanItems; i++) {
+		if (base + i < n) local += in[base + i];
+	}
+	T total;
+	BlockScanExclusive<T>(local, scratch, &total);
+	if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+// Single CTA: exclusive scan of the tile sums in place, grand total to *total.
+template <typename T> __global__ void __launch_bounds__(1024) ScanSums(T *sums, uint64_t count, T *total) {
+	__shared__ T scratch[33];
+	T carry = 0;
+	for (uint64_t c0 = 0; c0 < count; c0 += blockDim.x) {
+		const uint64_t i = c0 + threadIdx.x;
+		T v = i < count ? sums[i] : T(0);
+		T chunk_total;
+		T ex = BlockScanExclusive<T>(v, scratch, &chunk_total);
+		if (i < count) sums[i] = carry + ex;
+		carry += chunk_total;
+	}
+	if (threadIdx.x == 0 && total) *total = carry;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kScanBlock) ScanApply(const T *in, T *out, uint64_t n, const T *sums) {
+	__shared__ T scratch[33];
+	const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kScanTile + static_cast<uint64_t>(threadIdx.x) * kScanItems;
+	T vals[kScanItems];
+	T local = 0;
+#pragma unroll
+	for (int i = 0; i < kScanItems; i++) {
+		vals[i] = base + i < n ? in[base + i] : T(0);
+		local += vals[i];
+	}
+	T total;
+	T run = BlockScanExclusive<T>(local, scratch, &total) + sums[blockIdx.x];
+#pragma unroll
+	for (int i = 0; i < kScanItems; i++) {
+		if (base + i < n) out[base + i] = run;
+		run += vals[i];
+	}
+}
+
+template <typename T> void ExclusiveScan(const T *in, T *out, uint64_t n, T *total, Arena &arena) {
+	cudaStream_t s = arena.stream();
+	const uint64_t tiles = n == 0 ? 1 : (n + kScanTile - 1) / kScanTile;
+	T *sums = arena.AllocT<T>(tiles);
+	{
+		LaunchScope scope("scan_tiles", s, n * sizeof(T), n);
+		ScanTileSums<T><<<static_cast<unsigned>(tiles), kScanBlock, 0, s>>>(in, n, sums);
+	}
+	{
+		LaunchScope scope("scan_sums", s, tiles * sizeof(T), tiles);
+		ScanSums<T><<<1, 1024, 0, s>>>(sums, tiles, total);
+	}
+	if (n > 0) {
+		LaunchScope scope("scan_apply", s, 2 * n * sizeof(T), n);
+		ScanApply<T><<<static_cast<unsigned>(tiles), kScanBlock, 0, s>>>(in, out, n, sums);
+	}
+	VGPU_CUDA(cudaGetLastError());
+}
+
+__global__ void UnpackValidityKernel(const uint8_t *bitmap, uint8_t *bytes, uint64_t n) {
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+		bytes[i] = (bitmap[i >> 3] >> (i & 7)) & 1u;
+	}
+}
+
+__global__ void PackValidityKernel(const uint8_t *bytes, uint8_t *bitmap, uint64_t n) {
+	const uint64_t nbytes = (n + 7) / 8;
+	for (uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; b < nbytes; b += (uint64_t)gridDim.x * blockDim.x) {
+		uint8_t v = 0;
+		for (int k = 0; k < 8; k++) {
+			uint64_t i = b * 8 + k;
+			if (i < n && bytes[i]) v |= static_cast<uint8_t>(1u << k);
+		}
+		bitmap[b] = v;
+	}
+}
+
+template <typename T> __global__ void GatherKernel(const T *src, const uint32_t *idx, uint64_t n, T *dst) {
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+		dst[i] = src[idx[i]];
+	}
+}
+
+template <typename T> __global__ void WidenKernel(const T *src, uint64_t n, uint64_t *dst) {
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+		dst[i] = static_cast<uint64_t>(src[i]);
+	}
+}
+
+__global__ void MinMaxKernel(const uint64_t *keys, uint64_t n, uint64_t *minmax) {
+	uint64_t mn = ~0ull, mx = 0;
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+		uint64_t k = keys[i];
+		mn = k < mn ? k : mn;
+		mx = k > mx ? k : mx;
+	}
+	for (int o = 16; o > 0; o >>= 1) {
+		uint64_t a = __shfl_xor_sync(0xffffffffu, mn, o);
+		uint64_t b = __shfl_xor_sync(0xffffffffu, mx, o);
+		mn = a < mn ? a : mn;
+		mx = b > mx ? b : mx;
+	}
+	if ((threadIdx.x & 31) == 0) {
+		atomicMin(reinterpret_cast<unsigned long long *>(&minmax[0]), mn);
+		atomicMax(reinterpret_cast<unsigned long long *>(&minmax[1]), mx);
+	}
+}
+
+template <typename T> __global__ void MinMaxSignedKernel(const T *data, uint64_t n, int64_t *out) {
+	int64_t mn = INT64_MAX, mx = INT64_MIN;
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+		const int64_t v = static_cast<int64_t>(data[i]);
+		mn = v < mn ? v : mn;
+		mx = v > mx ? v : mx;
+	}
+	for (int o = 16; o > 0; o >>= 1) {
+		int64_t a = __shfl_xor_sync(0xffffffffu, mn, o);
+		int64_t b = __shfl_xor_sync(0xffffffffu, mx, o);
+		mn = a < mn ? a : mn;
+		mx = b > mx ? b : mx;
+	}
+	if ((threadIdx.x & 31) == 0) {
+		atomicMin(reinterpret_cast<long long *>(&out[0]), static_cast<long long>(mn));
+		atomicMax(reinterpret_cast<long long *>(&out[1]), static_cast<long long>(mx));
+	}
+}
+
+__global__ void InitMinMaxSignedKernel(int64_t *out) {
+	out[0] = INT64_MAX;
+	out[1] = INT64_MIN;
+}
+
+__global__ void InitMinMaxKernel(uint64_t *minmax) {
+	minmax[0] = ~0ull;
+	minmax[1] = 0ull;
+}
+
+__global__ void SubtractBiasKernel(uint64_t *keys, uint64_t n, uint64_t bias) {
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+		keys[i] -= bias;
+	}
+}
+
+__global__ void IotaKernel(uint32_t *out, uint64_t n) {
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+		out[i] = static_cast<uint32_t>(i);
+	}
+}
+
+// ---- LSD radix sort: 8-bit digits, stable warp-ordered local ranking ----------------------------
+
+constexpr int kSortBlock = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortBlock * kSortItems;
+constexpr int kSortWarps = kSortBlock / 32;
+
+__device__ __forceinline__ uint32_t LaneMaskLt() {
+	uint32_t m;
+	asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+	return m;
+}
+
+__global__ void __launch_bounds__(kSortBlock) RadixHistKernel(const uint64_t *keys, uint64_t n, int shift,
+                                                              uint32_t *hist, uint32_t ntiles) {
+	__shared__ uint32_t counts[256];
+	for (int i = threadIdx.x; i < 256; i += kSortBlock) counts[i] = 0;
+	__syncthreads();
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kSortTile + static_cast<uint64_t>(warp) * 32 * kSortItems;
+#pragma unroll 4
+	for (int k = 0; k < kSortItems; k++) {
+		const uint64_t idx = base + static_cast<uint64_t>(k) * 32 + lane;
+		const bool valid = idx < n;
+		const uint32_t active = __ballot_sync(0xffffffffu, valid);
+		if (valid) {
+			const uint32_t d = static_cast<uint32_t>(keys[idx] >> shift) & 255u;
+			const uint32_t peers = __match_any_sync(active, d);
+			if ((peers & LaneMaskLt()) == 0) atomicAdd(&counts[d], static_cast<uint32_t>(__popc(peers)));
+		}
+	}
+	__syncthreads();
+	for (int d = threadIdx.x; d < 256; d += kSortBlock) hist[static_cast<uint64_t>(d) * ntiles + blockIdx.x] = counts[d];
+}
+
+__global__ void __launch_bounds__(kSortBlock) RadixScatterKernel(const uint64_t *kin, const uint32_t *vin,
+                                                                 uint64_t *kout, uint32_t *vout, uint64_t n, int shift,
+                                                                 const uint32_t *offsets, uint32_t ntiles) {
+	__shared__ uint32_t wcount[kSortWarps][256];
+	for (int i = threadIdx.x; i < kSortWarps * 256; i += kSortBlock) (&wcount[0][0])[i] = 0;
+	__syncthreads();
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kSortTile + static_cast<uint64_t>(warp) * 32 * kSortItems;
+	uint64_t keys[kSortItems];
+	uint32_t vals[kSortItems];
+	uint32_t rank[kSortItems];
+#pragma unroll
+	for (int k = 0; k < kSortItems; k++) {
+		const uint64_t idx = base + static_cast<uint64_t>(k) * 32 + lane;
+		const bool valid = idx < n;
+		keys[k] = valid ? kin[idx] : 0ull;
+		vals[k] = valid ? vin[idx] : 0u;
+	}
+#pragma unroll
+	for (int k = 0; k < kSortItems; k++) {
+		const uint64_t idx = base + static_cast<uint64_t>(k) * 32 + lane;
+		const bool valid = idx < n;
+		const uint32_t active = __ballot_sync(0xffffffffu, valid);
+		uint32_t peers = 0, d = 0;
+		if (valid) {
+			d = static_cast<uint32_t>(keys[k] >> shift) & 255u;
+			peers = __match_any_sync(active, d);
+			rank[k] = wcount[warp][d] + static_cast<uint32_t>(__popc(peers & LaneMaskLt()));
+		}
+		__syncwarp();
+		if (valid && (peers & LaneMaskLt()) == 0) wcount[warp][d] += static_cast<uint32_t>(__popc(peers));
+		__syncwarp();
+	}
+	__syncthreads();
+	if (threadIdx.x < 256) {
+		uint32_t run = 0;
+		for (int w = 0; w < kSortWarps; w++) {
+			uint32_t c = wcount[w][threadIdx.x];
+			wcount[w][threadIdx.x] = run;
+			run += c;
+		}
+	}
+	__syncthreads();
+#pragma unroll
+	for (int k = 0; k < kSortItems; k++) {
+		const uint64_t idx = base + static_cast<uint64_t>(k) * 32 + lane;
+		if (idx < n) {
+			const uint32_t d = static_cast<uint32_t>(keys[k] >> shift) & 255u;
+			const uint32_t pos = offsets[static_cast<uint64_t>(d) * ntiles + blockIdx.x] + wcount[warp][d] + rank[k];
+			kout[pos] = keys[k];
+			vout[pos] = vals[k];
+		}
+	}
+}
+
+// ---- join -----------------------------------------------------------------------------------------
+
+__global__ void JoinSearchKernel(const uint64_t *probe, uint64_t n_probe, const uint64_t *sorted, uint64_t n_sorted,
+                                 uint64_t bias, uint64_t range, uint64_t *lower, uint64_t *count) {
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_probe; i += (uint64_t)gridDim.x * blockDim.x) {
+		const uint64_t x = probe[i];
+		uint64_t lo = 0, c = 0;
+		if (x >= bias && x - bias <= range) {
+			const uint64_t k = x - bias;
+			uint64_t a = 0, b = n_sorted;
+			while (a < b) {
+				uint64_t mid = (a + b) >> 1;
+				if (sorted[mid] < k) a = mid + 1; else b = mid;
+			}
+			lo = a;
+			uint64_t e = a;
+			b = n_sorted;
+			while (e < b) {
+				uint64_t mid = (e + b) >> 1;
+				if (sorted[mid] <= k) e = mid + 1; else b = mid;
+			}
+			c = e - lo;
+		}
+		lower[i] = lo;
+		count[i] = c;
+	}
+}
+
+__global__ void JoinExpandKernel(const uint64_t *offsets, const uint64_t *lower, uint64_t n_left,
+                                 const uint32_t *sorted_perm, uint64_t total, uint32_t *out_left, uint32_t *out_right) {
+	for (uint64_t o = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; o < total; o += (uint64_t)gridDim.x * blockDim.x) {
+		// last left row whose offset <= o (rows with zero matches share offsets; the upper bound skips them)
+		uint64_t a = 0, b = n_left;
+		while (a < b) {
+			uint64_t mid = (a + b) >> 1;
+			if (offsets[mid] <= o) a = mid + 1; else b = mid;
+		}
+		const uint64_t i = a - 1;
+		const uint64_t j = o - offsets[i];
+		out_left[o] = static_cast<uint32_t>(i);
+		out_right[o] = sorted_perm[lower[i] + j];
+	}
+}
+
+} // namespace
+
+void ExclusiveScanU32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *total, Arena &arena) {
+	ExclusiveScan<uint32_t>(in, out, n, total, arena);
+}
+
+void ExclusiveScanU64(const uint64_t *in, uint64_t *out, uint64_t n, uint64_t *total, Arena &arena) {
+	ExclusiveScan<uint64_t>(in, out, n, total, arena);
+}
+
+void UnpackValidity(const uint8_t *bitmap, uint8_t *bytes, uint64_t n, cudaStream_t stream) {
+	if (n == 0) return;
+	LaunchScope scope("unpack_validity", stream, n / 8 + n, n);
+	UnpackValidityKernel<<<GridFor(n, 256), 256, 0, stream>>>(bitmap, bytes, n);
+	VGPU_CUDA(cudaGetLastError());
+}
+
+void PackValidity(const uint8_t *bytes, uint8_t *bitmap, uint64_t n, cudaStream_t stream) {
+	if (n == 0) return;
+	LaunchScope scope("pack_validity", stream, n + n / 8, n);
+	PackValidityKernel<<<GridFor((n + 7) / 8, 256), 256, 0, stream>>>(bytes, bitmap, n);
+	VGPU_CUDA(cudaGetLastError());
+}
+
+void Gather(const void *src, size_t width, const uint32_t *idx, uint64_t n, void *dst, cudaStream_t stream) {
+	if (n == 0) return;
+	LaunchScope scope("gather", stream, n * (width * 2 + 4), n);
+	const unsigned grid = GridFor(n, 256);
+	switch (width) {
+	case 1:
+		GatherKernel<uint8_t><<<grid, 256, 0, stream>>>(static_cast<const uint8_t *>(src), idx, n, static_cast<uint8_t *>(dst));
+		break;
+	case 2:
+		GatherKernel<uint16_t><<<grid, 256, 0, stream>>>(static_cast<const uint16_t *>(src), idx, n, static_cast<uint16_t *>(dst));
+		break;
+	case 4:
+		GatherKernel<uint32_t><<<grid, 256, 0, stream>>>(static_cast<const uint32_t *>(src), idx, n, static_cast<uint32_t *>(dst));
+		break;
+	case 8:
+		GatherKernel<uint64_t><<<grid, 256, 0, stream>>>(static_cast<const uint64_t *>(src), idx, n, static_cast<uint64_t *>(dst));
+		break;
+	case 16:
+		GatherKernel<uint4><<<grid, 256, 0, stream>>>(static_cast<const uint4 *>(src), idx, n, static_cast<uint4 *>(dst));
+		break;
+	default:
+		Fail(VGPU_ERR_INTERNAL, "gather: unsupported width");
+	}
+	VGPU_CUDA(cudaGetLastError());
+}
+
+void WidenKeys(const void *src, size_t width, uint64_t n, uint64_t *dst, cudaStream_t stream) {
+	if (n == 0) return;
+	LaunchScope scope("widen_keys", stream, n * (width + 8), n);
+	const unsigned grid = GridFor(n, 256);
+	switch (width) {
+	case 1:
+		WidenKernel<uint8_t><<<grid, 256, 0, stream>>>(static_cast<const uint8_t *>(src), n, dst);
+		break;
+	case 2:
+		WidenKernel<uint16_t><<<grid, 256, 0, stream>>>(static_cast<const uint16_t *>(src), n, dst);
+		break;
+	case 4:
+		WidenKernel<uint32_t><<<grid, 256, 0, stream>>>(static_cast<const uint32_t *>(src), n, dst);
+		break;
+	case 8:
+		WidenKernel<uint64_t><<<grid, 256, 0, stream>>>(static_cast<const uint64_t *>(src), n, dst);
+		break;
+	default:
+		Fail(VGPU_ERR_INTERNAL, "widen: unsupported width");
+	}
+	VGPU_CUDA(cudaGetLastError());
+}
+
+void MinMaxU64(const uint64_t *keys, uint64_t n, uint64_t *minmax, cudaStream_t stream) {
+	LaunchScope scope("minmax", stream, n * 8, n);
+	InitMinMaxKernel<<<1, 1, 0, stream>>>(minmax);
+	if (n > 0) {
+		MinMaxKernel<<<GridFor(n, 256), 256, 0, stream>>>(keys, n, minmax);
+	}
+	VGPU_CUDA(cudaGetLastError());
+}
+
+void MinMaxSigned(const void *data, int type, uint64_t n, int64_t *out, cudaStream_t stream) {
+	LaunchScope scope("minmax_signed", stream, n * 8, n);
+	InitMinMaxSignedKernel<<<1, 1, 0, stream>>>(out);
+	if (n > 0) {
+		const unsigned grid = GridFor(n, 256);
+		switch (static_cast<ValueType>(type)) {
+		case ValueType::INT16:
+			MinMaxSignedKernel<int16_t><<<grid, 256, 0, stream>>>(static_cast<const int16_t *>(data), n, out);
+			break;
+		case ValueType::INT32:
+		case ValueType::DICTIONARY_STRING:
+			MinMaxSignedKernel<int32_t><<<grid, 256, 0, stream>>>(static_cast<const int32_t *>(data), n, out);
+			break;
+		case ValueType::INT64:
+			MinMaxSignedKernel<int64_t><<<grid, 256, 0, stream>>>(static_cast<const int64_t *>(data), n, out);
+			break;
+		case ValueType::BOOLEAN:
+			MinMaxSignedKernel<uint8_t><<<grid, 256, 0, stream>>>(static_cast<const uint8_t *>(data), n, out);
+			break;
+		default:
+			Fail(VGPU_ERR_INTERNAL, "min/max statistics need an integer column");
+		}
+	}
+	VGPU_CUDA(cudaGetLastError());
+}
+
+void RadixSortPairs(uint64_t *keys, uint32_t *values, uint64_t *keys_alt, uint32_t *values_alt, uint64_t n, int bits,
+                    Arena &arena) {
+	if (n <= 1 || bits <= 0) return;
+	cudaStream_t s = arena.stream();
+	const uint64_t ntiles64 = (n + kSortTile - 1) / kSortTile;
+	if (ntiles64 > 0xffffffffull) Fail(VGPU_ERR_UNSUPPORTED, "radix sort: too many rows");
+	const uint32_t ntiles = static_cast<uint32_t>(ntiles64);
+	uint32_t *hist = arena.AllocT<uint32_t>(static_cast<size_t>(ntiles) * 256);
+	uint32_t *total = arena.AllocT<uint32_t>(1);
+	uint64_t *kin = keys, *kout = keys_alt;
+	uint32_t *vin = values, *vout = values_alt;
+	const int passes = (bits + 7) / 8;
+	for (int p = 0; p < passes; p++) {
+		const int shift = 8 * p;
+		{
+			LaunchScope scope("radix_hist", s, n * 8, n);
+			RadixHistKernel<<<ntiles, kSortBlock, 0, s>>>(kin, n, shift, hist, ntiles);
+		}
+		ExclusiveScanU32(hist, hist, static_cast<uint64_t>(ntiles) * 256, total, arena);
+		{
+			LaunchScope scope("radix_scatter", s, n * 24, n);
+			RadixScatterKernel<<<ntiles, kSortBlock, 0, s>>>(kin, vin, kout, vout, n, shift, hist, ntiles);
+		}
+		VGPU_CUDA(cudaGetLastError());
+		std::swap(kin, kout);
+		std::swap(vin, vout);
+	}
+	if (kin != keys) {
+		VGPU_CUDA(cudaMemcpyAsync(keys, kin, n * 8, cudaMemcpyDeviceToDevice, s));
+		VGPU_CUDA(cudaMemcpyAsync(values, vin, n * 4, cudaMemcpyDeviceToDevice, s));
+	}
+}
+
+void SubtractBias(uint64_t *keys, uint64_t n, uint64_t bias, cudaStream_t stream) {
+	if (n == 0 || bias == 0) return;
+	LaunchScope scope("subtract_bias", stream, n * 16, n);
+	SubtractBiasKernel<<<GridFor(n, 256), 256, 0, stream>>>(keys, n, bias);
+	VGPU_CUDA(cudaGetLastError());
+}
+
+void Iota(uint32_t *out, uint64_t n, cudaStream_t stream) {
+	if (n == 0) return;
+	LaunchScope scope("iota", stream, n * 4, n);
+	IotaKernel<<<GridFor(n, 256), 256, 0, stream>>>(out, n);
+	VGPU_CUDA(cudaGetLastError());
+}
+
+void JoinSearch(const uint64_t *probe, uint64_t n_probe, const uint64_t *sorted, uint64_t n_sorted, uint64_t bias,
+                uint64_t *lower, uint64_t *count, cudaStream_t stream) {
+	if (n_probe == 0) return;
+	LaunchScope scope("join_search", stream, n_probe * 24, n_probe);
+	// range of normalized keys: sorted is ascending, so its last element bounds every match.
+	// (Passed as n_sorted-based sentinel: any k > sorted[n-1] finds no equal key anyway.)
+	JoinSearchKernel<<<GridFor(n_probe, 256), 256, 0, stream>>>(probe, n_probe, sorted, n_sorted, bias, ~0ull, lower,
+	                                                            count);
+	VGPU_CUDA(cudaGetLastError());
+}
+
+void JoinExpand(const uint64_t *offsets, const uint64_t *lower, uint64_t n_left, const uint32_t *sorted_perm,
+                uint64_t total, uint32_t *out_left, uint32_t *out_right, cudaStream_t stream) {
+	if (total == 0) return;
+	LaunchScope scope("join_expand", stream, total * 8, total);
+	JoinExpandKernel<<<GridFor(total, 256), 256, 0, stream>>>(offsets, lower, n_left, sorted_perm, total, out_left,
+	                                                          out_right);
+	VGPU_CUDA(cudaGetLastError());
+}
+
+} // namespace kern
+} // namespace vgpu

@@ -1,0 +1,52 @@
+// kernels.hpp -- precompiled (nvcc, sm_100a) device primitives used by the executor. Every entry
+// point launches on the given stream, takes temporaries from the given arena and never synchronizes.
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "runtime.hpp"
+
+namespace vgpu {
+namespace kern {
+
+//! out[i] = sum(in[0..i)), *total = sum(in) (device scalar). In-place (out == in) is allowed.
+void ExclusiveScanU32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *total, Arena &arena);
+void ExclusiveScanU64(const uint64_t *in, uint64_t *out, uint64_t n, uint64_t *total, Arena &arena);
+
+//! Arrow LSB-first bitmap <-> one byte per row.
+void UnpackValidity(const uint8_t *bitmap, uint8_t *bytes, uint64_t n, cudaStream_t stream);
+void PackValidity(const uint8_t *bytes, uint8_t *bitmap, uint64_t n, cudaStream_t stream);
+
+//! dst[o] = src[idx[o]] for `width`-byte values (1, 2, 4, 8 or 16).
+void Gather(const void *src, size_t width, const uint32_t *idx, uint64_t n, void *dst, cudaStream_t stream);
+
+//! Raw key bits zero-extended to 64 bits (the reference's WidenKeyKernel semantics,
+//! cuda_engine/src/operators/gpu_groupby.cu:76-94), plus the range of the widened values.
+void WidenKeys(const void *src, size_t width, uint64_t n, uint64_t *dst, cudaStream_t stream);
+void MinMaxU64(const uint64_t *keys, uint64_t n, uint64_t *minmax /* device [2] */, cudaStream_t stream);
+
+//! Signed range of an integer/boolean column: out[0] = min, out[1] = max (device i64[2]).
+void MinMaxSigned(const void *data, int type /* ValueType */, uint64_t n, int64_t *out, cudaStream_t stream);
+
+//! Stable LSD radix sort of (key, value) pairs over the low `bits` bits of the keys (8-bit digits).
+//! Results end in (keys, values); (keys_alt, values_alt) are the ping-pong buffers.
+void RadixSortPairs(uint64_t *keys, uint32_t *values, uint64_t *keys_alt, uint32_t *values_alt, uint64_t n, int bits,
+                    Arena &arena);
+
+//! keys[i] -= bias (normalizes a key range to start at zero before sorting).
+void SubtractBias(uint64_t *keys, uint64_t n, uint64_t bias, cudaStream_t stream);
+void Iota(uint32_t *out, uint64_t n, cudaStream_t stream);
+
+//! For each probe key (widened): the first index of an equal key in `sorted` (normalized by
+//! `bias`) and how many equal keys follow.
+void JoinSearch(const uint64_t *probe, uint64_t n_probe, const uint64_t *sorted, uint64_t n_sorted, uint64_t bias,
+                uint64_t *lower, uint64_t *count, cudaStream_t stream);
+
+//! One thread per output pair: left row i owns outputs [offsets[i], offsets[i] + count[i]).
+void JoinExpand(const uint64_t *offsets, const uint64_t *lower, uint64_t n_left, const uint32_t *sorted_perm,
+                uint64_t total, uint32_t *out_left, uint32_t *out_right, cudaStream_t stream);
+
+} // namespace kern
+} // namespace vgpu

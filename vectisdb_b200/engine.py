@@ -1,0 +1,533 @@
+"""Host-side mirror of the reference engine interface (cuda_engine/include/gpu_engine.hpp) over the
+C ABI of libvgpu.so: the same names, argument meanings and success/error_message contract, so parity
+tests read like the reference's own tests (cuda_engine/tests/test_gpu_executor.cpp).
+
+    plan = make_group_by(["k"], [make_aggregate(GpuAggregateKind.SUM, "v", GpuValueType.FLOAT64)],
+                         make_scan(["k", "v"]))
+    result = GpuEngine.instance().execute_plan(plan, [make_column("k", GpuValueType.INT32, k), ...])
+    if result.success: keys = result.columns[0].data
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import abi
+
+
+class GpuOpType(enum.IntEnum):  # gpu_engine.hpp:14-21
+    SCAN = 0
+    FILTER = 1
+    PROJECTION = 2
+    HASH_JOIN = 3
+    GROUP_BY_AGGREGATE = 4
+    CROSS_PRODUCT = 5
+
+
+class GpuValueType(enum.IntEnum):  # gpu_engine.hpp:29-38
+    INT16 = 0
+    INT32 = 1
+    INT64 = 2
+    FLOAT32 = 3
+    FLOAT64 = 4
+    BOOLEAN = 5
+    DICTIONARY_STRING = 6
+    HUGEINT = 7
+
+
+class GpuAggregateKind(enum.IntEnum):  # gpu_engine.hpp:85-92
+    COUNT_STAR = 0
+    COUNT = 1
+    SUM = 2
+    MIN = 3
+    MAX = 4
+    AVG = 5
+
+
+HUGEINT_DTYPE = np.dtype([("lower", "<u8"), ("upper", "<i8")])
+
+NUMPY_DTYPE = {
+    GpuValueType.INT16: np.dtype("<i2"),
+    GpuValueType.INT32: np.dtype("<i4"),
+    GpuValueType.INT64: np.dtype("<i8"),
+    GpuValueType.FLOAT32: np.dtype("<f4"),
+    GpuValueType.FLOAT64: np.dtype("<f8"),
+    GpuValueType.BOOLEAN: np.dtype("u1"),
+    GpuValueType.DICTIONARY_STRING: np.dtype("<i4"),
+    GpuValueType.HUGEINT: HUGEINT_DTYPE,
+}
+
+
+def hugeint_to_int(values: np.ndarray) -> list[int]:
+    """GpuHugeInt rows -> Python ints (two's complement over 128 bits)."""
+    return [int(v["upper"]) * (1 << 64) + int(v["lower"]) for v in values]
+
+
+@dataclass
+class GpuExpr:  # gpu_engine.hpp:56-80
+    generated_cuda_source: str
+    input_columns: list[str]
+    output_type: GpuValueType = GpuValueType.FLOAT64
+    source_hash: str = ""
+
+
+@dataclass
+class GpuAggregate:  # gpu_engine.hpp:96-104
+    kind: GpuAggregateKind = GpuAggregateKind.COUNT_STAR
+    input_column: str = ""
+    output_type: GpuValueType = GpuValueType.INT64
+
+
+@dataclass
+class GpuTableRef:
+    catalog: str = "memory"
+    schema: str = "main"
+    table: str = "t"
+
+
+@dataclass
+class GpuPlanNode:  # gpu_engine.hpp:135-185
+    op_type: GpuOpType = GpuOpType.SCAN
+    children: list["GpuPlanNode"] = field(default_factory=list)
+    estimated_rows: int = 0
+    estimated_row_width_bytes: int = 0
+    table: GpuTableRef = field(default_factory=GpuTableRef)
+    column_names: list[str] = field(default_factory=list)
+    expressions: list[GpuExpr] = field(default_factory=list)
+    build_keys: list[str] = field(default_factory=list)
+    probe_keys: list[str] = field(default_factory=list)
+    output_columns: list[str] = field(default_factory=list)
+    group_keys: list[str] = field(default_factory=list)
+    aggregate_exprs: list[str] = field(default_factory=list)
+    aggregates: list[GpuAggregate] = field(default_factory=list)
+
+
+@dataclass
+class GpuColumn:  # gpu_engine.hpp:199-213
+    name: str
+    type: GpuValueType
+    data: Optional[np.ndarray] = None      # host values (or None when device_ptr is set)
+    validity: Optional[np.ndarray] = None  # bool per row (True = valid) or None
+    row_count: int = 0
+    device_ptr: int = 0                    # device address (device-resident column)
+
+    def __post_init__(self):
+        if self.data is not None and self.row_count == 0:
+            self.row_count = len(self.data)
+
+
+@dataclass
+class GpuExecutionResult:  # gpu_engine.hpp:215-222
+    success: bool = False
+    error_message: str = ""
+    status: int = 0
+    columns: list[GpuColumn] = field(default_factory=list)
+
+
+# ---- builders mirroring cuda_engine/tests/test_gpu_executor.cpp:24-119 ------------------------------
+
+def make_column(name: str, type_: GpuValueType, values, validity=None) -> GpuColumn:
+    arr = np.ascontiguousarray(np.asarray(values, dtype=NUMPY_DTYPE[GpuValueType(type_)]))
+    v = None if validity is None else np.asarray(validity, dtype=bool)
+    return GpuColumn(name, GpuValueType(type_), arr, v, len(arr))
+
+
+def make_device_column(name: str, type_: GpuValueType, device_ptr: int, rows: int) -> GpuColumn:
+    return GpuColumn(name, GpuValueType(type_), None, None, rows, device_ptr)
+
+
+def make_scan(columns: Sequence[str], table: GpuTableRef | None = None) -> GpuPlanNode:
+    return GpuPlanNode(GpuOpType.SCAN, table=table or GpuTableRef(), column_names=list(columns))
+
+
+def make_expr(body: str, inputs: Sequence[str], out_type: GpuValueType) -> GpuExpr:
+    return GpuExpr(body, list(inputs), GpuValueType(out_type))
+
+
+def make_filter(exprs: Sequence[GpuExpr], child: GpuPlanNode) -> GpuPlanNode:
+    return GpuPlanNode(GpuOpType.FILTER, [child], expressions=list(exprs))
+
+
+def make_projection(exprs: Sequence[GpuExpr], child: GpuPlanNode) -> GpuPlanNode:
+    return GpuPlanNode(GpuOpType.PROJECTION, [child], expressions=list(exprs))
+
+
+def make_aggregate(kind: GpuAggregateKind, input_column: str, output_type: GpuValueType) -> GpuAggregate:
+    return GpuAggregate(GpuAggregateKind(kind), input_column, GpuValueType(output_type))
+
+
+def make_group_by(keys: Sequence[str], aggregates: Sequence[GpuAggregate], child: GpuPlanNode) -> GpuPlanNode:
+    return GpuPlanNode(GpuOpType.GROUP_BY_AGGREGATE, [child], group_keys=list(keys), aggregates=list(aggregates))
+
+
+def make_join(left_key: str, right_key: str, output_columns: Sequence[str], left: GpuPlanNode,
+              right: GpuPlanNode) -> GpuPlanNode:
+    return GpuPlanNode(GpuOpType.HASH_JOIN, [left, right], build_keys=[left_key], probe_keys=[right_key],
+                       output_columns=list(output_columns))
+
+
+def make_cross_product(output_columns: Sequence[str], left: GpuPlanNode, right: GpuPlanNode) -> GpuPlanNode:
+    return GpuPlanNode(GpuOpType.CROSS_PRODUCT, [left, right], output_columns=list(output_columns))
+
+
+# ---- serialization to the C ABI ---------------------------------------------------------------------
+
+class _Keep:
+    """Owns every ctypes buffer a serialized plan points into."""
+
+    def __init__(self):
+        self.refs: list = []
+
+    def s(self, text: str | None):
+        if text is None:
+            return None
+        b = C.c_char_p(text.encode())
+        self.refs.append(b)
+        return b.value
+
+    def names(self, items: Sequence[str]):
+        if not items:
+            return None, 0
+        arr = (C.c_char_p * len(items))(*[t.encode() for t in items])
+        self.refs.append(arr)
+        return C.cast(arr, C.POINTER(C.c_char_p)), len(items)
+
+
+def serialize_plan(plan: GpuPlanNode, keep: _Keep) -> abi.vgpu_plan:
+    flat: list[GpuPlanNode] = []
+    index: dict[int, int] = {}
+
+    def visit(node: GpuPlanNode) -> int:
+        i = len(flat)
+        flat.append(node)
+        index[id(node)] = i
+        for child in node.children:
+            visit(child)
+        return i
+
+    visit(plan)
+    nodes = (abi.vgpu_plan_node * len(flat))()
+    for i, node in enumerate(flat):
+        n = nodes[i]
+        n.op = int(node.op_type)
+        child_idx = [index[id(c)] for c in node.children]
+        if child_idx:
+            arr = (C.c_uint32 * len(child_idx))(*child_idx)
+            keep.refs.append(arr)
+            n.children = C.cast(arr, C.POINTER(C.c_uint32))
+        n.n_children = len(child_idx)
+        n.catalog = node.table.catalog.encode()
+        n.schema = node.table.schema.encode()
+        n.table = node.table.table.encode()
+        n.column_names, n.n_column_names = keep.names(node.column_names)
+        if node.expressions:
+            exprs = (abi.vgpu_expr * len(node.expressions))()
+            for j, e in enumerate(node.expressions):
+                exprs[j].source = e.generated_cuda_source.encode()
+                exprs[j].input_columns, exprs[j].n_input_columns = keep.names(e.input_columns)
+                exprs[j].output_type = int(e.output_type)
+            keep.refs.append(exprs)
+            n.expressions = C.cast(exprs, C.POINTER(abi.vgpu_expr))
+        n.n_expressions = len(node.expressions)
+        n.build_keys, n.n_build_keys = keep.names(node.build_keys)
+        n.probe_keys, n.n_probe_keys = keep.names(node.probe_keys)
+        n.output_columns, n.n_output_columns = keep.names(node.output_columns)
+        n.group_keys, n.n_group_keys = keep.names(node.group_keys)
+        if node.aggregates:
+            aggs = (abi.vgpu_aggregate * len(node.aggregates))()
+            for j, a in enumerate(node.aggregates):
+                aggs[j].kind = int(a.kind)
+                aggs[j].output_type = int(a.output_type)
+                aggs[j].input_column = a.input_column.encode() if a.input_column else None
+            keep.refs.append(aggs)
+            n.aggregates = C.cast(aggs, C.POINTER(abi.vgpu_aggregate))
+        n.n_aggregates = len(node.aggregates)
+        n.estimated_rows = node.estimated_rows
+        n.estimated_row_width_bytes = node.estimated_row_width_bytes
+    keep.refs.append(nodes)
+    plan_c = abi.vgpu_plan()
+    plan_c.nodes = C.cast(nodes, C.POINTER(abi.vgpu_plan_node))
+    plan_c.n_nodes = len(flat)
+    plan_c.root = 0
+    return plan_c
+
+
+def pack_validity(valid: np.ndarray) -> np.ndarray:
+    """bool per row -> Arrow LSB-first bitmap."""
+    return np.packbits(np.asarray(valid, dtype=bool), bitorder="little")
+
+
+def serialize_inputs(inputs: Sequence[GpuColumn], keep: _Keep):
+    arr = (abi.vgpu_column * max(1, len(inputs)))()
+    for i, col in enumerate(inputs):
+        c = arr[i]
+        c.name = col.name.encode()
+        c.type = int(col.type)
+        c.row_count = col.row_count
+        if col.device_ptr:
+            c.memory = abi.MEM_DEVICE
+            c.data = col.device_ptr
+        else:
+            c.memory = abi.MEM_HOST
+            data = np.ascontiguousarray(col.data) if col.data is not None else None
+            if data is not None:
+                keep.refs.append(data)
+                c.data = data.ctypes.data if data.size else None
+        if col.validity is not None:
+            bm = pack_validity(col.validity)
+            keep.refs.append(bm)
+            c.validity = bm.ctypes.data
+    keep.refs.append(arr)
+    return arr
+
+
+def _read_result(handle) -> list[GpuColumn]:
+    L = abi.lib()
+    cols = []
+    for i in range(L.vgpu_result_column_count(handle)):
+        c = abi.vgpu_column()
+        abi.check(L.vgpu_result_get_column(handle, i, C.byref(c)))
+        t = GpuValueType(c.type)
+        dt = NUMPY_DTYPE[t]
+        n = int(c.row_count)
+        if c.memory == abi.MEM_DEVICE:
+            cols.append(GpuColumn(c.name.decode(), t, None, None, n, int(c.data or 0)))
+            continue
+        if n and c.data:
+            buf = (C.c_uint8 * (n * dt.itemsize)).from_address(c.data)
+            data = np.frombuffer(bytes(buf), dtype=dt).copy()
+        else:
+            data = np.zeros(0, dtype=dt)
+        validity = None
+        if c.validity and n:
+            vb = (C.c_uint8 * ((n + 7) // 8)).from_address(c.validity)
+            validity = np.unpackbits(np.frombuffer(bytes(vb), dtype=np.uint8), bitorder="little")[:n].astype(bool)
+        cols.append(GpuColumn(c.name.decode(), t, data, validity, n))
+    return cols
+
+
+@dataclass
+class ExecuteOptions:  # GpuExecuteOptions (gpu_engine.hpp:357-385) + placement
+    stage_scan_to_cache: bool = False
+    serve_whole_scan_from_cache: bool = False
+    cache_chunk_index: int = -1
+    output_on_device: bool = False
+    no_sync: bool = False
+    stream: int = 0
+
+
+class DeviceResult:
+    """A result left on the device (output_on_device=True). Free it (or use `with`) when done."""
+
+    def __init__(self, handle, columns: list[GpuColumn]):
+        self._handle = handle
+        self.columns = columns
+
+    def free(self):
+        if self._handle:
+            abi.lib().vgpu_result_free(self._handle)
+            self._handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.free()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class GpuEngine:
+    """GpuEngine::Instance().ExecutePlan (gpu_engine.hpp:389-402) over the C ABI."""
+
+    _instance: "GpuEngine | None" = None
+
+    @classmethod
+    def instance(cls) -> "GpuEngine":
+        if cls._instance is None:
+            cls._instance = GpuEngine()
+        return cls._instance
+
+    def __init__(self):
+        self.lib = abi.lib()
+
+    def execute_plan(self, plan: GpuPlanNode, inputs: Sequence[GpuColumn],
+                     options: ExecuteOptions | None = None):
+        keep = _Keep()
+        plan_c = serialize_plan(plan, keep)
+        cols = serialize_inputs(inputs, keep)
+        opts = abi.vgpu_exec_options()
+        self.lib.vgpu_exec_options_init(C.byref(opts))
+        o = options or ExecuteOptions()
+        opts.serve_whole_scan_from_cache = int(o.serve_whole_scan_from_cache)
+        opts.stage_scan_to_cache = int(o.stage_scan_to_cache)
+        opts.cache_chunk_index = o.cache_chunk_index
+        opts.output_memory = abi.MEM_DEVICE if o.output_on_device else abi.MEM_HOST
+        opts.flags = abi.EXEC_NO_SYNC if o.no_sync else 0
+        opts.stream = o.stream or None
+        handle = C.c_void_p()
+        status = self.lib.vgpu_execute_plan(C.byref(plan_c), cols, len(inputs), C.byref(opts), C.byref(handle))
+        if status != abi.OK:
+            return GpuExecutionResult(False, abi.last_error(), status, [])
+        try:
+            columns = _read_result(handle)
+        except Exception:
+            self.lib.vgpu_result_free(handle)
+            raise
+        if o.output_on_device:
+            return DeviceResult(handle, columns)
+        self.lib.vgpu_result_free(handle)
+        return GpuExecutionResult(True, "", abi.OK, columns)
+
+
+# ---- engine-level helpers -----------------------------------------------------------------------------
+
+def sha256_hex(data: bytes) -> str:
+    out = C.create_string_buffer(65)
+    abi.lib().vgpu_sha256_hex(data, len(data), out)
+    return out.value.decode()
+
+
+def generate_source(plan: GpuPlanNode, inputs: Sequence[GpuColumn]) -> str:
+    keep = _Keep()
+    plan_c = serialize_plan(plan, keep)
+    cols = serialize_inputs(inputs, keep)
+    n = C.c_size_t()
+    L = abi.lib()
+    abi.check(L.vgpu_generate_source(C.byref(plan_c), cols, len(inputs), None, 0, C.byref(n)))
+    buf = C.create_string_buffer(n.value + 1)
+    abi.check(L.vgpu_generate_source(C.byref(plan_c), cols, len(inputs), buf, n.value + 1, C.byref(n)))
+    return buf.value.decode()
+
+
+def nvrtc_compile_check(source: str) -> int:
+    n = C.c_size_t()
+    abi.check(abi.lib().vgpu_nvrtc_compile_check(source.encode(), C.byref(n)))
+    return n.value
+
+
+def is_row_independent(plan: GpuPlanNode) -> bool:
+    keep = _Keep()
+    return bool(abi.lib().vgpu_is_row_independent(C.byref(serialize_plan(plan, keep))))
+
+
+def estimate_working_set(plan: GpuPlanNode, max_chunk_rows: int = 0) -> abi.vgpu_working_set:
+    keep = _Keep()
+    ws = abi.vgpu_working_set()
+    abi.check(abi.lib().vgpu_estimate_working_set(C.byref(serialize_plan(plan, keep)), max_chunk_rows, C.byref(ws)))
+    return ws
+
+
+def profile_enable(on: bool = True) -> None:
+    abi.check(abi.lib().vgpu_profile_enable(1 if on else 0))
+
+
+def profile_drain() -> list[tuple[str, float, int, int]]:
+    """Synchronizes and returns (kernel, ms, algorithmic bytes, rows) per engine launch since the last drain."""
+    L = abi.lib()
+    cap = 1 << 16
+    arr = (abi.vgpu_kernel_timing * cap)()
+    n = C.c_size_t()
+    abi.check(L.vgpu_profile_collect(arr, cap, C.byref(n)))
+    return [(arr[i].name.decode(), float(arr[i].ms), int(arr[i].bytes), int(arr[i].rows)) for i in range(min(n.value, cap))]
+
+
+def launch_count() -> int:
+    return int(abi.lib().vgpu_launch_count())
+
+
+def device_info() -> abi.vgpu_device_info:
+    info = abi.vgpu_device_info()
+    abi.check(abi.lib().vgpu_get_device_info(C.byref(info)))
+    return info
+
+
+def kernel_cache_stats() -> abi.vgpu_kernel_cache_stats:
+    s = abi.vgpu_kernel_cache_stats()
+    abi.check(abi.lib().vgpu_kernel_cache_stats_get(C.byref(s)))
+    return s
+
+
+def _table(t: GpuTableRef, keep: _Keep) -> abi.vgpu_table_ref:
+    ref = abi.vgpu_table_ref(t.catalog.encode(), t.schema.encode(), t.table.encode())
+    keep.refs.append(ref)
+    return ref
+
+
+class ColumnCache:
+    """GpuColumnCache (gpu_column_cache.hpp:107-281) over the C ABI."""
+
+    @staticmethod
+    def init(fraction: float = 0.5) -> None:
+        abi.check(abi.lib().vgpu_cache_init(fraction))
+
+    @staticmethod
+    def begin_staging(table: GpuTableRef) -> None:
+        keep = _Keep()
+        abi.check(abi.lib().vgpu_cache_begin_staging(C.byref(_table(table, keep))))
+
+    @staticmethod
+    def stage_chunk(table: GpuTableRef, column: GpuColumn) -> bool:
+        keep = _Keep()
+        arr = serialize_inputs([column], keep)
+        ok = C.c_int()
+        abi.check(abi.lib().vgpu_cache_stage_chunk(C.byref(_table(table, keep)), arr, C.byref(ok)))
+        return bool(ok.value)
+
+    @staticmethod
+    def commit_staging(table: GpuTableRef, scanned_rows: int) -> None:
+        keep = _Keep()
+        abi.check(abi.lib().vgpu_cache_commit_staging(C.byref(_table(table, keep)), scanned_rows))
+
+    @staticmethod
+    def abort_staging(table: GpuTableRef) -> None:
+        keep = _Keep()
+        abi.check(abi.lib().vgpu_cache_abort_staging(C.byref(_table(table, keep))))
+
+    @staticmethod
+    def replayable_chunk_rows(table: GpuTableRef, columns: Sequence[str]) -> list[int]:
+        keep = _Keep()
+        names, n = keep.names(columns)
+        cap = 4096
+        rows = (C.c_uint64 * cap)()
+        cnt = C.c_size_t()
+        abi.check(abi.lib().vgpu_cache_replayable_chunk_rows(C.byref(_table(table, keep)), names, n, rows, cap,
+                                                             C.byref(cnt)))
+        return [int(rows[i]) for i in range(min(cnt.value, cap))]
+
+    @staticmethod
+    def invalidate_table(table: GpuTableRef) -> None:
+        keep = _Keep()
+        abi.check(abi.lib().vgpu_cache_invalidate_table(C.byref(_table(table, keep))))
+
+    @staticmethod
+    def invalidate_all() -> None:
+        abi.check(abi.lib().vgpu_cache_invalidate_all())
+
+    @staticmethod
+    def current_bytes() -> int:
+        return int(abi.lib().vgpu_cache_current_bytes())
+
+    @staticmethod
+    def table_generation(table: GpuTableRef) -> int:
+        keep = _Keep()
+        return int(abi.lib().vgpu_cache_table_generation(C.byref(_table(table, keep))))
+
+    @staticmethod
+    def put_table(table: GpuTableRef, columns: Sequence[GpuColumn]) -> None:
+        """Stages every column as one chunk and commits (convenience for resident base tables)."""
+        ColumnCache.begin_staging(table)
+        rows = columns[0].row_count if columns else 0
+        for col in columns:
+            if not ColumnCache.stage_chunk(table, col):
+                ColumnCache.abort_staging(table)
+                raise abi.VgpuError(abi.ERR_OUT_OF_MEMORY, f"cache declined column {col.name}")
+        ColumnCache.commit_staging(table, rows)
