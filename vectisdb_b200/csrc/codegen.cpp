@@ -274,6 +274,11 @@ void PipelineCodegen::Resolve() {
 						}
 					}
 				}
+				// The chain code evaluates every projection, so every source it reads must be loaded
+				// (loads whose values end up unused are dead code the compiler drops).
+				for (int s : d) {
+					chain_sources_[s] = true;
+				}
 				c.nullable = nullable;
 				if (!nullable) {
 					c.valid = "true";

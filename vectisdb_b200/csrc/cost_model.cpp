@@ -192,8 +192,12 @@ std::string GenerateSourceText(const PlanNode &plan, const std::vector<vgpu_colu
 		spec_gb.aggs.push_back(s);
 	}
 	g.block = 512;
-	// Two translation units, separated by a marker line.
-	return cg.EmitGroupBy(spec_gb, false, g) + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_gb, true, g);
+	std::vector<int> key_columns;
+	for (auto &k : spec_gb.keys) key_columns.push_back(k.column);
+	Geometry gs;
+	// Separate translation units, separated by a marker line: direct, partitioned, key statistics.
+	return cg.EmitGroupBy(spec_gb, false, g) + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_gb, true, g) +
+	       "\n//@@VGPU_TU@@\n" + cg.EmitStats(key_columns, gs);
 }
 
 } // namespace vgpu

@@ -298,14 +298,14 @@ def _read_result(handle) -> list[GpuColumn]:
             cols.append(GpuColumn(c.name.decode(), t, None, None, n, int(c.data or 0)))
             continue
         if n and c.data:
-            buf = (C.c_uint8 * (n * dt.itemsize)).from_address(c.data)
-            data = np.frombuffer(bytes(buf), dtype=dt).copy()
+            raw = np.ctypeslib.as_array(C.cast(c.data, C.POINTER(C.c_uint8)), shape=(n * dt.itemsize,))
+            data = raw.copy().view(dt)
         else:
             data = np.zeros(0, dtype=dt)
         validity = None
         if c.validity and n:
-            vb = (C.c_uint8 * ((n + 7) // 8)).from_address(c.validity)
-            validity = np.unpackbits(np.frombuffer(bytes(vb), dtype=np.uint8), bitorder="little")[:n].astype(bool)
+            vb = np.ctypeslib.as_array(C.cast(c.validity, C.POINTER(C.c_uint8)), shape=((n + 7) // 8,))
+            validity = np.unpackbits(vb, bitorder="little")[:n].astype(bool)
         cols.append(GpuColumn(c.name.decode(), t, data, validity, n))
     return cols
 
