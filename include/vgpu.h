@@ -301,6 +301,23 @@ vgpu_status vgpu_cache_invalidate_all(void);
 uint64_t vgpu_cache_current_bytes(void);
 uint64_t vgpu_cache_table_generation(const vgpu_table_ref *table);
 
+/* ---- Group-by without device allocation ------------------------------------------------------
+ * No counterpart in the reference. For callers that cannot call cudaMalloc (a host callback or a
+ * graph-driven loop, a process whose device memory another allocator has reserved, a caller holding a
+ * lock an allocation could deadlock on): SELECT k, COUNT(*), SUM(v) GROUP BY k over keys in
+ * [key_min, key_min + domain), domain <= 65536. All pointers are device memory the caller owns;
+ * out_keys/out_counts/out_sums hold `domain` entries and receive the non-empty groups in key order,
+ * *out_groups their number. Rows with keys outside the range are skipped. Temporaries live in a fixed
+ * file-scope device array (about 1 MiB, held by every GPU that loads the library until exit), so the
+ * call allocates nothing; a larger domain is rejected with VGPU_ERR_INVALID_ARGUMENT. The first call
+ * on a device looks up that array's device address (cudaGetSymbolAddress) and should come before any
+ * stream capture. Work is queued on `stream` (NULL = legacy default stream) and not synchronized.
+ * Every call shares the one array, which keeps the last call's contents: calls whose work overlaps on
+ * the GPU (different streams, no ordering between them) race and corrupt each other's results. */
+vgpu_status vgpu_group_by_count_sum_noalloc(const int32_t *keys, const double *values, uint64_t n, int32_t key_min,
+                                            uint32_t domain, int32_t *out_keys, int64_t *out_counts,
+                                            double *out_sums, uint64_t *out_groups, void *stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

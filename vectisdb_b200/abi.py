@@ -129,6 +129,8 @@ SIGNATURES = [
     ("vgpu_cache_invalidate_all", C.c_int, []),
     ("vgpu_cache_current_bytes", C.c_uint64, []),
     ("vgpu_cache_table_generation", C.c_uint64, [C.POINTER(vgpu_table_ref)]),
+    ("vgpu_group_by_count_sum_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32, C.c_uint32,
+                                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 ]
 
 _LIB = None

@@ -51,6 +51,16 @@ template <typename F> vgpu_status Guard(F &&f) {
 	}
 }
 
+} // namespace
+
+namespace vgpu {
+void SetLastError(const std::string &message) {
+	g_last_error = message;
+}
+} // namespace vgpu
+
+namespace {
+
 TableRef ToTable(const vgpu_table_ref *t) {
 	if (t == nullptr) Fail(VGPU_ERR_INVALID_ARGUMENT, "null table reference");
 	return TableRef {t->catalog ? t->catalog : "", t->schema ? t->schema : "", t->table ? t->table : ""};
