@@ -95,3 +95,24 @@ def test_c2b_filtered_cross_product(side):
     count, ea, eb = O.c2b(a, b, 13)
     assert len(cols[0].data) == count
     assert np.array_equal(cols[0].data, ea) and np.array_equal(cols[1].data, eb)  # left-major order
+
+
+@pytest.mark.parametrize("tier1,retry", [("256", None), ("256", "64")])
+def test_c1_overflow_tiers_stay_exact(tier1, retry, monkeypatch):
+    """Tables far too small for their partitions: tier-1 overflows go to the device retry list, and
+    (with a tiny retry table too) on to the global-memory pass; the answer must not change."""
+    monkeypatch.setenv("VGPU_GB_TABLE_SLOTS", tier1)
+    if retry:
+        monkeypatch.setenv("VGPU_GB_RETRY_SLOTS", retry)
+    monkeypatch.setenv("VGPU_GB_PARTITIONS", "64")
+    wl = W.c1(n=1 << 18)
+    a, b, amt, v, ts = [c.data for c in wl.inputs]
+    cols = _run(wl)
+    ga, gb, gsum, gavg, gcnt, gmax = [c.data for c in cols]
+    order = np.lexsort((gb, ga))
+    exp = O.c1(a, b, amt, v, ts, wl.params["ts_gt"])
+    assert np.array_equal(ga[order], exp["a"]) and np.array_equal(gb[order], exp["b"])
+    assert np.array_equal(gcnt[order], exp["count"]) and np.array_equal(gmax[order], exp["max"])
+    gs = gsum[order]
+    assert np.array_equal(gs["lower"], exp["sum_lo"]) and np.array_equal(gs["upper"], exp["sum_hi"])
+    assert _close(gavg[order], exp["avg"])

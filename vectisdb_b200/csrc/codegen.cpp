@@ -361,6 +361,9 @@ std::string PipelineCodegen::LoadBlock(const Geometry &g, const std::vector<bool
 
 namespace {
 
+// KArgs word carrying the optional bucket diagnostics buffer (0 = off).
+constexpr int kDebugWord = 127;
+
 const char *kKernelHead = "\tconst u64 n = a.w[0];\n\tconst u64 m = a.w[1];\n\t(void)m;\n";
 
 } // namespace
@@ -595,7 +598,7 @@ std::string FinalizeCode(const PipelineCodegen::GroupBySpec &gb, const std::vect
 	for (auto &k : gb.keys) {
 		const auto &col = visible[k.column];
 		const char *t = CudaTypeName(col.type);
-		u_int64_t mask = k.bits >= 64 ? ~0ull : ((1ull << k.bits) - 1);
+		uint64_t mask = k.bits >= 64 ? ~0ull : ((1ull << k.bits) - 1);
 		o << "\t\t\t((" << t << "*)a.w[" << w << "])[" << pos << "] = (" << t << ")((i64)((" << key << " >> " << k.shift
 		  << ") & 0x" << std::hex << mask << std::dec << "ull) + (" << k.min << "LL));\n";
 		w++;
@@ -654,6 +657,24 @@ std::string FinalizeCode(const PipelineCodegen::GroupBySpec &gb, const std::vect
 
 int PipelineCodegen::StateWords(const GroupBySpec &gb) {
 	return static_cast<int>(StateFields(gb).size());
+}
+
+int PipelineCodegen::RecordStride(const GroupBySpec &gb) const {
+	// Same layout rule as EmitGroupBy: key u64, then each distinct carried value column at its
+	// natural alignment, rounded up to 32 bytes.
+	std::vector<int> value_cols;
+	for (auto &a : gb.aggs) {
+		if (a.column >= 0 && (a.kind != AggKind::COUNT && a.kind != AggKind::COUNT_STAR) &&
+		    std::find(value_cols.begin(), value_cols.end(), a.column) == value_cols.end()) {
+			value_cols.push_back(a.column);
+		}
+	}
+	int off = 8;
+	for (int c : value_cols) {
+		const int w = static_cast<int>(TypeSize(visible_[c].type));
+		off = (off + w - 1) / w * w + w;
+	}
+	return (off + 31) / 32 * 32;
 }
 
 std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned, const Geometry &g) const {
@@ -759,8 +780,44 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 	}
 
 	// ---- partitioned: radix partition on the mixed key, then one hash table per partition ----
+	// The intermediate is one fixed-size record per qualifying row: the packed key (u64) at byte 0,
+	// then each carried value at its natural width and alignment, stride RS a multiple of 32 bytes so
+	// every row's write covers whole sectors (no partial-sector read-modify-writes in DRAM however
+	// scattered the partitions are).
+	struct RecSlot {
+		int col, offset, width;
+	};
+	std::vector<RecSlot> rec;
+	int roff = 8;
+	for (int c : value_cols) {
+		const int w = static_cast<int>(TypeSize(visible_[c].type));
+		roff = (roff + w - 1) / w * w;
+		rec.push_back({c, roff, w});
+		roff += w;
+	}
+	const int RS = (roff + 31) / 32 * 32;
+	const int RW = RS / 4;
+	auto rec_value = [&](int col, const std::string &words) -> std::string {
+		for (auto &s : rec) {
+			if (s.col != col) continue;
+			const char *t = CudaTypeName(visible_[col].type);
+			const int wi = s.offset / 4, sh = (s.offset % 4) * 8;
+			std::string bits;
+			if (s.width == 8) {
+				bits = "((u64)" + words + "[" + std::to_string(wi) + "] | ((u64)" + words + "[" + std::to_string(wi + 1) +
+				       "] << 32))";
+			} else if (s.width == 4) {
+				bits = "(u64)" + words + "[" + std::to_string(wi) + "]";
+			} else {
+				const char *mask = s.width == 2 ? "0xffffu" : "0xffu";
+				bits = "(u64)((" + words + "[" + std::to_string(wi) + "] >> " + std::to_string(sh) + ") & " + mask + ")";
+			}
+			return "from_bits<" + std::string(t) + ">(" + bits + ")";
+		}
+		return "0";
+	};
 	// part_count / part_scatter args: cb+0 = P, cb+1 = pbits, cb+2 = tiles per CTA,
-	//   cb+3 = counts/offsets (u32, [p * G + cta]), cb+4 = keys out (u64), cb+5+v = value columns out.
+	//   cb+3 = counts/offsets (u32, [p * G + cta]), cb+4 = records out.
 	o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_gb_part_count(KArgs a) {\n"
 	  << kKernelHead << "\textern __shared__ __align__(16) u32 vgpu_hist[];\n"
 	  << "\tconst u32 P = (u32)a.w[" << cb << "]; const int pbits = (int)a.w[" << cb + 1 << "];\n"
@@ -773,14 +830,15 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 	  << "\t\t\tatomicAdd(&vgpu_hist[partition_of(" << pack.str() << ", pbits)], 1u);\n"
 	  << "\t\t}\n\t\t}\n\t}\n\t__syncthreads();\n"
 	  << "\tu32 *counts = (u32*)a.w[" << cb + 3 << "];\n"
-	  << "\tfor (u32 p = threadIdx.x; p < P; p += " << g.block << ") counts[(u64)p * gridDim.x + blockIdx.x] = vgpu_hist[p];\n}\n\n";
+	  << "\tfor (u32 p = threadIdx.x; p < P; p += " << g.block
+	  << ") counts[(u64)p * gridDim.x + blockIdx.x] = vgpu_hist[p];\n}\n\n";
 
 	o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_gb_part_scatter(KArgs a) {\n"
 	  << kKernelHead << "\textern __shared__ __align__(16) u32 vgpu_cursor[];\n"
 	  << "\tconst u32 P = (u32)a.w[" << cb << "]; const int pbits = (int)a.w[" << cb + 1 << "];\n"
 	  << "\tconst u64 tpc = a.w[" << cb + 2 << "];\n"
 	  << "\tconst u32 *offsets = (const u32*)a.w[" << cb + 3 << "];\n"
-	  << "\tu64 *keys_out = (u64*)a.w[" << cb + 4 << "];\n"
+	  << "\tchar *rec_out = (char*)a.w[" << cb + 4 << "];\n"
 	  << "\tfor (u32 p = threadIdx.x; p < P; p += " << g.block
 	  << ") vgpu_cursor[p] = offsets[(u64)p * gridDim.x + blockIdx.x];\n\t__syncthreads();\n"
 	  << tile_loop_head
@@ -789,91 +847,273 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 	  << LoadBlock(g, needed, true) << item_head << chain_code_ << "\t\tif (keep) {\n"
 	  << "\t\t\tconst u64 key = " << pack.str() << ";\n"
 	  << "\t\t\tconst u32 pos = atomicAdd(&vgpu_cursor[partition_of(key, pbits)], 1u);\n"
-	  << "\t\t\tkeys_out[pos] = key;\n";
-	for (size_t v = 0; v < value_cols.size(); v++) {
-		const auto &col = visible_[value_cols[v]];
-		o << "\t\t\t((" << CudaTypeName(col.type) << "*)a.w[" << cb + 5 + v << "])[pos] = " << col.value << ";\n";
+	  << "\t\t\tu32 rw[" << RW << "];\n"
+	  << "\t\t\t#pragma unroll\n\t\t\tfor (int q = 0; q < " << RW << "; ++q) rw[q] = 0u;\n"
+	  << "\t\t\trw[0] = (u32)key; rw[1] = (u32)(key >> 32);\n";
+	for (auto &s : rec) {
+		const auto &col = visible_[s.col];
+		const int wi = s.offset / 4, sh = (s.offset % 4) * 8;
+		o << "\t\t\t{ const u64 b = to_bits<" << CudaTypeName(col.type) << ">(" << col.value << ");\n";
+		if (s.width == 8) {
+			o << "\t\t\t  rw[" << wi << "] = (u32)b; rw[" << wi + 1 << "] = (u32)(b >> 32); }\n";
+		} else if (s.width == 4) {
+			o << "\t\t\t  rw[" << wi << "] = (u32)b; }\n";
+		} else {
+			o << "\t\t\t  rw[" << wi << "] |= ((u32)b & " << (s.width == 2 ? "0xffffu" : "0xffu") << ") << " << sh
+			  << "; }\n";
+		}
 	}
-	o << "\t\t}\n\t\t}\n\t}\n}\n\n";
+	o << "\t\t\tstore_record<" << RW << ">(rec_out + (u64)pos * " << RS << ", rw);\n"
+	  << "\t\t}\n\t\t}\n\t}\n}\n\n";
 
 	// bucket: args cb+0 = P, cb+1 = C (smem table slots), cb+2 = offsets (u32 [p*G]), cb+3 = G,
-	//   cb+4 = total ptr (u32*), cb+5 = keys in, cb+6+v = value columns in, then
-	//   W = cb+6+V: work counter (u32*), W+1 overflow flags (u32 [P]), W+2 overflow count (u32*),
-	//   W+3 output count (u64*), W+4.. outputs. Global-table variant: W+4+outs = partition list (u32*),
-	//   +1 list length, +2 table base (u64*), +3 per-list-entry table offsets (u64*), +4 capacities (u32*).
-	const int V = static_cast<int>(value_cols.size());
-	const int W = cb + 6 + V;
+	//   cb+4 = total ptr (u32*), cb+5 = records, then W = cb+6: work counter (u32*), W+1 overflow flags
+	//   (u32 [P]), W+2 overflow count (u32*), W+3 output count (u64*), W+4.. outputs. Global-table
+	//   variant: W+4+outs = partition list (u32*), +1 list length, +2 table base (u64*), +3 per-entry
+	//   table offsets (u64*), +4 capacities (u32*).
+	// Rows are read warp-contiguously: lane i of a warp takes record base + 32q + i, four 32-record
+	// steps per iteration with their loads hoisted. Lanes holding equal keys are found with
+	// __match_any_sync; when some group spans at least 4 lanes (a heavy key) the groups are combined by a
+	// rank tree of shuffles, so only each group's first lane updates the table. Counts are 32-bit
+	// atomics on the low half of the count word (a partition holds fewer than 2^32 rows).
+	const int W = cb + 6;
 	const int OUT = W + 4;
-	o << "__device__ __forceinline__ void vgpu_bucket_process(const KArgs &a, u32 p, u64 *tab, u32 C, bool *overflow) {\n"
+	std::ostringstream gdecl, gcomb, gupd, gxor, wdecl, wacc, wflush;
+	gdecl << "\t\t\tu32 gc = valid ? 1u : 0u;\n";
+	gxor << "\t\t\t\t\tgc += __shfl_xor_sync(0xffffffffu, gc, d);\n";
+	wdecl << "\tu64 my_pk = ~0ull; u64 wc = 0; u32 free_mask = 0xffu;\n"
+	      << "\tu64 pk_[8];\n\t#pragma unroll\n\tfor (int j = 0; j < 8; ++j) pk_[j] = ~0ull;\n";
+	wacc << "\t\t\t\t{ const u32 t_ = __shfl_sync(0xffffffffu, gc, src_); if (have_) wc += t_; }\n";
+	wflush << "\t\t\tatomicAdd((u32*)(T0 + s_), (u32)wc);\n";
+	gcomb << "\t\t\t\t\t{ const u32 o_ = __shfl_sync(0xffffffffu, gc, src_); if (take) gc += o_; }\n";
+	gupd << "\t\t\t\t\tatomicAdd((u32*)(T0 + s_), gc);\n";
+	for (int f = 1; f < F; f++) {
+		const auto &fd = fields[f];
+		const std::string v = "v" + std::to_string(fd.agg);
+		if (fd.kind == "f64") {
+			gdecl << "\t\t\tdouble gf" << f << " = valid ? (double)" << v << " : 0.0;\n";
+			gcomb << "\t\t\t\t\t{ const double o_ = __shfl_sync(0xffffffffu, gf" << f << ", src_); if (take) gf" << f
+			      << " += o_; }\n";
+			gupd << "\t\t\t\t\tatomicAdd((double*)(T" << f << " + s_), gf" << f << ");\n";
+			gxor << "\t\t\t\t\tgf" << f << " += __shfl_xor_sync(0xffffffffu, gf" << f << ", d);\n";
+			wdecl << "\tdouble wf" << f << " = 0.0;\n";
+			wacc << "\t\t\t\t{ const double t_ = __shfl_sync(0xffffffffu, gf" << f << ", src_); if (have_) wf" << f << " += t_; }\n";
+			wflush << "\t\t\tatomicAdd((double*)(T" << f << " + s_), wf" << f << ");\n";
+		} else if (fd.kind == "lo") {
+			gdecl << "\t\t\tu64 glo" << f << " = valid ? (u64)(i64)" << v << " : 0ull; i64 ghi" << f << " = (valid && (i64)"
+			      << v << " < 0) ? -1 : 0;\n";
+			gcomb << "\t\t\t\t\t{ const u64 ol_ = __shfl_sync(0xffffffffu, glo" << f
+			      << ", src_); const i64 oh_ = __shfl_sync(0xffffffffu, ghi" << f << ", src_);\n"
+			      << "\t\t\t\t\t  if (take) { const u64 nl_ = glo" << f << " + ol_; ghi" << f << " += oh_ + (nl_ < glo" << f
+			      << " ? 1 : 0); glo" << f << " = nl_; } }\n";
+			gupd << "\t\t\t\t\tatomic_add_i128_pair(T" << f << " + s_, (i64*)(T" << f + 1 << " + s_), glo" << f << ", ghi"
+			     << f << ");\n";
+			gxor << "\t\t\t\t\t{ const u64 ol_ = __shfl_xor_sync(0xffffffffu, glo" << f
+			     << ", d); const i64 oh_ = __shfl_xor_sync(0xffffffffu, ghi" << f << ", d); const u64 nl_ = glo" << f
+			     << " + ol_; ghi" << f << " += oh_ + (nl_ < glo" << f << " ? 1 : 0); glo" << f << " = nl_; }\n";
+			wdecl << "\tu64 wlo" << f << " = 0; i64 whi" << f << " = 0;\n";
+			wacc << "\t\t\t\t{ const u64 ol_ = __shfl_sync(0xffffffffu, glo" << f
+			     << ", src_); const i64 oh_ = __shfl_sync(0xffffffffu, ghi" << f << ", src_);\n"
+			     << "\t\t\t\t  if (have_) { const u64 nl_ = wlo" << f << " + ol_; whi" << f << " += oh_ + (nl_ < wlo" << f
+			     << " ? 1 : 0); wlo" << f << " = nl_; } }\n";
+			wflush << "\t\t\tatomic_add_i128_pair(T" << f << " + s_, (i64*)(T" << f + 1 << " + s_), wlo" << f << ", whi" << f
+			       << ");\n";
+		} else if (fd.kind == "min" || fd.kind == "max") {
+			const char *op = fd.kind == "min" ? "<" : ">";
+			const char *ident = fd.kind == "min" ? "0x7fffffffffffffffLL" : "(-0x7fffffffffffffffLL - 1)";
+			gdecl << "\t\t\ti64 gm" << f << " = valid ? (i64)" << v << " : " << ident << ";\n";
+			gcomb << "\t\t\t\t\t{ const i64 o_ = __shfl_sync(0xffffffffu, gm" << f << ", src_); if (take && o_ " << op
+			      << " gm" << f << ") gm" << f << " = o_; }\n";
+			gupd << "\t\t\t\t\tatomic_" << fd.kind << "_i64((i64*)(T" << f << " + s_), gm" << f << ");\n";
+			gxor << "\t\t\t\t\t{ const i64 o_ = __shfl_xor_sync(0xffffffffu, gm" << f << ", d); if (o_ " << op << " gm" << f
+			     << ") gm" << f << " = o_; }\n";
+			wdecl << "\ti64 wm" << f << " = " << ident << ";\n";
+			wacc << "\t\t\t\t{ const i64 t_ = __shfl_sync(0xffffffffu, gm" << f << ", src_); if (have_ && t_ " << op << " wm" << f
+			     << ") wm" << f << " = t_; }\n";
+			wflush << "\t\t\tatomic_" << fd.kind << "_i64((i64*)(T" << f << " + s_), wm" << f << ");\n";
+		}
+	}
+	o << "__device__ __forceinline__ int vgpu_find_slot(u64 *K, u32 C, u64 key, u32 limit) {\n"
+	  << "\tu32 slot = (u32)mix64(key) & (C - 1);\n"
+	  << "\tfor (u32 probe = 0; probe < limit; ++probe) {\n"
+	  << "\t\tconst u64 cur = *(volatile u64*)&K[slot];\n"
+	  << "\t\tif (cur == key) return (int)slot;\n"
+	  << "\t\tif (cur == ~0ull) {\n"
+	  << "\t\t\tconst u64 prev = atomicCAS((unsigned long long*)&K[slot], ~0ull, key);\n"
+	  << "\t\t\tif (prev == ~0ull || prev == key) return (int)slot;\n"
+	  << "\t\t}\n"
+	  << "\t\tslot = (slot + 1) & (C - 1);\n"
+	  << "\t}\n\treturn -1;\n}\n\n";
+	{
+		o << "__device__ __forceinline__ void vgpu_table_reset(u64 *tab, u32 C, u32 s) {\n\ttab[s] = ~0ull;\n";
+		for (int f = 0; f < F; f++) {
+			o << "\ttab[(u64)" << f + 1 << " * C + s] = " << InitValue(fields[f]) << ";\n";
+		}
+		o << "}\n\n__device__ __forceinline__ void vgpu_table_init(u64 *tab, u32 C) {\n"
+		  << "\tfor (u32 s = threadIdx.x; s < C; s += blockDim.x) vgpu_table_reset(tab, C, s);\n\t__syncthreads();\n}\n\n";
+	}
+	// probe runs longer than `limit` count as overflow: shared-memory tables give up after 64 probes
+	// (the partition is then retried with a larger table), global-memory tables probe all C slots
+	o << "__device__ __forceinline__ void vgpu_bucket_process(const KArgs &a, u32 p, u64 *tab, u32 C, u32 limit, bool *overflow) {\n"
 	  << "\tconst u32 P = (u32)a.w[" << cb << "];\n"
 	  << "\tconst u32 *offsets = (const u32*)a.w[" << cb + 2 << "];\n"
 	  << "\tconst u64 G = a.w[" << cb + 3 << "];\n"
 	  << "\tconst u32 total_rows = *(const u32*)a.w[" << cb + 4 << "];\n"
-	  << "\tconst u64 *keys_in = (const u64*)a.w[" << cb + 5 << "];\n";
-	for (int v = 0; v < V; v++) {
-		o << "\tconst void *vin" << v << " = (const void*)a.w[" << cb + 6 + v << "];\n";
-	}
-	o << "\tconst u32 start = offsets[(u64)p * G];\n"
-	  << "\tconst u32 end = (p + 1 < P) ? offsets[(u64)(p + 1) * G] : total_rows;\n"
+	  << "\tconst char *recs = (const char*)a.w[" << cb + 5 << "];\n"
+	  << "\tconst u64 start = offsets[(u64)p * G];\n"
+	  << "\tconst u64 end = (p + 1 < P) ? offsets[(u64)(p + 1) * G] : total_rows;\n"
+	  << "\tconst u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;\n"
+	  << "\tconst long long dbg_t0 = clock64();\n"
 	  << "\tu64 *K = tab;\n";
 	for (int f = 0; f < F; f++) {
 		o << "\tu64 *T" << f << " = tab + (u64)" << f + 1 << " * C;\n";
 	}
-	o << "\tfor (u32 s = threadIdx.x; s < C; s += blockDim.x) {\n\t\tK[s] = ~0ull;\n";
-	for (int f = 0; f < F; f++) {
-		o << "\t\tT" << f << "[s] = " << InitValue(fields[f]) << ";\n";
+	// The table is clean on entry (vgpu_table_init once per CTA; compaction resets what it visits).
+	// A warp keeps up to 8 pending runs for frequent keys: entry j lives in lane j (key my_pk, totals in
+	// its w* registers; every lane holds the 8 keys in pk_). A key is adopted once one of its groups
+	// spans 3 lanes of a step; later groups of that key are added in registers, so frequent keys cost no
+	// table atomics until the partition ends (64-bit and FP64 shared atomics are CAS loops that
+	// serialize badly on one hot word).
+	o << wdecl.str()
+	  << "\tfor (u64 base = start + (u64)warp * 128ull; base < end; base += (u64)nwarps * 128ull) {\n"
+	  << "\t\t// this table cannot hold the partition: stop early (one decision per warp, so the warp's\n"
+	  << "\t\t// lanes never split across the full-warp match/ballot/shuffle operations below)\n"
+	  << "\t\tif (__any_sync(0xffffffffu, *(volatile bool *)overflow)) break;\n"
+	  << "\t\tu32 rw[4][" << RW << "];\n"
+	  << "\t\t#pragma unroll\n\t\tfor (int q = 0; q < 4; ++q) {\n"
+	  << "\t\t\tconst u64 i = base + 32ull * q + lane;\n"
+	  << "\t\t\tload_record<" << RW << ">(recs + (i < end ? i : end - 1) * " << RS << ", rw[q]);\n\t\t}\n"
+	  << "\t\t#pragma unroll\n\t\tfor (int q = 0; q < 4; ++q) {\n"
+	  << "\t\t\tconst bool valid = base + 32ull * q + lane < end;\n"
+	  << "\t\t\tconst u64 key = valid ? ((u64)rw[q][0] | ((u64)rw[q][1] << 32)) : ~0ull;\n";
+	for (size_t i = 0; i < gb.aggs.size(); i++) {
+		const auto &ag = gb.aggs[i];
+		if (ag.column >= 0 && ag.kind != AggKind::COUNT && ag.kind != AggKind::COUNT_STAR) {
+			o << "\t\t\tconst " << CudaTypeName(visible_[ag.column].type) << " v" << i << " = "
+			  << rec_value(ag.column, "rw[q]") << ";\n";
+		}
 	}
-	o << "\t}\n\t__syncthreads();\n"
-	  << "\tfor (u32 i = start + threadIdx.x; i < end; i += blockDim.x) {\n"
-	  << "\t\tconst u64 key = keys_in[i];\n"
-	  << "\t\tu32 slot = (u32)mix64(key) & (C - 1);\n"
-	  << "\t\tbool found = false;\n"
-	  << "\t\tfor (u32 probe = 0; probe < C; ++probe) {\n"
-	  << "\t\t\tconst u64 cur = K[slot];\n"
-	  << "\t\t\tif (cur == key) { found = true; break; }\n"
-	  << "\t\t\tif (cur == ~0ull) {\n"
-	  << "\t\t\t\tconst u64 prev = atomicCAS(&K[slot], ~0ull, key);\n"
-	  << "\t\t\t\tif (prev == ~0ull || prev == key) { found = true; break; }\n"
+	o << gdecl.str()
+	  << "\t\t\tconst u32 peers = __match_any_sync(0xffffffffu, key);\n"
+	  << "\t\t\tbool leader = true;\n"
+	  << "\t\t\tif (peers == 0xffffffffu) {\n"
+	  << "\t\t\t\t#pragma unroll\n\t\t\t\tfor (int d = 16; d > 0; d >>= 1) {\n" << gxor.str() << "\t\t\t\t}\n"
+	  << "\t\t\t\tleader = lane == 0;\n"
+	  << "\t\t\t} else if (__ballot_sync(0xffffffffu, __popc(peers) >= 4)) {\n"
+	  << "\t\t\t\tconst u32 rank = __popc(peers & ((1u << lane) - 1u));\n"
+	  << "\t\t\t\tconst u32 size = __popc(peers);\n"
+	  << "\t\t\t\t#pragma unroll\n\t\t\t\tfor (u32 d = 1; d < 32; d <<= 1) {\n"
+	  << "\t\t\t\t\tconst u32 want = rank + d;\n"
+	  << "\t\t\t\t\tconst bool take = ((rank & (2 * d - 1)) == 0) && want < size;\n"
+	  << "\t\t\t\t\tconst u32 src_ = want < size ? __fns(peers, 0, (int)want + 1) : lane;\n"
+	  << gcomb.str()
+	  << "\t\t\t\t}\n"
+	  << "\t\t\t\tleader = rank == 0;\n"
 	  << "\t\t\t}\n"
-	  << "\t\t\tslot = (slot + 1) & (C - 1);\n"
-	  << "\t\t}\n"
-	  << "\t\tif (!found) { *overflow = true; break; }\n"
-	  << "\t\t{\n"
-	  << UpdateCode(fields, "T", "slot", part_values) << "\t\t}\n\t}\n\t__syncthreads();\n"
-	  << "\tif (*overflow) return;\n"
-	  << "\t__shared__ u32 scan_scratch[33];\n\t__shared__ u64 out_base;\n"
-	  << "\t// count live slots, reserve one output range, then write in slot order\n"
-	  << "\tu32 live = 0;\n"
-	  << "\tfor (u32 s = threadIdx.x; s < C; s += blockDim.x) live += (K[s] != ~0ull) ? 1u : 0u;\n"
-	  << "\tu32 live_total; block_exclusive_scan(live, scan_scratch, &live_total);\n"
-	  << "\tif (threadIdx.x == 0) out_base = atomicAdd((unsigned long long*)a.w[" << W + 3
-	  << "], (unsigned long long)live_total);\n"
+	  << "\t\t\t// groups whose key is pending hand their totals to the entry's lane\n"
+	  << "\t\t\tint pidx = -1;\n"
+	  << "\t\t\t#pragma unroll\n\t\t\tfor (int j = 0; j < 8; ++j) pidx = (valid && key == pk_[j]) ? j : pidx;\n"
+	  << "\t\t\tconst bool absorb = valid && leader && pidx >= 0;\n"
+	  << "\t\t\t// one pass per absorbing lane (warp-uniform count): every one of them is added\n"
+	  << "\t\t\tfor (u32 am_ = __ballot_sync(0xffffffffu, absorb); am_; am_ &= am_ - 1) {\n"
+	  << "\t\t\t\tconst u32 src_ = __ffs(am_) - 1;\n"
+	  << "\t\t\t\tconst bool have_ = (int)lane == __shfl_sync(0xffffffffu, pidx, src_);\n" << wacc.str()
+	  << "\t\t\t}\n"
+	  << "\t\t\tif (absorb) leader = false;\n"
+	  << "\t\t\t// adopt one new frequent key per step while entries are free\n"
+	  << "\t\t\tif (free_mask) {\n"
+	  << "\t\t\t\tconst u32 cand = __ballot_sync(0xffffffffu, valid && leader && __popc(peers) >= 3);\n"
+	  << "\t\t\t\tif (cand) {\n"
+	  << "\t\t\t\t\tconst u32 c_ = __ffs(cand) - 1, e_ = __ffs(free_mask) - 1;\n"
+	  << "\t\t\t\t\tconst u64 nk_ = __shfl_sync(0xffffffffu, key, c_);\n"
+	  << "\t\t\t\t\t#pragma unroll\n\t\t\t\t\tfor (int j = 0; j < 8; ++j) if ((u32)j == e_) pk_[j] = nk_;\n"
+	  << "\t\t\t\t\tfree_mask &= ~(1u << e_);\n"
+	  << "\t\t\t\t\tconst u32 src_ = c_; const bool have_ = lane == e_;\n"
+	  << "\t\t\t\t\tif (have_) my_pk = nk_;\n" << wacc.str()
+	  << "\t\t\t\t\tif (lane == c_) leader = false;\n"
+	  << "\t\t\t\t}\n"
+	  << "\t\t\t}\n"
+	  << "\t\t\tif (valid && leader) {\n"
+	  << "\t\t\t\tconst int s_ = vgpu_find_slot(K, C, key, limit);\n"
+	  << "\t\t\t\tif (s_ < 0) { *overflow = true; } else {\n"
+	  << gupd.str() << "\t\t\t\t}\n\t\t\t}\n\t\t}\n\t}\n"
+	  << "\tif (my_pk != ~0ull) {\n"
+	  << "\t\tconst int s_ = vgpu_find_slot(K, C, my_pk, limit);\n"
+	  << "\t\tif (s_ < 0) { *overflow = true; } else {\n" << wflush.str() << "\t\t}\n\t}\n"
 	  << "\t__syncthreads();\n"
-	  << "\tu64 base = out_base;\n"
-	  << "\tfor (u32 c0 = 0; c0 < C; c0 += blockDim.x) {\n"
-	  << "\t\tconst u32 s = c0 + threadIdx.x;\n"
-	  << "\t\tconst bool is_live = s < C && K[s] != ~0ull;\n"
-	  << "\t\tu32 chunk_total; const u32 off = block_exclusive_scan(is_live ? 1u : 0u, scan_scratch, &chunk_total);\n"
-	  << "\t\tif (is_live) {\n\t\t\tconst u64 pos = base + off;\n\t\t\tconst u64 key = K[s];\n"
-	  << FinalizeCode(gb, fields, visible_, "T", "s", "key", "pos", OUT) << "\t\t}\n"
-	  << "\t\tbase += chunk_total;\n\t}\n\t__syncthreads();\n}\n\n";
+	  << "\tconst long long dbg_t1 = clock64();\n"
+	  << "\tif (*overflow) { vgpu_table_init(tab, C); return; }\n"
+	  << "\t// compaction: 32-slot chunks round-robin over warps; pass 1 counts live slots per warp, one\n"
+	  << "\t// reservation for the partition, pass 2 writes each live slot and resets it for the next one\n"
+	  << "\t__shared__ u32 warp_live[32];\n\t__shared__ u64 out_base;\n"
+	  << "\tu32 mine = 0;\n"
+	  << "\tfor (u32 c0 = warp * 32u; c0 < C; c0 += nwarps * 32u) mine += __popc(__ballot_sync(0xffffffffu, K[c0 + lane] != ~0ull));\n"
+	  << "\tif (lane == 0) warp_live[warp] = mine;\n"
+	  << "\t__syncthreads();\n"
+	  << "\tu32 before = 0, total = 0;\n"
+	  << "\tfor (u32 w_ = 0; w_ < nwarps; ++w_) { const u32 x_ = warp_live[w_]; before += w_ < warp ? x_ : 0u; total += x_; }\n"
+	  << "\tif (threadIdx.x == 0) out_base = atomicAdd((unsigned long long*)a.w[" << W + 3
+	  << "], (unsigned long long)total);\n"
+	  << "\t__syncthreads();\n"
+	  << "\tu64 run = out_base + before;\n"
+	  << "\tfor (u32 c0 = warp * 32u; c0 < C; c0 += nwarps * 32u) {\n"
+	  << "\t\tconst u32 s = c0 + lane;\n"
+	  << "\t\tconst u64 key = K[s];\n"
+	  << "\t\tconst u32 live_mask = __ballot_sync(0xffffffffu, key != ~0ull);\n"
+	  << "\t\tif (key != ~0ull) {\n"
+	  << "\t\t\tconst u64 pos = run + __popc(live_mask & ((1u << lane) - 1u));\n"
+	  << FinalizeCode(gb, fields, visible_, "T", "s", "key", "pos", OUT)
+	  << "\t\t\tvgpu_table_reset(tab, C, s);\n\t\t}\n"
+	  << "\t\trun += __popc(live_mask);\n\t}\n\t__syncthreads();\n"
+	  << "\t// optional per-partition diagnostics (rows, groups, row-loop and compaction cycles, block)\n"
+	  << "\tif (threadIdx.x == 0 && a.w[" << kDebugWord << "]) {\n"
+	  << "\t\tu64 *d = (u64*)a.w[" << kDebugWord << "] + 8ull * p;\n"
+	  << "\t\td[0] = end - start; d[1] = total; d[2] = (u64)(dbg_t1 - dbg_t0); d[3] = (u64)(clock64() - dbg_t1);\n"
+	  << "\t\td[4] = blockIdx.x; d[5] = blockDim.x;\n\t}\n"
+	  << "}\n\n";
 
-	o << "extern \"C\" __global__ void __launch_bounds__(512) vgpu_gb_bucket(KArgs a) {\n"
+	const int L = OUT + out_words;
+	// Tier 1: every partition, small shared-memory table (C from the arguments, any block size).
+	// Partitions it cannot hold go to a device-side retry list instead of failing.
+	o << "extern \"C\" __global__ void __launch_bounds__(128, 4) vgpu_gb_bucket(KArgs a) {\n"
 	  << "\textern __shared__ __align__(16) u64 vgpu_tab[];\n"
 	  << "\t__shared__ u32 cur_p;\n\t__shared__ bool overflow;\n"
 	  << "\tconst u32 P = (u32)a.w[" << cb << "]; const u32 C = (u32)a.w[" << cb + 1 << "];\n"
+	  << "\tu32 next_p = 0;\n"
+	  << "\tif (threadIdx.x == 0) { cur_p = atomicAdd((u32*)a.w[" << W << "], 1u); overflow = false; }\n"
+	  << "\tvgpu_table_init(vgpu_tab, C);\n"
 	  << "\twhile (true) {\n"
-	  << "\t\tif (threadIdx.x == 0) { cur_p = atomicAdd((u32*)a.w[" << W << "], 1u); overflow = false; }\n"
-	  << "\t\t__syncthreads();\n"
 	  << "\t\tconst u32 p = cur_p;\n"
 	  << "\t\tif (p >= P) break;\n"
-	  << "\t\tvgpu_bucket_process(a, p, vgpu_tab, C, &overflow);\n"
+	  << "\t\t// the next partition's index is claimed now; its result is only needed after this one\n"
+	  << "\t\tif (threadIdx.x == 0) next_p = atomicAdd((u32*)a.w[" << W << "], 1u);\n"
+	  << "\t\tvgpu_bucket_process(a, p, vgpu_tab, C, C < 64u ? C : 64u, &overflow);\n"
+	  << "\t\tif (threadIdx.x == 0) {\n"
+	  << "\t\t\tif (overflow) { ((u32*)a.w[" << L + 5 << "])[atomicAdd((u32*)a.w[" << L + 6 << "], 1u)] = p; }\n"
+	  << "\t\t\toverflow = false;\n\t\t\tcur_p = next_p;\n\t\t}\n"
+	  << "\t\t__syncthreads();\n\t}\n}\n\n";
+
+	// Tier 2: the retry list with the largest shared-memory table (C2). Partitions that still do not
+	// fit are flagged for the host's global-memory pass.
+	o << "extern \"C\" __global__ void __launch_bounds__(512, 1) vgpu_gb_bucket_retry(KArgs a) {\n"
+	  << "\textern __shared__ __align__(16) u64 vgpu_tab[];\n"
+	  << "\t__shared__ u32 cur_i;\n\t__shared__ bool overflow;\n"
+	  << "\tconst u32 C = (u32)a.w[" << L + 8 << "];\n"
+	  << "\tconst u32 n_retry = *(volatile u32*)a.w[" << L + 6 << "];\n"
+	  << "\tif (n_retry == 0) return;\n"
+	  << "\tvgpu_table_init(vgpu_tab, C);\n"
+	  << "\twhile (true) {\n"
+	  << "\t\tif (threadIdx.x == 0) { cur_i = atomicAdd((u32*)a.w[" << L + 7 << "], 1u); overflow = false; }\n"
+	  << "\t\t__syncthreads();\n"
+	  << "\t\tconst u32 i = cur_i;\n"
+	  << "\t\tif (i >= n_retry) break;\n"
+	  << "\t\tconst u32 p = ((const u32*)a.w[" << L + 5 << "])[i];\n"
+	  << "\t\tvgpu_bucket_process(a, p, vgpu_tab, C, C < 64u ? C : 64u, &overflow);\n"
 	  << "\t\tif (threadIdx.x == 0 && overflow) { ((u32*)a.w[" << W + 1 << "])[p] = 1u; atomicAdd((u32*)a.w[" << W + 2
 	  << "], 1u); }\n"
 	  << "\t\t__syncthreads();\n\t}\n}\n\n";
 
-	const int L = OUT + out_words;
-	o << "extern \"C\" __global__ void __launch_bounds__(512) vgpu_gb_bucket_global(KArgs a) {\n"
+	o << "extern \"C\" __global__ void __launch_bounds__(512, 1) vgpu_gb_bucket_global(KArgs a) {\n"
 	  << "\t__shared__ bool overflow;\n"
 	  << "\tconst u32 *list = (const u32*)a.w[" << L << "];\n"
 	  << "\tconst u32 nlist = (u32)a.w[" << L + 1 << "];\n"
@@ -881,8 +1121,9 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 	  << "\tconst u64 *tab_off = (const u64*)a.w[" << L + 3 << "];\n"
 	  << "\tconst u32 *caps = (const u32*)a.w[" << L + 4 << "];\n"
 	  << "\tfor (u32 e = blockIdx.x; e < nlist; e += gridDim.x) {\n"
-	  << "\t\tif (threadIdx.x == 0) overflow = false;\n\t\t__syncthreads();\n"
-	  << "\t\tvgpu_bucket_process(a, list[e], tables + tab_off[e], caps[e], &overflow);\n"
+	  << "\t\tif (threadIdx.x == 0) overflow = false;\n"
+	  << "\t\tvgpu_table_init(tables + tab_off[e], caps[e]);\n"
+	  << "\t\tvgpu_bucket_process(a, list[e], tables + tab_off[e], caps[e], caps[e], &overflow);\n"
 	  << "\t\tif (threadIdx.x == 0 && overflow) atomicAdd((u32*)a.w[" << W + 2 << "], 1u);\n"
 	  << "\t\t__syncthreads();\n\t}\n}\n";
 	return o.str();

@@ -103,8 +103,10 @@ public:
 	//!  partitioned: vgpu_gb_part_count, vgpu_gb_part_scatter, vgpu_gb_bucket
 	std::string EmitGroupBy(const GroupBySpec &gb, bool partitioned, const Geometry &g) const;
 
-	//! Bytes of per-group aggregate state (excluding the key), as laid out by EmitGroupBy.
+	//! Number of 8-byte per-group aggregate state fields (excluding the key), as laid out by EmitGroupBy.
 	static int StateWords(const GroupBySpec &gb);
+	//! Byte stride of one partitioned-intermediate record (packed key + carried values, 32-byte multiple).
+	int RecordStride(const GroupBySpec &gb) const;
 
 private:
 	void Resolve();

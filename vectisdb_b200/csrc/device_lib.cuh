@@ -127,6 +127,27 @@ __device__ __forceinline__ void load_rows(const T *__restrict__ base, u64 row0, 
 	}
 }
 
+// Fixed-size row records (W 32-bit words, W a multiple of 4): whole 16-byte vector stores and
+// streaming vector loads.
+template <int W> __device__ __forceinline__ void store_record(void *dst, const u32 (&w)[W]) {
+#pragma unroll
+	for (int q = 0; q < W / 4; ++q) {
+		asm volatile("st.global.v4.u32 [%0], {%1,%2,%3,%4};" ::"l"(reinterpret_cast<char *>(dst) + 16 * q),
+		             "r"(w[4 * q]), "r"(w[4 * q + 1]), "r"(w[4 * q + 2]), "r"(w[4 * q + 3])
+		             : "memory");
+	}
+}
+template <int W> __device__ __forceinline__ void load_record(const void *src, u32 (&w)[W]) {
+#pragma unroll
+	for (int q = 0; q < W / 4; ++q) {
+		uint4 v = ld_stream_v4(reinterpret_cast<const char *>(src) + 16 * q);
+		w[4 * q] = v.x;
+		w[4 * q + 1] = v.y;
+		w[4 * q + 2] = v.z;
+		w[4 * q + 3] = v.w;
+	}
+}
+
 // Byte-per-row validity (the engine's internal null mask layout). nullptr = all valid.
 template <int R>
 __device__ __forceinline__ void load_valid(const u8 *__restrict__ base, u64 row0, u64 n, bool (&out)[R]) {

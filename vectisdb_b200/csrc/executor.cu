@@ -12,6 +12,8 @@
 #include "executor.hpp"
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <set>
 
@@ -620,21 +622,34 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		LaunchGenerated(*module, "vgpu_gb_direct_final", 1, 1024, 0, stream_, a, domain * F * 8, domain);
 		groups = ReadU64(count);
 	} else {
-		// Partitioned: table capacity from the shared-memory budget, partitions so each table runs at
-		// most half full on average.
+		// Partitioned. Tier-1 bucket tables are small (about 48 KB, 128 threads per CTA, several CTAs per
+		// SM): few warps share a table, so same-slot atomics of moderately heavy keys queue behind at most
+		// four warps. Partitions are sized so a tier-1 table would run half full at the key-range bound;
+		// the ones that do not fit are retried on the device with the largest shared-memory table.
+		const uint64_t slot_bytes = (1 + F) * 8;
 		const uint64_t smem_cap = std::min<uint64_t>(props.smem_optin > 4096 ? props.smem_optin - 4096 : 48 * 1024,
 		                                             200 * 1024);
-		const uint64_t C = std::max<uint64_t>(256, FloorPow2(smem_cap / ((1 + F) * 8)));
+		uint64_t C2 = std::max<uint64_t>(256, FloorPow2(smem_cap / slot_bytes));
+		if (const char *env = std::getenv("VGPU_GB_RETRY_SLOTS")) {  // tuning/testing override (power of two)
+			C2 = std::min<uint64_t>(C2, std::max<uint64_t>(64, FloorPow2(std::strtoull(env, nullptr, 10))));
+		}
+		uint64_t C = std::min<uint64_t>(C2, std::max<uint64_t>(256, FloorPow2((48 * 1024) / slot_bytes)));
+		if (const char *env = std::getenv("VGPU_GB_TABLE_SLOTS")) {  // tuning override (power of two)
+			C = std::min<uint64_t>(C2, std::max<uint64_t>(256, FloorPow2(std::strtoull(env, nullptr, 10))));
+		}
 		const uint64_t expected_groups = std::min<uint64_t>(domain, n);
 		uint64_t P = NextPow2(std::max<uint64_t>(1, (expected_groups + C / 2 - 1) / (C / 2)));
 		P = std::min<uint64_t>(P, 16384);
+		if (const char *env = std::getenv("VGPU_GB_PARTITIONS")) {  // tuning override (power of two)
+			P = std::min<uint64_t>(16384, std::max<uint64_t>(1, FloorPow2(std::strtoull(env, nullptr, 10))));
+		}
 		int pbits = BitsFor(P - 1);
 		if (P == 1) pbits = 0;
 		gb.partition_bits = pbits;
 		gb.table_capacity = static_cast<int>(C);
 		Geometry g;
-		g.block = 512;
-		g.items = 4;
+		g.block = 256;
+		g.items = 8;
 		std::string src = cg.EmitGroupBy(gb, true, g);
 		last_source = src;
 		auto module = Runtime::Get().modules().GetOrCompile(src);
@@ -648,14 +663,8 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		if (n >= (1ull << 32)) Fail(VGPU_ERR_UNSUPPORTED, "gpu_groupby: more than 2^32 input rows");
 		uint32_t *offsets = arena_.AllocT<uint32_t>(P * G);
 		uint32_t *total = arena_.AllocT<uint32_t>(1);
-		// value columns carried by the scatter (same order as EmitGroupBy's value_cols)
-		std::vector<int> value_cols;
-		for (auto &s : gb.aggs) {
-			if (s.column >= 0 && s.kind != AggKind::COUNT && s.kind != AggKind::COUNT_STAR &&
-			    std::find(value_cols.begin(), value_cols.end(), s.column) == value_cols.end()) {
-				value_cols.push_back(s.column);
-			}
-		}
+		// Records of the partitioned intermediate: packed key + carried values, RS bytes each.
+		const uint64_t RS = static_cast<uint64_t>(cg.RecordStride(gb));
 		KArgsHost a;
 		FillArgs(pin, a);
 		a.Set(cb, P);
@@ -664,18 +673,16 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		a.SetPtr(cb + 3, offsets);
 		LaunchGenerated(*module, "vgpu_gb_part_count", static_cast<unsigned>(G), g.block, part_smem, stream_, a, in_bytes, n);
 		kern::ExclusiveScanU32(offsets, offsets, P * G, total, arena_);
-		uint64_t *keys_part = arena_.AllocT<uint64_t>(n);
-		std::vector<void *> vals_part;
-		for (int c : value_cols) vals_part.push_back(arena_.Alloc(n * TypeSize(cg.visible()[c].type)));
-		a.SetPtr(cb + 4, keys_part);
-		for (size_t v = 0; v < vals_part.size(); v++) a.SetPtr(cb + 5 + static_cast<int>(v), vals_part[v]);
+		char *records = static_cast<char *>(arena_.Alloc(n * RS));
+		a.SetPtr(cb + 4, records);
 		LaunchGenerated(*module, "vgpu_gb_part_scatter", static_cast<unsigned>(G), g.block, part_smem, stream_, a, in_bytes, n);
-		// bucket tables
-		const int V = static_cast<int>(value_cols.size());
-		const int W = cb + 6 + V;
-		uint32_t *control = arena_.AllocT<uint32_t>(2 + P);
+		// bucket tables. control: [0] work counter, [1] overflow count, [2] retry count, [3] retry work
+		// counter, [4, 4+P) overflow flags, [4+P, 4+2P) retry list.
+		const int W = cb + 6;
+		const int L = W + 4 + out_words;
+		uint32_t *control = arena_.AllocT<uint32_t>(4 + 2 * P);
 		uint64_t *out_count = arena_.AllocT<uint64_t>(1);
-		VGPU_CUDA(cudaMemsetAsync(control, 0, (2 + P) * 4, stream_));
+		VGPU_CUDA(cudaMemsetAsync(control, 0, (4 + 2 * P) * 4, stream_));
 		VGPU_CUDA(cudaMemsetAsync(out_count, 0, 8, stream_));
 		KArgsHost b;
 		FillArgs(pin, b);
@@ -684,27 +691,60 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		b.SetPtr(cb + 2, offsets);
 		b.Set(cb + 3, G);
 		b.SetPtr(cb + 4, total);
-		b.SetPtr(cb + 5, keys_part);
-		for (int v = 0; v < V; v++) b.SetPtr(cb + 6 + v, vals_part[v]);
+		b.SetPtr(cb + 5, records);
 		b.SetPtr(W, control);           // work counter
-		b.SetPtr(W + 1, control + 2);   // overflow flags [P]
+		b.SetPtr(W + 1, control + 4);   // overflow flags [P]
 		b.SetPtr(W + 2, control + 1);   // overflow count
 		b.SetPtr(W + 3, out_count);
 		for (int w = 0; w < out_words; w++) b.SetPtr(W + 4 + w, out[w].data);
-		const size_t bucket_smem = static_cast<size_t>((1 + F) * 8 * C);
-		CUfunction fb = module->Get("vgpu_gb_bucket");
-		int bocc = std::max(1, Runtime::Get().MaxActiveBlocks(fb, 512, bucket_smem));
-		const unsigned bgrid = static_cast<unsigned>(std::min<uint64_t>(P, uint64_t(props.sm_count) * bocc));
-		uint64_t part_bytes = n * 8;
-		for (int c : value_cols) part_bytes += n * TypeSize(cg.visible()[c].type);
-		LaunchGenerated(*module, "vgpu_gb_bucket", bgrid, 512, bucket_smem, stream_, b, part_bytes, n);
+		b.SetPtr(L + 5, control + 4 + P);  // retry list
+		b.SetPtr(L + 6, control + 2);      // retry count
+		b.SetPtr(L + 7, control + 3);      // retry work counter
+		b.Set(L + 8, C2);
+		const uint64_t part_bytes = n * RS;
+		// VGPU_DEBUG_BUCKET=<file>: per-partition rows, groups and cycle counts of the bucket pass.
+		const char *debug_path = std::getenv("VGPU_DEBUG_BUCKET");
+		uint64_t *debug = nullptr;
+		if (debug_path) {
+			debug = arena_.AllocT<uint64_t>(P * 8);
+			VGPU_CUDA(cudaMemsetAsync(debug, 0, P * 64, stream_));
+			b.SetPtr(127, debug);
+		}
+		{
+			const size_t smem1 = static_cast<size_t>(slot_bytes * C);
+			CUfunction fb = module->Get("vgpu_gb_bucket");
+			const int occ1 = std::max(1, Runtime::Get().MaxActiveBlocks(fb, 128, smem1));
+			const unsigned grid1 = static_cast<unsigned>(std::min<uint64_t>(P, uint64_t(props.sm_count) * occ1));
+			LaunchGenerated(*module, "vgpu_gb_bucket", grid1, 128, smem1, stream_, b, part_bytes, n);
+		}
+		{
+			const size_t smem2 = static_cast<size_t>(slot_bytes * C2);
+			CUfunction fr = module->Get("vgpu_gb_bucket_retry");
+			const int occ2 = std::max(1, Runtime::Get().MaxActiveBlocks(fr, 512, smem2));
+			LaunchGenerated(*module, "vgpu_gb_bucket_retry", static_cast<unsigned>(props.sm_count * occ2), 512, smem2,
+			                stream_, b, 0, 0);
+		}
+		if (debug) {
+			std::vector<uint64_t> h(P * 8);
+			VGPU_CUDA(cudaMemcpyAsync(h.data(), debug, P * 64, cudaMemcpyDeviceToHost, stream_));
+			VGPU_CUDA(cudaStreamSynchronize(stream_));
+			if (FILE *f = std::fopen(debug_path, "w")) {
+				for (uint64_t p = 0; p < P; p++) {
+					std::fprintf(f, "%llu %llu %llu %llu %llu %llu %llu\n", (unsigned long long)p,
+					             (unsigned long long)h[p * 8], (unsigned long long)h[p * 8 + 1],
+					             (unsigned long long)h[p * 8 + 2], (unsigned long long)h[p * 8 + 3],
+					             (unsigned long long)h[p * 8 + 4], (unsigned long long)h[p * 8 + 5]);
+				}
+				std::fclose(f);
+			}
+		}
 		const uint32_t overflowed = ReadU32(control + 1);
 		if (overflowed > 0) {
 			// Partitions with more distinct keys than a shared-memory table holds: redo them with a
 			// global-memory table sized from the partition's row count.
 			std::vector<uint32_t> flags(P), offs(P * G);
 			uint32_t total_rows = ReadU32(total);
-			VGPU_CUDA(cudaMemcpyAsync(flags.data(), control + 2, P * 4, cudaMemcpyDeviceToHost, stream_));
+			VGPU_CUDA(cudaMemcpyAsync(flags.data(), control + 4, P * 4, cudaMemcpyDeviceToHost, stream_));
 			VGPU_CUDA(cudaMemcpyAsync(offs.data(), offsets, P * G * 4, cudaMemcpyDeviceToHost, stream_));
 			VGPU_CUDA(cudaStreamSynchronize(stream_));
 			std::vector<uint32_t> list, caps;
@@ -728,7 +768,6 @@ Relation Executor::GroupBy(const PlanNode &node) {
 			VGPU_CUDA(cudaMemcpyAsync(d_caps, caps.data(), caps.size() * 4, cudaMemcpyHostToDevice, stream_));
 			VGPU_CUDA(cudaMemcpyAsync(d_off, tab_off.data(), tab_off.size() * 8, cudaMemcpyHostToDevice, stream_));
 			VGPU_CUDA(cudaMemsetAsync(control + 1, 0, 4, stream_));
-			const int L = W + 4 + out_words;
 			b.SetPtr(L, d_list);
 			b.Set(L + 1, list.size());
 			b.SetPtr(L + 2, tables);

@@ -537,7 +537,7 @@ void Runtime::UnloadModule(CUmodule m) {
 }
 
 void Runtime::LaunchModuleKernel(CUfunction f, dim3 grid, dim3 block, size_t smem, cudaStream_t stream, void **args) {
-	if (smem > 48 * 1024) {
+	if (smem > 32 * 1024) {
 		DriverCheck(cuFuncSetAttribute_(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, static_cast<int>(smem)),
 		            "cuFuncSetAttribute(max dynamic smem)");
 	}
@@ -547,7 +547,7 @@ void Runtime::LaunchModuleKernel(CUfunction f, dim3 grid, dim3 block, size_t sme
 }
 
 int Runtime::MaxActiveBlocks(CUfunction f, int block, size_t smem) {
-	if (smem > 48 * 1024) {
+	if (smem > 32 * 1024) {
 		DriverCheck(cuFuncSetAttribute_(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, static_cast<int>(smem)),
 		            "cuFuncSetAttribute(max dynamic smem)");
 	}
