@@ -116,3 +116,71 @@ def test_c1_overflow_tiers_stay_exact(tier1, retry, monkeypatch):
     gs = gsum[order]
     assert np.array_equal(gs["lower"], exp["sum_lo"]) and np.array_equal(gs["upper"], exp["sum_hi"])
     assert _close(gavg[order], exp["avg"])
+
+
+@pytest.mark.parametrize("n,env", [
+    (1 << 14, {}),
+    (1 << 18, {}),
+    (3_000_001, {}),
+    (1 << 18, {"VGPU_GB_SPLIT_ROWS": "256"}),             # most partitions split into merged chunks
+    (1 << 18, {"VGPU_GB_DIRECT_BITS": "8"}),              # narrow tables, many partitions
+    (1 << 18, {"VGPU_GB_DIRECT_BITS": "8", "VGPU_GB_SPLIT_ROWS": "256", "VGPU_GB_BUCKET_THREADS": "128"}),
+])
+def test_c1_direct_partitioned_strategy(n, env, monkeypatch):
+    """The direct-partitioned strategy (bijective key mix, dense shared tables, split partitions merged
+    through global tables) gives the same groups and aggregates as the oracle."""
+    monkeypatch.setenv("VGPU_GB_STRATEGY", "direct")
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    wl = W.c1(n=n)
+    a, b, amt, v, ts = [c.data for c in wl.inputs]
+    cols = _run(wl)
+    ga, gb, gsum, gavg, gcnt, gmax = [c.data for c in cols]
+    order = np.lexsort((gb, ga))
+    exp = O.c1(a, b, amt, v, ts, wl.params["ts_gt"])
+    assert len(ga) == len(exp["a"])
+    assert np.array_equal(ga[order], exp["a"]) and np.array_equal(gb[order], exp["b"])
+    assert np.array_equal(gcnt[order], exp["count"]) and np.array_equal(gmax[order], exp["max"])
+    gs = gsum[order]
+    assert np.array_equal(gs["lower"], exp["sum_lo"]) and np.array_equal(gs["upper"], exp["sum_hi"])
+    assert _close(gavg[order], exp["avg"])
+
+
+@pytest.mark.parametrize("split", [None, "256"])
+def test_direct_partitioned_signed_sums_and_min(split, monkeypatch):
+    """Negative and beyond-64-bit integer sums through the 32-bit-word accumulators, plus MIN/MAX and
+    FP64 sums, on a key space wide enough to need several partitions."""
+    from vectisdb_b200.engine import GpuAggregateKind as A, GpuValueType as T
+    from vectisdb_b200 import make_aggregate, make_column, make_group_by, make_scan
+    monkeypatch.setenv("VGPU_GB_STRATEGY", "direct")
+    monkeypatch.setenv("VGPU_GB_DIRECT_BITS", "6")
+    if split:
+        monkeypatch.setenv("VGPU_GB_SPLIT_ROWS", split)
+    rng = np.random.default_rng(7)
+    n = 200_000
+    k = rng.integers(-3000, 3000, n).astype(np.int32)
+    k[: n // 4] = 17  # one heavy key
+    big = rng.integers(-(1 << 62), 1 << 62, n, dtype=np.int64)
+    x = rng.standard_normal(n)
+    plan = make_group_by(["k"], [make_aggregate(A.SUM, "v", T.HUGEINT), make_aggregate(A.MIN, "v", T.INT64),
+                                 make_aggregate(A.MAX, "v", T.INT64), make_aggregate(A.SUM, "x", T.FLOAT64),
+                                 make_aggregate(A.COUNT_STAR, "", T.INT64)],
+                         make_scan(["k", "v", "x"]))
+    r = GpuEngine.instance().execute_plan(plan, [make_column("k", T.INT32, k), make_column("v", T.INT64, big),
+                                                 make_column("x", T.FLOAT64, x)])
+    assert r.success, r.error_message
+    keys = r.columns[0].data
+    sums = hugeint_to_int(r.columns[1].data)
+    order = np.argsort(k, kind="stable")
+    uk, starts = np.unique(k[order], return_index=True)
+    assert np.array_equal(np.sort(keys), uk)
+    pos = {int(key): i for i, key in enumerate(keys.tolist())}
+    bounds = list(starts) + [n]
+    for j, key in enumerate(uk.tolist()):
+        rows = order[bounds[j]:bounds[j + 1]]
+        i = pos[key]
+        assert sums[i] == int(big[rows].astype(object).sum())
+        assert r.columns[2].data[i] == big[rows].min() and r.columns[3].data[i] == big[rows].max()
+        assert r.columns[5].data[i] == len(rows)
+        exp = float(np.sum(x[rows]))
+        assert abs(r.columns[4].data[i] - exp) <= 1e-9 * max(1.0, float(np.sum(np.abs(x[rows]))))

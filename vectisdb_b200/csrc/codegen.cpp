@@ -659,6 +659,16 @@ int PipelineCodegen::StateWords(const GroupBySpec &gb) {
 	return static_cast<int>(StateFields(gb).size());
 }
 
+int PipelineCodegen::DirectSlotBytes(const GroupBySpec &gb) {
+	int bytes = 0;
+	for (auto &f : StateFields(gb)) {
+		if (f.kind == "cnt") bytes += 4;
+		if (f.kind == "f64" || f.kind == "min" || f.kind == "max") bytes += 8;
+		if (f.kind == "lo") bytes += 16;
+	}
+	return bytes;
+}
+
 int PipelineCodegen::RecordStride(const GroupBySpec &gb) const {
 	// Same layout rule as EmitGroupBy: key u64, then each distinct carried value column at its
 	// natural alignment, rounded up to 32 bytes.
@@ -816,6 +826,20 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		}
 		return "0";
 	};
+	// Partition of a row: top bits of the mixed key (hashed strategy), or of the bijectively mixed key
+	// whose low direct_bits are the table slot (direct-partitioned strategy; the record then carries the
+	// mixed key).
+	const bool dpart = gb.direct_bits > 0;
+	const std::string part_of_pack = dpart ? "(u32)(vgpu_dmix(" + pack.str() + ") >> " + std::to_string(gb.direct_bits) + ")"
+	                                       : "partition_of(" + pack.str() + ", pbits)";
+	const std::string key_of_pack = dpart ? "vgpu_dmix(" + pack.str() + ")" : pack.str();
+	if (dpart) {
+		const uint64_t mask = gb.key_bits >= 64 ? ~0ull : ((1ull << gb.key_bits) - 1);
+		o << "__device__ __forceinline__ u64 vgpu_dmix(u64 k) { return (k * 0x" << std::hex << gb.key_mult << "ull) & 0x"
+		  << mask << "ull; }\n"
+		  << "__device__ __forceinline__ u64 vgpu_dunmix(u64 k) { return (k * 0x" << gb.key_mult_inv << "ull) & 0x" << mask
+		  << std::dec << "ull; }\n\n";
+	}
 	// part_count / part_scatter args: cb+0 = P, cb+1 = pbits, cb+2 = tiles per CTA,
 	//   cb+3 = counts/offsets (u32, [p * G + cta]), cb+4 = records out.
 	o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_gb_part_count(KArgs a) {\n"
@@ -827,7 +851,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 	  << "\tconst u64 t_end = (blockIdx.x + 1) * tpc < ntiles ? (blockIdx.x + 1) * tpc : ntiles;\n"
 	  << "\tfor (u64 tile = blockIdx.x * tpc; tile < t_end; ++tile) {\n"
 	  << LoadBlock(g, needed, true) << item_head << chain_code_ << "\t\tif (keep) {\n"
-	  << "\t\t\tatomicAdd(&vgpu_hist[partition_of(" << pack.str() << ", pbits)], 1u);\n"
+	  << "\t\t\tatomicAdd(&vgpu_hist[" << part_of_pack << "], 1u);\n"
 	  << "\t\t}\n\t\t}\n\t}\n\t__syncthreads();\n"
 	  << "\tu32 *counts = (u32*)a.w[" << cb + 3 << "];\n"
 	  << "\tfor (u32 p = threadIdx.x; p < P; p += " << g.block
@@ -844,9 +868,16 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 	  << tile_loop_head
 	  << "\tconst u64 t_end = (blockIdx.x + 1) * tpc < ntiles ? (blockIdx.x + 1) * tpc : ntiles;\n"
 	  << "\tfor (u64 tile = blockIdx.x * tpc; tile < t_end; ++tile) {\n"
-	  << LoadBlock(g, needed, true) << item_head << chain_code_ << "\t\tif (keep) {\n"
-	  << "\t\t\tconst u64 key = " << pack.str() << ";\n"
-	  << "\t\t\tconst u32 pos = atomicAdd(&vgpu_cursor[partition_of(key, pbits)], 1u);\n"
+	  << LoadBlock(g, needed, true)
+	  // every item's cursor reservation first, branch-free (rows that are filtered out add to a per-lane
+	  // dummy counter past P), so the tile's shared atomics are in flight together; then the records
+	  << "\t\tu32 vgpu_pos[" << g.items << "];\n"
+	  << item_head << chain_code_
+	  << "\t\tvgpu_pos[r] = atomicAdd(&vgpu_cursor[keep ? " << part_of_pack << " : P + (threadIdx.x & 31u)], 1u);\n"
+	  << "\t\t}\n"
+	  << item_head << chain_code_ << "\t\tif (keep) {\n"
+	  << "\t\t\tconst u64 key = " << key_of_pack << ";\n"
+	  << "\t\t\tconst u32 pos = vgpu_pos[r];\n"
 	  << "\t\t\tu32 rw[" << RW << "];\n"
 	  << "\t\t\t#pragma unroll\n\t\t\tfor (int q = 0; q < " << RW << "; ++q) rw[q] = 0u;\n"
 	  << "\t\t\trw[0] = (u32)key; rw[1] = (u32)(key >> 32);\n";
@@ -878,7 +909,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 	// atomics on the low half of the count word (a partition holds fewer than 2^32 rows).
 	const int W = cb + 6;
 	const int OUT = W + 4;
-	std::ostringstream gdecl, gcomb, gupd, gxor, wdecl, wacc, wflush;
+	std::ostringstream gdecl, gcomb, gupd, gxor, wdecl, wacc, wflush, wvars;
 	gdecl << "\t\t\tu32 gc = valid ? 1u : 0u;\n";
 	gxor << "\t\t\t\t\tgc += __shfl_xor_sync(0xffffffffu, gc, d);\n";
 	wdecl << "\tu64 my_pk = ~0ull; u64 wc = 0; u32 free_mask = 0xffu;\n"
@@ -897,6 +928,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			gupd << "\t\t\t\t\tatomicAdd((double*)(T" << f << " + s_), gf" << f << ");\n";
 			gxor << "\t\t\t\t\tgf" << f << " += __shfl_xor_sync(0xffffffffu, gf" << f << ", d);\n";
 			wdecl << "\tdouble wf" << f << " = 0.0;\n";
+			wvars << "\tdouble wf" << f << " = 0.0;\n";
 			wacc << "\t\t\t\t{ const double t_ = __shfl_sync(0xffffffffu, gf" << f << ", src_); if (have_) wf" << f << " += t_; }\n";
 			wflush << "\t\t\tatomicAdd((double*)(T" << f << " + s_), wf" << f << ");\n";
 		} else if (fd.kind == "lo") {
@@ -912,6 +944,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			     << ", d); const i64 oh_ = __shfl_xor_sync(0xffffffffu, ghi" << f << ", d); const u64 nl_ = glo" << f
 			     << " + ol_; ghi" << f << " += oh_ + (nl_ < glo" << f << " ? 1 : 0); glo" << f << " = nl_; }\n";
 			wdecl << "\tu64 wlo" << f << " = 0; i64 whi" << f << " = 0;\n";
+			wvars << "\tu64 wlo" << f << " = 0; i64 whi" << f << " = 0;\n";
 			wacc << "\t\t\t\t{ const u64 ol_ = __shfl_sync(0xffffffffu, glo" << f
 			     << ", src_); const i64 oh_ = __shfl_sync(0xffffffffu, ghi" << f << ", src_);\n"
 			     << "\t\t\t\t  if (have_) { const u64 nl_ = wlo" << f << " + ol_; whi" << f << " += oh_ + (nl_ < wlo" << f
@@ -928,10 +961,264 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			gxor << "\t\t\t\t\t{ const i64 o_ = __shfl_xor_sync(0xffffffffu, gm" << f << ", d); if (o_ " << op << " gm" << f
 			     << ") gm" << f << " = o_; }\n";
 			wdecl << "\ti64 wm" << f << " = " << ident << ";\n";
+			wvars << "\ti64 wm" << f << " = " << ident << ";\n";
 			wacc << "\t\t\t\t{ const i64 t_ = __shfl_sync(0xffffffffu, gm" << f << ", src_); if (have_ && t_ " << op << " wm" << f
 			     << ") wm" << f << " = t_; }\n";
 			wflush << "\t\t\tatomic_" << fd.kind << "_i64((i64*)(T" << f << " + s_), wm" << f << ");\n";
 		}
+	}
+	if (dpart) {
+		// ---- direct-partitioned buckets ----
+		// args: cb+0 = work items (uint4: partition, first row, end row, split index or ~0),
+		//   cb+1 = item count (u32*), cb+2 = records, cb+3 = global tables of split partitions (u64,
+		//   [split][field][D]), cb+4 = split info (u32 [2s] chunks, [2s+1] completed chunks),
+		//   cb+5 = work counter (u32*), cb+6 = output count (u64*), cb+7 = split partitions (init
+		//   kernel), cb+8.. outputs.
+		// Shared table of D slots, one array per state word: 8-byte arrays (FP64 sums, MIN/MAX) first,
+		// then 32-bit arrays (COUNT, and four words per integer SUM accumulated with 32-bit atomics).
+		const int dbits = gb.direct_bits;
+		const uint64_t D = 1ull << dbits;
+		struct DArr {
+			std::string name, type;
+			int bytes;
+		};
+		std::vector<DArr> arrs;
+		for (int f = 0; f < F; f++) {
+			const auto &fd = fields[f];
+			if (fd.kind == "f64") arrs.push_back({"DF" + std::to_string(f), "double", 8});
+			if (fd.kind == "min" || fd.kind == "max") arrs.push_back({"DM" + std::to_string(f), "i64", 8});
+		}
+		for (int f = 0; f < F; f++) {
+			const auto &fd = fields[f];
+			if (fd.kind == "cnt") arrs.push_back({"DC", "u32", 4});
+			if (fd.kind == "lo") {
+				for (int w = 0; w < 4; w++) arrs.push_back({"DW" + std::to_string(f) + "_" + std::to_string(w), "u32", 4});
+			}
+		}
+		std::ostringstream decl;  // array pointers into the shared table `sm`
+		uint64_t off = 0;
+		for (auto &ar : arrs) {
+			decl << "\t" << ar.type << " *" << ar.name << " = (" << ar.type << "*)(sm + " << off << ");\n";
+			off += D * ar.bytes;
+		}
+		auto reset_slot = [&](const std::string &sv) {
+			std::ostringstream r;
+			for (int f = 0; f < F; f++) {
+				const auto &fd = fields[f];
+				if (fd.kind == "cnt") r << "\t\t\tDC[" << sv << "] = 0u;\n";
+				if (fd.kind == "f64") r << "\t\t\tDF" << f << "[" << sv << "] = 0.0;\n";
+				if (fd.kind == "min" || fd.kind == "max") {
+					r << "\t\t\tDM" << f << "[" << sv << "] = (i64)" << InitValue(fd) << ";\n";
+				}
+				if (fd.kind == "lo") {
+					for (int w = 0; w < 4; w++) r << "\t\t\tDW" << f << "_" << w << "[" << sv << "] = 0u;\n";
+				}
+			}
+			return r.str();
+		};
+		// slot state in the u64 field format of the other strategies (S<f>[0])
+		auto load_slot = [&](const std::string &sv) {
+			std::ostringstream r;
+			for (int f = 0; f < F; f++) {
+				const auto &fd = fields[f];
+				if (fd.kind == "cnt") r << "\t\t\tS" << f << "[0] = (u64)DC[" << sv << "];\n";
+				if (fd.kind == "f64") r << "\t\t\tS" << f << "[0] = (u64)__double_as_longlong(DF" << f << "[" << sv << "]);\n";
+				if (fd.kind == "min" || fd.kind == "max") r << "\t\t\tS" << f << "[0] = (u64)DM" << f << "[" << sv << "];\n";
+				if (fd.kind == "lo") {
+					r << "\t\t\tS" << f << "[0] = (u64)DW" << f << "_0[" << sv << "] | ((u64)DW" << f << "_1[" << sv
+					  << "] << 32);\n"
+					  << "\t\t\tS" << f + 1 << "[0] = (u64)DW" << f << "_2[" << sv << "] | ((u64)DW" << f << "_3[" << sv
+					  << "] << 32);\n";
+				}
+			}
+			return r.str();
+		};
+		// update of slot `sv` with the register partials of prefix `g` (group) or `w` (hot run)
+		auto update = [&](const std::string &pre, const std::string &sv) {
+			std::ostringstream r;
+			for (int f = 0; f < F; f++) {
+				const auto &fd = fields[f];
+				const std::string fs = std::to_string(f);
+				if (fd.kind == "cnt") r << "\t\t\t\tatomicAdd(&DC[" << sv << "], (u32)" << pre << "c);\n";
+				if (fd.kind == "f64") r << "\t\t\t\tatomicAdd(&DF" << fs << "[" << sv << "], " << pre << "f" << fs << ");\n";
+				if (fd.kind == "min" || fd.kind == "max") {
+					r << "\t\t\t\tatomic_" << fd.kind << "_i64(&DM" << fs << "[" << sv << "], " << pre << "m" << fs << ");\n";
+				}
+				if (fd.kind == "lo") {
+					r << "\t\t\t\tatomic_add_i128_u32x4(&DW" << fs << "_0[" << sv << "], &DW" << fs << "_1[" << sv << "], &DW" << fs
+					  << "_2[" << sv << "], &DW" << fs << "_3[" << sv << "], " << pre << "lo" << fs << ", " << pre << "hi" << fs
+					  << ");\n";
+				}
+			}
+			return r.str();
+		};
+		std::ostringstream sdecl;
+		for (int f = 0; f < F; f++) sdecl << (f ? ", " : "\t\t\tu64 ") << "S" << f << "[1]";
+		sdecl << ";\n";
+		std::ostringstream gptr;  // global table arrays of split index `sidx`
+		for (int f = 0; f < F; f++) {
+			gptr << "\tu64 *G" << f << " = (u64*)a.w[" << cb + 3 << "] + ((u64)sidx * " << F << " + " << f << ") * " << D
+			     << "ull;\n";
+		}
+		const int OUTD = cb + 8;
+		// compaction of live groups into the outputs: `live` and `load` are per-slot code, `key`
+		// the packed key of slot s; two passes with one output reservation per item
+		auto compaction = [&](const std::string &live, const std::string &load, const std::string &reset) {
+			std::ostringstream r;
+			r << "\t{\n\tu32 mine = 0;\n"
+			  << "\tfor (u32 c0 = warp * 32u; c0 < " << D << "u; c0 += nwarps * 32u) { const u32 s = c0 + lane; mine += __popc(__ballot_sync(0xffffffffu, "
+			  << live << ")); }\n"
+			  << "\tif (lane == 0) warp_live[warp] = mine;\n\t__syncthreads();\n"
+			  << "\tu32 before = 0, total = 0;\n"
+			  << "\tfor (u32 w_ = 0; w_ < nwarps; ++w_) { const u32 x_ = warp_live[w_]; before += w_ < warp ? x_ : 0u; total += x_; }\n"
+			  << "\tif (threadIdx.x == 0) out_base = atomicAdd((unsigned long long*)a.w[" << cb + 6
+			  << "], (unsigned long long)total);\n\t__syncthreads();\n"
+			  << "\tu64 run = out_base + before;\n"
+			  << "\tfor (u32 c0 = warp * 32u; c0 < " << D << "u; c0 += nwarps * 32u) {\n"
+			  << "\t\tconst u32 s = c0 + lane;\n"
+			  << "\t\tconst bool lv = " << live << ";\n"
+			  << "\t\tconst u32 live_mask = __ballot_sync(0xffffffffu, lv);\n"
+			  << "\t\tif (lv) {\n" << sdecl.str() << load
+			  << "\t\t\tconst u64 pos = run + __popc(live_mask & ((1u << lane) - 1u));\n"
+			  << "\t\t\tconst u64 key = vgpu_dunmix(((u64)p << " << dbits << ") | s);\n"
+			  << FinalizeCode(gb, fields, visible_, "S", "0", "key", "pos", OUTD) << reset << "\t\t}\n"
+			  << "\t\trun += __popc(live_mask);\n\t}\n\t__syncthreads();\n\t}\n";
+			return r.str();
+		};
+		std::ostringstream gload;
+		for (int f = 0; f < F; f++) gload << "\t\t\tS" << f << "[0] = __ldcg(G" << f << " + s);\n";
+		// Groups spanning 4+ lanes are combined one at a time by a full-warp xor butterfly in which the
+		// group's lanes contribute their values and the others the identity: every lane ends with the
+		// group total and the group's lowest lane keeps it. A step whose 32 rows share one key takes
+		// exactly one butterfly; a step of distinct keys takes none.
+		std::ostringstream tinit, txor, ttake;
+		tinit << "\t\t\t\t\tu32 tc = mem ? gc : 0u;\n";
+		txor << "\t\t\t\t\t\ttc += __shfl_xor_sync(0xffffffffu, tc, d);\n";
+		ttake << "\t\t\t\t\t\tgc = tc;\n";
+		for (int f = 1; f < F; f++) {
+			const auto &fd = fields[f];
+			const std::string fs = std::to_string(f);
+			if (fd.kind == "f64") {
+				tinit << "\t\t\t\t\tdouble tf" << fs << " = mem ? gf" << fs << " : 0.0;\n";
+				txor << "\t\t\t\t\t\ttf" << fs << " += __shfl_xor_sync(0xffffffffu, tf" << fs << ", d);\n";
+				ttake << "\t\t\t\t\t\tgf" << fs << " = tf" << fs << ";\n";
+			} else if (fd.kind == "lo") {
+				tinit << "\t\t\t\t\tu64 tlo" << fs << " = mem ? glo" << fs << " : 0ull; i64 thi" << fs << " = mem ? ghi" << fs
+				      << " : 0;\n";
+				txor << "\t\t\t\t\t\t{ const u64 ol_ = __shfl_xor_sync(0xffffffffu, tlo" << fs
+				     << ", d); const i64 oh_ = __shfl_xor_sync(0xffffffffu, thi" << fs << ", d); const u64 nl_ = tlo" << fs
+				     << " + ol_; thi" << fs << " += oh_ + (nl_ < tlo" << fs << " ? 1 : 0); tlo" << fs << " = nl_; }\n";
+				ttake << "\t\t\t\t\t\tglo" << fs << " = tlo" << fs << "; ghi" << fs << " = thi" << fs << ";\n";
+			} else if (fd.kind == "min" || fd.kind == "max") {
+				const char *op = fd.kind == "min" ? "<" : ">";
+				const char *ident = fd.kind == "min" ? "0x7fffffffffffffffLL" : "(-0x7fffffffffffffffLL - 1)";
+				tinit << "\t\t\t\t\ti64 tm" << fs << " = mem ? gm" << fs << " : " << ident << ";\n";
+				txor << "\t\t\t\t\t\t{ const i64 o_ = __shfl_xor_sync(0xffffffffu, tm" << fs << ", d); if (o_ " << op
+				     << " tm" << fs << ") tm" << fs << " = o_; }\n";
+				ttake << "\t\t\t\t\t\tgm" << fs << " = tm" << fs << ";\n";
+			}
+		}
+
+		o << "__device__ __forceinline__ void vgpu_dslot_reset(char *sm, u32 s) {\n" << decl.str() << reset_slot("s")
+		  << "}\n\n";
+		o << "__device__ __forceinline__ void vgpu_ditem(const KArgs &a, const uint4 it, char *sm) {\n"
+		  << "\t__shared__ u32 warp_live[32];\n\t__shared__ u64 out_base;\n\t__shared__ bool last_chunk;\n"
+		  << "\tconst u32 p = it.x, sidx = it.w;\n"
+		  << "\tconst u64 start = it.y, end = it.z;\n"
+		  << "\tconst char *recs = (const char*)a.w[" << cb + 2 << "];\n"
+		  << "\tconst u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;\n"
+		  << decl.str()
+		  // hot run: the first key of a step whose group spans 8+ lanes; later groups of it add into lane
+		  // 0's registers instead of the table (FP64 shared adds are CAS loops that serialize on one word)
+		  << "\tu32 hot = ~0u; u64 wc = 0;\n" << wvars.str()
+		  << "\tfor (u64 base = start + (u64)warp * 128ull; base < end; base += (u64)nwarps * 128ull) {\n"
+		  << "\t\tu32 rw[4][" << RW << "];\n"
+		  << "\t\t#pragma unroll\n\t\tfor (int q = 0; q < 4; ++q) {\n"
+		  << "\t\t\tconst u64 i = base + 32ull * q + lane;\n"
+		  << "\t\t\tload_record<" << RW << ">(recs + (i < end ? i : end - 1) * " << RS << ", rw[q]);\n\t\t}\n"
+		  << "\t\t#pragma unroll\n\t\tfor (int q = 0; q < 4; ++q) {\n"
+		  << "\t\t\tconst bool valid = base + 32ull * q + lane < end;\n"
+		  << "\t\t\tconst u32 slot = valid ? (rw[q][0] & " << D - 1 << "u) : 0xffffffffu;\n";
+		for (size_t i = 0; i < gb.aggs.size(); i++) {
+			const auto &ag = gb.aggs[i];
+			if (ag.column >= 0 && ag.kind != AggKind::COUNT && ag.kind != AggKind::COUNT_STAR) {
+				o << "\t\t\tconst " << CudaTypeName(visible_[ag.column].type) << " v" << i << " = "
+				  << rec_value(ag.column, "rw[q]") << ";\n";
+			}
+		}
+		o << gdecl.str()
+		  << "\t\t\tconst u32 peers = __match_any_sync(0xffffffffu, slot);\n"
+		  << "\t\t\tbool leader = true;\n"
+		  << "\t\t\tfor (u32 todo = __ballot_sync(0xffffffffu, __popc(peers) >= 4); todo;) {\n"
+		  << "\t\t\t\tconst u32 src_ = __ffs(todo) - 1;\n"
+		  << "\t\t\t\tconst u32 gmask = __shfl_sync(0xffffffffu, peers, src_);\n"
+		  << "\t\t\t\tconst bool mem = (gmask >> lane) & 1u;\n"
+		  << "\t\t\t\t{\n" << tinit.str()
+		  << "\t\t\t\t\t#pragma unroll\n\t\t\t\t\tfor (int d = 16; d > 0; d >>= 1) {\n" << txor.str()
+		  << "\t\t\t\t\t}\n"
+		  << "\t\t\t\t\tif (mem) {\n" << ttake.str() << "\t\t\t\t\t\tleader = lane == src_;\n\t\t\t\t\t}\n"
+		  << "\t\t\t\t}\n"
+		  << "\t\t\t\ttodo &= ~gmask;\n"
+		  << "\t\t\t}\n"
+		  << "\t\t\tconst u32 hm = __ballot_sync(0xffffffffu, valid && leader && slot == hot);\n"
+		  << "\t\t\tfor (u32 m_ = hm; m_; m_ &= m_ - 1) {\n"
+		  << "\t\t\t\tconst u32 src_ = __ffs(m_) - 1; const bool have_ = lane == 0;\n" << wacc.str() << "\t\t\t}\n"
+		  << "\t\t\tif (hm & (1u << lane)) leader = false;\n"
+		  << "\t\t\tif (hot == ~0u) {\n"
+		  << "\t\t\t\tconst u32 cand = __ballot_sync(0xffffffffu, valid && leader && __popc(peers) >= 8);\n"
+		  << "\t\t\t\tif (cand) {\n"
+		  << "\t\t\t\t\tconst u32 src_ = __ffs(cand) - 1; const bool have_ = lane == 0;\n"
+		  << "\t\t\t\t\thot = __shfl_sync(0xffffffffu, slot, src_);\n" << wacc.str()
+		  << "\t\t\t\t\tif (lane == src_) leader = false;\n"
+		  << "\t\t\t\t}\n\t\t\t}\n"
+		  << "\t\t\tif (valid && leader) {\n" << update("g", "slot") << "\t\t\t}\n"
+		  << "\t\t}\n\t}\n"
+		  << "\tif (hot != ~0u && lane == 0) {\n" << update("w", "hot") << "\t}\n"
+		  << "\t__syncthreads();\n"
+		  << "\tif (sidx == ~0u) {\n"
+		  << compaction("DC[s] != 0u", load_slot("s"), reset_slot("s"))
+		  << "\t\treturn;\n\t}\n"
+		  << "\t// a chunk of a split partition: fold the table into the partition's global table; the last\n"
+		  << "\t// chunk to finish writes the partition's groups\n"
+		  << gptr.str()
+		  << "\tfor (u32 s = threadIdx.x; s < " << D << "u; s += blockDim.x) {\n"
+		  << "\t\tif (DC[s] != 0u) {\n" << sdecl.str() << load_slot("s") << MergeCode(fields, "S", "0", "G", "s")
+		  << reset_slot("s") << "\t\t}\n\t}\n"
+		  << "\t__threadfence();\n\t__syncthreads();\n"
+		  << "\tif (threadIdx.x == 0) {\n"
+		  << "\t\tu32 *info = (u32*)a.w[" << cb + 4 << "] + 2ull * sidx;\n"
+		  << "\t\tlast_chunk = atomicAdd(info + 1, 1u) + 1u == info[0];\n\t}\n"
+		  << "\t__syncthreads();\n"
+		  << "\tif (!last_chunk) return;\n"
+		  << "\t__threadfence();\n"
+		  << compaction("__ldcg(G0 + s) != 0ull", gload.str(), "")
+		  << "}\n\n";
+		// global tables of split partitions: identity values
+		o << "extern \"C\" __global__ void vgpu_gb_dtab_init(KArgs a) {\n"
+		  << "\tu64 *g = (u64*)a.w[" << cb + 3 << "];\n"
+		  << "\tconst u64 total = a.w[" << cb + 7 << "] * " << F * D << "ull;\n"
+		  << "\tfor (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < total; i += (u64)gridDim.x * blockDim.x) {\n"
+		  << "\t\tconst u32 f = (u32)((i / " << D << "ull) % " << F << "u);\n"
+		  << "\t\tu64 v = 0ull;\n";
+		for (int f = 0; f < F; f++) {
+			o << "\t\tif (f == " << f << "u) v = " << InitValue(fields[f]) << ";\n";
+		}
+		o << "\t\tg[i] = v;\n\t}\n}\n\n";
+		o << "extern \"C\" __global__ void __launch_bounds__(" << gb.bucket_threads << ") vgpu_gb_dbucket(KArgs a) {\n"
+		  << "\textern __shared__ __align__(16) char vgpu_dsm[];\n"
+		  << "\t__shared__ u32 cur;\n"
+		  << "\tfor (u32 s = threadIdx.x; s < " << D << "u; s += blockDim.x) vgpu_dslot_reset(vgpu_dsm, s);\n"
+		  << "\tconst u32 n_items = *(const u32*)a.w[" << cb + 1 << "];\n"
+		  << "\tconst uint4 *items = (const uint4*)a.w[" << cb << "];\n"
+		  << "\twhile (true) {\n"
+		  << "\t\tif (threadIdx.x == 0) cur = atomicAdd((u32*)a.w[" << cb + 5 << "], 1u);\n"
+		  << "\t\t__syncthreads();\n"
+		  << "\t\tconst u32 i = cur;\n"
+		  << "\t\t__syncthreads();\n"
+		  << "\t\tif (i >= n_items) break;\n"
+		  << "\t\tvgpu_ditem(a, items[i], vgpu_dsm);\n"
+		  << "\t}\n}\n";
+		return o.str();
 	}
 	o << "__device__ __forceinline__ int vgpu_find_slot(u64 *K, u32 C, u64 key, u32 limit) {\n"
 	  << "\tu32 slot = (u32)mix64(key) & (C - 1);\n"
@@ -1075,7 +1362,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 	const int L = OUT + out_words;
 	// Tier 1: every partition, small shared-memory table (C from the arguments, any block size).
 	// Partitions it cannot hold go to a device-side retry list instead of failing.
-	o << "extern \"C\" __global__ void __launch_bounds__(128, 4) vgpu_gb_bucket(KArgs a) {\n"
+	o << "extern \"C\" __global__ void __launch_bounds__(" << gb.bucket_threads << ") vgpu_gb_bucket(KArgs a) {\n"
 	  << "\textern __shared__ __align__(16) u64 vgpu_tab[];\n"
 	  << "\t__shared__ u32 cur_p;\n\t__shared__ bool overflow;\n"
 	  << "\tconst u32 P = (u32)a.w[" << cb << "]; const u32 C = (u32)a.w[" << cb + 1 << "];\n"

@@ -96,15 +96,25 @@ public:
 		uint64_t domain = 1; // number of packed key values (direct strategy)
 		int partition_bits = 0;
 		int table_capacity = 4096; // bucket hash-table slots (partitioned strategy)
+		int bucket_threads = 128;  // tier-1 bucket CTA size (partitioned strategy)
+		// Direct-partitioned strategy (direct_bits > 0): the packed key (key_bits wide) is mixed by an
+		// odd multiplier mod 2^key_bits (a bijection); the top bits pick the partition and the low
+		// direct_bits index a dense shared-memory table, so no hashing or probing is needed.
+		int direct_bits = 0;
+		int key_bits = 0;
+		uint64_t key_mult = 1, key_mult_inv = 1;
 	};
 
 	//! Group-by kernels (see executor for the argument layout), all in one translation unit:
 	//!  direct: vgpu_gb_direct_init, vgpu_gb_direct, vgpu_gb_direct_final
-	//!  partitioned: vgpu_gb_part_count, vgpu_gb_part_scatter, vgpu_gb_bucket
+	//!  partitioned: vgpu_gb_part_count, vgpu_gb_part_scatter, vgpu_gb_bucket (+ _retry, _global)
+	//!  direct-partitioned: vgpu_gb_part_count, vgpu_gb_part_scatter, vgpu_gb_dtab_init, vgpu_gb_dbucket
 	std::string EmitGroupBy(const GroupBySpec &gb, bool partitioned, const Geometry &g) const;
 
 	//! Number of 8-byte per-group aggregate state fields (excluding the key), as laid out by EmitGroupBy.
 	static int StateWords(const GroupBySpec &gb);
+	//! Shared-memory bytes per slot of a direct-partitioned table (32-bit count and sum words).
+	static int DirectSlotBytes(const GroupBySpec &gb);
 	//! Byte stride of one partitioned-intermediate record (packed key + carried values, 32-byte multiple).
 	int RecordStride(const GroupBySpec &gb) const;
 

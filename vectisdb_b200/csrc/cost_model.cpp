@@ -195,9 +195,18 @@ std::string GenerateSourceText(const PlanNode &plan, const std::vector<vgpu_colu
 	std::vector<int> key_columns;
 	for (auto &k : spec_gb.keys) key_columns.push_back(k.column);
 	Geometry gs;
-	// Separate translation units, separated by a marker line: direct, partitioned, key statistics.
+	// Direct-partitioned variant: 2^12-slot tables over the 16-bit-per-key packing.
+	PipelineCodegen::GroupBySpec spec_dp = spec_gb;
+	spec_dp.direct_bits = 12;
+	spec_dp.key_bits = shift;
+	spec_dp.key_mult = (0x9e3779b97f4a7c15ull & (shift >= 64 ? ~0ull : (1ull << shift) - 1)) | 1ull;
+	spec_dp.key_mult_inv = 1;
+	spec_dp.bucket_threads = 1024;
+	// Separate translation units, separated by a marker line: direct, partitioned, key statistics,
+	// direct-partitioned.
 	return cg.EmitGroupBy(spec_gb, false, g) + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_gb, true, g) +
-	       "\n//@@VGPU_TU@@\n" + cg.EmitStats(key_columns, gs);
+	       "\n//@@VGPU_TU@@\n" + cg.EmitStats(key_columns, gs) + "\n//@@VGPU_TU@@\n" +
+	       cg.EmitGroupBy(spec_dp, true, g);
 }
 
 } // namespace vgpu

@@ -216,6 +216,25 @@ __device__ __forceinline__ void atomic_add_i128_pair(u64 *lo, i64 *hi, u64 add_l
 	if (hi_add != 0) atomicAdd(reinterpret_cast<u64 *>(hi), (u64)hi_add);
 }
 
+// Exact 128-bit accumulation into four 32-bit words (w0 least significant) with native 32-bit shared
+// atomics only: each word's carry is computed against the value that add replaced and passed to the
+// next word, so the words hold the true total under any interleaving (carry out of bit 127 wraps,
+// i.e. the sum is mod 2^128 like the addends). Non-negative addends below 2^32 cost one atomic.
+__device__ __forceinline__ u32 add_word_carry(u32 *w, u64 t) {
+	if (t == 0) return 0u;
+	if (t == (1ull << 32)) return 1u;
+	const u32 x = (u32)t;
+	const u32 old = atomicAdd(w, x);
+	return (u32)(old + x) < old ? 1u : 0u;
+}
+__device__ __forceinline__ void atomic_add_i128_u32x4(u32 *w0, u32 *w1, u32 *w2, u32 *w3, u64 lo, i64 hi) {
+	u32 c = add_word_carry(w0, (u64)(u32)lo);
+	c = add_word_carry(w1, (u64)(u32)(lo >> 32) + c);
+	c = add_word_carry(w2, (u64)(u32)(u64)hi + c);
+	const u32 top = (u32)((u64)hi >> 32) + c;
+	if (top) atomicAdd(w3, top);
+}
+
 __device__ __forceinline__ void atomic_min_i64(i64 *p, i64 v) { atomicMin(reinterpret_cast<long long *>(p), (long long)v); }
 __device__ __forceinline__ void atomic_max_i64(i64 *p, i64 v) { atomicMax(reinterpret_cast<long long *>(p), (long long)v); }
 

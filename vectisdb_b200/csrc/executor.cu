@@ -100,6 +100,9 @@ private:
 	void ComputeStats(PipelineInput &pin, PipelineCodegen &cg, const std::vector<int> &cols,
 	                  std::vector<std::pair<int64_t, int64_t>> &out);
 	void FillArgs(const PipelineInput &pin, KArgsHost &args);
+	uint64_t DirectBuckets(Module &module, const PipelineCodegen::GroupBySpec &gb, const PipelineInput &pin, uint64_t P,
+	                       uint64_t G, const uint32_t *offsets, const uint32_t *total, const char *records, uint64_t n,
+	                       uint64_t RS, Relation &out, int out_words, int threads);
 	uint64_t ReadU64(const void *dev);
 	uint32_t ReadU32(const void *dev);
 
@@ -643,20 +646,57 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		if (const char *env = std::getenv("VGPU_GB_PARTITIONS")) {  // tuning override (power of two)
 			P = std::min<uint64_t>(16384, std::max<uint64_t>(1, FloorPow2(std::strtoull(env, nullptr, 10))));
 		}
+		// Direct-partitioned when the packed key space is dense enough to be walked slot by slot
+		// (at most 4 slots per input row) and splits into at most 2^14 partitions of the largest
+		// shared-memory table: a row then costs no hashing and no probing.
+		const uint64_t dslot = static_cast<uint64_t>(PipelineCodegen::DirectSlotBytes(gb));
+		const int dbits_max = BitsFor(FloorPow2(smem_cap / dslot)) - 1;
+		bool dpart = shift <= dbits_max + 14 && domain <= 4 * n;
+		if (const char *env = std::getenv("VGPU_GB_STRATEGY")) {  // testing override: "hash" or "direct"
+			if (std::strcmp(env, "hash") == 0) dpart = false;
+			if (std::strcmp(env, "direct") == 0) dpart = shift <= dbits_max + 14;
+		}
+		if (dpart) {
+			int dbits = std::min(dbits_max, std::max(shift, 5));
+			if (const char *env = std::getenv("VGPU_GB_DIRECT_BITS")) {  // tuning override
+				dbits = std::min(dbits_max, std::max(5, std::atoi(env)));
+			}
+			dbits = std::max(dbits, shift - 14);  // at most 2^14 partitions (the partition histograms)
+			gb.direct_bits = dbits;
+			gb.key_bits = shift;
+			const uint64_t mask = (1ull << shift) - 1;
+			const uint64_t M = (0x9e3779b97f4a7c15ull & mask) | 1ull;
+			uint64_t inv = M;  // Newton iteration for the inverse mod 2^64: each step doubles the valid bits
+			for (int it = 0; it < 6; it++) inv *= 2 - M * inv;
+			gb.key_mult = M;
+			gb.key_mult_inv = inv & mask;
+			P = 1ull << std::max(0, shift - dbits);
+		}
 		int pbits = BitsFor(P - 1);
 		if (P == 1) pbits = 0;
 		gb.partition_bits = pbits;
 		gb.table_capacity = static_cast<int>(C);
+		int T1 = gb.direct_bits > 0 ? 1024 : 128;
+		if (const char *env = std::getenv("VGPU_GB_BUCKET_THREADS")) {  // tuning override (128..1024)
+			T1 = static_cast<int>(std::min<uint64_t>(1024, std::max<uint64_t>(128, FloorPow2(std::strtoull(env, nullptr, 10)))));
+		}
+		gb.bucket_threads = T1;
 		Geometry g;
 		g.block = 256;
 		g.items = 8;
+		if (const char *env = std::getenv("VGPU_GB_PART_BLOCK")) {  // tuning override (128..1024)
+			g.block = static_cast<int>(std::min<uint64_t>(1024, std::max<uint64_t>(128, FloorPow2(std::strtoull(env, nullptr, 10)))));
+		}
 		std::string src = cg.EmitGroupBy(gb, true, g);
 		last_source = src;
 		auto module = Runtime::Get().modules().GetOrCompile(src);
 		CUfunction fcount = module->Get("vgpu_gb_part_count");
-		const size_t part_smem = P * 4;
+		const size_t part_smem = (P + 32) * 4;  // partition counters + per-lane dummies for filtered rows
 		int occ = std::max(1, Runtime::Get().MaxActiveBlocks(fcount, g.block, part_smem));
 		occ = std::min(occ, std::max(1, Runtime::Get().MaxActiveBlocks(module->Get("vgpu_gb_part_scatter"), g.block, part_smem)));
+		if (const char *env = std::getenv("VGPU_GB_PART_OCC")) {  // tuning override: CTAs per SM
+			occ = std::min(occ, std::max(1, std::atoi(env)));
+		}
 		const uint64_t ntiles = (n + g.tile() - 1) / g.tile();
 		const uint64_t G = std::max<uint64_t>(1, std::min<uint64_t>(ntiles, uint64_t(props.sm_count) * occ));
 		const uint64_t tpc = (ntiles + G - 1) / G;
@@ -676,6 +716,11 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		char *records = static_cast<char *>(arena_.Alloc(n * RS));
 		a.SetPtr(cb + 4, records);
 		LaunchGenerated(*module, "vgpu_gb_part_scatter", static_cast<unsigned>(G), g.block, part_smem, stream_, a, in_bytes, n);
+		if (gb.direct_bits > 0) {
+			groups = DirectBuckets(*module, gb, pin, P, G, offsets, total, records, n, RS, out, out_words, T1);
+			for (auto &c : out) c.rows = groups;
+			return out;
+		}
 		// bucket tables. control: [0] work counter, [1] overflow count, [2] retry count, [3] retry work
 		// counter, [4, 4+P) overflow flags, [4+P, 4+2P) retry list.
 		const int W = cb + 6;
@@ -713,9 +758,9 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		{
 			const size_t smem1 = static_cast<size_t>(slot_bytes * C);
 			CUfunction fb = module->Get("vgpu_gb_bucket");
-			const int occ1 = std::max(1, Runtime::Get().MaxActiveBlocks(fb, 128, smem1));
+			const int occ1 = std::max(1, Runtime::Get().MaxActiveBlocks(fb, T1, smem1));
 			const unsigned grid1 = static_cast<unsigned>(std::min<uint64_t>(P, uint64_t(props.sm_count) * occ1));
-			LaunchGenerated(*module, "vgpu_gb_bucket", grid1, 128, smem1, stream_, b, part_bytes, n);
+			LaunchGenerated(*module, "vgpu_gb_bucket", grid1, T1, smem1, stream_, b, part_bytes, n);
 		}
 		{
 			const size_t smem2 = static_cast<size_t>(slot_bytes * C2);
@@ -787,6 +832,59 @@ Relation Executor::GroupBy(const PlanNode &node) {
 	}
 	for (auto &c : out) c.rows = groups;
 	return out;
+}
+
+// Bucket pass of the direct-partitioned group-by: a longest-first work list of (partition, row range)
+// items, partitions too large for one CTA split into chunks merged through global tables, then one
+// persistent launch over the list. Returns the group count.
+uint64_t Executor::DirectBuckets(Module &module, const PipelineCodegen::GroupBySpec &gb, const PipelineInput &pin,
+                                 uint64_t P, uint64_t G, const uint32_t *offsets, const uint32_t *total,
+                                 const char *records, uint64_t n, uint64_t RS, Relation &out, int out_words,
+                                 int threads) {
+	const auto &props = Runtime::Get().props();
+	const uint64_t D = 1ull << gb.direct_bits;
+	const uint64_t F = static_cast<uint64_t>(PipelineCodegen::StateWords(gb));
+	const size_t smem = static_cast<size_t>(D * PipelineCodegen::DirectSlotBytes(gb));
+	CUfunction fb = module.Get("vgpu_gb_dbucket");
+	const int occ = Runtime::Get().MaxActiveBlocks(fb, threads, smem);
+	if (occ < 1) Fail(VGPU_ERR_UNSUPPORTED, "gpu_groupby: direct-partitioned table does not fit on an SM");
+	const uint32_t ctas = static_cast<uint32_t>(props.sm_count * occ);
+	uint32_t min_split = 16384;
+	if (const char *env = std::getenv("VGPU_GB_SPLIT_ROWS")) {  // testing/tuning override
+		min_split = static_cast<uint32_t>(std::max<uint64_t>(256, std::strtoull(env, nullptr, 10)));
+	}
+	const uint64_t cap = kern::PlanWorkCapacity(static_cast<uint32_t>(P), n, min_split);
+	const uint32_t max_split = static_cast<uint32_t>(n / min_split + 1);
+	void *items = arena_.Alloc(cap * 16);
+	uint32_t *control = arena_.AllocT<uint32_t>(4);  // [0] items, [1] split partitions, [2] work counter
+	uint32_t *split_info = arena_.AllocT<uint32_t>(2ull * max_split);
+	uint64_t *out_count = arena_.AllocT<uint64_t>(1);
+	VGPU_CUDA(cudaMemsetAsync(control, 0, 16, stream_));
+	VGPU_CUDA(cudaMemsetAsync(out_count, 0, 8, stream_));
+	kern::PlanWork(offsets, G, static_cast<uint32_t>(P), total, min_split, ctas, items, control, split_info, max_split,
+	               stream_);
+	const uint32_t n_split = ReadU32(control + 1);
+	if (n_split > max_split) Fail(VGPU_ERR_INTERNAL, "gpu_groupby: work plan produced more splits than planned");
+	uint64_t *gtab = n_split ? arena_.AllocT<uint64_t>(static_cast<uint64_t>(n_split) * F * D) : nullptr;
+	const int cb = 2 + 2 * static_cast<int>(pin.sources.size());  // first consumer argument word
+	KArgsHost b;
+	FillArgs(pin, b);
+	b.SetPtr(cb, items);
+	b.SetPtr(cb + 1, control);
+	b.SetPtr(cb + 2, records);
+	b.SetPtr(cb + 3, gtab);
+	b.SetPtr(cb + 4, split_info);
+	b.SetPtr(cb + 5, control + 2);
+	b.SetPtr(cb + 6, out_count);
+	b.Set(cb + 7, n_split);
+	for (int w = 0; w < out_words; w++) b.SetPtr(cb + 8 + w, out[w].data);
+	if (n_split) {
+		const uint64_t words = static_cast<uint64_t>(n_split) * F * D;
+		const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((words + 255) / 256, uint64_t(props.sm_count) * 8));
+		LaunchGenerated(module, "vgpu_gb_dtab_init", grid, 256, 0, stream_, b, words * 8, 0);
+	}
+	LaunchGenerated(module, "vgpu_gb_dbucket", ctas, threads, smem, stream_, b, n * RS, n);
+	return ReadU64(out_count);
 }
 
 // ---- HASH_JOIN (sort-merge) ------------------------------------------------------------------------

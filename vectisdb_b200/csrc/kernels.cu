@@ -346,7 +346,93 @@ __global__ void JoinExpandKernel(const uint64_t *offsets, const uint64_t *lower,
 	}
 }
 
+// Work list of a partitioned aggregation pass. Item = (partition, first row, end row, split index or
+// ~0). Partitions above `split_rows` rows become ceil(size / split_rows) chunks sharing one split
+// index; everything is ordered longest first by size class (chunks of split partitions, then
+// partitions by descending floor(log2(size))), so the longest items start first and the persistent
+// CTAs finish together. Empty partitions produce no item. One CTA.
+constexpr int kPlanBlock = 1024;
+
+__global__ void __launch_bounds__(kPlanBlock) PlanWorkKernel(const uint32_t *offsets, uint64_t stride, uint32_t P,
+                                                             const uint32_t *total_rows, uint32_t min_split,
+                                                             uint32_t ctas, uint4 *items, uint32_t *counts,
+                                                             uint32_t *split_info, uint32_t max_split) {
+	__shared__ uint32_t cls_count[34];
+	__shared__ uint32_t cls_cursor[34];
+	__shared__ uint32_t n_split;
+	__shared__ uint32_t split_rows;
+	if (threadIdx.x < 34) cls_count[threadIdx.x] = 0;
+	if (threadIdx.x == 0) {
+		n_split = 0;
+		// chunks small enough that every CTA gets several items on average
+		const uint32_t total = *total_rows;
+		const uint32_t even = static_cast<uint32_t>(total / (4ull * (ctas ? ctas : 1)));
+		split_rows = even > min_split ? even : min_split;
+	}
+	__syncthreads();
+	const uint32_t total = *total_rows;
+	const uint32_t S = split_rows;
+	for (uint32_t p = threadIdx.x; p < P; p += blockDim.x) {
+		const uint32_t r0 = offsets[static_cast<uint64_t>(p) * stride];
+		const uint32_t r1 = p + 1 < P ? offsets[static_cast<uint64_t>(p + 1) * stride] : total;
+		const uint32_t size = r1 - r0;
+		if (size == 0) continue;
+		const bool split = size > S;
+		const uint32_t nch = split ? (size + S - 1) / S : 1u;
+		const int cls = split ? 33 : 31 - __clz(size);
+		atomicAdd(&cls_count[cls], nch);
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		uint32_t run = 0;
+		for (int c = 33; c >= 0; --c) {
+			cls_cursor[c] = run;
+			run += cls_count[c];
+		}
+		counts[0] = run;
+	}
+	__syncthreads();
+	for (uint32_t p = threadIdx.x; p < P; p += blockDim.x) {
+		const uint32_t r0 = offsets[static_cast<uint64_t>(p) * stride];
+		const uint32_t r1 = p + 1 < P ? offsets[static_cast<uint64_t>(p + 1) * stride] : total;
+		const uint32_t size = r1 - r0;
+		if (size == 0) continue;
+		const bool split = size > S;
+		const uint32_t nch = split ? (size + S - 1) / S : 1u;
+		const int cls = split ? 33 : 31 - __clz(size);
+		const uint32_t pos = atomicAdd(&cls_cursor[cls], nch);
+		uint32_t sidx = ~0u;
+		if (split) {
+			sidx = atomicAdd(&n_split, 1u);
+			if (sidx < max_split) {
+				split_info[2 * sidx] = nch;
+				split_info[2 * sidx + 1] = 0;
+			}
+		}
+		for (uint32_t c = 0; c < nch; ++c) {
+			const uint32_t a = r0 + c * S;
+			const uint32_t b = (c + 1 == nch) ? r1 : a + S;
+			items[pos + c] = make_uint4(p, a, b, sidx);
+		}
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) counts[1] = n_split;
+}
+
 } // namespace
+
+uint64_t PlanWorkCapacity(uint32_t P, uint64_t rows, uint32_t min_split) {
+	return static_cast<uint64_t>(P) + rows / (min_split ? min_split : 1) + 1;
+}
+
+void PlanWork(const uint32_t *offsets, uint64_t stride, uint32_t P, const uint32_t *total_rows, uint32_t min_split,
+              uint32_t ctas, void *items, uint32_t *counts, uint32_t *split_info, uint32_t max_split,
+              cudaStream_t stream) {
+	LaunchScope scope("plan_work", stream, static_cast<uint64_t>(P) * 8, P);
+	PlanWorkKernel<<<1, kPlanBlock, 0, stream>>>(offsets, stride, P, total_rows, min_split, ctas,
+	                                             static_cast<uint4 *>(items), counts, split_info, max_split);
+	VGPU_CUDA(cudaGetLastError());
+}
 
 void ExclusiveScanU32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *total, Arena &arena) {
 	ExclusiveScan<uint32_t>(in, out, n, total, arena);

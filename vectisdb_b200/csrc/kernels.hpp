@@ -48,5 +48,16 @@ void JoinSearch(const uint64_t *probe, uint64_t n_probe, const uint64_t *sorted,
 void JoinExpand(const uint64_t *offsets, const uint64_t *lower, uint64_t n_left, const uint32_t *sorted_perm,
                 uint64_t total, uint32_t *out_left, uint32_t *out_right, cudaStream_t stream);
 
+//! Work list of a partitioned aggregation pass over `P` partitions whose row ranges start at
+//! offsets[p * stride] (the last ends at *total_rows): 16-byte items (partition, first row, end row,
+//! split index or ~0u), longest first, into `items` (capacity PlanWorkCapacity). Partitions larger
+//! than max(min_split, total / (4 * ctas)) rows are split into chunks; chunks of one partition share a
+//! split index s with split_info[2s] = chunk count and split_info[2s+1] = 0 (a completion counter).
+//! counts[0] = items, counts[1] = split partitions (split_info is written for the first max_split).
+uint64_t PlanWorkCapacity(uint32_t P, uint64_t rows, uint32_t min_split);
+void PlanWork(const uint32_t *offsets, uint64_t stride, uint32_t P, const uint32_t *total_rows, uint32_t min_split,
+              uint32_t ctas, void *items, uint32_t *counts, uint32_t *split_info, uint32_t max_split,
+              cudaStream_t stream);
+
 } // namespace kern
 } // namespace vgpu
