@@ -127,24 +127,46 @@ __device__ __forceinline__ void load_rows(const T *__restrict__ base, u64 row0, 
 	}
 }
 
-// Fixed-size row records (W 32-bit words, W a multiple of 4): whole 16-byte vector stores and
-// streaming vector loads.
+// Fixed-size row records (W 32-bit words, W a multiple of 4; records 32-byte aligned when W is a
+// multiple of 8). A 32-byte record moves as one 256-bit access (sm_100 global vector width): one
+// store request per scattered record instead of two half-sector ones, and one fully coalesced load
+// per warp of consecutive records.
 template <int W> __device__ __forceinline__ void store_record(void *dst, const u32 (&w)[W]) {
+	if constexpr (W % 8 == 0) {
 #pragma unroll
-	for (int q = 0; q < W / 4; ++q) {
-		asm volatile("st.global.v4.u32 [%0], {%1,%2,%3,%4};" ::"l"(reinterpret_cast<char *>(dst) + 16 * q),
-		             "r"(w[4 * q]), "r"(w[4 * q + 1]), "r"(w[4 * q + 2]), "r"(w[4 * q + 3])
-		             : "memory");
+		for (int q = 0; q < W / 8; ++q) {
+			asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(reinterpret_cast<char *>(dst) + 32 * q),
+			             "r"(w[8 * q]), "r"(w[8 * q + 1]), "r"(w[8 * q + 2]), "r"(w[8 * q + 3]), "r"(w[8 * q + 4]),
+			             "r"(w[8 * q + 5]), "r"(w[8 * q + 6]), "r"(w[8 * q + 7])
+			             : "memory");
+		}
+	} else {
+#pragma unroll
+		for (int q = 0; q < W / 4; ++q) {
+			asm volatile("st.global.v4.u32 [%0], {%1,%2,%3,%4};" ::"l"(reinterpret_cast<char *>(dst) + 16 * q),
+			             "r"(w[4 * q]), "r"(w[4 * q + 1]), "r"(w[4 * q + 2]), "r"(w[4 * q + 3])
+			             : "memory");
+		}
 	}
 }
 template <int W> __device__ __forceinline__ void load_record(const void *src, u32 (&w)[W]) {
+	if constexpr (W % 8 == 0) {
 #pragma unroll
-	for (int q = 0; q < W / 4; ++q) {
-		uint4 v = ld_stream_v4(reinterpret_cast<const char *>(src) + 16 * q);
-		w[4 * q] = v.x;
-		w[4 * q + 1] = v.y;
-		w[4 * q + 2] = v.z;
-		w[4 * q + 3] = v.w;
+		for (int q = 0; q < W / 8; ++q) {
+			asm volatile("ld.global.cs.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+			             : "=r"(w[8 * q]), "=r"(w[8 * q + 1]), "=r"(w[8 * q + 2]), "=r"(w[8 * q + 3]), "=r"(w[8 * q + 4]),
+			               "=r"(w[8 * q + 5]), "=r"(w[8 * q + 6]), "=r"(w[8 * q + 7])
+			             : "l"(reinterpret_cast<const char *>(src) + 32 * q));
+		}
+	} else {
+#pragma unroll
+		for (int q = 0; q < W / 4; ++q) {
+			uint4 v = ld_stream_v4(reinterpret_cast<const char *>(src) + 16 * q);
+			w[4 * q] = v.x;
+			w[4 * q + 1] = v.y;
+			w[4 * q + 2] = v.z;
+			w[4 * q + 3] = v.w;
+		}
 	}
 }
 
