@@ -65,3 +65,27 @@ def test_nvrtc_reports_compile_errors():
     with pytest.raises(abi.VgpuError) as e:
         nvrtc_compile_check('extern "C" __global__ void k() { this is not cuda; }')
     assert e.value.status == abi.ERR_COMPILE
+
+
+def test_engine_nvrtc_is_independent_of_an_older_preloaded_copy():
+    """A process that already holds another NVRTC of the same soname (PyTorch's wheel ships one) must
+    not lend it to the engine: the generated kernels use sm_100 instruction forms that only the
+    engine's own toolkit NVRTC assembles. Runs in a child process so the preload stays contained."""
+    import os
+    import subprocess
+    import sys
+    torch = pytest.importorskip("torch")
+    lib = os.path.join(os.path.dirname(torch.__file__), "..", "nvidia", "cuda_nvrtc", "lib", "libnvrtc.so.12")
+    if not os.path.exists(lib):
+        pytest.skip("no separately packaged NVRTC to preload")
+    code = (
+        "import ctypes, sys\n"
+        f"ctypes.CDLL({lib!r}, mode=ctypes.RTLD_GLOBAL)\n"
+        "from vectisdb_b200 import workloads as W\n"
+        "from vectisdb_b200.engine import generate_source, nvrtc_compile_check\n"
+        "src = generate_source(W.c1(n=64).plan, W.c1(n=64).inputs)\n"
+        "print(min(nvrtc_compile_check(tu) for tu in src.split('//@@VGPU_TU@@')))\n")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert int(out.stdout.strip().splitlines()[-1]) > 1000

@@ -76,14 +76,15 @@ def build_engine(verbose: bool = False) -> Path:
         obj = BUILD / (name + ".o")
         objs.append(obj)
         if _stale(obj, [src] + headers):
-            cmd = [NVCC] + NVCC_FLAGS + ["-I", str(BUILD), "-c", str(src), "-o", str(obj)]
+            cmd = [NVCC] + NVCC_FLAGS + ["-I", str(BUILD), f'-DVGPU_CUDA_LIB_DIR="{CUDA / "lib64"}"', "-c", str(src),
+                                         "-o", str(obj)]
             jobs.append(cmd)
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
         list(ex.map(_run, jobs))
     lib = PKG / "libvgpu.so"
     if jobs or _stale(lib, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", str(lib)] + [str(o) for o in objs] +
-             ["-L", str(CUDA / "lib64"), "-lnvrtc", "-Xlinker", f"-rpath={CUDA / 'lib64'}"])
+             ["-ldl"])
     if verbose:
         print(f"built {lib}")
     return lib

@@ -7,6 +7,8 @@
 #include <cstdlib>
 #include <fstream>
 #include <sstream>
+#include <dlfcn.h>
+#include <mutex>
 #include <sys/stat.h>
 
 #include <nvrtc.h>
@@ -158,42 +160,101 @@ void Arena::FreeNow(void *ptr) {
 // ============================================================================================
 // NVRTC
 
+// NVRTC is bound at run time from the CUDA toolkit the engine was built against (a full path, local
+// symbols), not through the dynamic linker: a process that already holds another NVRTC of the same
+// soname (PyTorch ships one) would otherwise hand the engine that copy, whose PTX assembler may not
+// know the sm_100 instruction forms the generated kernels use. VGPU_NVRTC_LIBRARY overrides the path.
+#ifndef VGPU_CUDA_LIB_DIR
+#define VGPU_CUDA_LIB_DIR "/usr/local/cuda/lib64"
+#endif
+
+namespace {
+
+struct NvrtcApi {
+	decltype(&nvrtcCreateProgram) create = nullptr;
+	decltype(&nvrtcCompileProgram) compile = nullptr;
+	decltype(&nvrtcGetProgramLogSize) log_size = nullptr;
+	decltype(&nvrtcGetProgramLog) log = nullptr;
+	decltype(&nvrtcGetCUBINSize) cubin_size = nullptr;
+	decltype(&nvrtcGetCUBIN) cubin = nullptr;
+	decltype(&nvrtcDestroyProgram) destroy = nullptr;
+	decltype(&nvrtcGetErrorString) error_string = nullptr;
+	decltype(&nvrtcVersion) version = nullptr;
+};
+
+const NvrtcApi &Nvrtc() {
+	static std::mutex mu;
+	static NvrtcApi api;
+	static bool loaded = false;
+	std::lock_guard<std::mutex> lock(mu);
+	if (loaded) {
+		return api;
+	}
+	const char *env = std::getenv("VGPU_NVRTC_LIBRARY");
+	const std::string path = env ? env : VGPU_CUDA_LIB_DIR "/libnvrtc.so.12";
+	void *h = dlopen(path.c_str(), RTLD_NOW | RTLD_LOCAL);
+	if (!h) {
+		const char *err = dlerror();
+		Fail(VGPU_ERR_COMPILE, "cannot load NVRTC from " + path + ": " + (err ? err : "unknown error"));
+	}
+	NvrtcApi a;
+	auto bind = [&](auto &fn, const char *name) {
+		fn = reinterpret_cast<std::remove_reference_t<decltype(fn)>>(dlsym(h, name));
+		if (!fn) Fail(VGPU_ERR_COMPILE, std::string("NVRTC library ") + path + " lacks " + name);
+	};
+	bind(a.create, "nvrtcCreateProgram");
+	bind(a.compile, "nvrtcCompileProgram");
+	bind(a.log_size, "nvrtcGetProgramLogSize");
+	bind(a.log, "nvrtcGetProgramLog");
+	bind(a.cubin_size, "nvrtcGetCUBINSize");
+	bind(a.cubin, "nvrtcGetCUBIN");
+	bind(a.destroy, "nvrtcDestroyProgram");
+	bind(a.error_string, "nvrtcGetErrorString");
+	bind(a.version, "nvrtcVersion");
+	api = a;
+	loaded = true;
+	return api;
+}
+
+} // namespace
+
 #define VGPU_NVRTC(call)                                                                                      \
 	do {                                                                                                       \
 		nvrtcResult _r = (call);                                                                               \
 		if (_r != NVRTC_SUCCESS) {                                                                             \
-			Fail(VGPU_ERR_COMPILE, std::string(#call) + ": " + nvrtcGetErrorString(_r));                       \
+			Fail(VGPU_ERR_COMPILE, std::string(#call) + ": " + Nvrtc().error_string(_r));                      \
 		}                                                                                                      \
 	} while (0)
 
 std::vector<char> CompileToCubin(const std::string &source, const std::string &arch, std::string *log_out) {
+	const NvrtcApi &nv = Nvrtc();
 	nvrtcProgram prog = nullptr;
 	const char *header_sources[] = {kDeviceLibSource};
 	const char *header_names[] = {"vgpu_device_lib.cuh"};
-	VGPU_NVRTC(nvrtcCreateProgram(&prog, source.c_str(), "vgpu_fused.cu", 1, header_sources, header_names));
+	VGPU_NVRTC(nv.create(&prog, source.c_str(), "vgpu_fused.cu", 1, header_sources, header_names));
 	std::string arch_opt = "--gpu-architecture=" + arch;
 	std::vector<const char *> opts = {arch_opt.c_str(), "--fmad=false", "-std=c++17", "-DVGPU_NVRTC=1",
 	                                  "--extra-device-vectorization", "-lineinfo"};
-	nvrtcResult r = nvrtcCompileProgram(prog, static_cast<int>(opts.size()), opts.data());
+	nvrtcResult r = nv.compile(prog, static_cast<int>(opts.size()), opts.data());
 	size_t log_size = 0;
-	nvrtcGetProgramLogSize(prog, &log_size);
+	nv.log_size(prog, &log_size);
 	std::string log;
 	if (log_size > 1) {
 		log.resize(log_size);
-		nvrtcGetProgramLog(prog, &log[0]);
+		nv.log(prog, &log[0]);
 	}
 	if (log_out) {
 		*log_out = log;
 	}
 	if (r != NVRTC_SUCCESS) {
-		nvrtcDestroyProgram(&prog);
+		nv.destroy(&prog);
 		Fail(VGPU_ERR_COMPILE, "NVRTC compilation failed:\n" + log + "\n--- generated source ---\n" + source);
 	}
 	size_t cubin_size = 0;
-	VGPU_NVRTC(nvrtcGetCUBINSize(prog, &cubin_size));
+	VGPU_NVRTC(nv.cubin_size(prog, &cubin_size));
 	std::vector<char> cubin(cubin_size);
-	VGPU_NVRTC(nvrtcGetCUBIN(prog, cubin.data()));
-	nvrtcDestroyProgram(&prog);
+	VGPU_NVRTC(nv.cubin(prog, cubin.data()));
+	nv.destroy(&prog);
 	return cubin;
 }
 
