@@ -74,9 +74,18 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except FileNotFoundError:
             self.proc = None
+            return
+        # nvidia-smi's start-up (NVML initialisation) competes with the driver for a moment: let it
+        # finish (first sample written) before anything is timed.
+        deadline = time.time() + 5.0
+        while time.time() < deadline and self.proc.poll() is None:
+            if self.path.exists() and self.path.read_text().count("\n") >= 1:
+                break
+            time.sleep(0.02)
+        time.sleep(0.1)
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -153,7 +162,7 @@ def run_reference(args, world, rank):
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=50)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c2b"])
