@@ -37,8 +37,13 @@ def hbm_peak():
     return 6650.0, "fallback"
 
 
-def make_workload(name: str, pinned: bool):
+def make_workload(name: str, pinned: bool, rows: int = 0):
+    """The named benchmark query on its full-size table, or on `rows` rows (probe rows for c2, side
+    length for c2b) for small profiling cases."""
     from vectisdb_b200 import workloads as W
+    if rows:
+        return {"c0": lambda: W.c0(n=rows, pinned=pinned), "c1": lambda: W.c1(n=rows, pinned=pinned),
+                "c2": lambda: W.c2(probe_n=rows, pinned=pinned), "c2b": lambda: W.c2b(side=rows)}[name]()
     return {"c0": lambda: W.c0(pinned=pinned), "c1": lambda: W.c1(pinned=pinned),
             "c2": lambda: W.c2(pinned=pinned), "c2b": lambda: W.c2b()}[name]()
 
@@ -50,6 +55,7 @@ def algorithmic_bytes(name: str, wl, kernel: str, passing: int, groups: int) -> 
         return {"vgpu_gb_part_count": 16 * n,                     # a, b, ts
                 "vgpu_gb_part_scatter": 32 * n + 32 * passing,    # all columns in; key+3 values out
                 "vgpu_gb_bucket": 32 * passing + 48 * groups,     # partitioned rows in; groups out
+                "vgpu_gb_dbucket": 32 * passing + 48 * groups,    # partitioned rows in; groups out
                 }.get(kernel, 0)
     if name == "c0":
         return {"vgpu_gb_direct": 20 * n}.get(kernel, 0)
@@ -168,6 +174,7 @@ def main():
     p.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c2b"])
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--rows", type=int, default=0, help="small-case size for profiling (0 = the full workload)")
     args = p.parse_args()
     world, rank, local = dist_setup()
 
@@ -187,7 +194,7 @@ def main():
 
     lib().vgpu_set_device(local)
     name = args.config
-    wl = make_workload(name, pinned=True)
+    wl = make_workload(name, pinned=True, rows=args.rows)
     engine = GpuEngine.instance()
     stream = torch.cuda.current_stream()
 
@@ -284,7 +291,7 @@ def main():
         if i > 0:
             e2e_ms.append(dt * 1000)
         d2h = sum(c.data.nbytes + (0 if c.validity is None else (len(c.validity) + 7) // 8) for c in r.columns)
-    e2e_value = wl.rows * world / (float(np.mean(e2e_ms)) / 1000.0)
+    e2e_value = wl.rows * world / (float(np.mean(e2e_ms)) / 1000.0) if e2e_ms else None
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -326,7 +333,7 @@ def main():
             "kernels": {k: {"launches": v[1], "ms": round(v[0], 4), "share": round(v[0] / total_ms, 4)}
                         for k, v in sorted(per.items(), key=lambda kv: -kv[1][0])},
             "e2e": {"value": e2e_value, "unit": "rows/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "ms_per_step": float(np.mean(e2e_ms))},
+                    "ms_per_step": float(np.mean(e2e_ms)) if e2e_ms else None},
             "gpu_launches": launches,
             "clocks": clocks,
             "cpu_baseline": cpu,
