@@ -181,6 +181,11 @@ size_t vgpu_result_column_count(const vgpu_result *result);
 vgpu_status vgpu_result_get_column(const vgpu_result *result, size_t index, vgpu_column *out);
 void vgpu_result_free(vgpu_result *result);
 
+/* Copies `bytes` of device memory (a device-resident result column, for instance) to host memory,
+ * ordered after the work already queued on `stream` (NULL = the engine's stream); returns when the
+ * copy is complete. No single reference counterpart: the reference always returns host columns. */
+vgpu_status vgpu_copy_to_host(void *dst, const void *src, size_t bytes, void *stream);
+
 /* Thread-local message describing the last failed call on this thread ("" if none). */
 const char *vgpu_last_error(void);
 const char *vgpu_status_string(vgpu_status status);
@@ -300,6 +305,45 @@ vgpu_status vgpu_cache_invalidate_table(const vgpu_table_ref *table);
 vgpu_status vgpu_cache_invalidate_all(void);
 uint64_t vgpu_cache_current_bytes(void);
 uint64_t vgpu_cache_table_generation(const vgpu_table_ref *table);
+
+/* ---- Batching: many queries in one persistent, graph-captured launch ------------------------------
+ * No single reference function: this is the batching form added beside the reference's
+ * one-plan-per-call ExecutePlan (gpu_engine.hpp:389-402). Plans of the form GROUP_BY(keys) <-
+ * FILTER/PROJECTION* <- SCAN whose expression sources differ only in numeric literals share one
+ * kernel; a persistent launch walks a (query, row tile) queue over all of them and one CTA per
+ * query writes its groups. The launch pair is captured in a CUDA graph on `options->stream` and
+ * replayed while a later call presents the same batch (same columns, constants and geometry).
+ * Other plans run one by one through vgpu_execute_plan. results[i] belongs to plans[i]; each is
+ * freed with vgpu_result_free. Device results of one call share buffers that live until the last
+ * of them is freed. */
+typedef struct vgpu_batch_options {
+	int32_t block;      /* threads per CTA; 0 = tuned or default */
+	int32_t items;      /* consecutive rows per thread; 0 = tuned or default */
+	int32_t tile_rows;  /* rows per queue item; 0 = tuned or default */
+	int32_t smem_slots; /* shared-memory table slots (queries with larger key spaces use global tables) */
+	int32_t use_graph;  /* capture and replay the launch pair in a CUDA graph (needs a non-legacy stream) */
+	int32_t autotune;   /* time the candidate geometries on this batch now and remember the best */
+} vgpu_batch_options;
+
+typedef struct vgpu_batch_stats {
+	uint64_t batched;       /* queries run by the batch kernel */
+	uint64_t fallback;      /* queries run one by one */
+	uint64_t templates;     /* distinct templates, one kernel each */
+	uint64_t graph_replays; /* graph launches that reused a captured graph */
+	int32_t block, items, tile_rows, smem_slots; /* geometry used for the last template */
+} vgpu_batch_stats;
+
+void vgpu_batch_options_init(vgpu_batch_options *options);
+vgpu_status vgpu_execute_batch(const vgpu_plan *const *plans, const vgpu_column *const *inputs,
+                               const size_t *n_inputs, size_t n_plans, const vgpu_exec_options *options,
+                               const vgpu_batch_options *batch_options, vgpu_result **results,
+                               vgpu_batch_stats *stats);
+/* The template of one expression source: its numeric literals replaced by per-query parameter reads
+ * (inputs[...] indices stay literal). Writes up to `capacity` bytes (NUL-terminated) and the number
+ * of parameters. Host-only; for tests and plan inspection. */
+vgpu_status vgpu_batch_template(const char *source, char *out, size_t capacity, size_t *length, size_t *n_params);
+/* Drops cached batch graphs and buffers and the in-memory autotuning table. */
+vgpu_status vgpu_batch_clear(void);
 
 /* ---- Group-by without device allocation ------------------------------------------------------
  * No counterpart in the reference. For callers that cannot call cudaMalloc (a host callback or a

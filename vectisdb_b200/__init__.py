@@ -5,6 +5,10 @@ the reference engine interface (`engine`), the ctypes ABI (`abi`), the synthetic
 (`workloads`) and the build script (`build`).
 """
 from .engine import (  # noqa: F401
+    BatchOptions,
+    batch_clear,
+    batch_template,
+    device_to_host,
     ColumnCache,
     DeviceResult,
     ExecuteOptions,

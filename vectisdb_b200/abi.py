@@ -60,6 +60,17 @@ class vgpu_exec_options(C.Structure):
                 ("stream", C.c_void_p)]
 
 
+class vgpu_batch_options(C.Structure):
+    _fields_ = [("block", C.c_int32), ("items", C.c_int32), ("tile_rows", C.c_int32), ("smem_slots", C.c_int32),
+                ("use_graph", C.c_int32), ("autotune", C.c_int32)]
+
+
+class vgpu_batch_stats(C.Structure):
+    _fields_ = [("batched", C.c_uint64), ("fallback", C.c_uint64), ("templates", C.c_uint64),
+                ("graph_replays", C.c_uint64), ("block", C.c_int32), ("items", C.c_int32),
+                ("tile_rows", C.c_int32), ("smem_slots", C.c_int32)]
+
+
 class vgpu_device_info(C.Structure):
     _fields_ = [("device", C.c_int32), ("sm_count", C.c_int32), ("cc_major", C.c_int32),
                 ("cc_minor", C.c_int32), ("total_memory", C.c_uint64), ("free_memory", C.c_uint64),
@@ -97,6 +108,15 @@ SIGNATURES = [
     ("vgpu_result_column_count", C.c_size_t, [C.c_void_p]),
     ("vgpu_result_get_column", C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(vgpu_column)]),
     ("vgpu_result_free", None, [C.c_void_p]),
+    ("vgpu_batch_options_init", None, [C.POINTER(vgpu_batch_options)]),
+    ("vgpu_execute_batch", C.c_int, [C.POINTER(C.POINTER(vgpu_plan)), C.POINTER(C.POINTER(vgpu_column)),
+                                     C.POINTER(C.c_size_t), C.c_size_t, C.POINTER(vgpu_exec_options),
+                                     C.POINTER(vgpu_batch_options), C.POINTER(C.c_void_p),
+                                     C.POINTER(vgpu_batch_stats)]),
+    ("vgpu_batch_template", C.c_int, [C.c_char_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t),
+                                      C.POINTER(C.c_size_t)]),
+    ("vgpu_batch_clear", C.c_int, []),
+    ("vgpu_copy_to_host", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
     ("vgpu_last_error", C.c_char_p, []),
     ("vgpu_status_string", C.c_char_p, [C.c_int]),
     ("vgpu_abi_version", C.c_int, []),

@@ -31,6 +31,7 @@ ENGINE_SOURCES = [
     "column_cache.cpp",
     "kernels.cu",
     "executor.cu",
+    "batch.cu",
     "noalloc.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

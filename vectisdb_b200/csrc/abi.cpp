@@ -12,6 +12,7 @@
 
 #include "column_cache.hpp"
 #include "cost_model.hpp"
+#include "batch.hpp"
 #include "executor.hpp"
 #include "plan.hpp"
 #include "runtime.hpp"
@@ -145,6 +146,94 @@ vgpu_status vgpu_execute_plan(const vgpu_plan *plan, const vgpu_column *inputs, 
 		}
 		*out = r;
 	});
+}
+
+void vgpu_batch_options_init(vgpu_batch_options *options) {
+	if (!options) return;
+	std::memset(options, 0, sizeof(*options));
+	options->use_graph = 1;
+}
+
+vgpu_status vgpu_execute_batch(const vgpu_plan *const *plans, const vgpu_column *const *inputs,
+                               const size_t *n_inputs, size_t n_plans, const vgpu_exec_options *options,
+                               const vgpu_batch_options *batch_options, vgpu_result **results,
+                               vgpu_batch_stats *stats) {
+	return Guard([&] {
+		if (n_plans > 0 && (plans == nullptr || results == nullptr)) Fail(VGPU_ERR_INVALID_ARGUMENT, "null plans or results");
+		for (size_t i = 0; i < n_plans; i++) results[i] = nullptr;
+		std::vector<std::shared_ptr<PlanNode>> roots;
+		std::vector<std::vector<vgpu_column>> ins(n_plans);
+		for (size_t i = 0; i < n_plans; i++) {
+			roots.push_back(ConvertPlan(plans[i]));
+			const size_t k = n_inputs ? n_inputs[i] : 0;
+			if (k > 0 && (inputs == nullptr || inputs[i] == nullptr)) Fail(VGPU_ERR_INVALID_ARGUMENT, "null inputs with nonzero count");
+			if (k > 0) ins[i].assign(inputs[i], inputs[i] + k);
+		}
+		ExecOptions eo;
+		cudaStream_t stream = nullptr;
+		if (options) {
+			eo.serve_whole_scan_from_cache = options->serve_whole_scan_from_cache != 0;
+			eo.cache_chunk_index = options->cache_chunk_index;
+			eo.stage_scan_to_cache = options->stage_scan_to_cache != 0;
+			eo.output_on_device = options->output_memory == VGPU_MEM_DEVICE;
+			stream = static_cast<cudaStream_t>(options->stream);
+		}
+		if (stream == nullptr) stream = Runtime::Get().default_stream();
+		BatchOptions bo;
+		if (batch_options) {
+			bo.block = batch_options->block;
+			bo.items = batch_options->items;
+			bo.tile_rows = batch_options->tile_rows;
+			bo.smem_slots = batch_options->smem_slots;
+			bo.use_graph = batch_options->use_graph != 0;
+			bo.autotune = batch_options->autotune != 0;
+		}
+		BatchStats st;
+		auto out = ExecuteBatch(roots, ins, eo, bo, stream, &st);
+		for (size_t i = 0; i < n_plans; i++) {
+			auto *r = new vgpu_result();
+			r->exec = std::move(out[i]);
+			results[i] = r;
+		}
+		if (stats) {
+			stats->batched = st.batched;
+			stats->fallback = st.fallback;
+			stats->templates = st.templates;
+			stats->graph_replays = st.graph_replays;
+			stats->block = st.block;
+			stats->items = st.items;
+			stats->tile_rows = st.tile_rows;
+			stats->smem_slots = st.smem_slots;
+		}
+	});
+}
+
+vgpu_status vgpu_batch_template(const char *source, char *out, size_t capacity, size_t *length, size_t *n_params) {
+	return Guard([&] {
+		if (!source) Fail(VGPU_ERR_INVALID_ARGUMENT, "null source");
+		TemplatedSource t = TemplateLiterals(source, 0);
+		if (length) *length = t.text.size();
+		if (n_params) *n_params = t.types.size();
+		if (out && capacity > 0) {
+			const size_t k = std::min(capacity - 1, t.text.size());
+			std::memcpy(out, t.text.data(), k);
+			out[k] = '\0';
+		}
+	});
+}
+
+vgpu_status vgpu_copy_to_host(void *dst, const void *src, size_t bytes, void *stream) {
+	return Guard([&] {
+		if (bytes == 0) return;
+		if (!dst || !src) Fail(VGPU_ERR_INVALID_ARGUMENT, "null pointer");
+		cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : Runtime::Get().default_stream();
+		VGPU_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+		VGPU_CUDA(cudaStreamSynchronize(s));
+	});
+}
+
+vgpu_status vgpu_batch_clear(void) {
+	return Guard([&] { ClearBatchCaches(); });
 }
 
 size_t vgpu_result_column_count(const vgpu_result *result) {

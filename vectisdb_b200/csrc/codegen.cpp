@@ -2,6 +2,7 @@
 #include "codegen.hpp"
 
 #include <algorithm>
+#include <cctype>
 #include <map>
 #include <regex>
 #include <set>
@@ -282,6 +283,23 @@ void PipelineCodegen::Resolve() {
 				c.nullable = nullable;
 				if (!nullable) {
 					c.valid = "true";
+				}
+				// An identity projection (out = in, same type) passes its source column through, so the
+				// source's statistics (key ranges for group-by packing) still describe it.
+				if (expr.input_columns.size() == 1) {
+					RewrittenExpr rw = RewriteExpression(expr.source, 1);
+					std::string st;
+					for (char ch : rw.statement) {
+						if (!std::isspace(static_cast<unsigned char>(ch))) st += ch;
+					}
+					if (st == "vgpu_out=vgpu_in_0;" && rw.input_ctypes[0] == rw.output_ctype) {
+						for (size_t cc = 0; cc < cols.size(); cc++) {
+							if (cols[cc].name == expr.input_columns[0] && cols[cc].source >= 0 &&
+							    cols[cc].type == expr.output_type) {
+								c.source = cols[cc].source;
+							}
+						}
+					}
 				}
 				next.push_back(c);
 				next_deps.push_back(d);
@@ -592,14 +610,15 @@ std::string MergeCode(const std::vector<Field> &fields, const std::string &src, 
 // Outputs start at word `out_base`: keys first, then aggregates (HUGEINT outputs are 16 bytes/row).
 std::string FinalizeCode(const PipelineCodegen::GroupBySpec &gb, const std::vector<Field> &fields,
                          const std::vector<PipeColumn> &visible, const std::string &tab, const std::string &s,
-                         const std::string &key, const std::string &pos, int out_base) {
+                         const std::string &key, const std::string &pos, int out_base,
+                         const std::string &out_array = "a.w") {
 	std::ostringstream o;
 	int w = out_base;
 	for (auto &k : gb.keys) {
 		const auto &col = visible[k.column];
 		const char *t = CudaTypeName(col.type);
 		uint64_t mask = k.bits >= 64 ? ~0ull : ((1ull << k.bits) - 1);
-		o << "\t\t\t((" << t << "*)a.w[" << w << "])[" << pos << "] = (" << t << ")((i64)((" << key << " >> " << k.shift
+		o << "\t\t\t((" << t << "*)" << out_array << "[" << w << "])[" << pos << "] = (" << t << ")((i64)((" << key << " >> " << k.shift
 		  << ") & 0x" << std::hex << mask << std::dec << "ull) + (" << k.min << "LL));\n";
 		w++;
 	}
@@ -607,7 +626,7 @@ std::string FinalizeCode(const PipelineCodegen::GroupBySpec &gb, const std::vect
 	for (size_t i = 0; i < gb.aggs.size(); i++) {
 		auto &a = gb.aggs[i];
 		int ai = static_cast<int>(i);
-		std::string out = "a.w[" + std::to_string(w) + "]";
+		std::string out = out_array + "[" + std::to_string(w) + "]";
 		switch (a.kind) {
 		case AggKind::COUNT_STAR:
 		case AggKind::COUNT:
@@ -1413,6 +1432,143 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 	  << "\t\tvgpu_bucket_process(a, list[e], tables + tab_off[e], caps[e], caps[e], &overflow);\n"
 	  << "\t\tif (threadIdx.x == 0 && overflow) atomicAdd((u32*)a.w[" << W + 2 << "], 1u);\n"
 	  << "\t\t__syncthreads();\n\t}\n}\n";
+	return o.str();
+}
+
+std::string PipelineCodegen::EmitBatchGroupBy(const GroupBySpec &gb, const Geometry &g, int tile_rows, int smem_slots,
+                                              const BatchLayout &L) const {
+	// One kernel for every query of a batch that shares this plan template. Query q's columns, key
+	// packing, table placement and literal constants come from its row of the query table (L.qwords
+	// u64 words): [0] rows, [1+2i] source i data, [2+2i] source i validity (unused), [key_base+2j]
+	// key j minimum, [key_base+2j+1] key j shift | bits << 8, [dom_base] table slots D,
+	// [dom_base+1] accumulator offset, [dom_base+2] output row offset, [dom_base+3] 1 = shared-memory
+	// table, [param_base..] the literal constants as 64-bit patterns.
+	// vgpu_batch_gb args: w[0] queries, w[1] query table, w[2] tiles (uint2 query, tile), w[3] tiles,
+	//   w[4] tile work counter (u32*, zero at launch), w[5] accumulators (u64, F arrays of w[6] words), w[6] accumulator words
+	//   per field, w[7] output pointer table (u64 [out words]), w[8] group counts (u64 [queries]).
+	std::ostringstream o;
+	o << Prologue();
+	o << "#define vgpu_qpd(j) __longlong_as_double((long long)vgpu_qp[(j)])\n"
+	  << "#define vgpu_qpf(j) __int_as_float((int)(u32)vgpu_qp[(j)])\n"
+	  << "#define vgpu_qpi(j) ((int)(long long)vgpu_qp[(j)])\n"
+	  << "#define vgpu_qpu(j) ((unsigned)vgpu_qp[(j)])\n"
+	  << "#define vgpu_qpl(j) ((long long)vgpu_qp[(j)])\n"
+	  << "#define vgpu_qpul(j) ((unsigned long long)vgpu_qp[(j)])\n\n";
+	const auto fields = StateFields(gb);
+	const int F = static_cast<int>(fields.size());
+	std::vector<int> used;
+	for (auto &k : gb.keys) used.push_back(k.column);
+	for (auto &a : gb.aggs) {
+		if (a.column >= 0) used.push_back(a.column);
+	}
+	auto needed = NeededSources(used);
+	std::ostringstream pack;
+	pack << "(0ull";
+	for (size_t j = 0; j < gb.keys.size(); j++) {
+		const auto &k = gb.keys[j];
+		pack << " | ((u64)((i64)(" << visible_[k.column].value << ") - (i64)qp[" << L.key_base + 2 * j
+		     << "]) << ((u32)qp[" << L.key_base + 2 * j + 1 << "] & 0xffu))";
+	}
+	pack << ")";
+	std::vector<std::string> values;
+	for (auto &a : gb.aggs) values.push_back(a.column >= 0 ? visible_[a.column].value : "0");
+	const int T = smem_slots;
+	o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_batch_gb(KArgs a) {\n"
+	  << "\textern __shared__ __align__(16) u64 vgpu_smem[];\n"
+	  << "\tconst u64 *qtab = (const u64*)a.w[1];\n"
+	  << "\tconst uint2 *tiles = (const uint2*)a.w[2];\n"
+	  << "\tconst u64 ntiles = a.w[3];\n\tu32 *work = (u32*)a.w[4];\n\t__shared__ u32 cur_t;\n"
+	  << "\tu64 *acc = (u64*)a.w[5];\n\tconst u64 ACC = a.w[6];\n";
+	for (int f = 0; f < F; f++) o << "\tu64 *T" << f << " = vgpu_smem + " << f * T << ";\n";
+	o << "\tfor (u32 s = threadIdx.x; s < " << T << "u; s += blockDim.x) {\n";
+	for (int f = 0; f < F; f++) o << "\t\tT" << f << "[s] = " << InitValue(fields[f]) << ";\n";
+	o << "\t}\n\t__syncthreads();\n"
+	  << "\tu32 cur_q = 0xffffffffu; bool cur_sm = false; u64 cur_d = 0;\n";
+	for (int f = 0; f < F; f++) o << "\tu64 *G" << f << " = acc;\n";
+	std::ostringstream flush;
+	flush << "\t\t\t__syncthreads();\n"
+	      << "\t\t\tfor (u32 s = threadIdx.x; s < (u32)cur_d; s += blockDim.x) {\n\t\t\t\tif (T0[s] != 0) {\n"
+	      << MergeCode(fields, "T", "s", "G", "s");
+	for (int f = 0; f < F; f++) flush << "\t\t\t\tT" << f << "[s] = " << InitValue(fields[f]) << ";\n";
+	flush << "\t\t\t\t}\n\t\t\t}\n\t\t\t__syncthreads();\n";
+	// tiles are claimed one at a time from a counter (queries differ in size by orders of magnitude;
+	// the queue lists the largest queries first)
+	o << "\twhile (true) {\n"
+	  << "\t\tif (threadIdx.x == 0) cur_t = atomicAdd(work, 1u);\n"
+	  << "\t\t__syncthreads();\n"
+	  << "\t\tconst u64 t = cur_t;\n"
+	  << "\t\t__syncthreads();\n"
+	  << "\t\tif (t >= ntiles) break;\n"
+	  << "\t\tconst uint2 tl = tiles[t];\n"
+	  << "\t\tconst u64 *qp = qtab + (u64)tl.x * " << L.qwords << "ull;\n"
+	  << "\t\tif (tl.x != cur_q) {\n"
+	  << "\t\t\t// the CTA moves to another query: its shared table goes to the previous query's accumulators\n"
+	  << "\t\t\tif (cur_sm) {\n" << flush.str() << "\t\t\t}\n"
+	  << "\t\t\tcur_q = tl.x; cur_d = qp[" << L.dom_base << "]; cur_sm = qp[" << L.dom_base + 3 << "] != 0;\n";
+	for (int f = 0; f < F; f++) {
+		o << "\t\t\tG" << f << " = acc + " << f << "ull * ACC + qp[" << L.dom_base + 1 << "];\n";
+	}
+	o << "\t\t}\n"
+	  << "\t\tconst u64 *vgpu_qp = qp + " << L.param_base << ";\n\t\t(void)vgpu_qp;\n"
+	  << "\t\tconst u64 n = qp[0];\n"
+	  << "\t\tconst u64 t0 = (u64)tl.y * " << tile_rows << "ull;\n"
+	  << "\t\tconst u64 t1 = t0 + " << tile_rows << "ull < n ? t0 + " << tile_rows << "ull : n;\n"
+	  << "\t\tfor (u64 sub = t0; sub < t1; sub += " << g.tile() << "ull) {\n"
+	  << "\t\tconst u64 row0 = sub + (u64)threadIdx.x * " << g.items << ";\n";
+	for (size_t i = 0; i < spec_.sources.size(); i++) {
+		if (!needed[i]) continue;
+		const char *t = CudaTypeName(spec_.sources[i].type);
+		o << "\t\t" << t << " s" << i << "[" << g.items << "];\n"
+		  << "\t\tload_rows<" << t << ", " << g.items << ">((const " << t << "*)qp[" << 1 + 2 * i << "], row0, t1, s" << i
+		  << ");\n";
+	}
+	o << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) {\n"
+	  << "\t\tconst u64 row = row0 + r; (void)row;\n\t\tbool keep = row < t1;\n"
+	  << chain_code_ << "\t\tif (keep) {\n"
+	  << "\t\t\tconst u64 slot = " << pack.str() << ";\n"
+	  << "\t\t\tif (cur_sm) {\n" << UpdateCode(fields, "T", "slot", values) << "\t\t\t} else {\n"
+	  << UpdateCode(fields, "G", "slot", values) << "\t\t\t}\n"
+	  << "\t\t}\n\t\t}\n\t\t}\n\t}\n"
+	  << "\tif (cur_sm) {\n" << flush.str() << "\t}\n}\n\n";
+
+	// accumulators to identity (first use of a batch's buffers; the final kernel resets what it reads)
+	o << "extern \"C\" __global__ void vgpu_batch_init(KArgs a) {\n"
+	  << "\tu64 *acc = (u64*)a.w[5];\n\tconst u64 ACC = a.w[6];\n"
+	  << "\tfor (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < " << F
+	  << "ull * ACC; i += (u64)gridDim.x * blockDim.x) {\n\t\tconst u64 f = i / ACC;\n\t\tu64 v = 0ull;\n";
+	for (int f = 0; f < F; f++) o << "\t\tif (f == " << f << "ull) v = " << InitValue(fields[f]) << ";\n";
+	o << "\t\tacc[i] = v;\n\t}\n}\n\n";
+
+	// one CTA per query: its live slots, in key order, into the outputs; the accumulators are reset
+	GroupBySpec aggs_only = gb;
+	aggs_only.keys.clear();
+	const int nk = static_cast<int>(gb.keys.size());
+	o << "extern \"C\" __global__ void __launch_bounds__(1024) vgpu_batch_final(KArgs a) {\n"
+	  << "\t__shared__ u32 scan_scratch[33];\n"
+	  << "\tconst u32 q = blockIdx.x;\n"
+	  << "\tconst u64 *qp = (const u64*)a.w[1] + (u64)q * " << L.qwords << "ull;\n"
+	  << "\tu64 *acc = (u64*)a.w[5];\n\tconst u64 ACC = a.w[6];\n"
+	  << "\tconst u64 *outp = (const u64*)a.w[7];\n"
+	  << "\tconst u64 D = qp[" << L.dom_base << "], outb = qp[" << L.dom_base + 2 << "];\n";
+	for (int f = 0; f < F; f++) o << "\tu64 *G" << f << " = acc + " << f << "ull * ACC + qp[" << L.dom_base + 1 << "];\n";
+	o << "\tu64 base = 0;\n"
+	  << "\tfor (u64 c0 = 0; c0 < D; c0 += blockDim.x) {\n"
+	  << "\t\tconst u64 s = c0 + threadIdx.x;\n"
+	  << "\t\tconst bool live = s < D && G0[s] != 0;\n"
+	  << "\t\tu32 total; const u32 off = block_exclusive_scan(live ? 1u : 0u, scan_scratch, &total);\n"
+	  << "\t\tif (live) {\n\t\t\tconst u64 pos = outb + base + off;\n\t\t\tconst u64 key = s;\n";
+	for (int j = 0; j < nk; j++) {
+		const char *t = CudaTypeName(visible_[gb.keys[j].column].type);
+		o << "\t\t\t{ const u32 sb = (u32)qp[" << L.key_base + 2 * j + 1 << "]; const u32 bits = sb >> 8;\n"
+		  << "\t\t\t  const u64 mask = bits >= 64 ? ~0ull : ((1ull << bits) - 1ull);\n"
+		  << "\t\t\t  ((" << t << "*)outp[" << j << "])[pos] = (" << t << ")((i64)((key >> (sb & 0xffu)) & mask) + (i64)qp["
+		  << L.key_base + 2 * j << "]); }\n";
+	}
+	o << FinalizeCode(aggs_only, fields, visible_, "G", "s", "key", "pos", nk, "outp") << "\t\t}\n"
+	  << "\t\tif (s < D) {\n";
+	for (int f = 0; f < F; f++) o << "\t\t\tG" << f << "[s] = " << InitValue(fields[f]) << ";\n";
+	o << "\t\t}\n\t\tbase += total;\n\t}\n"
+	  << "\tif (threadIdx.x == 0) ((u64*)a.w[8])[q] = base;\n}\n";
 	return o.str();
 }
 

@@ -111,6 +111,18 @@ public:
 	//!  direct-partitioned: vgpu_gb_part_count, vgpu_gb_part_scatter, vgpu_gb_dtab_init, vgpu_gb_dbucket
 	std::string EmitGroupBy(const GroupBySpec &gb, bool partitioned, const Geometry &g) const;
 
+	//! Word offsets inside one query's row of a batch query table (see EmitBatchGroupBy).
+	struct BatchLayout {
+		int qwords = 0;
+		int key_base = 0;
+		int dom_base = 0;
+		int param_base = 0;
+	};
+	//! Batched group-by over many queries sharing this plan template (literals read from the query
+	//! table through vgpu_qp*): vgpu_batch_init, vgpu_batch_gb (persistent over (query, tile) items),
+	//! vgpu_batch_final (one CTA per query).
+	std::string EmitBatchGroupBy(const GroupBySpec &gb, const Geometry &g, int tile_rows, int smem_slots,
+	                             const BatchLayout &L) const;
 	//! Number of 8-byte per-group aggregate state fields (excluding the key), as laid out by EmitGroupBy.
 	static int StateWords(const GroupBySpec &gb);
 	//! Shared-memory bytes per slot of a direct-partitioned table (32-bit count and sum words).

@@ -427,27 +427,10 @@ void Executor::ComputeStats(PipelineInput &pin, PipelineCodegen &cg, const std::
 
 // ---- GROUP BY --------------------------------------------------------------------------------------
 
-Relation Executor::GroupBy(const PlanNode &node) {
-	if (node.children.size() != 1) {
-		Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: GROUP_BY_AGGREGATE expects exactly one child");
-	}
-	if (node.group_keys.empty() && node.aggregates.empty()) {
-		Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_groupby: node has neither group keys nor aggregates");
-	}
-	std::vector<const PlanNode *> chain;
-	const PlanNode *cur = node.children[0].get();
-	while (cur->op == OpType::FILTER || cur->op == OpType::PROJECTION) {
-		if (cur->children.size() != 1) {
-			Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: FILTER/PROJECTION expects exactly one child");
-		}
-		chain.push_back(cur);
-		cur = cur->children[0].get();
-	}
-	PipelineInput pin = BuildPipeline(*cur, chain);
-	PipelineCodegen cg(pin.spec);
-	if (cg.visible().empty()) {
-		Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_groupby: input operator produced no columns to group");
-	}
+// Group-by validation shared by the single-query and batched paths. Mirrors
+// operators/gpu_groupby.cu:224-299 and :320-350.
+PipelineCodegen::GroupBySpec ValidateGroupByNode(const PlanNode &node, const PipelineCodegen &cg,
+                                                 std::vector<int> &key_cols) {
 	auto find = [&](const std::string &name, const char *what) {
 		int c = cg.FindVisible(name);
 		if (c < 0) {
@@ -456,7 +439,7 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		return c;
 	};
 	// Validation mirrors operators/gpu_groupby.cu:224-299 and :320-350.
-	std::vector<int> key_cols;
+	key_cols.clear();
 	for (auto &k : node.group_keys) {
 		int c = find(k, "group key");
 		const ValueType t = cg.visible()[c].type;
@@ -519,6 +502,32 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		}
 		gb.aggs.push_back(s);
 	}
+	return gb;
+}
+
+Relation Executor::GroupBy(const PlanNode &node) {
+	if (node.children.size() != 1) {
+		Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: GROUP_BY_AGGREGATE expects exactly one child");
+	}
+	if (node.group_keys.empty() && node.aggregates.empty()) {
+		Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_groupby: node has neither group keys nor aggregates");
+	}
+	std::vector<const PlanNode *> chain;
+	const PlanNode *cur = node.children[0].get();
+	while (cur->op == OpType::FILTER || cur->op == OpType::PROJECTION) {
+		if (cur->children.size() != 1) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: FILTER/PROJECTION expects exactly one child");
+		}
+		chain.push_back(cur);
+		cur = cur->children[0].get();
+	}
+	PipelineInput pin = BuildPipeline(*cur, chain);
+	PipelineCodegen cg(pin.spec);
+	if (cg.visible().empty()) {
+		Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_groupby: input operator produced no columns to group");
+	}
+	std::vector<int> key_cols;
+	PipelineCodegen::GroupBySpec gb = ValidateGroupByNode(node, cg, key_cols);
 	const uint64_t n = pin.rows;
 	auto empty_result = [&]() {
 		Relation out;
@@ -1009,6 +1018,10 @@ Relation Executor::Exec(const PlanNode &node) {
 }
 
 } // namespace
+
+PipelineCodegen::GroupBySpec ValidateGroupBy(const PlanNode &node, const PipelineCodegen &cg, std::vector<int> &key_cols) {
+	return ValidateGroupByNode(node, cg, key_cols);
+}
 
 ExecResult ExecutePlan(const PlanNode &plan, const std::vector<vgpu_column> &inputs, const ExecOptions &options,
                        cudaStream_t stream) {

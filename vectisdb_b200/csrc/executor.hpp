@@ -46,8 +46,14 @@ struct ExecOptions {
 struct ExecResult {
 	std::vector<HostColumnOut> columns;
 	std::vector<void *> device_buffers; // owned device memory (device output mode)
+	std::vector<std::shared_ptr<void>> keepalive; // device memory shared with other results (batches)
 	cudaStream_t stream = nullptr;
 };
+
+//! Validates a GROUP_BY_AGGREGATE node against its input pipeline and returns its aggregate spec;
+//! `key_cols` receives the visible column of each group key. Throws Error(VGPU_ERR_UNSUPPORTED /
+//! INVALID_ARGUMENT) for what this GPU path does not model.
+PipelineCodegen::GroupBySpec ValidateGroupBy(const PlanNode &node, const PipelineCodegen &cg, std::vector<int> &key_cols);
 
 //! Executes `plan` over `inputs`. Throws Error on any failure (nothing partial escapes).
 ExecResult ExecutePlan(const PlanNode &plan, const std::vector<vgpu_column> &inputs, const ExecOptions &options,

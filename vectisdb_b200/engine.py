@@ -388,6 +388,88 @@ class GpuEngine:
         return GpuExecutionResult(True, "", abi.OK, columns)
 
 
+    def execute_batch(self, plans: Sequence[GpuPlanNode], inputs: Sequence[Sequence[GpuColumn]],
+                      options: ExecuteOptions | None = None, batch: BatchOptions | None = None):
+        """Many plans in one call (vgpu_execute_batch): plans sharing a template run in one persistent,
+        graph-captured launch. Returns (results in plan order, stats dict). Raises VgpuError on failure."""
+        keep = _Keep()
+        n = len(plans)
+        if len(inputs) != n:
+            raise ValueError("one input list per plan")
+        plan_cs = [serialize_plan(p, keep) for p in plans]
+        col_cs = [serialize_inputs(cols, keep) if len(cols) else None for cols in inputs]
+        PlanPtr = C.POINTER(abi.vgpu_plan)
+        ColPtr = C.POINTER(abi.vgpu_column)
+        plan_arr = (PlanPtr * max(1, n))(*[C.pointer(pc) for pc in plan_cs])
+        col_arr = (ColPtr * max(1, n))(*[C.cast(c, ColPtr) if c is not None else ColPtr() for c in col_cs])
+        counts = (C.c_size_t * max(1, n))(*[len(cols) for cols in inputs])
+        opts = abi.vgpu_exec_options()
+        self.lib.vgpu_exec_options_init(C.byref(opts))
+        o = options or ExecuteOptions()
+        opts.serve_whole_scan_from_cache = int(o.serve_whole_scan_from_cache)
+        opts.output_memory = abi.MEM_DEVICE if o.output_on_device else abi.MEM_HOST
+        opts.stream = o.stream or None
+        bo = abi.vgpu_batch_options()
+        self.lib.vgpu_batch_options_init(C.byref(bo))
+        b = batch or BatchOptions()
+        bo.block, bo.items, bo.tile_rows, bo.smem_slots = b.block, b.items, b.tile_rows, b.smem_slots
+        bo.use_graph, bo.autotune = int(b.use_graph), int(b.autotune)
+        handles = (C.c_void_p * max(1, n))()
+        st = abi.vgpu_batch_stats()
+        abi.check(self.lib.vgpu_execute_batch(plan_arr, col_arr, counts, n, C.byref(opts), C.byref(bo), handles,
+                                              C.byref(st)))
+        results = []
+        for i in range(n):
+            h = C.c_void_p(handles[i])
+            try:
+                columns = _read_result(h)
+            except Exception:
+                for j in range(i, n):
+                    self.lib.vgpu_result_free(C.c_void_p(handles[j]))
+                raise
+            if o.output_on_device:
+                results.append(DeviceResult(h, columns))
+            else:
+                self.lib.vgpu_result_free(h)
+                results.append(GpuExecutionResult(True, "", abi.OK, columns))
+        stats = {k: getattr(st, k) for k, _ in abi.vgpu_batch_stats._fields_}
+        return results, stats
+
+
+@dataclass
+class BatchOptions:
+    """vgpu_batch_options: 0 = tuned or default."""
+    block: int = 0
+    items: int = 0
+    tile_rows: int = 0
+    smem_slots: int = 0
+    use_graph: bool = True
+    autotune: bool = False
+
+
+def batch_template(source: str) -> tuple[str, int]:
+    """The per-query template of an expression source and its parameter count."""
+    n, k = C.c_size_t(), C.c_size_t()
+    L = abi.lib()
+    abi.check(L.vgpu_batch_template(source.encode(), None, 0, C.byref(n), C.byref(k)))
+    buf = C.create_string_buffer(n.value + 1)
+    abi.check(L.vgpu_batch_template(source.encode(), buf, n.value + 1, C.byref(n), C.byref(k)))
+    return buf.value.decode(), k.value
+
+
+def device_to_host(col: GpuColumn, stream: int = 0) -> np.ndarray:
+    """Host copy of a device-resident result column (vgpu_copy_to_host, after `stream`'s queued work)."""
+    dt = NUMPY_DTYPE[col.type]
+    out = np.empty(col.row_count, dtype=dt)
+    if col.row_count:
+        abi.check(abi.lib().vgpu_copy_to_host(out.ctypes.data, col.device_ptr, out.nbytes, stream or None))
+    return out
+
+
+def batch_clear() -> None:
+    abi.check(abi.lib().vgpu_batch_clear())
+
+
 # ---- engine-level helpers -----------------------------------------------------------------------------
 
 def sha256_hex(data: bytes) -> str:

@@ -231,3 +231,24 @@ def c2b(side: int = C2B_SIDE, seed: int = 5, modulus: int = 13) -> Workload:
     return Workload("c2b", c2b_plan(modulus), [make_column("a", T.INT32, a), make_column("b", T.INT32, b)],
                     side * side, 0.0, {"modulus": modulus, "side": side},
                     {"c2b_l": ["a"], "c2b_r": ["b"]})
+
+
+C3_QUERIES = 256
+
+
+def c3(n_queries: int = C3_QUERIES, seed: int = 3, min_log2: int = 10, max_log2: int = 22, card_lo: int = 16,
+       card_hi: int = 1 << 16, pinned: bool = False) -> list[Workload]:
+    """Batching workload: C0-shaped filter + group-by queries, each over its own table. Row counts are
+    log-uniform over [2^min_log2, 2^max_log2], group cardinality log-uniform over [card_lo, card_hi];
+    every query has its own predicate constants (v < v_lt, w % w_mod <> 0)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(n_queries):
+        n = int(round(2 ** rng.uniform(min_log2, max_log2)))
+        k_card = int(round(2 ** rng.uniform(np.log2(card_lo), np.log2(card_hi))))
+        v_lt = float(np.round(rng.uniform(0.1, 0.9), 6))
+        w_mod = int(rng.integers(2, 17))
+        wl = c0(n=n, seed=(seed << 16) + q, k_card=k_card, v_lt=v_lt, w_mod=w_mod, pinned=pinned, table=f"c3_q{q}")
+        wl.name = "c3"
+        out.append(wl)
+    return out
