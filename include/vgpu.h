@@ -334,6 +334,17 @@ typedef struct vgpu_batch_stats {
 } vgpu_batch_stats;
 
 void vgpu_batch_options_init(vgpu_batch_options *options);
+
+/* A prepared batch: the plans converted, templated and grouped once, for repeated execution (the
+ * per-call work is then resolving the columns and launching). Freed with vgpu_batch_free. */
+typedef struct vgpu_batch vgpu_batch;
+vgpu_status vgpu_batch_prepare(const vgpu_plan *const *plans, size_t n_plans, vgpu_batch **out);
+size_t vgpu_batch_size(const vgpu_batch *batch);
+vgpu_status vgpu_batch_execute(vgpu_batch *batch, const vgpu_column *const *inputs, const size_t *n_inputs,
+                               const vgpu_exec_options *options, const vgpu_batch_options *batch_options,
+                               vgpu_result **results, vgpu_batch_stats *stats);
+void vgpu_batch_free(vgpu_batch *batch);
+/* One-shot form: prepare, execute, free. */
 vgpu_status vgpu_execute_batch(const vgpu_plan *const *plans, const vgpu_column *const *inputs,
                                const size_t *n_inputs, size_t n_plans, const vgpu_exec_options *options,
                                const vgpu_batch_options *batch_options, vgpu_result **results,

@@ -113,6 +113,12 @@ SIGNATURES = [
                                      C.POINTER(C.c_size_t), C.c_size_t, C.POINTER(vgpu_exec_options),
                                      C.POINTER(vgpu_batch_options), C.POINTER(C.c_void_p),
                                      C.POINTER(vgpu_batch_stats)]),
+    ("vgpu_batch_prepare", C.c_int, [C.POINTER(C.POINTER(vgpu_plan)), C.c_size_t, C.POINTER(C.c_void_p)]),
+    ("vgpu_batch_size", C.c_size_t, [C.c_void_p]),
+    ("vgpu_batch_execute", C.c_int, [C.c_void_p, C.POINTER(C.POINTER(vgpu_column)), C.POINTER(C.c_size_t),
+                                     C.POINTER(vgpu_exec_options), C.POINTER(vgpu_batch_options),
+                                     C.POINTER(C.c_void_p), C.POINTER(vgpu_batch_stats)]),
+    ("vgpu_batch_free", None, [C.c_void_p]),
     ("vgpu_batch_template", C.c_int, [C.c_char_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t),
                                       C.POINTER(C.c_size_t)]),
     ("vgpu_batch_clear", C.c_int, []),

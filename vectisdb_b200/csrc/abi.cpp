@@ -154,57 +154,110 @@ void vgpu_batch_options_init(vgpu_batch_options *options) {
 	options->use_graph = 1;
 }
 
+struct vgpu_batch {
+	std::shared_ptr<PreparedBatch> prepared;
+};
+
+namespace {
+
+void RunPreparedBatch(const PreparedBatch &pb, const vgpu_column *const *inputs, const size_t *n_inputs,
+                      const vgpu_exec_options *options, const vgpu_batch_options *batch_options,
+                      vgpu_result **results, vgpu_batch_stats *stats) {
+	const size_t n_plans = pb.plans.size();
+	if (n_plans > 0 && results == nullptr) Fail(VGPU_ERR_INVALID_ARGUMENT, "null results");
+	for (size_t i = 0; i < n_plans; i++) results[i] = nullptr;
+	std::vector<std::vector<vgpu_column>> ins(n_plans);
+	for (size_t i = 0; i < n_plans; i++) {
+		const size_t k = n_inputs ? n_inputs[i] : 0;
+		if (k > 0 && (inputs == nullptr || inputs[i] == nullptr)) Fail(VGPU_ERR_INVALID_ARGUMENT, "null inputs with nonzero count");
+		if (k > 0) ins[i].assign(inputs[i], inputs[i] + k);
+	}
+	ExecOptions eo;
+	cudaStream_t stream = nullptr;
+	if (options) {
+		eo.serve_whole_scan_from_cache = options->serve_whole_scan_from_cache != 0;
+		eo.cache_chunk_index = options->cache_chunk_index;
+		eo.stage_scan_to_cache = options->stage_scan_to_cache != 0;
+		eo.output_on_device = options->output_memory == VGPU_MEM_DEVICE;
+		stream = static_cast<cudaStream_t>(options->stream);
+	}
+	if (stream == nullptr) stream = Runtime::Get().default_stream();
+	BatchOptions bo;
+	if (batch_options) {
+		bo.block = batch_options->block;
+		bo.items = batch_options->items;
+		bo.tile_rows = batch_options->tile_rows;
+		bo.smem_slots = batch_options->smem_slots;
+		bo.use_graph = batch_options->use_graph != 0;
+		bo.autotune = batch_options->autotune != 0;
+	}
+	BatchStats st;
+	auto out = ExecutePrepared(pb, ins, eo, bo, stream, &st);
+	for (size_t i = 0; i < n_plans; i++) {
+		auto *r = new vgpu_result();
+		r->exec = std::move(out[i]);
+		results[i] = r;
+	}
+	if (stats) {
+		stats->batched = st.batched;
+		stats->fallback = st.fallback;
+		stats->templates = st.templates;
+		stats->graph_replays = st.graph_replays;
+		stats->block = st.block;
+		stats->items = st.items;
+		stats->tile_rows = st.tile_rows;
+		stats->smem_slots = st.smem_slots;
+	}
+}
+
+std::shared_ptr<PreparedBatch> PrepareFromAbi(const vgpu_plan *const *plans, size_t n_plans) {
+	if (n_plans > 0 && plans == nullptr) Fail(VGPU_ERR_INVALID_ARGUMENT, "null plans");
+	std::vector<std::shared_ptr<PlanNode>> roots;
+	for (size_t i = 0; i < n_plans; i++) roots.push_back(ConvertPlan(plans[i]));
+	return PrepareBatch(roots);
+}
+
+} // namespace
+
+vgpu_status vgpu_batch_prepare(const vgpu_plan *const *plans, size_t n_plans, vgpu_batch **out) {
+	return Guard([&] {
+		if (!out) Fail(VGPU_ERR_INVALID_ARGUMENT, "null batch pointer");
+		*out = nullptr;
+		auto *b = new vgpu_batch();
+		try {
+			b->prepared = PrepareFromAbi(plans, n_plans);
+		} catch (...) {
+			delete b;
+			throw;
+		}
+		*out = b;
+	});
+}
+
+size_t vgpu_batch_size(const vgpu_batch *batch) {
+	return batch && batch->prepared ? batch->prepared->plans.size() : 0;
+}
+
+vgpu_status vgpu_batch_execute(vgpu_batch *batch, const vgpu_column *const *inputs, const size_t *n_inputs,
+                               const vgpu_exec_options *options, const vgpu_batch_options *batch_options,
+                               vgpu_result **results, vgpu_batch_stats *stats) {
+	return Guard([&] {
+		if (!batch || !batch->prepared) Fail(VGPU_ERR_INVALID_ARGUMENT, "null batch");
+		RunPreparedBatch(*batch->prepared, inputs, n_inputs, options, batch_options, results, stats);
+	});
+}
+
+void vgpu_batch_free(vgpu_batch *batch) {
+	delete batch;
+}
+
 vgpu_status vgpu_execute_batch(const vgpu_plan *const *plans, const vgpu_column *const *inputs,
                                const size_t *n_inputs, size_t n_plans, const vgpu_exec_options *options,
                                const vgpu_batch_options *batch_options, vgpu_result **results,
                                vgpu_batch_stats *stats) {
 	return Guard([&] {
-		if (n_plans > 0 && (plans == nullptr || results == nullptr)) Fail(VGPU_ERR_INVALID_ARGUMENT, "null plans or results");
-		for (size_t i = 0; i < n_plans; i++) results[i] = nullptr;
-		std::vector<std::shared_ptr<PlanNode>> roots;
-		std::vector<std::vector<vgpu_column>> ins(n_plans);
-		for (size_t i = 0; i < n_plans; i++) {
-			roots.push_back(ConvertPlan(plans[i]));
-			const size_t k = n_inputs ? n_inputs[i] : 0;
-			if (k > 0 && (inputs == nullptr || inputs[i] == nullptr)) Fail(VGPU_ERR_INVALID_ARGUMENT, "null inputs with nonzero count");
-			if (k > 0) ins[i].assign(inputs[i], inputs[i] + k);
-		}
-		ExecOptions eo;
-		cudaStream_t stream = nullptr;
-		if (options) {
-			eo.serve_whole_scan_from_cache = options->serve_whole_scan_from_cache != 0;
-			eo.cache_chunk_index = options->cache_chunk_index;
-			eo.stage_scan_to_cache = options->stage_scan_to_cache != 0;
-			eo.output_on_device = options->output_memory == VGPU_MEM_DEVICE;
-			stream = static_cast<cudaStream_t>(options->stream);
-		}
-		if (stream == nullptr) stream = Runtime::Get().default_stream();
-		BatchOptions bo;
-		if (batch_options) {
-			bo.block = batch_options->block;
-			bo.items = batch_options->items;
-			bo.tile_rows = batch_options->tile_rows;
-			bo.smem_slots = batch_options->smem_slots;
-			bo.use_graph = batch_options->use_graph != 0;
-			bo.autotune = batch_options->autotune != 0;
-		}
-		BatchStats st;
-		auto out = ExecuteBatch(roots, ins, eo, bo, stream, &st);
-		for (size_t i = 0; i < n_plans; i++) {
-			auto *r = new vgpu_result();
-			r->exec = std::move(out[i]);
-			results[i] = r;
-		}
-		if (stats) {
-			stats->batched = st.batched;
-			stats->fallback = st.fallback;
-			stats->templates = st.templates;
-			stats->graph_replays = st.graph_replays;
-			stats->block = st.block;
-			stats->items = st.items;
-			stats->tile_rows = st.tile_rows;
-			stats->smem_slots = st.smem_slots;
-		}
+		auto pb = PrepareFromAbi(plans, n_plans);
+		RunPreparedBatch(*pb, inputs, n_inputs, options, batch_options, results, stats);
 	});
 }
 

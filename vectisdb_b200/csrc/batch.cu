@@ -776,20 +776,46 @@ void ClearBatchCaches() {
 	Tuner().Clear();
 }
 
+std::shared_ptr<PreparedBatch> PrepareBatch(const std::vector<std::shared_ptr<PlanNode>> &plans) {
+	auto pb = std::make_shared<PreparedBatch>();
+	for (auto &plan : plans) {
+		PreparedPlan pp;
+		pp.plan = plan;
+		pp.scan = BatchShape(*plan);
+		if (pp.scan) {
+			pp.templ = TemplatePlan(*plan, pp.ptypes, pp.params);
+			std::ostringstream sig;
+			Signature(*pp.templ, sig);
+			sig << "|params:" << std::string(pp.ptypes.begin(), pp.ptypes.end());
+			pp.sig_base = sig.str();
+		}
+		pb->plans.push_back(std::move(pp));
+	}
+	return pb;
+}
+
 std::vector<ExecResult> ExecuteBatch(const std::vector<std::shared_ptr<PlanNode>> &plans,
                                      const std::vector<std::vector<vgpu_column>> &inputs, const ExecOptions &options,
                                      const BatchOptions &bopts, cudaStream_t stream, BatchStats *stats) {
-	if (plans.size() != inputs.size()) Fail(VGPU_ERR_INVALID_ARGUMENT, "batch: one input list per plan");
+	return ExecutePrepared(*PrepareBatch(plans), inputs, options, bopts, stream, stats);
+}
+
+std::vector<ExecResult> ExecutePrepared(const PreparedBatch &pb, const std::vector<std::vector<vgpu_column>> &inputs,
+                                        const ExecOptions &options, const BatchOptions &bopts, cudaStream_t stream,
+                                        BatchStats *stats) {
+	const size_t nplans = pb.plans.size();
+	if (nplans != inputs.size()) Fail(VGPU_ERR_INVALID_ARGUMENT, "batch: one input list per plan");
 	if (options.cache_chunk_index >= 0 || options.stage_scan_to_cache) {
 		Fail(VGPU_ERR_UNSUPPORTED, "batch: chunked cache serving and staging run through vgpu_execute_plan");
 	}
-	std::vector<ExecResult> results(plans.size());
-	std::vector<Prepared> prep(plans.size());
+	std::vector<ExecResult> results(nplans);
+	std::vector<Prepared> prep(nplans);
 	Arena arena(stream);  // device copies of host inputs, alive until the batch has run
-	for (size_t i = 0; i < plans.size(); i++) {
+	for (size_t i = 0; i < nplans; i++) {
 		Prepared &p = prep[i];
 		p.index = i;
-		const PlanNode *scan = BatchShape(*plans[i]);
+		const PreparedPlan &pp = pb.plans[i];
+		const PlanNode *scan = pp.scan;
 		if (!scan) continue;
 		bool ok = true;
 		std::vector<DevColumn> cols;
@@ -825,12 +851,12 @@ std::vector<ExecResult> ExecuteBatch(const std::vector<std::shared_ptr<PlanNode>
 		if (!ok || cols.empty()) continue;
 		p.sources = cols;
 		p.rows = cols.front().rows;
-		p.templ = TemplatePlan(*plans[i], p.ptypes, p.params);
+		p.templ = pp.templ;
+		p.ptypes = pp.ptypes;
+		p.params = pp.params;
 		std::ostringstream sig;
-		Signature(*p.templ, sig);
-		sig << "|types:";
+		sig << pp.sig_base << "|types:";
 		for (auto &c : cols) sig << static_cast<int>(c.type) << ",";
-		sig << "|params:" << std::string(p.ptypes.begin(), p.ptypes.end());
 		p.sig = sig.str();
 		p.batchable = true;
 	}
@@ -841,16 +867,16 @@ std::vector<ExecResult> ExecuteBatch(const std::vector<std::shared_ptr<PlanNode>
 	for (auto &p : prep) {
 		if (p.batchable) groups[p.sig].push_back(&p);
 	}
-	std::vector<bool> done(plans.size(), false);
+	std::vector<bool> done(nplans, false);
 	for (auto &kv : groups) {
 		if (RunTemplate(kv.second, options, bopts, stream, results, stats)) {
 			for (auto *p : kv.second) done[p->index] = true;
 		}
 	}
 	VGPU_CUDA(cudaStreamSynchronize(stream));
-	for (size_t i = 0; i < plans.size(); i++) {
+	for (size_t i = 0; i < nplans; i++) {
 		if (done[i]) continue;
-		results[i] = ExecutePlan(*plans[i], inputs[i], options, stream);
+		results[i] = ExecutePlan(*pb.plans[i].plan, inputs[i], options, stream);
 		if (stats) stats->fallback++;
 	}
 	return results;

@@ -32,6 +32,23 @@ struct BatchStats {
 	int block = 0, items = 0, tile_rows = 0, smem_slots = 0;  // geometry of the last template
 };
 
+//! Plans converted, templated and signed once for repeated execution (a prepared batch).
+struct PreparedPlan {
+	std::shared_ptr<PlanNode> plan;
+	const PlanNode *scan = nullptr;  // the SCAN leaf when the plan has the batch form
+	std::shared_ptr<PlanNode> templ;
+	std::vector<char> ptypes;
+	std::vector<uint64_t> params;
+	std::string sig_base;
+};
+struct PreparedBatch {
+	std::vector<PreparedPlan> plans;
+};
+std::shared_ptr<PreparedBatch> PrepareBatch(const std::vector<std::shared_ptr<PlanNode>> &plans);
+std::vector<ExecResult> ExecutePrepared(const PreparedBatch &batch, const std::vector<std::vector<vgpu_column>> &inputs,
+                                        const ExecOptions &options, const BatchOptions &bopts, cudaStream_t stream,
+                                        BatchStats *stats);
+
 //! Executes every plan over its inputs; results in plan order. Queries of the form
 //! GROUP_BY(keys) <- FILTER/PROJECTION* <- SCAN, with pass-through integer keys and no NULLs, run in
 //! the batch kernel; any other plan runs through ExecutePlan. Throws Error on failure.

@@ -388,19 +388,29 @@ class GpuEngine:
         return GpuExecutionResult(True, "", abi.OK, columns)
 
 
-    def execute_batch(self, plans: Sequence[GpuPlanNode], inputs: Sequence[Sequence[GpuColumn]],
-                      options: ExecuteOptions | None = None, batch: BatchOptions | None = None):
-        """Many plans in one call (vgpu_execute_batch): plans sharing a template run in one persistent,
-        graph-captured launch. Returns (results in plan order, stats dict). Raises VgpuError on failure."""
+    def prepare_batch(self, plans: Sequence[GpuPlanNode]) -> "PreparedBatch":
+        """vgpu_batch_prepare: plans converted, templated and grouped once for repeated execution."""
         keep = _Keep()
+        plan_cs = [serialize_plan(p, keep) for p in plans]
         n = len(plans)
+        PlanPtr = C.POINTER(abi.vgpu_plan)
+        plan_arr = (PlanPtr * max(1, n))(*[C.pointer(pc) for pc in plan_cs])
+        handle = C.c_void_p()
+        abi.check(self.lib.vgpu_batch_prepare(plan_arr, n, C.byref(handle)))
+        return PreparedBatch(handle, n)
+
+    def execute_batch(self, plans, inputs: Sequence[Sequence[GpuColumn]], options: ExecuteOptions | None = None,
+                      batch: BatchOptions | None = None):
+        """Many plans in one call: plans sharing a template run in one persistent, graph-captured
+        launch. `plans` is a list of plans (vgpu_execute_batch) or a PreparedBatch
+        (vgpu_batch_execute). Returns (results in plan order, stats dict). Raises VgpuError."""
+        keep = _Keep()
+        prepared = plans if isinstance(plans, PreparedBatch) else None
+        n = prepared.size if prepared else len(plans)
         if len(inputs) != n:
             raise ValueError("one input list per plan")
-        plan_cs = [serialize_plan(p, keep) for p in plans]
         col_cs = [serialize_inputs(cols, keep) if len(cols) else None for cols in inputs]
-        PlanPtr = C.POINTER(abi.vgpu_plan)
         ColPtr = C.POINTER(abi.vgpu_column)
-        plan_arr = (PlanPtr * max(1, n))(*[C.pointer(pc) for pc in plan_cs])
         col_arr = (ColPtr * max(1, n))(*[C.cast(c, ColPtr) if c is not None else ColPtr() for c in col_cs])
         counts = (C.c_size_t * max(1, n))(*[len(cols) for cols in inputs])
         opts = abi.vgpu_exec_options()
@@ -416,8 +426,15 @@ class GpuEngine:
         bo.use_graph, bo.autotune = int(b.use_graph), int(b.autotune)
         handles = (C.c_void_p * max(1, n))()
         st = abi.vgpu_batch_stats()
-        abi.check(self.lib.vgpu_execute_batch(plan_arr, col_arr, counts, n, C.byref(opts), C.byref(bo), handles,
-                                              C.byref(st)))
+        if prepared:
+            abi.check(self.lib.vgpu_batch_execute(prepared.handle, col_arr, counts, C.byref(opts), C.byref(bo),
+                                                  handles, C.byref(st)))
+        else:
+            plan_cs = [serialize_plan(p, keep) for p in plans]
+            PlanPtr = C.POINTER(abi.vgpu_plan)
+            plan_arr = (PlanPtr * max(1, n))(*[C.pointer(pc) for pc in plan_cs])
+            abi.check(self.lib.vgpu_execute_batch(plan_arr, col_arr, counts, n, C.byref(opts), C.byref(bo), handles,
+                                                  C.byref(st)))
         results = []
         for i in range(n):
             h = C.c_void_p(handles[i])
@@ -434,6 +451,25 @@ class GpuEngine:
                 results.append(GpuExecutionResult(True, "", abi.OK, columns))
         stats = {k: getattr(st, k) for k, _ in abi.vgpu_batch_stats._fields_}
         return results, stats
+
+
+class PreparedBatch:
+    """A vgpu_batch handle (prepared plans); free() or garbage collection releases it."""
+
+    def __init__(self, handle, size: int):
+        self.handle = handle
+        self.size = size
+
+    def free(self):
+        if self.handle:
+            abi.lib().vgpu_batch_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 @dataclass
