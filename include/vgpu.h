@@ -356,6 +356,52 @@ vgpu_status vgpu_batch_template(const char *source, char *out, size_t capacity, 
 /* Drops cached batch graphs and buffers and the in-memory autotuning table. */
 vgpu_status vgpu_batch_clear(void);
 
+/* ---- Serving: admission against a device-memory budget, continuous batching ---------------------
+ * No single reference counterpart: the reference host runs one query at a time
+ * (extension/include/vector_gpu_host.hpp:71-76). A server owns `slots` worker threads, each with
+ * its own CUDA stream. Requests queue on submit and are admitted in arrival order while a slot is
+ * free and their estimated working set (vgpu_estimate_working_set, with the real input sizes) fits
+ * in what the budget has left; admitted requests run concurrently on the device. Queued requests
+ * whose plan has the batch form and shares the head request's template are admitted with it and run
+ * as one batched launch. A request whose estimate exceeds the whole budget completes at once with
+ * VGPU_ERR_OUT_OF_MEMORY. Host inputs must stay valid until vgpu_server_wait reports the request
+ * done; plans are copied at submit. */
+typedef struct vgpu_server_options {
+	int32_t slots;                /* requests running at once (default 4) */
+	int32_t batch_max;            /* most requests in one batched launch; 1 = no batching (default 64) */
+	uint64_t memory_budget_bytes; /* admission budget; 0 = min(120 GiB, the allocator budget) */
+} vgpu_server_options;
+
+typedef struct vgpu_request_info {
+	int32_t status;           /* vgpu_status of the request */
+	int32_t batch_size;       /* requests in the launch that ran it */
+	double queued_ms;         /* submit -> admission */
+	double run_ms;            /* admission -> completion */
+	uint64_t estimated_bytes; /* working-set estimate used for admission */
+	char error[256];
+} vgpu_request_info;
+
+typedef struct vgpu_server_stats {
+	uint64_t submitted, completed, failed, rejected;
+	uint64_t batches, batched_requests;
+	uint64_t in_flight, queued;
+	uint64_t reserved_bytes, peak_reserved_bytes, budget_bytes;
+	uint64_t peak_in_flight;
+} vgpu_server_stats;
+
+typedef struct vgpu_server vgpu_server;
+void vgpu_server_options_init(vgpu_server_options *options);
+vgpu_status vgpu_server_create(const vgpu_server_options *options, vgpu_server **out);
+vgpu_status vgpu_server_submit(vgpu_server *server, const vgpu_plan *plan, const vgpu_column *inputs, size_t n_inputs,
+                               const vgpu_exec_options *options, uint64_t *request_id);
+/* Waits up to timeout_ms (< 0 = no limit). *done = 1 when the request finished: then *result holds
+ * its columns (NULL if it failed; see info->status / info->error) and the id is released. */
+vgpu_status vgpu_server_wait(vgpu_server *server, uint64_t request_id, double timeout_ms, vgpu_result **result,
+                             vgpu_request_info *info, int *done);
+vgpu_status vgpu_server_stats_get(vgpu_server *server, vgpu_server_stats *out);
+/* Finishes the queued and running requests, then stops the workers. */
+void vgpu_server_destroy(vgpu_server *server);
+
 /* ---- Group-by without device allocation ------------------------------------------------------
  * No counterpart in the reference. For callers that cannot call cudaMalloc (a host callback or a
  * graph-driven loop, a process whose device memory another allocator has reserved, a caller holding a

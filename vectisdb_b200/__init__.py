@@ -7,6 +7,7 @@ the reference engine interface (`engine`), the ctypes ABI (`abi`), the synthetic
 from .engine import (  # noqa: F401
     BatchOptions,
     PreparedBatch,
+    Server,
     batch_clear,
     batch_template,
     device_to_host,

@@ -71,6 +71,21 @@ class vgpu_batch_stats(C.Structure):
                 ("tile_rows", C.c_int32), ("smem_slots", C.c_int32)]
 
 
+class vgpu_server_options(C.Structure):
+    _fields_ = [("slots", C.c_int32), ("batch_max", C.c_int32), ("memory_budget_bytes", C.c_uint64)]
+
+
+class vgpu_request_info(C.Structure):
+    _fields_ = [("status", C.c_int32), ("batch_size", C.c_int32), ("queued_ms", C.c_double), ("run_ms", C.c_double),
+                ("estimated_bytes", C.c_uint64), ("error", C.c_char * 256)]
+
+
+class vgpu_server_stats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("submitted", "completed", "failed", "rejected", "batches",
+                                          "batched_requests", "in_flight", "queued", "reserved_bytes",
+                                          "peak_reserved_bytes", "budget_bytes", "peak_in_flight")]
+
+
 class vgpu_device_info(C.Structure):
     _fields_ = [("device", C.c_int32), ("sm_count", C.c_int32), ("cc_major", C.c_int32),
                 ("cc_minor", C.c_int32), ("total_memory", C.c_uint64), ("free_memory", C.c_uint64),
@@ -122,6 +137,14 @@ SIGNATURES = [
     ("vgpu_batch_template", C.c_int, [C.c_char_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t),
                                       C.POINTER(C.c_size_t)]),
     ("vgpu_batch_clear", C.c_int, []),
+    ("vgpu_server_options_init", None, [C.POINTER(vgpu_server_options)]),
+    ("vgpu_server_create", C.c_int, [C.POINTER(vgpu_server_options), C.POINTER(C.c_void_p)]),
+    ("vgpu_server_submit", C.c_int, [C.c_void_p, C.POINTER(vgpu_plan), C.POINTER(vgpu_column), C.c_size_t,
+                                     C.POINTER(vgpu_exec_options), C.POINTER(C.c_uint64)]),
+    ("vgpu_server_wait", C.c_int, [C.c_void_p, C.c_uint64, C.c_double, C.POINTER(C.c_void_p),
+                                   C.POINTER(vgpu_request_info), C.POINTER(C.c_int)]),
+    ("vgpu_server_stats_get", C.c_int, [C.c_void_p, C.POINTER(vgpu_server_stats)]),
+    ("vgpu_server_destroy", None, [C.c_void_p]),
     ("vgpu_copy_to_host", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
     ("vgpu_last_error", C.c_char_p, []),
     ("vgpu_status_string", C.c_char_p, [C.c_int]),

@@ -32,6 +32,7 @@ ENGINE_SOURCES = [
     "kernels.cu",
     "executor.cu",
     "batch.cu",
+    "server.cpp",
     "noalloc.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

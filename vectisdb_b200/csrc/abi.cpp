@@ -13,6 +13,7 @@
 #include "column_cache.hpp"
 #include "cost_model.hpp"
 #include "batch.hpp"
+#include "server.hpp"
 #include "executor.hpp"
 #include "plan.hpp"
 #include "runtime.hpp"
@@ -259,6 +260,113 @@ vgpu_status vgpu_execute_batch(const vgpu_plan *const *plans, const vgpu_column 
 		auto pb = PrepareFromAbi(plans, n_plans);
 		RunPreparedBatch(*pb, inputs, n_inputs, options, batch_options, results, stats);
 	});
+}
+
+struct vgpu_server {
+	std::unique_ptr<Server> server;
+};
+
+void vgpu_server_options_init(vgpu_server_options *options) {
+	if (!options) return;
+	std::memset(options, 0, sizeof(*options));
+	options->slots = 4;
+	options->batch_max = 64;
+}
+
+vgpu_status vgpu_server_create(const vgpu_server_options *options, vgpu_server **out) {
+	return Guard([&] {
+		if (!out) Fail(VGPU_ERR_INVALID_ARGUMENT, "null server pointer");
+		*out = nullptr;
+		ServerOptions so;
+		if (options) {
+			so.slots = options->slots;
+			so.batch_max = options->batch_max;
+			so.memory_budget = options->memory_budget_bytes;
+		}
+		auto *s = new vgpu_server();
+		try {
+			s->server.reset(new Server(so));
+		} catch (...) {
+			delete s;
+			throw;
+		}
+		*out = s;
+	});
+}
+
+vgpu_status vgpu_server_submit(vgpu_server *server, const vgpu_plan *plan, const vgpu_column *inputs, size_t n_inputs,
+                               const vgpu_exec_options *options, uint64_t *request_id) {
+	return Guard([&] {
+		if (!server || !request_id) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		if (n_inputs > 0 && inputs == nullptr) Fail(VGPU_ERR_INVALID_ARGUMENT, "null inputs with nonzero count");
+		ExecOptions eo;
+		if (options) {
+			eo.serve_whole_scan_from_cache = options->serve_whole_scan_from_cache != 0;
+			eo.cache_chunk_index = options->cache_chunk_index;
+			eo.output_on_device = options->output_memory == VGPU_MEM_DEVICE;
+			if (options->stage_scan_to_cache) Fail(VGPU_ERR_UNSUPPORTED, "serving does not stage scans to the cache");
+			if (eo.serve_whole_scan_from_cache && eo.cache_chunk_index >= 0) {
+				Fail(VGPU_ERR_INVALID_ARGUMENT, "serve_whole_scan_from_cache and cache_chunk_index are exclusive");
+			}
+		}
+		std::vector<vgpu_column> in(inputs, inputs + n_inputs);
+		*request_id = server->server->Submit(ConvertPlan(plan), std::move(in), eo);
+	});
+}
+
+vgpu_status vgpu_server_wait(vgpu_server *server, uint64_t request_id, double timeout_ms, vgpu_result **result,
+                             vgpu_request_info *info, int *done) {
+	return Guard([&] {
+		if (!server || !done) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		*done = 0;
+		if (result) *result = nullptr;
+		ExecResult r;
+		RequestInfo ri;
+		if (!server->server->Wait(request_id, timeout_ms, &r, &ri)) return;
+		*done = 1;
+		if (info) {
+			std::memset(info, 0, sizeof(*info));
+			info->status = ri.status;
+			info->batch_size = static_cast<int32_t>(ri.batch_size);
+			info->queued_ms = ri.queued_ms;
+			info->run_ms = ri.run_ms;
+			info->estimated_bytes = ri.estimated_bytes;
+			std::snprintf(info->error, sizeof(info->error), "%s", ri.error.c_str());
+		}
+		if (ri.status == VGPU_OK && result) {
+			auto *res = new vgpu_result();
+			res->exec = std::move(r);
+			*result = res;
+		} else {
+			for (void *p : r.device_buffers) Runtime::Get().allocator().Free(p, r.stream);
+		}
+	});
+}
+
+vgpu_status vgpu_server_stats_get(vgpu_server *server, vgpu_server_stats *out) {
+	return Guard([&] {
+		if (!server || !out) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		ServerStats s = server->server->Stats();
+		out->submitted = s.submitted;
+		out->completed = s.completed;
+		out->failed = s.failed;
+		out->rejected = s.rejected;
+		out->batches = s.batches;
+		out->batched_requests = s.batched_requests;
+		out->in_flight = s.in_flight;
+		out->queued = s.queued;
+		out->reserved_bytes = s.reserved_bytes;
+		out->peak_reserved_bytes = s.peak_reserved_bytes;
+		out->budget_bytes = s.budget_bytes;
+		out->peak_in_flight = s.peak_in_flight;
+	});
+}
+
+void vgpu_server_destroy(vgpu_server *server) {
+	try {
+		delete server;
+	} catch (...) {
+	}
 }
 
 vgpu_status vgpu_batch_template(const char *source, char *out, size_t capacity, size_t *length, size_t *n_params) {

@@ -337,23 +337,23 @@ bool RunTemplate(const std::vector<Prepared *> &qs, const ExecOptions &options, 
 	// Query table rows, largest queries first in the tile queue.
 	const uint64_t kMaxBits = 22;
 	std::vector<size_t> order;
-	std::vector<uint64_t> qtab_host;
-	std::vector<uint64_t> dom(qs.size(), 0), bits_total(qs.size(), 0);
+	std::vector<uint64_t> dom(qs.size(), 0);
+	std::vector<Prepared *> fitting;
 	for (size_t qi = 0; qi < qs.size(); qi++) {
 		uint64_t b = 0;
 		for (int j = 0; j < nkeys; j++) {
 			const auto &r = ranges[qi][j];
-			if (r.first > r.second) {  // no rows
-				b += 0;
-				continue;
-			}
+			if (r.first > r.second) continue;  // no rows
 			b += BitsFor(static_cast<uint64_t>(r.second) - static_cast<uint64_t>(r.first));
 		}
-		if (b > kMaxBits) return false;  // a key space this wide belongs to the partitioned single-query path
-		bits_total[qi] = b;
-		dom[qi] = 1ull << b;
+		dom[qi] = 1ull << std::min<uint64_t>(b, 63);
+		if (b <= kMaxBits) fitting.push_back(qs[qi]);
 		order.push_back(qi);
 	}
+	// A key space wider than the batch accumulators take belongs to the partitioned single-query
+	// path: such queries leave the batch (they run alone afterwards) and the rest stay together.
+	if (fitting.empty()) return false;
+	if (fitting.size() != qs.size()) return RunTemplate(fitting, options, bopts, stream, results, stats);
 	std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return qs[a]->rows > qs[b]->rows; });
 
 	Geometry4 geo;
@@ -870,7 +870,8 @@ std::vector<ExecResult> ExecutePrepared(const PreparedBatch &pb, const std::vect
 	std::vector<bool> done(nplans, false);
 	for (auto &kv : groups) {
 		if (RunTemplate(kv.second, options, bopts, stream, results, stats)) {
-			for (auto *p : kv.second) done[p->index] = true;
+			// batched queries always carry their key and aggregate columns; the rest run alone below
+			for (auto *p : kv.second) done[p->index] = !results[p->index].columns.empty();
 		}
 	}
 	VGPU_CUDA(cudaStreamSynchronize(stream));

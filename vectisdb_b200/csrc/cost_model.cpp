@@ -85,7 +85,8 @@ struct Walker {
 				if (a.kind != AggKind::COUNT && a.kind != AggKind::COUNT_STAR) carried += 8;
 			}
 			uint64_t bytes = SatAdd(SatMul(c.rows, carried), SatMul(c.rows, out_width));
-			bytes = SatAdd(bytes, 16384ull * 2048 * 4); // partition offsets upper bound
+			// partition offsets: (partitions <= 2^14, about one per 1024 rows) x (CTAs <= 2048) x 4 B
+			bytes = SatAdd(bytes, SatMul(std::min<uint64_t>(16384, std::max<uint64_t>(1, c.rows / 1024)), 2048ull * 4));
 			e.rows = n.estimated_rows ? n.estimated_rows : c.rows;
 			e.width = out_width;
 			Charge("GROUP_BY_AGGREGATE", bytes);

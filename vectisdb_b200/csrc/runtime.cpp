@@ -262,6 +262,7 @@ std::vector<char> CompileToCubin(const std::string &source, const std::string &a
 // ModuleCache
 
 CUfunction Module::Get(const std::string &name) {
+	std::lock_guard<std::mutex> lock(mu);
 	auto it = functions.find(name);
 	if (it != functions.end()) {
 		return it->second;

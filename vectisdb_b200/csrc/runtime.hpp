@@ -86,7 +86,8 @@ private:
 // ---- Compiled modules ----------------------------------------------------------------------------
 struct Module {
 	CUmodule module = nullptr;
-	std::unordered_map<std::string, CUfunction> functions;
+	std::unordered_map<std::string, CUfunction> functions;  // guarded by mu (modules are shared across threads)
+	std::mutex mu;
 	size_t cubin_bytes = 0;
 	CUfunction Get(const std::string &name);
 };

@@ -472,6 +472,72 @@ class PreparedBatch:
             pass
 
 
+class Server:
+    """Serving (vgpu_server_*): admission against a device-memory budget, `slots` requests running
+    concurrently on their own streams, same-template group-by requests batched together."""
+
+    def __init__(self, slots: int = 4, batch_max: int = 64, memory_budget_bytes: int = 0):
+        L = abi.lib()
+        o = abi.vgpu_server_options()
+        L.vgpu_server_options_init(C.byref(o))
+        o.slots, o.batch_max, o.memory_budget_bytes = slots, batch_max, memory_budget_bytes
+        self._h = C.c_void_p()
+        abi.check(L.vgpu_server_create(C.byref(o), C.byref(self._h)))
+        self._keep = {}  # request id -> objects the request's host inputs live in
+
+    def submit(self, plan: GpuPlanNode, inputs: Sequence[GpuColumn], options: ExecuteOptions | None = None) -> int:
+        keep = _Keep()
+        plan_c = serialize_plan(plan, keep)
+        cols = serialize_inputs(inputs, keep)
+        opts = abi.vgpu_exec_options()
+        abi.lib().vgpu_exec_options_init(C.byref(opts))
+        o = options or ExecuteOptions()
+        opts.serve_whole_scan_from_cache = int(o.serve_whole_scan_from_cache)
+        opts.output_memory = abi.MEM_DEVICE if o.output_on_device else abi.MEM_HOST
+        rid = C.c_uint64()
+        abi.check(abi.lib().vgpu_server_submit(self._h, C.byref(plan_c), cols, len(inputs), C.byref(opts),
+                                               C.byref(rid)))
+        self._keep[rid.value] = (keep, cols, list(inputs), o.output_on_device)
+        return rid.value
+
+    def wait(self, request_id: int, timeout_ms: float = -1.0):
+        """(result or None if it failed / None on timeout, info dict or None on timeout)."""
+        h = C.c_void_p()
+        info = abi.vgpu_request_info()
+        done = C.c_int()
+        abi.check(abi.lib().vgpu_server_wait(self._h, request_id, timeout_ms, C.byref(h), C.byref(info),
+                                             C.byref(done)))
+        if not done.value:
+            return None, None
+        on_device = self._keep.pop(request_id, (None, None, None, False))[3]
+        d = {"status": info.status, "batch_size": info.batch_size, "queued_ms": info.queued_ms,
+             "run_ms": info.run_ms, "estimated_bytes": info.estimated_bytes, "error": info.error.decode()}
+        if not h.value:
+            return None, d
+        columns = _read_result(h)
+        if on_device:
+            return DeviceResult(h, columns), d
+        abi.lib().vgpu_result_free(h)
+        return GpuExecutionResult(True, "", abi.OK, columns), d
+
+    def stats(self) -> dict:
+        st = abi.vgpu_server_stats()
+        abi.check(abi.lib().vgpu_server_stats_get(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in abi.vgpu_server_stats._fields_}
+
+    def close(self):
+        if self._h:
+            abi.lib().vgpu_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 @dataclass
 class BatchOptions:
     """vgpu_batch_options: 0 = tuned or default."""
