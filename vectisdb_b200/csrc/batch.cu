@@ -169,7 +169,9 @@ struct BatchEntry {
 	uint64_t *qtab = nullptr, *acc = nullptr, *counts = nullptr, *outp = nullptr;
 	uint32_t *work = nullptr;
 	void *tiles = nullptr;
-	uint64_t *counts_host = nullptr, *outp_host = nullptr;  // pinned
+	uint64_t *counts_host = nullptr, *outp_host = nullptr;  // pinned (cached entries) or into host_stage
+	std::vector<uint64_t> host_stage;                        // transient entries
+	bool pinned = true;
 	cudaGraphExec_t graph = nullptr;
 	bool initialized = false;
 	uint64_t nq = 0, ntiles = 0, acc_words = 0, out_rows = 0, in_bytes = 0, rows = 0;
@@ -187,8 +189,8 @@ struct BatchEntry {
 		                static_cast<void *>(outp), static_cast<void *>(work), tiles}) {
 			if (p) al.Free(p, stream);
 		}
-		if (counts_host) cudaFreeHost(counts_host);
-		if (outp_host) cudaFreeHost(outp_host);
+		if (pinned && counts_host) cudaFreeHost(counts_host);
+		if (pinned && outp_host) cudaFreeHost(outp_host);
 		qtab = acc = counts = outp = nullptr;
 		work = nullptr;
 		tiles = nullptr;
@@ -431,9 +433,15 @@ bool RunTemplate(const std::vector<Prepared *> &qs, const ExecOptions &options, 
 			}
 			ntiles += t;
 		}
-		std::string key = q0.sig + "#" + g.ToString() + "#" +
-		                  Sha256Hex(qt.data(), qt.size() * 8) + Sha256Hex(tl.data(), tl.size() * 4);
-		if (auto e = Cache().Find(key)) return e;
+		// Without a graph to replay (a composition that changes from call to call, as in serving) the
+		// entry is transient: no cache lookup, no pinned staging, freed when the call ends.
+		const bool transient = !bopts.use_graph && !bopts.autotune;
+		std::string key = transient ? std::string()
+		                            : q0.sig + "#" + g.ToString() + "#" + Sha256Hex(qt.data(), qt.size() * 8) +
+		                                  Sha256Hex(tl.data(), tl.size() * 4);
+		if (!transient) {
+			if (auto e = Cache().Find(key)) return e;
+		}
 		auto e = std::make_shared<BatchEntry>();
 		e->key = key;
 		e->geo = g;
@@ -462,12 +470,19 @@ bool RunTemplate(const std::vector<Prepared *> &qs, const ExecOptions &options, 
 		e->counts = static_cast<uint64_t *>(al.Alloc(qs.size() * 8, stream));
 		e->outp = static_cast<uint64_t *>(al.Alloc(out_words * 8, stream));
 		e->work = static_cast<uint32_t *>(al.Alloc(16, stream));
-		VGPU_CUDA(cudaMallocHost(&e->counts_host, qs.size() * 8));
-		VGPU_CUDA(cudaMallocHost(&e->outp_host, out_words * 8));
+		if (transient) {
+			e->pinned = false;
+			e->host_stage.assign(qs.size() + out_words, 0);
+			e->counts_host = e->host_stage.data();
+			e->outp_host = e->host_stage.data() + qs.size();
+		} else {
+			VGPU_CUDA(cudaMallocHost(&e->counts_host, qs.size() * 8));
+			VGPU_CUDA(cudaMallocHost(&e->outp_host, out_words * 8));
+		}
 		VGPU_CUDA(cudaMemcpyAsync(e->qtab, qt.data(), qt.size() * 8, cudaMemcpyHostToDevice, stream));
 		if (!tl.empty()) VGPU_CUDA(cudaMemcpyAsync(e->tiles, tl.data(), tl.size() * 4, cudaMemcpyHostToDevice, stream));
 		VGPU_CUDA(cudaStreamSynchronize(stream));  // host staging vectors go out of scope
-		Cache().Insert(e, stream);
+		if (!transient) Cache().Insert(e, stream);
 		return e;
 	};
 
@@ -638,6 +653,7 @@ bool RunTemplate(const std::vector<Prepared *> &qs, const ExecOptions &options, 
 		if (options.output_on_device) r.keepalive.push_back(holder);
 		results[qs[qi]->index] = std::move(r);
 	}
+	if (!e.pinned) e.Release(stream);  // transient: every copy out of it has completed
 	if (stats) {
 		stats->batched += qs.size();
 		stats->templates++;

@@ -617,9 +617,10 @@ std::string FinalizeCode(const PipelineCodegen::GroupBySpec &gb, const std::vect
 	for (auto &k : gb.keys) {
 		const auto &col = visible[k.column];
 		const char *t = CudaTypeName(col.type);
-		uint64_t mask = k.bits >= 64 ? ~0ull : ((1ull << k.bits) - 1);
-		o << "\t\t\t((" << t << "*)" << out_array << "[" << w << "])[" << pos << "] = (" << t << ")((i64)((" << key << " >> " << k.shift
-		  << ") & 0x" << std::hex << mask << std::dec << "ull) + (" << k.min << "LL));\n";
+		const int j = static_cast<int>(&k - gb.keys.data());
+		o << "\t\t\t((" << t << "*)" << out_array << "[" << w << "])[" << pos << "] = (" << t << ")((i64)((" << key
+		  << " >> (u32)a.w[" << kKeyWord + 3 * j + 1 << "]) & a.w[" << kKeyWord + 3 * j + 2 << "]) + (i64)a.w["
+		  << kKeyWord + 3 * j << "]);\n";
 		w++;
 	}
 	const std::string cnt = tab + "0[" + s + "]";
@@ -734,7 +735,9 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 	std::ostringstream pack;
 	pack << "(0ull";
 	for (auto &k : gb.keys) {
-		pack << " | ((u64)((i64)(" << visible_[k.column].value << ") - (" << k.min << "LL)) << " << k.shift << ")";
+		const int j = static_cast<int>(&k - gb.keys.data());
+		pack << " | ((u64)((i64)(" << visible_[k.column].value << ") - (i64)a.w[" << kKeyWord + 3 * j << "]) << (u32)a.w["
+		     << kKeyWord + 3 * j + 1 << "])";
 	}
 	pack << ")";
 	auto value_of = [&](int agg_index, bool from_partition) -> std::string {
@@ -849,15 +852,15 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 	// whose low direct_bits are the table slot (direct-partitioned strategy; the record then carries the
 	// mixed key).
 	const bool dpart = gb.direct_bits > 0;
-	const std::string part_of_pack = dpart ? "(u32)(vgpu_dmix(" + pack.str() + ") >> " + std::to_string(gb.direct_bits) + ")"
+	const std::string part_of_pack = dpart ? "(u32)(vgpu_dmix(a, " + pack.str() + ") >> " + std::to_string(gb.direct_bits) + ")"
 	                                       : "partition_of(" + pack.str() + ", pbits)";
-	const std::string key_of_pack = dpart ? "vgpu_dmix(" + pack.str() + ")" : pack.str();
+	const std::string key_of_pack = dpart ? "vgpu_dmix(a, " + pack.str() + ")" : pack.str();
 	if (dpart) {
-		const uint64_t mask = gb.key_bits >= 64 ? ~0ull : ((1ull << gb.key_bits) - 1);
-		o << "__device__ __forceinline__ u64 vgpu_dmix(u64 k) { return (k * 0x" << std::hex << gb.key_mult << "ull) & 0x"
-		  << mask << "ull; }\n"
-		  << "__device__ __forceinline__ u64 vgpu_dunmix(u64 k) { return (k * 0x" << gb.key_mult_inv << "ull) & 0x" << mask
-		  << std::dec << "ull; }\n\n";
+		// multiplier, inverse and key mask come with the arguments, so the kernel does not depend on the data
+		o << "__device__ __forceinline__ u64 vgpu_dmix(const KArgs &a, u64 k) { return (k * a.w[" << kMixWord
+		  << "]) & a.w[" << kMixWord + 2 << "]; }\n"
+		  << "__device__ __forceinline__ u64 vgpu_dunmix(const KArgs &a, u64 k) { return (k * a.w[" << kMixWord + 1
+		  << "]) & a.w[" << kMixWord + 2 << "]; }\n\n";
 	}
 	// part_count / part_scatter args: cb+0 = P, cb+1 = pbits, cb+2 = tiles per CTA,
 	//   cb+3 = counts/offsets (u32, [p * G + cta]), cb+4 = records out.
@@ -1099,7 +1102,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			  << "\t\tconst u32 live_mask = __ballot_sync(0xffffffffu, lv);\n"
 			  << "\t\tif (lv) {\n" << sdecl.str() << load
 			  << "\t\t\tconst u64 pos = run + __popc(live_mask & ((1u << lane) - 1u));\n"
-			  << "\t\t\tconst u64 key = vgpu_dunmix(((u64)p << " << dbits << ") | s);\n"
+			  << "\t\t\tconst u64 key = vgpu_dunmix(a, ((u64)p << " << dbits << ") | s);\n"
 			  << FinalizeCode(gb, fields, visible_, "S", "0", "key", "pos", OUTD) << reset << "\t\t}\n"
 			  << "\t\trun += __popc(live_mask);\n\t}\n\t__syncthreads();\n\t}\n";
 			return r.str();

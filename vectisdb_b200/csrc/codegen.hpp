@@ -50,6 +50,14 @@ struct Geometry {
 	}
 };
 
+// Reserved KArgs words of the group-by kernels: the data-dependent key packing travels as arguments
+// so one compiled kernel serves every instance of a plan shape. Key j: [kKeyWord + 3j] minimum,
+// [+1] shift, [+2] mask (up to kMaxPackedKeys keys); the direct-partitioned mix: [kMixWord] odd
+// multiplier, [+1] its inverse, [+2] key mask. Ordinary arguments stay below kKeyWord.
+constexpr int kKeyWord = 96;
+constexpr int kMaxPackedKeys = 8;
+constexpr int kMixWord = 120;
+
 // KArgs word layout shared by every pipeline kernel:
 //   w[0] = rows (pairs n*m for CROSS), w[1] = right rows m (CROSS) else 0,
 //   w[2 + 2*i] = source i data pointer, w[3 + 2*i] = source i byte-validity pointer (or 0),

@@ -33,7 +33,11 @@ struct KArgsHost {
 		std::memset(w, 0, sizeof(w));
 	}
 	void Set(int i, uint64_t v) {
-		if (i >= 128) Fail(VGPU_ERR_UNSUPPORTED, "generated kernel needs more than 128 argument words");
+		if (i >= kKeyWord) Fail(VGPU_ERR_UNSUPPORTED, "generated kernel needs more than 96 argument words");
+		SetWord(i, v);
+	}
+	//! Reserved words (key packing, diagnostics) at or above kKeyWord.
+	void SetWord(int i, uint64_t v) {
 		w[i] = v;
 		used = std::max(used, i + 1);
 	}
@@ -48,6 +52,24 @@ void LaunchGenerated(Module &m, const char *name, dim3 grid, dim3 block, size_t 
 	LaunchScope scope(name, stream, bytes, rows);
 	void *params[] = {args.w};
 	Runtime::Get().LaunchModuleKernel(f, grid, block, smem, stream, params);
+}
+
+// Key packing of a group-by into its kernels' reserved argument words (see kKeyWord).
+void SetKeyWords(KArgsHost &k, const PipelineCodegen::GroupBySpec &gb) {
+	if (gb.keys.size() > static_cast<size_t>(kMaxPackedKeys)) {
+		Fail(VGPU_ERR_UNSUPPORTED, "gpu_groupby: more than 8 group keys");
+	}
+	for (size_t j = 0; j < gb.keys.size(); j++) {
+		const auto &key = gb.keys[j];
+		k.SetWord(kKeyWord + 3 * static_cast<int>(j), static_cast<uint64_t>(key.min));
+		k.SetWord(kKeyWord + 3 * static_cast<int>(j) + 1, static_cast<uint64_t>(key.shift));
+		k.SetWord(kKeyWord + 3 * static_cast<int>(j) + 2, key.bits >= 64 ? ~0ull : ((1ull << key.bits) - 1));
+	}
+	if (gb.direct_bits > 0) {
+		k.SetWord(kMixWord, gb.key_mult);
+		k.SetWord(kMixWord + 1, gb.key_mult_inv);
+		k.SetWord(kMixWord + 2, gb.key_bits >= 64 ? ~0ull : ((1ull << gb.key_bits) - 1));
+	}
 }
 
 int BitsFor(uint64_t range) {
@@ -618,6 +640,7 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		uint64_t *count = arena_.AllocT<uint64_t>(1);
 		KArgsHost a;
 		FillArgs(pin, a);
+		SetKeyWords(a, gb);
 		a.Set(cb, domain);
 		for (int f = 0; f < F; f++) a.SetPtr(cb + 1 + f, fields + domain * f);
 		for (int w = 0; w < out_words; w++) a.SetPtr(cb + 1 + F + w, out[w].data);
@@ -666,7 +689,9 @@ Relation Executor::GroupBy(const PlanNode &node) {
 			if (std::strcmp(env, "direct") == 0) dpart = shift <= dbits_max + 14;
 		}
 		if (dpart) {
-			int dbits = std::min(dbits_max, std::max(shift, 5));
+			// the table size depends on the plan shape only (slot bytes), not on the data, so every
+			// instance of a query shape reuses one compiled kernel
+			int dbits = dbits_max;
 			if (const char *env = std::getenv("VGPU_GB_DIRECT_BITS")) {  // tuning override
 				dbits = std::min(dbits_max, std::max(5, std::atoi(env)));
 			}
@@ -716,6 +741,7 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		const uint64_t RS = static_cast<uint64_t>(cg.RecordStride(gb));
 		KArgsHost a;
 		FillArgs(pin, a);
+		SetKeyWords(a, gb);
 		a.Set(cb, P);
 		a.Set(cb + 1, static_cast<uint64_t>(pbits));
 		a.Set(cb + 2, tpc);
@@ -740,6 +766,7 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		VGPU_CUDA(cudaMemsetAsync(out_count, 0, 8, stream_));
 		KArgsHost b;
 		FillArgs(pin, b);
+		SetKeyWords(b, gb);
 		b.Set(cb, P);
 		b.Set(cb + 1, C);
 		b.SetPtr(cb + 2, offsets);
@@ -762,7 +789,7 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		if (debug_path) {
 			debug = arena_.AllocT<uint64_t>(P * 8);
 			VGPU_CUDA(cudaMemsetAsync(debug, 0, P * 64, stream_));
-			b.SetPtr(127, debug);
+			b.SetWord(127, reinterpret_cast<uint64_t>(debug));
 		}
 		{
 			const size_t smem1 = static_cast<size_t>(slot_bytes * C);
@@ -878,6 +905,7 @@ uint64_t Executor::DirectBuckets(Module &module, const PipelineCodegen::GroupByS
 	const int cb = 2 + 2 * static_cast<int>(pin.sources.size());  // first consumer argument word
 	KArgsHost b;
 	FillArgs(pin, b);
+	SetKeyWords(b, gb);
 	b.SetPtr(cb, items);
 	b.SetPtr(cb + 1, control);
 	b.SetPtr(cb + 2, records);

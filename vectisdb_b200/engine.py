@@ -706,6 +706,20 @@ class ColumnCache:
         return int(abi.lib().vgpu_cache_table_generation(C.byref(_table(table, keep))))
 
     @staticmethod
+    def device_column(table: GpuTableRef, name: str, rows: int = 0) -> GpuColumn:
+        """A cache-resident column as a device input (borrowed; valid while the entry stays cached),
+        optionally its first `rows` rows."""
+        keep = _Keep()
+        c = abi.vgpu_column()
+        found = C.c_int()
+        abi.check(abi.lib().vgpu_cache_try_get_chunk(C.byref(_table(table, keep)), name.encode(), 0, C.byref(c),
+                                                     C.byref(found)))
+        if not found.value:
+            raise KeyError(f"{name} of {table} is not cache-resident")
+        n = int(c.row_count) if not rows else min(int(rows), int(c.row_count))
+        return GpuColumn(name, GpuValueType(c.type), None, None, n, int(c.data))
+
+    @staticmethod
     def put_table(table: GpuTableRef, columns: Sequence[GpuColumn]) -> None:
         """Stages every column as one chunk and commits (convenience for resident base tables)."""
         ColumnCache.begin_staging(table)
