@@ -224,6 +224,15 @@ void PipelineCodegen::Resolve() {
 	}
 	chain_sources_.assign(spec_.sources.size(), false);
 	std::ostringstream code;
+	if (spec_.join) {
+		// left rows without a match in the right side are not join output rows
+		if (spec_.join_key < 0 || spec_.join_key >= static_cast<int>(spec_.sources.size())) {
+			Fail(VGPU_ERR_INTERNAL, "join pipeline without a key source");
+		}
+		code << "\t\tkeep = keep && (jm[r] >= 0);\n";
+		chain_sources_[spec_.join_key] = true;
+		has_filter_ = true;
+	}
 	// Sources read by each visible column (transitively through projections).
 	std::vector<std::set<int>> deps(cols.size());
 	for (size_t i = 0; i < cols.size(); i++) {
@@ -362,6 +371,14 @@ std::string PipelineCodegen::LoadBlock(const Geometry &g, const std::vector<bool
 			if (src.nullable) {
 				o << "\t\tload_valid<" << g.items << ">((const u8*)a.w[" << w + 1 << "], row0, n, sv" << i << ");\n";
 			}
+		} else if (spec_.join) {
+			if (src.side == 0) {
+				o << "\t\tload_rows<" << t << ", " << g.items << ">((const " << t << "*)a.w[" << w << "], row0, n, s" << i
+				  << ");\n";
+				if (src.nullable) {
+					o << "\t\tload_valid<" << g.items << ">((const u8*)a.w[" << w + 1 << "], row0, n, sv" << i << ");\n";
+				}
+			}
 		} else {
 			const char *idx = src.side == 0 ? "li[r]" : "rj[r]";
 			o << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) {\n";
@@ -372,6 +389,30 @@ std::string PipelineCodegen::LoadBlock(const Geometry &g, const std::vector<bool
 				  << "] != 0) : false;\n";
 			}
 			o << "\t\t}\n";
+		}
+	}
+	if (spec_.join) {
+		// each item's match in the sorted right side, then the right columns at that position
+		const int key = spec_.join_key;
+		// keys widen by zero extension of their width, as the sorted side was widened
+		const size_t kw = TypeSize(spec_.sources[key].type);
+		const char *ut = kw == 1 ? "u8" : kw == 2 ? "unsigned short" : kw == 4 ? "u32" : "u64";
+		o << "\t\tlong long jm[" << g.items << "];\n"
+		  << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) {\n"
+		  << "\t\t\tjm[r] = row0 + r < n ? vgpu_join_find((u64)(" << ut << ")s" << key << "[r] - a.w[" << kJoinWord + 2
+		  << "], (const u64*)a.w[" << kJoinWord << "], (const u32*)a.w[" << kJoinWord + 1 << "], a.w[" << kJoinWord + 3
+		  << "] >> 8, (u32)(a.w[" << kJoinWord + 3 << "] & 0xffu)) : -1ll;\n\t\t}\n";
+		for (size_t i = 0; i < spec_.sources.size(); i++) {
+			const auto &src = spec_.sources[i];
+			if (!needed[i] || src.side != 1) continue;
+			const char *t = CudaTypeName(src.type);
+			const int w = 2 + 2 * static_cast<int>(i);
+			o << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) s" << i << "[r] = jm[r] >= 0 ? ((const "
+			  << t << "*)a.w[" << w << "])[jm[r]] : (" << t << ")0;\n";
+			if (src.nullable) {
+				o << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) sv" << i
+				  << "[r] = jm[r] >= 0 ? (((const u8*)a.w[" << w + 1 << "])[jm[r]] != 0) : false;\n";
+			}
 		}
 	}
 	return o.str();

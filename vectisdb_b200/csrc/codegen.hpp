@@ -29,6 +29,11 @@ struct SourceColumn {
 struct PipelineSpec {
 	std::vector<SourceColumn> sources;
 	bool cross = false;
+	// Equi-join source: row r is left row r; side-1 sources are the sorted right side's columns, read at
+	// the position of the left key's match (source join_key) in the unique sorted right keys; rows
+	// without a match are filtered out.
+	bool join = false;
+	int join_key = -1;
 	std::vector<const PlanNode *> chain; // FILTER / PROJECTION nodes, bottom-up
 };
 
@@ -57,6 +62,9 @@ struct Geometry {
 constexpr int kKeyWord = 96;
 constexpr int kMaxPackedKeys = 8;
 constexpr int kMixWord = 120;
+// Join-source words: [kJoinWord] sorted right keys (u64, biased), [+1] radix directory (u32),
+// [+2] bias (the right minimum), [+3] shift | bucket count << 8.
+constexpr int kJoinWord = 123;
 
 // KArgs word layout shared by every pipeline kernel:
 //   w[0] = rows (pairs n*m for CROSS), w[1] = right rows m (CROSS) else 0,

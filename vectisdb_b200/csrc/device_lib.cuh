@@ -261,6 +261,33 @@ __device__ __forceinline__ void atomic_min_i64(i64 *p, i64 v) { atomicMin(reinte
 __device__ __forceinline__ void atomic_max_i64(i64 *p, i64 v) { atomicMax(reinterpret_cast<long long *>(p), (long long)v); }
 
 // ---------------------------------------------------------------------------------------------
+// Equi-join lookup into a sorted unique key array through a radix directory: dir[b] is the first
+// position whose key >> shift >= b (dir[nb] = n), so a probe key's candidates are one bucket, which
+// a short binary search finishes. Keys are biased by the sorted side's minimum (u64 arithmetic);
+// a probe key below that minimum wraps to a bucket past nb and misses. Returns the position or -1.
+// shift == 0xff selects the dense form: dir is a position table over the whole key range
+// (dir[k] = position of key k, or 0xffffffff), nb its length.
+__device__ __forceinline__ long long vgpu_join_find(u64 k, const u64 *__restrict__ sorted, const u32 *__restrict__ dir,
+                                                    u64 nb, u32 shift) {
+	if (shift == 0xffu) {
+		if (k >= nb) return -1ll;
+		const u32 p = dir[k];
+		return p == 0xffffffffu ? -1ll : (long long)p;
+	}
+	const u64 b = k >> shift;
+	if (b >= nb) return -1ll;
+	u32 lo = dir[b];
+	const u32 end = dir[b + 1];
+	u32 hi = end;
+	while (lo < hi) {
+		const u32 mid = (lo + hi) >> 1;
+		if (sorted[mid] < k) lo = mid + 1;
+		else hi = mid;
+	}
+	return (lo < end && sorted[lo] == k) ? (long long)lo : -1ll;
+}
+
+// ---------------------------------------------------------------------------------------------
 // Hashing of packed group keys
 
 __device__ __forceinline__ u64 mix64(u64 k) {

@@ -110,6 +110,7 @@ private:
 		std::vector<DevColumn> sources; // parallel to spec.sources
 		uint64_t rows = 0;              // pairs for CROSS
 		uint64_t right_rows = 0;
+		uint64_t join_words[4] = {0, 0, 0, 0};  // join source: sorted keys, directory, bias, shift | nb << 8
 	};
 
 	Relation Scan(const PlanNode &node);
@@ -118,6 +119,8 @@ private:
 	Relation RunChain(const PlanNode &node);
 	Relation GroupBy(const PlanNode &node);
 	Relation Join(const PlanNode &node);
+	Relation JoinMaterialize(const PlanNode &node, Relation &left, Relation &right);
+	Relation JoinForPipeline(const PlanNode &node, PipelineInput &pin, bool *fused);
 	Relation CrossProduct(const PlanNode &node);
 	void ComputeStats(PipelineInput &pin, PipelineCodegen &cg, const std::vector<int> &cols,
 	                  std::vector<std::pair<int64_t, int64_t>> &out);
@@ -226,6 +229,9 @@ Relation Executor::Scan(const PlanNode &node) {
 void Executor::FillArgs(const PipelineInput &pin, KArgsHost &args) {
 	args.Set(0, pin.rows);
 	args.Set(1, pin.right_rows);
+	if (pin.spec.join) {
+		for (int i = 0; i < 4; i++) args.SetWord(kJoinWord + i, pin.join_words[i]);
+	}
 	for (size_t i = 0; i < pin.sources.size(); i++) {
 		args.SetPtr(2 + 2 * static_cast<int>(i), pin.sources[i].data);
 		args.SetPtr(3 + 2 * static_cast<int>(i), pin.sources[i].valid);
@@ -288,7 +294,14 @@ Executor::PipelineInput Executor::BuildPipeline(const PlanNode &top, std::vector
 		}
 		return pin;
 	}
-	Relation rel = top.op == OpType::SCAN ? Scan(top) : Exec(top);
+	Relation rel;
+	if (top.op == OpType::HASH_JOIN) {
+		bool fused = false;
+		rel = JoinForPipeline(top, pin, &fused);
+		if (fused) return pin;
+	} else {
+		rel = top.op == OpType::SCAN ? Scan(top) : Exec(top);
+	}
 	uint64_t rows = rel.empty() ? 0 : rel.front().rows;
 	for (auto &c : rel) {
 		if (c.rows != rows) {
@@ -938,6 +951,131 @@ Relation Executor::Join(const PlanNode &node) {
 	}
 	Relation left = Exec(*node.children[0]);
 	Relation right = Exec(*node.children[1]);
+	return JoinMaterialize(node, left, right);
+}
+
+// A join under a pipeline (filter, projection or group-by above it). When the right side's keys are
+// unique -- every left row has at most one match, the common key/foreign-key case -- the join is a
+// virtual source of the pipeline: left row r is output row r, its right columns are read at its
+// match in the sorted right side (a radix directory over the sorted keys, then a short binary search;
+// right columns gathered into sorted order once), and rows without a match are filtered out. The
+// match pairs are never materialized. Otherwise the join output is materialized as usual.
+Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, bool *fused) {
+	*fused = false;
+	if (node.children.size() != 2) {
+		Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: HASH_JOIN expects exactly two children");
+	}
+	if (node.build_keys.size() != 1 || node.probe_keys.size() != 1) {
+		Fail(VGPU_ERR_UNSUPPORTED, "gpu_hash_join: this GPU path joins on exactly one equality key column");
+	}
+	if (node.output_columns.empty()) {
+		Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_hash_join: node has no output columns");
+	}
+	Relation left = Exec(*node.children[0]);
+	Relation right = Exec(*node.children[1]);
+	const DevColumn *lk = nullptr, *rk = nullptr;
+	for (auto &c : left) if (c.name == node.build_keys[0]) { lk = &c; break; }
+	for (auto &c : right) if (c.name == node.probe_keys[0]) { rk = &c; break; }
+	const char *env = std::getenv("VGPU_JOIN_FUSED");  // "0": always materialize (testing)
+	const bool allowed = !(env && std::strcmp(env, "0") == 0);
+	if (!allowed || !lk || !rk || lk->type != rk->type || !IsIntegerKeyType(lk->type) || lk->rows == 0 ||
+	    rk->rows == 0 || lk->rows >= (1ull << 32) || rk->rows >= (1ull << 32) || rk->valid || lk->valid) {
+		return JoinMaterialize(node, left, right);
+	}
+	std::vector<const DevColumn *> outs;
+	std::vector<int> side;
+	for (auto &name : node.output_columns) {
+		const DevColumn *l = nullptr, *r = nullptr;
+		for (auto &c : left) if (c.name == name) { l = &c; break; }
+		for (auto &c : right) if (c.name == name) { r = &c; break; }
+		if (!l == !r) return JoinMaterialize(node, left, right);  // missing or ambiguous: its error path
+		outs.push_back(l ? l : r);
+		side.push_back(l ? 0 : 1);
+	}
+	const uint64_t ln = lk->rows, rn = rk->rows;
+	const size_t kw = TypeSize(rk->type);
+	uint64_t *rw = arena_.AllocT<uint64_t>(rn);
+	kern::WidenKeys(rk->data, kw, rn, rw, stream_);
+	uint64_t *mm = arena_.AllocT<uint64_t>(2);
+	kern::MinMaxU64(rw, rn, mm, stream_);
+	uint64_t host_mm[2];
+	VGPU_CUDA(cudaMemcpyAsync(host_mm, mm, 16, cudaMemcpyDeviceToHost, stream_));
+	VGPU_CUDA(cudaStreamSynchronize(stream_));
+	const uint64_t bias = host_mm[0];
+	const uint64_t range = host_mm[1] - host_mm[0];
+	const int bits = BitsFor(range);
+	kern::SubtractBias(rw, rn, bias, stream_);
+	uint32_t *perm = arena_.AllocT<uint32_t>(rn);
+	kern::Iota(perm, rn, stream_);
+	uint64_t *rw_alt = arena_.AllocT<uint64_t>(rn);
+	uint32_t *perm_alt = arena_.AllocT<uint32_t>(rn);
+	kern::RadixSortPairs(rw, perm, rw_alt, perm_alt, rn, bits, arena_);
+	arena_.FreeNow(rw_alt);
+	arena_.FreeNow(perm_alt);
+	uint32_t *dups = arena_.AllocT<uint32_t>(1);
+	kern::CountAdjacentEqual(rw, rn, dups, stream_);
+	if (ReadU32(dups) != 0) return JoinMaterialize(node, left, right);  // many-to-many
+	// Dense keys (range within 4x the key count, at most 2^28): a position table over the whole range,
+	// one read per probe. Otherwise a directory of at most 2^22 buckets and a short search.
+	uint32_t shift;
+	uint64_t nb;
+	uint32_t *dir;
+	if (range < (1ull << 28) && range < 4 * rn) {
+		shift = 0xffu;
+		nb = range + 1;
+		dir = arena_.AllocT<uint32_t>(nb);
+		kern::JoinPositions(rw, rn, range, dir, stream_);
+	} else {
+		shift = bits > 22 ? static_cast<uint32_t>(bits - 22) : 0u;
+		nb = (range >> shift) + 1;
+		dir = arena_.AllocT<uint32_t>(nb + 1);
+		kern::JoinDirectory(rw, rn, shift, nb, dir, stream_);
+	}
+	for (size_t i = 0; i < outs.size(); i++) {
+		DevColumn c = *outs[i];
+		c.name = node.output_columns[i];
+		if (side[i] == 1) {  // right columns in sorted-key order
+			const size_t w = TypeSize(c.type);
+			void *dst = arena_.Alloc(rn * w);
+			kern::Gather(outs[i]->data, w, perm, rn, dst, stream_);
+			c.data = dst;
+			if (outs[i]->valid) {
+				uint8_t *v = arena_.AllocT<uint8_t>(rn);
+				kern::Gather(outs[i]->valid, 1, perm, rn, v, stream_);
+				c.valid = v;
+			}
+		}
+		SourceColumn sc;
+		sc.name = c.name;
+		sc.type = c.type;
+		sc.nullable = c.valid != nullptr;
+		sc.side = side[i];
+		pin.spec.sources.push_back(sc);
+		pin.sources.push_back(c);
+	}
+	SourceColumn key;
+	key.name = "__vgpu_join_key";
+	key.type = lk->type;
+	key.side = 0;
+	pin.spec.join_key = static_cast<int>(pin.spec.sources.size());
+	pin.spec.sources.push_back(key);
+	DevColumn kc = *lk;
+	kc.name = key.name;
+	pin.sources.push_back(kc);
+	pin.spec.join = true;
+	pin.rows = ln;
+	pin.right_rows = 0;
+	pin.join_words[0] = reinterpret_cast<uint64_t>(rw);
+	pin.join_words[1] = reinterpret_cast<uint64_t>(dir);
+	pin.join_words[2] = bias;
+	pin.join_words[3] = shift | (nb << 8);
+	*fused = true;
+	return {};
+}
+
+// The join's output relation: right side sorted by key, per-left-row search, load-balanced expansion
+// of the match pairs, gathers of the output columns.
+Relation Executor::JoinMaterialize(const PlanNode &node, Relation &left, Relation &right) {
 	auto find = [](const Relation &rel, const std::string &name, const char *side) -> const DevColumn & {
 		for (auto &c : rel) {
 			if (c.name == name) return c;

@@ -346,6 +346,30 @@ __global__ void JoinExpandKernel(const uint64_t *offsets, const uint64_t *lower,
 	}
 }
 
+// Radix directory over a sorted key array (see vgpu_join_find): position i writes the entries of the
+// buckets that start at i, so every one of the nb + 1 entries is written exactly once.
+__global__ void JoinDirectoryKernel(const uint64_t *sorted, uint64_t n, uint32_t shift, uint64_t nb, uint32_t *dir) {
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i <= n; i += (uint64_t)gridDim.x * blockDim.x) {
+		const uint64_t lo = i == 0 ? 0 : (sorted[i - 1] >> shift) + 1;
+		const uint64_t hi = i == n ? nb : (sorted[i] >> shift);
+		for (uint64_t b = lo; b <= hi && b <= nb; ++b) dir[b] = static_cast<uint32_t>(i);
+	}
+}
+
+__global__ void JoinPositionsKernel(const uint64_t *sorted, uint64_t n, uint32_t *slots) {
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+		slots[sorted[i]] = static_cast<uint32_t>(i);
+	}
+}
+
+__global__ void CountAdjacentEqualKernel(const uint64_t *sorted, uint64_t n, uint32_t *out) {
+	uint32_t local = 0;
+	for (uint64_t i = 1 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+		local += sorted[i] == sorted[i - 1] ? 1u : 0u;
+	}
+	if (local) atomicAdd(out, local);
+}
+
 // Work list of a partitioned aggregation pass. Item = (partition, first row, end row, split index or
 // ~0). Partitions above `split_rows` rows become ceil(size / split_rows) chunks sharing one split
 // index; everything is ordered longest first by size class (chunks of split partitions, then
@@ -420,6 +444,27 @@ __global__ void __launch_bounds__(kPlanBlock) PlanWorkKernel(const uint32_t *off
 }
 
 } // namespace
+
+void JoinDirectory(const uint64_t *sorted, uint64_t n, uint32_t shift, uint64_t nb, uint32_t *dir, cudaStream_t stream) {
+	LaunchScope scope("join_directory", stream, n * 8 + (nb + 1) * 4, n);
+	JoinDirectoryKernel<<<GridFor(n + 1, 256), 256, 0, stream>>>(sorted, n, shift, nb, dir);
+	VGPU_CUDA(cudaGetLastError());
+}
+
+void JoinPositions(const uint64_t *sorted, uint64_t n, uint64_t range, uint32_t *slots, cudaStream_t stream) {
+	LaunchScope scope("join_positions", stream, n * 12 + (range + 1) * 4, n);
+	VGPU_CUDA(cudaMemsetAsync(slots, 0xff, (range + 1) * 4, stream));
+	JoinPositionsKernel<<<GridFor(n, 256), 256, 0, stream>>>(sorted, n, slots);
+	VGPU_CUDA(cudaGetLastError());
+}
+
+void CountAdjacentEqual(const uint64_t *sorted, uint64_t n, uint32_t *out, cudaStream_t stream) {
+	VGPU_CUDA(cudaMemsetAsync(out, 0, 4, stream));
+	if (n < 2) return;
+	LaunchScope scope("count_adjacent_equal", stream, n * 8, n);
+	CountAdjacentEqualKernel<<<GridFor(n, 256), 256, 0, stream>>>(sorted, n, out);
+	VGPU_CUDA(cudaGetLastError());
+}
 
 uint64_t PlanWorkCapacity(uint32_t P, uint64_t rows, uint32_t min_split) {
 	return static_cast<uint64_t>(P) + rows / (min_split ? min_split : 1) + 1;

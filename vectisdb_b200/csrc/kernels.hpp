@@ -48,6 +48,15 @@ void JoinSearch(const uint64_t *probe, uint64_t n_probe, const uint64_t *sorted,
 void JoinExpand(const uint64_t *offsets, const uint64_t *lower, uint64_t n_left, const uint32_t *sorted_perm,
                 uint64_t total, uint32_t *out_left, uint32_t *out_right, cudaStream_t stream);
 
+//! Radix directory of a sorted (biased) key array: dir[b] = first position whose key >> shift >= b,
+//! for b in [0, nb]; dir needs nb + 1 entries and nb must exceed every key >> shift.
+void JoinDirectory(const uint64_t *sorted, uint64_t n, uint32_t shift, uint64_t nb, uint32_t *dir, cudaStream_t stream);
+//! Dense position table of unique sorted (biased) keys, all <= range: slots[k] = position of key k,
+//! 0xffffffff where no key; slots needs range + 1 entries.
+void JoinPositions(const uint64_t *sorted, uint64_t n, uint64_t range, uint32_t *slots, cudaStream_t stream);
+//! *out = number of positions i > 0 with sorted[i] == sorted[i - 1].
+void CountAdjacentEqual(const uint64_t *sorted, uint64_t n, uint32_t *out, cudaStream_t stream);
+
 //! Work list of a partitioned aggregation pass over `P` partitions whose row ranges start at
 //! offsets[p * stride] (the last ends at *total_rows): 16-byte items (partition, first row, end row,
 //! split index or ~0u), longest first, into `items` (capacity PlanWorkCapacity). Partitions larger
