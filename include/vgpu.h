@@ -306,6 +306,42 @@ vgpu_status vgpu_cache_invalidate_all(void);
 uint64_t vgpu_cache_current_bytes(void);
 uint64_t vgpu_cache_table_generation(const vgpu_table_ref *table);
 
+/* ---- Stream pipeline (GpuStreamPipeline, cuda_engine/include/gpu_stream_pipeline.hpp:122-208) -------
+ * A row-independent projection chain (PROJECTION+ over SCAN, no filter) run batch by batch with upload,
+ * compute and download of consecutive batches overlapping on three streams. vgpu_pipeline_create
+ * allocates every buffer (depth + 1 stages of max_rows_per_batch rows) and compiles the fused kernel,
+ * failing there rather than mid-scan. Batches are host columns in the declared order (names and
+ * types checked); their memory may be reused as soon as vgpu_pipeline_submit returns. Results come
+ * back in submission order, in pinned host memory owned by the result's stage, valid until
+ * vgpu_pipeline_result_release. Columns are named col0, col1, ... (the top projection's
+ * expressions). Externally serialized: one call at a time on a pipeline. */
+typedef struct vgpu_pipeline vgpu_pipeline;
+typedef struct vgpu_pipeline_result vgpu_pipeline_result;
+/* GpuStreamPipeline::Supports (gpu_stream_pipeline.hpp:138-145): 1 when the plan has the shape. */
+int vgpu_pipeline_supports(const vgpu_plan *plan);
+/* Constructor (gpu_stream_pipeline.hpp:147-157); depth = batches in flight (0 = 3). */
+vgpu_status vgpu_pipeline_create(const vgpu_plan *plan, const char *const *input_names, const int32_t *input_types,
+                                 size_t n_inputs, uint64_t max_rows_per_batch, int32_t depth, vgpu_pipeline **out);
+size_t vgpu_pipeline_output_count(const vgpu_pipeline *pipeline);
+int32_t vgpu_pipeline_output_type(const vgpu_pipeline *pipeline, size_t index);
+/* Poll / CanSubmit (gpu_stream_pipeline.hpp:163-176). */
+void vgpu_pipeline_poll(vgpu_pipeline *pipeline);
+int vgpu_pipeline_can_submit(vgpu_pipeline *pipeline);
+/* Submit (gpu_stream_pipeline.hpp:178-186): queues one batch of `row_count` rows. */
+vgpu_status vgpu_pipeline_submit(vgpu_pipeline *pipeline, const vgpu_column *columns, size_t n_columns,
+                                 uint64_t row_count);
+/* TryTake / TakeBlocking (gpu_stream_pipeline.hpp:188-199): *out = the oldest batch's result, or NULL
+ * (not finished yet / nothing in flight). */
+vgpu_status vgpu_pipeline_try_take(vgpu_pipeline *pipeline, vgpu_pipeline_result **out);
+vgpu_status vgpu_pipeline_take_blocking(vgpu_pipeline *pipeline, vgpu_pipeline_result **out);
+size_t vgpu_pipeline_in_flight(const vgpu_pipeline *pipeline);
+uint64_t vgpu_pipeline_result_rows(const vgpu_pipeline_result *result);
+size_t vgpu_pipeline_result_column_count(const vgpu_pipeline_result *result);
+vgpu_status vgpu_pipeline_result_get_column(const vgpu_pipeline_result *result, size_t index, vgpu_column *out);
+/* GpuStreamResult::Reset: returns the stage for reuse. */
+void vgpu_pipeline_result_release(vgpu_pipeline_result *result);
+void vgpu_pipeline_destroy(vgpu_pipeline *pipeline);
+
 /* ---- Batching: many queries in one persistent, graph-captured launch ------------------------------
  * No single reference function: this is the batching form added beside the reference's
  * one-plan-per-call ExecutePlan (gpu_engine.hpp:389-402). Plans of the form GROUP_BY(keys) <-

@@ -89,3 +89,21 @@ def test_engine_nvrtc_is_independent_of_an_older_preloaded_copy():
     out = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     assert int(out.stdout.strip().splitlines()[-1]) > 1000
+
+
+def test_stream_pipeline_supports_projection_chains_only():
+    """GpuStreamPipeline::Supports: PROJECTION+ over a SCAN with resolvable inputs; no filter."""
+    from vectisdb_b200 import StreamPipeline, make_projection
+    scan = make_scan(["a", "b"])
+    ok = make_projection([make_expr("((long long*)out)[idx] = ((const long long*)inputs[0])[row] + 1;", ["a"],
+                                    T.INT64)], scan)
+    assert StreamPipeline.supports(ok)
+    assert StreamPipeline.supports(make_projection(
+        [make_expr("((long long*)out)[idx] = ((const long long*)inputs[0])[row];", ["col0"], T.INT64)], ok))
+    bad_input = make_projection([make_expr("((long long*)out)[idx] = ((const long long*)inputs[0])[row];", ["zz"],
+                                           T.INT64)], scan)
+    assert not StreamPipeline.supports(bad_input)
+    filt = make_filter([make_expr("((bool*)out)[idx] = ((const long long*)inputs[0])[row] > 0;", ["a"], T.BOOLEAN)],
+                       scan)
+    assert not StreamPipeline.supports(filt)
+    assert not StreamPipeline.supports(scan)

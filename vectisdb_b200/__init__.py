@@ -8,6 +8,7 @@ from .engine import (  # noqa: F401
     BatchOptions,
     PreparedBatch,
     Server,
+    StreamPipeline,
     batch_clear,
     batch_template,
     device_to_host,

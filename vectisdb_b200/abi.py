@@ -137,6 +137,22 @@ SIGNATURES = [
     ("vgpu_batch_template", C.c_int, [C.c_char_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t),
                                       C.POINTER(C.c_size_t)]),
     ("vgpu_batch_clear", C.c_int, []),
+    ("vgpu_pipeline_supports", C.c_int, [C.POINTER(vgpu_plan)]),
+    ("vgpu_pipeline_create", C.c_int, [C.POINTER(vgpu_plan), C.POINTER(C.c_char_p), C.POINTER(C.c_int32), C.c_size_t,
+                                       C.c_uint64, C.c_int32, C.POINTER(C.c_void_p)]),
+    ("vgpu_pipeline_output_count", C.c_size_t, [C.c_void_p]),
+    ("vgpu_pipeline_output_type", C.c_int32, [C.c_void_p, C.c_size_t]),
+    ("vgpu_pipeline_poll", None, [C.c_void_p]),
+    ("vgpu_pipeline_can_submit", C.c_int, [C.c_void_p]),
+    ("vgpu_pipeline_submit", C.c_int, [C.c_void_p, C.POINTER(vgpu_column), C.c_size_t, C.c_uint64]),
+    ("vgpu_pipeline_try_take", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    ("vgpu_pipeline_take_blocking", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    ("vgpu_pipeline_in_flight", C.c_size_t, [C.c_void_p]),
+    ("vgpu_pipeline_result_rows", C.c_uint64, [C.c_void_p]),
+    ("vgpu_pipeline_result_column_count", C.c_size_t, [C.c_void_p]),
+    ("vgpu_pipeline_result_get_column", C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(vgpu_column)]),
+    ("vgpu_pipeline_result_release", None, [C.c_void_p]),
+    ("vgpu_pipeline_destroy", None, [C.c_void_p]),
     ("vgpu_server_options_init", None, [C.POINTER(vgpu_server_options)]),
     ("vgpu_server_create", C.c_int, [C.POINTER(vgpu_server_options), C.POINTER(C.c_void_p)]),
     ("vgpu_server_submit", C.c_int, [C.c_void_p, C.POINTER(vgpu_plan), C.POINTER(vgpu_column), C.c_size_t,

@@ -33,6 +33,7 @@ ENGINE_SOURCES = [
     "executor.cu",
     "batch.cu",
     "server.cpp",
+    "stream_pipeline.cu",
     "noalloc.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

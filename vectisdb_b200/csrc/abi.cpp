@@ -14,6 +14,7 @@
 #include "cost_model.hpp"
 #include "batch.hpp"
 #include "server.hpp"
+#include "stream_pipeline.hpp"
 #include "executor.hpp"
 #include "plan.hpp"
 #include "runtime.hpp"
@@ -260,6 +261,142 @@ vgpu_status vgpu_execute_batch(const vgpu_plan *const *plans, const vgpu_column 
 		auto pb = PrepareFromAbi(plans, n_plans);
 		RunPreparedBatch(*pb, inputs, n_inputs, options, batch_options, results, stats);
 	});
+}
+
+struct vgpu_pipeline {
+	std::unique_ptr<StreamPipeline> p;
+	size_t outstanding = 0;  // results handed out and not yet released
+};
+
+struct vgpu_pipeline_result {
+	vgpu_pipeline *owner = nullptr;
+	int stage = -1;
+};
+
+int vgpu_pipeline_supports(const vgpu_plan *plan) {
+	try {
+		auto root = ConvertPlan(plan);
+		return StreamPipeline::Supports(*root) ? 1 : 0;
+	} catch (...) {
+		return 0;
+	}
+}
+
+vgpu_status vgpu_pipeline_create(const vgpu_plan *plan, const char *const *input_names, const int32_t *input_types,
+                                 size_t n_inputs, uint64_t max_rows_per_batch, int32_t depth, vgpu_pipeline **out) {
+	return Guard([&] {
+		if (!out || (n_inputs > 0 && (!input_names || !input_types))) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		*out = nullptr;
+		std::vector<std::string> names;
+		std::vector<ValueType> types;
+		for (size_t i = 0; i < n_inputs; i++) {
+			if (!input_names[i]) Fail(VGPU_ERR_INVALID_ARGUMENT, "null input name");
+			if (!IsValidValueType(input_types[i])) Fail(VGPU_ERR_INVALID_ARGUMENT, "input type out of range");
+			names.push_back(input_names[i]);
+			types.push_back(static_cast<ValueType>(input_types[i]));
+		}
+		auto *p = new vgpu_pipeline();
+		try {
+			p->p.reset(new StreamPipeline(ConvertPlan(plan), names, types, max_rows_per_batch, depth > 0 ? depth : 3));
+		} catch (...) {
+			delete p;
+			throw;
+		}
+		*out = p;
+	});
+}
+
+size_t vgpu_pipeline_output_count(const vgpu_pipeline *pipeline) {
+	return pipeline && pipeline->p ? pipeline->p->output_types().size() : 0;
+}
+
+int32_t vgpu_pipeline_output_type(const vgpu_pipeline *pipeline, size_t index) {
+	if (!pipeline || !pipeline->p || index >= pipeline->p->output_types().size()) return -1;
+	return static_cast<int32_t>(pipeline->p->output_types()[index]);
+}
+
+void vgpu_pipeline_poll(vgpu_pipeline *pipeline) {
+	if (pipeline && pipeline->p) pipeline->p->Poll();
+}
+
+int vgpu_pipeline_can_submit(vgpu_pipeline *pipeline) {
+	return pipeline && pipeline->p && pipeline->p->CanSubmit() ? 1 : 0;
+}
+
+vgpu_status vgpu_pipeline_submit(vgpu_pipeline *pipeline, const vgpu_column *columns, size_t n_columns,
+                                 uint64_t row_count) {
+	return Guard([&] {
+		if (!pipeline || !pipeline->p || (n_columns > 0 && !columns)) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		pipeline->p->Submit(std::vector<vgpu_column>(columns, columns + n_columns), row_count);
+	});
+}
+
+namespace {
+vgpu_status PipelineTake(vgpu_pipeline *pipeline, vgpu_pipeline_result **out, bool wait) {
+	return Guard([&] {
+		if (!pipeline || !pipeline->p || !out) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		*out = nullptr;
+		const int s = pipeline->p->Take(wait);
+		if (s < 0) return;
+		auto *r = new vgpu_pipeline_result();
+		r->owner = pipeline;
+		r->stage = s;
+		pipeline->outstanding++;
+		*out = r;
+	});
+}
+} // namespace
+
+vgpu_status vgpu_pipeline_try_take(vgpu_pipeline *pipeline, vgpu_pipeline_result **out) {
+	return PipelineTake(pipeline, out, false);
+}
+
+vgpu_status vgpu_pipeline_take_blocking(vgpu_pipeline *pipeline, vgpu_pipeline_result **out) {
+	return PipelineTake(pipeline, out, true);
+}
+
+size_t vgpu_pipeline_in_flight(const vgpu_pipeline *pipeline) {
+	return pipeline && pipeline->p ? pipeline->p->in_flight() : 0;
+}
+
+uint64_t vgpu_pipeline_result_rows(const vgpu_pipeline_result *result) {
+	return result && result->owner ? result->owner->p->StageRows(result->stage) : 0;
+}
+
+size_t vgpu_pipeline_result_column_count(const vgpu_pipeline_result *result) {
+	return result && result->owner ? result->owner->p->output_types().size() : 0;
+}
+
+vgpu_status vgpu_pipeline_result_get_column(const vgpu_pipeline_result *result, size_t index, vgpu_column *out) {
+	return Guard([&] {
+		if (!result || !result->owner || !out) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		auto &p = *result->owner->p;
+		if (index >= p.output_types().size()) Fail(VGPU_ERR_INVALID_ARGUMENT, "column index out of range");
+		auto v = p.StageOutput(result->stage, index);
+		std::memset(out, 0, sizeof(*out));
+		out->name = p.output_names()[index].c_str();
+		out->type = static_cast<int32_t>(p.output_types()[index]);
+		out->data = v.data;
+		out->validity = v.validity;
+		out->row_count = p.StageRows(result->stage);
+		out->memory = VGPU_MEM_HOST;
+	});
+}
+
+void vgpu_pipeline_result_release(vgpu_pipeline_result *result) {
+	if (!result) return;
+	if (result->owner && result->owner->p) {
+		result->owner->p->Release(result->stage);
+		result->owner->outstanding--;
+	}
+	delete result;
+}
+
+void vgpu_pipeline_destroy(vgpu_pipeline *pipeline) {
+	try {
+		delete pipeline;
+	} catch (...) {
+	}
 }
 
 struct vgpu_server {

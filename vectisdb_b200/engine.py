@@ -472,6 +472,92 @@ class PreparedBatch:
             pass
 
 
+class StreamPipeline:
+    """GpuStreamPipeline over the C ABI (vgpu_pipeline_*): a projection chain run batch by batch with
+    upload, compute and download of consecutive batches overlapping. take() copies a finished batch's
+    columns out and hands its stage back."""
+
+    def __init__(self, plan: GpuPlanNode, input_names: Sequence[str], input_types: Sequence[GpuValueType],
+                 max_rows_per_batch: int, depth: int = 3):
+        keep = _Keep()
+        plan_c = serialize_plan(plan, keep)
+        names = (C.c_char_p * len(input_names))(*[n.encode() for n in input_names])
+        types = (C.c_int32 * len(input_types))(*[int(t) for t in input_types])
+        self._h = C.c_void_p()
+        abi.check(abi.lib().vgpu_pipeline_create(C.byref(plan_c), names, types, len(input_names), max_rows_per_batch,
+                                                 depth, C.byref(self._h)))
+        self.input_names = list(input_names)
+        self.input_types = [GpuValueType(t) for t in input_types]
+
+    @staticmethod
+    def supports(plan: GpuPlanNode) -> bool:
+        keep = _Keep()
+        return bool(abi.lib().vgpu_pipeline_supports(C.byref(serialize_plan(plan, keep))))
+
+    @property
+    def output_types(self) -> list[GpuValueType]:
+        L = abi.lib()
+        return [GpuValueType(L.vgpu_pipeline_output_type(self._h, i)) for i in range(L.vgpu_pipeline_output_count(self._h))]
+
+    def can_submit(self) -> bool:
+        return bool(abi.lib().vgpu_pipeline_can_submit(self._h))
+
+    def in_flight(self) -> int:
+        return int(abi.lib().vgpu_pipeline_in_flight(self._h))
+
+    def submit(self, columns: Sequence[GpuColumn], rows: int | None = None) -> None:
+        keep = _Keep()
+        cols = serialize_inputs(columns, keep)
+        n = rows if rows is not None else (columns[0].row_count if columns else 0)
+        abi.check(abi.lib().vgpu_pipeline_submit(self._h, cols, len(columns), n))
+
+    def _take(self, wait: bool):
+        L = abi.lib()
+        h = C.c_void_p()
+        abi.check((L.vgpu_pipeline_take_blocking if wait else L.vgpu_pipeline_try_take)(self._h, C.byref(h)))
+        if not h.value:
+            return None
+        try:
+            n = int(L.vgpu_pipeline_result_rows(h))
+            out = []
+            for i in range(L.vgpu_pipeline_result_column_count(h)):
+                c = abi.vgpu_column()
+                abi.check(L.vgpu_pipeline_result_get_column(h, i, C.byref(c)))
+                t = GpuValueType(c.type)
+                dt = NUMPY_DTYPE[t]
+                data = np.zeros(0, dtype=dt)
+                if n:
+                    raw = np.ctypeslib.as_array(C.cast(c.data, C.POINTER(C.c_uint8)), shape=(n * dt.itemsize,))
+                    data = raw.copy().view(dt)
+                validity = None
+                if c.validity and n:
+                    vb = np.ctypeslib.as_array(C.cast(c.validity, C.POINTER(C.c_uint8)), shape=((n + 7) // 8,))
+                    validity = np.unpackbits(vb, bitorder="little")[:n].astype(bool)
+                out.append(GpuColumn(c.name.decode(), t, data, validity, n))
+            return out
+        finally:
+            L.vgpu_pipeline_result_release(h)
+
+    def try_take(self):
+        """The oldest batch's columns if it has finished, else None."""
+        return self._take(False)
+
+    def take_blocking(self):
+        """The oldest batch's columns, waiting for it; None when nothing is in flight."""
+        return self._take(True)
+
+    def close(self):
+        if self._h:
+            abi.lib().vgpu_pipeline_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Server:
     """Serving (vgpu_server_*): admission against a device-memory budget, `slots` requests running
     concurrently on their own streams, same-template group-by requests batched together."""
