@@ -84,8 +84,8 @@ class ClockSampler:
         except FileNotFoundError:
             self.proc = None
             return
-        # nvidia-smi's start-up (NVML initialisation) competes with the driver for a moment: let it
-        # finish (first sample written) before anything is timed.
+        # nvidia-smi's start-up (NVML initialisation) competes with the driver for a moment: wait for
+        # its first sample (callers also keep the first second after this untimed).
         deadline = time.time() + 5.0
         while time.time() < deadline and self.proc.poll() is None:
             if self.path.exists() and self.path.read_text().count("\n") >= 1:
@@ -243,6 +243,11 @@ def run_c3(args, world, rank, local):
         sampler = ClockSampler(local) if sample_clocks else None
         if sampler:
             sampler.start()
+            t_s = time.time()
+            while time.time() - t_s < 1.0:  # untimed until the sampler has settled
+                out = step_fn()
+                for r in (out[0] if isinstance(out, tuple) else out):
+                    r.free()
         profile_drain()
         profile_enable(True)
         torch.cuda.synchronize()
@@ -459,7 +464,7 @@ def main():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c2b", "c3", "c4"])
-    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--rows", type=int, default=0, help="small-case size for profiling (0 = the full workload)")
     args = p.parse_args()
@@ -507,12 +512,17 @@ def main():
             raise RuntimeError(f"engine failed: {r.error_message}")
         return r
 
+    # The clock sampler starts before the warm-up: nvidia-smi's first queries after start-up stall the
+    # driver for a few hundred ms, which must land in untimed work, not in the timed region.
+    sampler = ClockSampler(local if "CUDA_VISIBLE_DEVICES" not in os.environ else 0)
+    sampler.start()
+    t_sampler = time.time()
     for _ in range(args.warmup):
+        step().free()
+    while time.time() - t_sampler < 1.0:  # untimed steps until the sampler has settled
         step().free()
     torch.cuda.synchronize()
 
-    sampler = ClockSampler(local if "CUDA_VISIBLE_DEVICES" not in os.environ else 0)
-    sampler.start()
     profile_drain()
     profile_enable(True)
     if world > 1:
@@ -585,6 +595,7 @@ def main():
         if i > 0:
             e2e_ms.append(dt * 1000)
         d2h = sum(c.data.nbytes + (0 if c.validity is None else (len(c.validity) + 7) // 8) for c in r.columns)
+        del r  # a caller that is done with a result lets it go before the next call
     e2e_value = wl.rows * world / (float(np.mean(e2e_ms)) / 1000.0) if e2e_ms else None
 
     cpu = None

@@ -552,7 +552,7 @@ vgpu_status vgpu_result_get_column(const vgpu_result *result, size_t index, vgpu
 			out->validity = c.device_validity;
 		} else {
 			out->memory = VGPU_MEM_HOST;
-			out->data = c.data.empty() ? nullptr : c.data.data();
+			out->data = c.host ? static_cast<const void *>(c.host.get()) : (c.data.empty() ? nullptr : c.data.data());
 			out->validity = c.validity.empty() ? nullptr : c.validity.data();
 		}
 	});

@@ -1216,8 +1216,10 @@ ExecResult ExecutePlan(const PlanNode &plan, const std::vector<vgpu_column> &inp
 				o.device_validity = bm;
 			}
 		} else {
-			o.data.resize(bytes);
-			if (bytes) VGPU_CUDA(cudaMemcpyAsync(o.data.data(), c.data, bytes, cudaMemcpyDeviceToHost, stream));
+			if (bytes) {
+				o.host = PinnedPool::Get().Acquire(bytes);
+				VGPU_CUDA(cudaMemcpyAsync(o.host.get(), c.data, bytes, cudaMemcpyDeviceToHost, stream));
+			}
 			if (c.valid && c.rows > 0) {
 				const size_t vb = (c.rows + 7) / 8;
 				uint8_t *bm = ex.arena().AllocT<uint8_t>(vb);

@@ -30,6 +30,7 @@ struct HostColumnOut {
 	ValueType type;
 	uint64_t rows = 0;
 	std::vector<uint8_t> data;
+	std::shared_ptr<uint8_t> host;  // page-locked copy of the values (used instead of `data` when set)
 	std::vector<uint8_t> validity; // empty = all valid
 	void *device_data = nullptr;   // set when the result stays on the device
 	uint8_t *device_validity = nullptr;

@@ -21,6 +21,43 @@ std::string Sha256Hex(const void *data, size_t n);
 #include "device_lib_embed.inc"
 
 // ============================================================================================
+// PinnedPool
+
+PinnedPool &PinnedPool::Get() {
+	static PinnedPool *p = new PinnedPool();
+	return *p;
+}
+
+std::shared_ptr<uint8_t> PinnedPool::Acquire(size_t bytes) {
+	size_t cls = 64 * 1024;
+	while (cls < bytes) cls <<= 1;
+	void *p = nullptr;
+	{
+		std::lock_guard<std::mutex> lock(mu_);
+		auto it = free_.find(cls);
+		if (it != free_.end()) {
+			p = it->second;
+			free_.erase(it);
+			cached_ -= cls;
+		}
+	}
+	if (!p) VGPU_CUDA(cudaMallocHost(&p, cls));
+	return std::shared_ptr<uint8_t>(static_cast<uint8_t *>(p), [this, cls](uint8_t *q) { Return(q, cls); });
+}
+
+void PinnedPool::Return(void *p, size_t cls) {
+	{
+		std::lock_guard<std::mutex> lock(mu_);
+		if (cached_ + cls <= kMaxCached) {
+			free_.emplace(cls, p);
+			cached_ += cls;
+			return;
+		}
+	}
+	cudaFreeHost(p);
+}
+
+// ============================================================================================
 // DeviceAllocator
 
 void DeviceAllocator::EnsureBudgetLocked() {

@@ -7,6 +7,8 @@
 #include <cstdint>
 #include <list>
 #include <memory>
+#include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -35,6 +37,23 @@ struct DeviceProps {
 //! blocks cached so steady-state execution does not go back to the driver) with a hard byte budget
 //! checked before every allocation. The budget replaces the reference's per-plan cudaMalloc arena
 //! (cuda_engine/src/gpu_executor_internal.hpp:37-59) and its headroom oracle (src/rmm_pool.cpp).
+//! Page-locked host buffers for results copied to the host, reused across calls (the role of the
+//! reference's PinnedBufferPool, src/pinned_buffer_pool.cpp:78-116): a device->host copy into pinned
+//! memory runs at link speed, and page-locking a fresh buffer per result would cost more than the copy.
+//! Buffers come back to the pool when the last owner lets go; at most kMaxCached bytes stay cached.
+class PinnedPool {
+public:
+	static PinnedPool &Get();
+	std::shared_ptr<uint8_t> Acquire(size_t bytes);
+
+private:
+	void Return(void *p, size_t cls);
+	static constexpr size_t kMaxCached = 4ull << 30;
+	std::mutex mu_;
+	std::multimap<size_t, void *> free_;
+	size_t cached_ = 0;
+};
+
 class DeviceAllocator {
 public:
 	void *Alloc(size_t bytes, cudaStream_t stream);

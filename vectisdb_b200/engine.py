@@ -285,7 +285,22 @@ def serialize_inputs(inputs: Sequence[GpuColumn], keep: _Keep):
     return arr
 
 
-def _read_result(handle) -> list[GpuColumn]:
+class _ResultOwner:
+    """Keeps a vgpu_result alive while numpy views of its host columns exist (zero-copy results)."""
+
+    def __init__(self, handle):
+        self.handle = handle
+
+    def __del__(self):
+        try:
+            abi.lib().vgpu_result_free(self.handle)
+        except Exception:
+            pass
+
+
+def _read_result(handle, owner: "_ResultOwner | None" = None) -> list[GpuColumn]:
+    """Columns of a result. With `owner`, host columns are views of the result's own (page-locked)
+    memory that keep it alive; without, they are copies."""
     L = abi.lib()
     cols = []
     for i in range(L.vgpu_result_column_count(handle)):
@@ -297,7 +312,11 @@ def _read_result(handle) -> list[GpuColumn]:
         if c.memory == abi.MEM_DEVICE:
             cols.append(GpuColumn(c.name.decode(), t, None, None, n, int(c.data or 0)))
             continue
-        if n and c.data:
+        if n and c.data and owner is not None:
+            buf = (C.c_uint8 * (n * dt.itemsize)).from_address(c.data)
+            buf._vgpu_owner = owner
+            data = np.frombuffer(buf, dtype=dt)
+        elif n and c.data:
             raw = np.ctypeslib.as_array(C.cast(c.data, C.POINTER(C.c_uint8)), shape=(n * dt.itemsize,))
             data = raw.copy().view(dt)
         else:
@@ -377,14 +396,15 @@ class GpuEngine:
         status = self.lib.vgpu_execute_plan(C.byref(plan_c), cols, len(inputs), C.byref(opts), C.byref(handle))
         if status != abi.OK:
             return GpuExecutionResult(False, abi.last_error(), status, [])
-        try:
-            columns = _read_result(handle)
-        except Exception:
-            self.lib.vgpu_result_free(handle)
-            raise
         if o.output_on_device:
+            try:
+                columns = _read_result(handle)
+            except Exception:
+                self.lib.vgpu_result_free(handle)
+                raise
             return DeviceResult(handle, columns)
-        self.lib.vgpu_result_free(handle)
+        # host results: zero-copy views of the result's page-locked buffers, freed with the last view
+        columns = _read_result(handle, _ResultOwner(handle))
         return GpuExecutionResult(True, "", abi.OK, columns)
 
 
