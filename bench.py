@@ -109,6 +109,18 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def max_over_ranks(value: float, world: int, device: str = "cuda") -> float:
+    """The largest of every rank's `value` (a timed region's milliseconds): the job is as slow as its
+    slowest replica. Every rank calls it, in the same order."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -550,9 +562,7 @@ def main():
     groups = last.columns[0].row_count if last.columns else 0
     last.free()
     if world > 1:
-        t = torch.tensor([elapsed_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+        elapsed_ms = max_over_ranks(elapsed_ms, world)
     value = wl.rows * args.steps * world / (elapsed_ms / 1000.0)
 
     # passing rows (for per-kernel algorithmic bytes): one host-output run
