@@ -1,6 +1,7 @@
-"""Equi-join under a pipeline: the fused form (unique sorted side read through a radix directory, no
-materialized match pairs) against the materializing form and against numpy, including misses,
-negative keys, keys below the sorted side's minimum, and many-to-many fallback."""
+"""Equi-join under a pipeline: the fused forms (dense key tables holding a row index or the value
+itself; sorted keys with a radix directory), with no materialized match pairs, against the
+materializing form and against numpy, including misses, negative keys, keys below the right side's
+minimum, and many-to-many fallback."""
 import numpy as np
 import pytest
 
@@ -98,3 +99,29 @@ def test_filter_over_fused_join_keeps_left_order():
             exp_rv.append(int(rv[i]))
     assert np.array_equal(cols[0].data, np.array(exp_lv, np.int64))  # left-major order
     assert np.array_equal(cols[1].data, np.array(exp_rv, np.int32))
+
+
+@pytest.mark.parametrize("layout", ["dense_rows", "sorted_directory"])
+def test_fused_join_table_forms_match_numpy(layout):
+    """Dense keys with two right columns (row-index table) and sparse keys (sorted keys + radix
+    directory): every left row finds its right row or none, left order kept."""
+    rng = np.random.default_rng(21)
+    if layout == "dense_rows":
+        rk = rng.permutation(np.arange(-3000, 3000, dtype=np.int64))
+    else:
+        rk = np.unique(rng.integers(-(1 << 40), 1 << 40, 5000)).astype(np.int64)
+        rng.shuffle(rk)
+    r1 = rng.integers(0, 1000, len(rk)).astype(np.int32)
+    r2 = rng.standard_normal(len(rk))
+    lk = np.concatenate([rng.choice(rk, 20000), rng.integers(-(1 << 41), 1 << 41, 5000)]).astype(np.int64)
+    rng.shuffle(lk)
+    lv = np.arange(len(lk), dtype=np.int64)
+    join = make_join("lk", "rk", ["lv", "r1", "r2"], make_scan(["lk", "lv"]), make_scan(["rk", "r1", "r2"]))
+    plan = make_filter([make_expr("((bool*)out)[idx] = ((const int*)inputs[0])[row] >= 0;", ["r1"], T.BOOLEAN)], join)
+    cols = _run(plan, [make_column("lk", T.INT64, lk), make_column("lv", T.INT64, lv), make_column("rk", T.INT64, rk),
+                       make_column("r1", T.INT32, r1), make_column("r2", T.FLOAT64, r2)])
+    pos = {int(k): i for i, k in enumerate(rk.tolist())}
+    exp = [(v, pos[k]) for k, v in zip(lk.tolist(), lv.tolist()) if k in pos]
+    assert np.array_equal(cols[0].data, np.array([v for v, _ in exp], np.int64))
+    assert np.array_equal(cols[1].data, r1[[i for _, i in exp]])
+    assert np.array_equal(cols[2].data, r2[[i for _, i in exp]])

@@ -407,6 +407,11 @@ std::string PipelineCodegen::LoadBlock(const Geometry &g, const std::vector<bool
 			if (!needed[i] || src.side != 1) continue;
 			const char *t = CudaTypeName(src.type);
 			const int w = 2 + 2 * static_cast<int>(i);
+			if (spec_.join_inline) {
+				o << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) s" << i << "[r] = jm[r] >= 0 ? from_bits<"
+				  << t << ">((u64)(u32)jm[r]) : (" << t << ")0;\n";
+				continue;
+			}
 			o << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) s" << i << "[r] = jm[r] >= 0 ? ((const "
 			  << t << "*)a.w[" << w << "])[jm[r]] : (" << t << ")0;\n";
 			if (src.nullable) {

@@ -34,6 +34,8 @@ struct PipelineSpec {
 	// without a match are filtered out.
 	bool join = false;
 	int join_key = -1;
+	// The lookup returns the (single, <= 4-byte) right column's value itself instead of a position.
+	bool join_inline = false;
 	std::vector<const PlanNode *> chain; // FILTER / PROJECTION nodes, bottom-up
 };
 

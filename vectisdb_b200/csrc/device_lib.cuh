@@ -265,14 +265,20 @@ __device__ __forceinline__ void atomic_max_i64(i64 *p, i64 v) { atomicMax(reinte
 // position whose key >> shift >= b (dir[nb] = n), so a probe key's candidates are one bucket, which
 // a short binary search finishes. Keys are biased by the sorted side's minimum (u64 arithmetic);
 // a probe key below that minimum wraps to a bucket past nb and misses. Returns the position or -1.
-// shift == 0xff selects the dense form: dir is a position table over the whole key range
-// (dir[k] = position of key k, or 0xffffffff), nb its length.
+// Dense forms (tables indexed by the biased key over the whole range, nb entries): shift == 0xff,
+// dir holds row index + 1 of the key's right row (0 = no key); shift == 0xfe, `sorted` is reused as a
+// u64 table holding (1 << 32 | the right column's 32-bit value) (0 = no key), returned as is.
 __device__ __forceinline__ long long vgpu_join_find(u64 k, const u64 *__restrict__ sorted, const u32 *__restrict__ dir,
                                                     u64 nb, u32 shift) {
 	if (shift == 0xffu) {
 		if (k >= nb) return -1ll;
 		const u32 p = dir[k];
-		return p == 0xffffffffu ? -1ll : (long long)p;
+		return p == 0u ? -1ll : (long long)(p - 1u);
+	}
+	if (shift == 0xfeu) {
+		if (k >= nb) return -1ll;
+		const u64 e = sorted[k];
+		return e == 0ull ? -1ll : (long long)e;
 	}
 	const u64 b = k >> shift;
 	if (b >= nb) return -1ll;

@@ -1005,54 +1005,90 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 	const uint64_t range = host_mm[1] - host_mm[0];
 	const int bits = BitsFor(range);
 	kern::SubtractBias(rw, rn, bias, stream_);
-	uint32_t *perm = arena_.AllocT<uint32_t>(rn);
-	kern::Iota(perm, rn, stream_);
-	uint64_t *rw_alt = arena_.AllocT<uint64_t>(rn);
-	uint32_t *perm_alt = arena_.AllocT<uint32_t>(rn);
-	kern::RadixSortPairs(rw, perm, rw_alt, perm_alt, rn, bits, arena_);
-	arena_.FreeNow(rw_alt);
-	arena_.FreeNow(perm_alt);
-	uint32_t *dups = arena_.AllocT<uint32_t>(1);
-	kern::CountAdjacentEqual(rw, rn, dups, stream_);
-	if (ReadU32(dups) != 0) return JoinMaterialize(node, left, right);  // many-to-many
-	// Dense keys (range within 4x the key count, at most 2^28): a position table over the whole range,
-	// one read per probe. Otherwise a directory of at most 2^22 buckets and a short search.
-	uint32_t shift;
-	uint64_t nb;
-	uint32_t *dir;
-	if (range < (1ull << 28) && range < 4 * rn) {
-		shift = 0xffu;
-		nb = range + 1;
-		dir = arena_.AllocT<uint32_t>(nb);
-		kern::JoinPositions(rw, rn, range, dir, stream_);
-	} else {
-		shift = bits > 22 ? static_cast<uint32_t>(bits - 22) : 0u;
-		nb = (range >> shift) + 1;
-		dir = arena_.AllocT<uint32_t>(nb + 1);
-		kern::JoinDirectory(rw, rn, shift, nb, dir, stream_);
-	}
+	auto add_sources = [&](bool sorted_side, const uint32_t *perm) {
+		for (size_t i = 0; i < outs.size(); i++) {
+			DevColumn c = *outs[i];
+			c.name = node.output_columns[i];
+			if (side[i] == 1 && sorted_side) {  // right columns in sorted-key order
+				const size_t w = TypeSize(c.type);
+				void *dst = arena_.Alloc(rn * w);
+				kern::Gather(outs[i]->data, w, perm, rn, dst, stream_);
+				c.data = dst;
+				if (outs[i]->valid) {
+					uint8_t *v = arena_.AllocT<uint8_t>(rn);
+					kern::Gather(outs[i]->valid, 1, perm, rn, v, stream_);
+					c.valid = v;
+				}
+			}
+			SourceColumn sc;
+			sc.name = c.name;
+			sc.type = c.type;
+			sc.nullable = c.valid != nullptr;
+			sc.side = side[i];
+			pin.spec.sources.push_back(sc);
+			pin.sources.push_back(c);
+		}
+	};
+	size_t right_outs = 0;
+	const DevColumn *right_col = nullptr;
 	for (size_t i = 0; i < outs.size(); i++) {
-		DevColumn c = *outs[i];
-		c.name = node.output_columns[i];
-		if (side[i] == 1) {  // right columns in sorted-key order
-			const size_t w = TypeSize(c.type);
-			void *dst = arena_.Alloc(rn * w);
-			kern::Gather(outs[i]->data, w, perm, rn, dst, stream_);
-			c.data = dst;
-			if (outs[i]->valid) {
-				uint8_t *v = arena_.AllocT<uint8_t>(rn);
-				kern::Gather(outs[i]->valid, 1, perm, rn, v, stream_);
-				c.valid = v;
+		if (side[i] == 1) {
+			right_outs++;
+			right_col = outs[i];
+		}
+	}
+	uint32_t *dups = arena_.AllocT<uint32_t>(1);
+	bool built = false;
+	// Dense keys (range within 4x the key count, at most 2^28): a table indexed by the key over the whole
+	// range, filled without sorting. It holds the right row index, or -- when the join contributes one
+	// right column of at most 4 bytes -- that column's value itself, so a probe row costs one random
+	// read. A key met twice (many-to-many) falls back to the sorted form below.
+	if (range < (1ull << 28) && range < 4 * rn) {
+		if (right_outs == 1 && TypeSize(right_col->type) <= 4 && TypeSize(right_col->type) != 3 && !right_col->valid) {
+			uint64_t *table = arena_.AllocT<uint64_t>(range + 1);
+			kern::JoinDenseInline(rw, right_col->data, TypeSize(right_col->type), rn, range, table, dups, stream_);
+			if (ReadU32(dups) == 0) {
+				add_sources(false, nullptr);
+				pin.spec.join_inline = true;
+				pin.join_words[0] = reinterpret_cast<uint64_t>(table);
+				pin.join_words[1] = 0;
+				pin.join_words[3] = 0xfeu | ((range + 1) << 8);
+				built = true;
+			}
+		} else {
+			uint32_t *table = arena_.AllocT<uint32_t>(range + 1);
+			kern::JoinDenseRows(rw, rn, range, table, dups, stream_);
+			if (ReadU32(dups) == 0) {
+				add_sources(false, nullptr);
+				pin.join_words[0] = 0;
+				pin.join_words[1] = reinterpret_cast<uint64_t>(table);
+				pin.join_words[3] = 0xffu | ((range + 1) << 8);
+				built = true;
 			}
 		}
-		SourceColumn sc;
-		sc.name = c.name;
-		sc.type = c.type;
-		sc.nullable = c.valid != nullptr;
-		sc.side = side[i];
-		pin.spec.sources.push_back(sc);
-		pin.sources.push_back(c);
 	}
+	if (!built) {
+		// Sorted form: LSD radix sort of the right keys, uniqueness check, radix directory over the sorted
+		// keys (at most 2^22 buckets), right columns gathered into sorted order once.
+		uint32_t *perm = arena_.AllocT<uint32_t>(rn);
+		kern::Iota(perm, rn, stream_);
+		uint64_t *rw_alt = arena_.AllocT<uint64_t>(rn);
+		uint32_t *perm_alt = arena_.AllocT<uint32_t>(rn);
+		kern::RadixSortPairs(rw, perm, rw_alt, perm_alt, rn, bits, arena_);
+		arena_.FreeNow(rw_alt);
+		arena_.FreeNow(perm_alt);
+		kern::CountAdjacentEqual(rw, rn, dups, stream_);
+		if (ReadU32(dups) != 0) return JoinMaterialize(node, left, right);  // many-to-many
+		const uint32_t shift = bits > 22 ? static_cast<uint32_t>(bits - 22) : 0u;
+		const uint64_t nb = (range >> shift) + 1;
+		uint32_t *dir = arena_.AllocT<uint32_t>(nb + 1);
+		kern::JoinDirectory(rw, rn, shift, nb, dir, stream_);
+		add_sources(true, perm);
+		pin.join_words[0] = reinterpret_cast<uint64_t>(rw);
+		pin.join_words[1] = reinterpret_cast<uint64_t>(dir);
+		pin.join_words[3] = shift | (nb << 8);
+	}
+	pin.join_words[2] = bias;
 	SourceColumn key;
 	key.name = "__vgpu_join_key";
 	key.type = lk->type;
@@ -1065,10 +1101,6 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 	pin.spec.join = true;
 	pin.rows = ln;
 	pin.right_rows = 0;
-	pin.join_words[0] = reinterpret_cast<uint64_t>(rw);
-	pin.join_words[1] = reinterpret_cast<uint64_t>(dir);
-	pin.join_words[2] = bias;
-	pin.join_words[3] = shift | (nb << 8);
 	*fused = true;
 	return {};
 }

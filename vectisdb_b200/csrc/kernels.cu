@@ -356,10 +356,25 @@ __global__ void JoinDirectoryKernel(const uint64_t *sorted, uint64_t n, uint32_t
 	}
 }
 
-__global__ void JoinPositionsKernel(const uint64_t *sorted, uint64_t n, uint32_t *slots) {
+// Dense key tables: entry of (biased) key k = row index + 1, or (1 << 32 | value) with the row's
+// value inlined; a key met twice counts as a duplicate (compare-and-swap from empty).
+__global__ void JoinDenseRowsKernel(const uint64_t *keys, uint64_t n, uint32_t *table, uint32_t *dups) {
+	uint32_t local = 0;
 	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-		slots[sorted[i]] = static_cast<uint32_t>(i);
+		if (atomicCAS(&table[keys[i]], 0u, static_cast<uint32_t>(i + 1)) != 0u) local++;
 	}
+	if (local) atomicAdd(dups, local);
+}
+
+template <typename T>
+__global__ void JoinDenseInlineKernel(const uint64_t *keys, const T *values, uint64_t n, unsigned long long *table,
+                                      uint32_t *dups) {
+	uint32_t local = 0;
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+		const unsigned long long e = (1ull << 32) | static_cast<unsigned long long>(values[i]);
+		if (atomicCAS(&table[keys[i]], 0ull, e) != 0ull) local++;
+	}
+	if (local) atomicAdd(dups, local);
 }
 
 __global__ void CountAdjacentEqualKernel(const uint64_t *sorted, uint64_t n, uint32_t *out) {
@@ -451,10 +466,35 @@ void JoinDirectory(const uint64_t *sorted, uint64_t n, uint32_t shift, uint64_t 
 	VGPU_CUDA(cudaGetLastError());
 }
 
-void JoinPositions(const uint64_t *sorted, uint64_t n, uint64_t range, uint32_t *slots, cudaStream_t stream) {
-	LaunchScope scope("join_positions", stream, n * 12 + (range + 1) * 4, n);
-	VGPU_CUDA(cudaMemsetAsync(slots, 0xff, (range + 1) * 4, stream));
-	JoinPositionsKernel<<<GridFor(n, 256), 256, 0, stream>>>(sorted, n, slots);
+void JoinDenseRows(const uint64_t *keys, uint64_t n, uint64_t range, uint32_t *table, uint32_t *dups,
+                   cudaStream_t stream) {
+	LaunchScope scope("join_dense_table", stream, n * 12 + (range + 1) * 4, n);
+	VGPU_CUDA(cudaMemsetAsync(table, 0, (range + 1) * 4, stream));
+	VGPU_CUDA(cudaMemsetAsync(dups, 0, 4, stream));
+	JoinDenseRowsKernel<<<GridFor(n, 256), 256, 0, stream>>>(keys, n, table, dups);
+	VGPU_CUDA(cudaGetLastError());
+}
+
+void JoinDenseInline(const uint64_t *keys, const void *values, size_t width, uint64_t n, uint64_t range,
+                     uint64_t *table, uint32_t *dups, cudaStream_t stream) {
+	LaunchScope scope("join_dense_table", stream, n * (8 + width) + (range + 1) * 8, n);
+	VGPU_CUDA(cudaMemsetAsync(table, 0, (range + 1) * 8, stream));
+	VGPU_CUDA(cudaMemsetAsync(dups, 0, 4, stream));
+	auto *t = reinterpret_cast<unsigned long long *>(table);
+	const unsigned grid = GridFor(n, 256);
+	switch (width) {
+	case 1:
+		JoinDenseInlineKernel<uint8_t><<<grid, 256, 0, stream>>>(keys, static_cast<const uint8_t *>(values), n, t, dups);
+		break;
+	case 2:
+		JoinDenseInlineKernel<uint16_t><<<grid, 256, 0, stream>>>(keys, static_cast<const uint16_t *>(values), n, t, dups);
+		break;
+	case 4:
+		JoinDenseInlineKernel<uint32_t><<<grid, 256, 0, stream>>>(keys, static_cast<const uint32_t *>(values), n, t, dups);
+		break;
+	default:
+		Fail(VGPU_ERR_INTERNAL, "dense inline join table: value width must be 1, 2 or 4 bytes");
+	}
 	VGPU_CUDA(cudaGetLastError());
 }
 

@@ -51,9 +51,13 @@ void JoinExpand(const uint64_t *offsets, const uint64_t *lower, uint64_t n_left,
 //! Radix directory of a sorted (biased) key array: dir[b] = first position whose key >> shift >= b,
 //! for b in [0, nb]; dir needs nb + 1 entries and nb must exceed every key >> shift.
 void JoinDirectory(const uint64_t *sorted, uint64_t n, uint32_t shift, uint64_t nb, uint32_t *dir, cudaStream_t stream);
-//! Dense position table of unique sorted (biased) keys, all <= range: slots[k] = position of key k,
-//! 0xffffffff where no key; slots needs range + 1 entries.
-void JoinPositions(const uint64_t *sorted, uint64_t n, uint64_t range, uint32_t *slots, cudaStream_t stream);
+//! Dense join tables over (biased) keys all <= range, range + 1 entries, built without sorting:
+//! table[k] = row index + 1 of key k (0 = none), or (1 << 32 | value) with a <= 4-byte value of that
+//! row inlined. *dups = keys met more than once (then the table is not a valid lookup).
+void JoinDenseRows(const uint64_t *keys, uint64_t n, uint64_t range, uint32_t *table, uint32_t *dups,
+                   cudaStream_t stream);
+void JoinDenseInline(const uint64_t *keys, const void *values, size_t width, uint64_t n, uint64_t range,
+                     uint64_t *table, uint32_t *dups, cudaStream_t stream);
 //! *out = number of positions i > 0 with sorted[i] == sorted[i - 1].
 void CountAdjacentEqual(const uint64_t *sorted, uint64_t n, uint32_t *out, cudaStream_t stream);
 
