@@ -2,6 +2,7 @@
 #include "codegen.hpp"
 
 #include <algorithm>
+#include <mutex>
 #include <cctype>
 #include <map>
 #include <regex>
@@ -1619,6 +1620,54 @@ std::string PipelineCodegen::EmitBatchGroupBy(const GroupBySpec &gb, const Geome
 	o << "\t\t}\n\t\tbase += total;\n\t}\n"
 	  << "\tif (threadIdx.x == 0) ((u64*)a.w[8])[q] = base;\n}\n";
 	return o.str();
+}
+
+std::string SpecKey(const PipelineSpec &spec) {
+	std::ostringstream o;
+	o << "src:";
+	for (auto &sc : spec.sources) {
+		o << sc.name << '/' << static_cast<int>(sc.type) << '/' << sc.nullable << '/' << sc.side << ';';
+	}
+	o << "|cross:" << spec.cross << "|join:" << spec.join << '/' << spec.join_key << '/' << spec.join_inline << "|chain:";
+	for (const PlanNode *n : spec.chain) {
+		o << static_cast<int>(n->op) << '{';
+		for (auto &e : n->expressions) {
+			o << static_cast<int>(e.output_type) << ':' << e.source.size() << ':' << e.source << '(';
+			for (auto &in : e.input_columns) o << in << ',';
+			o << ')';
+		}
+		o << '}';
+	}
+	return o.str();
+}
+
+std::string GroupByKey(const PipelineCodegen::GroupBySpec &gb, bool partitioned) {
+	std::ostringstream o;
+	o << "gb:" << partitioned << "|keys:";
+	for (auto &k : gb.keys) o << k.column << ',';
+	o << "|aggs:";
+	for (auto &a : gb.aggs) {
+		o << static_cast<int>(a.kind) << '/' << a.column << '/' << static_cast<int>(a.input_type) << '/'
+		  << static_cast<int>(a.output_type) << ';';
+	}
+	o << "|db:" << gb.direct_bits << "|bt:" << gb.bucket_threads;
+	return o.str();
+}
+
+std::shared_ptr<const PipelineCodegen> CodegenFor(const PipelineSpec &spec) {
+	static std::mutex mu;
+	static std::map<std::string, std::shared_ptr<const PipelineCodegen>> memo;
+	const std::string key = SpecKey(spec);
+	{
+		std::lock_guard<std::mutex> lock(mu);
+		auto it = memo.find(key);
+		if (it != memo.end()) return it->second;
+	}
+	auto cg = std::make_shared<const PipelineCodegen>(spec);
+	std::lock_guard<std::mutex> lock(mu);
+	if (memo.size() >= 4096) memo.clear();  // bounded: plan shapes seen by one process are few
+	memo.emplace(key, cg);
+	return cg;
 }
 
 } // namespace vgpu

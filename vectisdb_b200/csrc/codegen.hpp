@@ -12,6 +12,7 @@
 // writing ((T*)out)[idx]. The generator rewrites those two access forms into register values.
 #pragma once
 
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -163,6 +164,15 @@ private:
 	std::vector<bool> chain_sources_;      // sources read by the chain itself
 	int expr_count_ = 0;
 };
+
+//! Everything a PipelineSpec contributes to generated code (sources, source kind, the chain's
+//! expressions), as a compact key: equal keys generate equal code.
+std::string SpecKey(const PipelineSpec &spec);
+//! The same for a group-by consumer: key columns, aggregates, strategy and table parameters.
+std::string GroupByKey(const PipelineCodegen::GroupBySpec &gb, bool partitioned);
+//! A code generator for `spec`, shared by every pipeline with the same SpecKey (the chain's nodes are
+//! read only while it is built).
+std::shared_ptr<const PipelineCodegen> CodegenFor(const PipelineSpec &spec);
 
 //! Registers the reference access forms of an expression source: returns the rewritten statement or
 //! throws Error(VGPU_ERR_UNSUPPORTED) when the source uses inputs/out/row/idx any other way.

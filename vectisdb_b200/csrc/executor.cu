@@ -102,7 +102,6 @@ public:
 	Arena &arena() {
 		return arena_;
 	}
-	std::string last_source;
 
 private:
 	struct PipelineInput {
@@ -122,7 +121,7 @@ private:
 	Relation JoinMaterialize(const PlanNode &node, Relation &left, Relation &right);
 	Relation JoinForPipeline(const PlanNode &node, PipelineInput &pin, bool *fused);
 	Relation CrossProduct(const PlanNode &node);
-	void ComputeStats(PipelineInput &pin, PipelineCodegen &cg, const std::vector<int> &cols,
+	void ComputeStats(PipelineInput &pin, const PipelineCodegen &cg, const std::vector<int> &cols,
 	                  std::vector<std::pair<int64_t, int64_t>> &out);
 	void FillArgs(const PipelineInput &pin, KArgsHost &args);
 	uint64_t DirectBuckets(Module &module, const PipelineCodegen::GroupBySpec &gb, const PipelineInput &pin, uint64_t P,
@@ -320,13 +319,15 @@ Executor::PipelineInput Executor::BuildPipeline(const PlanNode &top, std::vector
 
 Relation Executor::Materialize(PipelineInput &pin, const std::vector<int> &out_cols,
                                const std::vector<std::string> &names) {
-	PipelineCodegen cg(pin.spec);
+	auto cgp = CodegenFor(pin.spec);
+	const PipelineCodegen &cg = *cgp;
 	Geometry g;
 	g.block = 256;
 	g.items = 4;
-	std::string src = cg.EmitMaterialize(out_cols, g);
-	last_source = src;
-	auto module = Runtime::Get().modules().GetOrCompile(src);
+	std::string mkey = "mat|" + SpecKey(pin.spec) + "|outs:";
+	for (int c : out_cols) mkey += std::to_string(c) + ",";
+	mkey += "|g:" + std::to_string(g.block) + "x" + std::to_string(g.items);
+	auto module = Runtime::Get().modules().GetOrCompileMemo(mkey, [&] { return cg.EmitMaterialize(out_cols, g); });
 	const uint64_t n = pin.rows;
 	const uint64_t ntiles = (n + g.tile() - 1) / g.tile();
 	const int sms = Runtime::Get().props().sm_count;
@@ -389,7 +390,8 @@ Relation Executor::RunChain(const PlanNode &node) {
 		cur = cur->children[0].get();
 	}
 	PipelineInput pin = BuildPipeline(*cur, chain);
-	PipelineCodegen probe(pin.spec);
+	auto probe_cg = CodegenFor(pin.spec);
+	const PipelineCodegen &probe = *probe_cg;
 	std::vector<int> outs;
 	std::vector<std::string> names;
 	for (size_t i = 0; i < probe.visible().size(); i++) {
@@ -410,7 +412,7 @@ Relation Executor::CrossProduct(const PlanNode &node) {
 	return Materialize(pin, outs, names);
 }
 
-void Executor::ComputeStats(PipelineInput &pin, PipelineCodegen &cg, const std::vector<int> &cols,
+void Executor::ComputeStats(PipelineInput &pin, const PipelineCodegen &cg, const std::vector<int> &cols,
                             std::vector<std::pair<int64_t, int64_t>> &out) {
 	out.assign(cols.size(), {0, 0});
 	std::vector<int> missing;
@@ -430,8 +432,9 @@ void Executor::ComputeStats(PipelineInput &pin, PipelineCodegen &cg, const std::
 	Geometry g;
 	g.block = 256;
 	g.items = 4;
-	std::string src = cg.EmitStats(missing, g);
-	auto module = Runtime::Get().modules().GetOrCompile(src);
+	std::string skey = "stats|" + SpecKey(pin.spec) + "|cols:";
+	for (int c : missing) skey += std::to_string(c) + ",";
+	auto module = Runtime::Get().modules().GetOrCompileMemo(skey, [&] { return cg.EmitStats(missing, g); });
 	int64_t *mm = arena_.AllocT<int64_t>(2 * missing.size());
 	std::vector<int64_t> init(2 * missing.size());
 	for (size_t i = 0; i < missing.size(); i++) {
@@ -557,7 +560,8 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		cur = cur->children[0].get();
 	}
 	PipelineInput pin = BuildPipeline(*cur, chain);
-	PipelineCodegen cg(pin.spec);
+	auto cgp = CodegenFor(pin.spec);
+	const PipelineCodegen &cg = *cgp;
 	if (cg.visible().empty()) {
 		Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_groupby: input operator produced no columns to group");
 	}
@@ -645,10 +649,17 @@ Relation Executor::GroupBy(const PlanNode &node) {
 	if (direct) {
 		Geometry g;
 		g.block = 512;
-		g.items = 4;
-		std::string src = cg.EmitGroupBy(gb, false, g);
-		last_source = src;
-		auto module = Runtime::Get().modules().GetOrCompile(src);
+		// a join source's random lookups are independent per row: more rows per thread, more of them in flight
+		g.items = pin.spec.join ? 8 : 4;
+		if (const char *env = std::getenv("VGPU_GB_DIRECT_ITEMS")) {  // tuning override
+			g.items = std::max(1, std::min(32, std::atoi(env)));
+		}
+		if (const char *env = std::getenv("VGPU_GB_DIRECT_BLOCK")) {  // tuning override
+			g.block = std::max(64, std::min(1024, std::atoi(env)));
+		}
+		const std::string gkey = SpecKey(pin.spec) + "|" + GroupByKey(gb, false) + "|g:" + std::to_string(g.block) + "x" +
+		                         std::to_string(g.items);
+		auto module = Runtime::Get().modules().GetOrCompileMemo(gkey, [&] { return cg.EmitGroupBy(gb, false, g); });
 		uint64_t *fields = arena_.AllocT<uint64_t>(domain * F);
 		uint64_t *count = arena_.AllocT<uint64_t>(1);
 		KArgsHost a;
@@ -734,9 +745,9 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		if (const char *env = std::getenv("VGPU_GB_PART_BLOCK")) {  // tuning override (128..1024)
 			g.block = static_cast<int>(std::min<uint64_t>(1024, std::max<uint64_t>(128, FloorPow2(std::strtoull(env, nullptr, 10)))));
 		}
-		std::string src = cg.EmitGroupBy(gb, true, g);
-		last_source = src;
-		auto module = Runtime::Get().modules().GetOrCompile(src);
+		const std::string gkey = SpecKey(pin.spec) + "|" + GroupByKey(gb, true) + "|g:" + std::to_string(g.block) + "x" +
+		                         std::to_string(g.items);
+		auto module = Runtime::Get().modules().GetOrCompileMemo(gkey, [&] { return cg.EmitGroupBy(gb, true, g); });
 		CUfunction fcount = module->Get("vgpu_gb_part_count");
 		const size_t part_smem = (P + 32) * 4;  // partition counters + per-lane dummies for filtered rows
 		int occ = std::max(1, Runtime::Get().MaxActiveBlocks(fcount, g.block, part_smem));

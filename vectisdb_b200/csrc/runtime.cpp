@@ -353,6 +353,23 @@ bool ReadFile(const std::string &path, std::vector<char> &out) {
 
 } // namespace
 
+std::shared_ptr<Module> ModuleCache::GetOrCompileMemo(const std::string &memo_key,
+                                                      const std::function<std::string()> &source) {
+	{
+		std::lock_guard<std::mutex> lock(mu_);
+		auto it = memo_.find(memo_key);
+		if (it != memo_.end()) {
+			stats_.hits++;
+			return it->second;
+		}
+	}
+	auto module = GetOrCompile(source());
+	std::lock_guard<std::mutex> lock(mu_);
+	if (memo_.size() >= 4096) memo_.clear();
+	memo_[memo_key] = module;
+	return module;
+}
+
 std::shared_ptr<Module> ModuleCache::GetOrCompile(const std::string &source) {
 	auto &rt = Runtime::Get();
 	const std::string arch = rt.arch();

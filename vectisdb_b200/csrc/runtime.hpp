@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <list>
 #include <memory>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -122,10 +123,14 @@ std::vector<char> CompileToCubin(const std::string &source, const std::string &a
 class ModuleCache {
 public:
 	std::shared_ptr<Module> GetOrCompile(const std::string &source);
+	//! The module for `memo_key` (a description that determines the generated source): the source is
+	//! generated and hashed only the first time a key is seen in this process.
+	std::shared_ptr<Module> GetOrCompileMemo(const std::string &memo_key, const std::function<std::string()> &source);
 	vgpu_kernel_cache_stats Stats();
 
 private:
 	std::mutex mu_;
+	std::unordered_map<std::string, std::shared_ptr<Module>> memo_;
 	std::list<std::string> lru_;
 	std::unordered_map<std::string, std::pair<std::shared_ptr<Module>, std::list<std::string>::iterator>> map_;
 	vgpu_kernel_cache_stats stats_ {};
