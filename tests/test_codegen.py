@@ -21,6 +21,7 @@ def test_benchmark_query_kernels_compile(name):
     wl = W.c0(n=64) if name == "c0" else W.c1(n=64)
     src = generate_source(wl.plan, wl.inputs)
     assert "vgpu_gb_direct" in src and "vgpu_gb_bucket" in src and "vgpu_gb_dbucket" in src
+    assert "vgpu_gb_sample" in src and "vgpu_hmap" in src
     assert all(s > 1000 for s in _compile_all(src))
 
 

@@ -736,6 +736,16 @@ int PipelineCodegen::DirectSlotBytes(const GroupBySpec &gb) {
 	return bytes;
 }
 
+int PipelineCodegen::HeavySlotBytes(const GroupBySpec &gb) {
+	int bytes = 4;
+	for (auto &a : gb.aggs) {
+		if (a.column < 0 || a.kind == AggKind::COUNT || a.kind == AggKind::COUNT_STAR) continue;
+		const bool int_sum = (a.kind == AggKind::SUM || a.kind == AggKind::AVG) && !IsFloatType(a.input_type);
+		bytes += int_sum ? 16 : 8;
+	}
+	return bytes;
+}
+
 int PipelineCodegen::RecordStride(const GroupBySpec &gb) const {
 	// Same layout rule as EmitGroupBy: key u64, then each distinct carried value column at its
 	// natural alignment, rounded up to 32 bytes.
@@ -911,6 +921,212 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 	}
 	// part_count / part_scatter args: cb+0 = P, cb+1 = pbits, cb+2 = tiles per CTA,
 	//   cb+3 = counts/offsets (u32, [p * G + cta]), cb+4 = records out.
+	if (dpart && gb.heavy_slots > 0) {
+		// ---- heavy-key variants of the partition passes ----
+		// A partition holds at most one heavy key: hmap[p] = (state index << 16) | the key's slot in
+		// partition p, or ~0 (a slot is below 2^15, so ~0 never matches). Heavy rows fold into the
+		// CTA's partial state of their key; each CTA then writes one partial record per heavy key.
+		// Extra args: cb+5 = hmap (u32 [P]), cb+6 = sample keys (u64 [SC]), cb+7 = sample counts
+		// (u32 [SC]), cb+8 = SC, cb+9 = sampled tile stride, cb+10 = overflow flag (u32*),
+		// cb+11 = heavy keys (u32 [K], mixed keys), cb+12 = heavy key count (u32*).
+		const int K = gb.heavy_slots;
+		const int dbits = gb.direct_bits;
+		const std::string dmask = std::to_string((1u << dbits) - 1) + "u";
+		// per-CTA partial state of each heavy key: 8-byte arrays (FP64 sums, MIN/MAX) then 32-bit arrays
+		// (COUNT, four words per integer SUM)
+		struct HArr {
+			std::string name, type;
+			int bytes;
+		};
+		std::vector<HArr> harr;
+		std::vector<std::string> hkind(gb.aggs.size());
+		for (size_t i = 0; i < gb.aggs.size(); i++) {
+			const auto &ag = gb.aggs[i];
+			if (ag.column < 0 || ag.kind == AggKind::COUNT || ag.kind == AggKind::COUNT_STAR) continue;
+			const std::string is = std::to_string(i);
+			if (ag.kind == AggKind::MIN || ag.kind == AggKind::MAX) {
+				hkind[i] = ag.kind == AggKind::MIN ? "min" : "max";
+				harr.push_back({"HM" + is, "i64", 8});
+			} else if (IsFloatType(ag.input_type)) {
+				hkind[i] = "f64";
+				harr.push_back({"HF" + is, "double", 8});
+			} else {
+				hkind[i] = "int";
+			}
+		}
+		harr.push_back({"HC", "u32", 4});
+		for (size_t i = 0; i < gb.aggs.size(); i++) {
+			if (hkind[i] != "int") continue;
+			for (int w = 0; w < 4; w++) harr.push_back({"HW" + std::to_string(i) + "_" + std::to_string(w), "u32", 4});
+		}
+		// shared layout after the P + 32 counters: hmap [P], heavy keys [K], then the state arrays
+		// (16-byte aligned; the host sizes the launch with the same rule)
+		std::ostringstream hdecl;
+		hdecl << "\tconst u32 hoff = ((P + 32u) * 4u + 15u) & ~15u;\n"
+		      << "\tu32 *vgpu_hmap = (u32*)((char*)vgpu_smem + hoff);\n"
+		      << "\tu32 *vgpu_hkeys = vgpu_hmap + P;\n"
+		      << "\tchar *vgpu_hstate = (char*)vgpu_smem + ((hoff + 4u * P + " << 4 * K << "u + 15u) & ~15u);\n"
+		      << "\tconst u32 nheavy = *(const u32*)a.w[" << cb + 12 << "];\n";
+		uint64_t hbytes = 0;
+		for (auto &ar : harr) {
+			hdecl << "\t" << ar.type << " *" << ar.name << " = (" << ar.type << "*)(vgpu_hstate + " << hbytes << ");\n";
+			hbytes += static_cast<uint64_t>(K) * ar.bytes;
+		}
+		auto heavy_load = [&](bool with_state) {
+			std::ostringstream r;
+			r << "\tfor (u32 p = threadIdx.x; p < P; p += blockDim.x) vgpu_hmap[p] = ((const u32*)a.w[" << cb + 5
+			  << "])[p];\n"
+			  << "\tfor (u32 h = threadIdx.x; h < nheavy; h += blockDim.x) {\n"
+			  << "\t\tvgpu_hkeys[h] = ((const u32*)a.w[" << cb + 11 << "])[h];\n";
+			if (with_state) {
+				for (auto &ar : harr) {
+					std::string init = "0";
+					if (ar.name.rfind("HM", 0) == 0) {
+						const int ai = std::stoi(ar.name.substr(2));
+						init = hkind[ai] == "min" ? "0x7fffffffffffffffLL" : "(-0x7fffffffffffffffLL - 1)";
+					}
+					r << "\t\t" << ar.name << "[h] = (" << ar.type << ")" << init << ";\n";
+				}
+			}
+			r << "\t}\n";
+			return r.str();
+		};
+		const std::string mixed = "vgpu_dmix(a, " + pack.str() + ")";
+		// a kept row's heavy-state index, or -1
+		const std::string heavy_of = "((vgpu_hmap[(u32)(k0 >> " + std::to_string(dbits) + ")] & 0xffffu) == ((u32)k0 & " +
+		                             dmask + ") ? (int)(vgpu_hmap[(u32)(k0 >> " + std::to_string(dbits) +
+		                             ")] >> 16) : -1)";
+		// sample: one tile per CTA at a stride, counts of the mixed keys of the kept rows
+		o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_gb_sample(KArgs a) {\n"
+		  << kKernelHead
+		  << "\tu64 *skeys = (u64*)a.w[" << cb + 6 << "];\n\tu32 *scount = (u32*)a.w[" << cb + 7 << "];\n"
+		  << "\tconst u32 SC = (u32)a.w[" << cb + 8 << "];\n"
+		  << "\tconst u64 tile = (u64)blockIdx.x * a.w[" << cb + 9 << "];\n"
+		  << LoadBlock(g, needed, true) << item_head << chain_code_ << "\t\tif (keep) {\n"
+		  << "\t\t\tconst u64 k = " << mixed << ";\n"
+		  << "\t\t\tu32 s = (u32)mix64(k) & (SC - 1);\n"
+		  << "\t\t\t#pragma unroll 1\n\t\t\tfor (int i = 0; i < 32; ++i) {\n"
+		  << "\t\t\t\tconst u64 prev = atomicCAS((unsigned long long*)&skeys[s], ~0ull, k);\n"
+		  << "\t\t\t\tif (prev == ~0ull || prev == k) { atomicAdd(&scount[s], 1u); break; }\n"
+		  << "\t\t\t\ts = (s + 1) & (SC - 1);\n\t\t\t}\n"
+		  << "\t\t}\n\t\t}\n}\n\n";
+		// count: heavy rows are not counted; every CTA reserves one partial record per heavy key
+		o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_gb_part_count(KArgs a) {\n"
+		  << kKernelHead << "\textern __shared__ __align__(16) u32 vgpu_smem[];\n\tu32 *vgpu_hist = vgpu_smem;\n"
+		  << "\tconst u32 P = (u32)a.w[" << cb << "]; const int pbits = (int)a.w[" << cb + 1 << "]; (void)pbits;\n"
+		  << "\tconst u64 tpc = a.w[" << cb + 2 << "];\n"
+		  << hdecl.str()
+		  << "\tfor (u32 p = threadIdx.x; p < P; p += " << g.block << ") vgpu_hist[p] = 0;\n"
+		  << heavy_load(false) << "\t__syncthreads();\n"
+		  << tile_loop_head
+		  << "\tconst u64 t_end = (blockIdx.x + 1) * tpc < ntiles ? (blockIdx.x + 1) * tpc : ntiles;\n"
+		  << "\tfor (u64 tile = blockIdx.x * tpc; tile < t_end; ++tile) {\n"
+		  << LoadBlock(g, needed, true) << item_head << chain_code_ << "\t\tif (keep) {\n"
+		  << "\t\t\tconst u64 k0 = " << mixed << ";\n"
+		  << "\t\t\tif (" << heavy_of << " < 0) atomicAdd(&vgpu_hist[(u32)(k0 >> " << dbits << ")], 1u);\n"
+		  << "\t\t}\n\t\t}\n\t}\n\t__syncthreads();\n"
+		  << "\tfor (u32 h = threadIdx.x; h < nheavy; h += blockDim.x) atomicAdd(&vgpu_hist[vgpu_hkeys[h] >> " << dbits
+		  << "], 1u);\n"
+		  << "\t__syncthreads();\n"
+		  << "\tu32 *counts = (u32*)a.w[" << cb + 3 << "];\n"
+		  << "\tfor (u32 p = threadIdx.x; p < P; p += " << g.block
+		  << ") counts[(u64)p * gridDim.x + blockIdx.x] = vgpu_hist[p];\n}\n\n";
+		// scatter: heavy rows fold into the CTA's partial state, the rest are records; then one partial
+		// record per heavy key (flag bit 31 of the key word, row count in the next word, each aggregate's
+		// partial state in its value column's slot)
+		std::ostringstream hupd;
+		hupd << "\t\t\t\tatomicAdd(&HC[h], 1u);\n";
+		for (size_t i = 0; i < gb.aggs.size(); i++) {
+			if (hkind[i].empty()) continue;
+			const std::string is = std::to_string(i);
+			const std::string v = visible_[gb.aggs[i].column].value;
+			if (hkind[i] == "int") {
+				hupd << "\t\t\t\t{ const i64 x_ = (i64)(" << v << "); atomic_add_i128_u32x4(&HW" << is << "_0[h], &HW" << is
+				     << "_1[h], &HW" << is << "_2[h], &HW" << is << "_3[h], (u64)x_, x_ < 0 ? -1 : 0); }\n";
+			} else if (hkind[i] == "f64") {
+				hupd << "\t\t\t\tatomicAdd(&HF" << is << "[h], (double)(" << v << "));\n";
+			} else {
+				hupd << "\t\t\t\tatomic_" << hkind[i] << "_i64(&HM" << is << "[h], (i64)(" << v << "));\n";
+			}
+		}
+		std::ostringstream hflush;
+		hflush << "\t\t\tu32 rw[" << RW << "];\n"
+		       << "\t\t\t#pragma unroll\n\t\t\tfor (int q = 0; q < " << RW << "; ++q) rw[q] = 0u;\n"
+		       << "\t\t\trw[0] = k | 0x80000000u; rw[1] = HC[h];\n";
+		for (auto &sl : rec) {
+			int ai = -1;
+			for (size_t i = 0; i < gb.aggs.size(); i++) {
+				if (!hkind[i].empty() && gb.aggs[i].column == sl.col) ai = static_cast<int>(i);
+			}
+			if (ai < 0) continue;
+			const std::string is = std::to_string(ai);
+			const int wi = sl.offset / 4;
+			std::string bits;
+			if (hkind[ai] == "int") {
+				bits = "((u64)HW" + is + "_0[h] | ((u64)HW" + is + "_1[h] << 32))";
+				// the partial travels as a 64-bit value: a sum outside that range flags the launch,
+				// whose caller then runs the query without pre-aggregation
+				hflush << "\t\t\tif (HW" << is << "_2[h] != ((HW" << is << "_1[h] & 0x80000000u) ? 0xffffffffu : 0u) || HW"
+				       << is << "_3[h] != HW" << is << "_2[h]) atomicOr((u32*)a.w[" << cb + 10 << "], 1u);\n";
+			} else if (hkind[ai] == "f64") {
+				bits = "(u64)__double_as_longlong(HF" + is + "[h])";
+			} else {
+				bits = "(u64)HM" + is + "[h]";
+			}
+			hflush << "\t\t\t{ const u64 b = " << bits << "; rw[" << wi << "] = (u32)b; rw[" << wi + 1
+			       << "] = (u32)(b >> 32); }\n";
+		}
+		o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_gb_part_scatter(KArgs a) {\n"
+		  << kKernelHead << "\textern __shared__ __align__(16) u32 vgpu_smem[];\n\tu32 *vgpu_cursor = vgpu_smem;\n"
+		  << "\tconst u32 P = (u32)a.w[" << cb << "]; const int pbits = (int)a.w[" << cb + 1 << "]; (void)pbits;\n"
+		  << "\tconst u64 tpc = a.w[" << cb + 2 << "];\n"
+		  << "\tconst u32 *offsets = (const u32*)a.w[" << cb + 3 << "];\n"
+		  << "\tchar *rec_out = (char*)a.w[" << cb + 4 << "];\n"
+		  << hdecl.str()
+		  << "\tfor (u32 p = threadIdx.x; p < P; p += " << g.block
+		  << ") vgpu_cursor[p] = offsets[(u64)p * gridDim.x + blockIdx.x];\n"
+		  << heavy_load(true) << "\t__syncthreads();\n"
+		  << tile_loop_head
+		  << "\tconst u64 t_end = (blockIdx.x + 1) * tpc < ntiles ? (blockIdx.x + 1) * tpc : ntiles;\n"
+		  << "\tfor (u64 tile = blockIdx.x * tpc; tile < t_end; ++tile) {\n"
+		  << LoadBlock(g, needed, true)
+		  << "\t\tu32 vgpu_pos[" << g.items << "];\n\t\tint vgpu_hv[" << g.items << "];\n"
+		  << item_head << chain_code_
+		  << "\t\tconst u64 k0 = " << mixed << ";\n"
+		  << "\t\tvgpu_hv[r] = keep ? " << heavy_of << " : -1;\n"
+		  << "\t\tvgpu_pos[r] = atomicAdd(&vgpu_cursor[keep && vgpu_hv[r] < 0 ? (u32)(k0 >> " << dbits
+		  << ") : P + (threadIdx.x & 31u)], 1u);\n"
+		  << "\t\t}\n"
+		  << item_head << chain_code_ << "\t\tif (keep) {\n"
+		  << "\t\t\tconst int h = vgpu_hv[r];\n"
+		  << "\t\t\tif (h >= 0) {\n" << hupd.str() << "\t\t\t} else {\n"
+		  << "\t\t\tconst u64 key = " << key_of_pack << ";\n"
+		  << "\t\t\tconst u32 pos = vgpu_pos[r];\n"
+		  << "\t\t\tu32 rw[" << RW << "];\n"
+		  << "\t\t\t#pragma unroll\n\t\t\tfor (int q = 0; q < " << RW << "; ++q) rw[q] = 0u;\n"
+		  << "\t\t\trw[0] = (u32)key; rw[1] = (u32)(key >> 32);\n";
+		for (auto &sl : rec) {
+			const auto &col = visible_[sl.col];
+			const int wi = sl.offset / 4, sh = (sl.offset % 4) * 8;
+			o << "\t\t\t{ const u64 b = to_bits<" << CudaTypeName(col.type) << ">(" << col.value << ");\n";
+			if (sl.width == 8) {
+				o << "\t\t\t  rw[" << wi << "] = (u32)b; rw[" << wi + 1 << "] = (u32)(b >> 32); }\n";
+			} else if (sl.width == 4) {
+				o << "\t\t\t  rw[" << wi << "] = (u32)b; }\n";
+			} else {
+				o << "\t\t\t  rw[" << wi << "] |= ((u32)b & " << (sl.width == 2 ? "0xffffu" : "0xffu") << ") << " << sh
+				  << "; }\n";
+			}
+		}
+		o << "\t\t\tstore_record<" << RW << ">(rec_out + (u64)pos * " << RS << ", rw);\n"
+		  << "\t\t\t}\n\t\t}\n\t\t}\n\t}\n"
+		  << "\t__syncthreads();\n"
+		  << "\tfor (u32 h = threadIdx.x; h < nheavy; h += blockDim.x) {\n"
+		  << "\t\tconst u32 k = vgpu_hkeys[h];\n"
+		  << "\t\tconst u32 pos = atomicAdd(&vgpu_cursor[k >> " << dbits << "], 1u);\n"
+		  << "\t\t{\n" << hflush.str()
+		  << "\t\t\tstore_record<" << RW << ">(rec_out + (u64)pos * " << RS << ", rw);\n\t\t}\n\t}\n}\n\n";
+	} else {
 	o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_gb_part_count(KArgs a) {\n"
 	  << kKernelHead << "\textern __shared__ __align__(16) u32 vgpu_hist[];\n"
 	  << "\tconst u32 P = (u32)a.w[" << cb << "]; const int pbits = (int)a.w[" << cb + 1 << "];\n"
@@ -965,6 +1181,8 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 	}
 	o << "\t\t\tstore_record<" << RW << ">(rec_out + (u64)pos * " << RS << ", rw);\n"
 	  << "\t\t}\n\t\t}\n\t}\n}\n\n";
+
+	}
 
 	// bucket: args cb+0 = P, cb+1 = C (smem table slots), cb+2 = offsets (u32 [p*G]), cb+3 = G,
 	//   cb+4 = total ptr (u32*), cb+5 = records, then W = cb+6: work counter (u32*), W+1 overflow flags
@@ -1205,9 +1423,16 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		  << "\t\t#pragma unroll\n\t\tfor (int q = 0; q < 4; ++q) {\n"
 		  << "\t\t\tconst u64 i = base + 32ull * q + lane;\n"
 		  << "\t\t\tload_record<" << RW << ">(recs + (i < end ? i : end - 1) * " << RS << ", rw[q]);\n\t\t}\n"
-		  << "\t\t#pragma unroll\n\t\tfor (int q = 0; q < 4; ++q) {\n"
-		  << "\t\t\tconst bool valid = base + 32ull * q + lane < end;\n"
-		  << "\t\t\tconst u32 slot = valid ? (rw[q][0] & " << D - 1 << "u) : 0xffffffffu;\n";
+		  << "\t\t#pragma unroll\n\t\tfor (int q = 0; q < 4; ++q) {\n";
+		if (gb.heavy_slots > 0) {
+			// partial records of heavy keys: bit 31 of the key word, row count in the next word (0: the
+			// key had no rows in that CTA, the record holds identities and is skipped)
+			o << "\t\t\tconst bool part_rec = (rw[q][0] & 0x80000000u) != 0u;\n"
+			  << "\t\t\tconst bool valid = base + 32ull * q + lane < end && !(part_rec && rw[q][1] == 0u);\n";
+		} else {
+			o << "\t\t\tconst bool valid = base + 32ull * q + lane < end;\n";
+		}
+		o << "\t\t\tconst u32 slot = valid ? (rw[q][0] & " << D - 1 << "u) : 0xffffffffu;\n";
 		for (size_t i = 0; i < gb.aggs.size(); i++) {
 			const auto &ag = gb.aggs[i];
 			if (ag.column >= 0 && ag.kind != AggKind::COUNT && ag.kind != AggKind::COUNT_STAR) {
@@ -1215,7 +1440,12 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 				  << rec_value(ag.column, "rw[q]") << ";\n";
 			}
 		}
-		o << gdecl.str()
+		std::string gd = gdecl.str();
+		if (gb.heavy_slots > 0) {
+			const std::string one = "u32 gc = valid ? 1u : 0u;";
+			gd.replace(gd.find(one), one.size(), "u32 gc = valid ? (part_rec ? rw[q][1] : 1u) : 0u;");
+		}
+		o << gd
 		  << "\t\t\tconst u32 peers = __match_any_sync(0xffffffffu, slot);\n"
 		  << "\t\t\tbool leader = true;\n"
 		  << "\t\t\tfor (u32 todo = __ballot_sync(0xffffffffu, __popc(peers) >= 4); todo;) {\n"
@@ -1650,7 +1880,7 @@ std::string GroupByKey(const PipelineCodegen::GroupBySpec &gb, bool partitioned)
 		o << static_cast<int>(a.kind) << '/' << a.column << '/' << static_cast<int>(a.input_type) << '/'
 		  << static_cast<int>(a.output_type) << ';';
 	}
-	o << "|db:" << gb.direct_bits << "|bt:" << gb.bucket_threads;
+	o << "|db:" << gb.direct_bits << "|bt:" << gb.bucket_threads << "|hv:" << gb.heavy_slots;
 	return o.str();
 }
 

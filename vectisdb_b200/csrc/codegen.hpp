@@ -122,6 +122,11 @@ public:
 		int direct_bits = 0;
 		int key_bits = 0;
 		uint64_t key_mult = 1, key_mult_inv = 1;
+		// Heavy-key pre-aggregation (direct-partitioned only, > 0 = the most heavy keys, at most one
+		// per partition): rows of the query's most frequent keys are folded into per-CTA shared
+		// partial states during the scatter and leave as one partial record per key and CTA instead
+		// of one record per row.
+		int heavy_slots = 0;
 	};
 
 	//! Group-by kernels (see executor for the argument layout), all in one translation unit:
@@ -146,6 +151,9 @@ public:
 	static int StateWords(const GroupBySpec &gb);
 	//! Shared-memory bytes per slot of a direct-partitioned table (32-bit count and sum words).
 	static int DirectSlotBytes(const GroupBySpec &gb);
+	//! Shared-memory bytes of one heavy key's partial state in the heavy partition passes (row count,
+	//! partial state of every aggregate).
+	static int HeavySlotBytes(const GroupBySpec &gb);
 	//! Byte stride of one partitioned-intermediate record (packed key + carried values, 32-byte multiple).
 	int RecordStride(const GroupBySpec &gb) const;
 

@@ -203,11 +203,14 @@ std::string GenerateSourceText(const PlanNode &plan, const std::vector<vgpu_colu
 	spec_dp.key_mult = (0x9e3779b97f4a7c15ull & (shift >= 64 ? ~0ull : (1ull << shift) - 1)) | 1ull;
 	spec_dp.key_mult_inv = 1;
 	spec_dp.bucket_threads = 1024;
+	// ... and its heavy-key variant (sampling kernel, pre-aggregating partition passes)
+	PipelineCodegen::GroupBySpec spec_hv = spec_dp;
+	spec_hv.heavy_slots = 512;
 	// Separate translation units, separated by a marker line: direct, partitioned, key statistics,
-	// direct-partitioned.
+	// direct-partitioned, direct-partitioned with heavy keys.
 	return cg.EmitGroupBy(spec_gb, false, g) + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_gb, true, g) +
 	       "\n//@@VGPU_TU@@\n" + cg.EmitStats(key_columns, gs) + "\n//@@VGPU_TU@@\n" +
-	       cg.EmitGroupBy(spec_dp, true, g);
+	       cg.EmitGroupBy(spec_dp, true, g) + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_hv, true, g);
 }
 
 } // namespace vgpu

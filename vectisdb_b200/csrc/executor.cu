@@ -15,6 +15,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
+#include <map>
 #include <set>
 
 #include "column_cache.hpp"
@@ -129,6 +131,25 @@ private:
 	                       uint64_t RS, Relation &out, int out_words, int threads);
 	uint64_t ReadU64(const void *dev);
 	uint32_t ReadU32(const void *dev);
+	//! Heavy keys chosen for the partition passes of a direct-partitioned group-by (no module: none).
+	//! The selection stays on the device: hmap, the key list and its length are kernel inputs.
+	struct HeavyPlan {
+		std::shared_ptr<Module> module;  // the heavy variant of the group-by kernels
+		uint32_t *hmap = nullptr;        // [P] (state index << 16) | slot, or ~0
+		uint32_t *keys = nullptr;        // [max_keys] mixed keys
+		uint32_t *count = nullptr;       // selected keys (<= max_keys)
+		uint32_t *overflow = nullptr;    // set when an integer partial sum leaves 64 bits
+		uint32_t max_keys = 0;
+		uint64_t state_bytes = 0;        // per heavy key
+		size_t smem(uint64_t P) const {
+			const uint64_t hoff = ((P + 32) * 4 + 15) & ~uint64_t(15);
+			const uint64_t soff = (hoff + 4 * P + 4ull * max_keys + 15) & ~uint64_t(15);
+			return static_cast<size_t>(soff + max_keys * state_bytes);
+		}
+	};
+	using GroupByCompiler = std::function<std::shared_ptr<Module>(const PipelineCodegen::GroupBySpec &)>;
+	HeavyPlan PlanHeavy(const PipelineCodegen::GroupBySpec &gb, const PipelineCodegen &cg, const PipelineInput &pin,
+	                    const GroupByCompiler &compile, const Geometry &g, int cb, uint64_t P, uint64_t ntiles);
 
 	const std::vector<vgpu_column> &inputs_;
 	ExecOptions options_;
@@ -745,153 +766,243 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		if (const char *env = std::getenv("VGPU_GB_PART_BLOCK")) {  // tuning override (128..1024)
 			g.block = static_cast<int>(std::min<uint64_t>(1024, std::max<uint64_t>(128, FloorPow2(std::strtoull(env, nullptr, 10)))));
 		}
-		const std::string gkey = SpecKey(pin.spec) + "|" + GroupByKey(gb, true) + "|g:" + std::to_string(g.block) + "x" +
-		                         std::to_string(g.items);
-		auto module = Runtime::Get().modules().GetOrCompileMemo(gkey, [&] { return cg.EmitGroupBy(gb, true, g); });
-		CUfunction fcount = module->Get("vgpu_gb_part_count");
-		const size_t part_smem = (P + 32) * 4;  // partition counters + per-lane dummies for filtered rows
-		int occ = std::max(1, Runtime::Get().MaxActiveBlocks(fcount, g.block, part_smem));
-		occ = std::min(occ, std::max(1, Runtime::Get().MaxActiveBlocks(module->Get("vgpu_gb_part_scatter"), g.block, part_smem)));
-		if (const char *env = std::getenv("VGPU_GB_PART_OCC")) {  // tuning override: CTAs per SM
-			occ = std::min(occ, std::max(1, std::atoi(env)));
-		}
+		auto compile = [&](const PipelineCodegen::GroupBySpec &spec) {
+			const std::string gkey = SpecKey(pin.spec) + "|" + GroupByKey(spec, true) + "|g:" + std::to_string(g.block) +
+			                         "x" + std::to_string(g.items);
+			return Runtime::Get().modules().GetOrCompileMemo(gkey, [&] { return cg.EmitGroupBy(spec, true, g); });
+		};
 		const uint64_t ntiles = (n + g.tile() - 1) / g.tile();
-		const uint64_t G = std::max<uint64_t>(1, std::min<uint64_t>(ntiles, uint64_t(props.sm_count) * occ));
-		const uint64_t tpc = (ntiles + G - 1) / G;
 		if (n >= (1ull << 32)) Fail(VGPU_ERR_UNSUPPORTED, "gpu_groupby: more than 2^32 input rows");
-		uint32_t *offsets = arena_.AllocT<uint32_t>(P * G);
-		uint32_t *total = arena_.AllocT<uint32_t>(1);
 		// Records of the partitioned intermediate: packed key + carried values, RS bytes each.
 		const uint64_t RS = static_cast<uint64_t>(cg.RecordStride(gb));
-		KArgsHost a;
-		FillArgs(pin, a);
-		SetKeyWords(a, gb);
-		a.Set(cb, P);
-		a.Set(cb + 1, static_cast<uint64_t>(pbits));
-		a.Set(cb + 2, tpc);
-		a.SetPtr(cb + 3, offsets);
-		LaunchGenerated(*module, "vgpu_gb_part_count", static_cast<unsigned>(G), g.block, part_smem, stream_, a, in_bytes, n);
-		kern::ExclusiveScanU32(offsets, offsets, P * G, total, arena_);
-		char *records = static_cast<char *>(arena_.Alloc(n * RS));
-		a.SetPtr(cb + 4, records);
-		LaunchGenerated(*module, "vgpu_gb_part_scatter", static_cast<unsigned>(G), g.block, part_smem, stream_, a, in_bytes, n);
-		if (gb.direct_bits > 0) {
-			groups = DirectBuckets(*module, gb, pin, P, G, offsets, total, records, n, RS, out, out_words, T1);
-			for (auto &c : out) c.rows = groups;
-			return out;
-		}
-		// bucket tables. control: [0] work counter, [1] overflow count, [2] retry count, [3] retry work
-		// counter, [4, 4+P) overflow flags, [4+P, 4+2P) retry list.
-		const int W = cb + 6;
-		const int L = W + 4 + out_words;
-		uint32_t *control = arena_.AllocT<uint32_t>(4 + 2 * P);
-		uint64_t *out_count = arena_.AllocT<uint64_t>(1);
-		VGPU_CUDA(cudaMemsetAsync(control, 0, (4 + 2 * P) * 4, stream_));
-		VGPU_CUDA(cudaMemsetAsync(out_count, 0, 8, stream_));
-		KArgsHost b;
-		FillArgs(pin, b);
-		SetKeyWords(b, gb);
-		b.Set(cb, P);
-		b.Set(cb + 1, C);
-		b.SetPtr(cb + 2, offsets);
-		b.Set(cb + 3, G);
-		b.SetPtr(cb + 4, total);
-		b.SetPtr(cb + 5, records);
-		b.SetPtr(W, control);           // work counter
-		b.SetPtr(W + 1, control + 4);   // overflow flags [P]
-		b.SetPtr(W + 2, control + 1);   // overflow count
-		b.SetPtr(W + 3, out_count);
-		for (int w = 0; w < out_words; w++) b.SetPtr(W + 4 + w, out[w].data);
-		b.SetPtr(L + 5, control + 4 + P);  // retry list
-		b.SetPtr(L + 6, control + 2);      // retry count
-		b.SetPtr(L + 7, control + 3);      // retry work counter
-		b.Set(L + 8, C2);
-		const uint64_t part_bytes = n * RS;
-		// VGPU_DEBUG_BUCKET=<file>: per-partition rows, groups and cycle counts of the bucket pass.
-		const char *debug_path = std::getenv("VGPU_DEBUG_BUCKET");
-		uint64_t *debug = nullptr;
-		if (debug_path) {
-			debug = arena_.AllocT<uint64_t>(P * 8);
-			VGPU_CUDA(cudaMemsetAsync(debug, 0, P * 64, stream_));
-			b.SetWord(127, reinterpret_cast<uint64_t>(debug));
-		}
-		{
-			const size_t smem1 = static_cast<size_t>(slot_bytes * C);
-			CUfunction fb = module->Get("vgpu_gb_bucket");
-			const int occ1 = std::max(1, Runtime::Get().MaxActiveBlocks(fb, T1, smem1));
-			const unsigned grid1 = static_cast<unsigned>(std::min<uint64_t>(P, uint64_t(props.sm_count) * occ1));
-			LaunchGenerated(*module, "vgpu_gb_bucket", grid1, T1, smem1, stream_, b, part_bytes, n);
-		}
-		{
-			const size_t smem2 = static_cast<size_t>(slot_bytes * C2);
-			CUfunction fr = module->Get("vgpu_gb_bucket_retry");
-			const int occ2 = std::max(1, Runtime::Get().MaxActiveBlocks(fr, 512, smem2));
-			LaunchGenerated(*module, "vgpu_gb_bucket_retry", static_cast<unsigned>(props.sm_count * occ2), 512, smem2,
-			                stream_, b, 0, 0);
-		}
-		if (debug) {
-			std::vector<uint64_t> h(P * 8);
-			VGPU_CUDA(cudaMemcpyAsync(h.data(), debug, P * 64, cudaMemcpyDeviceToHost, stream_));
-			VGPU_CUDA(cudaStreamSynchronize(stream_));
-			if (FILE *f = std::fopen(debug_path, "w")) {
-				for (uint64_t p = 0; p < P; p++) {
-					std::fprintf(f, "%llu %llu %llu %llu %llu %llu %llu\n", (unsigned long long)p,
-					             (unsigned long long)h[p * 8], (unsigned long long)h[p * 8 + 1],
-					             (unsigned long long)h[p * 8 + 2], (unsigned long long)h[p * 8 + 3],
-					             (unsigned long long)h[p * 8 + 4], (unsigned long long)h[p * 8 + 5]);
+		const size_t part_smem = (P + 32) * 4;  // partition counters + per-lane dummies for filtered rows
+		// Heavy-key pre-aggregation (direct-partitioned): a sample of tiles finds the most frequent keys,
+		// whose rows the partition passes fold into per-CTA shared partial states; each CTA then writes
+		// one partial record per such key instead of one record per row.
+		HeavyPlan heavy = PlanHeavy(gb, cg, pin, compile, g, cb, P, ntiles);
+		for (int attempt = 0;; ++attempt) {
+			const bool use_heavy = heavy.module && attempt == 0;
+			auto module = use_heavy ? heavy.module : compile(gb);
+			const size_t smem = use_heavy ? heavy.smem(P) : part_smem;
+			CUfunction fcount = module->Get("vgpu_gb_part_count");
+			int occ = std::max(1, Runtime::Get().MaxActiveBlocks(fcount, g.block, smem));
+			occ = std::min(occ, std::max(1, Runtime::Get().MaxActiveBlocks(module->Get("vgpu_gb_part_scatter"), g.block, smem)));
+			if (const char *env = std::getenv("VGPU_GB_PART_OCC")) {  // tuning override: CTAs per SM
+				occ = std::min(occ, std::max(1, std::atoi(env)));
+			}
+			const uint64_t G = std::max<uint64_t>(1, std::min<uint64_t>(ntiles, uint64_t(props.sm_count) * occ));
+			const uint64_t tpc = (ntiles + G - 1) / G;
+			// every CTA writes one partial record per heavy key
+			const uint64_t n_rec = n + (use_heavy ? G * heavy.max_keys : 0);
+			if (n_rec >= (1ull << 32)) Fail(VGPU_ERR_UNSUPPORTED, "gpu_groupby: more than 2^32 partition records");
+			uint32_t *offsets = arena_.AllocT<uint32_t>(P * G);
+			uint32_t *total = arena_.AllocT<uint32_t>(1);
+			KArgsHost a;
+			FillArgs(pin, a);
+			SetKeyWords(a, gb);
+			a.Set(cb, P);
+			a.Set(cb + 1, static_cast<uint64_t>(pbits));
+			a.Set(cb + 2, tpc);
+			a.SetPtr(cb + 3, offsets);
+			if (use_heavy) {
+				a.SetPtr(cb + 5, heavy.hmap);
+				a.SetPtr(cb + 10, heavy.overflow);
+				a.SetPtr(cb + 11, heavy.keys);
+				a.SetPtr(cb + 12, heavy.count);
+			}
+			LaunchGenerated(*module, "vgpu_gb_part_count", static_cast<unsigned>(G), g.block, smem, stream_, a, in_bytes, n);
+			kern::ExclusiveScanU32(offsets, offsets, P * G, total, arena_);
+			char *records = static_cast<char *>(arena_.Alloc(n_rec * RS));
+			a.SetPtr(cb + 4, records);
+			LaunchGenerated(*module, "vgpu_gb_part_scatter", static_cast<unsigned>(G), g.block, smem, stream_, a, in_bytes, n);
+			if (gb.direct_bits > 0) {
+				groups = DirectBuckets(*module, gb, pin, P, G, offsets, total, records, n_rec, RS, out, out_words, T1);
+				if (use_heavy && ReadU32(heavy.overflow) != 0) continue;  // a partial sum left 64 bits: redo plainly
+				for (auto &c : out) c.rows = groups;
+				return out;
+			}
+			// bucket tables. control: [0] work counter, [1] overflow count, [2] retry count, [3] retry work
+			// counter, [4, 4+P) overflow flags, [4+P, 4+2P) retry list.
+			const int W = cb + 6;
+			const int L = W + 4 + out_words;
+			uint32_t *control = arena_.AllocT<uint32_t>(4 + 2 * P);
+			uint64_t *out_count = arena_.AllocT<uint64_t>(1);
+			VGPU_CUDA(cudaMemsetAsync(control, 0, (4 + 2 * P) * 4, stream_));
+			VGPU_CUDA(cudaMemsetAsync(out_count, 0, 8, stream_));
+			KArgsHost b;
+			FillArgs(pin, b);
+			SetKeyWords(b, gb);
+			b.Set(cb, P);
+			b.Set(cb + 1, C);
+			b.SetPtr(cb + 2, offsets);
+			b.Set(cb + 3, G);
+			b.SetPtr(cb + 4, total);
+			b.SetPtr(cb + 5, records);
+			b.SetPtr(W, control);           // work counter
+			b.SetPtr(W + 1, control + 4);   // overflow flags [P]
+			b.SetPtr(W + 2, control + 1);   // overflow count
+			b.SetPtr(W + 3, out_count);
+			for (int w = 0; w < out_words; w++) b.SetPtr(W + 4 + w, out[w].data);
+			b.SetPtr(L + 5, control + 4 + P);  // retry list
+			b.SetPtr(L + 6, control + 2);      // retry count
+			b.SetPtr(L + 7, control + 3);      // retry work counter
+			b.Set(L + 8, C2);
+			const uint64_t part_bytes = n * RS;
+			// VGPU_DEBUG_BUCKET=<file>: per-partition rows, groups and cycle counts of the bucket pass.
+			const char *debug_path = std::getenv("VGPU_DEBUG_BUCKET");
+			uint64_t *debug = nullptr;
+			if (debug_path) {
+				debug = arena_.AllocT<uint64_t>(P * 8);
+				VGPU_CUDA(cudaMemsetAsync(debug, 0, P * 64, stream_));
+				b.SetWord(127, reinterpret_cast<uint64_t>(debug));
+			}
+			{
+				const size_t smem1 = static_cast<size_t>(slot_bytes * C);
+				CUfunction fb = module->Get("vgpu_gb_bucket");
+				const int occ1 = std::max(1, Runtime::Get().MaxActiveBlocks(fb, T1, smem1));
+				const unsigned grid1 = static_cast<unsigned>(std::min<uint64_t>(P, uint64_t(props.sm_count) * occ1));
+				LaunchGenerated(*module, "vgpu_gb_bucket", grid1, T1, smem1, stream_, b, part_bytes, n);
+			}
+			{
+				const size_t smem2 = static_cast<size_t>(slot_bytes * C2);
+				CUfunction fr = module->Get("vgpu_gb_bucket_retry");
+				const int occ2 = std::max(1, Runtime::Get().MaxActiveBlocks(fr, 512, smem2));
+				LaunchGenerated(*module, "vgpu_gb_bucket_retry", static_cast<unsigned>(props.sm_count * occ2), 512, smem2,
+				                stream_, b, 0, 0);
+			}
+			if (debug) {
+				std::vector<uint64_t> h(P * 8);
+				VGPU_CUDA(cudaMemcpyAsync(h.data(), debug, P * 64, cudaMemcpyDeviceToHost, stream_));
+				VGPU_CUDA(cudaStreamSynchronize(stream_));
+				if (FILE *f = std::fopen(debug_path, "w")) {
+					for (uint64_t p = 0; p < P; p++) {
+						std::fprintf(f, "%llu %llu %llu %llu %llu %llu %llu\n", (unsigned long long)p,
+						             (unsigned long long)h[p * 8], (unsigned long long)h[p * 8 + 1],
+						             (unsigned long long)h[p * 8 + 2], (unsigned long long)h[p * 8 + 3],
+						             (unsigned long long)h[p * 8 + 4], (unsigned long long)h[p * 8 + 5]);
+					}
+					std::fclose(f);
 				}
-				std::fclose(f);
 			}
+			const uint32_t overflowed = ReadU32(control + 1);
+			if (overflowed > 0) {
+				// Partitions with more distinct keys than a shared-memory table holds: redo them with a
+				// global-memory table sized from the partition's row count.
+				std::vector<uint32_t> flags(P), offs(P * G);
+				uint32_t total_rows = ReadU32(total);
+				VGPU_CUDA(cudaMemcpyAsync(flags.data(), control + 4, P * 4, cudaMemcpyDeviceToHost, stream_));
+				VGPU_CUDA(cudaMemcpyAsync(offs.data(), offsets, P * G * 4, cudaMemcpyDeviceToHost, stream_));
+				VGPU_CUDA(cudaStreamSynchronize(stream_));
+				std::vector<uint32_t> list, caps;
+				std::vector<uint64_t> tab_off;
+				uint64_t words = 0;
+				for (uint64_t p = 0; p < P; p++) {
+					if (!flags[p]) continue;
+					const uint32_t start = offs[p * G];
+					const uint32_t end = p + 1 < P ? offs[(p + 1) * G] : total_rows;
+					const uint64_t cap = NextPow2(std::max<uint64_t>(64, 2ull * (end - start)));
+					list.push_back(static_cast<uint32_t>(p));
+					caps.push_back(static_cast<uint32_t>(cap));
+					tab_off.push_back(words);
+					words += cap * (1 + F);
+				}
+				uint64_t *tables = arena_.AllocT<uint64_t>(words);
+				uint32_t *d_list = arena_.AllocT<uint32_t>(list.size());
+				uint32_t *d_caps = arena_.AllocT<uint32_t>(caps.size());
+				uint64_t *d_off = arena_.AllocT<uint64_t>(tab_off.size());
+				VGPU_CUDA(cudaMemcpyAsync(d_list, list.data(), list.size() * 4, cudaMemcpyHostToDevice, stream_));
+				VGPU_CUDA(cudaMemcpyAsync(d_caps, caps.data(), caps.size() * 4, cudaMemcpyHostToDevice, stream_));
+				VGPU_CUDA(cudaMemcpyAsync(d_off, tab_off.data(), tab_off.size() * 8, cudaMemcpyHostToDevice, stream_));
+				VGPU_CUDA(cudaMemsetAsync(control + 1, 0, 4, stream_));
+				b.SetPtr(L, d_list);
+				b.Set(L + 1, list.size());
+				b.SetPtr(L + 2, tables);
+				b.SetPtr(L + 3, d_off);
+				b.SetPtr(L + 4, d_caps);
+				LaunchGenerated(*module, "vgpu_gb_bucket_global",
+				                static_cast<unsigned>(std::min<uint64_t>(list.size(), uint64_t(props.sm_count) * 2)), 512, 0,
+				                stream_, b, 0, 0);
+				if (ReadU32(control + 1) != 0) {
+					Fail(VGPU_ERR_INTERNAL, "gpu_groupby: global-table fallback overflowed");
+				}
+			}
+			groups = ReadU64(out_count);
+			break;
 		}
-		const uint32_t overflowed = ReadU32(control + 1);
-		if (overflowed > 0) {
-			// Partitions with more distinct keys than a shared-memory table holds: redo them with a
-			// global-memory table sized from the partition's row count.
-			std::vector<uint32_t> flags(P), offs(P * G);
-			uint32_t total_rows = ReadU32(total);
-			VGPU_CUDA(cudaMemcpyAsync(flags.data(), control + 4, P * 4, cudaMemcpyDeviceToHost, stream_));
-			VGPU_CUDA(cudaMemcpyAsync(offs.data(), offsets, P * G * 4, cudaMemcpyDeviceToHost, stream_));
-			VGPU_CUDA(cudaStreamSynchronize(stream_));
-			std::vector<uint32_t> list, caps;
-			std::vector<uint64_t> tab_off;
-			uint64_t words = 0;
-			for (uint64_t p = 0; p < P; p++) {
-				if (!flags[p]) continue;
-				const uint32_t start = offs[p * G];
-				const uint32_t end = p + 1 < P ? offs[(p + 1) * G] : total_rows;
-				const uint64_t cap = NextPow2(std::max<uint64_t>(64, 2ull * (end - start)));
-				list.push_back(static_cast<uint32_t>(p));
-				caps.push_back(static_cast<uint32_t>(cap));
-				tab_off.push_back(words);
-				words += cap * (1 + F);
-			}
-			uint64_t *tables = arena_.AllocT<uint64_t>(words);
-			uint32_t *d_list = arena_.AllocT<uint32_t>(list.size());
-			uint32_t *d_caps = arena_.AllocT<uint32_t>(caps.size());
-			uint64_t *d_off = arena_.AllocT<uint64_t>(tab_off.size());
-			VGPU_CUDA(cudaMemcpyAsync(d_list, list.data(), list.size() * 4, cudaMemcpyHostToDevice, stream_));
-			VGPU_CUDA(cudaMemcpyAsync(d_caps, caps.data(), caps.size() * 4, cudaMemcpyHostToDevice, stream_));
-			VGPU_CUDA(cudaMemcpyAsync(d_off, tab_off.data(), tab_off.size() * 8, cudaMemcpyHostToDevice, stream_));
-			VGPU_CUDA(cudaMemsetAsync(control + 1, 0, 4, stream_));
-			b.SetPtr(L, d_list);
-			b.Set(L + 1, list.size());
-			b.SetPtr(L + 2, tables);
-			b.SetPtr(L + 3, d_off);
-			b.SetPtr(L + 4, d_caps);
-			LaunchGenerated(*module, "vgpu_gb_bucket_global",
-			                static_cast<unsigned>(std::min<uint64_t>(list.size(), uint64_t(props.sm_count) * 2)), 512, 0,
-			                stream_, b, 0, 0);
-			if (ReadU32(control + 1) != 0) {
-				Fail(VGPU_ERR_INTERNAL, "gpu_groupby: global-table fallback overflowed");
-			}
-		}
-		groups = ReadU64(out_count);
 	}
 	if (node.group_keys.empty() && groups == 0) {
 		Fail(VGPU_ERR_UNSUPPORTED, kEmptyGlobal);
 	}
 	for (auto &c : out) c.rows = groups;
 	return out;
+}
+
+// Heavy keys of a direct-partitioned group-by. Eligible when every carried value is 8 bytes wide and
+// feeds exactly one aggregate (its partial state then fits the value's record slot), no input has
+// NULLs, the mixed key leaves bit 31 of the record's key word free for the partial-record flag and a
+// table slot fits 15 bits. 64 tiles spread over the input are sampled on the device; keys seen often
+// enough that one CTA's share of their rows beats its one partial record are selected (at most 512,
+// one per partition), and the selection is dropped on the device when they cover under a tenth of
+// the sampled rows. VGPU_GB_HEAVY: 0 = off, 2 = always, whatever the input size and coverage (testing).
+Executor::HeavyPlan Executor::PlanHeavy(const PipelineCodegen::GroupBySpec &gb, const PipelineCodegen &cg,
+                                        const PipelineInput &pin, const GroupByCompiler &compile, const Geometry &g,
+                                        int cb, uint64_t P, uint64_t ntiles) {
+	HeavyPlan none;
+	int mode = 1;
+	if (const char *env = std::getenv("VGPU_GB_HEAVY")) mode = std::atoi(env);
+	if (mode == 0 || gb.direct_bits <= 0 || gb.direct_bits > 15 || gb.key_bits > 31 || cb + 12 >= kKeyWord) return none;
+	if (mode == 1 && pin.rows < (1ull << 22)) return none;  // small inputs: sampling costs more than it saves
+	for (auto &s : pin.sources) {
+		if (s.valid) return none;
+	}
+	std::map<int, int> uses;
+	for (auto &a : gb.aggs) {
+		if (a.column < 0 || a.kind == AggKind::COUNT || a.kind == AggKind::COUNT_STAR) continue;
+		if (TypeSize(cg.visible()[a.column].type) != 8 || ++uses[a.column] > 1) return none;
+	}
+	const auto &props = Runtime::Get().props();
+	uint32_t K = 512;
+	if (const char *env = std::getenv("VGPU_GB_HEAVY_KEYS")) {  // tuning override
+		K = static_cast<uint32_t>(std::min<uint64_t>(4096, std::max<uint64_t>(1, std::strtoull(env, nullptr, 10))));
+	}
+	PipelineCodegen::GroupBySpec gbh = gb;
+	gbh.heavy_slots = static_cast<int>(K);
+	HeavyPlan hp;
+	hp.max_keys = K;
+	hp.state_bytes = static_cast<uint64_t>(PipelineCodegen::HeavySlotBytes(gbh));
+	if (hp.smem(P) + 1024 > static_cast<size_t>(props.smem_optin)) return none;
+	hp.module = compile(gbh);
+	const uint32_t SC = 1u << 16;
+	uint64_t *skeys = arena_.AllocT<uint64_t>(SC);
+	uint32_t *scount = arena_.AllocT<uint32_t>(SC);
+	hp.hmap = arena_.AllocT<uint32_t>(P);
+	hp.keys = arena_.AllocT<uint32_t>(K);
+	uint32_t *info = arena_.AllocT<uint32_t>(2);  // [0] selected keys, [1] overflow flag
+	hp.count = info;
+	hp.overflow = info + 1;
+	VGPU_CUDA(cudaMemsetAsync(skeys, 0xff, static_cast<size_t>(SC) * 8, stream_));
+	VGPU_CUDA(cudaMemsetAsync(scount, 0, static_cast<size_t>(SC) * 4, stream_));
+	VGPU_CUDA(cudaMemsetAsync(hp.hmap, 0xff, P * 4, stream_));
+	VGPU_CUDA(cudaMemsetAsync(info, 0, 8, stream_));
+	const uint64_t samples = std::min<uint64_t>(ntiles, 64);
+	const uint64_t stride = ntiles / samples;
+	KArgsHost a;
+	FillArgs(pin, a);
+	SetKeyWords(a, gbh);
+	a.SetPtr(cb + 6, skeys);
+	a.SetPtr(cb + 7, scount);
+	a.Set(cb + 8, SC);
+	a.Set(cb + 9, stride);
+	const uint64_t sampled_rows = samples * static_cast<uint64_t>(g.tile());
+	LaunchGenerated(*hp.module, "vgpu_gb_sample", static_cast<unsigned>(samples), g.block, 0, stream_, a, 0, sampled_rows);
+	// a key seen c times in the sample has about c * ntiles / samples rows, spread over about
+	// 2 * sm_count CTAs: selected when that is at least two rows per CTA
+	const uint64_t ctas = 2ull * props.sm_count;
+	uint32_t min_count = static_cast<uint32_t>(std::max<uint64_t>(2, (2 * ctas * samples + ntiles - 1) / ntiles));
+	if (mode == 2) min_count = 1;
+	kern::HeavySelect(skeys, scount, SC, hp.hmap, static_cast<uint32_t>(gb.direct_bits), hp.keys, K, min_count,
+	                  mode != 2, hp.count, stream_);
+	return hp;
 }
 
 // Bucket pass of the direct-partitioned group-by: a longest-first work list of (partition, row range)

@@ -510,6 +510,131 @@ uint64_t PlanWorkCapacity(uint32_t P, uint64_t rows, uint32_t min_split) {
 	return static_cast<uint64_t>(P) + rows / (min_split ? min_split : 1) + 1;
 }
 
+namespace {
+constexpr int kHeavyBlock = 1024;
+constexpr uint32_t kHeavyBins = 1024;  // counts at or above the last bin share it
+constexpr int kHeavyUnroll = 8;        // sample slots per thread and batch
+
+__device__ uint64_t HeavyBlockSum(uint64_t v, uint64_t *scratch) {
+	for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+	if ((threadIdx.x & 31) == 0) scratch[threadIdx.x >> 5] = v;
+	__syncthreads();
+	uint64_t total = 0;
+	for (uint32_t w = 0; w < blockDim.x / 32; ++w) total += scratch[w];
+	__syncthreads();
+	return total;
+}
+
+__global__ void __launch_bounds__(kHeavyBlock) HeavySelectKernel(const uint64_t *keys, uint32_t *counts, uint32_t SC,
+                                                                 uint32_t *hmap, uint32_t dbits, uint32_t *hkeys,
+                                                                 uint32_t K, uint32_t min_count, bool require_cover,
+                                                                 uint32_t *n_heavy) {
+	__shared__ uint32_t hist[kHeavyBins];
+	__shared__ uint64_t scratch[32];
+	__shared__ uint32_t threshold, n_keys;
+	const uint32_t dmask = (1u << dbits) - 1;
+	constexpr uint32_t kWon = 0x80000000u;
+	constexpr int kBatch = kHeavyUnroll;
+	for (uint32_t b = threadIdx.x; b < kHeavyBins; b += blockDim.x) hist[b] = 0;
+	if (threadIdx.x == 0) n_keys = 0;
+	__syncthreads();
+	// Every pass walks the table in batches of kBatch slots per thread, loads first (one CTA: the
+	// loads of a batch must be in flight together). SC is a multiple of kBatch * blockDim.x, so every
+	// lane of a warp runs every iteration.
+	const uint32_t step = kBatch * blockDim.x;
+	uint64_t sampled = 0;
+	for (uint32_t base = threadIdx.x; base < SC; base += step) {
+		uint32_t c[kBatch];
+#pragma unroll
+		for (int j = 0; j < kBatch; ++j) {
+			const uint32_t s = base + j * blockDim.x;
+			c[j] = keys[s] == ~0ull ? 0u : counts[s];
+		}
+#pragma unroll
+		for (int j = 0; j < kBatch; ++j) {
+			// most sampled keys share a few small counts: lanes of one bin add once
+			const uint32_t bin = c[j] < kHeavyBins ? c[j] : kHeavyBins - 1;
+			const uint32_t peers = __match_any_sync(0xffffffffu, bin);
+			if (bin && static_cast<uint32_t>(__ffs(peers) - 1) == (threadIdx.x & 31)) atomicAdd(&hist[bin], __popc(peers));
+			sampled += c[j];
+		}
+	}
+	sampled = HeavyBlockSum(sampled, scratch);
+	if (threadIdx.x == 0) {
+		// the smallest threshold whose keys fit in K (bins summed from the top)
+		uint32_t t = kHeavyBins, keys_at = 0;
+		while (t > min_count && keys_at + hist[t - 1] <= K) {
+			keys_at += hist[t - 1];
+			--t;
+		}
+		threshold = t;
+	}
+	__syncthreads();
+	const uint32_t t = threshold;
+	// claim each candidate's partition; the winner marks its sample slot
+	for (uint32_t base = threadIdx.x; base < SC; base += step) {
+		uint64_t k[kBatch];
+		uint32_t c[kBatch];
+#pragma unroll
+		for (int j = 0; j < kBatch; ++j) {
+			k[j] = keys[base + j * blockDim.x];
+			c[j] = counts[base + j * blockDim.x];
+		}
+#pragma unroll
+		for (int j = 0; j < kBatch; ++j) {
+			if (k[j] == ~0ull || c[j] < t) continue;
+			const uint32_t p = static_cast<uint32_t>(k[j] >> dbits);
+			if (atomicCAS(&hmap[p], ~0u, 0xfffe0000u | (static_cast<uint32_t>(k[j]) & dmask)) == ~0u) {
+				counts[base + j * blockDim.x] = c[j] | kWon;
+			}
+		}
+	}
+	__syncthreads();
+	uint64_t covered = 0;
+	for (uint32_t base = threadIdx.x; base < SC; base += step) {
+		uint32_t c[kBatch];
+#pragma unroll
+		for (int j = 0; j < kBatch; ++j) c[j] = counts[base + j * blockDim.x];
+#pragma unroll
+		for (int j = 0; j < kBatch; ++j) {
+			if (!(c[j] & kWon)) continue;
+			const uint32_t s = base + j * blockDim.x;
+			const uint64_t k = keys[s];
+			const uint32_t p = static_cast<uint32_t>(k >> dbits);
+			const uint32_t idx = atomicAdd(&n_keys, 1u);
+			if (idx < K) {
+				hmap[p] = (idx << 16) | (static_cast<uint32_t>(k) & dmask);
+				hkeys[idx] = static_cast<uint32_t>(k);
+				covered += c[j] & ~kWon;
+			} else {
+				hmap[p] = ~0u;
+				counts[s] = c[j] & ~kWon;
+			}
+		}
+	}
+	covered = HeavyBlockSum(covered, scratch);
+	const bool drop = require_cover && covered * 10 < sampled;
+	if (drop) {
+		for (uint32_t s = threadIdx.x; s < SC; s += blockDim.x) {
+			if (counts[s] & kWon) hmap[static_cast<uint32_t>(keys[s] >> dbits)] = ~0u;
+		}
+	}
+	if (threadIdx.x == 0) *n_heavy = drop ? 0u : (n_keys < K ? n_keys : K);
+}
+} // namespace
+
+void HeavySelect(const uint64_t *sample_keys, uint32_t *sample_counts, uint32_t SC, uint32_t *hmap, uint32_t dbits,
+                 uint32_t *heavy_keys, uint32_t K, uint32_t min_count, bool require_cover, uint32_t *n_heavy,
+                 cudaStream_t stream) {
+	if (SC % (kHeavyBlock * kHeavyUnroll) != 0) {
+		Fail(VGPU_ERR_INTERNAL, "heavy_select: sample table size must be a multiple of 8192");
+	}
+	LaunchScope scope("heavy_select", stream, static_cast<uint64_t>(SC) * 12, SC);
+	HeavySelectKernel<<<1, kHeavyBlock, 0, stream>>>(sample_keys, sample_counts, SC, hmap, dbits, heavy_keys, K,
+	                                                 min_count < 1 ? 1u : min_count, require_cover, n_heavy);
+	VGPU_CUDA(cudaGetLastError());
+}
+
 void PlanWork(const uint32_t *offsets, uint64_t stride, uint32_t P, const uint32_t *total_rows, uint32_t min_split,
               uint32_t ctas, void *items, uint32_t *counts, uint32_t *split_info, uint32_t max_split,
               cudaStream_t stream) {

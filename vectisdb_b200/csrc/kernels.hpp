@@ -67,6 +67,15 @@ void CountAdjacentEqual(const uint64_t *sorted, uint64_t n, uint32_t *out, cudaS
 //! than max(min_split, total / (4 * ctas)) rows are split into chunks; chunks of one partition share a
 //! split index s with split_info[2s] = chunk count and split_info[2s+1] = 0 (a completion counter).
 //! counts[0] = items, counts[1] = split partitions (split_info is written for the first max_split).
+//! Heavy keys of a direct-partitioned group-by from a sample: sample_keys/sample_counts ([SC], key ~0
+//! = empty) hold the sampled rows' mixed keys and counts (the counts are used as scratch). Keys seen
+//! at least t times, t >= min_count the smallest threshold that selects at most K keys, claim their
+//! partition (key >> dbits; the first claim wins, one heavy key per partition): hmap[p] = (index << 16)
+//! | (key & (2^dbits - 1)), heavy_keys[index] = key, *n_heavy = keys selected. hmap must hold ~0 on
+//! entry. With require_cover, a selection covering under a tenth of the sampled rows is dropped.
+void HeavySelect(const uint64_t *sample_keys, uint32_t *sample_counts, uint32_t SC, uint32_t *hmap, uint32_t dbits,
+                 uint32_t *heavy_keys, uint32_t K, uint32_t min_count, bool require_cover, uint32_t *n_heavy,
+                 cudaStream_t stream);
 uint64_t PlanWorkCapacity(uint32_t P, uint64_t rows, uint32_t min_split);
 void PlanWork(const uint32_t *offsets, uint64_t stride, uint32_t P, const uint32_t *total_rows, uint32_t min_split,
               uint32_t ctas, void *items, uint32_t *counts, uint32_t *split_info, uint32_t max_split,
