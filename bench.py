@@ -67,16 +67,66 @@ def algorithmic_bytes(name: str, wl, kernel: str, passing: int, groups: int) -> 
 
 
 class ClockSampler:
+    """SM clocks, power and clock-event (throttle) reasons of one GPU, sampled every 50 ms by a thread
+    of this process through NVML -- the library nvidia-smi reports from -- so no second process competes
+    with the timed region for the driver. mark_begin()/mark_end() bracket the timed region; the summary
+    covers the samples inside it (or the two nearest when it is shorter than a sampling period).
+    Falls back to an `nvidia-smi -lms` subprocess when NVML bindings are missing."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                   "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80}
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
+        self.thread = None
+        self.samples = []  # (time, sm MHz, max sm MHz, power W, reason bits)
+        self.window = [None, None]
         self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"vgpu_clocks_{os.getpid()}.csv"
 
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:  # the CUDA device's own PCI address: NVML numbers GPUs without CUDA_VISIBLE_DEVICES
+            import torch
+            pr = torch.cuda.get_device_properties(torch.cuda.current_device())
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+
     def start(self):
+        try:
+            nv, h = self._nvml_handle()
+        except Exception:
+            return self._start_smi()
+        import threading
+        self.stop_flag = threading.Event()
+
+        def run():
+            while not self.stop_flag.is_set():
+                try:
+                    self.samples.append((time.perf_counter(), nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                                         nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM),
+                                         nv.nvmlDeviceGetPowerUsage(h) / 1000.0,
+                                         nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+                except Exception:
+                    pass
+                self.stop_flag.wait(0.05)
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
+        time.sleep(0.12)
+
+    def mark_begin(self):
+        self.window[0] = time.perf_counter()
+
+    def mark_end(self):
+        self.window[1] = time.perf_counter()
+
+    def _start_smi(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -94,6 +144,22 @@ class ClockSampler:
         time.sleep(0.1)
 
     def stop(self) -> dict:
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join()
+            rows = self.samples
+            t0, t1 = self.window
+            if t0 is not None and t1 is not None:
+                inside = [r for r in rows if t0 <= r[0] <= t1]
+                if len(inside) < 2:  # a region shorter than the period: the samples around it
+                    inside = sorted(rows, key=lambda r: min(abs(r[0] - t0), abs(r[0] - t1)))[:2]
+                rows = inside
+            if not rows:
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "source": "nvml"}
+            reasons = sorted({k for r in rows for k, bit in self.REASON_BITS.items() if r[4] & bit})
+            return {"sm_mhz": float(np.median([r[1] for r in rows])), "sm_max_mhz": float(max(r[2] for r in rows)),
+                    "power_w": float(np.median([r[3] for r in rows])), "reasons": reasons, "samples": len(rows),
+                    "source": "nvml"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -106,7 +172,7 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if "Active" == r[5 + i].strip()})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "source": "nvidia-smi"}
 
 
 def max_over_ranks(value: float, world: int, device: str = "cuda") -> float:
@@ -260,11 +326,19 @@ def run_c3(args, world, rank, local):
                 out = step_fn()
                 for r in (out[0] if isinstance(out, tuple) else out):
                     r.free()
+        profile_enable(True)  # untimed: creates the profiler's events, which the timed steps reuse
+        for _ in range(steps):
+            out = step_fn()
+            for r in (out[0] if isinstance(out, tuple) else out):
+                r.free()
+        torch.cuda.synchronize()
         profile_drain()
         profile_enable(True)
         torch.cuda.synchronize()
         l0 = launch_count()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if sampler:
+            sampler.mark_begin()
         e0.record(stream)
         last = []
         for _ in range(steps):
@@ -275,6 +349,8 @@ def run_c3(args, world, rank, local):
             last = out
         e1.record(stream)
         torch.cuda.synchronize()
+        if sampler:
+            sampler.mark_end()
         ms = e0.elapsed_time(e1) / steps
         launches = launch_count() - l0
         prof = profile_drain()
@@ -439,6 +515,7 @@ def run_c4(args, world, rank, local):
     rates = [float(r) for r in (50, 100, 200, 400, 800, 1600)]
     sampler = ClockSampler(local)
     sampler.start()
+    sampler.mark_begin()
     l0 = launch_count()
     sweep = []
     for r in rates:
@@ -446,6 +523,7 @@ def run_c4(args, world, rank, local):
         serial = serve(r, 1, 1)
         sweep.append({"rate_per_s": r, "served": served, "serial": serial})
     launches = launch_count() - l0
+    sampler.mark_end()
     clocks = sampler.stop()
     top = sweep[-1]
     line = {
@@ -524,18 +602,22 @@ def main():
             raise RuntimeError(f"engine failed: {r.error_message}")
         return r
 
-    # The clock sampler starts before the warm-up: nvidia-smi's first queries after start-up stall the
-    # driver for a few hundred ms, which must land in untimed work, not in the timed region.
-    sampler = ClockSampler(local if "CUDA_VISIBLE_DEVICES" not in os.environ else 0)
+    # The clock sampler starts before the warm-up, so its start-up lands in untimed work.
+    sampler = ClockSampler(local)
     sampler.start()
     t_sampler = time.time()
     for _ in range(args.warmup):
         step().free()
     while time.time() - t_sampler < 1.0:  # untimed steps until the sampler has settled
         step().free()
+    # the launch profiler's CUDA events are created here, untimed: in the timed region its records
+    # only reuse them
+    profile_enable(True)
+    for _ in range(args.steps):
+        step().free()
     torch.cuda.synchronize()
-
     profile_drain()
+
     profile_enable(True)
     if world > 1:
         torch.distributed.barrier()
@@ -543,6 +625,7 @@ def main():
     launches0 = launch_count()
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
+    sampler.mark_begin()
     t_start.record(stream)
     last = None
     for i in range(args.steps):
@@ -552,6 +635,7 @@ def main():
         last = r
     t_end.record(stream)
     torch.cuda.synchronize()
+    sampler.mark_end()
     if world > 1:
         torch.distributed.barrier()
     elapsed_ms = t_start.elapsed_time(t_end)
