@@ -327,37 +327,51 @@ def run_c3(args, world, rank, local):
                 for r in (out[0] if isinstance(out, tuple) else out):
                     r.free()
         profile_enable(True)  # untimed: creates the profiler's events, which the timed steps reuse
-        for _ in range(steps):
+        for _ in range(steps * args.blocks):
             out = step_fn()
             for r in (out[0] if isinstance(out, tuple) else out):
                 r.free()
         torch.cuda.synchronize()
         profile_drain()
-        profile_enable(True)
-        torch.cuda.synchronize()
-        l0 = launch_count()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        profile_enable(False)
+        # timed blocks of exactly `steps` steps after half a second of untimed ones, two untimed
+        # steps between blocks, records collected after the last; the median block is reported
+        t_hot = time.time()
+        while time.time() - t_hot < 0.5:
+            out = step_fn()
+            for r in (out[0] if isinstance(out, tuple) else out):
+                r.free()
+        blocks, launches = [], 0
         if sampler:
             sampler.mark_begin()
-        e0.record(stream)
-        last = []
-        for _ in range(steps):
-            out = step_fn()
-            out = out[0] if isinstance(out, tuple) else out
+        for _b in range(args.blocks):
+            for _ in range(2):
+                out = step_fn()
+                for r in (out[0] if isinstance(out, tuple) else out):
+                    r.free()
+            torch.cuda.synchronize()
+            profile_enable(True)
+            l0 = launch_count()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            last = []
+            for _ in range(steps):
+                out = step_fn()
+                out = out[0] if isinstance(out, tuple) else out
+                for r in last:
+                    r.free()
+                last = out
+            e1.record(stream)
+            torch.cuda.synchronize()
+            profile_enable(False)
+            blocks.append(e0.elapsed_time(e1) / steps)
+            launches += launch_count() - l0
             for r in last:
                 r.free()
-            last = out
-        e1.record(stream)
-        torch.cuda.synchronize()
         if sampler:
             sampler.mark_end()
-        ms = e0.elapsed_time(e1) / steps
-        launches = launch_count() - l0
         prof = profile_drain()
-        profile_enable(False)
-        for r in last:
-            r.free()
-        return ms, launches, prof, (sampler.stop() if sampler else None)
+        return float(np.median(blocks)), launches // args.blocks, prof, (sampler.stop() if sampler else None)
 
     b_ms, b_launches, b_prof, clocks = timed(batched_step, args.steps, True)
     p_steps = max(3, args.steps // 5)
@@ -407,7 +421,8 @@ def run_c3(args, world, rank, local):
             "config": {"workload": "c3", "queries": len(wls), "rows": rows, "bytes_per_row": 20.0,
                        "inputs": "resident in the device column cache (larger than L2, no flush needed)",
                        "geometry": {k: tuned[k] for k in ("block", "items", "tile_rows", "smem_slots")},
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"replicas x{world}",
+                       "timing": f"median of {args.blocks} timed blocks of {args.steps} steps"},
             "plain": {"value": rows / (p_ms / 1000.0), "ms_per_step": p_ms, "steps": p_steps,
                       "form": "one vgpu_execute_plan per query, device outputs, no per-query sync"},
             "batched_over_plain": p_ms / b_ms,
@@ -555,6 +570,7 @@ def main():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c2b", "c3", "c4"])
     p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--blocks", type=int, default=5, help="timed blocks of --steps steps; the median is reported")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--rows", type=int, default=0, help="small-case size for profiling (0 = the full workload)")
     args = p.parse_args()
@@ -610,43 +626,58 @@ def main():
         step().free()
     while time.time() - t_sampler < 1.0:  # untimed steps until the sampler has settled
         step().free()
-    # the launch profiler's CUDA events are created here, untimed: in the timed region its records
+    # the launch profiler's CUDA events are created here, untimed: in the timed blocks its records
     # only reuse them
     profile_enable(True)
-    for _ in range(args.steps):
+    for _ in range(args.steps * args.blocks):
         step().free()
     torch.cuda.synchronize()
     profile_drain()
-
-    profile_enable(True)
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    launches0 = launch_count()
-    t_start = torch.cuda.Event(enable_timing=True)
-    t_end = torch.cuda.Event(enable_timing=True)
-    sampler.mark_begin()
-    t_start.record(stream)
-    last = None
-    for i in range(args.steps):
-        r = step()
-        if last is not None:
-            last.free()
-        last = r
-    t_end.record(stream)
-    torch.cuda.synchronize()
-    sampler.mark_end()
-    if world > 1:
-        torch.distributed.barrier()
-    elapsed_ms = t_start.elapsed_time(t_end)
-    launches = launch_count() - launches0
-    prof = profile_drain()
     profile_enable(False)
+
+    # Timed blocks of exactly K steps, each bracketed by a barrier and a device synchronize. After an
+    # idle gap of some milliseconds the GPU drops its clocks, and steps shortly after one have stalled
+    # for up to a second with the host asleep in the driver. So the GPU is kept busy for half a second
+    # first, blocks follow one another with two untimed steps between them and no host-side work (the
+    # profiler's records are collected after the last block), and the line reports the median block
+    # (every block's time is listed beside it).
+    t_hot = time.time()
+    while time.time() - t_hot < 0.5:
+        step().free()
+    blocks, launches = [], 0
+    sampler.mark_begin()
+    for b in range(args.blocks):
+        for _ in range(2):
+            step().free()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        profile_enable(True)
+        launches0 = launch_count()
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        last = None
+        for i in range(args.steps):
+            r = step()
+            if last is not None:
+                last.free()
+            last = r
+        t_end.record(stream)
+        torch.cuda.synchronize()
+        profile_enable(False)
+        if world > 1:
+            torch.distributed.barrier()
+        ms = t_start.elapsed_time(t_end)
+        blocks.append(max_over_ranks(ms, world) if world > 1 else ms)
+        launches += launch_count() - launches0
+        groups = last.columns[0].row_count if last.columns else 0
+        last.free()
+    sampler.mark_end()
+    prof = profile_drain()
     clocks = sampler.stop()
-    groups = last.columns[0].row_count if last.columns else 0
-    last.free()
-    if world > 1:
-        elapsed_ms = max_over_ranks(elapsed_ms, world)
+    launches //= args.blocks
+    elapsed_ms = float(np.median(blocks))
     value = wl.rows * args.steps * world / (elapsed_ms / 1000.0)
 
     # passing rows (for per-kernel algorithmic bytes): one host-output run
@@ -724,7 +755,9 @@ def main():
             "data": "synthetic",
             "config": {"workload": name, "rows": wl.rows, "bytes_per_row": wl.bytes_per_row,
                        "inputs": "resident in the device column cache (larger than L2, no flush needed)",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"replicas x{world}",
+                       "timing": f"median of {args.blocks} timed blocks of {args.steps} steps"},
+            "blocks_ms_per_step": [round(b / args.steps, 4) for b in blocks],
             "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                          "kernel_share": dom[1][0] / total_ms, "kernel_avg_ms": dom_avg_ms,
