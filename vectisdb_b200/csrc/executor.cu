@@ -48,12 +48,14 @@ struct KArgsHost {
 	}
 };
 
-void LaunchGenerated(Module &m, const char *name, dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
-                     KArgsHost &args, uint64_t bytes, uint64_t rows) {
+// Returns the launch's profiler record (-1 when profiling is off), for Profiler::SetBytes.
+int LaunchGenerated(Module &m, const char *name, dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                    KArgsHost &args, uint64_t bytes, uint64_t rows) {
 	CUfunction f = m.Get(name);
 	LaunchScope scope(name, stream, bytes, rows);
 	void *params[] = {args.w};
 	Runtime::Get().LaunchModuleKernel(f, grid, block, smem, stream, params);
+	return scope.index();
 }
 
 // Key packing of a group-by into its kernels' reserved argument words (see kKeyWord).
@@ -128,7 +130,7 @@ private:
 	void FillArgs(const PipelineInput &pin, KArgsHost &args);
 	uint64_t DirectBuckets(Module &module, const PipelineCodegen::GroupBySpec &gb, const PipelineInput &pin, uint64_t P,
 	                       uint64_t G, const uint32_t *offsets, const uint32_t *total, const char *records, uint64_t n,
-	                       uint64_t RS, Relation &out, int out_words, int threads);
+	                       uint64_t RS, Relation &out, int out_words, int threads, uint64_t *records_written);
 	uint64_t ReadU64(const void *dev);
 	uint32_t ReadU32(const void *dev);
 	//! Heavy keys chosen for the partition passes of a direct-partitioned group-by (no module: none).
@@ -814,9 +816,14 @@ Relation Executor::GroupBy(const PlanNode &node) {
 			kern::ExclusiveScanU32(offsets, offsets, P * G, total, arena_);
 			char *records = static_cast<char *>(arena_.Alloc(n_rec * RS));
 			a.SetPtr(cb + 4, records);
-			LaunchGenerated(*module, "vgpu_gb_part_scatter", static_cast<unsigned>(G), g.block, smem, stream_, a, in_bytes, n);
+			const int scatter_rec = LaunchGenerated(*module, "vgpu_gb_part_scatter", static_cast<unsigned>(G), g.block,
+			                                        smem, stream_, a, in_bytes, n);
 			if (gb.direct_bits > 0) {
-				groups = DirectBuckets(*module, gb, pin, P, G, offsets, total, records, n_rec, RS, out, out_words, T1);
+				uint64_t written = 0;
+				groups = DirectBuckets(*module, gb, pin, P, G, offsets, total, records, n_rec, RS, out, out_words, T1,
+				                       &written);
+				// the scatter's bytes: the columns it reads once and the records it wrote
+				Runtime::Get().profiler().SetBytes(scatter_rec, in_bytes + written * RS);
 				if (use_heavy && ReadU32(heavy.overflow) != 0) continue;  // a partial sum left 64 bits: redo plainly
 				for (auto &c : out) c.rows = groups;
 				return out;
@@ -1011,7 +1018,7 @@ Executor::HeavyPlan Executor::PlanHeavy(const PipelineCodegen::GroupBySpec &gb, 
 uint64_t Executor::DirectBuckets(Module &module, const PipelineCodegen::GroupBySpec &gb, const PipelineInput &pin,
                                  uint64_t P, uint64_t G, const uint32_t *offsets, const uint32_t *total,
                                  const char *records, uint64_t n, uint64_t RS, Relation &out, int out_words,
-                                 int threads) {
+                                 int threads, uint64_t *records_written) {
 	const auto &props = Runtime::Get().props();
 	const uint64_t D = 1ull << gb.direct_bits;
 	const uint64_t F = static_cast<uint64_t>(PipelineCodegen::StateWords(gb));
@@ -1034,7 +1041,11 @@ uint64_t Executor::DirectBuckets(Module &module, const PipelineCodegen::GroupByS
 	VGPU_CUDA(cudaMemsetAsync(out_count, 0, 8, stream_));
 	kern::PlanWork(offsets, G, static_cast<uint32_t>(P), total, min_split, ctas, items, control, split_info, max_split,
 	               stream_);
-	const uint32_t n_split = ReadU32(control + 1);
+	uint32_t plan[3];  // split partitions, work counter, partitioned rows (one read-back)
+	VGPU_CUDA(cudaMemcpyAsync(plan, control + 1, sizeof(plan), cudaMemcpyDeviceToHost, stream_));
+	VGPU_CUDA(cudaStreamSynchronize(stream_));
+	const uint32_t n_split = plan[0];
+	*records_written = plan[2];
 	if (n_split > max_split) Fail(VGPU_ERR_INTERNAL, "gpu_groupby: work plan produced more splits than planned");
 	uint64_t *gtab = n_split ? arena_.AllocT<uint64_t>(static_cast<uint64_t>(n_split) * F * D) : nullptr;
 	const int cb = 2 + 2 * static_cast<int>(pin.sources.size());  // first consumer argument word
@@ -1055,8 +1066,12 @@ uint64_t Executor::DirectBuckets(Module &module, const PipelineCodegen::GroupByS
 		const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((words + 255) / 256, uint64_t(props.sm_count) * 8));
 		LaunchGenerated(module, "vgpu_gb_dtab_init", grid, 256, 0, stream_, b, words * 8, 0);
 	}
-	LaunchGenerated(module, "vgpu_gb_dbucket", ctas, threads, smem, stream_, b, n * RS, n);
-	return ReadU64(out_count);
+	const int rec = LaunchGenerated(module, "vgpu_gb_dbucket", ctas, threads, smem, stream_, b, n * RS, n);
+	const uint64_t groups = ReadU64(out_count);
+	uint64_t out_row = 0;
+	for (int w = 0; w < out_words; w++) out_row += TypeSize(out[w].type);
+	Runtime::Get().profiler().SetBytes(rec, plan[2] * RS + groups * out_row);  // records in, groups out
+	return groups;
 }
 
 // ---- HASH_JOIN (sort-merge) ------------------------------------------------------------------------

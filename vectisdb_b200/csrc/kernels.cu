@@ -455,7 +455,10 @@ __global__ void __launch_bounds__(kPlanBlock) PlanWorkKernel(const uint32_t *off
 		}
 	}
 	__syncthreads();
-	if (threadIdx.x == 0) counts[1] = n_split;
+	if (threadIdx.x == 0) {
+		counts[1] = n_split;
+		counts[3] = *total_rows;  // read back with the split count: the partitioned row count
+	}
 }
 
 } // namespace

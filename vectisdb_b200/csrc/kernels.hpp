@@ -66,7 +66,8 @@ void CountAdjacentEqual(const uint64_t *sorted, uint64_t n, uint32_t *out, cudaS
 //! split index or ~0u), longest first, into `items` (capacity PlanWorkCapacity). Partitions larger
 //! than max(min_split, total / (4 * ctas)) rows are split into chunks; chunks of one partition share a
 //! split index s with split_info[2s] = chunk count and split_info[2s+1] = 0 (a completion counter).
-//! counts[0] = items, counts[1] = split partitions (split_info is written for the first max_split).
+//! counts[0] = items, counts[1] = split partitions (split_info is written for the first max_split),
+//! counts[3] = *total_rows.
 //! Heavy keys of a direct-partitioned group-by from a sample: sample_keys/sample_counts ([SC], key ~0
 //! = empty) hold the sampled rows' mixed keys and counts (the counts are used as scratch). Keys seen
 //! at least t times, t >= min_count the smallest threshold that selects at most K keys, claim their

@@ -492,6 +492,16 @@ void Profiler::End(int index, cudaStream_t stream) {
 	}
 }
 
+void Profiler::SetBytes(int index, uint64_t bytes) {
+	if (index < 0) {
+		return;
+	}
+	std::lock_guard<std::mutex> lock(mu_);
+	if (index < static_cast<int>(records_.size())) {
+		records_[index].bytes = bytes;
+	}
+}
+
 std::vector<vgpu_kernel_timing> Profiler::Collect() {
 	std::lock_guard<std::mutex> lock(mu_);
 	std::vector<vgpu_kernel_timing> out;

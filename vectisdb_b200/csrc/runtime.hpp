@@ -155,6 +155,8 @@ public:
 	//! Returns an index to pass to End, or -1 when disabled.
 	int Begin(const char *name, cudaStream_t stream, uint64_t bytes, uint64_t rows);
 	void End(int index, cudaStream_t stream);
+	//! Replaces a record's algorithmic bytes once the host knows them (after a later read-back).
+	void SetBytes(int index, uint64_t bytes);
 	std::vector<vgpu_kernel_timing> Collect();
 
 private:
@@ -170,6 +172,9 @@ class LaunchScope {
 public:
 	LaunchScope(const char *name, cudaStream_t stream, uint64_t bytes = 0, uint64_t rows = 0);
 	~LaunchScope();
+	int index() const {
+		return index_;
+	}
 
 private:
 	int index_;
