@@ -22,6 +22,7 @@ def test_benchmark_query_kernels_compile(name):
     src = generate_source(wl.plan, wl.inputs)
     assert "vgpu_gb_direct" in src and "vgpu_gb_bucket" in src and "vgpu_gb_dbucket" in src
     assert "vgpu_gb_sample" in src and "vgpu_hmap" in src
+    assert "stage_copy(" in src and "stage_wait(" in src
     assert all(s > 1000 for s in _compile_all(src))
 
 

@@ -746,6 +746,22 @@ int PipelineCodegen::HeavySlotBytes(const GroupBySpec &gb) {
 	return bytes;
 }
 
+int PipelineCodegen::StageRowBytes(const GroupBySpec &gb, bool scatter) const {
+	std::vector<int> used;
+	for (auto &k : gb.keys) used.push_back(k.column);
+	if (scatter) {
+		for (auto &a : gb.aggs) {
+			if (a.column >= 0) used.push_back(a.column);
+		}
+	}
+	const auto needed = NeededSources(used);
+	int bytes = 0;
+	for (size_t i = 0; i < spec_.sources.size(); i++) {
+		if (needed[i]) bytes += static_cast<int>(TypeSize(spec_.sources[i].type));
+	}
+	return bytes;
+}
+
 int PipelineCodegen::RecordStride(const GroupBySpec &gb) const {
 	// Same layout rule as EmitGroupBy: key u64, then each distinct carried value column at its
 	// natural alignment, rounded up to 32 bytes.
@@ -919,6 +935,103 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		  << "__device__ __forceinline__ u64 vgpu_dunmix(const KArgs &a, u64 k) { return (k * a.w[" << kMixWord + 1
 		  << "]) & a.w[" << kMixWord + 2 << "]; }\n\n";
 	}
+	// Staged tiles (g.staged, direct-partitioned count and scatter): args cb+13 = byte offset of the two
+	// stages in dynamic shared memory, cb+14 = error flag (u32*). A full tile's needed columns land in
+	// stage (local tile index & 1) by bulk copies that thread 0 issues two tiles ahead; the tail tile
+	// uses plain loads. A wait that gives up sets the flag and ends the CTA's tile loop.
+	std::vector<int> key_cols_used;
+	for (auto &k : gb.keys) key_cols_used.push_back(k.column);
+	const auto needed_count = NeededSources(key_cols_used);
+	struct StageCol {
+		int src, off, chunk;
+	};
+	auto stage_layout = [&](const std::vector<bool> &nd, int *stage_bytes) {
+		std::vector<StageCol> cols;
+		int off = 0;
+		for (size_t i = 0; i < spec_.sources.size(); i++) {
+			if (!nd[i]) continue;
+			const int chunk = static_cast<int>(TypeSize(spec_.sources[i].type)) * g.tile();
+			cols.push_back({static_cast<int>(i), off, chunk});
+			off += chunk;
+		}
+		*stage_bytes = off;
+		return cols;
+	};
+	auto stage_issue = [&](const std::vector<bool> &nd, const std::string &li, const std::string &t) {
+		int sb = 0;
+		const auto cols = stage_layout(nd, &sb);
+		std::ostringstream r;
+		r << "{ const u32 s_ = (u32)(" << li << ") & 1u; u64 *b_ = &vgpu_bar[s_]; char *d_ = vgpu_stage + s_ * " << sb
+		  << "u;\n"
+		  << "\t\t\tasm volatile(\"fence.proxy.async.shared::cta;\" ::: \"memory\");\n"
+		  << "\t\t\tstage_expect(b_, " << sb << "u);\n";
+		for (auto &c : cols) {
+			r << "\t\t\tstage_copy(d_ + " << c.off << ", (const char*)a.w[" << 2 + 2 * c.src << "] + (" << t << ") * (u64)"
+			  << c.chunk << ", " << c.chunk << "u, b_);\n";
+		}
+		r << "\t\t\tvgpu_pend |= 1u << s_; }\n";
+		return r.str();
+	};
+	auto stage_prologue = [&](const std::vector<bool> &nd, const char *smem_name) {
+		if (!g.staged) return std::string();
+		std::ostringstream r;
+		r << "\t__shared__ __align__(8) u64 vgpu_bar[2];\n"
+		  << "\tchar *vgpu_stage = (char*)" << smem_name << " + a.w[" << cb + 13 << "];\n"
+		  << "\tconst u64 vgpu_full = n / " << g.tile() << "ull;\n"
+		  << "\tconst u64 vgpu_t0 = blockIdx.x * tpc;\n"
+		  << "\tu32 vgpu_pend = 0, vgpu_phase = 0;\n\tbool vgpu_failed = false;\n"
+		  << "\tif (threadIdx.x == 0) { stage_barrier_init(&vgpu_bar[0]); stage_barrier_init(&vgpu_bar[1]); "
+		     "stage_barrier_fence(); }\n"
+		  << "\t__syncthreads();\n"
+		  << "\tif (threadIdx.x == 0) {\n"
+		  << "\t\tfor (u32 j_ = 0; j_ < 2u; ++j_) {\n"
+		  << "\t\t\tconst u64 t_ = vgpu_t0 + j_;\n"
+		  << "\t\t\tif (t_ < t_end && t_ < vgpu_full) " << stage_issue(nd, "j_", "t_") << "\t\t}\n\t}\n";
+		return r.str();
+	};
+	auto tile_load = [&](const std::vector<bool> &nd) {
+		if (!g.staged) return LoadBlock(g, nd, true);
+		int sb = 0;
+		const auto cols = stage_layout(nd, &sb);
+		std::ostringstream r;
+		r << "\t\tconst u64 row0 = tile * (u64)" << g.tile() << " + (u64)threadIdx.x * " << g.items << ";\n";
+		for (auto &c : cols) {
+			r << "\t\t" << CudaTypeName(spec_.sources[c.src].type) << " s" << c.src << "[" << g.items << "];\n";
+		}
+		r << "\t\tconst u32 vgpu_li = (u32)(tile - vgpu_t0);\n"
+		  << "\t\tif (tile < vgpu_full) {\n"
+		  << "\t\t\tconst u32 s_ = vgpu_li & 1u;\n"
+		  << "\t\t\tif (stage_wait(&vgpu_bar[s_], (vgpu_li >> 1) & 1u)) {\n"
+		  << "\t\t\t\tif (threadIdx.x == 0) { vgpu_pend &= ~(1u << s_); vgpu_phase ^= 1u << s_; }\n"
+		  << "\t\t\t} else {\n\t\t\t\tvgpu_failed = true;\n\t\t\t}\n"
+		  << "\t\t\tconst char *b_ = vgpu_stage + s_ * " << sb << "u;\n";
+		for (auto &c : cols) {
+			const char *t = CudaTypeName(spec_.sources[c.src].type);
+			r << "\t\t\tload_stage<" << t << ", " << g.items << ">((const " << t << "*)(b_ + " << c.off
+			  << ") + threadIdx.x * " << g.items << ", s" << c.src << ");\n";
+		}
+		r << "\t\t} else {\n";
+		for (auto &c : cols) {
+			const char *t = CudaTypeName(spec_.sources[c.src].type);
+			r << "\t\t\tload_rows<" << t << ", " << g.items << ">((const " << t << "*)a.w[" << 2 + 2 * c.src
+			  << "], row0, n, s" << c.src << ");\n";
+		}
+		r << "\t\t}\n"
+		  << "\t\tif (__syncthreads_or(vgpu_failed)) { vgpu_failed = true; break; }\n"
+		  << "\t\tif (threadIdx.x == 0 && tile + 2 < t_end && tile + 2 < vgpu_full) "
+		  << stage_issue(nd, "vgpu_li + 2u", "tile + 2");
+		return r.str();
+	};
+	auto stage_epilogue = [&]() {
+		if (!g.staged) return std::string();
+		std::ostringstream r;
+		r << "\tif (vgpu_failed && threadIdx.x == 0) {\n"
+		  << "\t\tatomicOr((u32*)a.w[" << cb + 14 << "], 1u);\n"
+		  << "\t\tfor (u32 s_ = 0; s_ < 2u; ++s_) {\n"
+		  << "\t\t\tif (vgpu_pend & (1u << s_)) (void)stage_wait(&vgpu_bar[s_], (vgpu_phase >> s_) & 1u);\n"
+		  << "\t\t}\n\t}\n";
+		return r.str();
+	};
 	// part_count / part_scatter args: cb+0 = P, cb+1 = pbits, cb+2 = tiles per CTA,
 	//   cb+3 = counts/offsets (u32, [p * G + cta]), cb+4 = records out.
 	if (dpart && gb.heavy_slots > 0) {
@@ -1020,11 +1133,12 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		  << heavy_load(false) << "\t__syncthreads();\n"
 		  << tile_loop_head
 		  << "\tconst u64 t_end = (blockIdx.x + 1) * tpc < ntiles ? (blockIdx.x + 1) * tpc : ntiles;\n"
+		  << stage_prologue(needed_count, "vgpu_smem")
 		  << "\tfor (u64 tile = blockIdx.x * tpc; tile < t_end; ++tile) {\n"
-		  << LoadBlock(g, needed, true) << item_head << chain_code_ << "\t\tif (keep) {\n"
+		  << tile_load(needed_count) << item_head << chain_code_ << "\t\tif (keep) {\n"
 		  << "\t\t\tconst u64 k0 = " << mixed << ";\n"
 		  << "\t\t\tif (" << heavy_of << " < 0) atomicAdd(&vgpu_hist[(u32)(k0 >> " << dbits << ")], 1u);\n"
-		  << "\t\t}\n\t\t}\n\t}\n\t__syncthreads();\n"
+		  << "\t\t}\n\t\t}\n\t}\n" << stage_epilogue() << "\t__syncthreads();\n"
 		  << "\tfor (u32 h = threadIdx.x; h < nheavy; h += blockDim.x) atomicAdd(&vgpu_hist[vgpu_hkeys[h] >> " << dbits
 		  << "], 1u);\n"
 		  << "\t__syncthreads();\n"
@@ -1088,8 +1202,9 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		  << heavy_load(true) << "\t__syncthreads();\n"
 		  << tile_loop_head
 		  << "\tconst u64 t_end = (blockIdx.x + 1) * tpc < ntiles ? (blockIdx.x + 1) * tpc : ntiles;\n"
+		  << stage_prologue(needed, "vgpu_smem")
 		  << "\tfor (u64 tile = blockIdx.x * tpc; tile < t_end; ++tile) {\n"
-		  << LoadBlock(g, needed, true)
+		  << tile_load(needed)
 		  << "\t\tu32 vgpu_pos[" << g.items << "];\n\t\tint vgpu_hv[" << g.items << "];\n"
 		  << item_head << chain_code_
 		  << "\t\tconst u64 k0 = " << mixed << ";\n"
@@ -1120,7 +1235,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		}
 		o << "\t\t\tstore_record<" << RW << ">(rec_out + (u64)pos * " << RS << ", rw);\n"
 		  << "\t\t\t}\n\t\t}\n\t\t}\n\t}\n"
-		  << "\t__syncthreads();\n"
+		  << stage_epilogue() << "\t__syncthreads();\n"
 		  << "\tfor (u32 h = threadIdx.x; h < nheavy; h += blockDim.x) {\n"
 		  << "\t\tconst u32 k = vgpu_hkeys[h];\n"
 		  << "\t\tconst u32 pos = atomicAdd(&vgpu_cursor[k >> " << dbits << "], 1u);\n"
@@ -1134,10 +1249,11 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 	  << "\tfor (u32 p = threadIdx.x; p < P; p += " << g.block << ") vgpu_hist[p] = 0;\n\t__syncthreads();\n"
 	  << tile_loop_head
 	  << "\tconst u64 t_end = (blockIdx.x + 1) * tpc < ntiles ? (blockIdx.x + 1) * tpc : ntiles;\n"
+	  << stage_prologue(needed_count, "vgpu_hist")
 	  << "\tfor (u64 tile = blockIdx.x * tpc; tile < t_end; ++tile) {\n"
-	  << LoadBlock(g, needed, true) << item_head << chain_code_ << "\t\tif (keep) {\n"
+	  << tile_load(needed_count) << item_head << chain_code_ << "\t\tif (keep) {\n"
 	  << "\t\t\tatomicAdd(&vgpu_hist[" << part_of_pack << "], 1u);\n"
-	  << "\t\t}\n\t\t}\n\t}\n\t__syncthreads();\n"
+	  << "\t\t}\n\t\t}\n\t}\n" << stage_epilogue() << "\t__syncthreads();\n"
 	  << "\tu32 *counts = (u32*)a.w[" << cb + 3 << "];\n"
 	  << "\tfor (u32 p = threadIdx.x; p < P; p += " << g.block
 	  << ") counts[(u64)p * gridDim.x + blockIdx.x] = vgpu_hist[p];\n}\n\n";
@@ -1152,8 +1268,9 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 	  << ") vgpu_cursor[p] = offsets[(u64)p * gridDim.x + blockIdx.x];\n\t__syncthreads();\n"
 	  << tile_loop_head
 	  << "\tconst u64 t_end = (blockIdx.x + 1) * tpc < ntiles ? (blockIdx.x + 1) * tpc : ntiles;\n"
+	  << stage_prologue(needed, "vgpu_cursor")
 	  << "\tfor (u64 tile = blockIdx.x * tpc; tile < t_end; ++tile) {\n"
-	  << LoadBlock(g, needed, true)
+	  << tile_load(needed)
 	  // every item's cursor reservation first, branch-free (rows that are filtered out add to a per-lane
 	  // dummy counter past P), so the tile's shared atomics are in flight together; then the records
 	  << "\t\tu32 vgpu_pos[" << g.items << "];\n"
@@ -1180,7 +1297,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		}
 	}
 	o << "\t\t\tstore_record<" << RW << ">(rec_out + (u64)pos * " << RS << ", rw);\n"
-	  << "\t\t}\n\t\t}\n\t}\n}\n\n";
+	  << "\t\t}\n\t\t}\n\t}\n" << stage_epilogue() << "}\n\n";
 
 	}
 

@@ -53,6 +53,9 @@ struct PipeColumn {
 struct Geometry {
 	int block = 256;
 	int items = 4; // consecutive rows per thread
+	// Direct-partitioned partition passes only: full tiles arrive through two shared-memory stages
+	// filled by bulk asynchronous copies (plain columns, 16-byte aligned, no NULLs, no join source).
+	bool staged = false;
 	int tile() const {
 		return block * items;
 	}
@@ -154,6 +157,9 @@ public:
 	//! Shared-memory bytes of one heavy key's partial state in the heavy partition passes (row count,
 	//! partial state of every aggregate).
 	static int HeavySlotBytes(const GroupBySpec &gb);
+	//! Bytes per row of one staged tile of the partition count (`scatter` false) or scatter pass: the
+	//! source columns that pass reads.
+	int StageRowBytes(const GroupBySpec &gb, bool scatter) const;
 	//! Byte stride of one partitioned-intermediate record (packed key + carried values, 32-byte multiple).
 	int RecordStride(const GroupBySpec &gb) const;
 

@@ -206,11 +206,17 @@ std::string GenerateSourceText(const PlanNode &plan, const std::vector<vgpu_colu
 	// ... and its heavy-key variant (sampling kernel, pre-aggregating partition passes)
 	PipelineCodegen::GroupBySpec spec_hv = spec_dp;
 	spec_hv.heavy_slots = 512;
+	// ... and both with tiles staged through shared memory by bulk copies
+	Geometry gst = g;
+	gst.items = 4;
+	gst.staged = true;
 	// Separate translation units, separated by a marker line: direct, partitioned, key statistics,
-	// direct-partitioned, direct-partitioned with heavy keys.
+	// direct-partitioned, direct-partitioned with heavy keys, the last two staged.
 	return cg.EmitGroupBy(spec_gb, false, g) + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_gb, true, g) +
 	       "\n//@@VGPU_TU@@\n" + cg.EmitStats(key_columns, gs) + "\n//@@VGPU_TU@@\n" +
-	       cg.EmitGroupBy(spec_dp, true, g) + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_hv, true, g);
+	       cg.EmitGroupBy(spec_dp, true, g) + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_hv, true, g) +
+	       "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_dp, true, gst) + "\n//@@VGPU_TU@@\n" +
+	       cg.EmitGroupBy(spec_hv, true, gst);
 }
 
 } // namespace vgpu

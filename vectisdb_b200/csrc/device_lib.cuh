@@ -127,6 +127,84 @@ __device__ __forceinline__ void load_rows(const T *__restrict__ base, u64 row0, 
 	}
 }
 
+// ---------------------------------------------------------------------------------------------
+// Tile staging through shared memory: column chunks of a tile move with bulk asynchronous copies
+// (cp.async.bulk, the TMA engine's 1-D form) whose completion an mbarrier counts in bytes, so a CTA
+// partitions one tile from registers while the next ones are in flight. Every wait is bounded.
+
+__device__ __forceinline__ u32 smem_addr(const void *p) { return (u32)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void stage_barrier_init(u64 *bar) {
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Makes initialized barriers visible to the copy engine (call once, after the inits, before a sync).
+__device__ __forceinline__ void stage_barrier_fence() {
+	asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Thread that issues a stage's copies: announces the stage's byte count on its barrier (one arrival).
+__device__ __forceinline__ void stage_expect(u64 *bar, u32 bytes) {
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+// `bytes` (a multiple of 16) from 16-byte aligned global `src` to 16-byte aligned shared `dst`.
+__device__ __forceinline__ void stage_copy(void *dst, const void *src, u32 bytes, u64 *bar) {
+	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+	                 smem_addr(dst)),
+	             "l"(src), "r"(bytes), "r"(smem_addr(bar))
+	             : "memory");
+}
+
+__device__ __forceinline__ bool stage_try_wait(u64 *bar, u32 parity) {
+	u32 done;
+	asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+	             : "=r"(done)
+	             : "r"(smem_addr(bar)), "r"(parity)
+	             : "memory");
+	return done != 0;
+}
+
+__device__ __forceinline__ u64 global_ns() {
+	u64 t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
+}
+
+// Waits for the barrier phase of the given parity to complete; false after about one second (or 2^26
+// polls) without it: the caller records an error and gives up on the tile.
+__device__ __forceinline__ bool stage_wait(u64 *bar, u32 parity) {
+	if (stage_try_wait(bar, parity)) return true;
+	const u64 t0 = global_ns();
+	for (u32 i = 0; i < (1u << 26); ++i) {
+		if (stage_try_wait(bar, parity)) return true;
+		if (global_ns() - t0 > 1000000000ull) return false;
+	}
+	return false;
+}
+
+// R consecutive elements of a staged column (16-byte aligned when R * sizeof(T) is a multiple of 16).
+template <typename T, int R> __device__ __forceinline__ void load_stage(const T *p, T (&out)[R]) {
+	constexpr int BYTES = (int)sizeof(T) * R;
+	if constexpr (BYTES % 16 == 0) {
+		u32 words[BYTES / 4];
+#pragma unroll
+		for (int q = 0; q < BYTES / 16; ++q) {
+			const uint4 v = reinterpret_cast<const uint4 *>(p)[q];
+			words[4 * q + 0] = v.x;
+			words[4 * q + 1] = v.y;
+			words[4 * q + 2] = v.z;
+			words[4 * q + 3] = v.w;
+		}
+#pragma unroll
+		for (int r = 0; r < R; ++r) out[r] = word_element<T>(words, r);
+	} else {
+#pragma unroll
+		for (int r = 0; r < R; ++r) out[r] = p[r];
+	}
+}
+
 // Fixed-size row records (W 32-bit words, W a multiple of 4; records 32-byte aligned when W is a
 // multiple of 8). A 32-byte record moves as one 256-bit access (sm_100 global vector width): one
 // store request per scattered record instead of two half-sector ones, and one fully coalesced load

@@ -76,6 +76,14 @@ void SetKeyWords(KArgsHost &k, const PipelineCodegen::GroupBySpec &gb) {
 	}
 }
 
+// Most heavy keys one direct-partitioned group-by pre-aggregates (VGPU_GB_HEAVY_KEYS overrides 512).
+uint32_t HeavyKeyCap() {
+	if (const char *env = std::getenv("VGPU_GB_HEAVY_KEYS")) {
+		return static_cast<uint32_t>(std::min<uint64_t>(4096, std::max<uint64_t>(1, std::strtoull(env, nullptr, 10))));
+	}
+	return 512;
+}
+
 int BitsFor(uint64_t range) {
 	int b = 0;
 	while (b < 64 && (range >> b) != 0) {
@@ -151,7 +159,8 @@ private:
 	};
 	using GroupByCompiler = std::function<std::shared_ptr<Module>(const PipelineCodegen::GroupBySpec &)>;
 	HeavyPlan PlanHeavy(const PipelineCodegen::GroupBySpec &gb, const PipelineCodegen &cg, const PipelineInput &pin,
-	                    const GroupByCompiler &compile, const Geometry &g, int cb, uint64_t P, uint64_t ntiles);
+	                    const GroupByCompiler &compile, const Geometry &g, int cb, uint64_t P, uint64_t ntiles,
+	                    uint64_t extra_smem);
 
 	const std::vector<vgpu_column> &inputs_;
 	ExecOptions options_;
@@ -765,12 +774,46 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		Geometry g;
 		g.block = 256;
 		g.items = 8;
+		// Staged tiles (direct-partitioned): the partition passes' full tiles arrive in shared memory by
+		// bulk asynchronous copies, two tiles ahead, instead of as per-thread loads. Needs plain columns
+		// (no join or cross-product source, no NULLs) whose base addresses are 16-byte aligned, and room
+		// for two stages beside the counters and the heavy-key state. 512 threads × 4 rows per tile.
+		// VGPU_GB_STAGED=0 turns it off.
+		const char *staged_env = std::getenv("VGPU_GB_STAGED");
+		bool staged = gb.direct_bits > 0 && !pin.spec.join && !pin.spec.cross && cb + 14 < kKeyWord &&
+		              !(staged_env && std::strcmp(staged_env, "0") == 0);
+		for (auto &src : pin.sources) {
+			if (src.valid || (reinterpret_cast<uintptr_t>(src.data) & 15u) != 0) staged = false;
+		}
+		const int tile_rows = 2048;  // both geometries: 256 threads × 8 rows, or staged 512 × 4
+		// bytes of the two stages of the count and the scatter pass
+		uint64_t stage2_count = 2ull * tile_rows * cg.StageRowBytes(gb, false);
+		uint64_t stage2_scatter = 2ull * tile_rows * cg.StageRowBytes(gb, true);
+		if (staged) {
+			// room for the stages beside the counters and, should heavy keys be chosen, their state:
+			// pre-aggregation saves more than staging, so staging yields when both do not fit
+			HeavyPlan room;
+			room.max_keys = HeavyKeyCap();
+			room.state_bytes = static_cast<uint64_t>(PipelineCodegen::HeavySlotBytes(gb));
+			if (room.smem(P) + 128 + stage2_scatter + 1024 > static_cast<uint64_t>(props.smem_optin)) staged = false;
+		}
+		if (staged) {
+			g.block = 512;
+			g.items = 4;
+		} else {
+			stage2_count = stage2_scatter = 0;
+		}
 		if (const char *env = std::getenv("VGPU_GB_PART_BLOCK")) {  // tuning override (128..1024)
 			g.block = static_cast<int>(std::min<uint64_t>(1024, std::max<uint64_t>(128, FloorPow2(std::strtoull(env, nullptr, 10)))));
+			if (staged) {
+				stage2_count = 2ull * g.tile() * cg.StageRowBytes(gb, false);
+				stage2_scatter = 2ull * g.tile() * cg.StageRowBytes(gb, true);
+			}
 		}
+		g.staged = staged;
 		auto compile = [&](const PipelineCodegen::GroupBySpec &spec) {
 			const std::string gkey = SpecKey(pin.spec) + "|" + GroupByKey(spec, true) + "|g:" + std::to_string(g.block) +
-			                         "x" + std::to_string(g.items);
+			                         "x" + std::to_string(g.items) + (g.staged ? "s" : "");
 			return Runtime::Get().modules().GetOrCompileMemo(gkey, [&] { return cg.EmitGroupBy(spec, true, g); });
 		};
 		const uint64_t ntiles = (n + g.tile() - 1) / g.tile();
@@ -781,14 +824,24 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		// Heavy-key pre-aggregation (direct-partitioned): a sample of tiles finds the most frequent keys,
 		// whose rows the partition passes fold into per-CTA shared partial states; each CTA then writes
 		// one partial record per such key instead of one record per row.
-		HeavyPlan heavy = PlanHeavy(gb, cg, pin, compile, g, cb, P, ntiles);
+		HeavyPlan heavy = PlanHeavy(gb, cg, pin, compile, g, cb, P, ntiles, staged ? 128 + stage2_scatter : 0);
+		uint32_t *stage_err = nullptr;
+		if (staged) {
+			stage_err = arena_.AllocT<uint32_t>(1);
+			VGPU_CUDA(cudaMemsetAsync(stage_err, 0, 4, stream_));
+		}
 		for (int attempt = 0;; ++attempt) {
 			const bool use_heavy = heavy.module && attempt == 0;
 			auto module = use_heavy ? heavy.module : compile(gb);
 			const size_t smem = use_heavy ? heavy.smem(P) : part_smem;
+			// stages after the counters (and heavy-key state), 128-byte aligned
+			const size_t stage_off = staged ? ((smem + 127) & ~size_t(127)) : 0;
+			const size_t smem_count = staged ? stage_off + stage2_count : smem;
+			const size_t smem_scatter = staged ? stage_off + stage2_scatter : smem;
 			CUfunction fcount = module->Get("vgpu_gb_part_count");
-			int occ = std::max(1, Runtime::Get().MaxActiveBlocks(fcount, g.block, smem));
-			occ = std::min(occ, std::max(1, Runtime::Get().MaxActiveBlocks(module->Get("vgpu_gb_part_scatter"), g.block, smem)));
+			int occ = std::max(1, Runtime::Get().MaxActiveBlocks(fcount, g.block, smem_count));
+			occ = std::min(occ, std::max(1, Runtime::Get().MaxActiveBlocks(module->Get("vgpu_gb_part_scatter"), g.block,
+			                                                             smem_scatter)));
 			if (const char *env = std::getenv("VGPU_GB_PART_OCC")) {  // tuning override: CTAs per SM
 				occ = std::min(occ, std::max(1, std::atoi(env)));
 			}
@@ -812,16 +865,24 @@ Relation Executor::GroupBy(const PlanNode &node) {
 				a.SetPtr(cb + 11, heavy.keys);
 				a.SetPtr(cb + 12, heavy.count);
 			}
-			LaunchGenerated(*module, "vgpu_gb_part_count", static_cast<unsigned>(G), g.block, smem, stream_, a, in_bytes, n);
+			if (staged) {
+				a.Set(cb + 13, stage_off);
+				a.SetPtr(cb + 14, stage_err);
+			}
+			LaunchGenerated(*module, "vgpu_gb_part_count", static_cast<unsigned>(G), g.block, smem_count, stream_, a,
+			                in_bytes, n);
 			kern::ExclusiveScanU32(offsets, offsets, P * G, total, arena_);
 			char *records = static_cast<char *>(arena_.Alloc(n_rec * RS));
 			a.SetPtr(cb + 4, records);
 			const int scatter_rec = LaunchGenerated(*module, "vgpu_gb_part_scatter", static_cast<unsigned>(G), g.block,
-			                                        smem, stream_, a, in_bytes, n);
+			                                        smem_scatter, stream_, a, in_bytes, n);
 			if (gb.direct_bits > 0) {
 				uint64_t written = 0;
 				groups = DirectBuckets(*module, gb, pin, P, G, offsets, total, records, n_rec, RS, out, out_words, T1,
 				                       &written);
+				if (staged && ReadU32(stage_err) != 0) {
+					Fail(VGPU_ERR_CUDA, "gpu_groupby: a staged tile copy did not complete within a second");
+				}
 				// the scatter's bytes: the columns it reads once and the records it wrote
 				Runtime::Get().profiler().SetBytes(scatter_rec, in_bytes + written * RS);
 				if (use_heavy && ReadU32(heavy.overflow) != 0) continue;  // a partial sum left 64 bits: redo plainly
@@ -953,7 +1014,7 @@ Relation Executor::GroupBy(const PlanNode &node) {
 // the sampled rows. VGPU_GB_HEAVY: 0 = off, 2 = always, whatever the input size and coverage (testing).
 Executor::HeavyPlan Executor::PlanHeavy(const PipelineCodegen::GroupBySpec &gb, const PipelineCodegen &cg,
                                         const PipelineInput &pin, const GroupByCompiler &compile, const Geometry &g,
-                                        int cb, uint64_t P, uint64_t ntiles) {
+                                        int cb, uint64_t P, uint64_t ntiles, uint64_t extra_smem) {
 	HeavyPlan none;
 	int mode = 1;
 	if (const char *env = std::getenv("VGPU_GB_HEAVY")) mode = std::atoi(env);
@@ -968,16 +1029,13 @@ Executor::HeavyPlan Executor::PlanHeavy(const PipelineCodegen::GroupBySpec &gb, 
 		if (TypeSize(cg.visible()[a.column].type) != 8 || ++uses[a.column] > 1) return none;
 	}
 	const auto &props = Runtime::Get().props();
-	uint32_t K = 512;
-	if (const char *env = std::getenv("VGPU_GB_HEAVY_KEYS")) {  // tuning override
-		K = static_cast<uint32_t>(std::min<uint64_t>(4096, std::max<uint64_t>(1, std::strtoull(env, nullptr, 10))));
-	}
+	const uint32_t K = HeavyKeyCap();
 	PipelineCodegen::GroupBySpec gbh = gb;
 	gbh.heavy_slots = static_cast<int>(K);
 	HeavyPlan hp;
 	hp.max_keys = K;
 	hp.state_bytes = static_cast<uint64_t>(PipelineCodegen::HeavySlotBytes(gbh));
-	if (hp.smem(P) + 1024 > static_cast<size_t>(props.smem_optin)) return none;
+	if (hp.smem(P) + extra_smem + 1024 > static_cast<size_t>(props.smem_optin)) return none;
 	hp.module = compile(gbh);
 	const uint32_t SC = 1u << 16;
 	uint64_t *skeys = arena_.AllocT<uint64_t>(SC);
