@@ -125,3 +125,46 @@ def test_fused_join_table_forms_match_numpy(layout):
     assert np.array_equal(cols[0].data, np.array([v for v, _ in exp], np.int64))
     assert np.array_equal(cols[1].data, r1[[i for _, i in exp]])
     assert np.array_equal(cols[2].data, r2[[i for _, i in exp]])
+
+
+@pytest.mark.parametrize("values,vtype", [
+    ("small", T.INT32),      # offsets below 255: 1-byte table
+    ("medium", T.INT32),     # below 65535: 2-byte table
+    ("wide", T.INT32),       # 4-byte table with the all-ones marker
+    ("full", T.INT32),       # -1 and 0 together span every 32-bit pattern: the 8-byte table stays
+    ("negative", T.INT32),   # all negative, a narrow span of high bit patterns
+    ("short", T.INT16),      # a 2-byte right column, negative values included
+])
+def test_dense_inline_table_widths(values, vtype, monkeypatch):
+    """The single right column inlined into the dense key table, narrowed to the fewest bytes that hold
+    every value's offset from the smallest: the same matches and values as numpy and as the 8-byte form."""
+    rng = np.random.default_rng(31)
+    rk = rng.permutation(np.arange(0, 50000, dtype=np.int64))
+    n_r = len(rk)
+    np_t = np.int16 if vtype == T.INT16 else np.int32
+    rv = {"small": lambda: rng.integers(7, 200, n_r), "medium": lambda: rng.integers(-30000, 30000, n_r),
+          "wide": lambda: rng.integers(-(1 << 30), 1 << 30, n_r),
+          "full": lambda: np.where(rng.random(n_r) < 0.5, -1, rng.integers(0, 1 << 31, n_r)),
+          "negative": lambda: rng.integers(-90, -1, n_r), "short": lambda: rng.integers(-32768, 32767, n_r)}[values]()
+    rv = rv.astype(np_t)
+    lk = rng.integers(-1000, 60000, 200000).astype(np.int64)
+    lv = np.arange(len(lk), dtype=np.int64)
+    join = make_join("lk", "rk", ["lv", "rv"], make_scan(["lk", "lv"]), make_scan(["rk", "rv"]))
+    plan = make_filter([make_expr("((bool*)out)[idx] = ((const long long*)inputs[0])[row] % 2 == 0;", ["lv"],
+                                  T.BOOLEAN)], join)
+    inputs = [make_column("lk", T.INT64, lk), make_column("lv", T.INT64, lv), make_column("rk", T.INT64, rk),
+              make_column("rv", vtype, rv)]
+    pos = np.full(60000, -1, np.int64)
+    pos[rk] = np.arange(n_r)
+    hit = (lk >= 0) & (lk < 60000)
+    hit[hit] = pos[lk[hit]] >= 0
+    keep = hit & (lv % 2 == 0)
+    exp_rv = rv[pos[lk[keep]]]
+    res = {}
+    for compact in ("1", "0"):
+        monkeypatch.setenv("VGPU_JOIN_COMPACT", compact)
+        cols = _run(plan, inputs)
+        assert np.array_equal(cols[0].data, lv[keep])
+        assert np.array_equal(cols[1].data, exp_rv)
+        res[compact] = cols[1].data
+    assert np.array_equal(res["1"], res["0"])

@@ -401,7 +401,7 @@ std::string PipelineCodegen::LoadBlock(const Geometry &g, const std::vector<bool
 		o << "\t\tlong long jm[" << g.items << "];\n"
 		  << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) {\n"
 		  << "\t\t\tjm[r] = row0 + r < n ? vgpu_join_find((u64)(" << ut << ")s" << key << "[r] - a.w[" << kJoinWord + 2
-		  << "], (const u64*)a.w[" << kJoinWord << "], (const u32*)a.w[" << kJoinWord + 1 << "], a.w[" << kJoinWord + 3
+		  << "], (const u64*)a.w[" << kJoinWord << "], a.w[" << kJoinWord + 1 << "], a.w[" << kJoinWord + 3
 		  << "] >> 8, (u32)(a.w[" << kJoinWord + 3 << "] & 0xffu)) : -1ll;\n\t\t}\n";
 		for (size_t i = 0; i < spec_.sources.size(); i++) {
 			const auto &src = spec_.sources[i];

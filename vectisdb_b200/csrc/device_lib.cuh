@@ -345,9 +345,11 @@ __device__ __forceinline__ void atomic_max_i64(i64 *p, i64 v) { atomicMax(reinte
 // a probe key below that minimum wraps to a bucket past nb and misses. Returns the position or -1.
 // Dense forms (tables indexed by the biased key over the whole range, nb entries): shift == 0xff,
 // dir holds row index + 1 of the key's right row (0 = no key); shift == 0xfe, `sorted` is reused as a
-// u64 table holding (1 << 32 | the right column's 32-bit value) (0 = no key), returned as is.
-__device__ __forceinline__ long long vgpu_join_find(u64 k, const u64 *__restrict__ sorted, const u32 *__restrict__ dir,
-                                                    u64 nb, u32 shift) {
+// u64 table holding (1 << 32 | the right column's 32-bit value) (0 = no key), returned as is;
+// shift == 0xfd / 0xfc / 0xfb, `sorted` is a u8 / u16 / u32 table of value bits minus `aux` (all ones =
+// no key), returned in the 0xfe form. `aux` is the directory word (the directory pointer otherwise).
+__device__ __forceinline__ long long vgpu_join_find(u64 k, const u64 *__restrict__ sorted, u64 aux, u64 nb, u32 shift) {
+	const u32 *__restrict__ dir = (const u32 *)aux;
 	if (shift == 0xffu) {
 		if (k >= nb) return -1ll;
 		const u32 p = dir[k];
@@ -357,6 +359,21 @@ __device__ __forceinline__ long long vgpu_join_find(u64 k, const u64 *__restrict
 		if (k >= nb) return -1ll;
 		const u64 e = sorted[k];
 		return e == 0ull ? -1ll : (long long)e;
+	}
+	if (shift >= 0xfbu) {
+		if (k >= nb) return -1ll;
+		u32 e;
+		if (shift == 0xfdu) {
+			e = ((const u8 *)sorted)[k];
+			if (e == 0xffu) return -1ll;
+		} else if (shift == 0xfcu) {
+			e = ((const unsigned short *)sorted)[k];
+			if (e == 0xffffu) return -1ll;
+		} else {
+			e = ((const u32 *)sorted)[k];
+			if (e == 0xffffffffu) return -1ll;
+		}
+		return (long long)((1ull << 32) | (u64)(u32)(e + (u32)aux));
 	}
 	const u64 b = k >> shift;
 	if (b >= nb) return -1ll;

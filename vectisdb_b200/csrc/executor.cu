@@ -1191,13 +1191,30 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 	const size_t kw = TypeSize(rk->type);
 	uint64_t *rw = arena_.AllocT<uint64_t>(rn);
 	kern::WidenKeys(rk->data, kw, rn, rw, stream_);
-	uint64_t *mm = arena_.AllocT<uint64_t>(2);
+	// The join contributes one right column of at most 4 bytes without NULLs: its value can be inlined
+	// into a dense key table; the value bits' bounds come back with the key range.
+	const DevColumn *inline_col = nullptr;
+	{
+		size_t right_outs = 0;
+		for (size_t i = 0; i < outs.size(); i++) {
+			if (side[i] == 1) {
+				right_outs++;
+				inline_col = outs[i];
+			}
+		}
+		if (right_outs != 1 || TypeSize(inline_col->type) > 4 || TypeSize(inline_col->type) == 3 || inline_col->valid) {
+			inline_col = nullptr;
+		}
+	}
+	uint64_t *mm = arena_.AllocT<uint64_t>(3);  // key min, key max, value bits (min, max)
 	kern::MinMaxU64(rw, rn, mm, stream_);
-	uint64_t host_mm[2];
-	VGPU_CUDA(cudaMemcpyAsync(host_mm, mm, 16, cudaMemcpyDeviceToHost, stream_));
+	if (inline_col) kern::ValueBits(inline_col->data, TypeSize(inline_col->type), rn, reinterpret_cast<uint32_t *>(mm + 2), stream_);
+	uint64_t host_mm[3] = {0, 0, 0};
+	VGPU_CUDA(cudaMemcpyAsync(host_mm, mm, inline_col ? 24 : 16, cudaMemcpyDeviceToHost, stream_));
 	VGPU_CUDA(cudaStreamSynchronize(stream_));
 	const uint64_t bias = host_mm[0];
 	const uint64_t range = host_mm[1] - host_mm[0];
+	const uint32_t vmin = static_cast<uint32_t>(host_mm[2]), vmax = static_cast<uint32_t>(host_mm[2] >> 32);
 	const int bits = BitsFor(range);
 	kern::SubtractBias(rw, rn, bias, stream_);
 	auto add_sources = [&](bool sorted_side, const uint32_t *perm) {
@@ -1224,24 +1241,34 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 			pin.sources.push_back(c);
 		}
 	};
-	size_t right_outs = 0;
-	const DevColumn *right_col = nullptr;
-	for (size_t i = 0; i < outs.size(); i++) {
-		if (side[i] == 1) {
-			right_outs++;
-			right_col = outs[i];
-		}
-	}
 	uint32_t *dups = arena_.AllocT<uint32_t>(1);
 	bool built = false;
 	// Dense keys (range within 4x the key count, at most 2^28): a table indexed by the key over the whole
 	// range, filled without sorting. It holds the right row index, or -- when the join contributes one
 	// right column of at most 4 bytes -- that column's value itself, so a probe row costs one random
-	// read. A key met twice (many-to-many) falls back to the sorted form below.
+	// read; the value is stored as its offset from the smallest value in the fewest bytes that hold every
+	// offset (all ones marks a missing key), so the table of a small-valued column stays in L2. A key met
+	// twice (many-to-many) falls back to the sorted form below.
 	if (range < (1ull << 28) && range < 4 * rn) {
-		if (right_outs == 1 && TypeSize(right_col->type) <= 4 && TypeSize(right_col->type) != 3 && !right_col->valid) {
+		const uint64_t span = static_cast<uint64_t>(vmax) - vmin;
+		const size_t width = !inline_col ? 0 : span < 0xffull ? 1 : span < 0xffffull ? 2 : span < 0xffffffffull ? 4 : 8;
+		const char *env_c = std::getenv("VGPU_JOIN_COMPACT");  // "0": 8-byte inline entries (testing)
+		const bool compact = width != 0 && width != 8 && !(env_c && std::strcmp(env_c, "0") == 0);
+		if (compact) {
+			void *table = arena_.Alloc((range + 1) * width);
+			kern::JoinDenseCompact(rw, inline_col->data, TypeSize(inline_col->type), rn, range, vmin, table, width, dups,
+			                       stream_);
+			if (ReadU32(dups) == 0) {
+				add_sources(false, nullptr);
+				pin.spec.join_inline = true;
+				pin.join_words[0] = reinterpret_cast<uint64_t>(table);
+				pin.join_words[1] = vmin;
+				pin.join_words[3] = (width == 1 ? 0xfdu : width == 2 ? 0xfcu : 0xfbu) | ((range + 1) << 8);
+				built = true;
+			}
+		} else if (inline_col) {
 			uint64_t *table = arena_.AllocT<uint64_t>(range + 1);
-			kern::JoinDenseInline(rw, right_col->data, TypeSize(right_col->type), rn, range, table, dups, stream_);
+			kern::JoinDenseInline(rw, inline_col->data, TypeSize(inline_col->type), rn, range, table, dups, stream_);
 			if (ReadU32(dups) == 0) {
 				add_sources(false, nullptr);
 				pin.spec.join_inline = true;

@@ -377,6 +377,58 @@ __global__ void JoinDenseInlineKernel(const uint64_t *keys, const T *values, uin
 	if (local) atomicAdd(dups, local);
 }
 
+template <typename T> __global__ void ValueBitsKernel(const T *values, uint64_t n, uint32_t *bounds) {
+	uint32_t lo = 0xffffffffu, hi = 0;
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+		const uint32_t bits = static_cast<uint32_t>(values[i]);
+		lo = bits < lo ? bits : lo;
+		hi = bits > hi ? bits : hi;
+	}
+	for (int d = 16; d > 0; d >>= 1) {
+		lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, d));
+		hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, d));
+	}
+	if ((threadIdx.x & 31) == 0) {
+		atomicMin(bounds, lo);
+		atomicMax(bounds + 1, hi);
+	}
+}
+
+// Compact inline table: entry = value bits - vmin in E (all ones = no key), filled by compare-and-swap
+// from the marker; a key met twice counts in *dups. One-byte entries swap their 32-bit word (bounded
+// retries while neighbours change it; running out counts as a duplicate, so the caller falls back).
+template <typename T, typename E>
+__global__ void JoinDenseCompactKernel(const uint64_t *keys, const T *values, uint64_t n, uint32_t vmin, E *table,
+                                       uint32_t *dups) {
+	uint32_t local = 0;
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+		const uint32_t entry = static_cast<uint32_t>(values[i]) - vmin;
+		E *slot = table + keys[i];
+		if constexpr (sizeof(E) == 4) {
+			if (atomicCAS(reinterpret_cast<unsigned int *>(slot), 0xffffffffu, entry) != 0xffffffffu) local++;
+		} else if constexpr (sizeof(E) == 2) {
+			if (atomicCAS(reinterpret_cast<unsigned short *>(slot), static_cast<unsigned short>(0xffffu),
+			              static_cast<unsigned short>(entry)) != 0xffffu) {
+				local++;
+			}
+		} else {
+			unsigned int *word = reinterpret_cast<unsigned int *>(reinterpret_cast<uintptr_t>(slot) & ~uintptr_t(3));
+			const uint32_t sh = static_cast<uint32_t>(reinterpret_cast<uintptr_t>(slot) & 3u) * 8u;
+			uint32_t old = *reinterpret_cast<volatile unsigned int *>(word);
+			bool done = false;
+			for (int t = 0; t < 4096 && !done; ++t) {
+				if (((old >> sh) & 0xffu) != 0xffu) break;  // taken: a duplicate key
+				const uint32_t want = (old & ~(0xffu << sh)) | ((entry & 0xffu) << sh);
+				const uint32_t prev = atomicCAS(word, old, want);
+				done = prev == old;
+				old = prev;
+			}
+			if (!done) local++;
+		}
+	}
+	if (local) atomicAdd(dups, local);
+}
+
 __global__ void CountAdjacentEqualKernel(const uint64_t *sorted, uint64_t n, uint32_t *out) {
 	uint32_t local = 0;
 	for (uint64_t i = 1 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -497,6 +549,59 @@ void JoinDenseInline(const uint64_t *keys, const void *values, size_t width, uin
 		break;
 	default:
 		Fail(VGPU_ERR_INTERNAL, "dense inline join table: value width must be 1, 2 or 4 bytes");
+	}
+	VGPU_CUDA(cudaGetLastError());
+}
+
+void ValueBits(const void *values, size_t width, uint64_t n, uint32_t *bounds, cudaStream_t stream) {
+	VGPU_CUDA(cudaMemsetAsync(bounds, 0xff, 4, stream));
+	VGPU_CUDA(cudaMemsetAsync(bounds + 1, 0, 4, stream));
+	if (n == 0) return;
+	LaunchScope scope("value_bits", stream, n * width, n);
+	const unsigned grid = std::min<unsigned>(GridFor(n, 256), 1184);
+	switch (width) {
+	case 1: ValueBitsKernel<uint8_t><<<grid, 256, 0, stream>>>(static_cast<const uint8_t *>(values), n, bounds); break;
+	case 2: ValueBitsKernel<uint16_t><<<grid, 256, 0, stream>>>(static_cast<const uint16_t *>(values), n, bounds); break;
+	case 4: ValueBitsKernel<uint32_t><<<grid, 256, 0, stream>>>(static_cast<const uint32_t *>(values), n, bounds); break;
+	default: Fail(VGPU_ERR_INTERNAL, "value bits: width must be 1, 2 or 4 bytes");
+	}
+	VGPU_CUDA(cudaGetLastError());
+}
+
+namespace {
+template <typename E>
+void LaunchDenseCompact(const uint64_t *keys, const void *values, size_t vwidth, uint64_t n, uint32_t vmin, E *table,
+                        uint32_t *dups, cudaStream_t stream) {
+	const unsigned grid = GridFor(n, 256);
+	switch (vwidth) {
+	case 1:
+		JoinDenseCompactKernel<uint8_t, E><<<grid, 256, 0, stream>>>(keys, static_cast<const uint8_t *>(values), n, vmin,
+		                                                             table, dups);
+		break;
+	case 2:
+		JoinDenseCompactKernel<uint16_t, E><<<grid, 256, 0, stream>>>(keys, static_cast<const uint16_t *>(values), n,
+		                                                              vmin, table, dups);
+		break;
+	case 4:
+		JoinDenseCompactKernel<uint32_t, E><<<grid, 256, 0, stream>>>(keys, static_cast<const uint32_t *>(values), n,
+		                                                              vmin, table, dups);
+		break;
+	default:
+		Fail(VGPU_ERR_INTERNAL, "compact join table: value width must be 1, 2 or 4 bytes");
+	}
+}
+} // namespace
+
+void JoinDenseCompact(const uint64_t *keys, const void *values, size_t vwidth, uint64_t n, uint64_t range,
+                      uint32_t vmin, void *table, size_t width, uint32_t *dups, cudaStream_t stream) {
+	LaunchScope scope("join_dense_table", stream, n * (8 + vwidth) + (range + 1) * width, n);
+	VGPU_CUDA(cudaMemsetAsync(table, 0xff, (range + 1) * width, stream));
+	VGPU_CUDA(cudaMemsetAsync(dups, 0, 4, stream));
+	switch (width) {
+	case 1: LaunchDenseCompact(keys, values, vwidth, n, vmin, static_cast<uint8_t *>(table), dups, stream); break;
+	case 2: LaunchDenseCompact(keys, values, vwidth, n, vmin, static_cast<uint16_t *>(table), dups, stream); break;
+	case 4: LaunchDenseCompact(keys, values, vwidth, n, vmin, static_cast<uint32_t *>(table), dups, stream); break;
+	default: Fail(VGPU_ERR_INTERNAL, "compact join table: width must be 1, 2 or 4 bytes");
 	}
 	VGPU_CUDA(cudaGetLastError());
 }

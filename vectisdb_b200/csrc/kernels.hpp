@@ -58,6 +58,12 @@ void JoinDenseRows(const uint64_t *keys, uint64_t n, uint64_t range, uint32_t *t
                    cudaStream_t stream);
 void JoinDenseInline(const uint64_t *keys, const void *values, size_t width, uint64_t n, uint64_t range,
                      uint64_t *table, uint32_t *dups, cudaStream_t stream);
+//! Smallest and largest raw bits (zero-extended to 32) of a 1-, 2- or 4-byte column: bounds[0], bounds[1].
+void ValueBits(const void *values, size_t width, uint64_t n, uint32_t *bounds, cudaStream_t stream);
+//! The inline table in `width` (1, 2 or 4) bytes per key: table[k] = value bits - vmin, all ones = no
+//! key (every value's offset must stay below that marker). *dups = keys met more than once.
+void JoinDenseCompact(const uint64_t *keys, const void *values, size_t vwidth, uint64_t n, uint64_t range,
+                      uint32_t vmin, void *table, size_t width, uint32_t *dups, cudaStream_t stream);
 //! *out = number of positions i > 0 with sorted[i] == sorted[i - 1].
 void CountAdjacentEqual(const uint64_t *sorted, uint64_t n, uint32_t *out, cudaStream_t stream);
 
