@@ -605,13 +605,17 @@ std::string InitValue(const Field &f) {
 }
 
 // Update of table T (u64 arrays T_f at slot S) with the value expression `v` of aggregate field f.
+// `shared`: the table is in shared memory, where a count moves as a 32-bit atomic on its low word with
+// an explicit carry into the high word (cheaper there than a 64-bit atomic, and exact).
 std::string UpdateCode(const std::vector<Field> &fields, const std::string &tab, const std::string &slot,
-                       const std::vector<std::string> &agg_values) {
+                       const std::vector<std::string> &agg_values, bool shared) {
 	std::ostringstream o;
 	for (size_t i = 0; i < fields.size(); i++) {
 		auto &f = fields[i];
 		std::string p = tab + std::to_string(i) + " + " + slot;
-		if (f.kind == "cnt") {
+		if (f.kind == "cnt" && shared) {
+			o << "\t\t\t{ u32 *w_ = (u32*)(" << p << "); if (atomicAdd(w_, 1u) == 0xffffffffu) atomicAdd(w_ + 1, 1u); }\n";
+		} else if (f.kind == "cnt") {
 			o << "\t\t\tatomicAdd(" << p << ", 1ull);\n";
 		} else if (f.kind == "f64") {
 			o << "\t\t\tatomicAdd((double*)(" << p << "), (double)(" << agg_values[f.agg] << "));\n";
@@ -859,7 +863,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		  << "\tfor (u64 tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n"
 		  << LoadBlock(g, needed, false) << item_head << chain_code_ << "\t\tif (keep) {\n"
 		  << "\t\t\tconst u64 slot = " << pack.str() << ";\n"
-		  << UpdateCode(fields, "T", "slot", pipe_values) << "\t\t}\n\t\t}\n\t}\n\t__syncthreads();\n";
+		  << UpdateCode(fields, "T", "slot", pipe_values, true) << "\t\t}\n\t\t}\n\t}\n\t__syncthreads();\n";
 		for (int f = 0; f < F; f++) {
 			o << "\tu64 *G" << f << " = (u64*)a.w[" << cb + 1 + f << "];\n";
 		}
@@ -1923,8 +1927,8 @@ std::string PipelineCodegen::EmitBatchGroupBy(const GroupBySpec &gb, const Geome
 	  << "\t\tconst u64 row = row0 + r; (void)row;\n\t\tbool keep = row < t1;\n"
 	  << chain_code_ << "\t\tif (keep) {\n"
 	  << "\t\t\tconst u64 slot = " << pack.str() << ";\n"
-	  << "\t\t\tif (cur_sm) {\n" << UpdateCode(fields, "T", "slot", values) << "\t\t\t} else {\n"
-	  << UpdateCode(fields, "G", "slot", values) << "\t\t\t}\n"
+	  << "\t\t\tif (cur_sm) {\n" << UpdateCode(fields, "T", "slot", values, true) << "\t\t\t} else {\n"
+	  << UpdateCode(fields, "G", "slot", values, false) << "\t\t\t}\n"
 	  << "\t\t}\n\t\t}\n\t\t}\n\t}\n"
 	  << "\tif (cur_sm) {\n" << flush.str() << "\t}\n}\n\n";
 
