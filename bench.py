@@ -576,7 +576,7 @@ def main():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c2b", "c3", "c4"])
     p.add_argument("--e2e-steps", type=int, default=5)
-    p.add_argument("--blocks", type=int, default=5, help="timed blocks of --steps steps; the median is reported")
+    p.add_argument("--blocks", type=int, default=7, help="timed blocks of --steps steps; the median is reported")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--rows", type=int, default=0, help="small-case size for profiling (0 = the full workload)")
     args = p.parse_args()

@@ -1380,8 +1380,8 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		// args: cb+0 = work items (uint4: partition, first row, end row, split index or ~0),
 		//   cb+1 = item count (u32*), cb+2 = records, cb+3 = global tables of split partitions (u64,
 		//   [split][field][D]), cb+4 = split info (u32 [2s] chunks, [2s+1] completed chunks),
-		//   cb+5 = work counter (u32*), cb+6 = output count (u64*), cb+7 = split partitions (init
-		//   kernel), cb+8.. outputs.
+		//   cb+5 = work counter (u32*), cb+6 = output count (u64*), cb+7 = split partition count (u32*,
+		//   read by the init kernel), cb+8.. outputs.
 		// Shared table of D slots, one array per state word: 8-byte arrays (FP64 sums, MIN/MAX) first,
 		// then 32-bit arrays (COUNT, and four words per integer SUM accumulated with 32-bit atomics).
 		const int dbits = gb.direct_bits;
@@ -1616,7 +1616,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		// global tables of split partitions: identity values
 		o << "extern \"C\" __global__ void vgpu_gb_dtab_init(KArgs a) {\n"
 		  << "\tu64 *g = (u64*)a.w[" << cb + 3 << "];\n"
-		  << "\tconst u64 total = a.w[" << cb + 7 << "] * " << F * D << "ull;\n"
+		  << "\tconst u64 total = (u64)*(const u32*)a.w[" << cb + 7 << "] * " << F * D << "ull;\n"
 		  << "\tfor (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < total; i += (u64)gridDim.x * blockDim.x) {\n"
 		  << "\t\tconst u32 f = (u32)((i / " << D << "ull) % " << F << "u);\n"
 		  << "\t\tu64 v = 0ull;\n";

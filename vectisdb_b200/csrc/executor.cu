@@ -138,7 +138,8 @@ private:
 	void FillArgs(const PipelineInput &pin, KArgsHost &args);
 	uint64_t DirectBuckets(Module &module, const PipelineCodegen::GroupBySpec &gb, const PipelineInput &pin, uint64_t P,
 	                       uint64_t G, const uint32_t *offsets, const uint32_t *total, const char *records, uint64_t n,
-	                       uint64_t RS, Relation &out, int out_words, int threads, uint64_t *records_written);
+	                       uint64_t RS, Relation &out, int out_words, int threads, uint32_t *status,
+	                       uint32_t *status_host);
 	uint64_t ReadU64(const void *dev);
 	uint32_t ReadU32(const void *dev);
 	//! Heavy keys chosen for the partition passes of a direct-partitioned group-by (no module: none).
@@ -825,11 +826,13 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		// whose rows the partition passes fold into per-CTA shared partial states; each CTA then writes
 		// one partial record per such key instead of one record per row.
 		HeavyPlan heavy = PlanHeavy(gb, cg, pin, compile, g, cb, P, ntiles, staged ? 128 + stage2_scatter : 0);
-		uint32_t *stage_err = nullptr;
-		if (staged) {
-			stage_err = arena_.AllocT<uint32_t>(1);
-			VGPU_CUDA(cudaMemsetAsync(stage_err, 0, 4, stream_));
-		}
+		// status words read back once per attempt: [0, 6) the bucket pass's plan and group count,
+		// [6] heavy-key partial overflow, [7] staging error
+		uint32_t *status = arena_.AllocT<uint32_t>(8);
+		uint32_t status_host[8];
+		VGPU_CUDA(cudaMemsetAsync(status, 0, 32, stream_));
+		if (heavy.module) heavy.overflow = status + 6;
+		uint32_t *stage_err = staged ? status + 7 : nullptr;
 		for (int attempt = 0;; ++attempt) {
 			const bool use_heavy = heavy.module && attempt == 0;
 			auto module = use_heavy ? heavy.module : compile(gb);
@@ -877,15 +880,14 @@ Relation Executor::GroupBy(const PlanNode &node) {
 			const int scatter_rec = LaunchGenerated(*module, "vgpu_gb_part_scatter", static_cast<unsigned>(G), g.block,
 			                                        smem_scatter, stream_, a, in_bytes, n);
 			if (gb.direct_bits > 0) {
-				uint64_t written = 0;
 				groups = DirectBuckets(*module, gb, pin, P, G, offsets, total, records, n_rec, RS, out, out_words, T1,
-				                       &written);
-				if (staged && ReadU32(stage_err) != 0) {
+				                       status, status_host);
+				if (staged && status_host[7] != 0) {
 					Fail(VGPU_ERR_CUDA, "gpu_groupby: a staged tile copy did not complete within a second");
 				}
 				// the scatter's bytes: the columns it reads once and the records it wrote
-				Runtime::Get().profiler().SetBytes(scatter_rec, in_bytes + written * RS);
-				if (use_heavy && ReadU32(heavy.overflow) != 0) continue;  // a partial sum left 64 bits: redo plainly
+				Runtime::Get().profiler().SetBytes(scatter_rec, in_bytes + static_cast<uint64_t>(status_host[3]) * RS);
+				if (use_heavy && status_host[6] != 0) continue;  // a partial sum left 64 bits: redo plainly
 				for (auto &c : out) c.rows = groups;
 				return out;
 			}
@@ -1073,10 +1075,13 @@ Executor::HeavyPlan Executor::PlanHeavy(const PipelineCodegen::GroupBySpec &gb, 
 // Bucket pass of the direct-partitioned group-by: a longest-first work list of (partition, row range)
 // items, partitions too large for one CTA split into chunks merged through global tables, then one
 // persistent launch over the list. Returns the group count.
+// `status` (device, 8 words, the caller's flags in [6] and [7]) holds the work plan's counts in [0, 4)
+// and the group count in [4, 6); it is read back once, into `status_host`, after the bucket pass --
+// the only host round trip of the pass.
 uint64_t Executor::DirectBuckets(Module &module, const PipelineCodegen::GroupBySpec &gb, const PipelineInput &pin,
                                  uint64_t P, uint64_t G, const uint32_t *offsets, const uint32_t *total,
                                  const char *records, uint64_t n, uint64_t RS, Relation &out, int out_words,
-                                 int threads, uint64_t *records_written) {
+                                 int threads, uint32_t *status, uint32_t *status_host) {
 	const auto &props = Runtime::Get().props();
 	const uint64_t D = 1ull << gb.direct_bits;
 	const uint64_t F = static_cast<uint64_t>(PipelineCodegen::StateWords(gb));
@@ -1090,22 +1095,17 @@ uint64_t Executor::DirectBuckets(Module &module, const PipelineCodegen::GroupByS
 		min_split = static_cast<uint32_t>(std::max<uint64_t>(256, std::strtoull(env, nullptr, 10)));
 	}
 	const uint64_t cap = kern::PlanWorkCapacity(static_cast<uint32_t>(P), n, min_split);
-	const uint32_t max_split = static_cast<uint32_t>(n / min_split + 1);
+	// Split partitions: each has more than max(min_split, ceil(rows / (4 * ctas))) rows, so there are
+	// fewer than this many, and their tables are sized without reading the plan back.
+	const uint32_t max_split = static_cast<uint32_t>(std::min<uint64_t>({P, 4ull * ctas, n / min_split + 1}));
 	void *items = arena_.Alloc(cap * 16);
-	uint32_t *control = arena_.AllocT<uint32_t>(4);  // [0] items, [1] split partitions, [2] work counter
+	uint32_t *control = status;  // [0] items, [1] split partitions, [2] work counter, [3] partitioned rows
 	uint32_t *split_info = arena_.AllocT<uint32_t>(2ull * max_split);
-	uint64_t *out_count = arena_.AllocT<uint64_t>(1);
-	VGPU_CUDA(cudaMemsetAsync(control, 0, 16, stream_));
-	VGPU_CUDA(cudaMemsetAsync(out_count, 0, 8, stream_));
+	uint64_t *out_count = reinterpret_cast<uint64_t *>(status + 4);
+	VGPU_CUDA(cudaMemsetAsync(status, 0, 24, stream_));
 	kern::PlanWork(offsets, G, static_cast<uint32_t>(P), total, min_split, ctas, items, control, split_info, max_split,
 	               stream_);
-	uint32_t plan[3];  // split partitions, work counter, partitioned rows (one read-back)
-	VGPU_CUDA(cudaMemcpyAsync(plan, control + 1, sizeof(plan), cudaMemcpyDeviceToHost, stream_));
-	VGPU_CUDA(cudaStreamSynchronize(stream_));
-	const uint32_t n_split = plan[0];
-	*records_written = plan[2];
-	if (n_split > max_split) Fail(VGPU_ERR_INTERNAL, "gpu_groupby: work plan produced more splits than planned");
-	uint64_t *gtab = n_split ? arena_.AllocT<uint64_t>(static_cast<uint64_t>(n_split) * F * D) : nullptr;
+	uint64_t *gtab = arena_.AllocT<uint64_t>(static_cast<uint64_t>(max_split) * F * D);
 	const int cb = 2 + 2 * static_cast<int>(pin.sources.size());  // first consumer argument word
 	KArgsHost b;
 	FillArgs(pin, b);
@@ -1117,18 +1117,24 @@ uint64_t Executor::DirectBuckets(Module &module, const PipelineCodegen::GroupByS
 	b.SetPtr(cb + 4, split_info);
 	b.SetPtr(cb + 5, control + 2);
 	b.SetPtr(cb + 6, out_count);
-	b.Set(cb + 7, n_split);
+	b.SetPtr(cb + 7, control + 1);
 	for (int w = 0; w < out_words; w++) b.SetPtr(cb + 8 + w, out[w].data);
-	if (n_split) {
-		const uint64_t words = static_cast<uint64_t>(n_split) * F * D;
+	{
+		// initializes the tables of the splits the plan made (a count it reads on the device)
+		const uint64_t words = static_cast<uint64_t>(max_split) * F * D;
 		const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((words + 255) / 256, uint64_t(props.sm_count) * 8));
-		LaunchGenerated(module, "vgpu_gb_dtab_init", grid, 256, 0, stream_, b, words * 8, 0);
+		LaunchGenerated(module, "vgpu_gb_dtab_init", grid, 256, 0, stream_, b, 0, 0);
 	}
 	const int rec = LaunchGenerated(module, "vgpu_gb_dbucket", ctas, threads, smem, stream_, b, n * RS, n);
-	const uint64_t groups = ReadU64(out_count);
+	VGPU_CUDA(cudaMemcpyAsync(status_host, status, 32, cudaMemcpyDeviceToHost, stream_));
+	VGPU_CUDA(cudaStreamSynchronize(stream_));
+	if (status_host[1] > max_split) {
+		Fail(VGPU_ERR_INTERNAL, "gpu_groupby: work plan produced more splits than its bound");
+	}
+	const uint64_t groups = static_cast<uint64_t>(status_host[4]) | (static_cast<uint64_t>(status_host[5]) << 32);
 	uint64_t out_row = 0;
 	for (int w = 0; w < out_words; w++) out_row += TypeSize(out[w].type);
-	Runtime::Get().profiler().SetBytes(rec, plan[2] * RS + groups * out_row);  // records in, groups out
+	Runtime::Get().profiler().SetBytes(rec, status_host[3] * RS + groups * out_row);  // records in, groups out
 	return groups;
 }
 

@@ -457,7 +457,10 @@ __global__ void __launch_bounds__(kPlanBlock) PlanWorkKernel(const uint32_t *off
 		n_split = 0;
 		// chunks small enough that every CTA gets several items on average
 		const uint32_t total = *total_rows;
-		const uint32_t even = static_cast<uint32_t>(total / (4ull * (ctas ? ctas : 1)));
+		// rounded up, so fewer than 4 * ctas partitions exceed it: the caller sizes the split tables from
+		// that bound without reading the plan back
+		const uint64_t quarter = 4ull * (ctas ? ctas : 1);
+		const uint32_t even = static_cast<uint32_t>((total + quarter - 1) / quarter);
 		split_rows = even > min_split ? even : min_split;
 	}
 	__syncthreads();

@@ -70,7 +70,8 @@ void CountAdjacentEqual(const uint64_t *sorted, uint64_t n, uint32_t *out, cudaS
 //! Work list of a partitioned aggregation pass over `P` partitions whose row ranges start at
 //! offsets[p * stride] (the last ends at *total_rows): 16-byte items (partition, first row, end row,
 //! split index or ~0u), longest first, into `items` (capacity PlanWorkCapacity). Partitions larger
-//! than max(min_split, total / (4 * ctas)) rows are split into chunks; chunks of one partition share a
+//! than max(min_split, ceil(total / (4 * ctas))) rows are split into chunks (so at most 4 * ctas and
+//! at most total / min_split partitions are split); chunks of one partition share a
 //! split index s with split_info[2s] = chunk count and split_info[2s+1] = 0 (a completion counter).
 //! counts[0] = items, counts[1] = split partitions (split_info is written for the first max_split),
 //! counts[3] = *total_rows.
