@@ -1114,7 +1114,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		                             dmask + ") ? (int)(vgpu_hmap[(u32)(k0 >> " + std::to_string(dbits) +
 		                             ")] >> 16) : -1)";
 		// sample: one tile per CTA at a stride, counts of the mixed keys of the kept rows
-		o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_gb_sample(KArgs a) {\n"
+		o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << (g.min_blocks > 0 ? ", " + std::to_string(g.min_blocks) : std::string()) << ") vgpu_gb_sample(KArgs a) {\n"
 		  << kKernelHead
 		  << "\tu64 *skeys = (u64*)a.w[" << cb + 6 << "];\n\tu32 *scount = (u32*)a.w[" << cb + 7 << "];\n"
 		  << "\tconst u32 SC = (u32)a.w[" << cb + 8 << "];\n"
@@ -1128,7 +1128,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		  << "\t\t\t\ts = (s + 1) & (SC - 1);\n\t\t\t}\n"
 		  << "\t\t}\n\t\t}\n}\n\n";
 		// count: heavy rows are not counted; every CTA reserves one partial record per heavy key
-		o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_gb_part_count(KArgs a) {\n"
+		o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << (g.min_blocks > 0 ? ", " + std::to_string(g.min_blocks) : std::string()) << ") vgpu_gb_part_count(KArgs a) {\n"
 		  << kKernelHead << "\textern __shared__ __align__(16) u32 vgpu_smem[];\n\tu32 *vgpu_hist = vgpu_smem;\n"
 		  << "\tconst u32 P = (u32)a.w[" << cb << "]; const int pbits = (int)a.w[" << cb + 1 << "]; (void)pbits;\n"
 		  << "\tconst u64 tpc = a.w[" << cb + 2 << "];\n"
@@ -1194,7 +1194,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			hflush << "\t\t\t{ const u64 b = " << bits << "; rw[" << wi << "] = (u32)b; rw[" << wi + 1
 			       << "] = (u32)(b >> 32); }\n";
 		}
-		o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_gb_part_scatter(KArgs a) {\n"
+		o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << (g.min_blocks > 0 ? ", " + std::to_string(g.min_blocks) : std::string()) << ") vgpu_gb_part_scatter(KArgs a) {\n"
 		  << kKernelHead << "\textern __shared__ __align__(16) u32 vgpu_smem[];\n\tu32 *vgpu_cursor = vgpu_smem;\n"
 		  << "\tconst u32 P = (u32)a.w[" << cb << "]; const int pbits = (int)a.w[" << cb + 1 << "]; (void)pbits;\n"
 		  << "\tconst u64 tpc = a.w[" << cb + 2 << "];\n"
@@ -1246,7 +1246,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		  << "\t\t{\n" << hflush.str()
 		  << "\t\t\tstore_record<" << RW << ">(rec_out + (u64)pos * " << RS << ", rw);\n\t\t}\n\t}\n}\n\n";
 	} else {
-	o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_gb_part_count(KArgs a) {\n"
+	o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << (g.min_blocks > 0 ? ", " + std::to_string(g.min_blocks) : std::string()) << ") vgpu_gb_part_count(KArgs a) {\n"
 	  << kKernelHead << "\textern __shared__ __align__(16) u32 vgpu_hist[];\n"
 	  << "\tconst u32 P = (u32)a.w[" << cb << "]; const int pbits = (int)a.w[" << cb + 1 << "];\n"
 	  << "\tconst u64 tpc = a.w[" << cb + 2 << "];\n"
@@ -1262,7 +1262,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 	  << "\tfor (u32 p = threadIdx.x; p < P; p += " << g.block
 	  << ") counts[(u64)p * gridDim.x + blockIdx.x] = vgpu_hist[p];\n}\n\n";
 
-	o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_gb_part_scatter(KArgs a) {\n"
+	o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << (g.min_blocks > 0 ? ", " + std::to_string(g.min_blocks) : std::string()) << ") vgpu_gb_part_scatter(KArgs a) {\n"
 	  << kKernelHead << "\textern __shared__ __align__(16) u32 vgpu_cursor[];\n"
 	  << "\tconst u32 P = (u32)a.w[" << cb << "]; const int pbits = (int)a.w[" << cb + 1 << "];\n"
 	  << "\tconst u64 tpc = a.w[" << cb + 2 << "];\n"

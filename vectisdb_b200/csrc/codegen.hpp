@@ -56,6 +56,8 @@ struct Geometry {
 	// Direct-partitioned partition passes only: full tiles arrive through two shared-memory stages
 	// filled by bulk asynchronous copies (plain columns, 16-byte aligned, no NULLs, no join source).
 	bool staged = false;
+	// > 0: CTAs per SM the partition kernels are compiled for (__launch_bounds__ minimum blocks).
+	int min_blocks = 0;
 	int tile() const {
 		return block * items;
 	}

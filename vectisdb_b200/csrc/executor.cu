@@ -778,7 +778,7 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		// Staged tiles (direct-partitioned): the partition passes' full tiles arrive in shared memory by
 		// bulk asynchronous copies, two tiles ahead, instead of as per-thread loads. Needs plain columns
 		// (no join or cross-product source, no NULLs) whose base addresses are 16-byte aligned, and room
-		// for two stages beside the counters and the heavy-key state. 512 threads × 4 rows per tile.
+		// for two stages beside the counters and the heavy-key state. 1024 threads × 2 rows per tile.
 		// VGPU_GB_STAGED=0 turns it off.
 		const char *staged_env = std::getenv("VGPU_GB_STAGED");
 		bool staged = gb.direct_bits > 0 && !pin.spec.join && !pin.spec.cross && cb + 14 < kKeyWord &&
@@ -786,35 +786,42 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		for (auto &src : pin.sources) {
 			if (src.valid || (reinterpret_cast<uintptr_t>(src.data) & 15u) != 0) staged = false;
 		}
-		const int tile_rows = 2048;  // both geometries: 256 threads × 8 rows, or staged 512 × 4
+		if (staged) {
+			// 32 warps per SM (one CTA, registers capped at 64 per thread): the passes are latency-bound on
+			// shared-memory atomics, so more warps beat more rows per thread
+			g.block = 1024;
+			g.items = 2;
+			g.min_blocks = 1;
+		}
+		// tuning overrides: threads per CTA (128..1024), rows per thread (1..8), CTAs per SM to compile for
+		if (const char *env = std::getenv("VGPU_GB_PART_BLOCK")) {
+			g.block = static_cast<int>(std::min<uint64_t>(1024, std::max<uint64_t>(128, FloorPow2(std::strtoull(env, nullptr, 10)))));
+		}
+		if (const char *env = std::getenv("VGPU_GB_PART_ITEMS")) {
+			g.items = static_cast<int>(std::min<uint64_t>(8, std::max<uint64_t>(1, FloorPow2(std::strtoull(env, nullptr, 10)))));
+		}
+		if (const char *env = std::getenv("VGPU_GB_PART_MINB")) g.min_blocks = std::max(0, std::min(4, std::atoi(env)));
 		// bytes of the two stages of the count and the scatter pass
-		uint64_t stage2_count = 2ull * tile_rows * cg.StageRowBytes(gb, false);
-		uint64_t stage2_scatter = 2ull * tile_rows * cg.StageRowBytes(gb, true);
+		uint64_t stage2_count = staged ? 2ull * g.tile() * cg.StageRowBytes(gb, false) : 0;
+		uint64_t stage2_scatter = staged ? 2ull * g.tile() * cg.StageRowBytes(gb, true) : 0;
 		if (staged) {
 			// room for the stages beside the counters and, should heavy keys be chosen, their state:
 			// pre-aggregation saves more than staging, so staging yields when both do not fit
 			HeavyPlan room;
 			room.max_keys = HeavyKeyCap();
 			room.state_bytes = static_cast<uint64_t>(PipelineCodegen::HeavySlotBytes(gb));
-			if (room.smem(P) + 128 + stage2_scatter + 1024 > static_cast<uint64_t>(props.smem_optin)) staged = false;
-		}
-		if (staged) {
-			g.block = 512;
-			g.items = 4;
-		} else {
-			stage2_count = stage2_scatter = 0;
-		}
-		if (const char *env = std::getenv("VGPU_GB_PART_BLOCK")) {  // tuning override (128..1024)
-			g.block = static_cast<int>(std::min<uint64_t>(1024, std::max<uint64_t>(128, FloorPow2(std::strtoull(env, nullptr, 10)))));
-			if (staged) {
-				stage2_count = 2ull * g.tile() * cg.StageRowBytes(gb, false);
-				stage2_scatter = 2ull * g.tile() * cg.StageRowBytes(gb, true);
+			if (room.smem(P) + 128 + stage2_scatter + 1024 > static_cast<uint64_t>(props.smem_optin)) {
+				staged = false;
+				stage2_count = stage2_scatter = 0;
+				g.block = 256;
+				g.items = 8;
+				g.min_blocks = 0;
 			}
 		}
 		g.staged = staged;
 		auto compile = [&](const PipelineCodegen::GroupBySpec &spec) {
 			const std::string gkey = SpecKey(pin.spec) + "|" + GroupByKey(spec, true) + "|g:" + std::to_string(g.block) +
-			                         "x" + std::to_string(g.items) + (g.staged ? "s" : "");
+			                         "x" + std::to_string(g.items) + (g.staged ? "s" : "") + "m" + std::to_string(g.min_blocks);
 			return Runtime::Get().modules().GetOrCompileMemo(gkey, [&] { return cg.EmitGroupBy(spec, true, g); });
 		};
 		const uint64_t ntiles = (n + g.tile() - 1) / g.tile();
