@@ -641,12 +641,11 @@ def main():
     profile_drain()
     profile_enable(False)
 
-    # Timed blocks of exactly K steps, each bracketed by a barrier and a device synchronize. After an
-    # idle gap of some milliseconds the GPU drops its clocks, and steps shortly after one have stalled
-    # for up to a second with the host asleep in the driver. So the GPU is kept busy for half a second
-    # first, blocks follow one another with two untimed steps between them and no host-side work (the
-    # profiler's records are collected after the last block), and the line reports the median block
-    # (every block's time is listed beside it).
+    # Timed blocks of exactly K steps, each bracketed by a barrier and a device synchronize, after half
+    # a second of busy lead-in; two untimed steps between blocks and no host-side work (the profiler's
+    # records are collected after the last block). The line reports the median block and lists every
+    # block: a step that stalls in the driver (memory-pool remapping did, before the engine kept its
+    # pool reserve ahead of the working set) shows up in one block without deciding the number.
     t_hot = time.time()
     while time.time() - t_hot < 0.5:
         step().free()

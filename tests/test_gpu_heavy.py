@@ -50,6 +50,8 @@ def _check_c1(wl, cols):
     (1 << 18, {"VGPU_GB_SPLIT_ROWS": "256"}),               # split partitions merged through global tables
     (1 << 18, {"VGPU_GB_DIRECT_BITS": "8", "VGPU_GB_BUCKET_THREADS": "128"}),
     (1 << 18, {"VGPU_GB_HEAVY_KEYS": "8"}),                 # few keys: the threshold caps the selection
+    ((1 << 20) + 12345, {}),                                # staged tiles with a partial tail tile
+    ((1 << 20) + 12345, {"VGPU_GB_STAGED": "0"}),           # the same through per-thread loads
 ])
 def test_c1_forced_heavy_keys_match_oracle(n, env, monkeypatch):
     monkeypatch.setenv("VGPU_GB_STRATEGY", "direct")

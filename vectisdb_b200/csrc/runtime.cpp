@@ -77,6 +77,34 @@ void DeviceAllocator::EnsureBudgetLocked() {
 	budget_set_ = true;
 }
 
+// The stream-ordered pool keeps what it has mapped (release threshold at the maximum), but a request
+// larger than any of its free ranges makes it unmap free blocks and map their pages again for the new
+// range: UVM driver calls that blocked the calling thread for 30 ms to 1 s at a time on the B200s
+// (seen with 4 GB partition intermediates). So the pool's reserve is kept at twice the peak bytes in
+// use (within the budget, in 1 GiB steps), grown ahead of the request by one allocation released at
+// once in stream order: requests then find a free range without remapping.
+void DeviceAllocator::GrowReserve(uint64_t in_use, cudaStream_t stream) {
+	constexpr uint64_t kStep = 1ull << 30;
+	const uint64_t want = std::min<uint64_t>(budget_, (2 * in_use + kStep - 1) / kStep * kStep);
+	if (want <= reserve_target_) return;
+	cudaMemPool_t pool;
+	int device = 0;
+	if (cudaGetDevice(&device) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) {
+		cudaGetLastError();
+		return;
+	}
+	uint64_t reserved = 0;
+	cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+	reserve_target_ = want;
+	if (reserved >= want) return;
+	void *block = nullptr;
+	if (cudaMallocAsync(&block, want - reserved, stream) == cudaSuccess) {
+		cudaFreeAsync(block, stream);
+	} else {
+		cudaGetLastError();  // no room to grow ahead: requests map on demand, as before
+	}
+}
+
 void *DeviceAllocator::Alloc(size_t bytes, cudaStream_t stream) {
 	if (bytes == 0) {
 		bytes = 16; // a valid, distinct pointer for empty columns
@@ -94,6 +122,7 @@ void *DeviceAllocator::Alloc(size_t bytes, cudaStream_t stream) {
 		in_use_ += bytes;
 		peak_ = std::max(peak_, in_use_);
 		allocations_++;
+		if (2 * in_use_ > reserve_target_) GrowReserve(in_use_, stream);
 	}
 	void *ptr = nullptr;
 	cudaError_t err = cudaMallocAsync(&ptr, bytes, stream);

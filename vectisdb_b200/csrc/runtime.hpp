@@ -66,9 +66,11 @@ public:
 
 private:
 	void EnsureBudgetLocked();
+	void GrowReserve(uint64_t in_use, cudaStream_t stream);
 	std::mutex mu_;
 	bool budget_set_ = false;
 	uint64_t budget_ = 0;
+	uint64_t reserve_target_ = 0;  // pool bytes kept mapped (see GrowReserve)
 	uint64_t in_use_ = 0;
 	uint64_t peak_ = 0;
 	uint64_t allocations_ = 0;
