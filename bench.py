@@ -533,7 +533,9 @@ def run_c4(args, world, rank, local):
     # warm-up: every kernel shape of the mix compiled, the memory pool grown to the mix's peak
     serve(1e6, 8, 64)
     serve(1e6, 1, 1)
-    rates = [float(r) for r in (50, 100, 200, 400, 800, 1600)]
+    # to saturation: at the top rates the 160 requests arrive within a few milliseconds, so the served
+    # and serial rows/s there are the two executors' capacities, not the arrival rate
+    rates = [float(r) for r in (50, 100, 200, 400, 800, 1600, 3200, 6400, 12800, 25600)]
     sampler = ClockSampler(local)
     sampler.start()
     sampler.mark_begin()
@@ -609,6 +611,10 @@ def main():
     engine = GpuEngine.instance()
     stream = torch.cuda.current_stream()
 
+    # Every timed step does the whole query: derived structures the engine can keep across queries
+    # (a join's dense table over a cached right side) are rebuilt each step; the kept-table figure is
+    # measured separately below.
+    os.environ["VGPU_JOIN_CACHE"] = "0"
     # Base columns resident in the device column cache (staged once, outside the timed region).
     ColumnCache.init(0.6)
     names_in_order = [c.name for c in wl.inputs]
@@ -684,6 +690,30 @@ def main():
     launches //= args.blocks
     elapsed_ms = float(np.median(blocks))
     value = wl.rows * args.steps * world / (elapsed_ms / 1000.0)
+
+    # A repeated join keeps its dense right-side table (the engine's join-table cache): the same query
+    # timed again with that reuse, reported beside the headline, never as it.
+    kept = None
+    if name == "c2":
+        os.environ["VGPU_JOIN_CACHE"] = "1"
+        for _ in range(3):
+            step().free()
+        torch.cuda.synchronize()
+        k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k0.record(stream)
+        last = None
+        for i in range(args.steps):
+            r = step()
+            if last is not None:
+                last.free()
+            last = r
+        k1.record(stream)
+        torch.cuda.synchronize()
+        last.free()
+        os.environ["VGPU_JOIN_CACHE"] = "0"
+        kms = k0.elapsed_time(k1) / args.steps
+        kept = {"ms_per_step": kms, "value": wl.rows * world / (kms / 1000.0),
+                "note": "right-side dense table kept across steps (not the headline)"}
 
     # passing rows (for per-kernel algorithmic bytes): one host-output run
     res_host = engine.execute_plan(wl.plan, [], ExecuteOptions(serve_whole_scan_from_cache=True))
@@ -789,6 +819,7 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
             "result_groups": groups,
+            "kept_join_table": kept,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -168,3 +168,49 @@ def test_dense_inline_table_widths(values, vtype, monkeypatch):
         assert np.array_equal(cols[1].data, exp_rv)
         res[compact] = cols[1].data
     assert np.array_equal(res["1"], res["0"])
+
+
+def test_join_table_kept_across_queries_until_invalidated():
+    """A right side read from the column cache: the second identical join reuses the dense table built
+    by the first (no build launch), and after the build table is invalidated and staged again with new
+    payload values the join rebuilds and returns the new values."""
+    from vectisdb_b200 import ColumnCache, ExecuteOptions, GpuTableRef
+    from vectisdb_b200.engine import profile_drain, profile_enable
+    rng = np.random.default_rng(17)
+    rk = rng.permutation(np.arange(0, 40000, dtype=np.int64))
+    lk = rng.integers(-100, 45000, 150000).astype(np.int64)
+    lv = rng.integers(-1000, 1000, len(lk)).astype(np.int64)
+    t_b, t_p = GpuTableRef("memory", "main", "jc_build"), GpuTableRef("memory", "main", "jc_probe")
+    ColumnCache.put_table(t_p, [make_column("lk", T.INT64, lk), make_column("lv", T.INT64, lv)])
+    plan = make_group_by(["rg"], [make_aggregate(A.SUM, "lv", T.HUGEINT), make_aggregate(A.COUNT_STAR, "", T.INT64)],
+                         make_join("lk", "rk", ["rg", "lv"], make_scan(["lk", "lv"], t_p), make_scan(["rk", "rg"], t_b)))
+    opts = ExecuteOptions(serve_whole_scan_from_cache=True)
+    from vectisdb_b200.engine import hugeint_to_int
+
+    def run(rg):
+        profile_enable(True)
+        profile_drain()
+        try:
+            r = GpuEngine.instance().execute_plan(plan, [], opts)
+            names = [k for k, _, _, _ in profile_drain()]
+        finally:
+            profile_enable(False)
+        assert r.success, r.error_message
+        sums, counts = _expected_join_group(lk, lv, rk, rg)
+        got = dict(zip(r.columns[0].data.tolist(), zip(hugeint_to_int(r.columns[1].data), r.columns[2].data.tolist())))
+        assert got == {g: (sums[g], counts[g]) for g in counts}
+        return names
+
+    try:
+        rg1 = rng.integers(0, 300, len(rk)).astype(np.int32)
+        ColumnCache.put_table(t_b, [make_column("rk", T.INT64, rk), make_column("rg", T.INT32, rg1)])
+        assert "join_dense_table" in run(rg1)
+        assert "join_dense_table" not in run(rg1)  # kept
+        ColumnCache.invalidate_table(t_b)
+        rg2 = rng.integers(1000, 1200, len(rk)).astype(np.int32)
+        ColumnCache.put_table(t_b, [make_column("rk", T.INT64, rk), make_column("rg", T.INT32, rg2)])
+        assert "join_dense_table" in run(rg2)  # new contents: rebuilt
+        assert "join_dense_table" not in run(rg2)
+    finally:
+        ColumnCache.invalidate_table(t_b)
+        ColumnCache.invalidate_table(t_p)

@@ -747,11 +747,17 @@ vgpu_status vgpu_cache_try_get_chunk(const vgpu_table_ref *table, const char *co
 }
 
 vgpu_status vgpu_cache_invalidate_table(const vgpu_table_ref *table) {
-	return Guard([&] { ColumnCache::Get().InvalidateTable(ToTable(table)); });
+	return Guard([&] {
+		ColumnCache::Get().InvalidateTable(ToTable(table));
+		ClearJoinTables();
+	});
 }
 
 vgpu_status vgpu_cache_invalidate_all(void) {
-	return Guard([&] { ColumnCache::Get().InvalidateAll(); });
+	return Guard([&] {
+		ColumnCache::Get().InvalidateAll();
+		ClearJoinTables();
+	});
 }
 
 uint64_t vgpu_cache_current_bytes(void) {

@@ -222,6 +222,7 @@ void ColumnCache::CommitStaging(const TableRef &table, uint64_t scanned_rows) {
 			}
 		}
 		const std::string key = Key(table, kv.first);
+		e.table_key = tk;
 		lru_.push_front(key);
 		e.lru = lru_.begin();
 		committed_ += e.bytes;
@@ -230,6 +231,7 @@ void ColumnCache::CommitStaging(const TableRef &table, uint64_t scanned_rows) {
 	}
 	VGPU_CUDA(cudaStreamSynchronize(s));
 	staging_.erase(it);
+	generation_[tk]++;  // new contents: identities taken before no longer match
 }
 
 void ColumnCache::AbortStaging(const TableRef &table) {
@@ -305,6 +307,25 @@ void ColumnCache::InvalidateAll() {
 uint64_t ColumnCache::CurrentBytes() {
 	std::lock_guard<std::mutex> lock(mu_);
 	return committed_ + staged_;
+}
+
+std::string ColumnCache::Identify(const void *data, ValueType type, uint64_t rows) {
+	if (data == nullptr) return std::string();
+	std::lock_guard<std::mutex> lock(mu_);
+	const uint64_t w = TypeSize(type);
+	const auto p = reinterpret_cast<uintptr_t>(data);
+	for (auto &kv : entries_) {
+		const DevColumn &c = kv.second.column;
+		if (c.type != type || c.valid) continue;
+		const auto base = reinterpret_cast<uintptr_t>(c.data);
+		if (p < base || (p - base) % w != 0) continue;
+		const uint64_t first = (p - base) / w;
+		if (first + rows > c.rows) continue;
+		auto g = generation_.find(kv.second.table_key);
+		return kv.first + "@" + std::to_string(g == generation_.end() ? 0 : g->second) + "+" + std::to_string(first) +
+		       "*" + std::to_string(rows);
+	}
+	return std::string();
 }
 
 uint64_t ColumnCache::Generation(const TableRef &table) {

@@ -33,6 +33,11 @@ public:
 	void InvalidateAll();
 	uint64_t CurrentBytes();
 	uint64_t Generation(const TableRef &table);
+	//! Identity of cache-owned device data: "(table, column)@generation+offset*rows" when `rows`
+	//! values of `type` at `data` lie inside one committed column, else "". Contents behind an identity
+	//! never change (re-staging or invalidating a table bumps its generation), so derived structures
+	//! keyed by it (join tables) stay valid.
+	std::string Identify(const void *data, ValueType type, uint64_t rows);
 
 private:
 	struct Chunk {
@@ -51,6 +56,7 @@ private:
 	};
 	struct Entry {
 		DevColumn column; // contiguous data (+ byte validity), stats filled
+		std::string table_key;
 		std::vector<uint64_t> chunk_rows;
 		uint64_t bytes = 0;
 		std::list<std::string>::iterator lru;

@@ -16,8 +16,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <list>
 #include <map>
 #include <set>
+#include <unordered_map>
 
 #include "column_cache.hpp"
 #include "kernels.hpp"
@@ -104,6 +106,62 @@ uint64_t FloorPow2(uint64_t x) {
 	return p;
 }
 
+// Dense join tables built from cache-owned columns, kept across executions and keyed by the columns'
+// identities (ColumnCache::Identify: contents behind an identity never change), so a repeated join with
+// the same right side skips its key widening, range passes, read-back and table build. LRU over at most
+// 2 GiB of tables. A table is freed when the cache has let go of it and no execution holds it; every
+// consumer of a fused join reads a count back before its execution ends, so by then its reads are done.
+struct CachedJoinTable {
+	void *table = nullptr;
+	uint64_t bytes = 0;
+	uint64_t words[4] = {0, 0, 0, 0};  // join words; [2] (the key bias) is `bias`
+	uint64_t bias = 0;
+	bool inline_value = false;
+	~CachedJoinTable() {
+		if (table) Runtime::Get().allocator().Free(table, Runtime::Get().default_stream());
+	}
+};
+
+class JoinTableCache {
+public:
+	static JoinTableCache &Get() {
+		static JoinTableCache *cache = new JoinTableCache();  // never destroyed: outlives static teardown
+		return *cache;
+	}
+	std::shared_ptr<CachedJoinTable> Find(const std::string &key) {
+		std::lock_guard<std::mutex> lock(mu_);
+		auto it = map_.find(key);
+		if (it == map_.end()) return nullptr;
+		lru_.splice(lru_.begin(), lru_, it->second.second);
+		return it->second.first;
+	}
+	void Insert(const std::string &key, const std::shared_ptr<CachedJoinTable> &t) {
+		std::lock_guard<std::mutex> lock(mu_);
+		if (t->bytes > kCapacity || map_.count(key)) return;
+		while (bytes_ + t->bytes > kCapacity && !lru_.empty()) EvictLocked(lru_.back());
+		lru_.push_front(key);
+		map_[key] = {t, lru_.begin()};
+		bytes_ += t->bytes;
+	}
+	void Clear() {
+		std::lock_guard<std::mutex> lock(mu_);
+		while (!lru_.empty()) EvictLocked(lru_.back());
+	}
+
+private:
+	static constexpr uint64_t kCapacity = 2ull << 30;
+	void EvictLocked(const std::string &key) {
+		auto it = map_.find(key);
+		bytes_ -= it->second.first->bytes;
+		lru_.erase(it->second.second);
+		map_.erase(it);
+	}
+	std::mutex mu_;
+	uint64_t bytes_ = 0;
+	std::list<std::string> lru_;
+	std::unordered_map<std::string, std::pair<std::shared_ptr<CachedJoinTable>, std::list<std::string>::iterator>> map_;
+};
+
 class Executor {
 public:
 	Executor(const std::vector<vgpu_column> &inputs, const ExecOptions &options, cudaStream_t stream, bool nulls_ok)
@@ -164,6 +222,7 @@ private:
 	                    uint64_t extra_smem);
 
 	const std::vector<vgpu_column> &inputs_;
+	std::vector<std::shared_ptr<void>> holds_;  // cached structures in use by this execution
 	ExecOptions options_;
 	cudaStream_t stream_;
 	Arena arena_;
@@ -1202,8 +1261,6 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 	}
 	const uint64_t ln = lk->rows, rn = rk->rows;
 	const size_t kw = TypeSize(rk->type);
-	uint64_t *rw = arena_.AllocT<uint64_t>(rn);
-	kern::WidenKeys(rk->data, kw, rn, rw, stream_);
 	// The join contributes one right column of at most 4 bytes without NULLs: its value can be inlined
 	// into a dense key table; the value bits' bounds come back with the key range.
 	const DevColumn *inline_col = nullptr;
@@ -1219,17 +1276,6 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 			inline_col = nullptr;
 		}
 	}
-	uint64_t *mm = arena_.AllocT<uint64_t>(3);  // key min, key max, value bits (min, max)
-	kern::MinMaxU64(rw, rn, mm, stream_);
-	if (inline_col) kern::ValueBits(inline_col->data, TypeSize(inline_col->type), rn, reinterpret_cast<uint32_t *>(mm + 2), stream_);
-	uint64_t host_mm[3] = {0, 0, 0};
-	VGPU_CUDA(cudaMemcpyAsync(host_mm, mm, inline_col ? 24 : 16, cudaMemcpyDeviceToHost, stream_));
-	VGPU_CUDA(cudaStreamSynchronize(stream_));
-	const uint64_t bias = host_mm[0];
-	const uint64_t range = host_mm[1] - host_mm[0];
-	const uint32_t vmin = static_cast<uint32_t>(host_mm[2]), vmax = static_cast<uint32_t>(host_mm[2] >> 32);
-	const int bits = BitsFor(range);
-	kern::SubtractBias(rw, rn, bias, stream_);
 	auto add_sources = [&](bool sorted_side, const uint32_t *perm) {
 		for (size_t i = 0; i < outs.size(); i++) {
 			DevColumn c = *outs[i];
@@ -1254,74 +1300,130 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 			pin.sources.push_back(c);
 		}
 	};
-	uint32_t *dups = arena_.AllocT<uint32_t>(1);
-	bool built = false;
-	// Dense keys (range within 4x the key count, at most 2^28): a table indexed by the key over the whole
-	// range, filled without sorting. It holds the right row index, or -- when the join contributes one
-	// right column of at most 4 bytes -- that column's value itself, so a probe row costs one random
-	// read; the value is stored as its offset from the smallest value in the fewest bytes that hold every
-	// offset (all ones marks a missing key), so the table of a small-valued column stays in L2. A key met
-	// twice (many-to-many) falls back to the sorted form below.
-	if (range < (1ull << 28) && range < 4 * rn) {
-		const uint64_t span = static_cast<uint64_t>(vmax) - vmin;
-		const size_t width = !inline_col ? 0 : span < 0xffull ? 1 : span < 0xffffull ? 2 : span < 0xffffffffull ? 4 : 8;
-		const char *env_c = std::getenv("VGPU_JOIN_COMPACT");  // "0": 8-byte inline entries (testing)
-		const bool compact = width != 0 && width != 8 && !(env_c && std::strcmp(env_c, "0") == 0);
-		if (compact) {
-			void *table = arena_.Alloc((range + 1) * width);
-			kern::JoinDenseCompact(rw, inline_col->data, TypeSize(inline_col->type), rn, range, vmin, table, width, dups,
-			                       stream_);
-			if (ReadU32(dups) == 0) {
-				add_sources(false, nullptr);
-				pin.spec.join_inline = true;
-				pin.join_words[0] = reinterpret_cast<uint64_t>(table);
-				pin.join_words[1] = vmin;
-				pin.join_words[3] = (width == 1 ? 0xfdu : width == 2 ? 0xfcu : 0xfbu) | ((range + 1) << 8);
-				built = true;
-			}
-		} else if (inline_col) {
-			uint64_t *table = arena_.AllocT<uint64_t>(range + 1);
-			kern::JoinDenseInline(rw, inline_col->data, TypeSize(inline_col->type), rn, range, table, dups, stream_);
-			if (ReadU32(dups) == 0) {
-				add_sources(false, nullptr);
-				pin.spec.join_inline = true;
-				pin.join_words[0] = reinterpret_cast<uint64_t>(table);
-				pin.join_words[1] = 0;
-				pin.join_words[3] = 0xfeu | ((range + 1) << 8);
-				built = true;
-			}
-		} else {
-			uint32_t *table = arena_.AllocT<uint32_t>(range + 1);
-			kern::JoinDenseRows(rw, rn, range, table, dups, stream_);
-			if (ReadU32(dups) == 0) {
-				add_sources(false, nullptr);
-				pin.join_words[0] = 0;
-				pin.join_words[1] = reinterpret_cast<uint64_t>(table);
-				pin.join_words[3] = 0xffu | ((range + 1) << 8);
-				built = true;
-			}
+	// A right side read from the column cache: its dense table may already be kept (see JoinTableCache).
+	std::string cache_key;
+	{
+		const std::string idk = ColumnCache::Get().Identify(rk->data, rk->type, rn);
+		const std::string idv = inline_col ? ColumnCache::Get().Identify(inline_col->data, inline_col->type, rn) : "";
+		const char *env_c = std::getenv("VGPU_JOIN_COMPACT");
+		const char *env_keep = std::getenv("VGPU_JOIN_CACHE");  // "0": build every time (measurement, testing)
+		const bool keep_allowed = !(env_keep && std::strcmp(env_keep, "0") == 0);
+		if (keep_allowed && !idk.empty() && (!inline_col || !idv.empty())) {
+			cache_key = idk + "|" + idv + "|" + std::to_string(inline_col ? static_cast<int>(inline_col->type) : -1) + "|" +
+			            (env_c ? env_c : "");
 		}
 	}
-	if (!built) {
-		// Sorted form: LSD radix sort of the right keys, uniqueness check, radix directory over the sorted
-		// keys (at most 2^22 buckets), right columns gathered into sorted order once.
-		uint32_t *perm = arena_.AllocT<uint32_t>(rn);
-		kern::Iota(perm, rn, stream_);
-		uint64_t *rw_alt = arena_.AllocT<uint64_t>(rn);
-		uint32_t *perm_alt = arena_.AllocT<uint32_t>(rn);
-		kern::RadixSortPairs(rw, perm, rw_alt, perm_alt, rn, bits, arena_);
-		arena_.FreeNow(rw_alt);
-		arena_.FreeNow(perm_alt);
-		kern::CountAdjacentEqual(rw, rn, dups, stream_);
-		if (ReadU32(dups) != 0) return JoinMaterialize(node, left, right);  // many-to-many
-		const uint32_t shift = bits > 22 ? static_cast<uint32_t>(bits - 22) : 0u;
-		const uint64_t nb = (range >> shift) + 1;
-		uint32_t *dir = arena_.AllocT<uint32_t>(nb + 1);
-		kern::JoinDirectory(rw, rn, shift, nb, dir, stream_);
-		add_sources(true, perm);
-		pin.join_words[0] = reinterpret_cast<uint64_t>(rw);
-		pin.join_words[1] = reinterpret_cast<uint64_t>(dir);
-		pin.join_words[3] = shift | (nb << 8);
+	uint64_t bias = 0;
+	std::shared_ptr<CachedJoinTable> hit = cache_key.empty() ? nullptr : JoinTableCache::Get().Find(cache_key);
+	if (hit) {
+		holds_.push_back(hit);
+		add_sources(false, nullptr);
+		pin.spec.join_inline = hit->inline_value;
+		pin.join_words[0] = hit->words[0];
+		pin.join_words[1] = hit->words[1];
+		pin.join_words[3] = hit->words[3];
+		bias = hit->bias;
+	} else {
+		// a dense table just built: handed from the execution's arena to the cache
+		auto keep = [&](void *table, uint64_t bytes, bool inline_value) {
+			if (cache_key.empty()) return;
+			arena_.Release(table);
+			auto t = std::make_shared<CachedJoinTable>();
+			t->table = table;
+			t->bytes = bytes;
+			t->inline_value = inline_value;
+			t->bias = bias;
+			t->words[0] = pin.join_words[0];
+			t->words[1] = pin.join_words[1];
+			t->words[3] = pin.join_words[3];
+			holds_.push_back(t);
+			JoinTableCache::Get().Insert(cache_key, t);
+		};
+		uint64_t *rw = arena_.AllocT<uint64_t>(rn);
+		kern::WidenKeys(rk->data, kw, rn, rw, stream_);
+		uint64_t *mm = arena_.AllocT<uint64_t>(3);  // key min, key max, value bits (min, max)
+		kern::MinMaxU64(rw, rn, mm, stream_);
+		if (inline_col) kern::ValueBits(inline_col->data, TypeSize(inline_col->type), rn, reinterpret_cast<uint32_t *>(mm + 2), stream_);
+		uint64_t host_mm[3] = {0, 0, 0};
+		VGPU_CUDA(cudaMemcpyAsync(host_mm, mm, inline_col ? 24 : 16, cudaMemcpyDeviceToHost, stream_));
+		VGPU_CUDA(cudaStreamSynchronize(stream_));
+		bias = host_mm[0];
+		const uint64_t range = host_mm[1] - host_mm[0];
+		const uint32_t vmin = static_cast<uint32_t>(host_mm[2]), vmax = static_cast<uint32_t>(host_mm[2] >> 32);
+		const int bits = BitsFor(range);
+		kern::SubtractBias(rw, rn, bias, stream_);
+		uint32_t *dups = arena_.AllocT<uint32_t>(1);
+		bool built = false;
+		// Dense keys (range within 4x the key count, at most 2^28): a table indexed by the key over the whole
+		// range, filled without sorting. It holds the right row index, or -- when the join contributes one
+		// right column of at most 4 bytes -- that column's value itself, so a probe row costs one random
+		// read; the value is stored as its offset from the smallest value in the fewest bytes that hold every
+		// offset (all ones marks a missing key), so the table of a small-valued column stays in L2. A key met
+		// twice (many-to-many) falls back to the sorted form below.
+		if (range < (1ull << 28) && range < 4 * rn) {
+			const uint64_t span = static_cast<uint64_t>(vmax) - vmin;
+			const size_t width = !inline_col ? 0 : span < 0xffull ? 1 : span < 0xffffull ? 2 : span < 0xffffffffull ? 4 : 8;
+			const char *env_c = std::getenv("VGPU_JOIN_COMPACT");  // "0": 8-byte inline entries (testing)
+			const bool compact = width != 0 && width != 8 && !(env_c && std::strcmp(env_c, "0") == 0);
+			if (compact) {
+				void *table = arena_.Alloc((range + 1) * width);
+				kern::JoinDenseCompact(rw, inline_col->data, TypeSize(inline_col->type), rn, range, vmin, table, width, dups,
+				                       stream_);
+				if (ReadU32(dups) == 0) {
+					add_sources(false, nullptr);
+					pin.spec.join_inline = true;
+					pin.join_words[0] = reinterpret_cast<uint64_t>(table);
+					pin.join_words[1] = vmin;
+					pin.join_words[3] = (width == 1 ? 0xfdu : width == 2 ? 0xfcu : 0xfbu) | ((range + 1) << 8);
+					built = true;
+					keep(table, (range + 1) * width, true);
+				}
+			} else if (inline_col) {
+				uint64_t *table = arena_.AllocT<uint64_t>(range + 1);
+				kern::JoinDenseInline(rw, inline_col->data, TypeSize(inline_col->type), rn, range, table, dups, stream_);
+				if (ReadU32(dups) == 0) {
+					add_sources(false, nullptr);
+					pin.spec.join_inline = true;
+					pin.join_words[0] = reinterpret_cast<uint64_t>(table);
+					pin.join_words[1] = 0;
+					pin.join_words[3] = 0xfeu | ((range + 1) << 8);
+					built = true;
+					keep(table, (range + 1) * 8, true);
+				}
+			} else {
+				uint32_t *table = arena_.AllocT<uint32_t>(range + 1);
+				kern::JoinDenseRows(rw, rn, range, table, dups, stream_);
+				if (ReadU32(dups) == 0) {
+					add_sources(false, nullptr);
+					pin.join_words[0] = 0;
+					pin.join_words[1] = reinterpret_cast<uint64_t>(table);
+					pin.join_words[3] = 0xffu | ((range + 1) << 8);
+					built = true;
+					keep(table, (range + 1) * 4, false);
+				}
+			}
+		}
+		if (!built) {
+			// Sorted form: LSD radix sort of the right keys, uniqueness check, radix directory over the sorted
+			// keys (at most 2^22 buckets), right columns gathered into sorted order once.
+			uint32_t *perm = arena_.AllocT<uint32_t>(rn);
+			kern::Iota(perm, rn, stream_);
+			uint64_t *rw_alt = arena_.AllocT<uint64_t>(rn);
+			uint32_t *perm_alt = arena_.AllocT<uint32_t>(rn);
+			kern::RadixSortPairs(rw, perm, rw_alt, perm_alt, rn, bits, arena_);
+			arena_.FreeNow(rw_alt);
+			arena_.FreeNow(perm_alt);
+			kern::CountAdjacentEqual(rw, rn, dups, stream_);
+			if (ReadU32(dups) != 0) return JoinMaterialize(node, left, right);  // many-to-many
+			const uint32_t shift = bits > 22 ? static_cast<uint32_t>(bits - 22) : 0u;
+			const uint64_t nb = (range >> shift) + 1;
+			uint32_t *dir = arena_.AllocT<uint32_t>(nb + 1);
+			kern::JoinDirectory(rw, rn, shift, nb, dir, stream_);
+			add_sources(true, perm);
+			pin.join_words[0] = reinterpret_cast<uint64_t>(rw);
+			pin.join_words[1] = reinterpret_cast<uint64_t>(dir);
+			pin.join_words[3] = shift | (nb << 8);
+		}
 	}
 	pin.join_words[2] = bias;
 	SourceColumn key;
@@ -1451,6 +1553,10 @@ Relation Executor::Exec(const PlanNode &node) {
 }
 
 } // namespace
+
+void ClearJoinTables() {
+	JoinTableCache::Get().Clear();
+}
 
 PipelineCodegen::GroupBySpec ValidateGroupBy(const PlanNode &node, const PipelineCodegen &cg, std::vector<int> &key_cols) {
 	return ValidateGroupByNode(node, cg, key_cols);

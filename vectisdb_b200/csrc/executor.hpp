@@ -56,6 +56,10 @@ struct ExecResult {
 //! INVALID_ARGUMENT) for what this GPU path does not model.
 PipelineCodegen::GroupBySpec ValidateGroupBy(const PlanNode &node, const PipelineCodegen &cg, std::vector<int> &key_cols);
 
+//! Drops every dense join table kept across executions (their memory is freed once no execution holds
+//! it). Called when cached base columns are invalidated.
+void ClearJoinTables();
+
 //! Executes `plan` over `inputs`. Throws Error on any failure (nothing partial escapes).
 ExecResult ExecutePlan(const PlanNode &plan, const std::vector<vgpu_column> &inputs, const ExecOptions &options,
                        cudaStream_t stream);

@@ -579,6 +579,13 @@ void Runtime::SetDevice(int device) {
 }
 
 void Runtime::EnsureDevice() {
+	// after initialization: no lock, and a device switch only when this thread's current device differs
+	// (concurrent serving threads call this on every step)
+	if (ready_.load(std::memory_order_acquire)) {
+		int current = -1;
+		if (cudaGetDevice(&current) != cudaSuccess || current != props_.device) VGPU_CUDA(cudaSetDevice(props_.device));
+		return;
+	}
 	std::lock_guard<std::mutex> lock(mu_);
 	if (initialized_) {
 		VGPU_CUDA(cudaSetDevice(props_.device));
@@ -612,6 +619,7 @@ void Runtime::EnsureDevice() {
 	VGPU_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
 	LoadDriverEntryPoints();
 	initialized_ = true;
+	ready_.store(true, std::memory_order_release);
 }
 
 const DeviceProps &Runtime::props() {

@@ -222,6 +222,7 @@ private:
 	void LoadDriverEntryPoints();
 	std::mutex mu_;
 	bool initialized_ = false;
+	std::atomic<bool> ready_ {false};  // initialized_, readable without mu_
 	int requested_device_ = 0;
 	DeviceProps props_;
 	cudaStream_t stream_ = nullptr;
