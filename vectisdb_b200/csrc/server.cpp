@@ -133,7 +133,7 @@ std::vector<std::shared_ptr<Server::Request>> Server::AdmitLocked() {
 	queue_.pop_front();
 	job.push_back(head);
 	reserved_ += head->est;
-	if (options_.batch_max > 1 && !head->tmpl.empty() && template_verdict_[head->tmpl] > 0) {
+	if (options_.batch_max > 1 && !head->tmpl.empty() && template_batches_[head->tmpl] > 0) {
 		for (auto it = queue_.begin(); it != queue_.end() && static_cast<int>(job.size()) < options_.batch_max;) {
 			auto &r = *it;
 			if (r->tmpl == head->tmpl && r->options.output_on_device == head->options.output_on_device &&
@@ -177,17 +177,17 @@ void Server::WorkerLoop(int slot) {
 			stats_.peak_in_flight = std::max(stats_.peak_in_flight, stats_.in_flight);
 			stats_.peak_reserved_bytes = std::max(stats_.peak_reserved_bytes, reserved_);
 		}
-		// Run the job: a template whose verdict is still unknown runs its first request through the
+		// Run the job: a template whose batching is still unknown runs its first request through the
 		// batch path alone to learn whether the batch kernel takes it.
 		const auto &head = job.front();
 		bool learn = false;
 		bool as_batch = job.size() > 1;
 		if (!as_batch && options_.batch_max > 1 && !head->tmpl.empty()) {
 			std::lock_guard<std::mutex> lock(mu_);
-			learn = template_verdict_[head->tmpl] == 0;
+			learn = template_batches_[head->tmpl] == 0;
 			as_batch = learn;
 		}
-		int verdict = 0;
+		int batched = 0;  // +1: the batch form took the job, -1: it ran one by one
 		std::vector<ExecResult> results(job.size());
 		std::vector<int> status(job.size(), VGPU_OK);
 		std::vector<std::string> errors(job.size());
@@ -203,7 +203,7 @@ void Server::WorkerLoop(int slot) {
 				bo.use_graph = false;  // compositions change from launch to launch
 				BatchStats st;
 				results = ExecutePrepared(*PrepareBatch(plans), ins, head->options, bo, stream, &st);
-				verdict = st.batched > 0 ? 1 : -1;
+				batched = st.batched > 0 ? 1 : -1;
 			} catch (const Error &e) {
 				for (size_t i = 0; i < job.size(); i++) {
 					status[i] = e.status();
@@ -232,7 +232,7 @@ void Server::WorkerLoop(int slot) {
 		const auto now = Clock::now();
 		{
 			std::lock_guard<std::mutex> lock(mu_);
-			if (learn && verdict != 0) template_verdict_[head->tmpl] = verdict;
+			if (learn && batched != 0) template_batches_[head->tmpl] = batched;
 			for (size_t i = 0; i < job.size(); i++) {
 				auto &r = job[i];
 				reserved_ -= r->est;

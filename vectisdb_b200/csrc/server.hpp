@@ -72,7 +72,7 @@ private:
 	std::condition_variable work_cv_, done_cv_;
 	std::deque<std::shared_ptr<Request>> queue_;
 	std::map<uint64_t, std::shared_ptr<Request>> requests_;
-	std::map<std::string, int> template_verdict_;  // +1 batches, -1 does not
+	std::map<std::string, int> template_batches_;  // +1 batches, -1 does not
 	uint64_t next_id_ = 1;
 	uint64_t reserved_ = 0;
 	bool stop_ = false;
