@@ -1109,10 +1109,11 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			return r.str();
 		};
 		const std::string mixed = "vgpu_dmix(a, " + pack.str() + ")";
-		// a kept row's heavy-state index, or -1
-		const std::string heavy_of = "((vgpu_hmap[(u32)(k0 >> " + std::to_string(dbits) + ")] & 0xffffu) == ((u32)k0 & " +
-		                             dmask + ") ? (int)(vgpu_hmap[(u32)(k0 >> " + std::to_string(dbits) +
-		                             ")] >> 16) : -1)";
+		// a kept row's heavy-state index, or -1 (one map load per row)
+		o << "__device__ __forceinline__ int vgpu_heavy_slot(const u32 *hmap, u64 k) {\n"
+		  << "\tconst u32 e = hmap[(u32)(k >> " << dbits << ")];\n"
+		  << "\treturn (e & 0xffffu) == ((u32)k & " << dmask << ") ? (int)(e >> 16) : -1;\n}\n\n";
+		const std::string heavy_of = "vgpu_heavy_slot(vgpu_hmap, k0)";
 		// sample: one tile per CTA at a stride, counts of the mixed keys of the kept rows
 		o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << (g.min_blocks > 0 ? ", " + std::to_string(g.min_blocks) : std::string()) << ") vgpu_gb_sample(KArgs a) {\n"
 		  << kKernelHead
@@ -1209,9 +1210,11 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		  << stage_prologue(needed, "vgpu_smem")
 		  << "\tfor (u64 tile = blockIdx.x * tpc; tile < t_end; ++tile) {\n"
 		  << tile_load(needed)
-		  << "\t\tu32 vgpu_pos[" << g.items << "];\n\t\tint vgpu_hv[" << g.items << "];\n"
+		  << "\t\tu32 vgpu_pos[" << g.items << "];\n\t\tint vgpu_hv[" << g.items << "];\n\t\tu64 vgpu_k[" << g.items
+		  << "];\n"
 		  << item_head << chain_code_
 		  << "\t\tconst u64 k0 = " << mixed << ";\n"
+		  << "\t\tvgpu_k[r] = k0;\n"
 		  << "\t\tvgpu_hv[r] = keep ? " << heavy_of << " : -1;\n"
 		  << "\t\tvgpu_pos[r] = atomicAdd(&vgpu_cursor[keep && vgpu_hv[r] < 0 ? (u32)(k0 >> " << dbits
 		  << ") : P + (threadIdx.x & 31u)], 1u);\n"
@@ -1219,7 +1222,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		  << item_head << chain_code_ << "\t\tif (keep) {\n"
 		  << "\t\t\tconst int h = vgpu_hv[r];\n"
 		  << "\t\t\tif (h >= 0) {\n" << hupd.str() << "\t\t\t} else {\n"
-		  << "\t\t\tconst u64 key = " << key_of_pack << ";\n"
+		  << "\t\t\tconst u64 key = vgpu_k[r];\n"
 		  << "\t\t\tconst u32 pos = vgpu_pos[r];\n"
 		  << "\t\t\tu32 rw[" << RW << "];\n"
 		  << "\t\t\t#pragma unroll\n\t\t\tfor (int q = 0; q < " << RW << "; ++q) rw[q] = 0u;\n"
@@ -1277,12 +1280,16 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 	  << tile_load(needed)
 	  // every item's cursor reservation first, branch-free (rows that are filtered out add to a per-lane
 	  // dummy counter past P), so the tile's shared atomics are in flight together; then the records
-	  << "\t\tu32 vgpu_pos[" << g.items << "];\n"
+	  << "\t\tu32 vgpu_pos[" << g.items << "];\n\t\tu64 vgpu_k[" << g.items << "];\n"
 	  << item_head << chain_code_
-	  << "\t\tvgpu_pos[r] = atomicAdd(&vgpu_cursor[keep ? " << part_of_pack << " : P + (threadIdx.x & 31u)], 1u);\n"
+	  << "\t\tconst u64 k0 = " << key_of_pack << ";\n"
+	  << "\t\tvgpu_k[r] = k0;\n"
+	  << "\t\tvgpu_pos[r] = atomicAdd(&vgpu_cursor[keep ? "
+	  << (dpart ? "(u32)(k0 >> " + std::to_string(gb.direct_bits) + ")" : std::string("partition_of(k0, pbits)"))
+	  << " : P + (threadIdx.x & 31u)], 1u);\n"
 	  << "\t\t}\n"
 	  << item_head << chain_code_ << "\t\tif (keep) {\n"
-	  << "\t\t\tconst u64 key = " << key_of_pack << ";\n"
+	  << "\t\t\tconst u64 key = vgpu_k[r];\n"
 	  << "\t\t\tconst u32 pos = vgpu_pos[r];\n"
 	  << "\t\t\tu32 rw[" << RW << "];\n"
 	  << "\t\t\t#pragma unroll\n\t\t\tfor (int q = 0; q < " << RW << "; ++q) rw[q] = 0u;\n"
