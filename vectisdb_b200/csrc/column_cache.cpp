@@ -328,6 +328,23 @@ std::string ColumnCache::Identify(const void *data, ValueType type, uint64_t row
 	return std::string();
 }
 
+bool ColumnCache::BoundsOf(const void *data, ValueType type, uint64_t rows, int64_t *min, int64_t *max) {
+	if (data == nullptr || rows == 0) return false;
+	std::lock_guard<std::mutex> lock(mu_);
+	const uint64_t w = TypeSize(type);
+	const auto p = reinterpret_cast<uintptr_t>(data);
+	for (auto &kv : entries_) {
+		const DevColumn &c = kv.second.column;
+		if (c.type != type || !c.has_stats) continue;
+		const auto base = reinterpret_cast<uintptr_t>(c.data);
+		if (p < base || (p - base) % w != 0 || (p - base) / w + rows > c.rows) continue;
+		*min = c.min;
+		*max = c.max;
+		return true;
+	}
+	return false;
+}
+
 uint64_t ColumnCache::Generation(const TableRef &table) {
 	std::lock_guard<std::mutex> lock(mu_);
 	auto it = generation_.find(TableKey(table));

@@ -38,6 +38,9 @@ public:
 	//! never change (re-staging or invalidating a table bumps its generation), so derived structures
 	//! keyed by it (join tables) stay valid.
 	std::string Identify(const void *data, ValueType type, uint64_t rows);
+	//! The committed column's value range when `rows` values at `data` lie inside one (a superset of
+	//! those rows' range, valid for key packing); false otherwise.
+	bool BoundsOf(const void *data, ValueType type, uint64_t rows, int64_t *min, int64_t *max);
 
 private:
 	struct Chunk {

@@ -292,6 +292,10 @@ Relation Executor::Scan(const PlanNode &node) {
 			col.data = const_cast<void *>(in.data);
 			if (col.data == nullptr) {
 				col.data = arena_.Alloc(16);
+			} else if (in.validity == nullptr && IsIntegerKeyType(col.type)) {
+				// rows of a cached column (a borrowed prefix, say): its range covers theirs, so group-by key
+				// packing needs no statistics pass
+				col.has_stats = ColumnCache::Get().BoundsOf(col.data, col.type, col.rows, &col.min, &col.max);
 			}
 		} else {
 			col.data = arena_.Alloc(bytes);
