@@ -1,0 +1,114 @@
+"""Sharded group-by merge (vectisdb_b200.distributed): two gloo ranks on the CPU each aggregate half of
+the rows, the partial groups are merged with all-reduces, and the result must equal the aggregation of
+all rows -- exactly for counts, MIN/MAX and 128-bit integer sums (values near 2^62 make the sums leave
+64 bits), within 1e-12 relative for FP64 sums. One rank with no rows contributes identities."""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _data(seed):
+    rng = np.random.default_rng(seed)
+    n = 20000
+    k = rng.integers(-50, 200, n)
+    k[rng.random(n) < 0.2] = 7  # one heavy key
+    x = rng.standard_normal(n)
+    v = rng.integers((1 << 62) - 1000, 1 << 62, n, dtype=np.int64)
+    v[rng.random(n) < 0.3] *= -1
+    w = rng.integers(-(1 << 40), 1 << 40, n, dtype=np.int64)
+    return k, x, v, w
+
+
+def _partial(k, x, v, w):
+    """What a rank's engine run returns: its groups with SUM(x), SUM(v) as HUGEINT, COUNT(*), MIN/MAX(w)."""
+    sys.path.insert(0, ROOT)
+    from vectisdb_b200.distributed import HUGEINT
+    keys = np.unique(k)
+    pos = np.searchsorted(keys, k)
+    sx = np.zeros(len(keys))
+    np.add.at(sx, pos, x)
+    cnt = np.bincount(pos, minlength=len(keys)).astype(np.int64)
+    mn = np.full(len(keys), np.iinfo(np.int64).max)
+    np.minimum.at(mn, pos, w)
+    mx = np.full(len(keys), np.iinfo(np.int64).min)
+    np.maximum.at(mx, pos, w)
+    sv = np.zeros(len(keys), HUGEINT)
+    for i, key in enumerate(keys.tolist()):
+        total = int(v[k == key].astype(object).sum())
+        sv[i]["lower"] = total & ((1 << 64) - 1)
+        u = (total >> 64) & ((1 << 64) - 1)
+        sv[i]["upper"] = u - (1 << 64) if u >= (1 << 63) else u
+    return keys, [("sum_f64", sx), ("sum_i128", sv), ("count", cnt), ("min", mn), ("max", mx)]
+
+
+def _rank(rank, world, port, seed, empty_rank, out):
+    import datetime
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    from vectisdb_b200.distributed import merge_dense_groupby
+    k, x, v, w = _data(seed)
+    lo, hi = (0, len(k) // 2) if rank == 0 else (len(k) // 2, len(k))
+    if rank == empty_rank:
+        lo = hi = 0
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        keys, aggs = _partial(k[lo:hi], x[lo:hi], v[lo:hi], w[lo:hi])
+        mk, magg = merge_dense_groupby(keys, aggs, -50, 199)
+        out[rank] = (mk, magg)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("empty_rank", [-1, 1])
+def test_merge_of_two_ranks_equals_the_whole(empty_rank):
+    ctx = mp.get_context("spawn")
+    manager = ctx.Manager()
+    out = manager.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, 5, empty_rank, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(180)
+        assert p.exitcode == 0
+    k, x, v, w = _data(5)
+    if empty_rank == 1:  # rank 1 contributed nothing: the whole is rank 0's half
+        half = len(k) // 2
+        k, x, v, w = k[:half], x[:half], v[:half], w[:half]
+    ek, eaggs = _partial(k, x, v, w)
+    for rank in (0, 1):
+        mk, magg = out[rank]
+        assert np.array_equal(mk, ek)
+        sx, sv, cnt, mn, mx = magg
+        assert np.all(np.abs(sx - eaggs[0][1]) <= 1e-12 * np.maximum(np.abs(eaggs[0][1]), 1e-300) + 1e-12)
+        assert np.array_equal(sv["lower"], eaggs[1][1]["lower"]) and np.array_equal(sv["upper"], eaggs[1][1]["upper"])
+        assert np.array_equal(cnt, eaggs[2][1]) and np.array_equal(mn, eaggs[3][1]) and np.array_equal(mx, eaggs[4][1])
+
+
+def test_sparse_domains_and_unknown_kinds_are_refused_before_any_collective():
+    """No process group exists here: each refusal must come before the first collective."""
+    sys.path.insert(0, ROOT)
+    from vectisdb_b200.distributed import merge_dense_groupby
+    with pytest.raises(ValueError, match="not dense"):
+        merge_dense_groupby(np.array([0]), [("count", np.array([1]))], 0, 1 << 24)
+    with pytest.raises(ValueError, match="does not merge"):
+        merge_dense_groupby(np.array([0]), [("avg", np.array([1.0]))], 0, 10)
+    with pytest.raises(ValueError, match="one value per key"):
+        merge_dense_groupby(np.array([0, 1]), [("count", np.array([1]))], 0, 10)
+    with pytest.raises(ValueError, match="outside"):
+        merge_dense_groupby(np.array([11]), [("count", np.array([1]))], 0, 10)

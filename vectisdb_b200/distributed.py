@@ -1,0 +1,106 @@
+"""Row-range sharding of a group-by across ranks (one process per GPU, `torch.distributed`): each rank
+runs the query on its own rows with the engine, and the partial groups are merged here.
+
+`merge_dense_groupby` handles key domains small enough to index directly (the filter + group-by and
+join + group-by shapes: at most 2^20 key values): every aggregate becomes a key-indexed array filled
+with the rank's partial values (the identity elsewhere) and is combined with one all-reduce -- SUM
+for sums and counts, MIN and MAX for those. 128-bit integer sums (DuckDB's HUGEINT, the engine's
+`{lower, upper}` pairs) travel as four 32-bit chunks summed in 64-bit lanes, which cannot overflow
+for fewer than 2^31 ranks, and are carried back into 128 bits, so the merged sum is exact. AVG does
+not merge from its outputs: shard its SUM and COUNT instead. Every rank makes the same collective
+calls in the same order, whatever rows it holds (an empty partial contributes identities).
+
+Works with the "gloo" backend on CPU tensors and with "nccl" on CUDA tensors of the rank's device.
+"""
+from __future__ import annotations
+
+from typing import Sequence
+
+import numpy as np
+
+KINDS = ("sum_f64", "sum_i128", "count", "min", "max")
+HUGEINT = np.dtype([("lower", "<u8"), ("upper", "<i8")])
+_MAX_DOMAIN = 1 << 20
+
+
+def _all_reduce(array: np.ndarray, op, device: str) -> np.ndarray:
+    import torch
+    import torch.distributed as dist
+    t = torch.from_numpy(np.ascontiguousarray(array)).to(device)
+    dist.all_reduce(t, op=op)
+    return t.cpu().numpy()
+
+
+def merge_dense_groupby(keys: np.ndarray, aggregates: Sequence[tuple[str, np.ndarray]], key_min: int, key_max: int,
+                        device: str = "cpu") -> tuple[np.ndarray, list[np.ndarray]]:
+    """Merges this rank's partial groups (`keys`, one value per key and aggregate) with every other
+    rank's. `key_min`/`key_max` bound the keys of all ranks (the same on every rank). Returns the
+    merged keys in ascending order and the merged aggregates, the same on every rank."""
+    import torch.distributed as dist
+    keys = np.asarray(keys, dtype=np.int64)
+    domain = int(key_max) - int(key_min) + 1
+    if domain <= 0 or domain > _MAX_DOMAIN:
+        raise ValueError(f"merge_dense_groupby: key domain of {domain} values is not dense (at most {_MAX_DOMAIN})")
+    if keys.size and (keys.min() < key_min or keys.max() > key_max):
+        raise ValueError("merge_dense_groupby: a key lies outside [key_min, key_max]")
+    for kind, values in aggregates:  # checked before any collective, so every rank fails alike
+        if kind not in KINDS:
+            raise ValueError(f"merge_dense_groupby: aggregate kind {kind!r} does not merge (one of {KINDS})")
+        if np.asarray(values).shape[0] != keys.shape[0]:
+            raise ValueError("merge_dense_groupby: one value per key is needed")
+    slot = keys - int(key_min)
+    present = np.zeros(domain, np.int64)
+    present[slot] = 1
+    present = _all_reduce(present, dist.ReduceOp.SUM, device)
+    live = np.nonzero(present)[0]
+    merged = []
+    for kind, values in aggregates:
+        values = np.asarray(values)
+        if kind == "sum_f64":
+            dense = np.zeros(domain, np.float64)
+            dense[slot] = values.astype(np.float64)
+            merged.append(_all_reduce(dense, dist.ReduceOp.SUM, device)[live])
+        elif kind == "count":
+            dense = np.zeros(domain, np.int64)
+            dense[slot] = values.astype(np.int64)
+            merged.append(_all_reduce(dense, dist.ReduceOp.SUM, device)[live])
+        elif kind in ("min", "max"):
+            info = np.iinfo(np.int64)
+            dense = np.full(domain, info.max if kind == "min" else info.min, np.int64)
+            dense[slot] = values.astype(np.int64)
+            op = dist.ReduceOp.MIN if kind == "min" else dist.ReduceOp.MAX
+            merged.append(_all_reduce(dense, op, device)[live])
+        else:
+            merged.append(_merge_i128(values, slot, domain, device)[live])
+    return live.astype(np.int64) + int(key_min), merged
+
+
+def _merge_i128(values: np.ndarray, slot: np.ndarray, domain: int, device: str) -> np.ndarray:
+    """Exact sum over ranks of 128-bit integers given as {lower u64, upper i64}."""
+    import torch.distributed as dist
+    v = np.asarray(values).astype(HUGEINT, copy=False)
+    lower = v["lower"].astype(np.uint64)
+    upper = v["upper"].astype(np.int64)
+    mask = np.uint64(0xFFFFFFFF)
+    chunks = [  # value = c0 + c1 2^32 + c2 2^64 + c3 2^96, c0..c2 in [0, 2^32), c3 signed 32-bit
+        (lower & mask).astype(np.int64),
+        (lower >> np.uint64(32)).astype(np.int64),
+        (upper.view(np.uint64) & mask).astype(np.int64),
+        upper >> np.int64(32),
+    ]
+    sums = []
+    for c in chunks:
+        dense = np.zeros(domain, np.int64)
+        dense[slot] = c
+        sums.append(_all_reduce(dense, dist.ReduceOp.SUM, device))
+    low = []
+    carry = np.zeros(domain, np.int64)
+    for s in sums[:3]:
+        t = s + carry  # non-negative: sums of non-negative chunks plus carries
+        low.append((t & 0xFFFFFFFF).astype(np.uint64))
+        carry = t >> 32
+    top = sums[3] + carry
+    out = np.empty(domain, HUGEINT)
+    out["lower"] = low[0] | (low[1] << np.uint64(32))
+    out["upper"] = (low[2] | (top.view(np.uint64) << np.uint64(32))).view(np.int64)
+    return out
