@@ -112,3 +112,60 @@ def test_sparse_domains_and_unknown_kinds_are_refused_before_any_collective():
         merge_dense_groupby(np.array([0, 1]), [("count", np.array([1]))], 0, 10)
     with pytest.raises(ValueError, match="outside"):
         merge_dense_groupby(np.array([11]), [("count", np.array([1]))], 0, 10)
+
+
+def _hc_data(seed):
+    rng = np.random.default_rng(seed)
+    n = 60000
+    k = rng.integers(0, 1 << 40, 30000)[rng.integers(0, 30000, n)]  # ~25k distinct sparse keys
+    k[rng.random(n) < 0.1] = 12345  # a heavy key
+    x = rng.standard_normal(n)
+    v = rng.integers((1 << 62) - 1000, 1 << 62, n, dtype=np.int64)
+    v[rng.random(n) < 0.4] *= -1
+    w = rng.integers(-(1 << 40), 1 << 40, n, dtype=np.int64)
+    return k, x, v, w
+
+
+def _rank_repart(rank, world, port, seed, out):
+    import datetime
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    from vectisdb_b200.distributed import repartition_merge_groupby
+    k, x, v, w = _hc_data(seed)
+    lo, hi = (0, len(k) // 3) if rank == 0 else (len(k) // 3, len(k))  # uneven halves
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        keys, aggs = _partial(k[lo:hi], x[lo:hi], v[lo:hi], w[lo:hi])
+        out[rank] = repartition_merge_groupby(keys, aggs)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_repartition_merge_of_high_cardinality_groups():
+    """Sparse 40-bit keys: each rank ends with the groups its hash owns -- disjoint shares that together
+    equal the aggregation of all rows."""
+    ctx = mp.get_context("spawn")
+    manager = ctx.Manager()
+    out = manager.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_repart, args=(r, 2, port, 9, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(240)
+        assert p.exitcode == 0
+    ek, eaggs = _partial(*_hc_data(9))
+    k0, a0 = out[0]
+    k1, a1 = out[1]
+    assert len(np.intersect1d(k0, k1)) == 0 and len(k0) > 0 and len(k1) > 0
+    keys = np.concatenate([k0, k1])
+    order = np.argsort(keys)
+    assert np.array_equal(keys[order], ek)
+    sx = np.concatenate([a0[0], a1[0]])[order]
+    sv = np.concatenate([a0[1], a1[1]])[order]
+    rest = [np.concatenate([a0[i], a1[i]])[order] for i in (2, 3, 4)]
+    assert np.all(np.abs(sx - eaggs[0][1]) <= 1e-12 * np.maximum(np.abs(eaggs[0][1]), 1e-300) + 1e-12)
+    assert np.array_equal(sv["lower"], eaggs[1][1]["lower"]) and np.array_equal(sv["upper"], eaggs[1][1]["upper"])
+    for got, (_, exp) in zip(rest, eaggs[2:]):
+        assert np.array_equal(got, exp)

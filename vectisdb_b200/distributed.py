@@ -7,8 +7,10 @@ with the rank's partial values (the identity elsewhere) and is combined with one
 for sums and counts, MIN and MAX for those. 128-bit integer sums (DuckDB's HUGEINT, the engine's
 `{lower, upper}` pairs) travel as four 32-bit chunks summed in 64-bit lanes, which cannot overflow
 for fewer than 2^31 ranks, and are carried back into 128 bits, so the merged sum is exact. AVG does
-not merge from its outputs: shard its SUM and COUNT instead. Every rank makes the same collective
-calls in the same order, whatever rows it holds (an empty partial contributes identities).
+not merge from its outputs: shard its SUM and COUNT instead. `repartition_merge_groupby` handles key
+spaces too large to index (the high-cardinality shape): partial groups move to the rank owning their
+key's hash with all-to-all exchanges and merge there. Every rank makes the same collective calls in
+the same order, whatever rows it holds (an empty partial contributes identities).
 
 Works with the "gloo" backend on CPU tensors and with "nccl" on CUDA tensors of the rank's device.
 """
@@ -93,14 +95,108 @@ def _merge_i128(values: np.ndarray, slot: np.ndarray, domain: int, device: str) 
         dense = np.zeros(domain, np.int64)
         dense[slot] = c
         sums.append(_all_reduce(dense, dist.ReduceOp.SUM, device))
+    return _i128_from_chunks(sums)
+
+
+def _owner(keys: np.ndarray, world: int) -> np.ndarray:
+    """Rank owning each key: a 64-bit mix of the key (so skewed or sequential keys spread), mod world."""
+    with np.errstate(over="ignore"):
+        k = keys.astype(np.uint64)
+        k = (k ^ (k >> np.uint64(33))) * np.uint64(0xFF51AFD7ED558CCD)
+        k = (k ^ (k >> np.uint64(33))) * np.uint64(0xC4CEB9FE1A85EC53)
+        k ^= k >> np.uint64(33)
+    return (k % np.uint64(world)).astype(np.int64)
+
+
+def _exchange(columns: list[np.ndarray], send_counts: np.ndarray, device: str) -> tuple[list[np.ndarray], np.ndarray]:
+    """all_to_all of row-aligned int64/float64 columns already ordered by destination rank."""
+    import torch
+    import torch.distributed as dist
+    world = send_counts.shape[0]
+    recv_counts = torch.empty(world, dtype=torch.int64, device=device)
+    dist.all_to_all_single(recv_counts, torch.from_numpy(send_counts.astype(np.int64)).to(device))
+    recv = recv_counts.cpu().numpy()
+    out = []
+    for col in columns:
+        src = torch.from_numpy(np.ascontiguousarray(col)).to(device)
+        dst = torch.empty(int(recv.sum()), dtype=src.dtype, device=device)
+        dist.all_to_all_single(dst, src, recv.tolist(), send_counts.tolist())
+        out.append(dst.cpu().numpy())
+    return out, recv
+
+
+def _i128_from_chunks(chunk_sums: list[np.ndarray]) -> np.ndarray:
+    """128-bit values from the sums of their 32-bit chunks (c0..c2 non-negative, c3 signed)."""
     low = []
-    carry = np.zeros(domain, np.int64)
-    for s in sums[:3]:
-        t = s + carry  # non-negative: sums of non-negative chunks plus carries
+    carry = np.zeros(chunk_sums[0].shape[0], np.int64)
+    for s in chunk_sums[:3]:
+        t = s + carry
         low.append((t & 0xFFFFFFFF).astype(np.uint64))
         carry = t >> 32
-    top = sums[3] + carry
-    out = np.empty(domain, HUGEINT)
+    top = chunk_sums[3] + carry
+    out = np.empty(chunk_sums[0].shape[0], HUGEINT)
     out["lower"] = low[0] | (low[1] << np.uint64(32))
     out["upper"] = (low[2] | (top.view(np.uint64) << np.uint64(32))).view(np.int64)
     return out
+
+
+def repartition_merge_groupby(keys: np.ndarray, aggregates: Sequence[tuple[str, np.ndarray]],
+                              device: str = "cpu") -> tuple[np.ndarray, list[np.ndarray]]:
+    """Merges partial groups of a key space too large to index (the high-cardinality shape): every
+    partial group goes to the rank that owns its key (a hash of the key), with one all-to-all per
+    column, and each rank merges what it received. `keys` are the packed group keys (int64). Returns
+    this rank's share of the merged groups, keys ascending; the ranks' shares are disjoint and together
+    hold every group. Exactness as in merge_dense_groupby."""
+    import torch.distributed as dist
+    keys = np.asarray(keys, dtype=np.int64)
+    for kind, values in aggregates:  # checked before any collective, so every rank fails alike
+        if kind not in KINDS:
+            raise ValueError(f"repartition_merge_groupby: aggregate kind {kind!r} does not merge (one of {KINDS})")
+        if np.asarray(values).shape[0] != keys.shape[0]:
+            raise ValueError("repartition_merge_groupby: one value per key is needed")
+    world = dist.get_world_size()
+    owner = _owner(keys, world)
+    order = np.argsort(owner, kind="stable")
+    send = np.bincount(owner, minlength=world).astype(np.int64)
+    columns = [keys[order]]
+    layout = []  # (kind, first column index, column count)
+    for kind, values in aggregates:
+        values = np.asarray(values)[order]
+        if kind == "sum_i128":
+            v = values.astype(HUGEINT, copy=False)
+            layout.append((kind, len(columns), 2))
+            columns += [v["lower"].view(np.int64), v["upper"].astype(np.int64)]
+        else:
+            layout.append((kind, len(columns), 1))
+            columns.append(values.astype(np.float64 if kind == "sum_f64" else np.int64))
+    got, _ = _exchange(columns, send, device)
+    rkeys = got[0]
+    ukeys, pos = np.unique(rkeys, return_inverse=True)
+    g = ukeys.shape[0]
+    merged = []
+    for kind, first, _n in layout:
+        col = got[first]
+        if kind == "sum_f64":
+            acc = np.zeros(g, np.float64)
+            np.add.at(acc, pos, col)
+        elif kind == "count":
+            acc = np.zeros(g, np.int64)
+            np.add.at(acc, pos, col)
+        elif kind in ("min", "max"):
+            info = np.iinfo(np.int64)
+            acc = np.full(g, info.max if kind == "min" else info.min, np.int64)
+            (np.minimum if kind == "min" else np.maximum).at(acc, pos, col)
+        else:
+            lower = col.view(np.uint64)
+            upper = got[first + 1]
+            mask = np.uint64(0xFFFFFFFF)
+            chunks = [(lower & mask).astype(np.int64), (lower >> np.uint64(32)).astype(np.int64),
+                      (upper.view(np.uint64) & mask).astype(np.int64), upper >> np.int64(32)]
+            sums = []
+            for c in chunks:  # at most 2^31 partials per group keep these sums inside 64 bits
+                acc_c = np.zeros(g, np.int64)
+                np.add.at(acc_c, pos, c)
+                sums.append(acc_c)
+            acc = _i128_from_chunks(sums)
+        merged.append(acc)
+    return ukeys, merged
