@@ -207,7 +207,7 @@ private:
 		uint32_t *hmap = nullptr;        // [P] (state index << 16) | slot, or ~0
 		uint32_t *keys = nullptr;        // [max_keys] mixed keys
 		uint32_t *count = nullptr;       // selected keys (<= max_keys)
-		uint32_t *overflow = nullptr;    // set when an integer partial sum leaves 64 bits
+		uint32_t *overflow = nullptr;    // set when an integer partial sum leaves 64 bits (status word)
 		uint32_t max_keys = 0;
 		uint64_t state_bytes = 0;        // per heavy key
 		size_t smem(uint64_t P) const {
@@ -1114,13 +1114,11 @@ Executor::HeavyPlan Executor::PlanHeavy(const PipelineCodegen::GroupBySpec &gb, 
 	uint32_t *scount = arena_.AllocT<uint32_t>(SC);
 	hp.hmap = arena_.AllocT<uint32_t>(P);
 	hp.keys = arena_.AllocT<uint32_t>(K);
-	uint32_t *info = arena_.AllocT<uint32_t>(2);  // [0] selected keys, [1] overflow flag
-	hp.count = info;
-	hp.overflow = info + 1;
+	hp.count = arena_.AllocT<uint32_t>(1);  // selected keys (the caller points `overflow` at its status block)
 	VGPU_CUDA(cudaMemsetAsync(skeys, 0xff, static_cast<size_t>(SC) * 8, stream_));
 	VGPU_CUDA(cudaMemsetAsync(scount, 0, static_cast<size_t>(SC) * 4, stream_));
 	VGPU_CUDA(cudaMemsetAsync(hp.hmap, 0xff, P * 4, stream_));
-	VGPU_CUDA(cudaMemsetAsync(info, 0, 8, stream_));
+	VGPU_CUDA(cudaMemsetAsync(hp.count, 0, 4, stream_));
 	const uint64_t samples = std::min<uint64_t>(ntiles, 64);
 	const uint64_t stride = ntiles / samples;
 	KArgsHost a;
