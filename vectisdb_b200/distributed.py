@@ -12,6 +12,11 @@ spaces too large to index (the high-cardinality shape): partial groups move to t
 key's hash with all-to-all exchanges and merge there. Every rank makes the same collective calls in
 the same order, whatever rows it holds (an empty partial contributes identities).
 
+`sharded_group_by` runs a whole GROUP BY plan this way: it rewrites AVG into SUM + COUNT(*), runs the
+plan on the rank's rows through a caller-supplied executor (the engine), packs multi-column keys from
+their global ranges, picks one of the two merges by the packed domain, and finishes AVG exactly as the
+engine's own finalize does.
+
 Works with the "gloo" backend on CPU tensors and with "nccl" on CUDA tensors of the rank's device.
 """
 from __future__ import annotations
@@ -200,3 +205,104 @@ def repartition_merge_groupby(keys: np.ndarray, aggregates: Sequence[tuple[str, 
             acc = _i128_from_chunks(sums)
         merged.append(acc)
     return ukeys, merged
+
+
+def sharded_group_by(node, run_local, column_types=None, device: str = "cpu"):
+    """A GROUP BY over rows split across ranks. `run_local(plan)` runs `plan` on this rank's rows (with
+    the engine, say `lambda p: GpuEngine.instance().execute_plan(p, my_inputs).columns`) and returns its
+    host result columns (GpuColumn-like: `.data` and `.validity`; the group keys, then one column per
+    aggregate). AVG runs as SUM plus COUNT(*) -- `column_types` maps each AVG input to its value type,
+    which decides the SUM: HUGEINT over integers, DOUBLE over floats -- and is finished after the merge
+    as the engine finishes it (the 128-bit sum correctly rounded to double, then divided by the group's
+    row count). Keys pack like the engine's: each key column offset by its global minimum (found with
+    an all-reduce) in as many bits as its global range needs. A packed domain of at most 2^20 values
+    merges densely and every rank gets the whole result; a larger one merges by hash repartition and
+    each rank gets a disjoint share. Groups come sorted by their keys, first key first. Dictionary-string
+    keys must use one dictionary on every rank. NULL group keys or NULL aggregate outputs are refused on
+    every rank alike. Returns
+    [(name, numpy array)]: the keys by name, then `agg_<i>` per aggregate of `node`, in order."""
+    import torch.distributed as dist
+    from .engine import GpuAggregateKind as A, GpuOpType, GpuPlanNode, GpuValueType as T, NUMPY_DTYPE, make_aggregate
+    if node.op_type != GpuOpType.GROUP_BY_AGGREGATE or not node.group_keys:
+        raise ValueError("sharded_group_by: a GROUP BY node with group keys is needed")
+    column_types = dict(column_types or {})
+    plan_aggs, kinds, finish = [], [], []
+    count_at = None
+    for a in node.aggregates:
+        if a.kind == A.AVG:
+            if a.input_column not in column_types:
+                raise ValueError(f"sharded_group_by: the value type of AVG input {a.input_column!r} is needed")
+            is_float = T(column_types[a.input_column]) in (T.FLOAT32, T.FLOAT64)
+            s = len(plan_aggs)
+            plan_aggs.append(make_aggregate(A.SUM, a.input_column, T.FLOAT64 if is_float else T.HUGEINT))
+            kinds.append("sum_f64" if is_float else "sum_i128")
+            if count_at is None:
+                count_at = len(plan_aggs)
+                plan_aggs.append(make_aggregate(A.COUNT_STAR, "", T.INT64))
+                kinds.append("count")
+            finish.append(("avg", s, is_float))
+        else:
+            out_t = T(a.output_type)
+            finish.append(("col", len(plan_aggs), out_t))
+            plan_aggs.append(a)
+            if a.kind in (A.COUNT_STAR, A.COUNT):
+                kinds.append("count")
+            elif a.kind in (A.MIN, A.MAX):
+                kinds.append("min" if a.kind == A.MIN else "max")
+            else:
+                kinds.append("sum_i128" if out_t == T.HUGEINT else "sum_f64")
+    plan = GpuPlanNode(node.op_type, list(node.children), estimated_rows=node.estimated_rows,
+                       estimated_row_width_bytes=node.estimated_row_width_bytes, group_keys=list(node.group_keys),
+                       aggregates=plan_aggs)
+    cols = list(run_local(plan))
+    nk = len(node.group_keys)
+    if len(cols) != nk + len(plan_aggs):
+        raise ValueError("sharded_group_by: the local result has the wrong number of columns")
+    nulls = any(c.validity is not None and not np.all(c.validity) for c in cols)
+    keys = [np.asarray(c.data).astype(np.int64) for c in cols[:nk]]
+    key_dtypes = [np.asarray(c.data).dtype for c in cols[:nk]]
+    rows = keys[0].shape[0]
+    info = np.iinfo(np.int64)
+    lo = _all_reduce(np.array([k.min() if rows else info.max for k in keys], np.int64), dist.ReduceOp.MIN, device)
+    hi = _all_reduce(np.array([k.max() if rows else info.min for k in keys] + [int(nulls)], np.int64),
+                     dist.ReduceOp.MAX, device)
+    if hi[-1]:
+        raise ValueError("sharded_group_by: NULL group keys or NULL aggregate values do not merge here")
+    hi = hi[:-1]
+    empty = lo[0] > hi[0]  # no rank has a group
+    bits = [0] * nk if empty else [int(h - l).bit_length() for l, h in zip(lo.tolist(), hi.tolist())]
+    if sum(bits) > 63:
+        raise ValueError("sharded_group_by: the group keys need more than 63 bits packed")
+    shifts = [sum(bits[i + 1:]) for i in range(nk)]  # first key highest: ascending packed = lexicographic
+    aggs = list(zip(kinds, [c.data for c in cols[nk:]]))
+    if empty:
+        mkeys = np.zeros(0, np.int64)
+        merged = [np.zeros(0, HUGEINT if k == "sum_i128" else np.float64 if k == "sum_f64" else np.int64)
+                  for k in kinds]
+    else:
+        packed = np.zeros(rows, np.int64)
+        for k, l, sh in zip(keys, lo.tolist(), shifts):
+            packed |= (k - l) << sh
+        if (1 << sum(bits)) <= _MAX_DOMAIN:
+            mkeys, merged = merge_dense_groupby(packed, aggs, 0, (1 << sum(bits)) - 1, device)
+        else:
+            mkeys, merged = repartition_merge_groupby(packed, aggs, device)
+    out = []
+    for name, l, b, sh, dt in zip(node.group_keys, lo.tolist(), bits, shifts, key_dtypes):
+        out.append((name, (((mkeys >> sh) & ((1 << b) - 1)) + l).astype(dt)))
+    for i, f in enumerate(finish):
+        if f[0] == "avg":
+            _, s, is_float = f
+            n = merged[count_at]
+            if is_float:
+                vals = merged[s] / n.astype(np.float64)
+            else:
+                h = merged[s]
+                vals = np.array([float((int(up) << 64) | int(lw)) / float(c)
+                                 for lw, up, c in zip(h["lower"].tolist(), h["upper"].tolist(), n.tolist())],
+                                np.float64)
+        else:
+            _, s, t = f
+            vals = merged[s] if t in (T.HUGEINT, T.FLOAT64) else merged[s].astype(NUMPY_DTYPE[t])
+        out.append((f"agg_{i}", vals))
+    return out
