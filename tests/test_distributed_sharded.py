@@ -5,7 +5,8 @@ result must equal the same GROUP BY over all rows: exactly for keys, counts, MIN
 integer AVG (the 128-bit sum is exact however the rows are split, so its correctly rounded quotient is
 too), within 1e-12 relative for FP64 sums and float AVG. Covered: two key columns in a dense packed
 domain (every rank gets the whole result), a sparse 40-bit key (hash repartition, disjoint shares), a
-rank with no rows, no rows anywhere, and NULL keys refused on both ranks without a hang."""
+rank with no rows, no rows anywhere, a join + group-by whose build side is broadcast from one rank
+while the probe rows are split, and NULL keys refused on both ranks without a hang."""
 import os
 import socket
 import sys
@@ -19,7 +20,7 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 from vectisdb_b200.engine import (GpuAggregateKind as A, GpuColumn, GpuValueType as T, HUGEINT_DTYPE,  # noqa: E402
-                                  make_aggregate, make_group_by, make_scan)
+                                  make_aggregate, make_group_by, make_join, make_scan)
 
 
 def _free_port():
@@ -116,6 +117,34 @@ def _sparse_case(seed):
     return node, arrays
 
 
+def _join_case(seed):
+    """A key/foreign-key join feeding a group-by on a build-side column (the join + group-by shape)."""
+    rng = np.random.default_rng(seed)
+    nb, n = 4096, 30000
+    build = {"bk": rng.permutation(nb).astype(np.int32), "bv": rng.integers(0, 300, nb).astype(np.int16),
+             "bh": np.zeros(nb, HUGEINT_DTYPE)}
+    build["bh"]["lower"] = rng.integers(0, 1 << 63, nb, dtype=np.int64).astype(np.uint64)
+    build["bh"]["upper"] = rng.integers(-5, 5, nb)
+    probe = {"pk": rng.integers(0, nb + 200, n).astype(np.int32),  # some probe keys miss
+             "x": rng.random(n) + 1.0,
+             "v": rng.integers((1 << 62) - 1000, 1 << 62, n, dtype=np.int64) * rng.choice([-1, 1], n)}
+    node = make_group_by(["bv"], [make_aggregate(A.COUNT_STAR, "", T.INT64), make_aggregate(A.AVG, "v", T.FLOAT64),
+                                  make_aggregate(A.SUM, "x", T.FLOAT64), make_aggregate(A.AVG, "x", T.FLOAT64)],
+                         make_join("bk", "pk", ["bv", "x", "v"], make_scan(["bk", "bv"]), make_scan(["pk", "x", "v"])))
+    return node, build, probe
+
+
+def _join(build, probe):
+    """Inner join of probe rows with the unique build keys: the probe rows that match, with bv."""
+    order = np.argsort(build["bk"])
+    sk = build["bk"][order]
+    pos = np.minimum(np.searchsorted(sk, probe["pk"]), len(sk) - 1)
+    hit = sk[pos] == probe["pk"]
+    out = {k: v[hit] for k, v in probe.items()}
+    out["bv"] = build["bv"][order][pos[hit]]
+    return out
+
+
 TYPES = {"x": T.FLOAT64, "v": T.INT64}
 
 
@@ -143,6 +172,13 @@ def _rank(rank, world, port, out):
         n = len(arrays["k"])
         part = _slice(arrays, 0, n // 2) if rank == 0 else _slice(arrays, n // 2, n)
         out[("sparse", rank)] = sharded_group_by(node, lambda p: _group(p, part, False), TYPES)
+        node, build, probe = _join_case(6)
+        from vectisdb_b200.distributed import broadcast_table
+        got = broadcast_table(build if rank == 0 else None)
+        out[("broadcast", rank)] = got
+        n = len(probe["pk"])
+        part = _slice(probe, 0, n // 4) if rank == 0 else _slice(probe, n // 4, n)
+        out[("join", rank)] = sharded_group_by(node, lambda p: _group(p, _join(got, part), False), TYPES)
         node, arrays = _dense_case(5)
         validity = (lambda g: np.arange(g) != 0) if rank == 1 else None  # one NULL key on rank 1 only
         try:
@@ -215,6 +251,16 @@ def test_sparse_keys_repartition_into_disjoint_shares(results):
     order = np.argsort(np.concatenate([a[0][1], b[0][1]]))
     got = [(na, np.concatenate([va, vb])[order]) for (na, va), (_, vb) in zip(a, b)]
     _check(got, exp, node)
+
+
+def test_broadcast_build_side_and_probe_sharded_join_group_by(results):
+    node, build, probe = _join_case(6)
+    for rank in (0, 1):
+        got = results[("broadcast", rank)]
+        assert list(got) == list(build)
+        for name in build:
+            assert got[name].dtype == build[name].dtype and got[name].tobytes() == build[name].tobytes()
+        _check(results[("join", rank)], _expect(node, _join(build, probe)), node)
 
 
 def test_null_keys_are_refused_on_both_ranks(results):

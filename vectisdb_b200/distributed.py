@@ -306,3 +306,34 @@ def sharded_group_by(node, run_local, column_types=None, device: str = "cpu"):
             vals = merged[s] if t in (T.HUGEINT, T.FLOAT64) else merged[s].astype(NUMPY_DTYPE[t])
         out.append((f"agg_{i}", vals))
     return out
+
+
+def broadcast_table(columns, src: int = 0, device: str = "cpu") -> dict:
+    """The join + group-by shape sharded by probe rows needs the whole build side on every rank: rank
+    `src` passes its columns ({name: 1-D numpy array}, any fixed-width dtype including HUGEINT), the
+    others pass None, and every rank returns the same columns. Names, dtypes and lengths travel first
+    (one object broadcast), then each column as its raw bytes (one broadcast per column)."""
+    import torch
+    import torch.distributed as dist
+    if dist.get_rank() == src:
+        cols = {name: np.ascontiguousarray(np.asarray(v)) for name, v in columns.items()}
+        if any(v.ndim != 1 or v.dtype.hasobject for v in cols.values()):
+            header = [None]  # refused on every rank after the header broadcast
+        else:
+            header = [[(name, v.dtype.descr if v.dtype.names else v.dtype.str, v.shape[0])
+                       for name, v in cols.items()]]
+    else:
+        cols, header = None, [None]
+    dist.broadcast_object_list(header, src=src)
+    if header[0] is None:
+        raise ValueError("broadcast_table: columns must be 1-D arrays of a fixed-width dtype")
+    out = {}
+    for name, descr, rows in header[0]:
+        dtype = np.dtype([tuple(f) for f in descr]) if isinstance(descr, list) else np.dtype(descr)
+        if cols is not None:
+            buf = torch.from_numpy(cols[name].view(np.uint8).copy()).to(device)
+        else:
+            buf = torch.empty(rows * dtype.itemsize, dtype=torch.uint8, device=device)
+        dist.broadcast(buf, src=src)
+        out[name] = buf.cpu().numpy().view(dtype)
+    return out
