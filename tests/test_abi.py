@@ -74,3 +74,48 @@ def test_row_independence_and_working_set():
     ws = estimate_working_set(plan)
     assert ws.total_bytes >= (1 << 27) * 32
     assert ws.largest_operator in (b"GROUP_BY_AGGREGATE", b"SCAN")
+
+
+def test_working_set_formulas():
+    """The serving admission estimate (csrc/cost_model.cpp), pinned on hand-computed plans: the scan's
+    rows x width; dense outputs plus per-tile counts for a filter; carried record words, output rows and
+    partition offsets for a group-by; widened keys, search/permutation buffers and output for a join;
+    every pair for a cross product. Sizes saturate instead of wrapping."""
+    from vectisdb_b200.engine import (GpuAggregateKind as A, GpuValueType as T, estimate_working_set, make_aggregate,
+                                      make_cross_product, make_expr, make_filter, make_group_by, make_join,
+                                      make_projection, make_scan)
+    scan = make_scan(["k", "v", "w"])
+    scan.estimated_rows, scan.estimated_row_width_bytes = 1000, 20
+    filt = make_filter([make_expr("out[idx] = 1;", ["v"], T.BOOLEAN)], scan)
+    gb = make_group_by(["k"], [make_aggregate(A.SUM, "v", T.FLOAT64), make_aggregate(A.COUNT_STAR, "", T.INT64)], filt)
+    ws = estimate_working_set(gb)
+    scan_b = 1000 * 20
+    filt_b = 1000 * 20 + 1000 // 256 + 64
+    gb_b = 1000 * (8 + 8) + 1000 * (8 * 3 + 8) + 1 * 2048 * 4  # key + SUM carried; keys+aggs+8 out; offsets
+    assert ws.total_bytes == scan_b + filt_b + gb_b
+    assert ws.largest_bytes == gb_b and ws.largest_operator == b"GROUP_BY_AGGREGATE" and not ws.chunk_capped
+
+    big = make_scan(["k"])
+    big.estimated_rows, big.estimated_row_width_bytes = 1_000_000, 4
+    proj = make_projection([make_expr("((int*)out)[idx] = ((const int*)inputs[0])[row];", ["k"], T.INT32)], big)
+    ws = estimate_working_set(proj, max_chunk_rows=1000)  # row-independent: charged one chunk at a time
+    assert ws.chunk_capped and ws.total_bytes == 1000 * 4 + (1000 * 8 + 1000 // 256 + 64)
+
+    left, right = make_scan(["a", "x"]), make_scan(["b", "g"])
+    left.estimated_rows, left.estimated_row_width_bytes = 100, 16
+    right.estimated_rows, right.estimated_row_width_bytes = 50, 12
+    join = make_join("a", "b", ["a", "x", "g"], left, right)
+    ws = estimate_working_set(join)
+    join_b = 100 * 24 + 50 * 24 + 100 * (3 * 8 + 8)
+    assert ws.total_bytes == 1600 + 600 + join_b and ws.largest_operator == b"HASH_JOIN"
+
+    l2, r2 = make_scan(["a"]), make_scan(["b"])
+    l2.estimated_rows, l2.estimated_row_width_bytes = 10, 4
+    r2.estimated_rows, r2.estimated_row_width_bytes = 20, 4
+    ws = estimate_working_set(make_cross_product(["a", "b"], l2, r2))
+    assert ws.total_bytes == 40 + 80 + 200 * 16 and ws.largest_operator == b"CROSS_PRODUCT"
+
+    huge = make_scan(["k"])
+    huge.estimated_rows, huge.estimated_row_width_bytes = 1 << 62, 8
+    ws = estimate_working_set(make_filter([make_expr("out[idx] = 1;", ["k"], T.BOOLEAN)], huge))
+    assert ws.total_bytes == (1 << 64) - 1
