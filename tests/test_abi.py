@@ -119,3 +119,19 @@ def test_working_set_formulas():
     huge.estimated_rows, huge.estimated_row_width_bytes = 1 << 62, 8
     ws = estimate_working_set(make_filter([make_expr("out[idx] = 1;", ["k"], T.BOOLEAN)], huge))
     assert ws.total_bytes == (1 << 64) - 1
+
+
+def test_row_independence_by_operator():
+    """Scans, projections and filters are row-wise (a chunk can run alone); a group-by, join or cross
+    product anywhere below the root makes the plan need its input whole (cost model IsRowIndependent)."""
+    from vectisdb_b200.engine import (GpuAggregateKind as A, GpuValueType as T, is_row_independent, make_aggregate,
+                                      make_cross_product, make_expr, make_filter, make_group_by, make_join,
+                                      make_projection, make_scan)
+    e = make_expr("out[idx] = 1;", ["a"], T.BOOLEAN)
+    assert is_row_independent(make_scan(["a"]))
+    assert is_row_independent(make_filter([e], make_projection([e], make_filter([e], make_scan(["a"])))))
+    gb = make_group_by(["a"], [make_aggregate(A.COUNT_STAR, "", T.INT64)], make_scan(["a"]))
+    assert not is_row_independent(gb)
+    assert not is_row_independent(make_filter([e], gb))
+    assert not is_row_independent(make_projection([e], make_join("a", "b", ["a"], make_scan(["a"]), make_scan(["b"]))))
+    assert not is_row_independent(make_cross_product(["a", "b"], make_scan(["a"]), make_scan(["b"])))
