@@ -29,6 +29,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 PEAKS = ROOT / "MEASURED_PEAKS.json"
+CPU_BASELINE_LABEL = "C++ restatement of the query (OpenMP, oracle/oracle.cpp), not DuckDB: DuckDB is not installed"
 
 
 def hbm_peak():
@@ -250,7 +251,7 @@ def run_reference(args, world, rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
             "impl": "reference",
             "config": {"workload": name, "rows_per_step": sample, "parallelism": "host threads"},
-            "cpu_baseline": {"value": value, "unit": "rows/s", "cores": cores, "kind": "port", "sample": desc},
+            "cpu_baseline": {"value": value, "unit": "rows/s", "cores": cores, "kind": "port", "label": CPU_BASELINE_LABEL, "sample": desc},
             "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -416,7 +417,7 @@ def run_c3(args, world, rank, local):
         for w in sample:
             O.c0(w.inputs[0].data, w.inputs[1].data, w.inputs[2].data, w.params["v_lt"], w.params["w_mod"])
         dt = time.perf_counter() - t0
-        cpu = {"value": sum(w.rows for w in sample) / dt, "unit": "rows/s", "cores": O.threads(), "kind": "port",
+        cpu = {"value": sum(w.rows for w in sample) / dt, "unit": "rows/s", "cores": O.threads(), "kind": "port", "label": CPU_BASELINE_LABEL,
                "sample": f"the first {len(sample)} of the {len(wls)} queries, run one after another"}
 
     if rank == 0:
@@ -776,14 +777,14 @@ def main():
             for _ in range(reps):
                 O.c1(*cols, s.params["ts_gt"])
             dt = (time.perf_counter() - t0) / reps
-            cpu = {"value": sample / dt, "unit": "rows/s", "cores": O.threads(), "kind": "port",
+            cpu = {"value": sample / dt, "unit": "rows/s", "cores": O.threads(), "kind": "port", "label": CPU_BASELINE_LABEL,
                    "sample": "first 2^23 rows of the c1 table (same generator and median rule)"}
         elif name == "c0":
             cols = [c.data for c in wl.inputs]
             t0 = time.perf_counter()
             O.c0(*cols, 0.5, 7)
             dt = time.perf_counter() - t0
-            cpu = {"value": wl.rows / dt, "unit": "rows/s", "cores": O.threads(), "kind": "port",
+            cpu = {"value": wl.rows / dt, "unit": "rows/s", "cores": O.threads(), "kind": "port", "label": CPU_BASELINE_LABEL,
                    "sample": "the full c0 table"}
         elif name == "c2":
             pkey, x, bkey, g = [c.data for c in wl.inputs]
@@ -792,7 +793,7 @@ def main():
             t0 = time.perf_counter()
             O.c2(bkey, g, pkey[:sample], x[:sample])
             dt = time.perf_counter() - t0
-            cpu = {"value": sample / dt, "unit": "rows/s", "cores": O.threads(), "kind": "port",
+            cpu = {"value": sample / dt, "unit": "rows/s", "cores": O.threads(), "kind": "port", "label": CPU_BASELINE_LABEL,
                    "sample": "the full 2^24-row build side joined with the first 2^24 probe rows (rows/s of "
                              "probe rows, build time included)"}
 
