@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define VGPU_ABI_VERSION 1
+#define VGPU_ABI_VERSION 2
 
 typedef enum vgpu_status {
 	VGPU_OK = 0,
@@ -88,6 +88,9 @@ typedef struct vgpu_expr {
 	const char *const *input_columns;
 	uint32_t n_input_columns;
 	uint32_t output_type; /* vgpu_value_type */
+	/* GpuExpr::estimated_ops_per_row (gpu_engine.hpp:79): weighted operations per row, priced by the
+	 * caller's translator; 0 = not priced. Read only by vgpu_analyze_plan_shape. */
+	double estimated_ops_per_row;
 } vgpu_expr;
 
 /* GpuAggregate (gpu_engine.hpp:96-104). input_column is NULL/empty for COUNT_STAR. */
@@ -262,6 +265,50 @@ typedef struct vgpu_working_set {
 int vgpu_is_row_independent(const vgpu_plan *plan);
 /* EstimateWorkingSet (gpu_engine.hpp:341), re-derived for this engine's own allocation sites. */
 vgpu_status vgpu_estimate_working_set(const vgpu_plan *plan, uint64_t max_chunk_rows, vgpu_working_set *out);
+
+/* Routing helpers the extension's table checker calls (extension/src/table_checker.cpp:400, 485-499).
+ * Plain arithmetic over the plan's advisory fields; no device is touched. */
+
+/* ExecutionMode (gpu_engine.hpp:23-27) */
+typedef enum vgpu_execution_mode {
+	VGPU_MODE_PIPELINE_STREAM_CACHED = 0,
+	VGPU_MODE_PIPELINE_STREAM_UNCACHED = 1,
+	VGPU_MODE_BATCH_DISPATCH = 2
+} vgpu_execution_mode;
+
+/* GpuWorkDensity (gpu_engine.hpp:250-264) */
+typedef enum vgpu_work_density {
+	VGPU_DENSITY_INSUFFICIENT = 0, /* priced, below VGPU_MIN_OPS_PER_SCANNED_ROW */
+	VGPU_DENSITY_INCONCLUSIVE = 1, /* between the thresholds, or nothing priced at all */
+	VGPU_DENSITY_SUFFICIENT = 2    /* at or above VGPU_OFFLOAD_OPS_PER_ROW */
+} vgpu_work_density;
+
+/* The reference's routing thresholds (gpu_engine.hpp:269, 279), kept so its routing decides alike. */
+#define VGPU_MIN_OPS_PER_SCANNED_ROW 3.0
+#define VGPU_OFFLOAD_OPS_PER_ROW 10.0
+
+/* GpuPlanShape (gpu_engine.hpp:284-317) */
+typedef struct vgpu_plan_shape {
+	uint64_t scanned_rows;  /* sum of SCAN estimated_rows (saturating) */
+	uint64_t scanned_bytes; /* sum of SCAN rows x row width (width 0 counts as 8 bytes) */
+	uint64_t max_rows;      /* largest estimated_rows of any node */
+	double total_ops;       /* sum over nodes of (sum of their expressions' ops per row) x rows evaluated */
+	double ops_per_scanned_row;
+	double ops_per_scanned_byte;
+	uint32_t density; /* vgpu_work_density */
+	double amplification; /* max_rows / scanned_rows (max_rows when nothing is scanned) */
+} vgpu_plan_shape;
+
+/* AnalyzePlanShape (gpu_engine.hpp:329). A FILTER's expressions are charged over the rows entering it
+ * (its child's estimated_rows), every other node's over its own estimated_rows. */
+vgpu_status vgpu_analyze_plan_shape(const vgpu_plan *plan, vgpu_plan_shape *out);
+/* EstimateColumnsSize (gpu_engine.hpp:342): sum of SCAN rows x row width (width 0 counts as 8 bytes). */
+vgpu_status vgpu_estimate_columns_size(const vgpu_plan *plan, uint64_t *out);
+/* DetermineExecutionMode (gpu_engine.hpp:348): PIPELINE_STREAM_UNCACHED when vram_budget > 0 and the
+ * scanned columns exceed vram_budget x threshold (the reference's default threshold is 0.75), else
+ * PIPELINE_STREAM_CACHED. `columns_size` (optional) receives the estimate it compared. */
+vgpu_status vgpu_determine_execution_mode(const vgpu_plan *plan, uint64_t vram_budget, double threshold,
+                                          uint32_t *mode, uint64_t *columns_size);
 
 /* ---- Device memory budget (cuda_engine/include/rmm_pool.hpp:32-141) -------------------------- */
 

@@ -135,3 +135,67 @@ def test_row_independence_by_operator():
     assert not is_row_independent(make_filter([e], gb))
     assert not is_row_independent(make_projection([e], make_join("a", "b", ["a"], make_scan(["a"]), make_scan(["b"]))))
     assert not is_row_independent(make_cross_product(["a", "b"], make_scan(["a"]), make_scan(["b"])))
+
+
+def test_plan_shape_columns_size_and_execution_mode():
+    """The routing helpers the extension's table checker calls, pinned on hand-computed plans: a
+    FILTER's price runs over the rows entering it, other nodes' over their own rows; nothing priced is
+    INCONCLUSIVE; below 3 ops per scanned row INSUFFICIENT, from 10 SUFFICIENT; a plan that scans nothing
+    keeps its numerators; a SCAN of width 0 counts 8 bytes per row; the uncached mode starts strictly
+    above budget x threshold."""
+    from vectisdb_b200.engine import (GpuAggregateKind as A, GpuExecutionMode as M, GpuValueType as T,
+                                      GpuWorkDensity as D, analyze_plan_shape, determine_execution_mode,
+                                      estimate_columns_size, make_aggregate, make_cross_product, make_expr,
+                                      make_filter, make_group_by, make_join, make_projection, make_scan,
+                                      serialize_plan_memo)
+
+    def chain(filter_prices, projection_price):
+        scan = make_scan(["a", "b"])
+        scan.estimated_rows, scan.estimated_row_width_bytes = 1000, 16
+        filt = make_filter([make_expr("out[idx] = 1;", ["a"], T.BOOLEAN, p) for p in filter_prices], scan)
+        filt.estimated_rows = 300
+        proj = make_projection([make_expr("out[idx] = 1;", ["a"], T.FLOAT64, projection_price)], filt)
+        proj.estimated_rows = 300
+        return proj
+
+    s = analyze_plan_shape(chain([2.0, 3.0], 4.0))
+    assert (s.scanned_rows, s.scanned_bytes, s.max_rows) == (1000, 16000, 1000)
+    assert s.total_ops == 5 * 1000 + 4 * 300 and s.ops_per_scanned_row == 6.2
+    assert s.ops_per_scanned_byte == 6200 / 16000 and s.amplification == 1.0 and s.density == D.INCONCLUSIVE
+    assert analyze_plan_shape(chain([2.0, 3.0], 40.0)).density == D.SUFFICIENT  # 17 ops per row
+    assert analyze_plan_shape(chain([2.0, 3.0], 50.0 / 3.0)).density == D.SUFFICIENT  # exactly 10
+    s = analyze_plan_shape(chain([1.0], 0.0))
+    assert s.ops_per_scanned_row == 1.0 and s.density == D.INSUFFICIENT
+
+    left, right = make_scan(["a"]), make_scan(["b"])
+    left.estimated_rows, right.estimated_rows = 100, 90
+    cross = make_cross_product(["a", "b"], left, right)
+    cross.estimated_rows = 9000
+    gb = make_group_by(["a"], [make_aggregate(A.COUNT_STAR, "", T.INT64)], cross)
+    gb.estimated_rows = 5
+    s = analyze_plan_shape(gb)  # unpriced: unmeasured, not cheap
+    assert s.total_ops == 0 and s.density == D.INCONCLUSIVE
+    assert s.scanned_bytes == 190 * 8 and s.amplification == 9000 / 190
+    assert estimate_columns_size(gb) == 1520
+
+    empty = make_scan(["a"])
+    proj = make_projection([make_expr("out[idx] = 1;", ["a"], T.FLOAT64, 2.0)], empty)
+    proj.estimated_rows = 10
+    s = analyze_plan_shape(proj)
+    assert s.scanned_rows == 0 and s.total_ops == 20 and s.ops_per_scanned_row == 20
+    assert s.ops_per_scanned_byte == 20 and s.amplification == 10 and s.density == D.SUFFICIENT
+
+    l2, r2 = make_scan(["a", "x"]), make_scan(["b"])
+    l2.estimated_rows, l2.estimated_row_width_bytes, r2.estimated_rows = 100, 16, 50
+    join = make_join("a", "b", ["a", "x"], l2, r2)
+    assert estimate_columns_size(join) == 100 * 16 + 50 * 8
+    assert determine_execution_mode(join, 0) == M.PIPELINE_STREAM_CACHED  # no budget: never uncached
+    assert determine_execution_mode(join, 2000) == M.PIPELINE_STREAM_UNCACHED  # 2000 > 1500
+    assert determine_execution_mode(join, 4000) == M.PIPELINE_STREAM_CACHED  # 2000 <= 3000
+    assert determine_execution_mode(join, 2000, 1.0) == M.PIPELINE_STREAM_CACHED  # strictly above
+
+    plan = chain([2.0], 4.0)  # the serialized-plan memo notices a changed price
+    first, _ = serialize_plan_memo(plan)
+    plan.expressions[0].estimated_ops_per_row = 5.0
+    again, _ = serialize_plan_memo(plan)
+    assert again is not first and again.nodes[again.root].expressions[0].estimated_ops_per_row == 5.0

@@ -12,7 +12,7 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / "libvgpu.so"
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # vgpu_status
 OK, ERR_INVALID_ARGUMENT, ERR_UNSUPPORTED, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_COMPILE, \
@@ -23,7 +23,8 @@ EXEC_NO_SYNC = 1
 
 class vgpu_expr(C.Structure):
     _fields_ = [("source", C.c_char_p), ("input_columns", C.POINTER(C.c_char_p)),
-                ("n_input_columns", C.c_uint32), ("output_type", C.c_uint32)]
+                ("n_input_columns", C.c_uint32), ("output_type", C.c_uint32),
+                ("estimated_ops_per_row", C.c_double)]
 
 
 class vgpu_aggregate(C.Structure):
@@ -106,6 +107,12 @@ class vgpu_working_set(C.Structure):
                 ("largest_operator", C.c_char * 32)]
 
 
+class vgpu_plan_shape(C.Structure):
+    _fields_ = [("scanned_rows", C.c_uint64), ("scanned_bytes", C.c_uint64), ("max_rows", C.c_uint64),
+                ("total_ops", C.c_double), ("ops_per_scanned_row", C.c_double),
+                ("ops_per_scanned_byte", C.c_double), ("density", C.c_uint32), ("amplification", C.c_double)]
+
+
 class vgpu_memory_stats(C.Structure):
     _fields_ = [("budget_bytes", C.c_uint64), ("in_use_bytes", C.c_uint64), ("peak_bytes", C.c_uint64),
                 ("allocations", C.c_uint64), ("failed_allocations", C.c_uint64)]
@@ -178,6 +185,10 @@ SIGNATURES = [
                                        C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     ("vgpu_is_row_independent", C.c_int, [C.POINTER(vgpu_plan)]),
     ("vgpu_estimate_working_set", C.c_int, [C.POINTER(vgpu_plan), C.c_uint64, C.POINTER(vgpu_working_set)]),
+    ("vgpu_analyze_plan_shape", C.c_int, [C.POINTER(vgpu_plan), C.POINTER(vgpu_plan_shape)]),
+    ("vgpu_estimate_columns_size", C.c_int, [C.POINTER(vgpu_plan), C.POINTER(C.c_uint64)]),
+    ("vgpu_determine_execution_mode", C.c_int, [C.POINTER(vgpu_plan), C.c_uint64, C.c_double,
+                                                 C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
     ("vgpu_memory_set_budget", C.c_int, [C.c_uint64]),
     ("vgpu_memory_stats_get", C.c_int, [C.POINTER(vgpu_memory_stats)]),
     ("vgpu_memory_has_headroom", C.c_int, [C.c_uint64]),

@@ -669,6 +669,32 @@ vgpu_status vgpu_estimate_working_set(const vgpu_plan *plan, uint64_t max_chunk_
 	});
 }
 
+vgpu_status vgpu_analyze_plan_shape(const vgpu_plan *plan, vgpu_plan_shape *out) {
+	return Guard([&] {
+		if (!out) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		auto root = ConvertPlan(plan);
+		*out = AnalyzePlanShape(*root);
+	});
+}
+
+vgpu_status vgpu_estimate_columns_size(const vgpu_plan *plan, uint64_t *out) {
+	return Guard([&] {
+		if (!out) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		auto root = ConvertPlan(plan);
+		*out = EstimateColumnsSize(*root);
+	});
+}
+
+vgpu_status vgpu_determine_execution_mode(const vgpu_plan *plan, uint64_t vram_budget, double threshold,
+                                          uint32_t *mode, uint64_t *columns_size) {
+	return Guard([&] {
+		if (!mode) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		auto root = ConvertPlan(plan);
+		*mode = DetermineExecutionMode(*root, vram_budget, threshold);
+		if (columns_size) *columns_size = EstimateColumnsSize(*root);
+	});
+}
+
 vgpu_status vgpu_memory_set_budget(uint64_t bytes) {
 	return Guard([&] {
 		Runtime::Get().EnsureDevice();

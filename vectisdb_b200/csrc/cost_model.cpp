@@ -132,6 +132,70 @@ vgpu_working_set EstimateWorkingSet(const PlanNode &plan, uint64_t max_chunk_row
 	return w.ws;
 }
 
+namespace {
+
+uint64_t ScanWidth(const PlanNode &n) {
+	return n.estimated_row_width_bytes ? n.estimated_row_width_bytes : 8;
+}
+
+// Post-order walk: SCAN leaves add their rows and bytes; every node may raise max_rows and adds its
+// expressions' price times the rows they run over (a FILTER tests every row entering it).
+void Shape(const PlanNode &n, vgpu_plan_shape &s) {
+	for (auto &c : n.children) Shape(*c, s);
+	if (n.op == OpType::SCAN) {
+		s.scanned_rows = SatAdd(s.scanned_rows, n.estimated_rows);
+		s.scanned_bytes = SatAdd(s.scanned_bytes, SatMul(n.estimated_rows, ScanWidth(n)));
+	}
+	s.max_rows = std::max<uint64_t>(s.max_rows, n.estimated_rows);
+	double price = 0.0;
+	for (auto &e : n.expressions) price += e.ops_per_row;
+	if (price != 0.0) {
+		uint64_t rows = n.estimated_rows;
+		if (n.op == OpType::FILTER) rows = n.children.empty() ? 0 : n.children[0]->estimated_rows;
+		s.total_ops += price * static_cast<double>(rows);
+	}
+}
+
+} // namespace
+
+vgpu_plan_shape AnalyzePlanShape(const PlanNode &plan) {
+	vgpu_plan_shape s;
+	std::memset(&s, 0, sizeof(s));
+	Shape(plan, s);
+	// Nothing scanned means nothing to amortise: the ratios fall back to the numerators themselves.
+	const double rows = static_cast<double>(s.scanned_rows);
+	const double bytes = static_cast<double>(s.scanned_bytes);
+	s.amplification = s.scanned_rows ? static_cast<double>(s.max_rows) / rows : static_cast<double>(s.max_rows);
+	s.ops_per_scanned_row = s.scanned_rows ? s.total_ops / rows : s.total_ops;
+	s.ops_per_scanned_byte = s.scanned_bytes ? s.total_ops / bytes : s.total_ops;
+	// Nothing priced is "unmeasured", never "cheap" (a group-by over a cross product carries no
+	// expression yet does the most work of all).
+	if (s.total_ops == 0.0) {
+		s.density = VGPU_DENSITY_INCONCLUSIVE;
+	} else if (s.ops_per_scanned_row >= VGPU_OFFLOAD_OPS_PER_ROW) {
+		s.density = VGPU_DENSITY_SUFFICIENT;
+	} else if (s.ops_per_scanned_row < VGPU_MIN_OPS_PER_SCANNED_ROW) {
+		s.density = VGPU_DENSITY_INSUFFICIENT;
+	} else {
+		s.density = VGPU_DENSITY_INCONCLUSIVE;
+	}
+	return s;
+}
+
+uint64_t EstimateColumnsSize(const PlanNode &plan) {
+	uint64_t total = plan.op == OpType::SCAN ? SatMul(plan.estimated_rows, ScanWidth(plan)) : 0;
+	for (auto &c : plan.children) total = SatAdd(total, EstimateColumnsSize(*c));
+	return total;
+}
+
+vgpu_execution_mode DetermineExecutionMode(const PlanNode &plan, uint64_t vram_budget, double threshold) {
+	const double size = static_cast<double>(EstimateColumnsSize(plan));
+	if (vram_budget > 0 && size > static_cast<double>(vram_budget) * threshold) {
+		return VGPU_MODE_PIPELINE_STREAM_UNCACHED;
+	}
+	return VGPU_MODE_PIPELINE_STREAM_CACHED;
+}
+
 std::string GenerateSourceText(const PlanNode &plan, const std::vector<vgpu_column> &inputs) {
 	const PlanNode *gb = nullptr;
 	const PlanNode *cur = &plan;

@@ -16,6 +16,18 @@ vgpu_working_set EstimateWorkingSet(const PlanNode &plan, uint64_t max_chunk_row
                                     const std::vector<uint64_t> *scan_rows = nullptr,
                                     const std::vector<uint32_t> *scan_widths = nullptr);
 
+//! Work-to-data ratio of a plan from its advisory fields (the reference's AnalyzePlanShape,
+//! cuda_engine/include/gpu_engine.hpp:284-329): the routing input of the extension's table checker.
+vgpu_plan_shape AnalyzePlanShape(const PlanNode &plan);
+
+//! Bytes of every SCAN's columns: estimated_rows x row width, width 0 counting as 8 bytes
+//! (EstimateColumnsSize, gpu_engine.hpp:342).
+uint64_t EstimateColumnsSize(const PlanNode &plan);
+
+//! PIPELINE_STREAM_UNCACHED when the scanned columns exceed vram_budget x threshold and a budget is
+//! given, else PIPELINE_STREAM_CACHED (DetermineExecutionMode, gpu_engine.hpp:344-348).
+vgpu_execution_mode DetermineExecutionMode(const PlanNode &plan, uint64_t vram_budget, double threshold);
+
 //! Generated source for the topmost pipeline of `plan` using only input descriptors (no device):
 //! lets a host without a GPU check that every fused kernel compiles. Group keys are assumed to span
 //! 16 bits each.

@@ -70,6 +70,7 @@ std::shared_ptr<PlanNode> ConvertPlan(const vgpu_plan *plan) {
 			expr.source = e.source;
 			expr.input_columns = Names(e.input_columns, e.n_input_columns, "expression inputs");
 			expr.output_type = static_cast<ValueType>(e.output_type);
+			expr.ops_per_row = e.estimated_ops_per_row;
 			node->expressions.push_back(std::move(expr));
 		}
 		node->build_keys = Names(src.build_keys, src.n_build_keys, "build_keys");

@@ -32,6 +32,7 @@ struct Expr {
 	std::string source;
 	std::vector<std::string> input_columns;
 	ValueType output_type = ValueType::FLOAT64;
+	double ops_per_row = 0.0;  // caller's price of one row (routing only); 0 = not priced
 };
 
 struct Aggregate {

@@ -41,6 +41,18 @@ class GpuValueType(enum.IntEnum):  # gpu_engine.hpp:29-38
     HUGEINT = 7
 
 
+class GpuExecutionMode(enum.IntEnum):  # gpu_engine.hpp:23-27
+    PIPELINE_STREAM_CACHED = 0
+    PIPELINE_STREAM_UNCACHED = 1
+    BATCH_DISPATCH = 2
+
+
+class GpuWorkDensity(enum.IntEnum):  # gpu_engine.hpp:250-264
+    INSUFFICIENT = 0
+    INCONCLUSIVE = 1
+    SUFFICIENT = 2
+
+
 class GpuAggregateKind(enum.IntEnum):  # gpu_engine.hpp:85-92
     COUNT_STAR = 0
     COUNT = 1
@@ -75,6 +87,7 @@ class GpuExpr:  # gpu_engine.hpp:56-80
     input_columns: list[str]
     output_type: GpuValueType = GpuValueType.FLOAT64
     source_hash: str = ""
+    estimated_ops_per_row: float = 0.0  # the translator's price of one row (routing only); 0 = not priced
 
 
 @dataclass
@@ -146,8 +159,8 @@ def make_scan(columns: Sequence[str], table: GpuTableRef | None = None) -> GpuPl
     return GpuPlanNode(GpuOpType.SCAN, table=table or GpuTableRef(), column_names=list(columns))
 
 
-def make_expr(body: str, inputs: Sequence[str], out_type: GpuValueType) -> GpuExpr:
-    return GpuExpr(body, list(inputs), GpuValueType(out_type))
+def make_expr(body: str, inputs: Sequence[str], out_type: GpuValueType, ops_per_row: float = 0.0) -> GpuExpr:
+    return GpuExpr(body, list(inputs), GpuValueType(out_type), estimated_ops_per_row=float(ops_per_row))
 
 
 def make_filter(exprs: Sequence[GpuExpr], child: GpuPlanNode) -> GpuPlanNode:
@@ -232,6 +245,7 @@ def serialize_plan(plan: GpuPlanNode, keep: _Keep) -> abi.vgpu_plan:
                 exprs[j].source = e.generated_cuda_source.encode()
                 exprs[j].input_columns, exprs[j].n_input_columns = keep.names(e.input_columns)
                 exprs[j].output_type = int(e.output_type)
+                exprs[j].estimated_ops_per_row = float(e.estimated_ops_per_row)
             keep.refs.append(exprs)
             n.expressions = C.cast(exprs, C.POINTER(abi.vgpu_expr))
         n.n_expressions = len(node.expressions)
@@ -261,7 +275,8 @@ def serialize_plan(plan: GpuPlanNode, keep: _Keep) -> abi.vgpu_plan:
 def _plan_snapshot(node: GpuPlanNode) -> tuple:
     """Every field serialize_plan reads, as nested tuples (equal snapshots serialize identically)."""
     return (int(node.op_type), node.table.catalog, node.table.schema, node.table.table, tuple(node.column_names),
-            tuple((e.generated_cuda_source, tuple(e.input_columns), int(e.output_type)) for e in node.expressions),
+            tuple((e.generated_cuda_source, tuple(e.input_columns), int(e.output_type), float(e.estimated_ops_per_row))
+                  for e in node.expressions),
             tuple(node.build_keys), tuple(node.probe_keys), tuple(node.output_columns), tuple(node.group_keys),
             tuple((int(a.kind), int(a.output_type), a.input_column) for a in node.aggregates),
             node.estimated_rows, node.estimated_row_width_bytes, tuple(_plan_snapshot(c) for c in node.children))
@@ -750,6 +765,32 @@ def estimate_working_set(plan: GpuPlanNode, max_chunk_rows: int = 0) -> abi.vgpu
     ws = abi.vgpu_working_set()
     abi.check(abi.lib().vgpu_estimate_working_set(C.byref(serialize_plan(plan, keep)), max_chunk_rows, C.byref(ws)))
     return ws
+
+
+def analyze_plan_shape(plan: GpuPlanNode) -> abi.vgpu_plan_shape:
+    """AnalyzePlanShape (gpu_engine.hpp:329): work per scanned row from the plan's advisory fields."""
+    keep = _Keep()
+    shape = abi.vgpu_plan_shape()
+    abi.check(abi.lib().vgpu_analyze_plan_shape(C.byref(serialize_plan(plan, keep)), C.byref(shape)))
+    return shape
+
+
+def estimate_columns_size(plan: GpuPlanNode) -> int:
+    """EstimateColumnsSize (gpu_engine.hpp:342): bytes of every SCAN's columns."""
+    keep = _Keep()
+    out = C.c_uint64()
+    abi.check(abi.lib().vgpu_estimate_columns_size(C.byref(serialize_plan(plan, keep)), C.byref(out)))
+    return int(out.value)
+
+
+def determine_execution_mode(plan: GpuPlanNode, vram_budget: int, threshold: float = 0.75) -> GpuExecutionMode:
+    """DetermineExecutionMode (gpu_engine.hpp:348): uncached streaming when the scanned columns exceed
+    vram_budget x threshold."""
+    keep = _Keep()
+    mode = C.c_uint32()
+    abi.check(abi.lib().vgpu_determine_execution_mode(C.byref(serialize_plan(plan, keep)), int(vram_budget),
+                                                      float(threshold), C.byref(mode), None))
+    return GpuExecutionMode(mode.value)
 
 
 def profile_enable(on: bool = True) -> None:
