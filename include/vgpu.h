@@ -80,6 +80,12 @@ typedef enum vgpu_aggregate_kind {
 	VGPU_AGG_AVG = 5
 } vgpu_aggregate_kind;
 
+/* GpuWindowPrimitive (gpu_engine.hpp:48-51) */
+typedef enum vgpu_window_primitive {
+	VGPU_WINDOW_NONE = 0,
+	VGPU_WINDOW_RUNNING_SUM = 1
+} vgpu_window_primitive;
+
 /* GpuExpr (gpu_engine.hpp:56-80). `source` is a CUDA statement that reads its inputs as
  * ((const T*)inputs[i])[row] and writes ((T*)out)[idx], exactly the form the reference's
  * expression translator emits (extension/src/expression_translator.cpp:311-315, 489-493). */
@@ -88,6 +94,11 @@ typedef struct vgpu_expr {
 	const char *const *input_columns;
 	uint32_t n_input_columns;
 	uint32_t output_type; /* vgpu_value_type */
+	/* GpuExpr::window_primitive (gpu_engine.hpp:48-51, 67): vgpu_window_primitive. RUNNING_SUM asks for
+	 * the running total of the expression across every row streamed so far; it is carried so that a
+	 * caller's plan never loses it, and every execution path of this engine refuses it with
+	 * VGPU_ERR_UNSUPPORTED (vgpu_pipeline_supports answers 0), so the caller runs it elsewhere. */
+	uint32_t window_primitive;
 	/* GpuExpr::estimated_ops_per_row (gpu_engine.hpp:79): weighted operations per row, priced by the
 	 * caller's translator; 0 = not priced. Read only by vgpu_analyze_plan_shape. */
 	double estimated_ops_per_row;

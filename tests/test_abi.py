@@ -199,3 +199,31 @@ def test_plan_shape_columns_size_and_execution_mode():
     plan.expressions[0].estimated_ops_per_row = 5.0
     again, _ = serialize_plan_memo(plan)
     assert again is not first and again.nodes[again.root].expressions[0].estimated_ops_per_row == 5.0
+
+
+def test_running_sum_window_expressions_are_refused_everywhere():
+    """A RUNNING_SUM window expression (GpuExpr::window_primitive) crosses the boundary intact and is
+    refused by execution with VGPU_ERR_UNSUPPORTED before any device work, and by the stream pipeline's
+    support check, so the caller runs it elsewhere instead of getting a plain projection's values. An
+    out-of-range primitive is a malformed plan. Routing helpers still read the plan."""
+    from vectisdb_b200.engine import (GpuValueType as T, GpuWindowPrimitive as W, StreamPipeline, _Keep,
+                                      estimate_columns_size, make_expr, make_projection, make_scan, serialize_plan)
+    lib = abi.lib()
+    e = make_expr("((double*)out)[idx] = ((const double*)inputs[0])[row];", ["x"], T.FLOAT64)
+    e.window_primitive = W.RUNNING_SUM
+    plan = make_projection([e], make_scan(["x"]))
+    keep = _Keep()
+    plan_c = serialize_plan(plan, keep)
+    assert plan_c.nodes[plan_c.root].expressions[0].window_primitive == 1
+    res = C.c_void_p()
+    assert lib.vgpu_execute_plan(C.byref(plan_c), None, 0, None, C.byref(res)) == abi.ERR_UNSUPPORTED
+    assert b"RUNNING_SUM" in lib.vgpu_last_error() and not res.value
+    assert not StreamPipeline.supports(plan)
+    e.window_primitive = W.NONE
+    assert StreamPipeline.supports(plan)
+    plan.children[0].estimated_rows = 10
+    assert estimate_columns_size(plan) == 80
+    plan_c = serialize_plan(plan, keep)
+    plan_c.nodes[plan_c.root].expressions[0].window_primitive = 7
+    assert lib.vgpu_execute_plan(C.byref(plan_c), None, 0, None, C.byref(res)) == abi.ERR_INVALID_ARGUMENT
+    assert b"window primitive" in lib.vgpu_last_error()

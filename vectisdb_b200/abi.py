@@ -24,7 +24,7 @@ EXEC_NO_SYNC = 1
 class vgpu_expr(C.Structure):
     _fields_ = [("source", C.c_char_p), ("input_columns", C.POINTER(C.c_char_p)),
                 ("n_input_columns", C.c_uint32), ("output_type", C.c_uint32),
-                ("estimated_ops_per_row", C.c_double)]
+                ("window_primitive", C.c_uint32), ("estimated_ops_per_row", C.c_double)]
 
 
 class vgpu_aggregate(C.Structure):

@@ -121,6 +121,7 @@ vgpu_status vgpu_execute_plan(const vgpu_plan *plan, const vgpu_column *inputs, 
 		*out = nullptr;
 		if (n_inputs > 0 && inputs == nullptr) Fail(VGPU_ERR_INVALID_ARGUMENT, "null inputs with nonzero count");
 		auto root = ConvertPlan(plan);
+		RefuseWindowPrimitives(*root);  // before anything touches the device
 		ExecOptions eo;
 		cudaStream_t stream = nullptr;
 		if (options) {

@@ -797,7 +797,7 @@ std::shared_ptr<PreparedBatch> PrepareBatch(const std::vector<std::shared_ptr<Pl
 	for (auto &plan : plans) {
 		PreparedPlan pp;
 		pp.plan = plan;
-		pp.scan = BatchShape(*plan);
+		pp.scan = HasWindowPrimitive(*plan) ? nullptr : BatchShape(*plan);  // one by one: refused there
 		if (pp.scan) {
 			pp.templ = TemplatePlan(*plan, pp.ptypes, pp.params);
 			std::ostringstream sig;

@@ -1566,6 +1566,7 @@ PipelineCodegen::GroupBySpec ValidateGroupBy(const PlanNode &node, const Pipelin
 
 ExecResult ExecutePlan(const PlanNode &plan, const std::vector<vgpu_column> &inputs, const ExecOptions &options,
                        cudaStream_t stream) {
+	RefuseWindowPrimitives(plan);
 	Runtime::Get().EnsureDevice();
 	Executor ex(inputs, options, stream, IsRowIndependent(plan));
 	Relation rel = ex.Exec(plan);

@@ -71,6 +71,10 @@ std::shared_ptr<PlanNode> ConvertPlan(const vgpu_plan *plan) {
 			expr.input_columns = Names(e.input_columns, e.n_input_columns, "expression inputs");
 			expr.output_type = static_cast<ValueType>(e.output_type);
 			expr.ops_per_row = e.estimated_ops_per_row;
+			if (e.window_primitive > VGPU_WINDOW_RUNNING_SUM) {
+				Fail(VGPU_ERR_INVALID_ARGUMENT, "plan: expression window primitive out of range");
+			}
+			expr.window = e.window_primitive;
 			node->expressions.push_back(std::move(expr));
 		}
 		node->build_keys = Names(src.build_keys, src.n_build_keys, "build_keys");
@@ -121,6 +125,22 @@ void CollectScans(const PlanNode &node, std::vector<const PlanNode *> &out) {
 
 // IsRowIndependent (cuda_engine/include/gpu_engine.hpp:239-248): SCAN/PROJECTION are row-wise and
 // FILTER only drops rows; every other operator combines rows and must see its input whole.
+bool HasWindowPrimitive(const PlanNode &node) {
+	for (auto &e : node.expressions) {
+		if (e.window != VGPU_WINDOW_NONE) return true;
+	}
+	for (auto &c : node.children) {
+		if (HasWindowPrimitive(*c)) return true;
+	}
+	return false;
+}
+
+void RefuseWindowPrimitives(const PlanNode &node) {
+	if (HasWindowPrimitive(node)) {
+		Fail(VGPU_ERR_UNSUPPORTED, "gpu_executor: RUNNING_SUM window expressions are not supported by this engine");
+	}
+}
+
 bool IsRowIndependent(const PlanNode &node) {
 	switch (node.op) {
 	case OpType::SCAN:

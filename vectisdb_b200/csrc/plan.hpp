@@ -33,6 +33,7 @@ struct Expr {
 	std::vector<std::string> input_columns;
 	ValueType output_type = ValueType::FLOAT64;
 	double ops_per_row = 0.0;  // caller's price of one row (routing only); 0 = not priced
+	uint32_t window = VGPU_WINDOW_NONE;  // vgpu_window_primitive
 };
 
 struct Aggregate {
@@ -74,5 +75,12 @@ std::shared_ptr<PlanNode> ConvertPlan(const vgpu_plan *plan);
 void CollectScans(const PlanNode &node, std::vector<const PlanNode *> &out);
 
 bool IsRowIndependent(const PlanNode &node);
+
+//! True when an expression anywhere in the plan carries a window primitive (RUNNING_SUM).
+bool HasWindowPrimitive(const PlanNode &node);
+
+//! Fails with VGPU_ERR_UNSUPPORTED when the plan carries a window primitive: no execution path of this
+//! engine computes running totals across calls, and running one as a plain expression would be wrong.
+void RefuseWindowPrimitives(const PlanNode &node);
 
 } // namespace vgpu

@@ -37,6 +37,7 @@ bool StreamPipeline::Supports(const PlanNode &plan) {
 		std::vector<std::string> names;
 		for (size_t i = 0; i < (*it)->expressions.size(); i++) {
 			const auto &e = (*it)->expressions[i];
+			if (e.window != VGPU_WINDOW_NONE) return false;  // running totals are not computed here
 			for (auto &in : e.input_columns) {
 				if (std::find(below.begin(), below.end(), in) == below.end()) return false;
 			}

@@ -41,6 +41,11 @@ class GpuValueType(enum.IntEnum):  # gpu_engine.hpp:29-38
     HUGEINT = 7
 
 
+class GpuWindowPrimitive(enum.IntEnum):  # gpu_engine.hpp:48-51
+    NONE = 0
+    RUNNING_SUM = 1  # carried; every execution path refuses it (VGPU_ERR_UNSUPPORTED)
+
+
 class GpuExecutionMode(enum.IntEnum):  # gpu_engine.hpp:23-27
     PIPELINE_STREAM_CACHED = 0
     PIPELINE_STREAM_UNCACHED = 1
@@ -88,6 +93,7 @@ class GpuExpr:  # gpu_engine.hpp:56-80
     output_type: GpuValueType = GpuValueType.FLOAT64
     source_hash: str = ""
     estimated_ops_per_row: float = 0.0  # the translator's price of one row (routing only); 0 = not priced
+    window_primitive: GpuWindowPrimitive = GpuWindowPrimitive.NONE
 
 
 @dataclass
@@ -246,6 +252,7 @@ def serialize_plan(plan: GpuPlanNode, keep: _Keep) -> abi.vgpu_plan:
                 exprs[j].input_columns, exprs[j].n_input_columns = keep.names(e.input_columns)
                 exprs[j].output_type = int(e.output_type)
                 exprs[j].estimated_ops_per_row = float(e.estimated_ops_per_row)
+                exprs[j].window_primitive = int(e.window_primitive)
             keep.refs.append(exprs)
             n.expressions = C.cast(exprs, C.POINTER(abi.vgpu_expr))
         n.n_expressions = len(node.expressions)
@@ -275,8 +282,8 @@ def serialize_plan(plan: GpuPlanNode, keep: _Keep) -> abi.vgpu_plan:
 def _plan_snapshot(node: GpuPlanNode) -> tuple:
     """Every field serialize_plan reads, as nested tuples (equal snapshots serialize identically)."""
     return (int(node.op_type), node.table.catalog, node.table.schema, node.table.table, tuple(node.column_names),
-            tuple((e.generated_cuda_source, tuple(e.input_columns), int(e.output_type), float(e.estimated_ops_per_row))
-                  for e in node.expressions),
+            tuple((e.generated_cuda_source, tuple(e.input_columns), int(e.output_type), float(e.estimated_ops_per_row),
+                   int(e.window_primitive)) for e in node.expressions),
             tuple(node.build_keys), tuple(node.probe_keys), tuple(node.output_columns), tuple(node.group_keys),
             tuple((int(a.kind), int(a.output_type), a.input_column) for a in node.aggregates),
             node.estimated_rows, node.estimated_row_width_bytes, tuple(_plan_snapshot(c) for c in node.children))
