@@ -143,6 +143,10 @@ typedef struct vgpu_plan_node {
 	/* cost-model inputs (advisory) */
 	uint64_t estimated_rows;
 	uint32_t estimated_row_width_bytes;
+	/* GROUP_BY_AGGREGATE: GpuPlanNode::aggregate_exprs (gpu_engine.hpp:181), one human-readable
+	 * descriptor per aggregate, or none; any other count is a malformed plan (gpu_groupby.cu:311-312). */
+	const char *const *aggregate_exprs;
+	uint32_t n_aggregate_exprs;
 } vgpu_plan_node;
 
 typedef struct vgpu_plan {

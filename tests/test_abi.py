@@ -227,3 +227,24 @@ def test_running_sum_window_expressions_are_refused_everywhere():
     plan_c.nodes[plan_c.root].expressions[0].window_primitive = 7
     assert lib.vgpu_execute_plan(C.byref(plan_c), None, 0, None, C.byref(res)) == abi.ERR_INVALID_ARGUMENT
     assert b"window primitive" in lib.vgpu_last_error()
+
+
+def test_aggregate_descriptors_cross_the_boundary_and_are_checked():
+    """GpuPlanNode::aggregate_exprs: none, or one descriptor per aggregate (the reference's group-by
+    refuses any other count); the descriptors are carried, never executed."""
+    from vectisdb_b200.engine import (GpuAggregateKind as A, GpuValueType as T, _Keep, estimate_working_set,
+                                      make_aggregate, make_group_by, make_scan, serialize_plan)
+    lib = abi.lib()
+    gb = make_group_by(["k"], [make_aggregate(A.COUNT_STAR, "", T.INT64), make_aggregate(A.SUM, "v", T.FLOAT64)],
+                       make_scan(["k", "v"]))
+    estimate_working_set(gb)  # no descriptors: fine
+    gb.aggregate_exprs = ["count_star()", "sum(v)"]
+    keep = _Keep()
+    plan_c = serialize_plan(gb, keep)
+    node = plan_c.nodes[plan_c.root]
+    assert node.n_aggregate_exprs == 2 and node.aggregate_exprs[1] == b"sum(v)"
+    estimate_working_set(gb)  # one per aggregate: fine
+    gb.aggregate_exprs = ["count_star()"]
+    res = C.c_void_p()
+    assert lib.vgpu_execute_plan(C.byref(serialize_plan(gb, keep)), None, 0, None, C.byref(res)) == abi.ERR_INVALID_ARGUMENT
+    assert b"disagree in length" in lib.vgpu_last_error()

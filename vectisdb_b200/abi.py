@@ -43,6 +43,7 @@ class vgpu_plan_node(C.Structure):
         ("group_keys", C.POINTER(C.c_char_p)), ("n_group_keys", C.c_uint32),
         ("aggregates", C.POINTER(vgpu_aggregate)), ("n_aggregates", C.c_uint32),
         ("estimated_rows", C.c_uint64), ("estimated_row_width_bytes", C.c_uint32),
+        ("aggregate_exprs", C.POINTER(C.c_char_p)), ("n_aggregate_exprs", C.c_uint32),
     ]
 
 

@@ -95,6 +95,10 @@ std::shared_ptr<PlanNode> ConvertPlan(const vgpu_plan *plan) {
 			agg.input_column = Str(a.input_column);
 			node->aggregates.push_back(std::move(agg));
 		}
+		node->aggregate_exprs = Names(src.aggregate_exprs, src.n_aggregate_exprs, "aggregate_exprs");
+		if (!node->aggregate_exprs.empty() && node->aggregate_exprs.size() != node->aggregates.size()) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_groupby: aggregates and aggregate_exprs disagree in length");
+		}
 		node->estimated_rows = src.estimated_rows;
 		node->estimated_row_width_bytes = src.estimated_row_width_bytes;
 		if (src.n_children > 0 && src.children == nullptr) {

@@ -63,6 +63,7 @@ struct PlanNode {
 	std::vector<std::string> output_columns;
 	std::vector<std::string> group_keys;
 	std::vector<Aggregate> aggregates;
+	std::vector<std::string> aggregate_exprs;  // descriptors only: never executed
 	uint64_t estimated_rows = 0;
 	uint32_t estimated_row_width_bytes = 0;
 };

@@ -269,6 +269,7 @@ def serialize_plan(plan: GpuPlanNode, keep: _Keep) -> abi.vgpu_plan:
             keep.refs.append(aggs)
             n.aggregates = C.cast(aggs, C.POINTER(abi.vgpu_aggregate))
         n.n_aggregates = len(node.aggregates)
+        n.aggregate_exprs, n.n_aggregate_exprs = keep.names(node.aggregate_exprs)
         n.estimated_rows = node.estimated_rows
         n.estimated_row_width_bytes = node.estimated_row_width_bytes
     keep.refs.append(nodes)
@@ -285,7 +286,7 @@ def _plan_snapshot(node: GpuPlanNode) -> tuple:
             tuple((e.generated_cuda_source, tuple(e.input_columns), int(e.output_type), float(e.estimated_ops_per_row),
                    int(e.window_primitive)) for e in node.expressions),
             tuple(node.build_keys), tuple(node.probe_keys), tuple(node.output_columns), tuple(node.group_keys),
-            tuple((int(a.kind), int(a.output_type), a.input_column) for a in node.aggregates),
+            tuple((int(a.kind), int(a.output_type), a.input_column) for a in node.aggregates), tuple(node.aggregate_exprs),
             node.estimated_rows, node.estimated_row_width_bytes, tuple(_plan_snapshot(c) for c in node.children))
 
 
