@@ -95,9 +95,9 @@ typedef struct vgpu_expr {
 	uint32_t n_input_columns;
 	uint32_t output_type; /* vgpu_value_type */
 	/* GpuExpr::window_primitive (gpu_engine.hpp:48-51, 67): vgpu_window_primitive. RUNNING_SUM asks for
-	 * the running total of the expression across every row streamed so far; it is carried so that a
-	 * caller's plan never loses it, and every execution path of this engine refuses it with
-	 * VGPU_ERR_UNSUPPORTED (vgpu_pipeline_supports answers 0), so the caller runs it elsewhere. */
+	 * the running total of the expression across every row streamed so far. The stream pipeline computes
+	 * it for top-level INT16/INT32/INT64/FLOAT32/FLOAT64 outputs of batches without NULLs (integers wrap
+	 * in their width); vgpu_execute_plan, batches and serving refuse it with VGPU_ERR_UNSUPPORTED. */
 	uint32_t window_primitive;
 	/* GpuExpr::estimated_ops_per_row (gpu_engine.hpp:79): weighted operations per row, priced by the
 	 * caller's translator; 0 = not priced. Read only by vgpu_analyze_plan_shape. */

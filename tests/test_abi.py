@@ -201,10 +201,10 @@ def test_plan_shape_columns_size_and_execution_mode():
     assert again is not first and again.nodes[again.root].expressions[0].estimated_ops_per_row == 5.0
 
 
-def test_running_sum_window_expressions_are_refused_everywhere():
-    """A RUNNING_SUM window expression (GpuExpr::window_primitive) crosses the boundary intact and is
-    refused by execution with VGPU_ERR_UNSUPPORTED before any device work, and by the stream pipeline's
-    support check, so the caller runs it elsewhere instead of getting a plain projection's values. An
+def test_running_sum_window_expressions_reach_only_the_stream_pipeline():
+    """A RUNNING_SUM window expression (GpuExpr::window_primitive) crosses the boundary intact. The
+    stream pipeline takes it on top-level numeric outputs only; plain execution refuses it with
+    VGPU_ERR_UNSUPPORTED before any device work, instead of returning a plain projection's values. An
     out-of-range primitive is a malformed plan. Routing helpers still read the plan."""
     from vectisdb_b200.engine import (GpuValueType as T, GpuWindowPrimitive as W, StreamPipeline, _Keep,
                                       estimate_columns_size, make_expr, make_projection, make_scan, serialize_plan)
@@ -218,9 +218,13 @@ def test_running_sum_window_expressions_are_refused_everywhere():
     res = C.c_void_p()
     assert lib.vgpu_execute_plan(C.byref(plan_c), None, 0, None, C.byref(res)) == abi.ERR_UNSUPPORTED
     assert b"RUNNING_SUM" in lib.vgpu_last_error() and not res.value
-    assert not StreamPipeline.supports(plan)
-    e.window_primitive = W.NONE
-    assert StreamPipeline.supports(plan)
+    assert StreamPipeline.supports(plan)  # top level, DOUBLE
+    above = make_projection([make_expr("((double*)out)[idx] = ((const double*)inputs[0])[row];", ["col0"], T.FLOAT64)],
+                            plan)
+    assert not StreamPipeline.supports(above)  # a running total below the top level
+    b = make_expr("((bool*)out)[idx] = ((const double*)inputs[0])[row] > 0;", ["x"], T.BOOLEAN)
+    b.window_primitive = W.RUNNING_SUM
+    assert not StreamPipeline.supports(make_projection([b], make_scan(["x"])))  # not a numeric output
     plan.children[0].estimated_rows = 10
     assert estimate_columns_size(plan) == 80
     plan_c = serialize_plan(plan, keep)

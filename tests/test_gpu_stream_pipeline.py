@@ -84,3 +84,51 @@ def test_nulls_propagate_and_unsupported_shapes_refused():
     assert not StreamPipeline.supports(filt)
     with pytest.raises(Exception):
         StreamPipeline(filt, ["a", "b"], [T.INT64, T.INT64], 1024)
+
+
+def test_running_sum_continues_across_batches():
+    """RUNNING_SUM (the reference pipeline's window primitive, gpu_stream_pipeline.cu:133-166, 700-704):
+    each value of a window column is that column's total over every row submitted so far, across batches
+    of uneven sizes (one row, just below and above the 4096-row tile, several tiles). INT16 wraps in its
+    width; the FLOAT64 inputs are multiples of 1/512 whose partial sums stay exact, so every column
+    compares bit for bit. A batch with NULLs under a window column is refused and leaves the total as it
+    was."""
+    from vectisdb_b200.engine import GpuWindowPrimitive as W
+    rng = np.random.default_rng(7)
+    exprs = [make_expr("((long long*)out)[idx] = ((const long long*)inputs[0])[row];", ["a"], T.INT64),
+             make_expr("((double*)out)[idx] = ((const double*)inputs[0])[row] * 2.0;", ["x"], T.FLOAT64),
+             make_expr("((short*)out)[idx] = ((const short*)inputs[0])[row];", ["s"], T.INT16),
+             make_expr("((long long*)out)[idx] = ((const long long*)inputs[0])[row];", ["a"], T.INT64)]
+    for e in exprs[:3]:
+        e.window_primitive = W.RUNNING_SUM
+    plan = make_projection(exprs, make_scan(["a", "x", "s"]))
+    assert StreamPipeline.supports(plan)
+    p = StreamPipeline(plan, ["a", "x", "s"], [T.INT64, T.FLOAT64, T.INT16], max_rows_per_batch=20000, depth=3)
+    sizes = [20000, 1, 4095, 4096, 4097, 12345, 1, 777]
+    batches = [(rng.integers(-(1 << 40), 1 << 40, n), rng.integers(0, 1 << 20, n) / 1024.0,
+                rng.integers(-32768, 32768, n).astype(np.int16)) for n in sizes]
+    got = []
+    for i, (a, x, s) in enumerate(batches):
+        while not p.can_submit():
+            got.append(p.take_blocking())
+        if i == 5:  # a NULL under a window column: refused before it takes a stage
+            with pytest.raises(Exception, match="RUNNING_SUM"):
+                p.submit([make_column("a", T.INT64, a, np.arange(len(a)) != 3), make_column("x", T.FLOAT64, x),
+                          make_column("s", T.INT16, s)])
+        p.submit([make_column("a", T.INT64, a), make_column("x", T.FLOAT64, x), make_column("s", T.INT16, s)])
+    while True:
+        r = p.take_blocking()
+        if r is None:
+            break
+        got.append(r)
+    assert len(got) == len(batches)
+    a_all = np.concatenate([b[0] for b in batches])
+    x_all = np.concatenate([b[1] for b in batches])
+    s_all = np.concatenate([b[2] for b in batches])
+    want = [np.cumsum(a_all), np.cumsum(x_all * 2.0), np.cumsum(s_all.astype(np.int64)).astype(np.int16), a_all]
+    at = 0
+    for (a, _, _), cols in zip(batches, got):
+        n = len(a)
+        for c, w in zip(cols, want):
+            assert c.data.dtype == w.dtype and np.array_equal(c.data, w[at:at + n]), (c.name, at, n)
+        at += n

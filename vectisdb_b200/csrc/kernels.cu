@@ -1,6 +1,8 @@
 // kernels.cu -- precompiled device primitives (see kernels.hpp).
 #include "kernels.hpp"
 
+#include <type_traits>
+
 #include <utility>
 
 #include "device_lib.cuh"
@@ -926,6 +928,158 @@ void JoinExpand(const uint64_t *offsets, const uint64_t *lower, uint64_t n_left,
 	JoinExpandKernel<<<GridFor(total, 256), 256, 0, stream>>>(offsets, lower, n_left, sorted_perm, total, out_left,
 	                                                          out_right);
 	VGPU_CUDA(cudaGetLastError());
+}
+
+// ---- running total (the stream pipeline's RUNNING_SUM window primitive) ----------------------------
+//
+// Three passes over tiles of 4096 values (1024 threads x 4 consecutive values): each tile's total; one
+// block turning the totals into per-tile starting values that continue from the carried state; each
+// tile's inclusive scan from its starting value. Integer values are summed as unsigned words of at
+// least their width (wrap-around, truncated on store), floats in their own type.
+
+namespace {
+
+constexpr int kSumThreads = 1024;
+constexpr int kSumItems = 4;
+constexpr uint64_t kSumTile = uint64_t(kSumThreads) * kSumItems;
+
+template <class T, class A> __device__ __forceinline__ A SumLoad(const T *p) {
+	if constexpr (sizeof(T) == 2) {
+		return static_cast<A>(static_cast<uint16_t>(*p));
+	} else if constexpr (std::is_integral<T>::value) {
+		return static_cast<A>(*p);
+	} else {
+		return *p;
+	}
+}
+
+template <class T, class A> __device__ __forceinline__ void SumStore(T *p, A v) {
+	*p = static_cast<T>(v);
+}
+
+// Block-wide scan of one value per thread (1024 threads): inclusive and exclusive prefixes and the
+// block total, all in the same addition order.
+template <class A> __device__ void SumBlockScan(A x, A *warp_sums, A &incl, A &excl, A &total) {
+	const int lane = threadIdx.x & 31;
+	const int warp = threadIdx.x >> 5;
+	for (int d = 1; d < 32; d <<= 1) {
+		const A y = __shfl_up_sync(0xffffffffu, x, d);
+		if (lane >= d) x = static_cast<A>(x + y);
+	}
+	A prev = __shfl_up_sync(0xffffffffu, x, 1);
+	if (lane == 31) warp_sums[warp] = x;
+	__syncthreads();
+	if (warp == 0) {
+		A w = warp_sums[lane];
+		for (int d = 1; d < 32; d <<= 1) {
+			const A y = __shfl_up_sync(0xffffffffu, w, d);
+			if (lane >= d) w = static_cast<A>(w + y);
+		}
+		warp_sums[lane] = w;
+	}
+	__syncthreads();
+	if (warp == 0) {
+		incl = x;
+		excl = lane == 0 ? A(0) : prev;
+	} else {
+		const A before = warp_sums[warp - 1];
+		incl = static_cast<A>(before + x);
+		excl = lane == 0 ? before : static_cast<A>(before + prev);
+	}
+	total = warp_sums[31];
+	__syncthreads();  // warp_sums is rewritten by the next call
+}
+
+template <class T, class A>
+__global__ void __launch_bounds__(kSumThreads) SumTileTotalsKernel(const T *data, uint64_t rows, A *totals) {
+	__shared__ A warp_sums[32];
+	const uint64_t base = blockIdx.x * kSumTile + uint64_t(threadIdx.x) * kSumItems;
+	A s = A(0);
+	for (int j = 0; j < kSumItems; j++) {
+		if (base + j < rows) s = static_cast<A>(s + SumLoad<T, A>(data + base + j));
+	}
+	A incl, excl, total;
+	SumBlockScan(s, warp_sums, incl, excl, total);
+	if (threadIdx.x == 0) totals[blockIdx.x] = total;
+}
+
+// One block: totals[i] becomes the value before tile i (the carried state plus the tiles before it).
+template <class T, class A>
+__global__ void __launch_bounds__(kSumThreads) SumTileStartsKernel(A *totals, uint64_t tiles, const T *state) {
+	__shared__ A warp_sums[32];
+	A carry = SumLoad<T, A>(state);
+	for (uint64_t c = 0; c < tiles; c += kSumThreads) {
+		const uint64_t i = c + threadIdx.x;
+		const A x = i < tiles ? totals[i] : A(0);
+		A incl, excl, chunk;
+		SumBlockScan(x, warp_sums, incl, excl, chunk);
+		if (i < tiles) totals[i] = static_cast<A>(carry + excl);
+		carry = static_cast<A>(carry + chunk);
+	}
+}
+
+template <class T, class A>
+__global__ void __launch_bounds__(kSumThreads) SumTileScanKernel(T *data, uint64_t rows, const A *starts, T *state) {
+	__shared__ A warp_sums[32];
+	const uint64_t base = blockIdx.x * kSumTile + uint64_t(threadIdx.x) * kSumItems;
+	A v[kSumItems];
+	A s = A(0);
+	for (int j = 0; j < kSumItems; j++) {
+		v[j] = base + j < rows ? SumLoad<T, A>(data + base + j) : A(0);
+		s = static_cast<A>(s + v[j]);
+	}
+	A incl, excl, total;
+	SumBlockScan(s, warp_sums, incl, excl, total);
+	A run = static_cast<A>(starts[blockIdx.x] + excl);
+	for (int j = 0; j < kSumItems; j++) {
+		run = static_cast<A>(run + v[j]);
+		if (base + j < rows) {
+			SumStore<T, A>(data + base + j, run);
+			if (base + j == rows - 1) SumStore<T, A>(state, run);
+		}
+	}
+}
+
+template <class T, class A> void RunningSumTyped(void *data, uint64_t rows, void *state, void *scratch, cudaStream_t stream) {
+	const uint64_t tiles = (rows + kSumTile - 1) / kSumTile;
+	T *d = static_cast<T *>(data);
+	T *st = static_cast<T *>(state);
+	A *sums = static_cast<A *>(scratch);
+	SumTileTotalsKernel<T, A><<<static_cast<unsigned>(tiles), kSumThreads, 0, stream>>>(d, rows, sums);
+	SumTileStartsKernel<T, A><<<1, kSumThreads, 0, stream>>>(sums, tiles, st);
+	SumTileScanKernel<T, A><<<static_cast<unsigned>(tiles), kSumThreads, 0, stream>>>(d, rows, sums, st);
+	VGPU_CUDA(cudaGetLastError());
+}
+
+} // namespace
+
+size_t RunningSumScratchBytes(uint64_t rows) {
+	return static_cast<size_t>((rows + kSumTile - 1) / kSumTile) * sizeof(uint64_t) + 16;
+}
+
+void RunningSum(void *data, ValueType t, uint64_t rows, void *state, void *scratch, cudaStream_t stream) {
+	if (rows == 0) return;
+	if (rows >= (1ull << 32)) Fail(VGPU_ERR_INVALID_ARGUMENT, "running sum: at most 2^32 - 1 rows per call");
+	LaunchScope scope("vgpu_running_sum", stream, 2 * rows * TypeSize(t) + rows * TypeSize(t), rows);
+	switch (t) {
+	case ValueType::INT16:
+		RunningSumTyped<int16_t, uint32_t>(data, rows, state, scratch, stream);
+		break;
+	case ValueType::INT32:
+		RunningSumTyped<int32_t, uint32_t>(data, rows, state, scratch, stream);
+		break;
+	case ValueType::INT64:
+		RunningSumTyped<int64_t, uint64_t>(data, rows, state, scratch, stream);
+		break;
+	case ValueType::FLOAT32:
+		RunningSumTyped<float, float>(data, rows, state, scratch, stream);
+		break;
+	case ValueType::FLOAT64:
+		RunningSumTyped<double, double>(data, rows, state, scratch, stream);
+		break;
+	default:
+		Fail(VGPU_ERR_UNSUPPORTED, std::string("running sum: unsupported type ") + TypeName(t));
+	}
 }
 
 } // namespace kern

@@ -15,6 +15,13 @@ namespace kern {
 void ExclusiveScanU32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *total, Arena &arena);
 void ExclusiveScanU64(const uint64_t *in, uint64_t *out, uint64_t n, uint64_t *total, Arena &arena);
 
+//! Running total in place: data[i] = *state + data[0] + ... + data[i] for `rows` values of type `t`
+//! (INT16/INT32/INT64 wrapping in their width, FLOAT32/FLOAT64 in their own precision), then
+//! *state = data[rows - 1] (device scalar of type `t`), so consecutive calls continue one total.
+//! `scratch` holds RunningSumScratchBytes(rows) bytes. Three launches, no host synchronization.
+size_t RunningSumScratchBytes(uint64_t rows);
+void RunningSum(void *data, ValueType t, uint64_t rows, void *state, void *scratch, cudaStream_t stream);
+
 //! Arrow LSB-first bitmap <-> one byte per row.
 void UnpackValidity(const uint8_t *bitmap, uint8_t *bytes, uint64_t n, cudaStream_t stream);
 void PackValidity(const uint8_t *bytes, uint8_t *bitmap, uint64_t n, cudaStream_t stream);

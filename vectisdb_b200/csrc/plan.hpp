@@ -80,8 +80,8 @@ bool IsRowIndependent(const PlanNode &node);
 //! True when an expression anywhere in the plan carries a window primitive (RUNNING_SUM).
 bool HasWindowPrimitive(const PlanNode &node);
 
-//! Fails with VGPU_ERR_UNSUPPORTED when the plan carries a window primitive: no execution path of this
-//! engine computes running totals across calls, and running one as a plain expression would be wrong.
+//! Fails with VGPU_ERR_UNSUPPORTED when the plan carries a window primitive: only the stream pipeline
+//! keeps a running total across calls, and running one as a plain expression would be wrong.
 void RefuseWindowPrimitives(const PlanNode &node);
 
 } // namespace vgpu

@@ -35,9 +35,17 @@ bool StreamPipeline::Supports(const PlanNode &plan) {
 	std::vector<std::string> below = scan->column_names;
 	for (auto it = chain.rbegin(); it != chain.rend(); ++it) {
 		std::vector<std::string> names;
+		const bool top = *it == chain.front();
 		for (size_t i = 0; i < (*it)->expressions.size(); i++) {
 			const auto &e = (*it)->expressions[i];
-			if (e.window != VGPU_WINDOW_NONE) return false;  // running totals are not computed here
+			// RUNNING_SUM: a running total of a numeric output column (the chain runs fused, so only the
+			// top level's outputs are materialized to scan).
+			if (e.window != VGPU_WINDOW_NONE) {
+				if (!top || e.output_type == ValueType::BOOLEAN || e.output_type == ValueType::DICTIONARY_STRING ||
+				    e.output_type == ValueType::HUGEINT) {
+					return false;
+				}
+			}
 			for (auto &in : e.input_columns) {
 				if (std::find(below.begin(), below.end(), in) == below.end()) return false;
 			}
@@ -79,7 +87,10 @@ StreamPipeline::StreamPipeline(std::shared_ptr<PlanNode> plan, const std::vector
 	Runtime::Get().EnsureDevice();
 	const Variant &v0 = GetVariant(0);  // compile (or fetch) the no-NULL kernel now: fail here, not mid-scan
 	(void)v0;
-	for (auto &e : chain.front()->expressions) out_types_.push_back(e.output_type);
+	for (auto &e : chain.front()->expressions) {
+		if (e.window != VGPU_WINDOW_NONE) window_cols_.push_back(out_types_.size());
+		out_types_.push_back(e.output_type);
+	}
 	for (size_t i = 0; i < out_types_.size(); i++) out_names_.push_back("col" + std::to_string(i));
 	for (cudaStream_t *s : {&s_h2d_, &s_exec_, &s_d2h_}) VGPU_CUDA(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking));
 	auto &al = Runtime::Get().allocator();
@@ -114,6 +125,15 @@ StreamPipeline::StreamPipeline(std::shared_ptr<PlanNode> plan, const std::vector
 		for (cudaEvent_t *e : {&st.h2d, &st.exec, &st.d2h}) VGPU_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
 	}
 	for (size_t i = 0; i < stages_.size(); i++) free_.push_back(static_cast<int>(i));
+	if (!window_cols_.empty()) {
+		// one running state per RUNNING_SUM column, starting at zero; one scratch (batches run in order
+		// on the compute stream, so they share it)
+		for (size_t c : window_cols_) {
+			running_state_.push_back(dev(TypeSize(out_types_[c])));
+			VGPU_CUDA(cudaMemsetAsync(running_state_.back(), 0, TypeSize(out_types_[c]), s_exec_));
+		}
+		running_scratch_ = dev(kern::RunningSumScratchBytes(max_rows_));
+	}
 	VGPU_CUDA(cudaStreamSynchronize(s_exec_));
 }
 
@@ -196,6 +216,11 @@ void StreamPipeline::Submit(const std::vector<vgpu_column> &cols, uint64_t rows)
 		if (c.validity) mask |= 1ull << i;
 	}
 	const Variant &v = GetVariant(mask);
+	for (size_t c : window_cols_) {
+		if (v.out_nullable[c]) {
+			Fail(VGPU_ERR_UNSUPPORTED, "gpu_stream_pipeline: RUNNING_SUM over a batch with NULL inputs is not supported");
+		}
+	}
 	const int s = free_.front();
 	free_.pop_front();
 	Stage &st = stages_[s];
@@ -240,6 +265,10 @@ void StreamPipeline::Submit(const std::vector<vgpu_column> &cols, uint64_t rows)
 			LaunchScope scope("vgpu_mat_write", s_exec_, 0, rows);
 			void *params[] = {w};
 			Runtime::Get().LaunchModuleKernel(v.module->Get("vgpu_mat_write"), dim3(grid), dim3(kBlock), 0, s_exec_, params);
+		}
+		for (size_t k = 0; k < window_cols_.size(); k++) {
+			const size_t c = window_cols_[k];
+			kern::RunningSum(st.out_dev[c], out_types_[c], rows, running_state_[k], running_scratch_, s_exec_);
 		}
 		for (size_t c = 0; c < out_types_.size(); c++) {
 			if (v.out_nullable[c]) kern::PackValidity(static_cast<uint8_t *>(st.out_valid_dev[c]),

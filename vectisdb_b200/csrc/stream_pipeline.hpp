@@ -9,6 +9,10 @@
 // pipeline's own pinned buffers, so the caller's buffers are free again when Submit returns; NULLs
 // are handled (byte masks on the device, Arrow bitmaps at both ends). Every buffer is allocated at
 // construction (depth + 1 stage sets: one more than in flight, for the result the consumer holds).
+// A top-level expression marked RUNNING_SUM (the reference's window primitive,
+// gpu_stream_pipeline.cu:133-166, 700-704) leaves the running total of its values over every batch
+// submitted so far: each batch is scanned on the compute stream after the fused kernel, continuing from
+// a state kept on the device (integers wrap in their width, floats add in their own precision).
 // Externally serialized: one call at a time.
 #pragma once
 
@@ -27,7 +31,8 @@ namespace vgpu {
 class StreamPipeline {
 public:
 	//! PROJECTION+ over a SCAN, every level with at least one expression whose inputs resolve against
-	//! the level below, fixed-width output types.
+	//! the level below, fixed-width output types; RUNNING_SUM only on top-level INT16/INT32/INT64/
+	//! FLOAT32/FLOAT64 outputs (a batch whose window column would carry NULLs is refused at Submit).
 	static bool Supports(const PlanNode &plan);
 
 	StreamPipeline(std::shared_ptr<PlanNode> plan, const std::vector<std::string> &input_names,
@@ -92,6 +97,9 @@ private:
 	std::deque<int> free_, fifo_;
 	cudaStream_t s_h2d_ = nullptr, s_exec_ = nullptr, s_d2h_ = nullptr;
 	std::vector<void *> device_owned_, host_owned_;
+	std::vector<size_t> window_cols_;      // output columns carrying RUNNING_SUM
+	std::vector<void *> running_state_;    // per window column: the total so far (device, its type)
+	void *running_scratch_ = nullptr;      // per-tile totals of the batch being scanned
 };
 
 } // namespace vgpu

@@ -43,7 +43,7 @@ class GpuValueType(enum.IntEnum):  # gpu_engine.hpp:29-38
 
 class GpuWindowPrimitive(enum.IntEnum):  # gpu_engine.hpp:48-51
     NONE = 0
-    RUNNING_SUM = 1  # carried; every execution path refuses it (VGPU_ERR_UNSUPPORTED)
+    RUNNING_SUM = 1  # the stream pipeline's running total; other execution paths refuse it
 
 
 class GpuExecutionMode(enum.IntEnum):  # gpu_engine.hpp:23-27
