@@ -169,3 +169,23 @@ def test_repartition_merge_of_high_cardinality_groups():
     assert np.array_equal(sv["lower"], eaggs[1][1]["lower"]) and np.array_equal(sv["upper"], eaggs[1][1]["upper"])
     for got, (_, exp) in zip(rest, eaggs[2:]):
         assert np.array_equal(got, exp)
+
+
+def test_i128_to_f64_rounds_like_python_ints():
+    """The AVG finish's 128-bit -> double conversion is the nearest double, ties to even, like Python's
+    int -> float: values at the int64 edges, ties above 2^53 and values far outside 64 bits."""
+    sys.path.insert(0, ROOT)
+    from vectisdb_b200.distributed import HUGEINT, _i128_to_f64
+    rng = np.random.default_rng(11)
+    vals = [0, 1, -1, (1 << 53) + 1, (1 << 53) + 3, -(1 << 53) - 1, (1 << 63) - 1, -(1 << 63), 1 << 63, -(1 << 63) - 1,
+            (1 << 64) + 2048, (1 << 100) + (1 << 47), -(1 << 127), (1 << 127) - 1]
+    vals += [int(x) for x in rng.integers(-(1 << 62), 1 << 62, 200)]
+    vals += [int(x) * (1 << 40) + int(y) for x, y in zip(rng.integers(-(1 << 60), 1 << 60, 200),
+                                                        rng.integers(0, 1 << 40, 200))]
+    arr = np.zeros(len(vals), HUGEINT)
+    for i, v in enumerate(vals):
+        arr[i]["lower"] = v & ((1 << 64) - 1)
+        u = (v >> 64) & ((1 << 64) - 1)
+        arr[i]["upper"] = u - (1 << 64) if u >= 1 << 63 else u
+    got = _i128_to_f64(arr)
+    assert [float(v) for v in vals] == got.tolist()

@@ -145,6 +145,18 @@ def _i128_from_chunks(chunk_sums: list[np.ndarray]) -> np.ndarray:
     return out
 
 
+def _i128_to_f64(values: np.ndarray) -> np.ndarray:
+    """128-bit integers ({lower, upper}) to the nearest doubles (ties to even): values inside int64
+    through numpy's int64 -> float64 conversion, which rounds that way; the rest through Python ints."""
+    lower = values["lower"].astype(np.uint64)
+    upper = values["upper"].astype(np.int64)
+    small = ((upper == 0) & (lower < np.uint64(1 << 63))) | ((upper == -1) & (lower >= np.uint64(1 << 63)))
+    out = lower.view(np.int64).astype(np.float64)
+    for i in np.flatnonzero(~small).tolist():
+        out[i] = float((int(upper[i]) << 64) | int(lower[i]))
+    return out
+
+
 def repartition_merge_groupby(keys: np.ndarray, aggregates: Sequence[tuple[str, np.ndarray]],
                               device: str = "cpu") -> tuple[np.ndarray, list[np.ndarray]]:
     """Merges partial groups of a key space too large to index (the high-cardinality shape): every
@@ -175,34 +187,35 @@ def repartition_merge_groupby(keys: np.ndarray, aggregates: Sequence[tuple[str, 
             layout.append((kind, len(columns), 1))
             columns.append(values.astype(np.float64 if kind == "sum_f64" else np.int64))
     got, _ = _exchange(columns, send, device)
-    rkeys = got[0]
-    ukeys, pos = np.unique(rkeys, return_inverse=True)
-    g = ukeys.shape[0]
+    # Group the received partials by key: a stable sort, then one reduceat per column over each run of
+    # equal keys (exact for the int64 words; FP64 sums add in arrival order within a group).
+    order = np.argsort(got[0], kind="stable")
+    rkeys = got[0][order]
+    if rkeys.shape[0] == 0:
+        starts = np.zeros(0, np.int64)
+    else:
+        starts = np.flatnonzero(np.concatenate(([True], rkeys[1:] != rkeys[:-1])))
+    ukeys = rkeys[starts]
+
+    def reduce(ufunc, col):
+        col = col[order]
+        return ufunc.reduceat(col, starts) if starts.shape[0] else col[:0]
+
     merged = []
     for kind, first, _n in layout:
         col = got[first]
-        if kind == "sum_f64":
-            acc = np.zeros(g, np.float64)
-            np.add.at(acc, pos, col)
-        elif kind == "count":
-            acc = np.zeros(g, np.int64)
-            np.add.at(acc, pos, col)
+        if kind in ("sum_f64", "count"):
+            acc = reduce(np.add, col)
         elif kind in ("min", "max"):
-            info = np.iinfo(np.int64)
-            acc = np.full(g, info.max if kind == "min" else info.min, np.int64)
-            (np.minimum if kind == "min" else np.maximum).at(acc, pos, col)
+            acc = reduce(np.minimum if kind == "min" else np.maximum, col)
         else:
             lower = col.view(np.uint64)
             upper = got[first + 1]
             mask = np.uint64(0xFFFFFFFF)
             chunks = [(lower & mask).astype(np.int64), (lower >> np.uint64(32)).astype(np.int64),
                       (upper.view(np.uint64) & mask).astype(np.int64), upper >> np.int64(32)]
-            sums = []
-            for c in chunks:  # at most 2^31 partials per group keep these sums inside 64 bits
-                acc_c = np.zeros(g, np.int64)
-                np.add.at(acc_c, pos, c)
-                sums.append(acc_c)
-            acc = _i128_from_chunks(sums)
+            # at most 2^31 partials per group keep these sums inside 64 bits
+            acc = _i128_from_chunks([reduce(np.add, c) for c in chunks])
         merged.append(acc)
     return ukeys, merged
 
@@ -297,10 +310,7 @@ def sharded_group_by(node, run_local, column_types=None, device: str = "cpu"):
             if is_float:
                 vals = merged[s] / n.astype(np.float64)
             else:
-                h = merged[s]
-                vals = np.array([float((int(up) << 64) | int(lw)) / float(c)
-                                 for lw, up, c in zip(h["lower"].tolist(), h["upper"].tolist(), n.tolist())],
-                                np.float64)
+                vals = _i128_to_f64(merged[s]) / n.astype(np.float64)
         else:
             _, s, t = f
             vals = merged[s] if t in (T.HUGEINT, T.FLOAT64) else merged[s].astype(NUMPY_DTYPE[t])
