@@ -187,35 +187,34 @@ def repartition_merge_groupby(keys: np.ndarray, aggregates: Sequence[tuple[str, 
             layout.append((kind, len(columns), 1))
             columns.append(values.astype(np.float64 if kind == "sum_f64" else np.int64))
     got, _ = _exchange(columns, send, device)
-    # Group the received partials by key: a stable sort, then one reduceat per column over each run of
-    # equal keys (exact for the int64 words; FP64 sums add in arrival order within a group).
-    order = np.argsort(got[0], kind="stable")
-    rkeys = got[0][order]
-    if rkeys.shape[0] == 0:
-        starts = np.zeros(0, np.int64)
-    else:
-        starts = np.flatnonzero(np.concatenate(([True], rkeys[1:] != rkeys[:-1])))
-    ukeys = rkeys[starts]
-
-    def reduce(ufunc, col):
-        col = col[order]
-        return ufunc.reduceat(col, starts) if starts.shape[0] else col[:0]
-
+    rkeys = got[0]
+    ukeys, pos = np.unique(rkeys, return_inverse=True)
+    g = ukeys.shape[0]
     merged = []
     for kind, first, _n in layout:
         col = got[first]
-        if kind in ("sum_f64", "count"):
-            acc = reduce(np.add, col)
+        if kind == "sum_f64":
+            acc = np.zeros(g, np.float64)
+            np.add.at(acc, pos, col)
+        elif kind == "count":
+            acc = np.zeros(g, np.int64)
+            np.add.at(acc, pos, col)
         elif kind in ("min", "max"):
-            acc = reduce(np.minimum if kind == "min" else np.maximum, col)
+            info = np.iinfo(np.int64)
+            acc = np.full(g, info.max if kind == "min" else info.min, np.int64)
+            (np.minimum if kind == "min" else np.maximum).at(acc, pos, col)
         else:
             lower = col.view(np.uint64)
             upper = got[first + 1]
             mask = np.uint64(0xFFFFFFFF)
             chunks = [(lower & mask).astype(np.int64), (lower >> np.uint64(32)).astype(np.int64),
                       (upper.view(np.uint64) & mask).astype(np.int64), upper >> np.int64(32)]
-            # at most 2^31 partials per group keep these sums inside 64 bits
-            acc = _i128_from_chunks([reduce(np.add, c) for c in chunks])
+            sums = []
+            for c in chunks:  # at most 2^31 partials per group keep these sums inside 64 bits
+                acc_c = np.zeros(g, np.int64)
+                np.add.at(acc_c, pos, c)
+                sums.append(acc_c)
+            acc = _i128_from_chunks(sums)
         merged.append(acc)
     return ukeys, merged
 
