@@ -189,3 +189,51 @@ def test_i128_to_f64_rounds_like_python_ints():
         arr[i]["upper"] = u - (1 << 64) if u >= 1 << 63 else u
     got = _i128_to_f64(arr)
     assert [float(v) for v in vals] == got.tolist()
+
+
+def _rank_reagg(rank, world, port, seed, out):
+    import datetime
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    from oracle.plan_oracle import evaluate
+    from vectisdb_b200.distributed import repartition_merge_groupby
+    k, x, v, w = _hc_data(seed)
+    lo, hi = (0, len(k) // 3) if rank == 0 else (len(k) // 3, len(k))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        keys, aggs = _partial(k[lo:hi], x[lo:hi], v[lo:hi], w[lo:hi])
+        plain = repartition_merge_groupby(keys, aggs)
+        calls = []
+
+        def run(plan, columns):  # the plan oracle standing in for the engine's GROUP BY
+            calls.append([a.kind for a in plan.aggregates])
+            return evaluate(plan, columns)
+
+        out[rank] = (plain, repartition_merge_groupby(keys, aggs, reaggregate=run), calls)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_repartition_merge_through_a_group_by_executor():
+    """The received partials re-aggregated by a GROUP BY executor (the engine's, in a deployment) give
+    the numpy merge's result: counts, MIN/MAX and 128-bit sums exactly (the sums travel as four 32-bit
+    chunk columns), FP64 sums within 1e-12 relative."""
+    ctx = mp.get_context("spawn")
+    manager = ctx.Manager()
+    out = manager.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_reagg, args=(r, 2, port, 13, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(240)
+        assert p.exitcode == 0
+    for rank in (0, 1):
+        (pk, pa), (rk, ra), calls = out[rank]
+        assert len(calls) == 1 and len(calls[0]) == 1 + 4 + 1 + 1 + 1  # SUM f64, 4 chunk SUMs, COUNT, MIN, MAX
+        assert np.array_equal(pk, rk) and len(pk) > 0
+        assert np.all(np.abs(ra[0] - pa[0]) <= 1e-12 * np.abs(pa[0]) + 1e-12)
+        assert np.array_equal(ra[1]["lower"], pa[1]["lower"]) and np.array_equal(ra[1]["upper"], pa[1]["upper"])
+        for got, want in zip(ra[2:], pa[2:]):
+            assert got.dtype == want.dtype and np.array_equal(got, want)

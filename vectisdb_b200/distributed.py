@@ -158,12 +158,19 @@ def _i128_to_f64(values: np.ndarray) -> np.ndarray:
 
 
 def repartition_merge_groupby(keys: np.ndarray, aggregates: Sequence[tuple[str, np.ndarray]],
-                              device: str = "cpu") -> tuple[np.ndarray, list[np.ndarray]]:
+                              device: str = "cpu", reaggregate=None) -> tuple[np.ndarray, list[np.ndarray]]:
     """Merges partial groups of a key space too large to index (the high-cardinality shape): every
     partial group goes to the rank that owns its key (a hash of the key), with one all-to-all per
     column, and each rank merges what it received. `keys` are the packed group keys (int64). Returns
     this rank's share of the merged groups, keys ascending; the ranks' shares are disjoint and together
-    hold every group. Exactness as in merge_dense_groupby."""
+    hold every group. Exactness as in merge_dense_groupby.
+
+    `reaggregate(plan, columns)`, when given, merges the received partials with a GROUP BY instead of
+    numpy: the engine's, so the merge runs where the engine does (`lambda p, c:
+    GpuEngine.instance().execute_plan(p, c).columns`). It gets a plan grouping INT64 column `k` with
+    SUM (FP64 sums, and counts as 128-bit sums), MIN and MAX over the partial columns -- 128-bit sums
+    as four 32-bit chunk columns whose exact sums are carried back into 128 bits -- and returns the
+    result columns (`.data`): key, then one per aggregate of the plan."""
     import torch.distributed as dist
     keys = np.asarray(keys, dtype=np.int64)
     for kind, values in aggregates:  # checked before any collective, so every rank fails alike
@@ -187,6 +194,8 @@ def repartition_merge_groupby(keys: np.ndarray, aggregates: Sequence[tuple[str, 
             layout.append((kind, len(columns), 1))
             columns.append(values.astype(np.float64 if kind == "sum_f64" else np.int64))
     got, _ = _exchange(columns, send, device)
+    if reaggregate is not None:
+        return _reaggregate(got, layout, reaggregate)
     rkeys = got[0]
     ukeys, pos = np.unique(rkeys, return_inverse=True)
     g = ukeys.shape[0]
@@ -219,7 +228,53 @@ def repartition_merge_groupby(keys: np.ndarray, aggregates: Sequence[tuple[str, 
     return ukeys, merged
 
 
-def sharded_group_by(node, run_local, column_types=None, device: str = "cpu"):
+def _reaggregate(got: list[np.ndarray], layout, run) -> tuple[np.ndarray, list[np.ndarray]]:
+    """The received partials merged by `run(plan, columns)` (a GROUP BY executor, see
+    repartition_merge_groupby)."""
+    from .engine import GpuAggregateKind as A, GpuValueType as T, make_aggregate, make_column, make_group_by, make_scan
+    rows = got[0].shape[0]
+    empty = {"sum_f64": np.float64, "count": np.int64, "min": np.int64, "max": np.int64, "sum_i128": HUGEINT}
+    if rows == 0:  # nothing arrived: no executor call (no collective follows, so ranks stay in step)
+        return np.zeros(0, np.int64), [np.zeros(0, empty[kind]) for kind, _, _ in layout]
+    names, cols, aggs, slots = ["k"], [make_column("k", T.INT64, got[0])], [], []
+    mask = np.uint64(0xFFFFFFFF)
+    for i, (kind, first, _n) in enumerate(layout):
+        if kind == "sum_i128":
+            lower, upper = got[first].view(np.uint64), got[first + 1]
+            parts = [(lower & mask).astype(np.int64), (lower >> np.uint64(32)).astype(np.int64),
+                     (upper.view(np.uint64) & mask).astype(np.int64), upper >> np.int64(32)]
+        else:
+            parts = [got[first]]
+        slots.append(len(aggs))
+        for j, part in enumerate(parts):
+            name = f"p{i}_{j}"
+            names.append(name)
+            if kind == "sum_f64":
+                cols.append(make_column(name, T.FLOAT64, part))
+                aggs.append(make_aggregate(A.SUM, name, T.FLOAT64))
+            else:
+                cols.append(make_column(name, T.INT64, part))
+                agg = {"min": A.MIN, "max": A.MAX}.get(kind, A.SUM)
+                aggs.append(make_aggregate(agg, name, T.HUGEINT if agg == A.SUM else T.INT64))
+    out = [np.asarray(c.data) for c in run(make_group_by(["k"], aggs, make_scan(names)), cols)]
+    if len(out) != 1 + len(aggs):
+        raise ValueError("repartition_merge_groupby: the re-aggregation returned the wrong number of columns")
+    order = np.argsort(out[0], kind="stable")
+    ukeys = out[0][order].astype(np.int64)
+    merged = []
+    for (kind, _, _), at in zip(layout, slots):
+        if kind == "sum_f64":
+            merged.append(out[1 + at][order].astype(np.float64))
+        elif kind in ("min", "max"):
+            merged.append(out[1 + at][order].astype(np.int64))
+        elif kind == "count":  # a 128-bit sum of counts: its low word
+            merged.append(out[1 + at][order]["lower"].view(np.int64))
+        else:  # four chunk sums, each below 2^63 for fewer than 2^31 partials per group
+            merged.append(_i128_from_chunks([out[1 + at + j][order]["lower"].view(np.int64) for j in range(4)]))
+    return ukeys, merged
+
+
+def sharded_group_by(node, run_local, column_types=None, device: str = "cpu", reaggregate=None):
     """A GROUP BY over rows split across ranks. `run_local(plan)` runs `plan` on this rank's rows (with
     the engine, say `lambda p: GpuEngine.instance().execute_plan(p, my_inputs).columns`) and returns its
     host result columns (GpuColumn-like: `.data` and `.validity`; the group keys, then one column per
@@ -231,7 +286,7 @@ def sharded_group_by(node, run_local, column_types=None, device: str = "cpu"):
     merges densely and every rank gets the whole result; a larger one merges by hash repartition and
     each rank gets a disjoint share. Groups come sorted by their keys, first key first. Dictionary-string
     keys must use one dictionary on every rank. NULL group keys or NULL aggregate outputs are refused on
-    every rank alike. Returns
+    every rank alike. `reaggregate` is passed to repartition_merge_groupby. Returns
     [(name, numpy array)]: the keys by name, then `agg_<i>` per aggregate of `node`, in order."""
     import torch.distributed as dist
     from .engine import GpuAggregateKind as A, GpuOpType, GpuPlanNode, GpuValueType as T, NUMPY_DTYPE, make_aggregate
@@ -298,7 +353,7 @@ def sharded_group_by(node, run_local, column_types=None, device: str = "cpu"):
         if (1 << sum(bits)) <= _MAX_DOMAIN:
             mkeys, merged = merge_dense_groupby(packed, aggs, 0, (1 << sum(bits)) - 1, device)
         else:
-            mkeys, merged = repartition_merge_groupby(packed, aggs, device)
+            mkeys, merged = repartition_merge_groupby(packed, aggs, device, reaggregate)
     out = []
     for name, l, b, sh, dt in zip(node.group_keys, lo.tolist(), bits, shifts, key_dtypes):
         out.append((name, (((mkeys >> sh) & ((1 << b) - 1)) + l).astype(dt)))
