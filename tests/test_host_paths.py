@@ -38,3 +38,25 @@ def test_clock_sampler_reports_unavailable_without_a_gpu():
     s.mark_end()
     out = s.stop()
     assert set(out) >= {"sm_mhz", "sm_max_mhz", "reasons"}
+
+
+def test_reference_arm_prints_one_contract_line():
+    """bench.py --impl reference runs the CPU restatement (no GPU needed) and prints one JSON line with
+    the keys the bench contract requires, its cpu_baseline and e2e describing the same run."""
+    import json
+    import subprocess
+    import sys
+    root = Path(__file__).resolve().parents[1]
+    r = subprocess.run([sys.executable, str(root / "bench.py"), "--impl", "reference", "--config", "c0", "--steps", "1",
+                        "--warmup", "1"], capture_output=True, text=True, timeout=600, cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+                "vs_baseline", "dtype", "data", "config", "impl", "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["impl"] == "reference" and line["steps"] == 1 and line["value"] > 0
+    cpu = line["cpu_baseline"]
+    assert cpu["value"] == line["value"] and cpu["kind"] == "port" and cpu["cores"] >= 1 and "not DuckDB" in cpu["label"]
+    assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
