@@ -60,3 +60,15 @@ def test_reference_arm_prints_one_contract_line():
     cpu = line["cpu_baseline"]
     assert cpu["value"] == line["value"] and cpu["kind"] == "port" and cpu["cores"] >= 1 and "not DuckDB" in cpu["label"]
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_reference_arm_runs_on_rank_zero_only():
+    """Under torchrun the reference arm's other ranks exit 0 at once, printing nothing."""
+    import os
+    import subprocess
+    import sys
+    root = Path(__file__).resolve().parents[1]
+    env = dict(os.environ, RANK="1", LOCAL_RANK="1", WORLD_SIZE="2")
+    r = subprocess.run([sys.executable, str(root / "bench.py"), "--impl", "reference", "--gpus", "2", "--steps", "1",
+                        "--warmup", "1"], capture_output=True, text=True, timeout=300, cwd=root, env=env)
+    assert r.returncode == 0 and r.stdout.strip() == "", (r.stdout[-500:], r.stderr[-500:])
