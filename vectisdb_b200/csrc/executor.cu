@@ -117,8 +117,16 @@ struct CachedJoinTable {
 	uint64_t words[4] = {0, 0, 0, 0};  // join words; [2] (the key bias) is `bias`
 	uint64_t bias = 0;
 	bool inline_value = false;
+	bool cached = false;  // held by the cache (guarded by the cache's mutex)
+	// Freed when the last holder lets go, on the runtime's stream: a holder whose kernels may still read
+	// the table lets go only after they finish (Executor::ReleaseHolds).
 	~CachedJoinTable() {
-		if (table) Runtime::Get().allocator().Free(table, Runtime::Get().default_stream());
+		if (!table) return;
+		try {
+			Runtime::Get().allocator().Free(table, Runtime::Get().default_stream());
+		} catch (...) {
+			// a destructor must not throw; a failing free leaves the bytes to the pool's teardown
+		}
 	}
 };
 
@@ -142,6 +150,18 @@ public:
 		lru_.push_front(key);
 		map_[key] = {t, lru_.begin()};
 		bytes_ += t->bytes;
+		t->cached = true;
+	}
+	//! Drops an execution's references when every table in `holds` is still cached (the cache's own
+	//! reference then outlives them, so nothing is freed here) and returns true; otherwise leaves
+	//! `holds` alone and returns false: one of them may be the last reference.
+	bool ReleaseIfCached(std::vector<std::shared_ptr<CachedJoinTable>> &holds) {
+		std::lock_guard<std::mutex> lock(mu_);
+		for (auto &h : holds) {
+			if (!h->cached) return false;
+		}
+		holds.clear();
+		return true;
 	}
 	void Clear() {
 		std::lock_guard<std::mutex> lock(mu_);
@@ -152,6 +172,7 @@ private:
 	static constexpr uint64_t kCapacity = 2ull << 30;
 	void EvictLocked(const std::string &key) {
 		auto it = map_.find(key);
+		it->second.first->cached = false;
 		bytes_ -= it->second.first->bytes;
 		lru_.erase(it->second.second);
 		map_.erase(it);
@@ -167,6 +188,11 @@ public:
 	Executor(const std::vector<vgpu_column> &inputs, const ExecOptions &options, cudaStream_t stream, bool nulls_ok)
 	    : inputs_(inputs), options_(options), stream_(stream), arena_(stream), nulls_supported_(nulls_ok) {
 	}
+	~Executor() {
+		ReleaseHolds();
+	}
+	Executor(const Executor &) = delete;
+	Executor &operator=(const Executor &) = delete;
 
 	Relation Exec(const PlanNode &node);
 	Arena &arena() {
@@ -222,7 +248,14 @@ private:
 	                    uint64_t extra_smem);
 
 	const std::vector<vgpu_column> &inputs_;
-	std::vector<std::shared_ptr<void>> holds_;  // cached structures in use by this execution
+	//! Join tables this execution's kernels read. A table evicted meanwhile (or never cached) is freed
+	//! with its last reference, on another stream, so this execution's kernels must finish first.
+	void ReleaseHolds() {
+		if (holds_.empty() || JoinTableCache::Get().ReleaseIfCached(holds_)) return;
+		cudaStreamSynchronize(stream_);  // an error here is the query's own, already reported
+		holds_.clear();
+	}
+	std::vector<std::shared_ptr<CachedJoinTable>> holds_;  // kept join tables in use by this execution
 	ExecOptions options_;
 	cudaStream_t stream_;
 	Arena arena_;
