@@ -338,6 +338,9 @@ typedef struct vgpu_memory_stats {
 /* 0 = derive from VECTOR_GPU_VRAM_FRACTION (default 0.85) of free memory at first use. */
 vgpu_status vgpu_memory_set_budget(uint64_t bytes);
 vgpu_status vgpu_memory_stats_get(vgpu_memory_stats *out);
+/* Restarts peak_bytes at the bytes in use now, so that the peak of the next calls can be read back
+ * (the reference samples cudaMemGetInfo for this, cuda_engine/tests/test_gpu_cost_model.cpp:16-40). */
+vgpu_status vgpu_memory_reset_peak(void);
 /* HasHeadroomFor (cuda_engine/src/rmm_pool.cpp:172-191) */
 int vgpu_memory_has_headroom(uint64_t bytes);
 

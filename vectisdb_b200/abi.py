@@ -193,6 +193,7 @@ SIGNATURES = [
     ("vgpu_memory_set_budget", C.c_int, [C.c_uint64]),
     ("vgpu_memory_stats_get", C.c_int, [C.POINTER(vgpu_memory_stats)]),
     ("vgpu_memory_has_headroom", C.c_int, [C.c_uint64]),
+    ("vgpu_memory_reset_peak", C.c_int, []),
     ("vgpu_cache_init", C.c_int, [C.c_double]),
     ("vgpu_cache_begin_staging", C.c_int, [C.POINTER(vgpu_table_ref)]),
     ("vgpu_cache_stage_chunk", C.c_int, [C.POINTER(vgpu_table_ref), C.POINTER(vgpu_column), C.POINTER(C.c_int)]),

@@ -711,6 +711,13 @@ vgpu_status vgpu_memory_stats_get(vgpu_memory_stats *out) {
 	});
 }
 
+vgpu_status vgpu_memory_reset_peak(void) {
+	return Guard([&] {
+		Runtime::Get().EnsureDevice();
+		Runtime::Get().allocator().ResetPeak();
+	});
+}
+
 int vgpu_memory_has_headroom(uint64_t bytes) {
 	try {
 		Runtime::Get().EnsureDevice();

@@ -192,6 +192,11 @@ vgpu_memory_stats DeviceAllocator::Stats() {
 	return s;
 }
 
+void DeviceAllocator::ResetPeak() {
+	std::lock_guard<std::mutex> lock(mu_);
+	peak_ = in_use_;
+}
+
 // ============================================================================================
 // Arena
 

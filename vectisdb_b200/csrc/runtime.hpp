@@ -63,6 +63,8 @@ public:
 	uint64_t Budget();
 	bool HasHeadroom(uint64_t bytes);
 	vgpu_memory_stats Stats();
+	//! Restarts the peak at the bytes in use now (the pool's reserve is unaffected).
+	void ResetPeak();
 
 private:
 	void EnsureBudgetLocked();

@@ -775,6 +775,18 @@ def estimate_working_set(plan: GpuPlanNode, max_chunk_rows: int = 0) -> abi.vgpu
     return ws
 
 
+def memory_stats() -> dict:
+    """The engine allocator's budget, bytes in use, peak, allocation and failure counts."""
+    s = abi.vgpu_memory_stats()
+    abi.check(abi.lib().vgpu_memory_stats_get(C.byref(s)))
+    return {name: int(getattr(s, name)) for name, _ in abi.vgpu_memory_stats._fields_}
+
+
+def memory_reset_peak() -> None:
+    """Restarts the allocator's peak at the bytes in use now."""
+    abi.check(abi.lib().vgpu_memory_reset_peak())
+
+
 def analyze_plan_shape(plan: GpuPlanNode) -> abi.vgpu_plan_shape:
     """AnalyzePlanShape (gpu_engine.hpp:329): work per scanned row from the plan's advisory fields."""
     keep = _Keep()
