@@ -179,6 +179,11 @@ def _rank(rank, world, port, out):
         n = len(probe["pk"])
         part = _slice(probe, 0, n // 4) if rank == 0 else _slice(probe, n // 4, n)
         out[("join", rank)] = sharded_group_by(node, lambda p: _group(p, _join(got, part), False), TYPES)
+        try:  # a column that is not fixed-width: refused on both ranks, after the one header broadcast
+            broadcast_table({"names": np.array(["a", "b"], dtype=object)} if rank == 0 else None)
+            out[("bad_broadcast", rank)] = "sent"
+        except ValueError as e:
+            out[("bad_broadcast", rank)] = str(e)
         node, arrays = _dense_case(5)
         validity = (lambda g: np.arange(g) != 0) if rank == 1 else None  # one NULL key on rank 1 only
         try:
@@ -261,6 +266,11 @@ def test_broadcast_build_side_and_probe_sharded_join_group_by(results):
         for name in build:
             assert got[name].dtype == build[name].dtype and got[name].tobytes() == build[name].tobytes()
         _check(results[("join", rank)], _expect(node, _join(build, probe)), node)
+
+
+def test_broadcast_refuses_object_columns_on_both_ranks(results):
+    for rank in (0, 1):
+        assert "fixed-width" in results[("bad_broadcast", rank)]
 
 
 def test_null_keys_are_refused_on_both_ranks(results):
