@@ -203,6 +203,12 @@ def _rank_reagg(rank, world, port, seed, out):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         keys, aggs = _partial(k[lo:hi], x[lo:hi], v[lo:hi], w[lo:hi])
+        pos = np.searchsorted(keys, k[lo:hi])  # MIN/MAX of the DOUBLE column x merge as floats
+        xmn = np.full(len(keys), np.inf)
+        np.minimum.at(xmn, pos, x[lo:hi])
+        xmx = np.full(len(keys), -np.inf)
+        np.maximum.at(xmx, pos, x[lo:hi])
+        aggs += [("min_f64", xmn), ("max_f64", xmx)]
         plain = repartition_merge_groupby(keys, aggs)
         calls = []
 
@@ -231,9 +237,23 @@ def test_repartition_merge_through_a_group_by_executor():
         assert p.exitcode == 0
     for rank in (0, 1):
         (pk, pa), (rk, ra), calls = out[rank]
-        assert len(calls) == 1 and len(calls[0]) == 1 + 4 + 1 + 1 + 1  # SUM f64, 4 chunk SUMs, COUNT, MIN, MAX
+        # SUM f64, 4 chunk SUMs, COUNT, MIN, MAX, float MIN, float MAX
+        assert len(calls) == 1 and len(calls[0]) == 1 + 4 + 1 + 1 + 1 + 2
         assert np.array_equal(pk, rk) and len(pk) > 0
         assert np.all(np.abs(ra[0] - pa[0]) <= 1e-12 * np.abs(pa[0]) + 1e-12)
         assert np.array_equal(ra[1]["lower"], pa[1]["lower"]) and np.array_equal(ra[1]["upper"], pa[1]["upper"])
         for got, want in zip(ra[2:], pa[2:]):
             assert got.dtype == want.dtype and np.array_equal(got, want)
+        assert pa[5].dtype == np.float64 and np.any(pa[5] != np.round(pa[5])) and np.any(pa[5] < 0)
+    k, x, _, _ = _hc_data(13)  # the float MIN/MAX equal those over all rows
+    keys = np.concatenate([out[0][0][0], out[1][0][0]])
+    order = np.argsort(keys)
+    ek = np.unique(k)
+    assert np.array_equal(keys[order], ek)
+    pos = np.searchsorted(ek, k)
+    emn = np.full(len(ek), np.inf)
+    np.minimum.at(emn, pos, x)
+    emx = np.full(len(ek), -np.inf)
+    np.maximum.at(emx, pos, x)
+    assert np.array_equal(np.concatenate([out[0][0][1][5], out[1][0][1][5]])[order], emn)
+    assert np.array_equal(np.concatenate([out[0][0][1][6], out[1][0][1][6]])[order], emx)

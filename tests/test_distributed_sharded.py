@@ -71,7 +71,7 @@ def _group(plan, arrays, allow_avg, validity=None):
                 u = (t >> 64) & ((1 << 64) - 1)
                 vals[i]["upper"] = u - (1 << 64) if u >= 1 << 63 else u
         elif a.kind in (A.MIN, A.MAX):
-            info = np.iinfo(x.dtype)
+            info = np.finfo(x.dtype) if x.dtype.kind == "f" else np.iinfo(x.dtype)
             vals = np.full(g, info.max if a.kind == A.MIN else info.min, x.dtype)
             (np.minimum if a.kind == A.MIN else np.maximum).at(vals, pos, x)
         elif a.kind == A.AVG and allow_avg:
@@ -114,6 +114,24 @@ def _sparse_case(seed):
               "v": rng.integers((1 << 62) - 1000, 1 << 62, n, dtype=np.int64) * rng.choice([-1, 1], n)}
     node = make_group_by(["k"], [make_aggregate(A.AVG, "v", T.FLOAT64), make_aggregate(A.SUM, "v", T.HUGEINT),
                                  make_aggregate(A.COUNT_STAR, "", T.INT64)], make_scan(list(arrays)))
+    return node, arrays
+
+
+def _float_minmax_case(seed, sparse):
+    """MIN/MAX over DOUBLE and FLOAT columns with negative and fractional values (they must merge as
+    floats, not be truncated to integers), beside SUM and COUNT(*); dense or sparse 40-bit keys."""
+    rng = np.random.default_rng(seed)
+    n = 30000
+    if sparse:
+        k = rng.integers(0, 1 << 40, 20000)[rng.integers(0, 20000, n)].astype(np.int64)
+    else:
+        k = rng.integers(-7, 60, n).astype(np.int32)
+    arrays = {"k": k, "d": rng.standard_normal(n) * 1e3 - 0.25,
+              "f": (rng.standard_normal(n) * 7.5).astype(np.float32)}
+    node = make_group_by(["k"], [make_aggregate(A.MIN, "d", T.FLOAT64), make_aggregate(A.MAX, "d", T.FLOAT64),
+                                 make_aggregate(A.MIN, "f", T.FLOAT32), make_aggregate(A.MAX, "f", T.FLOAT32),
+                                 make_aggregate(A.COUNT_STAR, "", T.INT64), make_aggregate(A.SUM, "d", T.FLOAT64)],
+                         make_scan(list(arrays)))
     return node, arrays
 
 
@@ -172,6 +190,11 @@ def _rank(rank, world, port, out):
         n = len(arrays["k"])
         part = _slice(arrays, 0, n // 2) if rank == 0 else _slice(arrays, n // 2, n)
         out[("sparse", rank)] = sharded_group_by(node, lambda p: _group(p, part, False), TYPES)
+        for sparse in (False, True):
+            node, arrays = _float_minmax_case(8, sparse)
+            n = len(arrays["k"])
+            part = _slice(arrays, 0, n // 3) if rank == 0 else _slice(arrays, n // 3, n)
+            out[("float_minmax", sparse, rank)] = sharded_group_by(node, lambda p: _group(p, part, False), TYPES)
         node, build, probe = _join_case(6)
         from vectisdb_b200.distributed import broadcast_table
         got = broadcast_table(build if rank == 0 else None)
@@ -221,7 +244,9 @@ def _check(got, exp, node):
     nk = len(node.group_keys)
     for (name, g), (_, e), i in zip(got, exp, range(len(exp))):
         a = node.aggregates[i - nk] if i >= nk else None
-        if a is not None and a.output_type == T.FLOAT64 and not (a.kind == A.AVG and a.input_column == "v"):
+        if a is not None and a.kind in (A.MIN, A.MAX):  # MIN/MAX of any type: bit-exact, its own dtype
+            assert g.dtype == e.dtype and np.array_equal(g, e), name
+        elif a is not None and a.output_type == T.FLOAT64 and not (a.kind == A.AVG and a.input_column == "v"):
             assert g.dtype == np.float64
             assert np.all(np.abs(g - e) <= 1e-12 * np.abs(e)), name
         elif a is not None and a.output_type == T.HUGEINT:
@@ -256,6 +281,22 @@ def test_sparse_keys_repartition_into_disjoint_shares(results):
     order = np.argsort(np.concatenate([a[0][1], b[0][1]]))
     got = [(na, np.concatenate([va, vb])[order]) for (na, va), (_, vb) in zip(a, b)]
     _check(got, exp, node)
+
+
+def test_float_min_max_merge_as_floats(results):
+    """MIN/MAX over DOUBLE/FLOAT keep their fractional and negative values and their dtype through the
+    dense merge (every rank gets the whole result) and the hash repartition (disjoint shares)."""
+    node, arrays = _float_minmax_case(8, False)
+    exp = _expect(node, arrays)
+    assert np.any(exp[1][1] != np.round(exp[1][1])) and np.any(exp[1][1] < 0)
+    for rank in (0, 1):
+        _check(results[("float_minmax", False, rank)], exp, node)
+    node, arrays = _float_minmax_case(8, True)
+    exp = _expect(node, arrays)
+    a, b = results[("float_minmax", True, 0)], results[("float_minmax", True, 1)]
+    assert len(a[0][1]) > 0 and len(b[0][1]) > 0 and len(np.intersect1d(a[0][1], b[0][1])) == 0
+    order = np.argsort(np.concatenate([a[0][1], b[0][1]]))
+    _check([(na, np.concatenate([va, vb])[order]) for (na, va), (_, vb) in zip(a, b)], exp, node)
 
 
 def test_broadcast_build_side_and_probe_sharded_join_group_by(results):

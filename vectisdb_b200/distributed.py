@@ -4,7 +4,8 @@ runs the query on its own rows with the engine, and the partial groups are merge
 `merge_dense_groupby` handles key domains small enough to index directly (the filter + group-by and
 join + group-by shapes: at most 2^20 key values): every aggregate becomes a key-indexed array filled
 with the rank's partial values (the identity elsewhere) and is combined with one all-reduce -- SUM
-for sums and counts, MIN and MAX for those. 128-bit integer sums (DuckDB's HUGEINT, the engine's
+for sums and counts, MIN and MAX for those (in int64 over integer columns, in float64 with +-inf as
+the identity over FLOAT32/FLOAT64 columns: kinds "min_f64"/"max_f64"). 128-bit integer sums (DuckDB's HUGEINT, the engine's
 `{lower, upper}` pairs) travel as four 32-bit chunks summed in 64-bit lanes, which cannot overflow
 for fewer than 2^31 ranks, and are carried back into 128 bits, so the merged sum is exact. AVG does
 not merge from its outputs: shard its SUM and COUNT instead. `repartition_merge_groupby` handles key
@@ -25,7 +26,9 @@ from typing import Sequence
 
 import numpy as np
 
-KINDS = ("sum_f64", "sum_i128", "count", "min", "max")
+KINDS = ("sum_f64", "sum_i128", "count", "min", "max", "min_f64", "max_f64")
+# MIN/MAX over integer columns merge as int64, over FLOAT32/FLOAT64 columns as float64 (identity +-inf)
+_FLOAT_KINDS = ("sum_f64", "min_f64", "max_f64")
 HUGEINT = np.dtype([("lower", "<u8"), ("upper", "<i8")])
 _MAX_DOMAIN = 1 << 20
 
@@ -76,6 +79,11 @@ def merge_dense_groupby(keys: np.ndarray, aggregates: Sequence[tuple[str, np.nda
             dense = np.full(domain, info.max if kind == "min" else info.min, np.int64)
             dense[slot] = values.astype(np.int64)
             op = dist.ReduceOp.MIN if kind == "min" else dist.ReduceOp.MAX
+            merged.append(_all_reduce(dense, op, device)[live])
+        elif kind in ("min_f64", "max_f64"):
+            dense = np.full(domain, np.inf if kind == "min_f64" else -np.inf, np.float64)
+            dense[slot] = values.astype(np.float64)
+            op = dist.ReduceOp.MIN if kind == "min_f64" else dist.ReduceOp.MAX
             merged.append(_all_reduce(dense, op, device)[live])
         else:
             merged.append(_merge_i128(values, slot, domain, device)[live])
@@ -169,7 +177,8 @@ def repartition_merge_groupby(keys: np.ndarray, aggregates: Sequence[tuple[str, 
     numpy: the engine's, so the merge runs where the engine does (`lambda p, c:
     GpuEngine.instance().execute_plan(p, c).columns`). It gets a plan grouping INT64 column `k` with
     SUM (FP64 sums, and counts as 128-bit sums), MIN and MAX over the partial columns -- 128-bit sums
-    as four 32-bit chunk columns whose exact sums are carried back into 128 bits -- and returns the
+    as four 32-bit chunk columns whose exact sums are carried back into 128 bits, float MIN/MAX as
+    order-preserving int64 words (the engine's MIN/MAX takes integer columns only) -- and returns the
     result columns (`.data`): key, then one per aggregate of the plan."""
     import torch.distributed as dist
     keys = np.asarray(keys, dtype=np.int64)
@@ -192,7 +201,7 @@ def repartition_merge_groupby(keys: np.ndarray, aggregates: Sequence[tuple[str, 
             columns += [v["lower"].view(np.int64), v["upper"].astype(np.int64)]
         else:
             layout.append((kind, len(columns), 1))
-            columns.append(values.astype(np.float64 if kind == "sum_f64" else np.int64))
+            columns.append(values.astype(np.float64 if kind in _FLOAT_KINDS else np.int64))
     got, _ = _exchange(columns, send, device)
     if reaggregate is not None:
         return _reaggregate(got, layout, reaggregate)
@@ -212,6 +221,9 @@ def repartition_merge_groupby(keys: np.ndarray, aggregates: Sequence[tuple[str, 
             info = np.iinfo(np.int64)
             acc = np.full(g, info.max if kind == "min" else info.min, np.int64)
             (np.minimum if kind == "min" else np.maximum).at(acc, pos, col)
+        elif kind in ("min_f64", "max_f64"):
+            acc = np.full(g, np.inf if kind == "min_f64" else -np.inf, np.float64)
+            (np.minimum if kind == "min_f64" else np.maximum).at(acc, pos, col)
         else:
             lower = col.view(np.uint64)
             upper = got[first + 1]
@@ -228,12 +240,21 @@ def repartition_merge_groupby(keys: np.ndarray, aggregates: Sequence[tuple[str, 
     return ukeys, merged
 
 
+def _f64_order_bits(values: np.ndarray) -> np.ndarray:
+    """float64 values <-> int64 words whose signed order is the floats' order (NaN above +inf): the
+    sign bit kept, the other 63 bits flipped for negative values. The map is its own inverse, so it
+    also turns such words (given as int64) back into the float64 bit patterns."""
+    b = np.ascontiguousarray(values).view(np.int64)
+    return np.where(b < 0, b ^ np.int64(0x7FFFFFFFFFFFFFFF), b)
+
+
 def _reaggregate(got: list[np.ndarray], layout, run) -> tuple[np.ndarray, list[np.ndarray]]:
     """The received partials merged by `run(plan, columns)` (a GROUP BY executor, see
     repartition_merge_groupby)."""
     from .engine import GpuAggregateKind as A, GpuValueType as T, make_aggregate, make_column, make_group_by, make_scan
     rows = got[0].shape[0]
-    empty = {"sum_f64": np.float64, "count": np.int64, "min": np.int64, "max": np.int64, "sum_i128": HUGEINT}
+    empty = {"sum_f64": np.float64, "count": np.int64, "min": np.int64, "max": np.int64, "sum_i128": HUGEINT,
+             "min_f64": np.float64, "max_f64": np.float64}
     if rows == 0:  # nothing arrived: no executor call (no collective follows, so ranks stay in step)
         return np.zeros(0, np.int64), [np.zeros(0, empty[kind]) for kind, _, _ in layout]
     names, cols, aggs, slots = ["k"], [make_column("k", T.INT64, got[0])], [], []
@@ -252,6 +273,9 @@ def _reaggregate(got: list[np.ndarray], layout, run) -> tuple[np.ndarray, list[n
             if kind == "sum_f64":
                 cols.append(make_column(name, T.FLOAT64, part))
                 aggs.append(make_aggregate(A.SUM, name, T.FLOAT64))
+            elif kind in ("min_f64", "max_f64"):  # as order-preserving int64 (the GPU MIN/MAX is integer-only)
+                cols.append(make_column(name, T.INT64, _f64_order_bits(part)))
+                aggs.append(make_aggregate(A.MIN if kind == "min_f64" else A.MAX, name, T.INT64))
             else:
                 cols.append(make_column(name, T.INT64, part))
                 agg = {"min": A.MIN, "max": A.MAX}.get(kind, A.SUM)
@@ -265,6 +289,8 @@ def _reaggregate(got: list[np.ndarray], layout, run) -> tuple[np.ndarray, list[n
     for (kind, _, _), at in zip(layout, slots):
         if kind == "sum_f64":
             merged.append(out[1 + at][order].astype(np.float64))
+        elif kind in ("min_f64", "max_f64"):
+            merged.append(_f64_order_bits(out[1 + at][order].astype(np.int64)).view(np.float64))
         elif kind in ("min", "max"):
             merged.append(out[1 + at][order].astype(np.int64))
         elif kind == "count":  # a 128-bit sum of counts: its low word
@@ -315,7 +341,8 @@ def sharded_group_by(node, run_local, column_types=None, device: str = "cpu", re
             if a.kind in (A.COUNT_STAR, A.COUNT):
                 kinds.append("count")
             elif a.kind in (A.MIN, A.MAX):
-                kinds.append("min" if a.kind == A.MIN else "max")
+                suffix = "_f64" if out_t in (T.FLOAT32, T.FLOAT64) else ""
+                kinds.append(("min" if a.kind == A.MIN else "max") + suffix)
             else:
                 kinds.append("sum_i128" if out_t == T.HUGEINT else "sum_f64")
     plan = GpuPlanNode(node.op_type, list(node.children), estimated_rows=node.estimated_rows,
@@ -344,7 +371,7 @@ def sharded_group_by(node, run_local, column_types=None, device: str = "cpu", re
     aggs = list(zip(kinds, [c.data for c in cols[nk:]]))
     if empty:
         mkeys = np.zeros(0, np.int64)
-        merged = [np.zeros(0, HUGEINT if k == "sum_i128" else np.float64 if k == "sum_f64" else np.int64)
+        merged = [np.zeros(0, HUGEINT if k == "sum_i128" else np.float64 if k in _FLOAT_KINDS else np.int64)
                   for k in kinds]
     else:
         packed = np.zeros(rows, np.int64)
