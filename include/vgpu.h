@@ -515,7 +515,11 @@ void vgpu_server_destroy(vgpu_server *server);
  * on a device looks up that array's device address (cudaGetSymbolAddress) and should come before any
  * stream capture. Work is queued on `stream` (NULL = legacy default stream) and not synchronized.
  * Every call shares the one array, which keeps the last call's contents: calls whose work overlaps on
- * the GPU (different streams, no ordering between them) race and corrupt each other's results. */
+ * the GPU (different streams, no ordering between them) race and corrupt each other's results.
+ * SUM(v) is accumulated with FP64 atomics, so its order -- and its last bits -- vary from call to call
+ * (COUNT is exact). The looked-up address belongs to the device's current context: after a
+ * cudaDeviceReset (or any reset of the primary context) in the same process it is stale, so do not
+ * call this entry point after such a reset. */
 vgpu_status vgpu_group_by_count_sum_noalloc(const int32_t *keys, const double *values, uint64_t n, int32_t key_min,
                                             uint32_t domain, int32_t *out_keys, int64_t *out_counts,
                                             double *out_sums, uint64_t *out_groups, void *stream);

@@ -9,7 +9,10 @@
 // The array is file-scope device memory: every GPU that loads this library holds it
 // (kNoAllocMaxDomain * 16 + 8 bytes, about 1 MiB) until the process exits. Host code may not use the
 // symbol itself as an address -- there it is only a host-side stand-in -- so the device address is
-// looked up once per device with cudaGetSymbolAddress, with that device current.
+// looked up once per device with cudaGetSymbolAddress, with that device current. That address belongs
+// to the device's context of the time: a cudaDeviceReset makes it stale, so the entry point is not for
+// use after a reset in the same process. SUM(v) accumulates with FP64 atomics, so its last bits depend
+// on the order they land in and vary between calls.
 #include <cstdint>
 #include <mutex>
 
