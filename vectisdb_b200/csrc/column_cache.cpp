@@ -3,6 +3,7 @@
 // gate, byte-budget LRU, whole-table invalidation with a generation counter.
 #include "column_cache.hpp"
 
+#include <algorithm>
 #include <cstdlib>
 
 #include "kernels.hpp"
@@ -56,8 +57,10 @@ void ColumnCache::EvictLocked(const std::string &key) {
 	if (it == entries_.end()) return;
 	auto &alloc = Runtime::Get().allocator();
 	cudaStream_t s = Runtime::Get().default_stream();
-	// Borrowers may still have kernels queued on other streams: let them finish first.
-	cudaDeviceSynchronize();
+	// Engine executions that read the column may still have kernels queued on their streams: the free is
+	// ordered after the marks they left (no device-wide wait). Pointers handed out by GetWhole/TryGetChunk
+	// to other code are borrows valid until the next call that can evict, as in the reference's cache.
+	it->second.readers->WaitAll(s);
 	alloc.Free(it->second.column.data, s);
 	alloc.Free(it->second.column.valid, s);
 	committed_ -= it->second.bytes;
@@ -96,7 +99,9 @@ void ColumnCache::BeginStaging(const TableRef &table) {
 	EnsureInitialized(0.5);
 	std::lock_guard<std::mutex> lock(mu_);
 	AbortLocked(table);
-	EvictTableLocked(table);
+	// Committed columns of the table stay (as in the reference's cache, gpu_column_cache.cpp:163-172):
+	// frequently queried column subsets remain resident; a column staged again replaces its entry at
+	// commit, and InvalidateTable drops them all when the table changes.
 	if (budget_ == 0) return;
 	staging_[TableKey(table)];
 }
@@ -222,12 +227,15 @@ void ColumnCache::CommitStaging(const TableRef &table, uint64_t scanned_rows) {
 			}
 		}
 		const std::string key = Key(table, kv.first);
+		const bool replaced = entries_.count(key) != 0;
+		if (replaced) EvictLocked(key);  // the column staged again: the new contents replace the old entry
 		e.table_key = tk;
 		lru_.push_front(key);
 		e.lru = lru_.begin();
 		committed_ += e.bytes;
 		entries_[key] = std::move(e);
-		table_columns_[tk].push_back(kv.first);
+		auto &cols = table_columns_[tk];
+		if (std::find(cols.begin(), cols.end(), kv.first) == cols.end()) cols.push_back(kv.first);
 	}
 	VGPU_CUDA(cudaStreamSynchronize(s));
 	staging_.erase(it);
@@ -343,6 +351,23 @@ bool ColumnCache::BoundsOf(const void *data, ValueType type, uint64_t rows, int6
 		return true;
 	}
 	return false;
+}
+
+void ColumnCache::AddReaders(const std::vector<const void *> &ptrs, const std::shared_ptr<StreamMark> &mark) {
+	if (!mark || ptrs.empty()) return;
+	std::lock_guard<std::mutex> lock(mu_);
+	for (auto &kv : entries_) {
+		const DevColumn &c = kv.second.column;
+		const auto base = reinterpret_cast<uintptr_t>(c.data);
+		const auto end = base + c.rows * TypeSize(c.type);
+		for (const void *p : ptrs) {
+			const auto q = reinterpret_cast<uintptr_t>(p);
+			if (q >= base && q < end) {
+				kv.second.readers->Add(mark);
+				break;
+			}
+		}
+	}
 }
 
 uint64_t ColumnCache::Generation(const TableRef &table) {

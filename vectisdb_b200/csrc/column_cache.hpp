@@ -41,6 +41,10 @@ public:
 	//! The committed column's value range when `rows` values at `data` lie inside one (a superset of
 	//! those rows' range, valid for key packing); false otherwise.
 	bool BoundsOf(const void *data, ValueType type, uint64_t rows, int64_t *min, int64_t *max);
+	//! Records `mark` (after an execution's last kernel) on every committed column that one of `ptrs`
+	//! points into: evicting such a column frees its buffers only after the marked work. Pointers
+	//! outside the cache are ignored.
+	void AddReaders(const std::vector<const void *> &ptrs, const std::shared_ptr<StreamMark> &mark);
 
 private:
 	struct Chunk {
@@ -63,6 +67,7 @@ private:
 		std::vector<uint64_t> chunk_rows;
 		uint64_t bytes = 0;
 		std::list<std::string>::iterator lru;
+		std::shared_ptr<ReaderMarks> readers = std::make_shared<ReaderMarks>();  // engine executions that read it
 	};
 	static std::string Key(const TableRef &t, const std::string &column);
 	static std::string TableKey(const TableRef &t);

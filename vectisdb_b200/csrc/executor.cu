@@ -109,8 +109,9 @@ uint64_t FloorPow2(uint64_t x) {
 // Dense join tables built from cache-owned columns, kept across executions and keyed by the columns'
 // identities (ColumnCache::Identify: contents behind an identity never change), so a repeated join with
 // the same right side skips its key widening, range passes, read-back and table build. LRU over at most
-// 2 GiB of tables. A table is freed when the cache has let go of it and no execution holds it; every
-// consumer of a fused join reads a count back before its execution ends, so by then its reads are done.
+// 2 GiB of tables. A table is freed when the cache has let go of it and no execution holds it, on the
+// runtime's stream after the events its readers recorded (CachedJoinTable::AddReader).
+
 struct CachedJoinTable {
 	void *table = nullptr;
 	uint64_t bytes = 0;
@@ -118,12 +119,16 @@ struct CachedJoinTable {
 	uint64_t bias = 0;
 	bool inline_value = false;
 	bool cached = false;  // held by the cache (guarded by the cache's mutex)
-	// Freed when the last holder lets go, on the runtime's stream: a holder whose kernels may still read
-	// the table lets go only after they finish (Executor::ReleaseHolds).
+	//! Marks left by the executions that read the table: the free waits for all of them, wherever the
+	//! last reference is dropped (an eviction by another query, a cache clear, or the reader itself).
+	ReaderMarks readers;
+	// Freed when the last holder lets go, on the runtime's stream, after every reader's mark.
 	~CachedJoinTable() {
 		if (!table) return;
 		try {
-			Runtime::Get().allocator().Free(table, Runtime::Get().default_stream());
+			cudaStream_t s = Runtime::Get().default_stream();
+			readers.WaitAll(s);
+			Runtime::Get().allocator().Free(table, s);
 		} catch (...) {
 			// a destructor must not throw; a failing free leaves the bytes to the pool's teardown
 		}
@@ -151,17 +156,6 @@ public:
 		map_[key] = {t, lru_.begin()};
 		bytes_ += t->bytes;
 		t->cached = true;
-	}
-	//! Drops an execution's references when every table in `holds` is still cached (the cache's own
-	//! reference then outlives them, so nothing is freed here) and returns true; otherwise leaves
-	//! `holds` alone and returns false: one of them may be the last reference.
-	bool ReleaseIfCached(std::vector<std::shared_ptr<CachedJoinTable>> &holds) {
-		std::lock_guard<std::mutex> lock(mu_);
-		for (auto &h : holds) {
-			if (!h->cached) return false;
-		}
-		holds.clear();
-		return true;
 	}
 	void Clear() {
 		std::lock_guard<std::mutex> lock(mu_);
@@ -248,13 +242,20 @@ private:
 	                    uint64_t extra_smem);
 
 	const std::vector<vgpu_column> &inputs_;
-	//! Join tables this execution's kernels read. A table evicted meanwhile (or never cached) is freed
-	//! with its last reference, on another stream, so this execution's kernels must finish first.
+	//! Long-lived buffers this execution's kernels read -- kept join tables and committed cache columns
+	//! -- get a mark recorded after its last kernel, which their frees wait for; the references then
+	//! drop without waiting for the stream (with VGPU_EXEC_NO_SYNC the execution returns before its
+	//! kernels finish), and whoever frees such a buffer later (an eviction, an invalidation, this
+	//! execution dropping a table's last reference) frees it only after those kernels.
 	void ReleaseHolds() {
-		if (holds_.empty() || JoinTableCache::Get().ReleaseIfCached(holds_)) return;
-		cudaStreamSynchronize(stream_);  // an error here is the query's own, already reported
+		if (holds_.empty() && cache_reads_.empty()) return;
+		auto mark = StreamMark::After(stream_);
+		for (auto &h : holds_) h->readers.Add(mark);
 		holds_.clear();
+		if (mark) ColumnCache::Get().AddReaders(cache_reads_, mark);
+		cache_reads_.clear();
 	}
+	std::vector<const void *> cache_reads_;  // device data this execution read that may be cache-owned
 	std::vector<std::shared_ptr<CachedJoinTable>> holds_;  // kept join tables in use by this execution
 	ExecOptions options_;
 	cudaStream_t stream_;
@@ -297,6 +298,7 @@ Relation Executor::Scan(const PlanNode &node) {
 				Fail(VGPU_ERR_UNSUPPORTED, "gpu_executor: cached column '" + name +
 				                               "' contains NULLs, which this operator does not model");
 			}
+			cache_reads_.push_back(col.data);
 			out.push_back(col);
 		}
 		return out;
@@ -323,6 +325,7 @@ Relation Executor::Scan(const PlanNode &node) {
 		}
 		if (in.memory == VGPU_MEM_DEVICE) {
 			col.data = const_cast<void *>(in.data);
+			if (col.data != nullptr) cache_reads_.push_back(col.data);  // may be rows of a cached column
 			if (col.data == nullptr) {
 				col.data = arena_.Alloc(16);
 			} else if (in.validity == nullptr && IsIntegerKeyType(col.type)) {

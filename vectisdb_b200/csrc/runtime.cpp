@@ -724,4 +724,37 @@ int Runtime::MaxActiveBlocks(CUfunction f, int block, size_t smem) {
 	return n;
 }
 
+// ---- Reader marks -------------------------------------------------------------------------------
+
+std::shared_ptr<StreamMark> StreamMark::After(cudaStream_t stream) {
+	auto m = std::make_shared<StreamMark>();
+	if (cudaEventCreateWithFlags(&m->ev_, cudaEventDisableTiming) != cudaSuccess ||
+	    cudaEventRecord(m->ev_, stream) != cudaSuccess) {
+		cudaGetLastError();
+		cudaStreamSynchronize(stream);
+		return nullptr;
+	}
+	return m;
+}
+
+bool StreamMark::Done() const {
+	const cudaError_t e = cudaEventQuery(ev_);
+	if (e == cudaErrorNotReady) cudaGetLastError();  // a status, not an error: leave none behind
+	return e != cudaErrorNotReady;
+}
+
+void ReaderMarks::Add(const std::shared_ptr<StreamMark> &m) {
+	if (!m) return;
+	std::lock_guard<std::mutex> lock(mu_);
+	marks_.erase(std::remove_if(marks_.begin(), marks_.end(), [](const std::shared_ptr<StreamMark> &r) { return r->Done(); }),
+	             marks_.end());
+	marks_.push_back(m);
+}
+
+void ReaderMarks::WaitAll(cudaStream_t stream) {
+	std::lock_guard<std::mutex> lock(mu_);
+	for (auto &m : marks_) m->WaitOn(stream);
+	marks_.clear();
+}
+
 } // namespace vgpu

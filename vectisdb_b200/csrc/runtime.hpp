@@ -80,6 +80,44 @@ private:
 	std::unordered_map<void *, size_t> sizes_;
 };
 
+// ---- Reader marks -------------------------------------------------------------------------------
+//! An event recorded on a stream after the last kernel of one execution that read long-lived device
+//! buffers (committed cache columns, kept join tables). The free of such a buffer is enqueued on the
+//! runtime's stream after a wait on every mark its readers left, so it is ordered after their kernels
+//! without synchronizing the device or the readers' streams.
+class StreamMark {
+public:
+	StreamMark() = default;
+	StreamMark(const StreamMark &) = delete;
+	StreamMark &operator=(const StreamMark &) = delete;
+	~StreamMark() {
+		if (ev_) cudaEventDestroy(ev_);  // a wait already enqueued on it still holds
+	}
+	//! A mark after the work enqueued on `stream` so far; nullptr when no event could be made, in which
+	//! case `stream` has been synchronized instead (the reads are then over).
+	static std::shared_ptr<StreamMark> After(cudaStream_t stream);
+	//! True once the marked work has finished (a not-ready query leaves no error behind).
+	bool Done() const;
+	void WaitOn(cudaStream_t stream) const {
+		cudaStreamWaitEvent(stream, ev_, 0);
+	}
+
+private:
+	cudaEvent_t ev_ = nullptr;
+};
+
+//! Marks of the executions that read one buffer; finished marks are dropped as new ones arrive.
+class ReaderMarks {
+public:
+	void Add(const std::shared_ptr<StreamMark> &m);
+	//! Enqueues on `stream` a wait for every reader still marked.
+	void WaitAll(cudaStream_t stream);
+
+private:
+	std::mutex mu_;
+	std::vector<std::shared_ptr<StreamMark>> marks_;
+};
+
 // ---- Per-execution arena -----------------------------------------------------------------------
 //! Every temporary one execution allocates, released stream-ordered when the execution ends (so the
 //! release needs no device synchronization). `Release` hands a buffer's ownership to the caller.
