@@ -7,7 +7,8 @@
 //   - COUNT(*) -> BIGINT; MIN/MAX keep the input type; SUM over BIGINT/DECIMAL(18,2) is exact and
 //     128-bit (DECIMAL(38,2)); SUM/AVG over DOUBLE accumulate in double (order-dependent, compared
 //     within 1e-12 relative); BIGINT % truncates toward zero (C semantics).
-//   - INNER equi-join emits each matching (left, right) pair once; cross product is left-major.
+//   - INNER equi-join emits each matching (left, right) pair once (a build key repeated r times pairs
+//     every matching probe row r times); cross product is left-major.
 // Built with -ffp-contract=off so v*2+1 rounds twice, as DuckDB (and the engine, --fmad=false) do.
 //
 // Reference anchors: the aggregate rules follow cuda_engine/src/operators/gpu_groupby.cu:24-37 and
@@ -194,39 +195,71 @@ int64_t oracle_c1(const int32_t *a, const int32_t *b, const int64_t *amt, const 
 	return static_cast<int64_t>(all.size());
 }
 
-// SELECT b.g, SUM(p.x) FROM probe p JOIN build b ON p.key = b.key GROUP BY b.g
-// Sort-merge: build side sorted by key, each probe row binary-searches its equal range.
-// Outputs sorted by g.
+// SELECT b.g, SUM(p.x), COUNT(*) FROM probe p JOIN build b ON p.key = b.key GROUP BY b.g
+// A hash join, as DuckDB's CPU plan runs it: the build side goes into an open-addressing table (linear
+// probing, duplicate keys kept as separate entries), each probe row walks its run of the table and
+// emits one pair per equal key, so a build key that repeats r times counts the probe row r times.
+// Per-thread partial aggregates in row order, merged in thread order. Outputs sorted by g.
 int64_t oracle_c2(const int64_t *bkey, const int32_t *bg, uint64_t bn, const int64_t *pkey, const double *px,
                   uint64_t pn, int32_t *out_g, double *out_sum, int64_t *out_cnt, uint64_t capacity) {
-	std::vector<std::pair<int64_t, int32_t>> build(bn);
-#pragma omp parallel for schedule(static)
-	for (int64_t i = 0; i < static_cast<int64_t>(bn); i++) build[i] = {bkey[i], bg[i]};
-	std::sort(build.begin(), build.end(),
-	          [](const auto &x, const auto &y) { return x.first < y.first; });
+	uint64_t slots = 16;
+	while (slots < 2 * bn) slots <<= 1;
+	const uint64_t mask = slots - 1;
+	std::vector<int64_t> tkey(slots);
+	std::vector<int32_t> tg(slots);
+	std::vector<uint8_t> used(slots, 0);
+	for (uint64_t i = 0; i < bn; i++) {
+		uint64_t h = Mix(static_cast<uint64_t>(bkey[i])) & mask;
+		while (used[h]) h = (h + 1) & mask;
+		used[h] = 1;
+		tkey[h] = bkey[i];
+		tg[h] = bg[i];
+	}
+	int32_t gmin = INT32_MAX, gmax = INT32_MIN;
+	for (uint64_t i = 0; i < bn; i++) {
+		gmin = std::min(gmin, bg[i]);
+		gmax = std::max(gmax, bg[i]);
+	}
 	const int T = omp_get_max_threads();
+	const bool dense = bn > 0 && static_cast<int64_t>(gmax) - gmin < (1 << 20);
+	const uint64_t G = dense ? static_cast<uint64_t>(static_cast<int64_t>(gmax) - gmin + 1) : 0;
+	std::vector<std::vector<double>> dsum(T, std::vector<double>(G, 0.0));
+	std::vector<std::vector<int64_t>> dcnt(T, std::vector<int64_t>(G, 0));
 	std::vector<std::unordered_map<int32_t, std::pair<double, int64_t>>> partial(T);
 #pragma omp parallel
 	{
-		auto &m = partial[omp_get_thread_num()];
+		const int t = omp_get_thread_num();
+		auto &m = partial[t];
+		auto &ds = dsum[t];
+		auto &dc = dcnt[t];
 #pragma omp for schedule(static)
 		for (int64_t i = 0; i < static_cast<int64_t>(pn); i++) {
 			const int64_t key = pkey[i];
-			auto lo = std::lower_bound(build.begin(), build.end(), key,
-			                           [](const auto &e, int64_t k) { return e.first < k; });
-			for (auto it = lo; it != build.end() && it->first == key; ++it) {
-				auto &s = m[it->second];
-				s.first += px[i];
-				s.second += 1;
+			for (uint64_t h = Mix(static_cast<uint64_t>(key)) & mask; used[h]; h = (h + 1) & mask) {
+				if (tkey[h] != key) continue;
+				if (dense) {
+					ds[tg[h] - gmin] += px[i];
+					dc[tg[h] - gmin] += 1;
+				} else {
+					auto &st = m[tg[h]];
+					st.first += px[i];
+					st.second += 1;
+				}
 			}
 		}
 	}
 	std::unordered_map<int32_t, std::pair<double, int64_t>> merged;
-	for (auto &m : partial) {
-		for (auto &kv : m) {
-			auto &s = merged[kv.first];
-			s.first += kv.second.first;
-			s.second += kv.second.second;
+	for (int t = 0; t < T; t++) {
+		for (uint64_t j = 0; j < G; j++) {
+			if (dcnt[t][j] == 0) continue;
+			auto &st = merged[static_cast<int32_t>(gmin + static_cast<int64_t>(j))];
+			st.first += dsum[t][j];
+			st.second += dcnt[t][j];
+		}
+		for (auto &kv : partial[t]) {
+			auto &st = merged[kv.first];
+			st.first += kv.second.first;
+			st.second += kv.second.second;
 		}
 	}
 	std::vector<int32_t> keys;

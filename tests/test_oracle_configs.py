@@ -86,3 +86,19 @@ def test_c2_probe_hit_fraction():
     pkey = wl.inputs[0].data
     hits = np.mean(pkey < (1 << 14))
     assert 0.88 < hits < 0.92
+
+
+def test_c2_oracle_with_repeated_build_keys_matches_plan_oracle():
+    """Build keys that repeat (each key twice, some three times): every probe row pairs with every equal
+    build row, as DuckDB's join does."""
+    wl = W.c2(probe_n=40_000, build_n=2048, miss_lo=2048, miss_span=2048)
+    pkey, x, bkey, g = [c.data for c in wl.inputs]
+    rng = np.random.default_rng(8)
+    bkey2 = np.concatenate([bkey, bkey, bkey[:300]])
+    g2 = rng.integers(0, 64, len(bkey2)).astype(np.int32)
+    exp = O.c2(bkey2, g2, pkey, x)
+    from vectisdb_b200.engine import GpuValueType as T, make_column
+    got = _by_key(evaluate(wl.plan, [make_column("pkey", T.INT64, pkey), make_column("x", T.FLOAT64, x),
+                                     make_column("bkey", T.INT64, bkey2), make_column("g", T.INT32, g2)]), 1)
+    assert np.array_equal(exp["g"], got[0])
+    assert np.allclose(exp["sum"], got[1], rtol=1e-12, atol=0)
