@@ -106,6 +106,39 @@ int64_t oracle_c0(const int32_t *k, const double *v, const int64_t *w, uint64_t 
 	return static_cast<int64_t>(keys.size());
 }
 
+// SELECT k, v*2+1, w FROM t WHERE v < v_lt AND w % w_mod <> 0 -- the filter and projection alone,
+// passing rows in input order (the reference's stable compaction, gpu_executor.cu:645-746).
+// Pass out_k == nullptr to only count. Returns the passing row count.
+int64_t oracle_cp(const int32_t *k, const double *v, const int64_t *w, uint64_t n, double v_lt, int64_t w_mod,
+                  int32_t *out_k, double *out_v, int64_t *out_w, uint64_t capacity) {
+	const int T = omp_get_max_threads();
+	std::vector<uint64_t> start(static_cast<size_t>(T) + 1, 0);
+#pragma omp parallel
+	{
+		const int t = omp_get_thread_num();
+		const uint64_t lo = n * t / T, hi = n * (t + 1) / T;
+		uint64_t c = 0;
+		for (uint64_t i = lo; i < hi; i++) c += (v[i] < v_lt && (w[i] % w_mod) != 0);
+		start[t + 1] = c;
+#pragma omp barrier
+#pragma omp single
+		for (int j = 0; j < T; j++) start[j + 1] += start[j];
+		if (out_k != nullptr && start[T] <= capacity) {
+			uint64_t pos = start[t];
+			for (uint64_t i = lo; i < hi; i++) {
+				if (v[i] < v_lt && (w[i] % w_mod) != 0) {
+					out_k[pos] = k[i];
+					out_v[pos] = v[i] * 2.0 + 1.0;
+					out_w[pos] = w[i];
+					pos++;
+				}
+			}
+		}
+	}
+	if (out_k != nullptr && start[T] > capacity) return -1;
+	return static_cast<int64_t>(start[T]);
+}
+
 // SELECT a, b, SUM(amt), AVG(v), COUNT(*), MAX(ts) FROM t WHERE ts > ts_gt GROUP BY a, b
 // Radix-partitioned hash aggregation. Outputs sorted by (a, b); SUM(amt) as (lower, upper) halves.
 int64_t oracle_c1(const int32_t *a, const int32_t *b, const int64_t *amt, const double *v, const int64_t *ts,

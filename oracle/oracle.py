@@ -37,6 +37,8 @@ def lib() -> C.CDLL:
         L.oracle_c2.argtypes = [vp, vp, u64, vp, vp, u64, vp, vp, vp, u64]
         L.oracle_c2.restype = i64
         L.oracle_c2b.argtypes = [vp, u64, vp, u64, C.c_int32, vp, vp, u64]
+        L.oracle_cp.argtypes = [vp, vp, vp, u64, C.c_double, i64, vp, vp, vp, u64]
+        L.oracle_cp.restype = i64
         L.oracle_c2b.restype = i64
         L.oracle_threads.restype = C.c_int
         L.oracle_set_threads.argtypes = [C.c_int]
@@ -66,6 +68,15 @@ def c0(k, v, w, v_lt=0.5, w_mod=7, capacity=None):
     if g < 0:
         raise RuntimeError("oracle c0: capacity too small")
     return {key: val[:g] for key, val in out.items()}
+
+
+def cp(k, v, w, v_lt=0.5, w_mod=7):
+    """-> dict(k, v, w): the passing rows of the filter, projected (v*2+1), in input order."""
+    L = lib()
+    n = L.oracle_cp(_p(k), _p(v), _p(w), len(k), v_lt, w_mod, None, None, None, 0)
+    out = {"k": np.empty(max(n, 1), "<i4"), "v": np.empty(max(n, 1), "<f8"), "w": np.empty(max(n, 1), "<i8")}
+    L.oracle_cp(_p(k), _p(v), _p(w), len(k), v_lt, w_mod, _p(out["k"]), _p(out["v"]), _p(out["w"]), n)
+    return {key: val[:n] for key, val in out.items()}
 
 
 def c1(a, b, amt, v, ts, ts_gt, capacity=None):

@@ -102,3 +102,14 @@ def test_c2_oracle_with_repeated_build_keys_matches_plan_oracle():
                                      make_column("bkey", T.INT64, bkey2), make_column("g", T.INT32, g2)]), 1)
     assert np.array_equal(exp["g"], got[0])
     assert np.allclose(exp["sum"], got[1], rtol=1e-12, atol=0)
+
+
+def test_cp_oracle_matches_plan_oracle():
+    wl = W.cp(n=100_000)
+    k, v, w = [c.data for c in wl.inputs]
+    exp = O.cp(k, v, w, 0.5, 7)
+    got = evaluate(wl.plan, wl.inputs)
+    assert len(got[0].data) == len(exp["k"]) > 0
+    assert np.array_equal(exp["k"], got[0].data)
+    assert np.array_equal(exp["v"], got[1].data)  # v*2+1 rounds twice on both sides: bit-exact
+    assert np.array_equal(exp["w"], got[2].data)

@@ -252,3 +252,42 @@ def c3(n_queries: int = C3_QUERIES, seed: int = 3, min_log2: int = 10, max_log2:
         wl.name = "c3"
         out.append(wl)
     return out
+
+
+def cp_plan(v_lt: float = 0.5, w_mod: int = 7, table: GpuTableRef | None = None) -> GpuPlanNode:
+    """Filter + projection without the GROUP BY: SELECT k, v*2+1, w FROM t WHERE v<v_lt AND w%w_mod<>0."""
+    return c0_plan(v_lt, w_mod, table).children[0]
+
+
+def cp(n: int = C0_ROWS, seed: int = 0, pinned: bool = False, table: str = "c0") -> Workload:
+    """The c0 table under its filter and projection alone (the fused FILTER/PROJECTION chain): 20 input
+    bytes per row, and 20 bytes written per passing row (about 43% pass)."""
+    wl = c0(n=n, seed=seed, pinned=pinned, table=table)
+    wl.name = "cp"
+    wl.plan = cp_plan(0.5, 7, GpuTableRef("memory", "main", table))
+    return wl
+
+
+def c2dup(probe_n: int = C2_PROBE_ROWS, build_n: int = C2_BUILD_ROWS, seed: int = 6, pinned: bool = False,
+          repeat: int = 2) -> Workload:
+    """The c2 join with a build side whose keys repeat: build_n rows holding build_n / repeat distinct keys
+    (a seeded permutation, each key `repeat` times, in shuffled order) with their own g; probe keys drawn
+    like c2's over the distinct keys (90% hits, Zipf(0.8) ranks; 10% misses). Every hit pairs with
+    `repeat` build rows, so the join emits about 0.9 * repeat * probe_n pairs before the GROUP BY."""
+    distinct = build_n // repeat
+    keys = permutation_i64(seed, 0, distinct, pinned=False)
+    order = permutation_i64(seed, 4, build_n, pinned=False)
+    bkey = _alloc(build_n, "<i8", pinned)
+    bkey[:] = np.tile(keys, repeat)[order]
+    g = uniform_i32(seed, 1, build_n, 0, 4096, pinned=pinned)
+    cdf = zipf_cdf(distinct, 0.8)
+    pkey = _alloc(probe_n, "<i8", pinned)
+    datagen().vgdg_probe_keys_i64(seed, 2, 0, probe_n, keys.ctypes.data, cdf.ctypes.data, distinct, 0.9,
+                                  max(1 << 24, build_n), 1 << 24, pkey.ctypes.data)
+    x = uniform_f64(seed, 3, probe_n, pinned=pinned)
+    return Workload("c2dup", c2_plan(GpuTableRef("memory", "main", "c2dup_probe"),
+                                     GpuTableRef("memory", "main", "c2dup_build")),
+                    [make_column("pkey", T.INT64, pkey), make_column("x", T.FLOAT64, x),
+                     make_column("bkey", T.INT64, bkey), make_column("g", T.INT32, g)],
+                    probe_n, 16.0 + 12.0 * build_n / probe_n, {"build_n": build_n, "repeat": repeat},
+                    {"c2dup_probe": ["pkey", "x"], "c2dup_build": ["bkey", "g"]})
