@@ -280,6 +280,12 @@ typedef struct vgpu_working_set {
 int vgpu_is_row_independent(const vgpu_plan *plan);
 /* EstimateWorkingSet (gpu_engine.hpp:341), re-derived for this engine's own allocation sites. */
 vgpu_status vgpu_estimate_working_set(const vgpu_plan *plan, uint64_t max_chunk_rows, vgpu_working_set *out);
+/* The same estimate for one execution with its actual inputs and options (no reference counterpart:
+ * the reference's caller passes the plan alone): rows and widths from `inputs` (or from the cached
+ * columns a cache-served scan reads); scans over cache-served or device-memory columns are borrowed
+ * and charge nothing. The serving admission controller uses it. */
+vgpu_status vgpu_estimate_working_set_for(const vgpu_plan *plan, const vgpu_column *inputs, size_t n_inputs,
+                                          const vgpu_exec_options *options, vgpu_working_set *out);
 
 /* Routing helpers the extension's table checker calls (extension/src/table_checker.cpp:400, 485-499).
  * Plain arithmetic over the plan's advisory fields; no device is touched. */

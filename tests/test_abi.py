@@ -77,10 +77,13 @@ def test_row_independence_and_working_set():
 
 
 def test_working_set_formulas():
-    """The serving admission estimate (csrc/cost_model.cpp), pinned on hand-computed plans: the scan's
-    rows x width; dense outputs plus per-tile counts for a filter; carried record words, output rows and
-    partition offsets for a group-by; widened keys, search/permutation buffers and output for a join;
-    every pair for a cross product. Sizes saturate instead of wrapping."""
+    """The working-set estimate (csrc/cost_model.cpp), pinned on hand-computed plans. It charges what the
+    executor allocates: host scans are copied (rows x width); a FILTER/PROJECTION chain, and a join or
+    cross product under one, is one fused pipeline that allocates only where its rows are materialized
+    (the root, a join's build side); a GROUP BY whose state fits the one-pass strategy allocates per group,
+    otherwise one 32-byte-aligned record per input row plus outputs per group, partition offsets and
+    split-partition tables; a fused join its build-side table, a materializing join its key, search and
+    index buffers and outputs; a root cross product every pair. Sizes saturate instead of wrapping."""
     from vectisdb_b200.engine import (GpuAggregateKind as A, GpuValueType as T, estimate_working_set, make_aggregate,
                                       make_cross_product, make_expr, make_filter, make_group_by, make_join,
                                       make_projection, make_scan)
@@ -90,35 +93,68 @@ def test_working_set_formulas():
     gb = make_group_by(["k"], [make_aggregate(A.SUM, "v", T.FLOAT64), make_aggregate(A.COUNT_STAR, "", T.INT64)], filt)
     ws = estimate_working_set(gb)
     scan_b = 1000 * 20
-    filt_b = 1000 * 20 + 1000 // 256 + 64
-    gb_b = 1000 * (8 + 8) + 1000 * (8 * 3 + 8) + 1 * 2048 * 4  # key + SUM carried; keys+aggs+8 out; offsets
-    assert ws.total_bytes == scan_b + filt_b + gb_b
+    gb_b = 1000 * (2 * 8 + (8 + 8 + 8)) + 64  # one pass: state words (COUNT, SUM) + key/SUM/COUNT outputs
+    assert ws.total_bytes == scan_b + gb_b  # the filter streams into the group-by: nothing of its own
     assert ws.largest_bytes == gb_b and ws.largest_operator == b"GROUP_BY_AGGREGATE" and not ws.chunk_capped
+
+    many = make_scan(["a", "b", "amt", "v", "ts"])
+    many.estimated_rows, many.estimated_row_width_bytes = 1 << 20, 32
+    hc = make_group_by(["a", "b"], [make_aggregate(A.SUM, "amt", T.HUGEINT), make_aggregate(A.AVG, "v", T.FLOAT64),
+                                    make_aggregate(A.COUNT_STAR, "", T.INT64), make_aggregate(A.MAX, "ts", T.INT64)],
+                       many)
+    hc.estimated_rows = 300_000  # groups
+    ws = estimate_working_set(hc)
+    fields = 1 + 2 + 1 + 1  # COUNT, 128-bit SUM, FP64 sum of AVG, MAX
+    hc_b = (1 << 20) * 32 + 300_000 * (16 + 16 + 8 + 8 + 8) + 16384 * 2048 * 4 // 8 + fields * 8 * 4096 * 4 * 148
+    assert ws.total_bytes == (1 << 20) * 32 + hc_b
 
     big = make_scan(["k"])
     big.estimated_rows, big.estimated_row_width_bytes = 1_000_000, 4
     proj = make_projection([make_expr("((int*)out)[idx] = ((const int*)inputs[0])[row];", ["k"], T.INT32)], big)
     ws = estimate_working_set(proj, max_chunk_rows=1000)  # row-independent: charged one chunk at a time
-    assert ws.chunk_capped and ws.total_bytes == 1000 * 4 + (1000 * 8 + 1000 // 256 + 64)
+    assert ws.chunk_capped and ws.total_bytes == 1000 * 4 + (1000 * 4 + 1000 // 256 + 64)
 
     left, right = make_scan(["a", "x"]), make_scan(["b", "g"])
     left.estimated_rows, left.estimated_row_width_bytes = 100, 16
     right.estimated_rows, right.estimated_row_width_bytes = 50, 12
     join = make_join("a", "b", ["a", "x", "g"], left, right)
-    ws = estimate_working_set(join)
+    ws = estimate_working_set(join)  # at the root: materializing
     join_b = 100 * 24 + 50 * 24 + 100 * (3 * 8 + 8)
     assert ws.total_bytes == 1600 + 600 + join_b and ws.largest_operator == b"HASH_JOIN"
+    fused = make_group_by(["g"], [make_aggregate(A.SUM, "x", T.FLOAT64)], make_join("a", "b", ["g", "x"], left, right))
+    ws = estimate_working_set(fused)  # under a group-by: the join is the pipeline's source
+    assert ws.total_bytes == 1600 + 600 + 50 * 32 + (100 * (2 * 8 + 16) + 64)
 
     l2, r2 = make_scan(["a"]), make_scan(["b"])
     l2.estimated_rows, l2.estimated_row_width_bytes = 10, 4
     r2.estimated_rows, r2.estimated_row_width_bytes = 20, 4
     ws = estimate_working_set(make_cross_product(["a", "b"], l2, r2))
     assert ws.total_bytes == 40 + 80 + 200 * 16 and ws.largest_operator == b"CROSS_PRODUCT"
+    pred = make_filter([make_expr("out[idx] = 1;", ["a", "b"], T.BOOLEAN)], make_cross_product(["a", "b"], l2, r2))
+    pred.estimated_rows = 15
+    ws = estimate_working_set(pred)  # the pairs stay virtual; the filter materializes what passes
+    assert ws.total_bytes == 40 + 80 + 15 * 16 + 15 // 256 + 64 and ws.largest_operator == b"FILTER"
 
     huge = make_scan(["k"])
     huge.estimated_rows, huge.estimated_row_width_bytes = 1 << 62, 8
     ws = estimate_working_set(make_filter([make_expr("out[idx] = 1;", ["k"], T.BOOLEAN)], huge))
     assert ws.total_bytes == (1 << 64) - 1
+
+
+def test_working_set_for_inputs_skips_borrowed_scans():
+    """With the execution's actual inputs, a scan over device-memory columns is borrowed (no charge),
+    host columns are copied (rows x width from the inputs, not from the plan's estimates)."""
+    import numpy as np
+    from vectisdb_b200.engine import (GpuColumn, GpuValueType as T, estimate_working_set_for, make_column, make_expr,
+                                      make_projection, make_scan)
+    proj = make_projection([make_expr("((double*)out)[idx] = ((const double*)inputs[0])[row] * 2.0;", ["v"],
+                                      T.FLOAT64)], make_scan(["v"]))
+    host = make_column("v", T.FLOAT64, np.zeros(5000))
+    ws = estimate_working_set_for(proj, [host])
+    assert ws.total_bytes == 5000 * 8 + (5000 * 8 + 5000 // 256 + 64)
+    dev = GpuColumn("v", T.FLOAT64, None, None, 5000, 0x1000)  # a device pointer is only described, never read
+    ws = estimate_working_set_for(proj, [dev])
+    assert ws.total_bytes == 5000 * 8 + 5000 // 256 + 64
 
 
 def test_row_independence_by_operator():

@@ -186,6 +186,8 @@ SIGNATURES = [
                                        C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     ("vgpu_is_row_independent", C.c_int, [C.POINTER(vgpu_plan)]),
     ("vgpu_estimate_working_set", C.c_int, [C.POINTER(vgpu_plan), C.c_uint64, C.POINTER(vgpu_working_set)]),
+    ("vgpu_estimate_working_set_for", C.c_int, [C.POINTER(vgpu_plan), C.POINTER(vgpu_column), C.c_size_t,
+                                                 C.POINTER(vgpu_exec_options), C.POINTER(vgpu_working_set)]),
     ("vgpu_analyze_plan_shape", C.c_int, [C.POINTER(vgpu_plan), C.POINTER(vgpu_plan_shape)]),
     ("vgpu_estimate_columns_size", C.c_int, [C.POINTER(vgpu_plan), C.POINTER(C.c_uint64)]),
     ("vgpu_determine_execution_mode", C.c_int, [C.POINTER(vgpu_plan), C.c_uint64, C.c_double,

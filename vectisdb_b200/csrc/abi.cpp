@@ -670,6 +670,16 @@ vgpu_status vgpu_estimate_working_set(const vgpu_plan *plan, uint64_t max_chunk_
 	});
 }
 
+vgpu_status vgpu_estimate_working_set_for(const vgpu_plan *plan, const vgpu_column *inputs, size_t n_inputs,
+                                          const vgpu_exec_options *options, vgpu_working_set *out) {
+	return Guard([&] {
+		if (!out || (n_inputs && !inputs)) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		auto root = ConvertPlan(plan);
+		std::vector<vgpu_column> in(inputs, inputs + n_inputs);
+		*out = EstimateWorkingSetFor(*root, in, options && options->serve_whole_scan_from_cache);
+	});
+}
+
 vgpu_status vgpu_analyze_plan_shape(const vgpu_plan *plan, vgpu_plan_shape *out) {
 	return Guard([&] {
 		if (!out) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");

@@ -6,6 +6,7 @@
 #include <cstring>
 
 #include "codegen.hpp"
+#include "column_cache.hpp"
 
 namespace vgpu {
 
@@ -25,10 +26,22 @@ uint64_t SatMul(uint64_t a, uint64_t b) {
 	return a > UINT64_MAX / b ? UINT64_MAX : a * b;
 }
 
+// Byte width of one value of a plan-level type (HUGEINT sums are 16 bytes, key types unknown here
+// count as 8).
+uint64_t ValueBytes(ValueType t) {
+	return TypeSize(t);
+}
+
+// Walk of the plan that charges what this engine's executor allocates for it (its arena and the result
+// buffers), operator by operator. A FILTER / PROJECTION chain, and a join or cross product under one,
+// is one fused kernel pipeline: it allocates only where its rows are materialized -- at the plan's root,
+// or as the right (build) side of a join -- while under a GROUP BY it streams straight into the
+// aggregation and allocates nothing per row.
 struct Walker {
 	uint64_t cap = 0;
 	const std::vector<uint64_t> *scan_rows;
 	const std::vector<uint32_t> *scan_widths;
+	const std::vector<bool> *scan_resident;
 	size_t scan_index = 0;
 	vgpu_working_set ws {};
 
@@ -40,8 +53,7 @@ struct Walker {
 		}
 	}
 
-	uint64_t Rows(const PlanNode &n, uint64_t fallback) {
-		uint64_t r = n.estimated_rows ? n.estimated_rows : fallback;
+	uint64_t Capped(uint64_t r) {
 		if (cap && r > cap) {
 			ws.chunk_capped = 1;
 			r = cap;
@@ -49,68 +61,101 @@ struct Walker {
 		return r;
 	}
 
-	Estimate Walk(const PlanNode &n) {
+	// `materialize`: this node's rows become device columns (the root, a join's build side, a cross
+	// product's sides); otherwise they stream into the pipeline above.
+	Estimate Walk(const PlanNode &n, bool materialize) {
 		Estimate e;
 		switch (n.op) {
 		case OpType::SCAN: {
 			uint64_t rows = n.estimated_rows;
 			uint64_t width = n.estimated_row_width_bytes ? n.estimated_row_width_bytes : 8 * n.column_names.size();
+			bool resident = false;
 			if (scan_rows && scan_index < scan_rows->size()) rows = (*scan_rows)[scan_index];
 			if (scan_widths && scan_index < scan_widths->size()) width = (*scan_widths)[scan_index];
+			if (scan_resident && scan_index < scan_resident->size()) resident = (*scan_resident)[scan_index];
 			scan_index++;
-			if (cap && rows > cap) {
-				ws.chunk_capped = 1;
-				rows = cap;
-			}
-			e.rows = rows;
+			e.rows = Capped(rows);
 			e.width = width;
-			Charge("SCAN", SatMul(rows, width));
+			// host columns are copied to the device; resident ones (cache-served, device inputs) are borrowed
+			if (!resident) Charge("SCAN", SatMul(e.rows, width));
 			return e;
 		}
 		case OpType::FILTER:
 		case OpType::PROJECTION: {
-			Estimate c = n.children.empty() ? Estimate {} : Walk(*n.children[0]);
+			Estimate c = n.children.empty() ? Estimate {} : Walk(*n.children[0], false);
 			e.rows = c.rows;
-			e.width = n.op == OpType::PROJECTION ? 8 * std::max<size_t>(1, n.expressions.size()) : c.width;
-			// dense outputs plus per-tile counts
-			Charge(n.op == OpType::FILTER ? "FILTER" : "PROJECTION", SatAdd(SatMul(e.rows, e.width), e.rows / 256 + 64));
+			if (n.op == OpType::FILTER && n.estimated_rows) e.rows = std::min(c.rows, Capped(n.estimated_rows));
+			if (n.op == OpType::PROJECTION) {
+				e.width = 0;
+				for (auto &x : n.expressions) e.width += ValueBytes(x.output_type);
+				if (e.width == 0) e.width = 8;
+			} else {
+				e.width = c.width;
+			}
+			if (materialize) {  // dense outputs plus per-tile counts of the compaction
+				Charge(n.op == OpType::FILTER ? "FILTER" : "PROJECTION", SatAdd(SatMul(e.rows, e.width), e.rows / 256 + 64));
+			}
 			return e;
 		}
 		case OpType::GROUP_BY_AGGREGATE: {
-			Estimate c = n.children.empty() ? Estimate {} : Walk(*n.children[0]);
-			const uint64_t out_width = 8 * (n.group_keys.size() + n.aggregates.size()) + 8;
-			// partitioned strategy: packed key + carried values per row, bucket outputs sized by rows
-			uint64_t carried = 8;
+			Estimate c = n.children.empty() ? Estimate {} : Walk(*n.children[0], false);
+			// state words per group: COUNT, then one per FP64 sum / MIN / MAX and two per integer sum
+			uint64_t fields = 1, carried = 8, out_width = 8 * n.group_keys.size();
 			for (auto &a : n.aggregates) {
-				if (a.kind != AggKind::COUNT && a.kind != AggKind::COUNT_STAR) carried += 8;
+				out_width += ValueBytes(a.output_type);
+				if (a.kind == AggKind::COUNT || a.kind == AggKind::COUNT_STAR) continue;
+				carried += 8;
+				const bool int_sum = (a.kind == AggKind::SUM || a.kind == AggKind::AVG) && a.output_type == ValueType::HUGEINT;
+				fields += int_sum ? 2 : 1;
 			}
-			uint64_t bytes = SatAdd(SatMul(c.rows, carried), SatMul(c.rows, out_width));
-			// partition offsets: (partitions <= 2^14, about one per 1024 rows) x (CTAs <= 2048) x 4 B
-			bytes = SatAdd(bytes, SatMul(std::min<uint64_t>(16384, std::max<uint64_t>(1, c.rows / 1024)), 2048ull * 4));
-			e.rows = n.estimated_rows ? n.estimated_rows : c.rows;
+			const uint64_t groups = n.estimated_rows ? std::min(c.rows, n.estimated_rows) : c.rows;
+			uint64_t bytes;
+			if (SatMul(groups, fields * 8) <= 96 * 1024) {
+				// one pass: per-CTA shared tables, one global table over the key domain, outputs
+				bytes = SatAdd(SatMul(groups, fields * 8 + out_width), 64);
+			} else {
+				// partitioned: one record per passing row (packed key + carried values, 32-byte aligned),
+				// outputs per group, per-(partition, CTA) offsets, tables of split partitions
+				const uint64_t record = (carried + 31) / 32 * 32;
+				bytes = SatMul(c.rows, record);
+				bytes = SatAdd(bytes, SatMul(groups, out_width));
+				bytes = SatAdd(bytes, 16384ull * 2048 * 4 / 8);
+				bytes = SatAdd(bytes, SatMul(fields * 8 * 4096, 4 * 148));
+			}
+			e.rows = groups;
 			e.width = out_width;
 			Charge("GROUP_BY_AGGREGATE", bytes);
 			return e;
 		}
 		case OpType::HASH_JOIN: {
-			Estimate l = n.children.size() > 0 ? Walk(*n.children[0]) : Estimate {};
-			Estimate r = n.children.size() > 1 ? Walk(*n.children[1]) : Estimate {};
-			// widened keys + search results (left), widened keys + permutation + sort buffers (right)
-			uint64_t bytes = SatAdd(SatMul(l.rows, 24), SatMul(r.rows, 24));
-			const uint64_t out_rows = Rows(n, std::max(l.rows, r.rows));
+			Estimate l = n.children.size() > 0 ? Walk(*n.children[0], !materialize ? false : true) : Estimate {};
+			Estimate r = n.children.size() > 1 ? Walk(*n.children[1], true) : Estimate {};
 			const uint64_t out_width = 8 * std::max<size_t>(1, n.output_columns.size());
-			bytes = SatAdd(bytes, SatMul(out_rows, out_width + 8));
-			e.rows = out_rows;
+			uint64_t bytes;
+			if (!materialize) {
+				// the join as a pipeline source: right keys widened, their range, a dense table (at most
+				// 8 bytes per key of the range) or sorted keys with a radix directory
+				bytes = SatMul(r.rows, 32);
+				e.rows = n.estimated_rows ? Capped(n.estimated_rows) : l.rows;
+			} else {
+				// materializing: both sides' keys widened, the right side sorted with a permutation and
+				// its double buffers, per-left-row ranges, one index pair and the output columns per match
+				const uint64_t out_rows = n.estimated_rows ? Capped(n.estimated_rows) : std::max(l.rows, r.rows);
+				bytes = SatAdd(SatMul(l.rows, 24), SatMul(r.rows, 24));
+				bytes = SatAdd(bytes, SatMul(out_rows, out_width + 8));
+				e.rows = out_rows;
+			}
 			e.width = out_width;
 			Charge("HASH_JOIN", bytes);
 			return e;
 		}
 		case OpType::CROSS_PRODUCT: {
-			Estimate l = n.children.size() > 0 ? Walk(*n.children[0]) : Estimate {};
-			Estimate r = n.children.size() > 1 ? Walk(*n.children[1]) : Estimate {};
+			Estimate l = n.children.size() > 0 ? Walk(*n.children[0], true) : Estimate {};
+			Estimate r = n.children.size() > 1 ? Walk(*n.children[1], true) : Estimate {};
 			e.rows = SatMul(l.rows, r.rows);
 			e.width = 8 * std::max<size_t>(1, n.output_columns.size());
-			Charge("CROSS_PRODUCT", SatMul(e.rows, e.width));
+			// a virtual pair space under a pipeline; materialized only at the root
+			if (materialize) Charge("CROSS_PRODUCT", SatMul(e.rows, e.width));
 			return e;
 		}
 		}
@@ -122,14 +167,49 @@ struct Walker {
 
 vgpu_working_set EstimateWorkingSet(const PlanNode &plan, uint64_t max_chunk_rows,
                                     const std::vector<uint64_t> *scan_rows,
-                                    const std::vector<uint32_t> *scan_widths) {
+                                    const std::vector<uint32_t> *scan_widths,
+                                    const std::vector<bool> *scan_resident) {
 	Walker w;
 	w.cap = IsRowIndependent(plan) ? max_chunk_rows : 0;
 	w.scan_rows = scan_rows;
 	w.scan_widths = scan_widths;
+	w.scan_resident = scan_resident;
 	std::memset(&w.ws, 0, sizeof(w.ws));
-	w.Walk(plan);
+	w.Walk(plan, true);
 	return w.ws;
+}
+
+vgpu_working_set EstimateWorkingSetFor(const PlanNode &plan, const std::vector<vgpu_column> &inputs,
+                                       bool serve_from_cache) {
+	std::vector<const PlanNode *> scans;
+	CollectScans(plan, scans);
+	std::vector<uint64_t> rows;
+	std::vector<uint32_t> widths;
+	std::vector<bool> resident;
+	size_t cursor = 0;
+	for (auto *scan : scans) {
+		uint64_t r = 0;
+		uint32_t w = 0;
+		bool res = true;
+		for (auto &name : scan->column_names) {
+			if (serve_from_cache) {
+				DevColumn col;
+				if (ColumnCache::Get().GetWhole(scan->table, name, col)) {
+					r = col.rows;
+					w += static_cast<uint32_t>(TypeSize(col.type));
+				}
+			} else if (cursor < inputs.size()) {
+				const vgpu_column &in = inputs[cursor++];
+				r = in.row_count;
+				if (IsValidValueType(in.type)) w += static_cast<uint32_t>(TypeSize(static_cast<ValueType>(in.type)));
+				if (in.memory != VGPU_MEM_DEVICE) res = false;
+			}
+		}
+		rows.push_back(r);
+		widths.push_back(w);
+		resident.push_back(res);
+	}
+	return EstimateWorkingSet(plan, 0, &rows, &widths, &resident);
 }
 
 namespace {

@@ -10,11 +10,21 @@
 
 namespace vgpu {
 
-//! Row counts come from each SCAN's input (`scan_rows`, traversal order) when given, else from the
-//! nodes' estimated_rows. Chunk-capped when the plan is row-independent and max_chunk_rows > 0.
+//! Row counts and widths come from each SCAN's input (`scan_rows`, `scan_widths`, traversal order) when
+//! given, else from the nodes' estimated_rows / estimated_row_width_bytes; a SCAN marked in
+//! `scan_resident` (cache-served or device-memory inputs) is borrowed, not copied, and charges nothing.
+//! A GROUP BY's estimated_rows is its group count. Chunk-capped when the plan is row-independent and
+//! max_chunk_rows > 0.
 vgpu_working_set EstimateWorkingSet(const PlanNode &plan, uint64_t max_chunk_rows,
                                     const std::vector<uint64_t> *scan_rows = nullptr,
-                                    const std::vector<uint32_t> *scan_widths = nullptr);
+                                    const std::vector<uint32_t> *scan_widths = nullptr,
+                                    const std::vector<bool> *scan_resident = nullptr);
+
+//! The estimate for one execution with its actual inputs and options: rows and widths from the
+//! inputs (or the cached columns a cache-served scan reads), SCANs over cache-served or device-memory
+//! columns charging nothing.
+vgpu_working_set EstimateWorkingSetFor(const PlanNode &plan, const std::vector<vgpu_column> &inputs,
+                                       bool serve_from_cache);
 
 //! Work-to-data ratio of a plan from its advisory fields (the reference's AnalyzePlanShape,
 //! cuda_engine/include/gpu_engine.hpp:284-329): the routing input of the extension's table checker.

@@ -63,31 +63,8 @@ Server::~Server() {
 }
 
 uint64_t Server::Estimate(const PlanNode &plan, const std::vector<vgpu_column> &inputs, const ExecOptions &options) {
-	std::vector<const PlanNode *> scans;
-	CollectScans(plan, scans);
-	std::vector<uint64_t> rows;
-	std::vector<uint32_t> widths;
-	size_t cursor = 0;
-	for (auto *scan : scans) {
-		uint64_t r = 0;
-		uint32_t w = 0;
-		for (auto &name : scan->column_names) {
-			if (options.serve_whole_scan_from_cache) {
-				DevColumn col;
-				if (ColumnCache::Get().GetWhole(scan->table, name, col)) {
-					r = col.rows;
-					w += static_cast<uint32_t>(TypeSize(col.type));
-				}
-			} else if (cursor < inputs.size()) {
-				const vgpu_column &in = inputs[cursor++];
-				r = in.row_count;
-				if (IsValidValueType(in.type)) w += static_cast<uint32_t>(TypeSize(static_cast<ValueType>(in.type)));
-			}
-		}
-		rows.push_back(r);
-		widths.push_back(w);
-	}
-	return EstimateWorkingSet(plan, 0, &rows, &widths).total_bytes;
+	// what the execution allocates: cache-served and device-memory columns are borrowed, not copied
+	return EstimateWorkingSetFor(plan, inputs, options.serve_whole_scan_from_cache).total_bytes;
 }
 
 uint64_t Server::Submit(std::shared_ptr<PlanNode> plan, std::vector<vgpu_column> inputs, const ExecOptions &options) {

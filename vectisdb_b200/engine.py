@@ -775,6 +775,21 @@ def estimate_working_set(plan: GpuPlanNode, max_chunk_rows: int = 0) -> abi.vgpu
     return ws
 
 
+def estimate_working_set_for(plan: GpuPlanNode, inputs: Sequence[GpuColumn],
+                             options: "ExecuteOptions | None" = None) -> abi.vgpu_working_set:
+    """The working-set estimate of one execution with these inputs and options: scans over cache-served
+    or device-memory columns are borrowed and charge nothing."""
+    keep = _Keep()
+    ws = abi.vgpu_working_set()
+    opts = abi.vgpu_exec_options()
+    abi.lib().vgpu_exec_options_init(C.byref(opts))
+    opts.serve_whole_scan_from_cache = int(bool(options and options.serve_whole_scan_from_cache))
+    cols = serialize_inputs(inputs, keep)
+    abi.check(abi.lib().vgpu_estimate_working_set_for(C.byref(serialize_plan(plan, keep)), cols, len(inputs),
+                                                      C.byref(opts), C.byref(ws)))
+    return ws
+
+
 def memory_stats() -> dict:
     """The engine allocator's budget, bytes in use, peak, allocation and failure counts."""
     s = abi.vgpu_memory_stats()
