@@ -109,3 +109,18 @@ def test_stream_pipeline_supports_projection_chains_only():
                        scan)
     assert not StreamPipeline.supports(filt)
     assert not StreamPipeline.supports(scan)
+
+
+def test_join_source_kernels_compile_single_and_multi_match():
+    """The join + group-by query's fused kernels, for a unique-key right side and for repeated keys
+    (each probe row expands into its run of matches): materialization, key statistics and the
+    one-pass group-by all compile; right columns are never read at left row positions."""
+    wl = W.c2(probe_n=64, build_n=16, miss_lo=16, miss_span=16)
+    src = generate_source(wl.plan, wl.inputs)
+    tus = src.split("//@@VGPU_TU@@")
+    assert len(tus) == 5
+    assert "vgpu_join_find" in tus[0] and "vgpu_join_run" in tus[1] and "vgpu_join_run" in tus[4]
+    assert "for (u32 jx_ = 0; jx_ < jn_; ++jx_)" in tus[4]
+    # the right column g (source 0) is loaded only through the lookup, never by load_rows at row0
+    assert "load_rows<int, 8>((const int*)a.w[2]" not in tus[3] and "load_rows<int, 8>((const int*)a.w[2]" not in tus[4]
+    assert all(s > 1000 for s in _compile_all(src))

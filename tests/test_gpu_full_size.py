@@ -85,7 +85,7 @@ def test_c2_at_full_size_fused_join():
     wl = W.c2()
     assert wl.rows == 1 << 28 and wl.params["build_n"] == 1 << 24
     (gg, gs), launched = _run_resident(wl)
-    assert "join_dense_table" in launched and "join_search" not in launched, sorted(launched)
+    assert "join_dense_table" in launched and "join_expand" not in launched, sorted(launched)
     pkey, x, bkey, g = [c.data for c in wl.inputs]
     exp = O.c2(bkey, g, pkey, x)
     order = np.argsort(gg)

@@ -214,3 +214,92 @@ def test_join_table_kept_across_queries_until_invalidated():
     finally:
         ColumnCache.invalidate_table(t_b)
         ColumnCache.invalidate_table(t_p)
+
+
+def _launched(fn):
+    from vectisdb_b200.engine import profile_drain, profile_enable
+    profile_enable(True)
+    profile_drain()
+    try:
+        out = fn()
+        names = [k for k, _, _, _ in profile_drain()]
+    finally:
+        profile_enable(False)
+    return out, names
+
+
+def test_repeated_build_keys_fuse_into_the_group_by():
+    """The join + group-by with every build key repeated (the c2 shape with two build rows per key):
+    each probe row expands into its run of matches inside the group-by kernel -- no match pairs are
+    materialized -- and the result equals the oracle's hash join."""
+    wl = W.c2dup(probe_n=1 << 22, build_n=1 << 20)
+    pkey, x, bkey, g = [c.data for c in wl.inputs]
+    (gg, gs), names = _launched(lambda: [c.data for c in _run(wl.plan, wl.inputs)])
+    assert "max_run_length" in names and "join_runs" not in names and "join_expand" not in names, names
+    exp = O.c2(bkey, g, pkey, x)
+    order = np.argsort(gg)
+    assert np.array_equal(gg[order], exp["g"])
+    assert _close(gs[order], exp["sum"])
+
+
+@pytest.mark.parametrize("repeat", [2, 7])
+def test_filter_over_multi_match_join_keeps_left_then_right_order(repeat):
+    """A filter over a join whose right keys repeat: outputs are left-major, and a left row's matches
+    follow the right side's original order (the stable sort), as the reference's join emits them."""
+    rng = np.random.default_rng(31 + repeat)
+    base = rng.permutation(np.arange(-3000, 3000, dtype=np.int64))[:2500]
+    rk = np.concatenate([base] * repeat)[rng.permutation(2500 * repeat)]
+    rv = rng.integers(0, 1000, len(rk)).astype(np.int32)
+    lk = rng.integers(-4000, 4000, 50000).astype(np.int64)
+    lv = np.arange(len(lk), dtype=np.int64)
+    join = make_join("lk", "rk", ["lv", "rv"], make_scan(["lk", "lv"]), make_scan(["rk", "rv"]))
+    plan = make_filter([make_expr("((bool*)out)[idx] = (((const int*)inputs[0])[row] % 3) != 1;", ["rv"],
+                                  T.BOOLEAN)], join)
+    cols, names = _launched(lambda: _run(plan, [make_column("lk", T.INT64, lk), make_column("lv", T.INT64, lv),
+                                                make_column("rk", T.INT64, rk), make_column("rv", T.INT32, rv)]))
+    assert "join_expand" not in names, names
+    by_key = {}
+    for i, k in enumerate(rk.tolist()):
+        by_key.setdefault(k, []).append(i)
+    exp_lv, exp_rv = [], []
+    for k, v in zip(lk.tolist(), lv.tolist()):
+        for i in by_key.get(k, ()):
+            if rv[i] % 3 != 1:
+                exp_lv.append(v)
+                exp_rv.append(int(rv[i]))
+    assert np.array_equal(cols[0].data, np.array(exp_lv, np.int64))
+    assert np.array_equal(cols[1].data, np.array(exp_rv, np.int32))
+
+
+def test_multi_match_join_under_a_high_cardinality_group_by():
+    """Grouping a repeated-key join by a key with too many values for the one-pass tables: the matches
+    are expanded into a relation first, then partitioned; exact sums and counts."""
+    rng = np.random.default_rng(12)
+    rk = np.repeat(rng.permutation(200_000).astype(np.int64), 3)
+    rg = rng.integers(0, 1 << 20, len(rk)).astype(np.int32)
+    lk = rng.integers(0, 220_000, 300_000).astype(np.int64)
+    lv = rng.integers(-1000, 1000, len(lk)).astype(np.int64)
+    cols = _run(_join_group_plan(T.INT64), [make_column("lk", T.INT64, lk), make_column("lv", T.INT64, lv),
+                                            make_column("rk", T.INT64, rk), make_column("rg", T.INT32, rg)])
+    from vectisdb_b200.engine import hugeint_to_int
+    sums, counts = _expected_join_group(lk, lv, rk, rg)
+    got = dict(zip(cols[0].data.tolist(), zip(hugeint_to_int(cols[1].data), cols[2].data.tolist())))
+    assert got == {g: (sums[g], counts[g]) for g in counts}
+
+
+def test_very_long_runs_use_the_load_balanced_join():
+    """A right key repeated more than 65536 times is spread over many threads by the materializing
+    join's expansion instead of one thread walking the run."""
+    rk = np.concatenate([np.full(70_000, 5, np.int64), np.arange(10, 1010, dtype=np.int64)])
+    rg = (np.arange(len(rk)) % 17).astype(np.int32)
+    lk = np.array([5, 6, 10, 5, 1009, 2000], np.int64)
+    lv = np.array([1, 2, 3, 4, 5, 6], np.int64)
+    cols, names = _launched(lambda: _run(_join_group_plan(T.INT64), [make_column("lk", T.INT64, lk),
+                                                                      make_column("lv", T.INT64, lv),
+                                                                      make_column("rk", T.INT64, rk),
+                                                                      make_column("rg", T.INT32, rg)]))
+    assert "join_expand" in names, names
+    from vectisdb_b200.engine import hugeint_to_int
+    sums, counts = _expected_join_group(lk, lv, rk, rg)
+    got = dict(zip(cols[0].data.tolist(), zip(hugeint_to_int(cols[1].data), cols[2].data.tolist())))
+    assert got == {g: (sums[g], counts[g]) for g in counts}

@@ -366,19 +366,20 @@ std::string PipelineCodegen::LoadBlock(const Geometry &g, const std::vector<bool
 		if (src.nullable) {
 			o << "\t\tbool sv" << i << "[" << g.items << "];\n";
 		}
-		if (!spec_.cross) {
-			o << "\t\tload_rows<" << t << ", " << g.items << ">((const " << t << "*)a.w[" << w << "], row0, n, s" << i
-			  << ");\n";
-			if (src.nullable) {
-				o << "\t\tload_valid<" << g.items << ">((const u8*)a.w[" << w + 1 << "], row0, n, sv" << i << ");\n";
-			}
-		} else if (spec_.join) {
+		if (spec_.join) {
+			// left columns at the left rows; right columns come from the lookup below
 			if (src.side == 0) {
 				o << "\t\tload_rows<" << t << ", " << g.items << ">((const " << t << "*)a.w[" << w << "], row0, n, s" << i
 				  << ");\n";
 				if (src.nullable) {
 					o << "\t\tload_valid<" << g.items << ">((const u8*)a.w[" << w + 1 << "], row0, n, sv" << i << ");\n";
 				}
+			}
+		} else if (!spec_.cross) {
+			o << "\t\tload_rows<" << t << ", " << g.items << ">((const " << t << "*)a.w[" << w << "], row0, n, s" << i
+			  << ");\n";
+			if (src.nullable) {
+				o << "\t\tload_valid<" << g.items << ">((const u8*)a.w[" << w + 1 << "], row0, n, sv" << i << ");\n";
 			}
 		} else {
 			const char *idx = src.side == 0 ? "li[r]" : "rj[r]";
@@ -398,6 +399,17 @@ std::string PipelineCodegen::LoadBlock(const Geometry &g, const std::vector<bool
 		// keys widen by zero extension of their width, as the sorted side was widened
 		const size_t kw = TypeSize(spec_.sources[key].type);
 		const char *ut = kw == 1 ? "u8" : kw == 2 ? "unsigned short" : kw == 4 ? "u32" : "u64";
+		if (spec_.join_multi) {
+			// the run of equal keys: start and length (0 = no match); the right columns are read per match
+			o << "\t\tlong long jm[" << g.items << "];\n\t\tu32 jc[" << g.items << "];\n"
+			  << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) {\n"
+			  << "\t\t\tu32 c_ = 0u;\n"
+			  << "\t\t\tjm[r] = row0 + r < n ? vgpu_join_run((u64)(" << ut << ")s" << key << "[r] - a.w[" << kJoinWord + 2
+			  << "], (const u64*)a.w[" << kJoinWord << "], (const u32*)a.w[" << kJoinWord + 1 << "], a.w[" << kJoinWord + 3
+			  << "] >> 8, (u32)(a.w[" << kJoinWord + 3 << "] & 0xffu), &c_) : -1ll;\n"
+			  << "\t\t\tjc[r] = c_;\n\t\t}\n";
+			return o.str();
+		}
 		o << "\t\tlong long jm[" << g.items << "];\n"
 		  << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) {\n"
 		  << "\t\t\tjm[r] = row0 + r < n ? vgpu_join_find((u64)(" << ut << ")s" << key << "[r] - a.w[" << kJoinWord + 2
@@ -424,6 +436,33 @@ std::string PipelineCodegen::LoadBlock(const Geometry &g, const std::vector<bool
 	return o.str();
 }
 
+std::string PipelineCodegen::ItemOpen(const Geometry &g, const std::vector<bool> &needed) const {
+	std::ostringstream o;
+	o << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) {\n\t\tconst u64 row = row0 + r; (void)row;\n";
+	if (!spec_.join_multi) {
+		o << "\t\tbool keep = row < n;\n";
+		return o.str();
+	}
+	// one item per match of the row's key, right columns read at the match's sorted position
+	o << "\t\tconst u32 jn_ = (row < n && jm[r] >= 0) ? jc[r] : 0u;\n"
+	  << "\t\tfor (u32 jx_ = 0; jx_ < jn_; ++jx_) {\n"
+	  << "\t\tconst u64 jp_ = (u64)jm[r] + jx_;\n";
+	for (size_t i = 0; i < spec_.sources.size(); i++) {
+		const auto &src = spec_.sources[i];
+		if (!needed[i] || src.side != 1) continue;
+		const char *t = CudaTypeName(src.type);
+		const int w = 2 + 2 * static_cast<int>(i);
+		o << "\t\ts" << i << "[r] = ((const " << t << "*)a.w[" << w << "])[jp_];\n";
+		if (src.nullable) o << "\t\tsv" << i << "[r] = ((const u8*)a.w[" << w + 1 << "])[jp_] != 0;\n";
+	}
+	o << "\t\tbool keep = true;\n";
+	return o.str();
+}
+
+std::string PipelineCodegen::ItemClose() const {
+	return spec_.join_multi ? "\t\t}\n\t\t}\n" : "\t\t}\n";
+}
+
 namespace {
 
 // KArgs word carrying the optional bucket diagnostics buffer (0 = off).
@@ -440,25 +479,43 @@ std::string PipelineCodegen::EmitMaterialize(const std::vector<int> &outs, const
 	std::vector<int> out_cols = outs;
 	auto needed = NeededSources(out_cols);
 	const std::string loads = LoadBlock(g, needed, false);
+	// tile counts and offsets: 32-bit, or 64-bit when a multi-match join source can expand past 2^32 rows
+	const char *cnt_t = spec_.join_multi ? "u64" : "u32";
 	if (has_filter_) {
+		const auto count_needed = NeededSources({});
 		o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_mat_count(KArgs a) {\n"
 		  << kKernelHead << "\t__shared__ u32 scan_scratch[33];\n"
-		  << "\tu32 *tile_counts = (u32*)a.w[" << cb << "];\n"
+		  << "\t" << cnt_t << " *tile_counts = (" << cnt_t << "*)a.w[" << cb << "];\n"
 		  << "\tconst u64 ntiles = (n + " << g.tile() - 1 << ") / " << g.tile() << ";\n"
 		  << "\tfor (u64 tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n"
-		  << LoadBlock(g, NeededSources({}), false) << "\t\tu32 cnt = 0;\n"
-		  << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) {\n"
-		  << "\t\tconst u64 row = row0 + r; (void)row;\n\t\tbool keep = row < n;\n"
-		  << chain_code_ << "\t\tcnt += keep ? 1u : 0u;\n\t\t}\n"
+		  << LoadBlock(g, count_needed, false) << "\t\tu32 cnt = 0;\n"
+		  << ItemOpen(g, count_needed) << chain_code_ << "\t\tcnt += keep ? 1u : 0u;\n" << ItemClose()
 		  << "\t\tu32 total; block_exclusive_scan(cnt, scan_scratch, &total);\n"
 		  << "\t\tif (threadIdx.x == 0) tile_counts[tile] = total;\n\t}\n}\n\n";
 	}
 	o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_mat_write(KArgs a) {\n"
 	  << kKernelHead << "\t__shared__ u32 scan_scratch[33];\n"
-	  << "\tconst u32 *tile_offsets = (const u32*)a.w[" << cb << "]; (void)tile_offsets;\n"
+	  << "\tconst " << cnt_t << " *tile_offsets = (const " << cnt_t << "*)a.w[" << cb << "]; (void)tile_offsets;\n"
 	  << "\tconst u64 ntiles = (n + " << g.tile() - 1 << ") / " << g.tile() << ";\n"
 	  << "\tfor (u64 tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n"
-	  << loads << "\t\tbool kv[" << g.items << "];\n";
+	  << loads;
+	if (spec_.join_multi) {
+		// a row's matches are not bounded: count this thread's outputs, then evaluate again and write
+		o << "\t\tu32 cnt = 0;\n" << ItemOpen(g, needed) << chain_code_ << "\t\tcnt += keep ? 1u : 0u;\n" << ItemClose()
+		  << "\t\tu32 total; u64 pos = (u64)block_exclusive_scan(cnt, scan_scratch, &total) + tile_offsets[tile];\n"
+		  << ItemOpen(g, needed) << chain_code_ << "\t\tif (keep) {\n";
+		for (size_t c = 0; c < out_cols.size(); c++) {
+			const auto &col = visible_[out_cols[c]];
+			int w = cb + 1 + 2 * static_cast<int>(c);
+			o << "\t\t\t((" << CudaTypeName(col.type) << "*)a.w[" << w << "])[pos] = " << col.value << ";\n";
+			if (col.nullable) {
+				o << "\t\t\tif (a.w[" << w + 1 << "]) ((u8*)a.w[" << w + 1 << "])[pos] = (" << col.valid << ") ? 1 : 0;\n";
+			}
+		}
+		o << "\t\t\t++pos;\n\t\t}\n" << ItemClose() << "\t}\n}\n";
+		return o.str();
+	}
+	o << "\t\tbool kv[" << g.items << "];\n";
 	for (size_t c = 0; c < out_cols.size(); c++) {
 		const auto &col = visible_[out_cols[c]];
 		o << "\t\t" << CudaTypeName(col.type) << " o" << c << "[" << g.items << "];\n";
@@ -466,9 +523,7 @@ std::string PipelineCodegen::EmitMaterialize(const std::vector<int> &outs, const
 			o << "\t\tbool ov" << c << "[" << g.items << "];\n";
 		}
 	}
-	o << "\t\tu32 cnt = 0;\n\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) {\n"
-	  << "\t\tconst u64 row = row0 + r; (void)row;\n\t\tbool keep = row < n;\n"
-	  << chain_code_ << "\t\tkv[r] = keep;\n\t\tcnt += keep ? 1u : 0u;\n";
+	o << "\t\tu32 cnt = 0;\n" << ItemOpen(g, needed) << chain_code_ << "\t\tkv[r] = keep;\n\t\tcnt += keep ? 1u : 0u;\n";
 	for (size_t c = 0; c < out_cols.size(); c++) {
 		const auto &col = visible_[out_cols[c]];
 		o << "\t\to" << c << "[r] = " << col.value << ";\n";
@@ -476,7 +531,7 @@ std::string PipelineCodegen::EmitMaterialize(const std::vector<int> &outs, const
 			o << "\t\tov" << c << "[r] = " << col.valid << ";\n";
 		}
 	}
-	o << "\t\t}\n";
+	o << ItemClose();
 	if (has_filter_) {
 		o << "\t\tu32 total; u32 pos = block_exclusive_scan(cnt, scan_scratch, &total) + tile_offsets[tile];\n";
 	} else {
@@ -523,15 +578,13 @@ std::string PipelineCodegen::EmitStats(const std::vector<int> &columns, const Ge
 	}
 	o << "\tconst u64 ntiles = (n + " << g.tile() - 1 << ") / " << g.tile() << ";\n"
 	  << "\tfor (u64 tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n"
-	  << LoadBlock(g, load_needed, false) << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) {\n"
-	  << "\t\tconst u64 row = row0 + r; (void)row;\n\t\tbool keep = row < n;\n"
-	  << chain_code_ << "\t\tif (row < n) {\n";
+	  << LoadBlock(g, load_needed, false) << ItemOpen(g, load_needed) << chain_code_ << "\t\tif (row < n) {\n";
 	for (size_t c = 0; c < columns.size(); c++) {
 		const auto &col = visible_[columns[c]];
 		o << "\t\t\t{ const i64 x = (i64)(" << col.value << "); mn" << c << " = x < mn" << c << " ? x : mn" << c
 		  << "; mx" << c << " = x > mx" << c << " ? x : mx" << c << "; }\n";
 	}
-	o << "\t\t}\n\t\t}\n\t}\n";
+	o << "\t\t}\n" << ItemClose() << "\t}\n";
 	for (size_t c = 0; c < columns.size(); c++) {
 		o << "\tfor (int off = 16; off > 0; off >>= 1) {\n"
 		  << "\t\ti64 a1 = __shfl_xor_sync(0xffffffffu, mn" << c << ", off); mn" << c << " = a1 < mn" << c << " ? a1 : mn"
@@ -861,9 +914,9 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		}
 		o << "\t}\n\t__syncthreads();\n" << tile_loop_head
 		  << "\tfor (u64 tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n"
-		  << LoadBlock(g, needed, false) << item_head << chain_code_ << "\t\tif (keep) {\n"
+		  << LoadBlock(g, needed, false) << ItemOpen(g, needed) << chain_code_ << "\t\tif (keep) {\n"
 		  << "\t\t\tconst u64 slot = " << pack.str() << ";\n"
-		  << UpdateCode(fields, "T", "slot", pipe_values, true) << "\t\t}\n\t\t}\n\t}\n\t__syncthreads();\n";
+		  << UpdateCode(fields, "T", "slot", pipe_values, true) << "\t\t}\n" << ItemClose() << "\t}\n\t__syncthreads();\n";
 		for (int f = 0; f < F; f++) {
 			o << "\tu64 *G" << f << " = (u64*)a.w[" << cb + 1 + f << "];\n";
 		}
@@ -888,6 +941,9 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		return o.str();
 	}
 
+	if (spec_.join_multi) {
+		Fail(VGPU_ERR_INTERNAL, "partitioned group-by over a multi-match join source (materialize the join first)");
+	}
 	// ---- partitioned: radix partition on the mixed key, then one hash table per partition ----
 	// The intermediate is one fixed-size record per qualifying row: the packed key (u64) at byte 0,
 	// then each carried value at its natural width and alignment, stride RS a multiple of 32 bytes so
@@ -1986,7 +2042,7 @@ std::string SpecKey(const PipelineSpec &spec) {
 	for (auto &sc : spec.sources) {
 		o << sc.name << '/' << static_cast<int>(sc.type) << '/' << sc.nullable << '/' << sc.side << ';';
 	}
-	o << "|cross:" << spec.cross << "|join:" << spec.join << '/' << spec.join_key << '/' << spec.join_inline << "|chain:";
+	o << "|cross:" << spec.cross << "|join:" << spec.join << '/' << spec.join_key << '/' << spec.join_inline << '/' << spec.join_multi << "|chain:";
 	for (const PlanNode *n : spec.chain) {
 		o << static_cast<int>(n->op) << '{';
 		for (auto &e : n->expressions) {

@@ -37,6 +37,10 @@ struct PipelineSpec {
 	int join_key = -1;
 	// The lookup returns the (single, <= 4-byte) right column's value itself instead of a position.
 	bool join_inline = false;
+	// Right keys repeat: the lookup returns the run of equal keys in the sorted right side (start and
+	// length), and every left row expands into one pipeline item per match, in sorted right order.
+	// Consumers that support it: materialization, key statistics, the one-pass group-by.
+	bool join_multi = false;
 	std::vector<const PlanNode *> chain; // FILTER / PROJECTION nodes, bottom-up
 };
 
@@ -170,6 +174,10 @@ private:
 	std::string EmitExpression(const Expr &expr, const std::vector<PipeColumn> &cols, int index);
 	std::string Prologue() const;
 	std::string LoadBlock(const Geometry &g, const std::vector<bool> &needed, bool chunked) const;
+	//! Opens the per-item loop of a tile: `row`, `keep` and (for a multi-match join source) the loop over
+	//! the row's matches with the needed right columns loaded at each; ItemClose closes what it opened.
+	std::string ItemOpen(const Geometry &g, const std::vector<bool> &needed) const;
+	std::string ItemClose() const;
 	std::vector<bool> NeededSources(const std::vector<int> &extra_columns) const;
 
 	PipelineSpec spec_;

@@ -290,24 +290,101 @@ std::string GenerateSourceText(const PlanNode &plan, const std::vector<vgpu_colu
 		chain.push_back(cur);
 		cur = cur->children[0].get();
 	}
-	if (cur->op != OpType::SCAN) {
-		Fail(VGPU_ERR_UNSUPPORTED, "source generation without a device covers pipelines over a SCAN");
-	}
 	std::reverse(chain.begin(), chain.end());
 	PipelineSpec spec;
 	spec.chain = chain;
-	if (inputs.size() < cur->column_names.size()) {
-		Fail(VGPU_ERR_INVALID_ARGUMENT, "plan expects more scanned columns than were supplied");
-	}
-	for (size_t i = 0; i < cur->column_names.size(); i++) {
-		SourceColumn s;
-		s.name = inputs[i].name ? inputs[i].name : "";
-		s.type = static_cast<ValueType>(inputs[i].type);
-		s.nullable = inputs[i].validity != nullptr;
-		spec.sources.push_back(s);
+	if (cur->op == OpType::HASH_JOIN) {
+		// a join source over two SCANs: left columns, then the right output columns, then the left key;
+		// the one-match and the multi-match lookups are both generated
+		if (cur->children.size() != 2 || cur->children[0]->op != OpType::SCAN || cur->children[1]->op != OpType::SCAN ||
+		    cur->build_keys.size() != 1) {
+			Fail(VGPU_ERR_UNSUPPORTED, "source generation without a device covers joins of two SCANs");
+		}
+		const auto &ln = cur->children[0]->column_names, &rn = cur->children[1]->column_names;
+		if (inputs.size() < ln.size() + rn.size()) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "plan expects more scanned columns than were supplied");
+		}
+		auto input_of = [&](const std::string &name, int *side) -> const vgpu_column * {
+			for (size_t i = 0; i < ln.size(); i++) {
+				if (ln[i] == name) { *side = 0; return &inputs[i]; }
+			}
+			for (size_t i = 0; i < rn.size(); i++) {
+				if (rn[i] == name) { *side = 1; return &inputs[ln.size() + i]; }
+			}
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "join column '" + name + "' not found");
+		};
+		for (auto &name : cur->output_columns) {
+			int side = 0;
+			const vgpu_column *in = input_of(name, &side);
+			SourceColumn s;
+			s.name = name;
+			s.type = static_cast<ValueType>(in->type);
+			s.nullable = in->validity != nullptr;
+			s.side = side;
+			spec.sources.push_back(s);
+		}
+		int side = 0;
+		const vgpu_column *key = input_of(cur->build_keys[0], &side);
+		SourceColumn k;
+		k.name = "__vgpu_join_key";
+		k.type = static_cast<ValueType>(key->type);
+		spec.join_key = static_cast<int>(spec.sources.size());
+		spec.sources.push_back(k);
+		spec.join = true;
+	} else if (cur->op != OpType::SCAN) {
+		Fail(VGPU_ERR_UNSUPPORTED, "source generation without a device covers pipelines over a SCAN or a join");
+	} else {
+		if (inputs.size() < cur->column_names.size()) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "plan expects more scanned columns than were supplied");
+		}
+		for (size_t i = 0; i < cur->column_names.size(); i++) {
+			SourceColumn s;
+			s.name = inputs[i].name ? inputs[i].name : "";
+			s.type = static_cast<ValueType>(inputs[i].type);
+			s.nullable = inputs[i].validity != nullptr;
+			spec.sources.push_back(s);
+		}
 	}
 	PipelineCodegen cg(spec);
 	Geometry g;
+	if (spec.join) {
+		PipelineSpec multi = spec;
+		multi.join_multi = true;
+		PipelineCodegen cgm(multi);
+		std::vector<int> outs;
+		for (size_t i = 0; i < cg.visible().size(); i++) outs.push_back(static_cast<int>(i));
+		std::string text = cg.EmitMaterialize(outs, g) + "\n//@@VGPU_TU@@\n" + cgm.EmitMaterialize(outs, g) +
+		                   "\n//@@VGPU_TU@@\n" + cgm.EmitStats(outs, g);
+		if (!gb) return text;
+		PipelineCodegen::GroupBySpec spec_gb;
+		int shift = 0;
+		for (auto &kname : gb->group_keys) {
+			PipelineCodegen::GroupKey key;
+			key.column = cg.FindVisible(kname);
+			if (key.column < 0) Fail(VGPU_ERR_INVALID_ARGUMENT, "group key '" + kname + "' not found");
+			key.min = 0;
+			key.bits = 16;
+			key.shift = shift;
+			shift += 16;
+			spec_gb.keys.push_back(key);
+		}
+		for (auto &a : gb->aggregates) {
+			PipelineCodegen::AggSpec as;
+			as.kind = a.kind;
+			as.output_type = a.output_type;
+			if (a.kind != AggKind::COUNT_STAR) {
+				as.column = cg.FindVisible(a.input_column);
+				if (as.column < 0) Fail(VGPU_ERR_INVALID_ARGUMENT, "aggregate input '" + a.input_column + "' not found");
+				as.input_type = cg.visible()[as.column].type;
+			}
+			spec_gb.aggs.push_back(as);
+		}
+		Geometry gj;
+		gj.block = 512;
+		gj.items = 8;
+		return text + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_gb, false, gj) + "\n//@@VGPU_TU@@\n" +
+		       cgm.EmitGroupBy(spec_gb, false, gj);
+	}
 	if (!gb) {
 		std::vector<int> outs;
 		for (size_t i = 0; i < cg.visible().size(); i++) outs.push_back(static_cast<int>(i));

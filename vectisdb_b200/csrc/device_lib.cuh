@@ -388,6 +388,36 @@ __device__ __forceinline__ long long vgpu_join_find(u64 k, const u64 *__restrict
 	return (lo < end && sorted[lo] == k) ? (long long)lo : -1ll;
 }
 
+// The run of right rows whose (biased) key equals k in a sorted key array that may repeat keys, through
+// the radix directory above: returns the run's first position and sets *count to its length, or
+// returns -1 (count 0) when k is absent. With shift == 0 the directory is indexed by the key itself
+// (one bucket per key value), so the run is the whole bucket: two adjacent loads and no search.
+__device__ __forceinline__ long long vgpu_join_run(u64 k, const u64 *__restrict__ sorted, const u32 *__restrict__ dir,
+                                                   u64 nb, u32 shift, u32 *count) {
+	const u64 b = k >> shift;
+	*count = 0u;
+	if (b >= nb) return -1ll;
+	const u32 lo0 = dir[b], end = dir[b + 1];
+	if (shift == 0u) {
+		*count = end - lo0;
+		return end > lo0 ? (long long)lo0 : -1ll;
+	}
+	u32 lo = lo0, hi = end;
+	while (lo < hi) {  // first position with key >= k
+		const u32 mid = (lo + hi) >> 1;
+		if (sorted[mid] < k) lo = mid + 1;
+		else hi = mid;
+	}
+	u32 up = lo, top = end;
+	while (up < top) {  // first position with key > k
+		const u32 mid = (up + top) >> 1;
+		if (sorted[mid] <= k) up = mid + 1;
+		else top = mid;
+	}
+	*count = up - lo;
+	return up > lo ? (long long)lo : -1ll;
+}
+
 // ---------------------------------------------------------------------------------------------
 // Hashing of packed group keys
 

@@ -29,6 +29,8 @@ namespace vgpu {
 namespace {
 
 constexpr uint64_t kMaxOutputRows = 1ull << 32; // same backstop as the reference's join/cross caps
+// Longest run of one right key a fused multi-match join source takes (one thread walks a row's run).
+constexpr uint32_t kMaxJoinRun = 1u << 16;
 
 struct KArgsHost {
 	uint64_t w[128];
@@ -203,13 +205,17 @@ private:
 	};
 
 	Relation Scan(const PlanNode &node);
-	PipelineInput BuildPipeline(const PlanNode &top, std::vector<const PlanNode *> chain_top_down);
+	//! `multi_ok`: the consumer accepts a join source whose right keys repeat (join_multi).
+	PipelineInput BuildPipeline(const PlanNode &top, std::vector<const PlanNode *> chain_top_down, bool multi_ok = false);
+	//! A pipeline with no chain over the columns of a relation.
+	PipelineInput PipelineOver(const Relation &rel);
 	Relation Materialize(PipelineInput &pin, const std::vector<int> &out_cols, const std::vector<std::string> &names);
 	Relation RunChain(const PlanNode &node);
 	Relation GroupBy(const PlanNode &node);
 	Relation Join(const PlanNode &node);
 	Relation JoinMaterialize(const PlanNode &node, Relation &left, Relation &right);
-	Relation JoinForPipeline(const PlanNode &node, PipelineInput &pin, bool *fused);
+	Relation JoinForPipeline(const PlanNode &node, PipelineInput &pin, bool *fused, bool multi_ok);
+	Relation GroupByPipeline(const PlanNode &node, PipelineInput &pin);
 	Relation CrossProduct(const PlanNode &node);
 	void ComputeStats(PipelineInput &pin, const PipelineCodegen &cg, const std::vector<int> &cols,
 	                  std::vector<std::pair<int64_t, int64_t>> &out);
@@ -369,7 +375,7 @@ void Executor::FillArgs(const PipelineInput &pin, KArgsHost &args) {
 	}
 }
 
-Executor::PipelineInput Executor::BuildPipeline(const PlanNode &top, std::vector<const PlanNode *> chain) {
+Executor::PipelineInput Executor::BuildPipeline(const PlanNode &top, std::vector<const PlanNode *> chain, bool multi_ok) {
 	// `top` is the first non-FILTER/PROJECTION node below the chain.
 	PipelineInput pin;
 	std::reverse(chain.begin(), chain.end()); // bottom-up
@@ -428,11 +434,18 @@ Executor::PipelineInput Executor::BuildPipeline(const PlanNode &top, std::vector
 	Relation rel;
 	if (top.op == OpType::HASH_JOIN) {
 		bool fused = false;
-		rel = JoinForPipeline(top, pin, &fused);
+		rel = JoinForPipeline(top, pin, &fused, multi_ok);
 		if (fused) return pin;
 	} else {
 		rel = top.op == OpType::SCAN ? Scan(top) : Exec(top);
 	}
+	PipelineInput over = PipelineOver(rel);
+	over.spec.chain = pin.spec.chain;
+	return over;
+}
+
+Executor::PipelineInput Executor::PipelineOver(const Relation &rel) {
+	PipelineInput pin;
 	uint64_t rows = rel.empty() ? 0 : rel.front().rows;
 	for (auto &c : rel) {
 		if (c.rows != rows) {
@@ -466,19 +479,33 @@ Relation Executor::Materialize(PipelineInput &pin, const std::vector<int> &out_c
 	const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ntiles, uint64_t(sms) * 8)));
 	const int cb = cg.ConsumerBase();
 	uint64_t out_rows = n;
-	uint32_t *tile_offsets = nullptr;
+	void *tile_offsets = nullptr;
 	if (cg.has_filter() && n > 0) {
-		uint32_t *tile_counts = arena_.AllocT<uint32_t>(ntiles);
-		uint32_t *total = arena_.AllocT<uint32_t>(1);
-		KArgsHost a;
-		FillArgs(pin, a);
-		a.SetPtr(cb, tile_counts);
 		uint64_t in_bytes = 0;
 		for (auto &s : pin.sources) in_bytes += s.rows * TypeSize(s.type);
-		LaunchGenerated(*module, "vgpu_mat_count", grid, g.block, 0, stream_, a, in_bytes, n);
-		kern::ExclusiveScanU32(tile_counts, tile_counts, ntiles, total, arena_);
-		out_rows = ReadU32(total);
-		tile_offsets = tile_counts;
+		KArgsHost a;
+		FillArgs(pin, a);
+		if (pin.spec.join_multi) {  // 64-bit tile counts: the matches can outnumber the rows
+			uint64_t *tile_counts = arena_.AllocT<uint64_t>(ntiles);
+			uint64_t *total = arena_.AllocT<uint64_t>(1);
+			a.SetPtr(cb, tile_counts);
+			LaunchGenerated(*module, "vgpu_mat_count", grid, g.block, 0, stream_, a, in_bytes, n);
+			kern::ExclusiveScanU64(tile_counts, tile_counts, ntiles, total, arena_);
+			out_rows = ReadU64(total);
+			if (out_rows >= kMaxOutputRows) {
+				Fail(VGPU_ERR_UNSUPPORTED, "gpu_hash_join: join produces " + std::to_string(out_rows) +
+				                               " rows, more than this GPU path materializes");
+			}
+			tile_offsets = tile_counts;
+		} else {
+			uint32_t *tile_counts = arena_.AllocT<uint32_t>(ntiles);
+			uint32_t *total = arena_.AllocT<uint32_t>(1);
+			a.SetPtr(cb, tile_counts);
+			LaunchGenerated(*module, "vgpu_mat_count", grid, g.block, 0, stream_, a, in_bytes, n);
+			kern::ExclusiveScanU32(tile_counts, tile_counts, ntiles, total, arena_);
+			out_rows = ReadU32(total);
+			tile_offsets = tile_counts;
+		}
 	}
 	Relation out;
 	KArgsHost a;
@@ -521,7 +548,7 @@ Relation Executor::RunChain(const PlanNode &node) {
 		chain.push_back(cur);
 		cur = cur->children[0].get();
 	}
-	PipelineInput pin = BuildPipeline(*cur, chain);
+	PipelineInput pin = BuildPipeline(*cur, chain, true);
 	auto probe_cg = CodegenFor(pin.spec);
 	const PipelineCodegen &probe = *probe_cg;
 	std::vector<int> outs;
@@ -691,7 +718,11 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		chain.push_back(cur);
 		cur = cur->children[0].get();
 	}
-	PipelineInput pin = BuildPipeline(*cur, chain);
+	PipelineInput pin = BuildPipeline(*cur, chain, true);
+	return GroupByPipeline(node, pin);
+}
+
+Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 	auto cgp = CodegenFor(pin.spec);
 	const PipelineCodegen &cg = *cgp;
 	if (cg.visible().empty()) {
@@ -749,6 +780,19 @@ Relation Executor::GroupBy(const PlanNode &node) {
 	const uint64_t domain = 1ull << shift;
 	const uint64_t direct_smem = domain * static_cast<uint64_t>(F) * 8;
 	const bool direct = direct_smem <= 96 * 1024;
+	if (!direct && pin.spec.join_multi) {
+		// the partitioned strategies take one item per input row: expand the join's matches into a
+		// relation first, then group that
+		std::vector<int> outs;
+		std::vector<std::string> names;
+		for (size_t i = 0; i < cg.visible().size(); i++) {
+			outs.push_back(static_cast<int>(i));
+			names.push_back(cg.visible()[i].name);
+		}
+		Relation flat = Materialize(pin, outs, names);
+		PipelineInput over = PipelineOver(flat);
+		return GroupByPipeline(node, over);
+	}
 	const int key_words = static_cast<int>(gb.keys.size());
 	const int out_words = key_words + static_cast<int>(gb.aggs.size());
 	gb.domain = domain;
@@ -1265,7 +1309,7 @@ Relation Executor::Join(const PlanNode &node) {
 // match in the sorted right side (a radix directory over the sorted keys, then a short binary search;
 // right columns gathered into sorted order once), and rows without a match are filtered out. The
 // match pairs are never materialized. Otherwise the join output is materialized as usual.
-Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, bool *fused) {
+Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, bool *fused, bool multi_ok) {
 	*fused = false;
 	if (node.children.size() != 2) {
 		Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: HASH_JOIN expects exactly two children");
@@ -1452,8 +1496,20 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 			arena_.FreeNow(rw_alt);
 			arena_.FreeNow(perm_alt);
 			kern::CountAdjacentEqual(rw, rn, dups, stream_);
-			if (ReadU32(dups) != 0) return JoinMaterialize(node, left, right);  // many-to-many
-			const uint32_t shift = bits > 22 ? static_cast<uint32_t>(bits - 22) : 0u;
+			bool multi = false;
+			if (ReadU32(dups) != 0) {
+				// Right keys repeat: a consumer that takes one item per match reads each probe row's run of
+				// equal keys (sorted right order); runs longer than kMaxJoinRun go to the load-balanced
+				// materializing join instead, which spreads one row's matches over many threads.
+				if (!multi_ok) return JoinMaterialize(node, left, right);
+				uint32_t *maxrun = arena_.AllocT<uint32_t>(1);
+				kern::MaxRunLength(rw, rn, maxrun, stream_);
+				if (ReadU32(maxrun) > kMaxJoinRun) return JoinMaterialize(node, left, right);
+				multi = true;
+			}
+			// a dense key range gets one directory bucket per key value (the run is the bucket)
+			const bool dense_runs = multi && range < (1ull << 28) && range < 4 * rn;
+			const uint32_t shift = dense_runs ? 0u : bits > 22 ? static_cast<uint32_t>(bits - 22) : 0u;
 			const uint64_t nb = (range >> shift) + 1;
 			uint32_t *dir = arena_.AllocT<uint32_t>(nb + 1);
 			kern::JoinDirectory(rw, rn, shift, nb, dir, stream_);
@@ -1461,6 +1517,7 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 			pin.join_words[0] = reinterpret_cast<uint64_t>(rw);
 			pin.join_words[1] = reinterpret_cast<uint64_t>(dir);
 			pin.join_words[3] = shift | (nb << 8);
+			pin.spec.join_multi = multi;
 		}
 	}
 	pin.join_words[2] = bias;
@@ -1551,9 +1608,16 @@ Relation Executor::JoinMaterialize(const PlanNode &node, Relation &left, Relatio
 	kern::RadixSortPairs(rw, perm, rw_alt, perm_alt, rn, bits, arena_);
 	arena_.FreeNow(rw_alt);
 	arena_.FreeNow(perm_alt);
+	// each left key's run of equal right keys through a radix directory: one bucket per key value when
+	// the key range is dense (the run is read, not searched), else 2^22 buckets and a short search
+	const uint64_t range = host_mm[1] - host_mm[0];
+	const uint32_t shift = (range < (1ull << 28) && range < 4 * rn) ? 0u : bits > 22 ? static_cast<uint32_t>(bits - 22) : 0u;
+	const uint64_t nb = (range >> shift) + 1;
+	uint32_t *dir = arena_.AllocT<uint32_t>(nb + 1);
+	kern::JoinDirectory(rw, rn, shift, nb, dir, stream_);
 	uint64_t *lower = arena_.AllocT<uint64_t>(ln);
 	uint64_t *counts = arena_.AllocT<uint64_t>(ln);
-	kern::JoinSearch(lw, ln, rw, rn, bias, lower, counts, stream_);
+	kern::JoinRuns(lw, ln, rw, dir, nb, shift, bias, lower, counts, stream_);
 	uint64_t *total = arena_.AllocT<uint64_t>(1);
 	kern::ExclusiveScanU64(counts, counts, ln, total, arena_);
 	const uint64_t total_rows = ReadU64(total);

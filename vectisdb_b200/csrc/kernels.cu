@@ -1,6 +1,8 @@
 // kernels.cu -- precompiled device primitives (see kernels.hpp).
 #include "kernels.hpp"
 
+#include <algorithm>
+
 #include <type_traits>
 
 #include <utility>
@@ -306,45 +308,101 @@ __global__ void __launch_bounds__(kSortBlock) RadixScatterKernel(const uint64_t 
 
 // ---- join -----------------------------------------------------------------------------------------
 
-__global__ void JoinSearchKernel(const uint64_t *probe, uint64_t n_probe, const uint64_t *sorted, uint64_t n_sorted,
-                                 uint64_t bias, uint64_t range, uint64_t *lower, uint64_t *count) {
-	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_probe; i += (uint64_t)gridDim.x * blockDim.x) {
-		const uint64_t x = probe[i];
-		uint64_t lo = 0, c = 0;
-		if (x >= bias && x - bias <= range) {
-			const uint64_t k = x - bias;
-			uint64_t a = 0, b = n_sorted;
-			while (a < b) {
-				uint64_t mid = (a + b) >> 1;
-				if (sorted[mid] < k) a = mid + 1; else b = mid;
-			}
-			lo = a;
-			uint64_t e = a;
-			b = n_sorted;
-			while (e < b) {
-				uint64_t mid = (e + b) >> 1;
-				if (sorted[mid] <= k) e = mid + 1; else b = mid;
-			}
-			c = e - lo;
+// Load-balanced expansion of the match pairs (a merge path over the left rows' output offsets): each
+// CTA owns a fixed tile of output positions, finds once which left rows those positions span, stages
+// those rows' offsets in shared memory (when they fit) and every thread places its outputs by a search
+// there; writes are coalesced across the tile. Left rows with no match share an offset with the next
+// row, so "last row whose offset <= o" skips them.
+constexpr int kExpandBlock = 256;
+constexpr int kExpandItems = 8;
+constexpr int kExpandTile = kExpandBlock * kExpandItems;
+constexpr int kExpandWindow = 4096;
+
+__device__ __forceinline__ uint64_t LastAtMost(const uint64_t *offsets, uint64_t a, uint64_t b, uint64_t o) {
+	// offsets[a] <= o; returns the last index in [a, b) with offsets[index] <= o
+	uint64_t lo = a + 1, hi = b;
+	while (lo < hi) {
+		const uint64_t mid = (lo + hi) >> 1;
+		if (offsets[mid] <= o) lo = mid + 1;
+		else hi = mid;
+	}
+	return lo - 1;
+}
+
+__global__ void __launch_bounds__(kExpandBlock) JoinExpandKernel(const uint64_t *offsets, const uint64_t *lower,
+                                                                 uint64_t n_left, const uint32_t *sorted_perm,
+                                                                 uint64_t total, uint32_t *out_left, uint32_t *out_right) {
+	__shared__ uint64_t s_off[kExpandWindow];
+	__shared__ uint64_t s_first, s_end;
+	for (uint64_t tile = blockIdx.x; tile * kExpandTile < total; tile += gridDim.x) {
+		const uint64_t o_begin = tile * kExpandTile;
+		const uint64_t o_last = o_begin + kExpandTile < total ? o_begin + kExpandTile - 1 : total - 1;
+		if (threadIdx.x == 0) {
+			const uint64_t first = LastAtMost(offsets, 0, n_left, o_begin);
+			s_first = first;
+			s_end = LastAtMost(offsets, first, n_left, o_last) + 1;
 		}
-		lower[i] = lo;
-		count[i] = c;
+		__syncthreads();
+		const uint64_t first = s_first, end = s_end, window = end - first;
+		const bool staged = window <= kExpandWindow;
+		if (staged) {
+			for (uint64_t r = threadIdx.x; r < window; r += kExpandBlock) s_off[r] = offsets[first + r];
+		}
+		__syncthreads();
+		for (int t = 0; t < kExpandItems; ++t) {
+			const uint64_t o = o_begin + static_cast<uint64_t>(t) * kExpandBlock + threadIdx.x;
+			if (o > o_last) break;
+			uint64_t i;
+			if (staged) {
+				uint32_t lo = 1, hi = static_cast<uint32_t>(window);
+				while (lo < hi) {
+					const uint32_t mid = (lo + hi) >> 1;
+					if (s_off[mid] <= o) lo = mid + 1;
+					else hi = mid;
+				}
+				i = first + lo - 1;
+			} else {
+				i = LastAtMost(offsets, first, end, o);
+			}
+			const uint64_t j = o - (staged ? s_off[i - first] : offsets[i]);
+			out_left[o] = static_cast<uint32_t>(i);
+			out_right[o] = sorted_perm[lower[i] + j];
+		}
+		__syncthreads();
 	}
 }
 
-__global__ void JoinExpandKernel(const uint64_t *offsets, const uint64_t *lower, uint64_t n_left,
-                                 const uint32_t *sorted_perm, uint64_t total, uint32_t *out_left, uint32_t *out_right) {
-	for (uint64_t o = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; o < total; o += (uint64_t)gridDim.x * blockDim.x) {
-		// last left row whose offset <= o (rows with zero matches share offsets; the upper bound skips them)
-		uint64_t a = 0, b = n_left;
-		while (a < b) {
-			uint64_t mid = (a + b) >> 1;
-			if (offsets[mid] <= o) a = mid + 1; else b = mid;
+// Each probe key's run in the sorted right keys through a radix directory (see vgpu_join_run): shift 0
+// indexes the directory by the key itself, so the run is read, not searched.
+__global__ void JoinRunKernel(const uint64_t *probe, uint64_t n_probe, const uint64_t *sorted, const uint32_t *dir,
+                              uint64_t nb, uint32_t shift, uint64_t bias, uint64_t *lower, uint64_t *count) {
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_probe; i += (uint64_t)gridDim.x * blockDim.x) {
+		const uint64_t k = probe[i] - bias;  // below the bias wraps past every bucket: no match
+		const uint64_t b = k >> shift;
+		uint64_t lo = 0, c = 0;
+		if (b < nb) {
+			uint64_t a = dir[b], e = dir[b + 1];
+			if (shift != 0) {
+				uint64_t hi = e;
+				while (a < hi) {
+					const uint64_t mid = (a + hi) >> 1;
+					if (sorted[mid] < k) a = mid + 1;
+					else hi = mid;
+				}
+				uint64_t up = a;
+				hi = e;
+				while (up < hi) {
+					const uint64_t mid = (up + hi) >> 1;
+					if (sorted[mid] <= k) up = mid + 1;
+					else hi = mid;
+				}
+				e = up;
+			}
+			lo = a;
+			c = e - a;
 		}
-		const uint64_t i = a - 1;
-		const uint64_t j = o - offsets[i];
-		out_left[o] = static_cast<uint32_t>(i);
-		out_right[o] = sorted_perm[lower[i] + j];
+		lower[i] = lo;
+		count[i] = c;
 	}
 }
 
@@ -437,6 +495,36 @@ __global__ void CountAdjacentEqualKernel(const uint64_t *sorted, uint64_t n, uin
 		local += sorted[i] == sorted[i - 1] ? 1u : 0u;
 	}
 	if (local) atomicAdd(out, local);
+}
+
+// Longest run of equal keys in a sorted array: every run start finds its end by a galloping then a
+// binary search, and the lengths meet in one atomic maximum.
+__global__ void MaxRunLengthKernel(const uint64_t *sorted, uint64_t n, uint32_t *out) {
+	uint32_t local = 0;
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+		const uint64_t k = sorted[i];
+		if (i > 0 && sorted[i - 1] == k) continue;
+		// gallop: `good` holds k, `bad` is the first probe past the run (or n)
+		uint64_t good = i, step = 1, bad = n;
+		while (good + step < n) {
+			if (sorted[good + step] != k) {
+				bad = good + step;
+				break;
+			}
+			good += step;
+			step <<= 1;
+		}
+		// the run ends in (good, bad]: binary search for the first position without k
+		uint64_t a = good + 1, b = bad;
+		while (a < b) {
+			const uint64_t mid = (a + b) >> 1;
+			if (sorted[mid] == k) a = mid + 1;
+			else b = mid;
+		}
+		const uint64_t len = a - i;
+		local = max(local, len > 0xffffffffull ? 0xffffffffu : static_cast<uint32_t>(len));
+	}
+	if (local) atomicMax(out, local);
 }
 
 // Work list of a partitioned aggregation pass. Item = (partition, first row, end row, split index or
@@ -616,6 +704,14 @@ void CountAdjacentEqual(const uint64_t *sorted, uint64_t n, uint32_t *out, cudaS
 	if (n < 2) return;
 	LaunchScope scope("count_adjacent_equal", stream, n * 8, n);
 	CountAdjacentEqualKernel<<<GridFor(n, 256), 256, 0, stream>>>(sorted, n, out);
+	VGPU_CUDA(cudaGetLastError());
+}
+
+void MaxRunLength(const uint64_t *sorted, uint64_t n, uint32_t *out, cudaStream_t stream) {
+	VGPU_CUDA(cudaMemsetAsync(out, 0, 4, stream));
+	if (n == 0) return;
+	LaunchScope scope("max_run_length", stream, n * 8, n);
+	MaxRunLengthKernel<<<GridFor(n, 256), 256, 0, stream>>>(sorted, n, out);
 	VGPU_CUDA(cudaGetLastError());
 }
 
@@ -910,23 +1006,21 @@ void Iota(uint32_t *out, uint64_t n, cudaStream_t stream) {
 	VGPU_CUDA(cudaGetLastError());
 }
 
-void JoinSearch(const uint64_t *probe, uint64_t n_probe, const uint64_t *sorted, uint64_t n_sorted, uint64_t bias,
-                uint64_t *lower, uint64_t *count, cudaStream_t stream) {
-	if (n_probe == 0) return;
-	LaunchScope scope("join_search", stream, n_probe * 24, n_probe);
-	// range of normalized keys: sorted is ascending, so its last element bounds every match.
-	// (Passed as n_sorted-based sentinel: any k > sorted[n-1] finds no equal key anyway.)
-	JoinSearchKernel<<<GridFor(n_probe, 256), 256, 0, stream>>>(probe, n_probe, sorted, n_sorted, bias, ~0ull, lower,
-	                                                            count);
-	VGPU_CUDA(cudaGetLastError());
-}
-
 void JoinExpand(const uint64_t *offsets, const uint64_t *lower, uint64_t n_left, const uint32_t *sorted_perm,
                 uint64_t total, uint32_t *out_left, uint32_t *out_right, cudaStream_t stream) {
 	if (total == 0) return;
 	LaunchScope scope("join_expand", stream, total * 8, total);
-	JoinExpandKernel<<<GridFor(total, 256), 256, 0, stream>>>(offsets, lower, n_left, sorted_perm, total, out_left,
-	                                                          out_right);
+	const uint64_t tiles = (total + kExpandTile - 1) / kExpandTile;
+	const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(tiles, 148ull * 8));
+	JoinExpandKernel<<<grid, kExpandBlock, 0, stream>>>(offsets, lower, n_left, sorted_perm, total, out_left, out_right);
+	VGPU_CUDA(cudaGetLastError());
+}
+
+void JoinRuns(const uint64_t *probe, uint64_t n_probe, const uint64_t *sorted, const uint32_t *dir, uint64_t nb,
+              uint32_t shift, uint64_t bias, uint64_t *lower, uint64_t *count, cudaStream_t stream) {
+	if (n_probe == 0) return;
+	LaunchScope scope("join_runs", stream, n_probe * 24, n_probe);
+	JoinRunKernel<<<GridFor(n_probe, 256), 256, 0, stream>>>(probe, n_probe, sorted, dir, nb, shift, bias, lower, count);
 	VGPU_CUDA(cudaGetLastError());
 }
 

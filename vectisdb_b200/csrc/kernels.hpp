@@ -46,14 +46,15 @@ void RadixSortPairs(uint64_t *keys, uint32_t *values, uint64_t *keys_alt, uint32
 void SubtractBias(uint64_t *keys, uint64_t n, uint64_t bias, cudaStream_t stream);
 void Iota(uint32_t *out, uint64_t n, cudaStream_t stream);
 
-//! For each probe key (widened): the first index of an equal key in `sorted` (normalized by
-//! `bias`) and how many equal keys follow.
-void JoinSearch(const uint64_t *probe, uint64_t n_probe, const uint64_t *sorted, uint64_t n_sorted, uint64_t bias,
-                uint64_t *lower, uint64_t *count, cudaStream_t stream);
-
-//! One thread per output pair: left row i owns outputs [offsets[i], offsets[i] + count[i]).
+//! Left row i owns outputs [offsets[i], offsets[i + 1]) (offsets ascending, offsets[0] = 0): output o
+//! becomes (i, sorted_perm[lower[i] + o - offsets[i]]). Load-balanced: fixed tiles of outputs per CTA,
+//! the left rows a tile spans staged in shared memory.
 void JoinExpand(const uint64_t *offsets, const uint64_t *lower, uint64_t n_left, const uint32_t *sorted_perm,
                 uint64_t total, uint32_t *out_left, uint32_t *out_right, cudaStream_t stream);
+//! For each probe key (widened): the first position of its run of equal keys in `sorted` (normalized by
+//! `bias`) and the run's length, through the radix directory `dir` (nb buckets of key >> shift).
+void JoinRuns(const uint64_t *probe, uint64_t n_probe, const uint64_t *sorted, const uint32_t *dir, uint64_t nb,
+              uint32_t shift, uint64_t bias, uint64_t *lower, uint64_t *count, cudaStream_t stream);
 
 //! Radix directory of a sorted (biased) key array: dir[b] = first position whose key >> shift >= b,
 //! for b in [0, nb]; dir needs nb + 1 entries and nb must exceed every key >> shift.
@@ -73,6 +74,8 @@ void JoinDenseCompact(const uint64_t *keys, const void *values, size_t vwidth, u
                       uint32_t vmin, void *table, size_t width, uint32_t *dups, cudaStream_t stream);
 //! *out = number of positions i > 0 with sorted[i] == sorted[i - 1].
 void CountAdjacentEqual(const uint64_t *sorted, uint64_t n, uint32_t *out, cudaStream_t stream);
+//! *out = the length of the longest run of equal keys in `sorted` (saturating at 2^32 - 1).
+void MaxRunLength(const uint64_t *sorted, uint64_t n, uint32_t *out, cudaStream_t stream);
 
 //! Work list of a partitioned aggregation pass over `P` partitions whose row ranges start at
 //! offsets[p * stride] (the last ends at *total_rows): 16-byte items (partition, first row, end row,
