@@ -787,10 +787,16 @@ int PipelineCodegen::DirectSlotBytes(const GroupBySpec &gb) {
 	int bytes = 0;
 	for (auto &f : StateFields(gb)) {
 		if (f.kind == "cnt") bytes += 4;
-		if (f.kind == "f64" || f.kind == "min" || f.kind == "max") bytes += 8;
+		if ((f.kind == "f64" && !gb.f64_l2) || f.kind == "min" || f.kind == "max") bytes += 8;
 		if (f.kind == "lo") bytes += 16;
 	}
 	return bytes;
+}
+
+int PipelineCodegen::F64Fields(const GroupBySpec &gb) {
+	int n = 0;
+	for (auto &f : StateFields(gb)) n += f.kind == "f64" ? 1 : 0;
+	return n;
 }
 
 int PipelineCodegen::HeavySlotBytes(const GroupBySpec &gb) {
@@ -1456,7 +1462,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		std::vector<DArr> arrs;
 		for (int f = 0; f < F; f++) {
 			const auto &fd = fields[f];
-			if (fd.kind == "f64") arrs.push_back({"DF" + std::to_string(f), "double", 8});
+			if (fd.kind == "f64" && !gb.f64_l2) arrs.push_back({"DF" + std::to_string(f), "double", 8});
 			if (fd.kind == "min" || fd.kind == "max") arrs.push_back({"DM" + std::to_string(f), "i64", 8});
 		}
 		for (int f = 0; f < F; f++) {
@@ -1472,6 +1478,23 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			decl << "\t" << ar.type << " *" << ar.name << " = (" << ar.type << "*)(sm + " << off << ");\n";
 			off += D * ar.bytes;
 		}
+		// FP64 sums in the CTA's own tables of the global region (L2-resident: reductions, no CAS loops)
+		const int OUTD_ = cb + 8;
+		const int SCR = OUTD_ + static_cast<int>(gb.keys.size() + gb.aggs.size());
+		if (gb.f64_l2) {
+			int fi = 0;
+			const int nf = F64Fields(gb);
+			for (int f = 0; f < F; f++) {
+				if (fields[f].kind != "f64") continue;
+				decl << "\tdouble *DF" << f << " = (double*)a.w[" << SCR << "] + ((u64)blockIdx.x * " << nf << "u + " << fi
+				     << "u) * " << D << "ull;\n";
+				fi++;
+			}
+		}
+		// a sum field's current value (the global tables are read past L1: reductions land in L2)
+		auto f64_load = [&](int f, const std::string &sv) {
+			return gb.f64_l2 ? "__ldcg(&DF" + std::to_string(f) + "[" + sv + "])" : "DF" + std::to_string(f) + "[" + sv + "]";
+		};
 		auto reset_slot = [&](const std::string &sv) {
 			std::ostringstream r;
 			for (int f = 0; f < F; f++) {
@@ -1493,7 +1516,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			for (int f = 0; f < F; f++) {
 				const auto &fd = fields[f];
 				if (fd.kind == "cnt") r << "\t\t\tS" << f << "[0] = (u64)DC[" << sv << "];\n";
-				if (fd.kind == "f64") r << "\t\t\tS" << f << "[0] = (u64)__double_as_longlong(DF" << f << "[" << sv << "]);\n";
+				if (fd.kind == "f64") r << "\t\t\tS" << f << "[0] = (u64)__double_as_longlong(" << f64_load(f, sv) << ");\n";
 				if (fd.kind == "min" || fd.kind == "max") r << "\t\t\tS" << f << "[0] = (u64)DM" << f << "[" << sv << "];\n";
 				if (fd.kind == "lo") {
 					r << "\t\t\tS" << f << "[0] = (u64)DW" << f << "_0[" << sv << "] | ((u64)DW" << f << "_1[" << sv
@@ -1590,7 +1613,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			}
 		}
 
-		o << "__device__ __forceinline__ void vgpu_dslot_reset(char *sm, u32 s) {\n" << decl.str() << reset_slot("s")
+		o << "__device__ __forceinline__ void vgpu_dslot_reset(const KArgs &a, char *sm, u32 s) {\n\t(void)a;\n" << decl.str() << reset_slot("s")
 		  << "}\n\n";
 		o << "__device__ __forceinline__ void vgpu_ditem(const KArgs &a, const uint4 it, char *sm) {\n"
 		  << "\t__shared__ u32 warp_live[32];\n\t__shared__ u64 out_base;\n\t__shared__ bool last_chunk;\n"
@@ -1657,6 +1680,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		  << "\t\t\tif (valid && leader) {\n" << update("g", "slot") << "\t\t\t}\n"
 		  << "\t\t}\n\t}\n"
 		  << "\tif (hot != ~0u && lane == 0) {\n" << update("w", "hot") << "\t}\n"
+		  << (gb.f64_l2 ? "\t__threadfence();  // this thread's reductions are performed before the tables are read\n" : "")
 		  << "\t__syncthreads();\n"
 		  << "\tif (sidx == ~0u) {\n"
 		  << compaction("DC[s] != 0u", load_slot("s"), reset_slot("s"))
@@ -1690,11 +1714,12 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		o << "extern \"C\" __global__ void __launch_bounds__(" << gb.bucket_threads << ") vgpu_gb_dbucket(KArgs a) {\n"
 		  << "\textern __shared__ __align__(16) char vgpu_dsm[];\n"
 		  << "\t__shared__ u32 cur;\n"
-		  << "\tfor (u32 s = threadIdx.x; s < " << D << "u; s += blockDim.x) vgpu_dslot_reset(vgpu_dsm, s);\n"
+		  << "\tfor (u32 s = threadIdx.x; s < " << D << "u; s += blockDim.x) vgpu_dslot_reset(a, vgpu_dsm, s);\n"
 		  << "\tconst u32 n_items = *(const u32*)a.w[" << cb + 1 << "];\n"
 		  << "\tconst uint4 *items = (const uint4*)a.w[" << cb << "];\n"
 		  << "\twhile (true) {\n"
 		  << "\t\tif (threadIdx.x == 0) cur = atomicAdd((u32*)a.w[" << cb + 5 << "], 1u);\n"
+		  << (gb.f64_l2 ? "\t\t__threadfence();  // resets of the global sums land before the next reductions\n" : "")
 		  << "\t\t__syncthreads();\n"
 		  << "\t\tconst u32 i = cur;\n"
 		  << "\t\t__syncthreads();\n"
@@ -2064,7 +2089,7 @@ std::string GroupByKey(const PipelineCodegen::GroupBySpec &gb, bool partitioned)
 		o << static_cast<int>(a.kind) << '/' << a.column << '/' << static_cast<int>(a.input_type) << '/'
 		  << static_cast<int>(a.output_type) << ';';
 	}
-	o << "|db:" << gb.direct_bits << "|bt:" << gb.bucket_threads << "|hv:" << gb.heavy_slots;
+	o << "|db:" << gb.direct_bits << "|bt:" << gb.bucket_threads << "|hv:" << gb.heavy_slots << "|f64l2:" << gb.f64_l2;
 	return o.str();
 }
 

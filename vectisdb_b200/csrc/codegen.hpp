@@ -136,6 +136,10 @@ public:
 		// partial states during the scatter and leave as one partial record per key and CTA instead
 		// of one record per row.
 		int heavy_slots = 0;
+		// Direct-partitioned bucket pass: FP64 sums accumulate in a per-CTA table in global memory (it
+		// stays in L2) with fire-and-forget reductions, instead of shared-memory compare-and-swap loops.
+		// Argument word: the region (CTAs x FP64 fields x slots doubles, zero on entry and left zero).
+		bool f64_l2 = false;
 	};
 
 	//! Group-by kernels (see executor for the argument layout), all in one translation unit:
@@ -160,6 +164,8 @@ public:
 	static int StateWords(const GroupBySpec &gb);
 	//! Shared-memory bytes per slot of a direct-partitioned table (32-bit count and sum words).
 	static int DirectSlotBytes(const GroupBySpec &gb);
+	//! FP64 sum fields of a group-by's state (the per-CTA region of f64_l2 holds one table each).
+	static int F64Fields(const GroupBySpec &gb);
 	//! Shared-memory bytes of one heavy key's partial state in the heavy partition passes (row count,
 	//! partial state of every aggregate).
 	static int HeavySlotBytes(const GroupBySpec &gb);

@@ -898,6 +898,9 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 			dbits = std::max(dbits, shift - 14);  // at most 2^14 partitions (the partition histograms)
 			gb.direct_bits = dbits;
 			gb.key_bits = shift;
+			// FP64 sums of the bucket pass in L2 through reductions (VGPU_GB_F64_L2=0: shared CAS loops)
+			const char *env_l2 = std::getenv("VGPU_GB_F64_L2");
+			gb.f64_l2 = PipelineCodegen::F64Fields(gb) > 0 && !(env_l2 && std::strcmp(env_l2, "0") == 0);
 			const uint64_t mask = (1ull << shift) - 1;
 			const uint64_t M = (0x9e3779b97f4a7c15ull & mask) | 1ull;
 			uint64_t inv = M;  // Newton iteration for the inverse mod 2^64: each step doubles the valid bits
@@ -1267,6 +1270,10 @@ uint64_t Executor::DirectBuckets(Module &module, const PipelineCodegen::GroupByS
 	b.SetPtr(cb + 6, out_count);
 	b.SetPtr(cb + 7, control + 1);
 	for (int w = 0; w < out_words; w++) b.SetPtr(cb + 8 + w, out[w].data);
+	if (gb.f64_l2) {  // per-CTA FP64 sum tables (the kernel clears its own on entry and leaves them clear)
+		const uint64_t nf = static_cast<uint64_t>(PipelineCodegen::F64Fields(gb));
+		b.SetPtr(cb + 8 + out_words, arena_.Alloc(static_cast<uint64_t>(ctas) * nf * D * 8));
+	}
 	{
 		// initializes the tables of the splits the plan made (a count it reads on the device)
 		const uint64_t words = static_cast<uint64_t>(max_split) * F * D;
