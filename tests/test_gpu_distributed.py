@@ -2,7 +2,8 @@
 plus COUNT(*)), run by the engine, merged and finished on the host, must equal the engine's own run of
 the original plan -- keys, counts, MIN/MAX and 128-bit sums bit for bit, AVG over DOUBLE within 1e-12
 relative (the engine's FP64 sums are order-dependent). C0's 1024 keys take the dense merge; C1's two
-keys (about 24 packed bits) take the hash repartition."""
+keys (about 24 packed bits) take the hash repartition, merged in numpy or re-aggregated by the engine
+(its GROUP BY over the exchanged partial columns)."""
 import datetime
 import socket
 
@@ -29,7 +30,7 @@ def one_rank():
     dist.destroy_process_group()
 
 
-def _compare(plan, inputs, column_types):
+def _compare(plan, inputs, column_types, reaggregate=None):
     from vectisdb_b200.distributed import sharded_group_by
     eng = GpuEngine.instance()
     direct = eng.execute_plan(plan, inputs)
@@ -43,7 +44,7 @@ def _compare(plan, inputs, column_types):
         assert r.success, r.error_message
         return r.columns
 
-    got = sharded_group_by(plan, run_local, column_types)
+    got = sharded_group_by(plan, run_local, column_types, reaggregate=reaggregate)
     assert [n for n, _ in got] == list(plan.group_keys) + [f"agg_{i}" for i in range(len(plan.aggregates))]
     for (name, g), c in zip(got, direct.columns):
         want = c.data[order]
@@ -68,3 +69,20 @@ def test_high_cardinality_keys_and_avg_through_the_engine(one_rank):
     wl = W.c1(n=1 << 18)
     groups = _compare(wl.plan, wl.inputs, {"v": T.FLOAT64})
     assert groups > (1 << 14)
+
+
+def test_high_cardinality_merge_re_aggregated_by_the_engine(one_rank):
+    """The repartitioned partial groups merged by the engine's own GROUP BY (128-bit sums as exact
+    32-bit chunk sums, counts as 128-bit sums, float MIN/MAX as order-preserving integers)."""
+    wl = W.c1(n=1 << 18)
+    eng = GpuEngine.instance()
+    calls = []
+
+    def reaggregate(p, cols):
+        calls.append(len(cols))
+        r = eng.execute_plan(p, cols)
+        assert r.success, r.error_message
+        return r.columns
+
+    groups = _compare(wl.plan, wl.inputs, {"v": T.FLOAT64}, reaggregate)
+    assert groups > (1 << 14) and len(calls) == 1
