@@ -267,6 +267,41 @@ vgpu_status vgpu_nvrtc_compile_check(const char *source, size_t *cubin_bytes);
 vgpu_status vgpu_generate_source(const vgpu_plan *plan, const vgpu_column *inputs, size_t n_inputs,
                                  char *out, size_t capacity, size_t *length);
 
+/* ---- Expression translation (extension/src/expression_translator.cpp:287-460, 489-493) ----------
+ * A bound expression (DuckDB's BoundColumnRef / BoundConstant / BoundComparison / BoundFunction) as a
+ * node array; `children` index into the same array. The translation is the statement the engine's
+ * vgpu_expr contract carries, the ordered input columns it reads and its output type. */
+typedef enum vgpu_bexpr_kind {
+	VGPU_BEXPR_COLUMN = 0,   /* name = the scanned column; return_type its type */
+	VGPU_BEXPR_CONSTANT = 1, /* integer/BOOLEAN value in i64, FLOAT/DOUBLE in f64; is_null refuses */
+	VGPU_BEXPR_COMPARE = 2,  /* name = "=", "!=", "<>", "<", ">", "<=", ">="; two children */
+	VGPU_BEXPR_FUNCTION = 3  /* name = DuckDB function ("+", "-", "*", "/", "%", "__cast", "abs", "sqrt", "ln", ...) */
+} vgpu_bexpr_kind;
+
+typedef struct vgpu_bexpr {
+	uint32_t kind;        /* vgpu_bexpr_kind */
+	uint32_t return_type; /* vgpu_value_type of the expression's DuckDB return type */
+	const char *name;
+	const uint32_t *children;
+	uint32_t n_children;
+	uint32_t is_null;
+	int64_t i64;
+	double f64;
+} vgpu_bexpr;
+
+#define VGPU_TRANSLATE_FP32 1u      /* VECTOR_GPU_FP32_RELAXATION: math functions in float */
+#define VGPU_TRANSLATE_STRICT_FP 2u /* VECTOR_GPU_STRICT_FP: only the bit-exact math functions */
+
+/* TranslateExpression + WrapAsOutputStatement: writes the statement ('\0'-terminated) into `statement`
+ * and the input column names, each '\0'-terminated one after another, into `inputs`; *n_inputs and
+ * *output_type receive their count and the output type. VGPU_ERR_UNSUPPORTED (with the reason in
+ * vgpu_last_error) for shapes the GPU path does not lower; VGPU_ERR_INVALID_ARGUMENT when a buffer is
+ * too small (the needed sizes are in *statement_len / *inputs_len). */
+vgpu_status vgpu_translate_expression(const vgpu_bexpr *nodes, uint32_t n_nodes, uint32_t root, uint32_t flags,
+                                      char *statement, size_t statement_cap, size_t *statement_len, char *inputs,
+                                      size_t inputs_cap, size_t *inputs_len, uint32_t *n_inputs,
+                                      uint32_t *output_type);
+
 /* ---- Cost model (cuda_engine/include/gpu_engine.hpp:187-348; src/gpu_cost_model.cpp) ------- */
 
 typedef struct vgpu_working_set {

@@ -119,6 +119,12 @@ class vgpu_memory_stats(C.Structure):
                 ("allocations", C.c_uint64), ("failed_allocations", C.c_uint64)]
 
 
+class vgpu_bexpr(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("return_type", C.c_uint32), ("name", C.c_char_p),
+                ("children", C.POINTER(C.c_uint32)), ("n_children", C.c_uint32), ("is_null", C.c_uint32),
+                ("i64", C.c_int64), ("f64", C.c_double)]
+
+
 class vgpu_table_ref(C.Structure):
     _fields_ = [("catalog", C.c_char_p), ("schema", C.c_char_p), ("table", C.c_char_p)]
 
@@ -186,6 +192,9 @@ SIGNATURES = [
                                        C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     ("vgpu_is_row_independent", C.c_int, [C.POINTER(vgpu_plan)]),
     ("vgpu_estimate_working_set", C.c_int, [C.POINTER(vgpu_plan), C.c_uint64, C.POINTER(vgpu_working_set)]),
+    ("vgpu_translate_expression", C.c_int, [C.POINTER(vgpu_bexpr), C.c_uint32, C.c_uint32, C.c_uint32, C.c_char_p,
+                                             C.c_size_t, C.POINTER(C.c_size_t), C.c_char_p, C.c_size_t,
+                                             C.POINTER(C.c_size_t), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     ("vgpu_estimate_working_set_for", C.c_int, [C.POINTER(vgpu_plan), C.POINTER(vgpu_column), C.c_size_t,
                                                  C.POINTER(vgpu_exec_options), C.POINTER(vgpu_working_set)]),
     ("vgpu_analyze_plan_shape", C.c_int, [C.POINTER(vgpu_plan), C.POINTER(vgpu_plan_shape)]),

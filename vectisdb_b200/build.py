@@ -35,6 +35,7 @@ ENGINE_SOURCES = [
     "server.cpp",
     "stream_pipeline.cu",
     "noalloc.cu",
+    "translator.cpp",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [

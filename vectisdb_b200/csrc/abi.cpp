@@ -12,6 +12,7 @@
 
 #include "column_cache.hpp"
 #include "cost_model.hpp"
+#include "translator.hpp"
 #include "batch.hpp"
 #include "server.hpp"
 #include "stream_pipeline.hpp"
@@ -677,6 +678,29 @@ vgpu_status vgpu_estimate_working_set_for(const vgpu_plan *plan, const vgpu_colu
 		auto root = ConvertPlan(plan);
 		std::vector<vgpu_column> in(inputs, inputs + n_inputs);
 		*out = EstimateWorkingSetFor(*root, in, options && options->serve_whole_scan_from_cache);
+	});
+}
+
+vgpu_status vgpu_translate_expression(const vgpu_bexpr *nodes, uint32_t n_nodes, uint32_t root, uint32_t flags,
+                                      char *statement, size_t statement_cap, size_t *statement_len, char *inputs,
+                                      size_t inputs_cap, size_t *inputs_len, uint32_t *n_inputs,
+                                      uint32_t *output_type) {
+	return Guard([&] {
+		const TranslatedExpr t = TranslateExpression(nodes, n_nodes, root, flags);
+		std::string names;
+		for (auto &n : t.inputs) {
+			names += n;
+			names.push_back('\0');
+		}
+		if (statement_len) *statement_len = t.statement.size() + 1;
+		if (inputs_len) *inputs_len = names.size();
+		if (n_inputs) *n_inputs = static_cast<uint32_t>(t.inputs.size());
+		if (output_type) *output_type = static_cast<uint32_t>(t.output_type);
+		if (!statement || statement_cap < t.statement.size() + 1 || (!names.empty() && (!inputs || inputs_cap < names.size()))) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "vgpu_translate_expression: output buffer too small");
+		}
+		std::memcpy(statement, t.statement.c_str(), t.statement.size() + 1);
+		if (!names.empty()) std::memcpy(inputs, names.data(), names.size());
 	});
 }
 
