@@ -412,6 +412,38 @@ vgpu_status vgpu_cache_invalidate_all(void);
 uint64_t vgpu_cache_current_bytes(void);
 uint64_t vgpu_cache_table_generation(const vgpu_table_ref *table);
 
+/* ---- Host ingest (extension/src/vector_converter.cpp:87-273, gpu_batch_accumulator.cpp:126-249) -----
+ * One vector of a scanned chunk in DuckDB's UnifiedVectorFormat: logical row i reads physical index
+ * sel[i] (identity when sel is NULL; 0 for every row of a constant vector); validity holds DuckDB's
+ * 64-bit mask words by physical index, LSB first, bit set = valid (NULL = all valid). */
+typedef struct vgpu_vector {
+	const void *data;
+	const uint32_t *sel;
+	const uint64_t *validity;
+	uint32_t constant;
+} vgpu_vector;
+
+/* ConvertVectorToGpuColumn: `count` logical rows (through row_sel first, when given) of a vector of
+ * `type` into dense out_data and, when out_validity is given, an Arrow LSB-first bitmap (bit set =
+ * valid); *any_null says whether a NULL was met (the reference attaches the bitmap only then). */
+vgpu_status vgpu_convert_vector(const vgpu_vector *vector, uint32_t type, uint64_t count, const uint32_t *row_sel,
+                                void *out_data, uint8_t *out_validity, int *any_null);
+
+/* The accumulator + upload of a scan into the device column cache: chunks appended to a handle are
+ * converted into page-locked batches of batch_rows rows; each full batch is uploaded asynchronously on
+ * the handle's own stream and staged in the cache as one chunk per column (no second copy), so the
+ * conversion of the next batch overlaps the transfer. vgpu_ingest_finish uploads the rest, waits and
+ * commits the table (replacing the re-staged columns, keeping the others); a handle destroyed before
+ * finishing aborts its staging. One handle per table scan; calls on one handle are serialized. */
+typedef struct vgpu_ingest vgpu_ingest;
+vgpu_status vgpu_ingest_create(const vgpu_table_ref *table, const char *const *names, const int32_t *types,
+                               size_t n_columns, uint64_t batch_rows, vgpu_ingest **out);
+/* `vectors` holds one vector per column; `row_sel` (optional) selects `count` rows of the chunk. */
+vgpu_status vgpu_ingest_append(vgpu_ingest *ingest, const vgpu_vector *vectors, uint64_t count,
+                               const uint32_t *row_sel);
+vgpu_status vgpu_ingest_finish(vgpu_ingest *ingest, uint64_t *rows);
+void vgpu_ingest_destroy(vgpu_ingest *ingest);
+
 /* ---- Stream pipeline (GpuStreamPipeline, cuda_engine/include/gpu_stream_pipeline.hpp:122-208) -------
  * A row-independent projection chain (PROJECTION+ over SCAN, no filter) run batch by batch with upload,
  * compute and download of consecutive batches overlapping on three streams. vgpu_pipeline_create

@@ -125,6 +125,11 @@ class vgpu_bexpr(C.Structure):
                 ("i64", C.c_int64), ("f64", C.c_double)]
 
 
+class vgpu_vector(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("sel", C.POINTER(C.c_uint32)), ("validity", C.POINTER(C.c_uint64)),
+                ("constant", C.c_uint32)]
+
+
 class vgpu_table_ref(C.Structure):
     _fields_ = [("catalog", C.c_char_p), ("schema", C.c_char_p), ("table", C.c_char_p)]
 
@@ -192,6 +197,13 @@ SIGNATURES = [
                                        C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     ("vgpu_is_row_independent", C.c_int, [C.POINTER(vgpu_plan)]),
     ("vgpu_estimate_working_set", C.c_int, [C.POINTER(vgpu_plan), C.c_uint64, C.POINTER(vgpu_working_set)]),
+    ("vgpu_convert_vector", C.c_int, [C.POINTER(vgpu_vector), C.c_uint32, C.c_uint64, C.POINTER(C.c_uint32),
+                                       C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
+    ("vgpu_ingest_create", C.c_int, [C.POINTER(vgpu_table_ref), C.POINTER(C.c_char_p), C.POINTER(C.c_int32),
+                                      C.c_size_t, C.c_uint64, C.POINTER(C.c_void_p)]),
+    ("vgpu_ingest_append", C.c_int, [C.c_void_p, C.POINTER(vgpu_vector), C.c_uint64, C.POINTER(C.c_uint32)]),
+    ("vgpu_ingest_finish", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    ("vgpu_ingest_destroy", None, [C.c_void_p]),
     ("vgpu_translate_expression", C.c_int, [C.POINTER(vgpu_bexpr), C.c_uint32, C.c_uint32, C.c_uint32, C.c_char_p,
                                              C.c_size_t, C.POINTER(C.c_size_t), C.c_char_p, C.c_size_t,
                                              C.POINTER(C.c_size_t), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),

@@ -36,6 +36,7 @@ ENGINE_SOURCES = [
     "stream_pipeline.cu",
     "noalloc.cu",
     "translator.cpp",
+    "ingest.cpp",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [

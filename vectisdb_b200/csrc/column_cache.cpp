@@ -162,6 +162,44 @@ bool ColumnCache::StageChunk(const TableRef &table, const vgpu_column &chunk) {
 	return true;
 }
 
+bool ColumnCache::StageOwnedChunk(const TableRef &table, const std::string &column, ValueType type, uint64_t rows,
+                                  void *data, uint8_t *valid, cudaStream_t stream) {
+	std::lock_guard<std::mutex> lock(mu_);
+	auto &alloc = Runtime::Get().allocator();
+	auto refuse = [&](Staged *st) {
+		alloc.Free(data, stream);
+		alloc.Free(valid, stream);
+		if (st) {
+			st->failed = true;
+			for (auto &c : st->chunks) {
+				staged_ -= c.bytes;
+				FreeChunk(c);
+			}
+			st->chunks.clear();
+		}
+		return false;
+	};
+	auto it = staging_.find(TableKey(table));
+	if (it == staging_.end()) return refuse(nullptr);
+	Staged &st = it->second[column];
+	if (st.failed) return refuse(nullptr);
+	if (st.type_known && st.type != type) return refuse(&st);
+	const uint64_t bytes = rows * TypeSize(type) + (valid ? rows : 0);
+	if (!MakeRoomLocked(bytes)) return refuse(&st);
+	Chunk c;
+	c.data = data;
+	c.valid = valid;
+	c.rows = rows;
+	c.bytes = bytes;
+	st.type = type;
+	st.type_known = true;
+	st.rows += rows;
+	st.bytes += bytes;
+	staged_ += bytes;
+	st.chunks.push_back(c);
+	return true;
+}
+
 void ColumnCache::CommitStaging(const TableRef &table, uint64_t scanned_rows) {
 	std::lock_guard<std::mutex> lock(mu_);
 	auto tk = TableKey(table);

@@ -23,6 +23,13 @@ public:
 	void EnsureInitialized(double fraction_of_vram);
 	void BeginStaging(const TableRef &table);
 	bool StageChunk(const TableRef &table, const vgpu_column &chunk);
+	//! Stages a chunk whose device buffers the caller allocated from the engine's allocator and filled
+	//! with work on `stream`: the cache takes ownership without copying (data: rows values of `type`;
+	//! valid: one byte per row, 1 = valid, or nullptr). The caller synchronizes `stream` before the
+	//! commit. False (buffers freed on `stream`) when the slot is closed, the type changed or the
+	//! budget has no room.
+	bool StageOwnedChunk(const TableRef &table, const std::string &column, ValueType type, uint64_t rows, void *data,
+	                     uint8_t *valid, cudaStream_t stream);
 	void CommitStaging(const TableRef &table, uint64_t scanned_rows);
 	void AbortStaging(const TableRef &table);
 	std::vector<uint64_t> ReplayableChunkRows(const TableRef &table, const std::vector<std::string> &columns);
