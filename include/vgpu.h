@@ -197,6 +197,13 @@ vgpu_status vgpu_execute_plan(const vgpu_plan *plan, const vgpu_column *inputs, 
  * vgpu_result_free; their memory space is vgpu_exec_options.output_memory. */
 size_t vgpu_result_column_count(const vgpu_result *result);
 vgpu_status vgpu_result_get_column(const vgpu_result *result, size_t index, vgpu_column *out);
+/* Rows [offset, offset + count) of result column `index` as borrowed pointers into the result (no copy):
+ * the emission of STANDARD_VECTOR_SIZE chunks (extension/src/physical_gpu_execute.cpp:506-517). Values
+ * are laid out as DuckDB's flat vectors hold them (HUGEINT as hugeint_t {lower, upper}), and the
+ * validity bitmap, LSB first with bit set = valid, is byte for byte DuckDB's 64-bit validity words, so a
+ * column with validity is sliced at multiples of 64 rows (a 2048-row chunk is 32 whole words). */
+vgpu_status vgpu_result_column_range(const vgpu_result *result, size_t index, uint64_t offset, uint64_t count,
+                                     vgpu_column *out);
 void vgpu_result_free(vgpu_result *result);
 
 /* Copies `bytes` of device memory (a device-resident result column, for instance) to host memory,

@@ -303,3 +303,4 @@ def test_very_long_runs_use_the_load_balanced_join():
     sums, counts = _expected_join_group(lk, lv, rk, rg)
     got = dict(zip(cols[0].data.tolist(), zip(hugeint_to_int(cols[1].data), cols[2].data.tolist())))
     assert got == {g: (sums[g], counts[g]) for g in counts}
+

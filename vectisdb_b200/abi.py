@@ -140,6 +140,7 @@ SIGNATURES = [
     ("vgpu_execute_plan", C.c_int, [C.POINTER(vgpu_plan), C.POINTER(vgpu_column), C.c_size_t,
                                     C.POINTER(vgpu_exec_options), C.POINTER(C.c_void_p)]),
     ("vgpu_result_column_count", C.c_size_t, [C.c_void_p]),
+    ("vgpu_result_column_range", C.c_int, [C.c_void_p, C.c_size_t, C.c_uint64, C.c_uint64, C.POINTER(vgpu_column)]),
     ("vgpu_result_get_column", C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(vgpu_column)]),
     ("vgpu_result_free", None, [C.c_void_p]),
     ("vgpu_batch_options_init", None, [C.POINTER(vgpu_batch_options)]),

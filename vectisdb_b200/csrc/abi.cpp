@@ -560,6 +560,31 @@ vgpu_status vgpu_result_get_column(const vgpu_result *result, size_t index, vgpu
 	});
 }
 
+vgpu_status vgpu_result_column_range(const vgpu_result *result, size_t index, uint64_t offset, uint64_t count,
+                                     vgpu_column *out) {
+	return Guard([&] {
+		if (!result || !out) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		vgpu_column whole;
+		if (vgpu_result_get_column(result, index, &whole) != VGPU_OK) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "vgpu_result_column_range: column index out of range");
+		}
+		if (offset > whole.row_count || count > whole.row_count - offset) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "vgpu_result_column_range: rows [" + std::to_string(offset) + ", " +
+			                                    std::to_string(offset + count) + ") exceed the column's " +
+			                                    std::to_string(whole.row_count));
+		}
+		if (whole.validity != nullptr && offset % 64 != 0) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "vgpu_result_column_range: a column with validity is sliced at multiples "
+			                                "of 64 rows (whole validity words)");
+		}
+		*out = whole;
+		out->row_count = count;
+		const size_t width = TypeSize(static_cast<ValueType>(whole.type));
+		if (whole.data) out->data = static_cast<const uint8_t *>(whole.data) + offset * width;
+		if (whole.validity) out->validity = whole.validity + offset / 8;
+	});
+}
+
 void vgpu_result_free(vgpu_result *result) {
 	if (!result) return;
 	try {

@@ -467,6 +467,52 @@ class GpuEngine:
         return GpuExecutionResult(True, "", abi.OK, columns)
 
 
+    def execute_plan_chunks(self, plan: GpuPlanNode, inputs: Sequence[GpuColumn], chunk_rows: int = 2048,
+                            options: ExecuteOptions | None = None):
+        """Executes `plan` with host results and yields them `chunk_rows` rows at a time (DuckDB's
+        STANDARD_VECTOR_SIZE by default) as lists of (data, validity words or None): the data are numpy
+        views into the result's own memory (vgpu_result_column_range: no copy), valid until the iteration
+        ends; the validity words are DuckDB's 64-bit mask layout. Raises abi.VgpuError when the execution
+        fails."""
+        if chunk_rows <= 0 or chunk_rows % 64:
+            raise ValueError("chunk_rows must be a positive multiple of 64 (whole validity words)")
+        o = options or ExecuteOptions()
+        if o.output_on_device:
+            raise ValueError("chunked emission reads host results")
+        plan_c, _plan_keep = serialize_plan_memo(plan)
+        keep = _Keep()
+        cols = serialize_inputs(inputs, keep)
+        opts = abi.vgpu_exec_options()
+        self.lib.vgpu_exec_options_init(C.byref(opts))
+        opts.serve_whole_scan_from_cache = int(o.serve_whole_scan_from_cache)
+        opts.stream = o.stream or None
+        handle = C.c_void_p()
+        abi.check(self.lib.vgpu_execute_plan(C.byref(plan_c), cols, len(inputs), C.byref(opts), C.byref(handle)))
+        try:
+            ncols = self.lib.vgpu_result_column_count(handle)
+            whole = abi.vgpu_column()
+            abi.check(self.lib.vgpu_result_get_column(handle, 0, C.byref(whole))) if ncols else None
+            rows = int(whole.row_count) if ncols else 0
+            for off in range(0, rows, chunk_rows):
+                count = min(chunk_rows, rows - off)
+                chunk = []
+                for i in range(ncols):
+                    c = abi.vgpu_column()
+                    abi.check(self.lib.vgpu_result_column_range(handle, i, off, count, C.byref(c)))
+                    dt = NUMPY_DTYPE[GpuValueType(c.type)]
+                    data = np.ctypeslib.as_array(C.cast(c.data, C.POINTER(C.c_uint8)), shape=(count * dt.itemsize,)).view(dt)
+                    words = None
+                    if c.validity:  # the chunk's bitmap bytes, padded to whole 64-bit words
+                        nbytes = (count + 7) // 8
+                        raw = np.ctypeslib.as_array(C.cast(c.validity, C.POINTER(C.c_uint8)), shape=(nbytes,))
+                        padded = np.zeros((count + 63) // 64 * 8, dtype=np.uint8)
+                        padded[:nbytes] = raw
+                        words = padded.view(np.uint64)
+                    chunk.append((data, words))
+                yield chunk
+        finally:
+            self.lib.vgpu_result_free(handle)
+
     def prepare_batch(self, plans: Sequence[GpuPlanNode]) -> "PreparedBatch":
         """vgpu_batch_prepare: plans converted, templated and grouped once for repeated execution."""
         keep = _Keep()
