@@ -1230,6 +1230,59 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 				hupd << "\t\t\t\tatomic_" << hkind[i] << "_i64(&HM" << is << "[h], (i64)(" << v << "));\n";
 			}
 		}
+		// Warp-aggregated form (gb.heavy_warp): the lanes of a step holding the same heavy key (found with
+		// __match_any_sync) fold their rows into the group's lowest lane by shuffles -- count, 128-bit
+		// integer sums, FP64 sums, MIN/MAX -- and that lane alone updates the shared state, so a hot key
+		// costs one set of shared atomics per warp step instead of one per row.
+		std::ostringstream hgrp;
+		hgrp << "\t\t\tconst u32 ln_ = threadIdx.x & 31u, lead_ = __ffs(hpeers_) - 1u;\n"
+		     << "\t\t\tu32 gc_ = 1u;\n";
+		for (size_t i = 0; i < gb.aggs.size(); i++) {
+			if (hkind[i].empty()) continue;
+			const std::string is = std::to_string(i);
+			const std::string v = visible_[gb.aggs[i].column].value;
+			if (hkind[i] == "int") {
+				hgrp << "\t\t\tu64 glo" << is << " = (u64)(i64)(" << v << "); i64 ghi" << is << " = ((i64)(" << v
+				     << ") < 0) ? -1 : 0;\n";
+			} else if (hkind[i] == "f64") {
+				hgrp << "\t\t\tdouble gf" << is << " = (double)(" << v << ");\n";
+			} else {
+				hgrp << "\t\t\ti64 gm" << is << " = (i64)(" << v << ");\n";
+			}
+		}
+		hgrp << "\t\t\tfor (u32 m_ = hpeers_ & ~(1u << lead_); m_; m_ &= m_ - 1u) {\n"
+		     << "\t\t\t\tconst u32 src_ = __ffs(m_) - 1u;\n"
+		     << "\t\t\t\tconst bool me_ = ln_ == lead_;\n"
+		     << "\t\t\t\tgc_ += me_ ? 1u : 0u;\n";
+		for (size_t i = 0; i < gb.aggs.size(); i++) {
+			if (hkind[i].empty()) continue;
+			const std::string is = std::to_string(i);
+			if (hkind[i] == "int") {
+				hgrp << "\t\t\t\t{ const u64 ol_ = __shfl_sync(hpeers_, glo" << is << ", src_); const i64 oh_ = __shfl_sync(hpeers_, ghi"
+				     << is << ", src_);\n\t\t\t\t  if (me_) { const u64 nl_ = glo" << is << " + ol_; ghi" << is
+				     << " += oh_ + (nl_ < glo" << is << " ? 1 : 0); glo" << is << " = nl_; } }\n";
+			} else if (hkind[i] == "f64") {
+				hgrp << "\t\t\t\t{ const double o_ = __shfl_sync(hpeers_, gf" << is << ", src_); if (me_) gf" << is << " += o_; }\n";
+			} else {
+				const char *op = hkind[i] == "min" ? "<" : ">";
+				hgrp << "\t\t\t\t{ const i64 o_ = __shfl_sync(hpeers_, gm" << is << ", src_); if (me_ && o_ " << op << " gm" << is
+				     << ") gm" << is << " = o_; }\n";
+			}
+		}
+		hgrp << "\t\t\t}\n\t\t\tif (ln_ == lead_) {\n\t\t\t\tatomicAdd(&HC[h], gc_);\n";
+		for (size_t i = 0; i < gb.aggs.size(); i++) {
+			if (hkind[i].empty()) continue;
+			const std::string is = std::to_string(i);
+			if (hkind[i] == "int") {
+				hgrp << "\t\t\t\tatomic_add_i128_u32x4(&HW" << is << "_0[h], &HW" << is << "_1[h], &HW" << is << "_2[h], &HW" << is
+				     << "_3[h], glo" << is << ", ghi" << is << ");\n";
+			} else if (hkind[i] == "f64") {
+				hgrp << "\t\t\t\tatomicAdd(&HF" << is << "[h], gf" << is << ");\n";
+			} else {
+				hgrp << "\t\t\t\tatomic_" << hkind[i] << "_i64(&HM" << is << "[h], gm" << is << ");\n";
+			}
+		}
+		hgrp << "\t\t\t}\n";
 		std::ostringstream hflush;
 		hflush << "\t\t\tu32 rw[" << RW << "];\n"
 		       << "\t\t\t#pragma unroll\n\t\t\tfor (int q = 0; q < " << RW << "; ++q) rw[q] = 0u;\n"
@@ -1281,10 +1334,18 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		  << "\t\tvgpu_pos[r] = atomicAdd(&vgpu_cursor[keep && vgpu_hv[r] < 0 ? (u32)(k0 >> " << dbits
 		  << ") : P + (threadIdx.x & 31u)], 1u);\n"
 		  << "\t\t}\n"
-		  << item_head << chain_code_ << "\t\tif (keep) {\n"
-		  << "\t\t\tconst int h = vgpu_hv[r];\n"
-		  << "\t\t\tif (h >= 0) {\n" << hupd.str() << "\t\t\t} else {\n"
-		  << "\t\t\tconst u64 key = vgpu_k[r];\n"
+		  << item_head << chain_code_;
+		if (gb.heavy_warp) {
+			// every lane of the warp reaches the match (the item loop has no divergent exit)
+			o << "\t\tconst int hh_ = keep ? vgpu_hv[r] : -1;\n"
+			  << "\t\tconst u32 hpeers_ = __match_any_sync(0xffffffffu, hh_);\n"
+			  << "\t\tif (hh_ >= 0) {\n\t\t\tconst int h = hh_;\n" << hgrp.str() << "\t\t} else if (keep) {\n\t\t{\n";
+		} else {
+			o << "\t\tif (keep) {\n"
+			  << "\t\t\tconst int h = vgpu_hv[r];\n"
+			  << "\t\t\tif (h >= 0) {\n" << hupd.str() << "\t\t\t} else {\n";
+		}
+		o << "\t\t\tconst u64 key = vgpu_k[r];\n"
 		  << "\t\t\tconst u32 pos = vgpu_pos[r];\n"
 		  << "\t\t\tu32 rw[" << RW << "];\n"
 		  << "\t\t\t#pragma unroll\n\t\t\tfor (int q = 0; q < " << RW << "; ++q) rw[q] = 0u;\n"
@@ -2089,7 +2150,7 @@ std::string GroupByKey(const PipelineCodegen::GroupBySpec &gb, bool partitioned)
 		o << static_cast<int>(a.kind) << '/' << a.column << '/' << static_cast<int>(a.input_type) << '/'
 		  << static_cast<int>(a.output_type) << ';';
 	}
-	o << "|db:" << gb.direct_bits << "|bt:" << gb.bucket_threads << "|hv:" << gb.heavy_slots << "|f64l2:" << gb.f64_l2;
+	o << "|db:" << gb.direct_bits << "|bt:" << gb.bucket_threads << "|hv:" << gb.heavy_slots << "|f64l2:" << gb.f64_l2 << "|hw:" << gb.heavy_warp;
 	return o.str();
 }
 

@@ -140,6 +140,9 @@ public:
 		// stays in L2) with fire-and-forget reductions, instead of shared-memory compare-and-swap loops.
 		// Argument word: the region (CTAs x FP64 fields x slots doubles, zero on entry and left zero).
 		bool f64_l2 = false;
+		// Heavy-key partition scatter: lanes of a warp step with the same heavy key combine their rows by
+		// shuffles and one lane updates the CTA's partial state (fewer, uncontended shared atomics).
+		bool heavy_warp = false;
 	};
 
 	//! Group-by kernels (see executor for the argument layout), all in one translation unit:

@@ -427,6 +427,7 @@ std::string GenerateSourceText(const PlanNode &plan, const std::vector<vgpu_colu
 	// ... and its heavy-key variant (sampling kernel, pre-aggregating partition passes)
 	PipelineCodegen::GroupBySpec spec_hv = spec_dp;
 	spec_hv.heavy_slots = 512;
+	spec_hv.heavy_warp = true;
 	spec_hv.f64_l2 = PipelineCodegen::F64Fields(spec_hv) > 0;  // FP64 sums of its bucket pass in L2
 	// ... and both with tiles staged through shared memory by bulk copies
 	Geometry gst = g;

@@ -1187,6 +1187,10 @@ Executor::HeavyPlan Executor::PlanHeavy(const PipelineCodegen::GroupBySpec &gb, 
 	const uint32_t K = HeavyKeyCap();
 	PipelineCodegen::GroupBySpec gbh = gb;
 	gbh.heavy_slots = static_cast<int>(K);
+	{  // heavy rows combined per warp step before the shared atomics (VGPU_GB_HEAVY_WARP=0: one update per row)
+		const char *env = std::getenv("VGPU_GB_HEAVY_WARP");
+		gbh.heavy_warp = !(env && std::strcmp(env, "0") == 0);
+	}
 	HeavyPlan hp;
 	hp.max_keys = K;
 	hp.state_bytes = static_cast<uint64_t>(PipelineCodegen::HeavySlotBytes(gbh));
