@@ -251,14 +251,23 @@ __global__ void __launch_bounds__(kSortBlock) RadixHistKernel(const uint64_t *ke
 	for (int d = threadIdx.x; d < 256; d += kSortBlock) hist[static_cast<uint64_t>(d) * ntiles + blockIdx.x] = counts[d];
 }
 
+// Scatter of one pass: the tile's keys are ranked stably (warp-ordered: a warp's items in order, warps
+// in order), placed in shared memory in digit order, then written out by consecutive threads to
+// consecutive positions of each digit's run, so the global stores are coalesced runs instead of one
+// scattered store per key.
 __global__ void __launch_bounds__(kSortBlock) RadixScatterKernel(const uint64_t *kin, const uint32_t *vin,
                                                                  uint64_t *kout, uint32_t *vout, uint64_t n, int shift,
                                                                  const uint32_t *offsets, uint32_t ntiles) {
 	__shared__ uint32_t wcount[kSortWarps][256];
+	__shared__ uint32_t tile_start[256];  // first local position of each digit in the tile
+	__shared__ uint32_t global_start[256];
+	__shared__ uint64_t skeys[kSortTile];  // the tile in digit order: keys, then (reused) values
+	__shared__ uint8_t sdig[kSortTile];
 	for (int i = threadIdx.x; i < kSortWarps * 256; i += kSortBlock) (&wcount[0][0])[i] = 0;
 	__syncthreads();
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kSortTile + static_cast<uint64_t>(warp) * 32 * kSortItems;
+	const uint64_t tile0 = static_cast<uint64_t>(blockIdx.x) * kSortTile;
+	const uint64_t base = tile0 + static_cast<uint64_t>(warp) * 32 * kSortItems;
 	uint64_t keys[kSortItems];
 	uint32_t vals[kSortItems];
 	uint32_t rank[kSortItems];
@@ -285,24 +294,66 @@ __global__ void __launch_bounds__(kSortBlock) RadixScatterKernel(const uint64_t 
 		__syncwarp();
 	}
 	__syncthreads();
-	if (threadIdx.x < 256) {
+	if (threadIdx.x < 256) {  // per digit: warps' starts within the digit, the digit's count in the tile
 		uint32_t run = 0;
 		for (int w = 0; w < kSortWarps; w++) {
-			uint32_t c = wcount[w][threadIdx.x];
+			const uint32_t c = wcount[w][threadIdx.x];
 			wcount[w][threadIdx.x] = run;
 			run += c;
 		}
+		tile_start[threadIdx.x] = run;  // the count, turned into a start below
+		global_start[threadIdx.x] = offsets[static_cast<uint64_t>(threadIdx.x) * ntiles + blockIdx.x];
 	}
 	__syncthreads();
+	if (threadIdx.x < 32) {  // exclusive scan of the 256 digit counts by one warp (8 per lane)
+		uint32_t c[8], sum = 0;
+#pragma unroll
+		for (int j = 0; j < 8; j++) {
+			c[j] = tile_start[threadIdx.x * 8 + j];
+			sum += c[j];
+		}
+		uint32_t incl = sum;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+			if (lane >= o) incl += y;
+		}
+		uint32_t run = incl - sum;
+#pragma unroll
+		for (int j = 0; j < 8; j++) {
+			tile_start[threadIdx.x * 8 + j] = run;
+			run += c[j];
+		}
+	}
+	__syncthreads();
+	uint32_t lpos[kSortItems];
 #pragma unroll
 	for (int k = 0; k < kSortItems; k++) {
 		const uint64_t idx = base + static_cast<uint64_t>(k) * 32 + lane;
 		if (idx < n) {
 			const uint32_t d = static_cast<uint32_t>(keys[k] >> shift) & 255u;
-			const uint32_t pos = offsets[static_cast<uint64_t>(d) * ntiles + blockIdx.x] + wcount[warp][d] + rank[k];
-			kout[pos] = keys[k];
-			vout[pos] = vals[k];
+			lpos[k] = tile_start[d] + wcount[warp][d] + rank[k];
+			skeys[lpos[k]] = keys[k];
+			sdig[lpos[k]] = static_cast<uint8_t>(d);
 		}
+	}
+	__syncthreads();
+	const uint32_t valid_rows = static_cast<uint32_t>(n - tile0 < kSortTile ? n - tile0 : kSortTile);
+	for (uint32_t i = threadIdx.x; i < valid_rows; i += kSortBlock) {
+		const uint32_t d = sdig[i];
+		kout[global_start[d] + (i - tile_start[d])] = skeys[i];
+	}
+	__syncthreads();
+	uint32_t *svals = reinterpret_cast<uint32_t *>(skeys);
+#pragma unroll
+	for (int k = 0; k < kSortItems; k++) {
+		const uint64_t idx = base + static_cast<uint64_t>(k) * 32 + lane;
+		if (idx < n) svals[lpos[k]] = vals[k];
+	}
+	__syncthreads();
+	for (uint32_t i = threadIdx.x; i < valid_rows; i += kSortBlock) {
+		const uint32_t d = sdig[i];
+		vout[global_start[d] + (i - tile_start[d])] = svals[i];
 	}
 }
 
