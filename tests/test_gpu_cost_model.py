@@ -71,7 +71,9 @@ def _resident(wl):
 
 
 @pytest.mark.parametrize("name", ["c0", "c1", "c2", "c2b", "cp"])
-def test_benchmark_shapes_over_resident_columns(name):
+def test_benchmark_shapes_over_resident_columns(name, monkeypatch):
+    # every run builds its join table (a table kept from the warm-up run would allocate nothing)
+    monkeypatch.setenv("VGPU_JOIN_CACHE", "0")
     wl = {"c0": lambda: W.c0(n=1 << 22), "c1": lambda: W.c1(n=1 << 22), "c2": lambda: W.c2(probe_n=1 << 22, build_n=1 << 20),
           "c2b": lambda: W.c2b(side=2048), "cp": lambda: W.cp(n=1 << 22)}[name]()
     if name == "c1":

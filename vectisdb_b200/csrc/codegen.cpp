@@ -1713,8 +1713,11 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			const std::string one = "u32 gc = valid ? 1u : 0u;";
 			gd.replace(gd.find(one), one.size(), "u32 gc = valid ? (part_rec ? rw[q][1] : 1u) : 0u;");
 		}
-		o << gd
-		  << "\t\t\tconst u32 peers = __match_any_sync(0xffffffffu, slot);\n"
+		o << gd;
+		if (gb.bucket_plain) {  // every record updates its slot itself: no warp grouping, no hot run
+			o << "\t\t\tif (valid) {\n" << update("g", "slot") << "\t\t\t}\n";
+		} else {
+		o << "\t\t\tconst u32 peers = __match_any_sync(0xffffffffu, slot);\n"
 		  << "\t\t\tbool leader = true;\n"
 		  << "\t\t\tfor (u32 todo = __ballot_sync(0xffffffffu, __popc(peers) >= 4); todo;) {\n"
 		  << "\t\t\t\tconst u32 src_ = __ffs(todo) - 1;\n"
@@ -1738,8 +1741,9 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		  << "\t\t\t\t\thot = __shfl_sync(0xffffffffu, slot, src_);\n" << wacc.str()
 		  << "\t\t\t\t\tif (lane == src_) leader = false;\n"
 		  << "\t\t\t\t}\n\t\t\t}\n"
-		  << "\t\t\tif (valid && leader) {\n" << update("g", "slot") << "\t\t\t}\n"
-		  << "\t\t}\n\t}\n"
+		  << "\t\t\tif (valid && leader) {\n" << update("g", "slot") << "\t\t\t}\n";
+		}
+		o << "\t\t}\n\t}\n"
 		  << "\tif (hot != ~0u && lane == 0) {\n" << update("w", "hot") << "\t}\n"
 		  << (gb.f64_l2 ? "\t__threadfence();  // this thread's reductions are performed before the tables are read\n" : "")
 		  << "\t__syncthreads();\n"
@@ -2150,7 +2154,7 @@ std::string GroupByKey(const PipelineCodegen::GroupBySpec &gb, bool partitioned)
 		o << static_cast<int>(a.kind) << '/' << a.column << '/' << static_cast<int>(a.input_type) << '/'
 		  << static_cast<int>(a.output_type) << ';';
 	}
-	o << "|db:" << gb.direct_bits << "|bt:" << gb.bucket_threads << "|hv:" << gb.heavy_slots << "|f64l2:" << gb.f64_l2 << "|hw:" << gb.heavy_warp;
+	o << "|db:" << gb.direct_bits << "|bt:" << gb.bucket_threads << "|hv:" << gb.heavy_slots << "|f64l2:" << gb.f64_l2 << "|hw:" << gb.heavy_warp << "|bp:" << gb.bucket_plain;
 	return o.str();
 }
 

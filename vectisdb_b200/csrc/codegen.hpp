@@ -143,6 +143,9 @@ public:
 		// Heavy-key partition scatter: lanes of a warp step with the same heavy key combine their rows by
 		// shuffles and one lane updates the CTA's partial state (fewer, uncontended shared atomics).
 		bool heavy_warp = false;
+		// Direct-partitioned bucket pass without the warp's equal-slot grouping and hot-key register run:
+		// every record updates its slot with shared atomics (cheaper once heavy keys are pre-aggregated).
+		bool bucket_plain = false;
 	};
 
 	//! Group-by kernels (see executor for the argument layout), all in one translation unit:

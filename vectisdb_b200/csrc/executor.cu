@@ -901,6 +901,9 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 			// FP64 sums of the bucket pass in L2 through reductions (VGPU_GB_F64_L2=0: shared CAS loops)
 			const char *env_l2 = std::getenv("VGPU_GB_F64_L2");
 			gb.f64_l2 = PipelineCodegen::F64Fields(gb) > 0 && !(env_l2 && std::strcmp(env_l2, "0") == 0);
+			// VGPU_GB_BUCKET_PLAIN=1: records update their slots one by one (no warp grouping)
+			const char *env_plain = std::getenv("VGPU_GB_BUCKET_PLAIN");
+			gb.bucket_plain = env_plain && std::strcmp(env_plain, "1") == 0;
 			const uint64_t mask = (1ull << shift) - 1;
 			const uint64_t M = (0x9e3779b97f4a7c15ull & mask) | 1ull;
 			uint64_t inv = M;  // Newton iteration for the inverse mod 2^64: each step doubles the valid bits
