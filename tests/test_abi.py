@@ -105,7 +105,8 @@ def test_working_set_formulas():
     hc.estimated_rows = 300_000  # groups
     ws = estimate_working_set(hc)
     fields = 1 + 2 + 1 + 1  # COUNT, 128-bit SUM, FP64 sum of AVG, MAX
-    hc_b = (1 << 20) * 32 + 300_000 * (16 + 16 + 8 + 8 + 8) + 16384 * 2048 * 4 // 8 + fields * 8 * 4096 * 4 * 148
+    hc_b = ((1 << 20) * 32 + 300_000 * (16 + 16 + 8 + 8 + 8) + min(16384 * 2048 * 4 // 8, (1 << 20) * 8)
+            + fields * 8 * 4096 * min(4 * 148, (1 << 20) // 16384 + 1))
     assert ws.total_bytes == (1 << 20) * 32 + hc_b
 
     big = make_scan(["k"])

@@ -88,7 +88,7 @@ def test_chunks_land_in_the_column_cache_across_batches():
         gk, gv, gw = r.columns
         assert np.array_equal(gk.data, k[kept]) and np.array_equal(gv.data, v[kept])
         valid = w_valid[kept]
-        assert np.array_equal(np.unpackbits(gw.validity, bitorder="little")[: len(kept)].astype(bool), valid)
+        assert np.array_equal(np.asarray(gw.validity, bool), valid)  # per-row validity of the host result
         assert np.array_equal(gw.data[valid], w[kept][valid])
         plan = make_group_by(["k"], [make_aggregate(A.COUNT_STAR, "", T.INT64)], make_scan(["k"], t))
         r = GpuEngine.instance().execute_plan(plan, [], ExecuteOptions(serve_whole_scan_from_cache=True))

@@ -119,8 +119,10 @@ struct Walker {
 				const uint64_t record = (carried + 31) / 32 * 32;
 				bytes = SatMul(c.rows, record);
 				bytes = SatAdd(bytes, SatMul(groups, out_width));
-				bytes = SatAdd(bytes, 16384ull * 2048 * 4 / 8);
-				bytes = SatAdd(bytes, SatMul(fields * 8 * 4096, 4 * 148));
+				// (at most 2^14 partitions x the CTAs' counters, bounded by the rows), and the split tables
+				// (one per partition chunk of at least 16384 rows, at most 4 per SM of 148)
+				bytes = SatAdd(bytes, std::min<uint64_t>(16384ull * 2048 * 4 / 8, SatMul(c.rows, 8)));
+				bytes = SatAdd(bytes, SatMul(fields * 8 * 4096, std::min<uint64_t>(4 * 148, c.rows / 16384 + 1)));
 			}
 			e.rows = groups;
 			e.width = out_width;
