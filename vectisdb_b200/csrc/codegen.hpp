@@ -146,6 +146,9 @@ public:
 		// Direct-partitioned bucket pass without the warp's equal-slot grouping and hot-key register run:
 		// every record updates its slot with shared atomics (cheaper once heavy keys are pre-aggregated).
 		bool bucket_plain = false;
+		// One-pass group-by: fewer than 2^32 items feed it (a multi-match join source counts its matches
+		// too), so shared counts add without carries.
+		bool narrow_count = false;
 	};
 
 	//! Group-by kernels (see executor for the argument layout), all in one translation unit:

@@ -433,17 +433,21 @@ std::string GenerateSourceText(const PlanNode &plan, const std::vector<vgpu_colu
 	PipelineCodegen::GroupBySpec spec_plain = spec_dp;
 	spec_plain.bucket_plain = true;
 	spec_hv.f64_l2 = PipelineCodegen::F64Fields(spec_hv) > 0;  // FP64 sums of its bucket pass in L2
+	PipelineCodegen::GroupBySpec spec_nc = spec_gb;
+	spec_nc.narrow_count = true;  // one-pass tables whose counts take no carries
 	// ... and both with tiles staged through shared memory by bulk copies
 	Geometry gst = g;
 	gst.items = 4;
 	gst.staged = true;
 	// Separate translation units, separated by a marker line: direct, partitioned, key statistics,
-	// direct-partitioned, direct-partitioned with heavy keys, the last two staged, and the plain bucket pass.
+	// direct-partitioned, direct-partitioned with heavy keys, the last two staged, the plain bucket pass,
+	// and the direct one with narrow counts.
 	return cg.EmitGroupBy(spec_gb, false, g) + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_gb, true, g) +
 	       "\n//@@VGPU_TU@@\n" + cg.EmitStats(key_columns, gs) + "\n//@@VGPU_TU@@\n" +
 	       cg.EmitGroupBy(spec_dp, true, g) + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_hv, true, g) +
 	       "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_dp, true, gst) + "\n//@@VGPU_TU@@\n" +
-	       cg.EmitGroupBy(spec_hv, true, gst) + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_plain, true, g);
+	       cg.EmitGroupBy(spec_hv, true, gst) + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_plain, true, g) +
+	       "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_nc, false, g);
 }
 
 } // namespace vgpu

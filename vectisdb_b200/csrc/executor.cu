@@ -823,6 +823,8 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 	uint64_t groups = 0;
 
 	if (direct) {
+		// a CTA's table sees at most n items (a multi-match join source can expand past n: keep carries)
+		gb.narrow_count = !pin.spec.join_multi && n < (1ull << 32);
 		Geometry g;
 		g.block = 512;
 		// a join source's random lookups are independent per row: more rows per thread, more of them in flight
