@@ -604,6 +604,65 @@ vgpu_status vgpu_group_by_count_sum_noalloc(const int32_t *keys, const double *v
                                             uint32_t domain, int32_t *out_keys, int64_t *out_counts,
                                             double *out_sums, uint64_t *out_groups, void *stream);
 
+/* ---- Sharded GROUP BY: the exchange step on the device -----------------------------------------
+ * No counterpart in the reference, which runs on one device (cuda_engine/src/code_generator.cpp:53
+ * takes device 0). A GROUP BY split by rows across GPUs (one process per GPU) runs the plan on each
+ * rank's rows with partial states (AVG as SUM + COUNT), routes every partial group to the rank owning
+ * its key with vgpu_shard_route, moves the rows with one all-to-all (NCCL, the caller's), turns the
+ * received rows into columns with vgpu_shard_columns, re-aggregates them with vgpu_execute_plan (a
+ * GROUP BY over the key word: SUM over FLOAT64 words and over INT64 count / 128-bit-chunk words, MIN
+ * and MAX over INT64 words) and builds the output columns with vgpu_shard_finish. All buffers are
+ * device memory; NULL keys or partial states are refused. */
+typedef enum vgpu_shard_kind {
+	VGPU_SHARD_SUM_F64 = 0,  /* FLOAT64 sum: 1 word (its bits; merged by a FLOAT64 SUM) */
+	VGPU_SHARD_SUM_I128 = 1, /* HUGEINT sum: 4 words, 32-bit chunks c0..c2 unsigned, c3 signed (INT64 SUMs) */
+	VGPU_SHARD_COUNT = 2,    /* integer count: 1 word (INT64 SUM) */
+	VGPU_SHARD_MIN = 3,      /* integer MIN / MAX: 1 word, sign-extended (INT64 MIN / MAX) */
+	VGPU_SHARD_MAX = 4,
+	VGPU_SHARD_MIN_F64 = 5,  /* FLOAT32/FLOAT64 MIN / MAX: 1 word whose signed order is the float order */
+	VGPU_SHARD_MAX_F64 = 6
+} vgpu_shard_kind;
+
+/* 64-bit words per exchanged row: 1 (the packed key) + 4 per SUM_I128 + 1 per other kind. */
+int32_t vgpu_shard_words(const int32_t *kinds, int32_t n_values);
+
+/* Packs `rows` partial groups -- key columns keys[0..n_keys) (integer types), packed as the sum of
+ * (key_j - key_min[j]) << key_shift[j], and partial states values[0..n_values) of kinds[] -- into rows
+ * of vgpu_shard_words() int64 words, written to `send` (device, rows x words, row-major) grouped by
+ * owner rank (mix64(packed key) mod world, mix64 = MurmurHash3's 64-bit finalizer): the rows for rank
+ * r start after send_counts[0..r). send_counts (host, `world` entries) receives the rows per rank.
+ * Queued on `stream` (NULL = the runtime's stream), which is synchronized once for the counts. */
+vgpu_status vgpu_shard_route(const vgpu_column *keys, int32_t n_keys, const int64_t *key_min, const int32_t *key_shift,
+                             const vgpu_column *values, const int32_t *kinds, int32_t n_values, uint64_t rows,
+                             int32_t world, int64_t *send, uint64_t *send_counts, void *stream);
+
+/* Received rows (device, rows x words, row-major) to `words` device columns of `rows` int64 values:
+ * column j at out + j * rows. Queued on `stream`, not synchronized. */
+vgpu_status vgpu_shard_columns(const int64_t *recv, uint64_t rows, int32_t words, int64_t *out, void *stream);
+
+typedef enum vgpu_shard_op {
+	VGPU_SHARD_OUT_WORD = 0,          /* src[0]'s 64-bit word (the low word of a HUGEINT sum) */
+	VGPU_SHARD_OUT_KEY = 1,           /* key column: ((src[0] >> key_shift) & (2^key_bits - 1)) + key_min, as key_type */
+	VGPU_SHARD_OUT_I128 = 2,          /* HUGEINT from the sums of its four chunk words src[0..3] */
+	VGPU_SHARD_OUT_AVG_F64 = 3,       /* FLOAT64: src[0] (a FLOAT64 sum) / count */
+	VGPU_SHARD_OUT_AVG_I128 = 4,      /* FLOAT64: the 128-bit sum of src[0..3] rounded to nearest double, / count */
+	VGPU_SHARD_OUT_F64_FROM_ORDER = 5 /* FLOAT64 from an order-preserving word (MIN_F64 / MAX_F64) */
+} vgpu_shard_op;
+
+typedef struct vgpu_shard_output {
+	int32_t op;          /* vgpu_shard_op */
+	int32_t key_type;    /* OUT_KEY: the key column's vgpu_value_type */
+	int32_t key_shift;   /* OUT_KEY */
+	int32_t key_bits;    /* OUT_KEY */
+	int64_t key_min;     /* OUT_KEY */
+	vgpu_column src[4];  /* re-aggregated columns read (INT64, FLOAT64 or HUGEINT sums; device) */
+	vgpu_column count;   /* AVG ops: the merged count column (INT64 or HUGEINT) */
+	void *dst;           /* device output, `rows` values of the op's type */
+} vgpu_shard_output;
+
+/* Writes each output of outs[0..n_outs) for `rows` merged groups. Queued on `stream`, not synchronized. */
+vgpu_status vgpu_shard_finish(const vgpu_shard_output *outs, int32_t n_outs, uint64_t rows, void *stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

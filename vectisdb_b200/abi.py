@@ -19,6 +19,8 @@ OK, ERR_INVALID_ARGUMENT, ERR_UNSUPPORTED, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_COMP
     ERR_NOT_READY, ERR_TIMEOUT, ERR_REJECTED, ERR_INTERNAL = range(10)
 MEM_HOST, MEM_DEVICE = 0, 1
 EXEC_NO_SYNC = 1
+# vgpu_shard_op
+SHARD_OUT_WORD, SHARD_OUT_KEY, SHARD_OUT_I128, SHARD_OUT_AVG_F64, SHARD_OUT_AVG_I128, SHARD_OUT_F64_FROM_ORDER = range(6)
 
 
 class vgpu_expr(C.Structure):
@@ -54,6 +56,11 @@ class vgpu_plan(C.Structure):
 class vgpu_column(C.Structure):
     _fields_ = [("name", C.c_char_p), ("type", C.c_uint32), ("memory", C.c_uint32),
                 ("data", C.c_void_p), ("validity", C.c_void_p), ("row_count", C.c_uint64)]
+
+
+class vgpu_shard_output(C.Structure):
+    _fields_ = [("op", C.c_int32), ("key_type", C.c_int32), ("key_shift", C.c_int32), ("key_bits", C.c_int32),
+                ("key_min", C.c_int64), ("src", vgpu_column * 4), ("count", vgpu_column), ("dst", C.c_void_p)]
 
 
 class vgpu_exec_options(C.Structure):
@@ -233,6 +240,12 @@ SIGNATURES = [
     ("vgpu_cache_table_generation", C.c_uint64, [C.POINTER(vgpu_table_ref)]),
     ("vgpu_group_by_count_sum_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32, C.c_uint32,
                                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("vgpu_shard_words", C.c_int32, [C.POINTER(C.c_int32), C.c_int32]),
+    ("vgpu_shard_route", C.c_int, [C.POINTER(vgpu_column), C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int32),
+                                   C.POINTER(vgpu_column), C.POINTER(C.c_int32), C.c_int32, C.c_uint64, C.c_int32,
+                                   C.c_void_p, C.POINTER(C.c_uint64), C.c_void_p]),
+    ("vgpu_shard_columns", C.c_int, [C.c_void_p, C.c_uint64, C.c_int32, C.c_void_p, C.c_void_p]),
+    ("vgpu_shard_finish", C.c_int, [C.POINTER(vgpu_shard_output), C.c_int32, C.c_uint64, C.c_void_p]),
 ]
 
 _LIB = None

@@ -34,6 +34,7 @@ ENGINE_SOURCES = [
     "batch.cu",
     "server.cpp",
     "stream_pipeline.cu",
+    "shard.cu",
     "noalloc.cu",
     "translator.cpp",
     "ingest.cpp",

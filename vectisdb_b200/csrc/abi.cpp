@@ -19,6 +19,7 @@
 #include "executor.hpp"
 #include "plan.hpp"
 #include "runtime.hpp"
+#include "shard.hpp"
 
 namespace vgpu {
 std::string Sha256Hex(const void *data, size_t n);
@@ -867,6 +868,42 @@ uint64_t vgpu_cache_table_generation(const vgpu_table_ref *table) {
 	} catch (...) {
 		return 0;
 	}
+}
+
+int32_t vgpu_shard_words(const int32_t *kinds, int32_t n_values) {
+	if (n_values < 0 || (n_values > 0 && !kinds)) return 0;
+	return ShardWords(kinds, n_values);
+}
+
+vgpu_status vgpu_shard_route(const vgpu_column *keys, int32_t n_keys, const int64_t *key_min, const int32_t *key_shift,
+                             const vgpu_column *values, const int32_t *kinds, int32_t n_values, uint64_t rows,
+                             int32_t world, int64_t *send, uint64_t *send_counts, void *stream) {
+	return Guard([&] {
+		if (!keys || !key_min || !key_shift || !send_counts || (n_values > 0 && (!values || !kinds))) {
+			Fail(VGPU_ERR_INVALID_ARGUMENT, "vgpu_shard_route: null argument");
+		}
+		Runtime::Get().EnsureDevice();
+		cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : Runtime::Get().default_stream();
+		ShardRoute(keys, n_keys, key_min, key_shift, values, kinds, n_values, rows, static_cast<uint32_t>(world), send,
+		           send_counts, s);
+	});
+}
+
+vgpu_status vgpu_shard_columns(const int64_t *recv, uint64_t rows, int32_t words, int64_t *out, void *stream) {
+	return Guard([&] {
+		Runtime::Get().EnsureDevice();
+		cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : Runtime::Get().default_stream();
+		ShardColumns(recv, rows, words, out, s);
+	});
+}
+
+vgpu_status vgpu_shard_finish(const vgpu_shard_output *outs, int32_t n_outs, uint64_t rows, void *stream) {
+	return Guard([&] {
+		if (n_outs < 0 || (n_outs > 0 && !outs)) Fail(VGPU_ERR_INVALID_ARGUMENT, "vgpu_shard_finish: null argument");
+		Runtime::Get().EnsureDevice();
+		cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : Runtime::Get().default_stream();
+		ShardFinish(outs, n_outs, rows, s);
+	});
 }
 
 } // extern "C"

@@ -300,31 +300,20 @@ def _reaggregate(got: list[np.ndarray], layout, run) -> tuple[np.ndarray, list[n
     return ukeys, merged
 
 
-def sharded_group_by(node, run_local, column_types=None, device: str = "cpu", reaggregate=None):
-    """A GROUP BY over rows split across ranks. `run_local(plan)` runs `plan` on this rank's rows (with
-    the engine, say `lambda p: GpuEngine.instance().execute_plan(p, my_inputs).columns`) and returns its
-    host result columns (GpuColumn-like: `.data` and `.validity`; the group keys, then one column per
-    aggregate). AVG runs as SUM plus COUNT(*) -- `column_types` maps each AVG input to its value type,
-    which decides the SUM: HUGEINT over integers, DOUBLE over floats -- and is finished after the merge
-    as the engine finishes it (the 128-bit sum correctly rounded to double, then divided by the group's
-    row count). Keys pack like the engine's: each key column offset by its global minimum (found with
-    an all-reduce) in as many bits as its global range needs. A packed domain of at most 2^20 values
-    merges densely and every rank gets the whole result; a larger one merges by hash repartition and
-    each rank gets a disjoint share. Groups come sorted by their keys, first key first. Dictionary-string
-    keys must use one dictionary on every rank. NULL group keys or NULL aggregate outputs are refused on
-    every rank alike. `reaggregate` is passed to repartition_merge_groupby. Returns
-    [(name, numpy array)]: the keys by name, then `agg_<i>` per aggregate of `node`, in order."""
-    import torch.distributed as dist
-    from .engine import GpuAggregateKind as A, GpuOpType, GpuPlanNode, GpuValueType as T, NUMPY_DTYPE, make_aggregate
+def _partial_plan(node, column_types, who: str):
+    """The GROUP BY `node` rewritten to partial states that merge: AVG as SUM (HUGEINT over integers,
+    DOUBLE over floats, per `column_types`) plus one shared COUNT(*). Returns (plan, merge kinds,
+    finish steps, index of the shared count or None)."""
+    from .engine import GpuAggregateKind as A, GpuOpType, GpuPlanNode, GpuValueType as T, make_aggregate
     if node.op_type != GpuOpType.GROUP_BY_AGGREGATE or not node.group_keys:
-        raise ValueError("sharded_group_by: a GROUP BY node with group keys is needed")
+        raise ValueError(f"{who}: a GROUP BY node with group keys is needed")
     column_types = dict(column_types or {})
     plan_aggs, kinds, finish = [], [], []
     count_at = None
     for a in node.aggregates:
         if a.kind == A.AVG:
             if a.input_column not in column_types:
-                raise ValueError(f"sharded_group_by: the value type of AVG input {a.input_column!r} is needed")
+                raise ValueError(f"{who}: the value type of AVG input {a.input_column!r} is needed")
             is_float = T(column_types[a.input_column]) in (T.FLOAT32, T.FLOAT64)
             s = len(plan_aggs)
             plan_aggs.append(make_aggregate(A.SUM, a.input_column, T.FLOAT64 if is_float else T.HUGEINT))
@@ -348,6 +337,27 @@ def sharded_group_by(node, run_local, column_types=None, device: str = "cpu", re
     plan = GpuPlanNode(node.op_type, list(node.children), estimated_rows=node.estimated_rows,
                        estimated_row_width_bytes=node.estimated_row_width_bytes, group_keys=list(node.group_keys),
                        aggregates=plan_aggs)
+    return plan, kinds, finish, count_at
+
+
+def sharded_group_by(node, run_local, column_types=None, device: str = "cpu", reaggregate=None):
+    """A GROUP BY over rows split across ranks. `run_local(plan)` runs `plan` on this rank's rows (with
+    the engine, say `lambda p: GpuEngine.instance().execute_plan(p, my_inputs).columns`) and returns its
+    host result columns (GpuColumn-like: `.data` and `.validity`; the group keys, then one column per
+    aggregate). AVG runs as SUM plus COUNT(*) -- `column_types` maps each AVG input to its value type,
+    which decides the SUM: HUGEINT over integers, DOUBLE over floats -- and is finished after the merge
+    as the engine finishes it (the 128-bit sum correctly rounded to double, then divided by the group's
+    row count). Keys pack like the engine's: each key column offset by its global minimum (found with
+    an all-reduce) in as many bits as its global range needs. A packed domain of at most 2^20 values
+    merges densely and every rank gets the whole result; a larger one merges by hash repartition and
+    each rank gets a disjoint share. Groups come sorted by their keys, first key first. Dictionary-string
+    keys must use one dictionary on every rank. NULL group keys or NULL aggregate outputs are refused on
+    every rank alike. `reaggregate` is passed to repartition_merge_groupby. Returns
+    [(name, numpy array)]: the keys by name, then `agg_<i>` per aggregate of `node`, in order."""
+    import torch.distributed as dist
+    from .engine import GpuValueType as T, NUMPY_DTYPE
+    plan, kinds, finish, count_at = _partial_plan(node, column_types, "sharded_group_by")
+    plan_aggs = plan.aggregates
     cols = list(run_local(plan))
     nk = len(node.group_keys)
     if len(cols) != nk + len(plan_aggs):
@@ -396,6 +406,253 @@ def sharded_group_by(node, run_local, column_types=None, device: str = "cpu", re
             _, s, t = f
             vals = merged[s] if t in (T.HUGEINT, T.FLOAT64) else merged[s].astype(NUMPY_DTYPE[t])
         out.append((f"agg_{i}", vals))
+    return out
+
+
+def _raw_column(result, i: int):
+    """The vgpu_column of a device result (its device data and validity pointers)."""
+    import ctypes as C
+    from . import abi
+    c = abi.vgpu_column()
+    abi.check(abi.lib().vgpu_result_get_column(result._handle, i, C.byref(c)))
+    return c
+
+
+_TORCH_KEY_DTYPE = {"BOOLEAN": "uint8", "INT16": "int16", "INT32": "int32", "INT64": "int64", "DICTIONARY_STRING": "int32"}
+
+
+def device_sharded_group_by(node, inputs, column_types=None):
+    """A GROUP BY over rows split across ranks, merged on the GPUs: the device counterpart of
+    sharded_group_by for the nccl backend (one process per GPU, torch's current device and stream).
+
+    The plan runs on this rank's `inputs` with the engine, results left on the device (partial states:
+    AVG as SUM + COUNT(*), as in sharded_group_by). The key ranges meet in two small all-reduces; every
+    partial group is then packed into one row of 64-bit words and routed to the rank owning its key
+    (vgpu_shard_route), the rows cross the ranks in one all-to-all of device buffers, become columns
+    again (vgpu_shard_columns), are re-aggregated by the engine's GROUP BY on the owning rank, and the
+    output columns are built on the device (vgpu_shard_finish). Nothing passes through the host but the
+    per-rank row counts and the key ranges.
+
+    Returns [(name, torch tensor on this rank's device)]: the keys by name, then `agg_<i>` per aggregate
+    of `node` (HUGEINT as an (n, 2) int64 tensor of {lower, upper}). This rank holds a disjoint share of
+    the groups, in no particular order; the shares of all ranks hold every group once. Exactness as
+    sharded_group_by (FP64 sums merged in an order that depends on the exchange). Every rank makes the
+    same collective calls in the same order; NULL keys or partial states are refused on every rank."""
+    import torch
+    import torch.distributed as dist
+    plan, kinds, finish, count_at = _partial_plan(node, column_types, "device_sharded_group_by")
+    world = dist.get_world_size()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    # Everything -- engine calls, shard kernels, torch allocations and the NCCL exchange -- is ordered on
+    # one stream the engine can be handed (not the legacy default stream, which the engine's own stream
+    # does not wait on).
+    caller = torch.cuda.current_stream()
+    side = caller if caller.cuda_stream != 0 else torch.cuda.Stream()
+    side.wait_stream(caller)
+    with torch.cuda.stream(side):
+        out = _device_sharded_group_by_on(node, inputs, plan, kinds, finish, count_at, world, dev, side.cuda_stream)
+    if side is not caller:
+        caller.wait_stream(side)
+        for _, t in out:
+            t.record_stream(caller)
+    return out
+
+
+def _device_sharded_group_by_on(node, inputs, plan, kinds, finish, count_at, world, dev, sp):
+    import torch
+    import torch.distributed as dist
+    from .engine import (DeviceResult, ExecuteOptions, GpuAggregateKind as A, GpuEngine, GpuValueType as T,
+                         make_aggregate, make_device_column, make_group_by, make_scan)
+    opts = ExecuteOptions(output_on_device=True, stream=sp)
+    eng = GpuEngine.instance()
+    nk = len(node.group_keys)
+    held = []
+
+    def run(p, cols):
+        r = eng.execute_plan(p, cols, opts)
+        if not isinstance(r, DeviceResult):
+            raise RuntimeError(f"device_sharded_group_by: {r.error_message}")
+        held.append(r)
+        return r
+
+    try:
+        local = run(plan, inputs)
+        raw = [_raw_column(local, i) for i in range(len(local.columns))]
+        if len(raw) != nk + len(plan.aggregates):
+            raise ValueError("device_sharded_group_by: the local result has the wrong number of columns")
+        rows = int(raw[0].row_count)
+        key_types = [T(c.type) for c in raw[:nk]]
+        nulls = any(bool(c.validity) for c in raw)
+        info = np.iinfo(np.int64)
+        lo_l, hi_l = [info.max] * nk, [info.min] * nk
+        if rows:  # local key ranges: the engine's MIN/MAX without group keys over the key columns
+            names = [f"k{j}" for j in range(nk)]
+            aggs = [make_aggregate(kd, n, t) for n, t in zip(names, key_types) for kd in (A.MIN, A.MAX)]
+            mm = eng.execute_plan(make_group_by([], aggs, make_scan(names)),
+                                  [make_device_column(n, t, int(c.data), rows) for n, t, c in zip(names, key_types, raw)],
+                                  ExecuteOptions(stream=sp))
+            if not mm.success:
+                raise RuntimeError(f"device_sharded_group_by: {mm.error_message}")
+            lo_l = [int(mm.columns[2 * j].data[0]) for j in range(nk)]
+            hi_l = [int(mm.columns[2 * j + 1].data[0]) for j in range(nk)]
+        lo = _all_reduce(np.array(lo_l, np.int64), dist.ReduceOp.MIN, dev)
+        hi = _all_reduce(np.array(hi_l + [int(nulls)], np.int64), dist.ReduceOp.MAX, dev)
+        if hi[-1]:
+            raise ValueError("device_sharded_group_by: NULL group keys or NULL aggregate values do not merge here")
+        hi = hi[:-1]
+        empty = bool(lo[0] > hi[0])
+        bits = [0] * nk if empty else [int(h - l).bit_length() for l, h in zip(lo.tolist(), hi.tolist())]
+        if sum(bits) > 63:
+            raise ValueError("device_sharded_group_by: the group keys need more than 63 bits packed")
+        shifts = [sum(bits[i + 1:]) for i in range(nk)]
+        send, send_splits = _route_partials(raw, nk, kinds, [int(x) for x in lo.tolist()], shifts, world, sp)
+        recv = exchange_rows(send, send_splits)
+        del send
+        return _merge_exchanged(recv, kinds, finish, count_at, list(node.group_keys), key_types, shifts, bits,
+                                [int(x) for x in lo.tolist()], run, sp)
+    finally:
+        for r in held:  # frees on the stream the work was queued on, after it
+            r.free()
+
+
+def exchange_rows(send, send_splits):
+    """The all-to-all of routed rows: `send` is a (rows, words) int64 tensor on this rank's device (CUDA
+    with nccl, CPU with gloo) whose first send_splits[0] rows go to rank 0, the next send_splits[1] to
+    rank 1, and so on. The row counts cross first (one all-to-all of `world` int64), then the rows (one
+    all-to-all). Returns the received rows, sender by sender, as a (received rows, words) tensor."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size()
+    if len(send_splits) != world or sum(send_splits) != int(send.shape[0]):
+        raise ValueError("exchange_rows: one row count per rank, summing to the rows sent")
+    dev = send.device
+    recv_counts = torch.empty(world, dtype=torch.int64, device=dev)
+    dist.all_to_all_single(recv_counts, torch.tensor(list(send_splits), dtype=torch.int64, device=dev))
+    recv_splits = recv_counts.cpu().tolist()
+    recv = torch.empty((int(sum(recv_splits)), int(send.shape[1])), dtype=torch.int64, device=dev)
+    dist.all_to_all_single(recv, send, recv_splits, list(send_splits))
+    return recv
+
+
+def _route_partials(raw, nk: int, kinds, lo, shifts, world: int, stream: int):
+    """vgpu_shard_route over a device result's columns (nk keys, then the partial states): the rows as
+    an int64 (rows, words) tensor grouped by owner rank, and the rows per rank (host list)."""
+    import ctypes as C
+    import torch
+    from . import abi
+    L = abi.lib()
+    rows = int(raw[0].row_count)
+    codes = [KINDS.index(k) for k in kinds]
+    kinds_c = (C.c_int32 * max(1, len(codes)))(*codes)
+    words = int(L.vgpu_shard_words(kinds_c, len(codes)))
+    send = torch.empty((rows, words), dtype=torch.int64, device=torch.device("cuda", torch.cuda.current_device()))
+    counts = (C.c_uint64 * world)()
+    abi.check(L.vgpu_shard_route((abi.vgpu_column * nk)(*raw[:nk]), nk, (C.c_int64 * nk)(*lo), (C.c_int32 * nk)(*shifts),
+                                 (abi.vgpu_column * max(1, len(codes)))(*raw[nk:]), kinds_c, len(codes), rows, world,
+                                 C.c_void_p(send.data_ptr() if rows else 0), counts, C.c_void_p(stream)))
+    return send, [int(x) for x in counts]
+
+
+def _merge_exchanged(recv, kinds, finish, count_at, key_names, key_types, shifts, bits, lo, run, stream: int):
+    """Received partial-group rows (int64 (R, words) device tensor) re-aggregated by the engine's GROUP
+    BY (`run(plan, columns)` returns a device result it keeps alive) and finished into the query's output
+    columns: [(name, tensor)] as device_sharded_group_by returns them."""
+    import ctypes as C
+    import torch
+    from . import abi
+    from .engine import GpuAggregateKind as A, GpuValueType as T, make_aggregate, make_device_column, make_group_by, make_scan
+    L = abi.lib()
+    dev = recv.device
+    R, W = int(recv.shape[0]), int(recv.shape[1])
+    nk = len(key_names)
+    out_names = list(key_names) + [f"agg_{i}" for i in range(len(finish))]
+    if R == 0:  # nothing arrived: no engine call (no collective follows, so ranks stay in step)
+        return _empty_device_outputs(out_names, key_types, finish, kinds, dev)
+    cols = torch.empty((W, R), dtype=torch.int64, device=dev)
+    abi.check(L.vgpu_shard_columns(C.c_void_p(recv.data_ptr()), R, W, C.c_void_p(cols.data_ptr()), C.c_void_p(stream)))
+    names, dcols, aggs, at = ["k"], [make_device_column("k", T.INT64, cols[0].data_ptr(), R)], [], []
+    w = 1
+    for kind in kinds:
+        at.append(len(aggs))
+        for _ in range(4 if kind == "sum_i128" else 1):
+            name = f"w{w}"
+            names.append(name)
+            if kind == "sum_f64":
+                dcols.append(make_device_column(name, T.FLOAT64, cols[w].data_ptr(), R))
+                aggs.append(make_aggregate(A.SUM, name, T.FLOAT64))
+            else:
+                dcols.append(make_device_column(name, T.INT64, cols[w].data_ptr(), R))
+                if kind in ("min", "max", "min_f64", "max_f64"):
+                    aggs.append(make_aggregate(A.MIN if kind.startswith("min") else A.MAX, name, T.INT64))
+                else:
+                    aggs.append(make_aggregate(A.SUM, name, T.HUGEINT))
+            w += 1
+    merged = run(make_group_by(["k"], aggs, make_scan(names)), dcols)
+    mraw = [_raw_column(merged, i) for i in range(len(merged.columns))]
+    G = int(mraw[0].row_count)
+    outs, tensors = [], []
+
+    def output(op, dst, srcs=(), count=None, key=None):
+        o = abi.vgpu_shard_output()
+        o.op = op
+        for j, c in enumerate(srcs):
+            o.src[j] = c
+        if count is not None:
+            o.count = count
+        if key is not None:
+            o.key_type, o.key_shift, o.key_bits, o.key_min = key
+        o.dst = dst.data_ptr()
+        outs.append(o)
+        tensors.append(dst)
+
+    for j in range(nk):
+        t = torch.empty(G, dtype=getattr(torch, _TORCH_KEY_DTYPE[key_types[j].name]), device=dev)
+        output(abi.SHARD_OUT_KEY, t, [mraw[0]], key=(int(key_types[j]), shifts[j], bits[j], int(lo[j])))
+    count_col = mraw[1 + at[count_at]] if count_at is not None else None
+    for f in finish:
+        s = f[1]
+        src = mraw[1 + at[s]: 1 + at[s] + (4 if kinds[s] == "sum_i128" else 1)]
+        if f[0] == "avg":
+            op = abi.SHARD_OUT_AVG_F64 if f[2] else abi.SHARD_OUT_AVG_I128
+            output(op, torch.empty(G, dtype=torch.float64, device=dev), src, count=count_col)
+        elif kinds[s] == "sum_i128":
+            output(abi.SHARD_OUT_I128, torch.empty((G, 2), dtype=torch.int64, device=dev), src)
+        elif kinds[s] in ("min_f64", "max_f64"):
+            output(abi.SHARD_OUT_F64_FROM_ORDER, torch.empty(G, dtype=torch.float64, device=dev), src)
+        elif kinds[s] == "sum_f64":
+            output(abi.SHARD_OUT_WORD, torch.empty(G, dtype=torch.float64, device=dev), src)
+        else:
+            output(abi.SHARD_OUT_WORD, torch.empty(G, dtype=torch.int64, device=dev), src)
+    abi.check(L.vgpu_shard_finish((abi.vgpu_shard_output * len(outs))(*outs), len(outs), G, C.c_void_p(stream)))
+    result = []
+    for name, t, f in zip(out_names, tensors, [None] * nk + list(finish)):
+        if f is not None and f[0] == "col" and kinds[f[1]] in ("count", "min", "max", "min_f64", "max_f64"):
+            want = _torch_dtype_of(f[2])
+            if want is not None and t.dtype != want:
+                t = t.to(want)
+        result.append((name, t))
+    return result
+
+
+def _torch_dtype_of(t):
+    import torch
+    return {"INT16": torch.int16, "INT32": torch.int32, "INT64": torch.int64, "FLOAT32": torch.float32,
+            "FLOAT64": torch.float64, "BOOLEAN": torch.uint8}.get(t.name)
+
+
+def _empty_device_outputs(names, key_types, finish, kinds, dev):
+    """The outputs of a rank that received no groups (the same names, dtypes and shapes, no rows)."""
+    import torch
+    out = [(name, torch.empty(0, dtype=getattr(torch, _TORCH_KEY_DTYPE[t.name]), device=dev))
+           for name, t in zip(names, key_types)]
+    for i, f in enumerate(finish):
+        if f[0] == "avg":
+            t = torch.empty(0, dtype=torch.float64, device=dev)
+        elif kinds[f[1]] == "sum_i128":
+            t = torch.empty((0, 2), dtype=torch.int64, device=dev)
+        else:
+            t = torch.empty(0, dtype=_torch_dtype_of(f[2]) or torch.int64, device=dev)
+        out.append((f"agg_{i}", t))
     return out
 
 
