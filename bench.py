@@ -820,6 +820,102 @@ def measure_c4(args, world: int, rank: int, local: int, rates, n_req: int, sampl
     return out
 
 
+class _Share:
+    """A sharded step's output columns (torch tensors), dropped by free() like an engine result."""
+
+    def __init__(self, cols):
+        self.cols = cols
+
+    def free(self):
+        self.cols = None
+
+
+def measure_sharded(args, world: int, rank: int, local: int, steps: int, blocks: int, sample_clocks: bool):
+    """c1 as ONE query split by rows across the ranks: rank r holds its own slice of 2^27 rows (rank 0's
+    is the one-GPU c1 table, seed 1; rank r > 0 draws from seed 1 + r), runs the GROUP BY on it, and the
+    partial groups are merged on the GPUs (distributed.device_sharded_group_by: routing kernel, NCCL
+    all-to-all of device rows, engine re-aggregation, finish kernels). Every timed step is the whole
+    distributed query; value = rows of all ranks / time (max over ranks). Parity: at one rank, the
+    merged groups against the oracle on the same table."""
+    import datetime
+    import socket
+    import torch.distributed as dist
+    own_group = not dist.is_initialized()
+    if own_group:  # one GPU: a one-rank nccl group, so the exchange runs as it does on N ranks
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                                timeout=datetime.timedelta(seconds=120))
+    try:
+        return _measure_sharded(args, world, rank, local, steps, blocks, sample_clocks)
+    finally:
+        if own_group:
+            dist.destroy_process_group()
+
+
+def _measure_sharded(args, world, rank, local, steps, blocks, sample_clocks):
+    import torch
+    from vectisdb_b200 import ColumnCache, GpuTableRef
+    from vectisdb_b200 import workloads as W
+    from vectisdb_b200.distributed import device_sharded_group_by
+    from vectisdb_b200.engine import GpuValueType as T
+
+    rows = args.rows or W.C1_ROWS
+    wl = W.c1(n=rows, seed=1 + rank, pinned=True, table="c1_shard")
+    ref = GpuTableRef("memory", "main", "c1_shard")
+    ColumnCache.put_table(ref, wl.inputs)
+    cols = [ColumnCache.device_column(ref, c.name, rows) for c in wl.inputs]
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        def step():
+            return _Share(device_sharded_group_by(wl.plan, cols, {"v": T.FLOAT64}))
+
+        sampler = ClockSampler(local) if sample_clocks else None
+        if sampler:
+            sampler.start()
+        t_start = time.time()
+        for _ in range(args.warmup):
+            step().free()
+        while time.time() - t_start < (1.0 if sampler else 0.2):
+            step().free()
+        blocks_ms, launches, prof, last = timed_blocks(step, steps, blocks, side, world, sampler)
+        clocks = sampler.stop() if sampler else None
+        host = [(name, t.cpu().numpy()) for name, t in last.cols]
+        last.free()
+    elapsed_ms = float(np.median(blocks_ms))
+    value = rows * steps * world / (elapsed_ms / 1000.0)
+    groups = len(host[0][1]) if host else 0
+    passing = int(host[4][1].sum()) if host else 0
+    parity = None
+    if world == 1 and args.parity:
+        d = dict(host)
+        order = np.lexsort((d["b"], d["a"]))
+        s = d["agg_0"][order]
+        hug = np.empty(len(order), dtype=[("lower", "<u8"), ("upper", "<i8")])
+        hug["lower"], hug["upper"] = s[:, 0].view(np.uint64), s[:, 1]
+        parity = parity_check("c1", [d["a"][order], d["b"][order], hug, d["agg_1"][order], d["agg_2"][order],
+                                     d["agg_3"][order]], oracle_result("c1", wl))
+    ColumnCache.invalidate_table(ref)
+    per = kernel_table(prof)
+    roofline, kernels = roofline_of("c1", wl, per, passing, groups)
+    exchange = {k: v for k, v in kernels.items() if k.startswith("shard_")}
+    out = {"metric": "c1_rows_per_s", "value": value, "unit": "rows/s", "ms_per_step": elapsed_ms / steps,
+           "steps": steps, "blocks_ms_per_step": [round(b / steps, 4) for b in blocks_ms],
+           "config": {"workload": "c1", "rows": rows * world, "rows_per_rank": rows, "bytes_per_row": 32.0,
+                      "inputs": "resident in the device column cache (larger than L2, no flush needed)",
+                      "timing": f"median of {blocks} timed blocks of {steps} steps",
+                      "merge": "partial groups routed to owner ranks, NCCL all-to-all of device rows, "
+                               "engine re-aggregation"},
+           "parity": parity, "result_rows_rank0": groups, "roofline": roofline, "kernels": kernels,
+           "exchange_kernels": exchange, "e2e": None, "gpu_launches": launches, "clocks": clocks,
+           "cpu_baseline": None}
+    del wl
+    gc.collect()
+    return out
+
+
 def run_reference(args, world, rank):
     """The reference arm: the CPU restatement of the query (oracle/oracle.cpp, OpenMP, every host
     core) on the same full-size table the GPU arm runs, timed per step like it. Rank 0 only."""
@@ -879,6 +975,9 @@ def main():
     p.add_argument("--per-config", choices=["auto", "on", "off"], default="auto",
                    help="also measure every other query (auto: with the c1 headline at full size on one GPU)")
     p.add_argument("--rows", type=int, default=0, help="small-case size for profiling (0 = the full workload)")
+    p.add_argument("--mode", choices=["replicas", "sharded"], default="replicas",
+                   help="N>1: independent replicas of the query (default), or c1 as one query split by rows "
+                        "across the ranks with the partial groups merged on the GPUs")
     args = p.parse_args()
     world, rank, local = dist_setup()
 
@@ -899,7 +998,11 @@ def main():
 
     name = args.config
     cpu_reps = 0 if args.no_cpu_baseline or rank != 0 else (2 if name in ("c1", "c2", "c2dup") else 3)
-    if name == "c3":
+    if args.mode == "sharded":
+        if name != "c1":
+            raise SystemExit("--mode sharded runs the c1 query")
+        line = measure_sharded(args, world, rank, local, args.steps, args.blocks, True)
+    elif name == "c3":
         line = measure_c3(args, world, rank, local, args.steps, args.blocks, 0 if args.no_cpu_baseline else 64, True)
     elif name == "c4":
         rates = [50.0, 100.0, 200.0, 400.0, 800.0, 1600.0, 3200.0, 6400.0, 12800.0, 25600.0]
@@ -908,8 +1011,9 @@ def main():
         line = measure_plain(name, args, world, rank, local, args.steps, args.blocks, args.e2e_steps, cpu_reps, True)
     line.update({"n_gpus": world, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                  "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic"})
-    line["config"]["parallelism"] = f"replicas x{world}"
-    per_config = args.per_config == "on" or (args.per_config == "auto" and name == "c1" and world == 1 and not args.rows)
+    line["config"]["parallelism"] = f"row-sharded x{world}" if args.mode == "sharded" else f"replicas x{world}"
+    per_config = args.per_config == "on" or (args.per_config == "auto" and name == "c1" and world == 1 and not args.rows
+                                             and args.mode == "replicas")
     if per_config:
         per = {}
         for other in PER_CONFIG_ORDER:
