@@ -775,9 +775,15 @@ def measure_c4(args, world: int, rank: int, local: int, rates, n_req: int, sampl
 
     # warm-up: every kernel shape of the mix compiled, the memory pool grown to the mix's peak; the
     # served and the serial results of every request are compared here
-    _, served_res = serve(1e6, 8, 64, keep=True)
-    _, serial_res = serve(1e6, 1, 1, keep=True)
-    results_match = all(same(a, b) for a, b in zip(served_res, serial_res))
+    served_info, served_res = serve(1e6, 8, 64, keep=True)
+    serial_info, serial_res = serve(1e6, 1, 1, keep=True)
+    mismatched = [i for i, (a, b) in enumerate(zip(served_res, serial_res)) if not same(a, b)]
+    results_match = not mismatched
+    mismatch_examples = [{"request": i, "kind": trace[i][0], "rows": trace[i][3],
+                          "served_rows": None if served_res[i] is None else len(served_res[i][0]),
+                          "serial_rows": None if serial_res[i] is None else len(serial_res[i][0])}
+                         for i in mismatched[:4]]
+    failed_warmup = {"served": served_info["failed"], "serial": serial_info["failed"]}
     del served_res, serial_res
     sampler = ClockSampler(local) if sample_clocks else None
     if sampler:
@@ -809,6 +815,7 @@ def measure_c4(args, world: int, rank: int, local: int, rates, n_req: int, sampl
                    "p99_ms": top["serial"]["p99_ms"]},
         "served_over_serial": top["served"]["rows_per_s"] / top["serial"]["rows_per_s"],
         "results_match_serial": bool(results_match),
+        "mismatches": len(mismatched), "mismatch_examples": mismatch_examples, "failed_in_comparison": failed_warmup,
         "sweep": sweep,
         "e2e": None,
         "gpu_launches": launches,

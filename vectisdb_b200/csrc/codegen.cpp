@@ -689,12 +689,15 @@ std::string UpdateCode(const std::vector<Field> &fields, const std::string &tab,
 }
 
 // Merge of source table slot into destination table slot (both u64 field arrays).
+// `l2_src`: FP64 sum fields of the source live in global memory updated by reductions; they are read
+// through L2 (__ldcg), past any line this SM's L1 might hold.
 std::string MergeCode(const std::vector<Field> &fields, const std::string &src, const std::string &ss,
-                      const std::string &dst, const std::string &ds) {
+                      const std::string &dst, const std::string &ds, bool l2_src = false) {
 	std::ostringstream o;
 	for (size_t i = 0; i < fields.size(); i++) {
 		auto &f = fields[i];
 		std::string ps = src + std::to_string(i) + "[" + ss + "]";
+		if (l2_src && f.kind == "f64") ps = "__ldcg(&" + ps + ")";
 		std::string pd = dst + std::to_string(i) + " + " + ds;
 		if (f.kind == "cnt") {
 			o << "\t\t\tatomicAdd(" << pd << ", " << ps << ");\n";
@@ -912,11 +915,21 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			o << "\t\t((u64*)a.w[" << cb + 1 + f << "])[s] = " << InitValue(fields[f]) << ";\n";
 		}
 		o << "\t}\n}\n\n";
+		// With f64_l2 the FP64 sums leave shared memory (where an FP64 atomic add is a compare-and-swap
+		// loop) for this CTA's own region of a global array (arg cb+2+F+out_words), updated by native L2
+		// reductions; the region stays L2-resident (D * 8 bytes per sum and CTA).
+		const bool l2 = gb.f64_l2;
+		const int nl2 = l2 ? F64Fields(gb) : 0;
 		o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_gb_direct(KArgs a) {\n"
 		  << kKernelHead << "\textern __shared__ __align__(16) u64 vgpu_smem[];\n"
 		  << "\tconst u64 D = a.w[" << cb << "];\n";
-		for (int f = 0; f < F; f++) {
-			o << "\tu64 *T" << f << " = vgpu_smem + " << f << " * D;\n";
+		for (int f = 0, sh = 0, gl = 0; f < F; f++) {
+			if (l2 && fields[f].kind == "f64") {
+				o << "\tu64 *T" << f << " = (u64*)a.w[" << cb + 2 + F + out_words << "] + ((u64)blockIdx.x * " << nl2
+				  << " + " << gl++ << ") * D;\n";
+			} else {
+				o << "\tu64 *T" << f << " = vgpu_smem + " << sh++ << " * D;\n";
+			}
 		}
 		o << "\tfor (u64 s = threadIdx.x; s < D; s += " << g.block << ") {\n";
 		for (int f = 0; f < F; f++) {
@@ -927,12 +940,14 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		  << LoadBlock(g, needed, false) << ItemOpen(g, needed) << chain_code_ << "\t\tif (keep) {\n"
 		  << "\t\t\tconst u64 slot = " << pack.str() << ";\n"
 		  << UpdateCode(fields, "T", "slot", pipe_values, true, gb.narrow_count) << "\t\t}\n" << ItemClose()
-		  << "\t}\n\t__syncthreads();\n";
+		  << "\t}\n"
+		  << (l2 ? "\t__threadfence();  // this thread's reductions are performed before the sums are read\n" : "")
+		  << "\t__syncthreads();\n";
 		for (int f = 0; f < F; f++) {
 			o << "\tu64 *G" << f << " = (u64*)a.w[" << cb + 1 + f << "];\n";
 		}
 		o << "\tfor (u64 s = threadIdx.x; s < D; s += " << g.block << ") {\n\t\tif (T0[s] != 0) {\n"
-		  << MergeCode(fields, "T", "s", "G", "s") << "\t\t}\n\t}\n}\n\n";
+		  << MergeCode(fields, "T", "s", "G", "s", l2) << "\t\t}\n\t}\n}\n\n";
 		// final: one CTA compacts the non-empty groups in key order
 		o << "extern \"C\" __global__ void vgpu_gb_direct_final(KArgs a) {\n"
 		  << "\t__shared__ u32 scan_scratch[33];\n"

@@ -136,9 +136,10 @@ public:
 		// partial states during the scatter and leave as one partial record per key and CTA instead
 		// of one record per row.
 		int heavy_slots = 0;
-		// Direct-partitioned bucket pass: FP64 sums accumulate in a per-CTA table in global memory (it
-		// stays in L2) with fire-and-forget reductions, instead of shared-memory compare-and-swap loops.
-		// Argument word: the region (CTAs x FP64 fields x slots doubles, zero on entry and left zero).
+		// FP64 sums accumulate in a per-CTA table in global memory (it stays in L2) with fire-and-forget
+		// reductions, instead of shared-memory compare-and-swap loops. Direct-partitioned bucket pass:
+		// the region (CTAs x FP64 fields x slots doubles) is zero on entry and left zero. One-pass
+		// group-by: argument word cb+2+F+outputs, CTAs x FP64 fields x D doubles, set by each CTA.
 		bool f64_l2 = false;
 		// Heavy-key partition scatter: lanes of a warp step with the same heavy key combine their rows by
 		// shuffles and one lane updates the CTA's partial state (fewer, uncontended shared atomics).

@@ -778,8 +778,13 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 	const auto &props = Runtime::Get().props();
 	const int F = PipelineCodegen::StateWords(gb);
 	const uint64_t domain = 1ull << shift;
-	const uint64_t direct_smem = domain * static_cast<uint64_t>(F) * 8;
+	uint64_t direct_smem = domain * static_cast<uint64_t>(F) * 8;
 	const bool direct = direct_smem <= 96 * 1024;
+	// FP64 sums of the one-pass group-by in L2-resident per-CTA tables (VGPU_GB_DIRECT_F64_L2=1)
+	const char *env_dl2 = std::getenv("VGPU_GB_DIRECT_F64_L2");
+	const int direct_f64 = PipelineCodegen::F64Fields(gb);
+	const bool direct_l2 = direct && direct_f64 > 0 && env_dl2 && std::strcmp(env_dl2, "1") == 0;
+	if (direct_l2) direct_smem = domain * static_cast<uint64_t>(F - direct_f64) * 8;
 	if (!direct && pin.spec.join_multi) {
 		// the partitioned strategies take one item per input row: expand the join's matches into a
 		// relation first, then group that
@@ -825,6 +830,7 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 	if (direct) {
 		// a CTA's table sees at most n items (a multi-match join source can expand past n: keep carries)
 		gb.narrow_count = !pin.spec.join_multi && n < (1ull << 32);
+		gb.f64_l2 = direct_l2;
 		Geometry g;
 		g.block = 512;
 		// a join source's random lookups are independent per row: more rows per thread, more of them in flight
@@ -855,6 +861,7 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 		const uint64_t ntiles = (n + g.tile() - 1) / g.tile();
 		const unsigned grid =
 		    static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ntiles, uint64_t(props.sm_count) * occ)));
+		if (direct_l2) a.SetPtr(cb + 2 + F + out_words, arena_.AllocT<uint64_t>(uint64_t(grid) * direct_f64 * domain));
 		LaunchGenerated(*module, "vgpu_gb_direct", grid, g.block, smem, stream_, a, in_bytes, n);
 		LaunchGenerated(*module, "vgpu_gb_direct_final", 1, 1024, 0, stream_, a, domain * F * 8, domain);
 		groups = ReadU64(count);

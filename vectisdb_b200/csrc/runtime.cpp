@@ -28,27 +28,46 @@ PinnedPool &PinnedPool::Get() {
 	return *p;
 }
 
+size_t PinnedPool::Budget() {
+	if (budget_ == 0) {
+		budget_ = 16ull << 30;
+		if (const char *env = std::getenv("VECTOR_GPU_PINNED_CACHE_MB")) {
+			const unsigned long long mb = std::strtoull(env, nullptr, 10);
+			if (mb > 0) budget_ = static_cast<size_t>(mb) << 20;
+		}
+	}
+	return budget_;
+}
+
 std::shared_ptr<uint8_t> PinnedPool::Acquire(size_t bytes) {
+	// size class: at least 64 KiB, rounded up to an eighth of the power of two at or below it
 	size_t cls = 64 * 1024;
-	while (cls < bytes) cls <<= 1;
+	if (bytes > cls) {
+		size_t top = 1;
+		while ((top << 1) <= bytes) top <<= 1;
+		const size_t step = std::max<size_t>(top / 8, 1);
+		cls = (bytes + step - 1) / step * step;
+	}
 	void *p = nullptr;
+	size_t got = cls;
 	{
 		std::lock_guard<std::mutex> lock(mu_);
-		auto it = free_.find(cls);
-		if (it != free_.end()) {
+		auto it = free_.lower_bound(cls);  // the smallest cached buffer that holds the request ...
+		if (it != free_.end() && it->first <= 2 * cls) {  // ... unless it is over twice the size
 			p = it->second;
+			got = it->first;
+			cached_ -= got;
 			free_.erase(it);
-			cached_ -= cls;
 		}
 	}
 	if (!p) VGPU_CUDA(cudaMallocHost(&p, cls));
-	return std::shared_ptr<uint8_t>(static_cast<uint8_t *>(p), [this, cls](uint8_t *q) { Return(q, cls); });
+	return std::shared_ptr<uint8_t>(static_cast<uint8_t *>(p), [this, got](uint8_t *q) { Return(q, got); });
 }
 
 void PinnedPool::Return(void *p, size_t cls) {
 	{
 		std::lock_guard<std::mutex> lock(mu_);
-		if (cached_ + cls <= kMaxCached) {
+		if (cached_ + cls <= Budget()) {
 			free_.emplace(cls, p);
 			cached_ += cls;
 			return;

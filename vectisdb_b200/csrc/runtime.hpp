@@ -41,7 +41,11 @@ struct DeviceProps {
 //! Page-locked host buffers for results copied to the host, reused across calls (the role of the
 //! reference's PinnedBufferPool, src/pinned_buffer_pool.cpp:78-116): a device->host copy into pinned
 //! memory runs at link speed, and page-locking a fresh buffer per result would cost more than the copy.
-//! Buffers come back to the pool when the last owner lets go; at most kMaxCached bytes stay cached.
+//! Buffers come back to the pool when the last owner lets go and are handed out again to any request
+//! of at least half their size (sizes round up to eighths of a power of two), so results of varying
+//! sizes reuse page-locked memory instead of pinning more: pinning costs far more than the copy, and
+//! freeing page-locked memory synchronizes the device. At most the cache budget stays cached (16 GiB,
+//! VECTOR_GPU_PINNED_CACHE_MB to change it); beyond it a returned buffer is freed.
 class PinnedPool {
 public:
 	static PinnedPool &Get();
@@ -49,10 +53,11 @@ public:
 
 private:
 	void Return(void *p, size_t cls);
-	static constexpr size_t kMaxCached = 4ull << 30;
+	size_t Budget();
 	std::mutex mu_;
 	std::multimap<size_t, void *> free_;
 	size_t cached_ = 0;
+	size_t budget_ = 0;
 };
 
 class DeviceAllocator {

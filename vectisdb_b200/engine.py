@@ -725,11 +725,10 @@ class Server:
              "run_ms": info.run_ms, "estimated_bytes": info.estimated_bytes, "error": info.error.decode()}
         if not h.value:
             return None, d
-        columns = _read_result(h)
         if on_device:
-            return DeviceResult(h, columns), d
-        abi.lib().vgpu_result_free(h)
-        return GpuExecutionResult(True, "", abi.OK, columns), d
+            return DeviceResult(h, _read_result(h)), d
+        # host results: zero-copy views of the result's page-locked buffers, freed with the last view
+        return GpuExecutionResult(True, "", abi.OK, _read_result(h, _ResultOwner(h))), d
 
     def stats(self) -> dict:
         st = abi.vgpu_server_stats()
