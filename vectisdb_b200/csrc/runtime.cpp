@@ -104,7 +104,16 @@ void DeviceAllocator::EnsureBudgetLocked() {
 // once in stream order: requests then find a free range without remapping.
 void DeviceAllocator::GrowReserve(uint64_t in_use, cudaStream_t stream) {
 	constexpr uint64_t kStep = 1ull << 30;
-	const uint64_t want = std::min<uint64_t>(budget_, (2 * in_use + kStep - 1) / kStep * kStep);
+	ReserveLocked(std::min<uint64_t>(budget_, (2 * in_use + kStep - 1) / kStep * kStep), stream);
+}
+
+void DeviceAllocator::Reserve(uint64_t bytes, cudaStream_t stream) {
+	std::lock_guard<std::mutex> lock(mu_);
+	EnsureBudgetLocked();
+	ReserveLocked(std::min<uint64_t>(budget_, bytes), stream);
+}
+
+void DeviceAllocator::ReserveLocked(uint64_t want, cudaStream_t stream) {
 	if (want <= reserve_target_) return;
 	cudaMemPool_t pool;
 	int device = 0;

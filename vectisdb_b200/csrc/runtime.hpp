@@ -66,6 +66,10 @@ public:
 	void Free(void *ptr, cudaStream_t stream);
 	void SetBudget(uint64_t bytes);
 	uint64_t Budget();
+	//! Maps `bytes` (within the budget) into the stream-ordered pool ahead of use, so requests that
+	//! come later find free ranges without the pool remapping pages (a server about to run many
+	//! requests at once reserves what they will hold together).
+	void Reserve(uint64_t bytes, cudaStream_t stream);
 	bool HasHeadroom(uint64_t bytes);
 	vgpu_memory_stats Stats();
 	//! Restarts the peak at the bytes in use now (the pool's reserve is unaffected).
@@ -74,6 +78,7 @@ public:
 private:
 	void EnsureBudgetLocked();
 	void GrowReserve(uint64_t in_use, cudaStream_t stream);
+	void ReserveLocked(uint64_t want, cudaStream_t stream);
 	std::mutex mu_;
 	bool budget_set_ = false;
 	uint64_t budget_ = 0;

@@ -41,6 +41,13 @@ Server::Server(const ServerOptions &options) : options_(options) {
 	const uint64_t default_budget = 120ull << 30;
 	budget_ = options_.memory_budget ? options_.memory_budget : std::min(default_budget, allocator_budget);
 	stats_.budget_bytes = budget_;
+	// Concurrent requests hold more device memory together than one at a time, and a pool that has to
+	// grow or remap pages while they run stalls every slot's allocations: map half the admission
+	// budget up front (what admitted requests hold at once stays under the budget).
+	if (options_.slots > 1) {
+		rt.allocator().Reserve(budget_ / 2, rt.default_stream());
+		VGPU_CUDA(cudaStreamSynchronize(rt.default_stream()));
+	}
 	for (int s = 0; s < options_.slots; s++) workers_.emplace_back([this, s] { WorkerLoop(s); });
 }
 
