@@ -682,7 +682,7 @@ def measure_c4(args, world: int, rank: int, local: int, rates, n_req: int, sampl
     Every request's result in the served run is checked against its result in the serial run."""
     import threading
     import torch
-    from vectisdb_b200 import ColumnCache, ExecuteOptions, GpuTableRef, Server
+    from vectisdb_b200 import ColumnCache, ExecuteOptions, GpuTableRef, Server, device_to_host
     from vectisdb_b200 import workloads as W
     from vectisdb_b200.engine import launch_count
 
@@ -735,10 +735,12 @@ def measure_c4(args, world: int, rank: int, local: int, rates, n_req: int, sampl
                     time.sleep(0.0002)
                 res, info = srv.wait(ids[i])
                 done[i] = info
-                if res is not None and hasattr(res, "free"):
+                if res is not None:
                     if keep:
-                        results[i] = [np.array(c.data, copy=True) for c in res.columns]
-                    res.free()
+                        results[i] = [device_to_host(c) if c.data is None else np.array(c.data, copy=True)
+                                      for c in res.columns]
+                    if hasattr(res, "free"):
+                        res.free()
 
         th = threading.Thread(target=collector)
         th.start()

@@ -112,15 +112,20 @@ def test_stream_pipeline_supports_projection_chains_only():
 
 
 def test_join_source_kernels_compile_single_and_multi_match():
-    """The join + group-by query's fused kernels, for a unique-key right side and for repeated keys
-    (each probe row expands into its run of matches): materialization, key statistics and the
-    one-pass group-by all compile; right columns are never read at left row positions."""
+    """The join + group-by query's fused kernels, for a unique-key right side, for repeated keys (each
+    probe row expands into its run of matches) and for repeated keys whose right column sits inline in
+    the dense table (one slot per match): materialization, key statistics and the one-pass group-by all
+    compile; right columns are never read at left row positions."""
     wl = W.c2(probe_n=64, build_n=16, miss_lo=16, miss_span=16)
     src = generate_source(wl.plan, wl.inputs)
     tus = src.split("//@@VGPU_TU@@")
-    assert len(tus) == 5
-    assert "vgpu_join_find" in tus[0] and "vgpu_join_run" in tus[1] and "vgpu_join_run" in tus[4]
-    assert "for (u32 jx_ = 0; jx_ < jn_; ++jx_)" in tus[4]
+    # materialize: unique, run, inline-run; key statistics: run; group-by: unique, run, inline-run
+    assert len(tus) == 7
+    assert "vgpu_join_find" in tus[0] and "vgpu_join_run" in tus[1] and "vgpu_join_run" in tus[5]
+    assert "vgpu_join_minline(" in tus[3] and "vgpu_join_minline(" in tus[6]
+    assert "vgpu_join_minline_value(je[r], jx_" in tus[6]
+    assert "for (u32 jx_ = 0; jx_ < jn_; ++jx_)" in tus[5] and "for (u32 jx_ = 0; jx_ < jn_; ++jx_)" in tus[6]
     # the right column g (source 0) is loaded only through the lookup, never by load_rows at row0
-    assert "load_rows<int, 8>((const int*)a.w[2]" not in tus[3] and "load_rows<int, 8>((const int*)a.w[2]" not in tus[4]
+    for t in tus[4:]:
+        assert "load_rows<int, 8>((const int*)a.w[2]" not in t
     assert all(s > 1000 for s in _compile_all(src))

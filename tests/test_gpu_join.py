@@ -230,16 +230,48 @@ def _launched(fn):
 
 def test_repeated_build_keys_fuse_into_the_group_by():
     """The join + group-by with every build key repeated (the c2 shape with two build rows per key):
-    each probe row expands into its run of matches inside the group-by kernel -- no match pairs are
-    materialized -- and the result equals the oracle's hash join."""
+    each probe row expands into its matches inside the group-by kernel -- no match pairs are
+    materialized -- read from the dense multi-match table (two 12-bit slots per 4-byte entry, filled
+    without sorting), and the result equals the oracle's hash join."""
     wl = W.c2dup(probe_n=1 << 22, build_n=1 << 20)
     pkey, x, bkey, g = [c.data for c in wl.inputs]
     (gg, gs), names = _launched(lambda: [c.data for c in _run(wl.plan, wl.inputs)])
-    assert "max_run_length" in names and "join_runs" not in names and "join_expand" not in names, names
+    assert "join_dense_multi" in names and "radix_scatter" not in names, names
+    assert "join_runs" not in names and "join_expand" not in names, names
     exp = O.c2(bkey, g, pkey, x)
     order = np.argsort(gg)
     assert np.array_equal(gg[order], exp["g"])
     assert _close(gs[order], exp["sum"])
+
+
+@pytest.mark.parametrize("repeat,card,path", [
+    (2, 1 << 20, "wide"),     # 20-bit values: one 4-byte entry holds one slot, an 8-byte one three
+    (5, 4096, "wide"),        # five 12-bit slots need the 8-byte entry
+    (6, 4096, "sorted"),      # more matches than an entry holds: the sorted runs
+    (3, 2, "narrow"),         # 1-bit values, three slots in 4 bytes
+])
+def test_join_group_by_over_repeated_keys_every_table_form(repeat, card, path):
+    """A join + group-by whose right keys each repeat `repeat` times, with right values of `card`
+    distinct values: the dense multi-match table in 4- or 8-byte entries while the matches fit its
+    slots, the sorted runs when a key has more; exact HUGEINT sums and counts per group against a
+    Python hash join, misses and negative keys included."""
+    rng = np.random.default_rng(40 + repeat)
+    base = rng.permutation(np.arange(-20_000, 20_000, dtype=np.int64))[:30_000]
+    rk = np.repeat(base, repeat)[rng.permutation(30_000 * repeat)]
+    rg = rng.integers(0, card, len(rk)).astype(np.int32)
+    lk = rng.integers(-25_000, 25_000, 400_000).astype(np.int64)
+    lv = rng.integers(-(1 << 40), 1 << 40, len(lk)).astype(np.int64)
+    cols, names = _launched(lambda: _run(_join_group_plan(T.INT64), [
+        make_column("lk", T.INT64, lk), make_column("lv", T.INT64, lv),
+        make_column("rk", T.INT64, rk), make_column("rg", T.INT32, rg)]))
+    if path == "sorted":
+        assert "radix_scatter" in names and "join_expand" not in names, names
+    else:
+        assert "join_dense_multi" in names and "radix_scatter" not in names, names
+    from vectisdb_b200.engine import hugeint_to_int
+    sums, counts = _expected_join_group(lk, lv, rk, rg)
+    got = dict(zip(cols[0].data.tolist(), zip(hugeint_to_int(cols[1].data), cols[2].data.tolist())))
+    assert got == {k: (sums[k], counts[k]) for k in counts}
 
 
 @pytest.mark.parametrize("repeat", [2, 7])

@@ -399,6 +399,17 @@ std::string PipelineCodegen::LoadBlock(const Geometry &g, const std::vector<bool
 		// keys widen by zero extension of their width, as the sorted side was widened
 		const size_t kw = TypeSize(spec_.sources[key].type);
 		const char *ut = kw == 1 ? "u8" : kw == 2 ? "unsigned short" : kw == 4 ? "u32" : "u64";
+		if (spec_.join_minline) {
+			// the key's entry in the dense multi-match inline table: match count and one value slot per match
+			o << "\t\tlong long jm[" << g.items << "];\n\t\tu32 jc[" << g.items << "];\n\t\tu64 je[" << g.items << "];\n"
+			  << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) {\n"
+			  << "\t\t\tu32 c_ = 0u;\n"
+			  << "\t\t\tje[r] = row0 + r < n ? vgpu_join_minline((u64)(" << ut << ")s" << key << "[r] - a.w[" << kJoinWord + 2
+			  << "], (const void*)a.w[" << kJoinWord << "], a.w[" << kJoinWord + 3 << "] >> 8, (u32)(a.w[" << kJoinWord + 3
+			  << "] & 0xffu), &c_) : 0ull;\n"
+			  << "\t\t\tjc[r] = c_;\n\t\t\tjm[r] = c_ ? 0ll : -1ll;\n\t\t}\n";
+			return o.str();
+		}
 		if (spec_.join_multi) {
 			// the run of equal keys: start and length (0 = no match); the right columns are read per match
 			o << "\t\tlong long jm[" << g.items << "];\n\t\tu32 jc[" << g.items << "];\n"
@@ -446,11 +457,16 @@ std::string PipelineCodegen::ItemOpen(const Geometry &g, const std::vector<bool>
 	// one item per match of the row's key, right columns read at the match's sorted position
 	o << "\t\tconst u32 jn_ = (row < n && jm[r] >= 0) ? jc[r] : 0u;\n"
 	  << "\t\tfor (u32 jx_ = 0; jx_ < jn_; ++jx_) {\n"
-	  << "\t\tconst u64 jp_ = (u64)jm[r] + jx_;\n";
+	  << "\t\tconst u64 jp_ = (u64)jm[r] + jx_; (void)jp_;\n";
 	for (size_t i = 0; i < spec_.sources.size(); i++) {
 		const auto &src = spec_.sources[i];
 		if (!needed[i] || src.side != 1) continue;
 		const char *t = CudaTypeName(src.type);
+		if (spec_.join_minline) {  // the (single) right column from the match's slot of the entry
+			o << "\t\ts" << i << "[r] = from_bits<" << t << ">((u64)vgpu_join_minline_value(je[r], jx_, (u32)(a.w["
+			  << kJoinWord + 3 << "] & 0xffu), (u32)a.w[" << kJoinWord + 1 << "]));\n";
+			continue;
+		}
 		const int w = 2 + 2 * static_cast<int>(i);
 		o << "\t\ts" << i << "[r] = ((const " << t << "*)a.w[" << w << "])[jp_];\n";
 		if (src.nullable) o << "\t\tsv" << i << "[r] = ((const u8*)a.w[" << w + 1 << "])[jp_] != 0;\n";
@@ -2152,7 +2168,7 @@ std::string SpecKey(const PipelineSpec &spec) {
 	for (auto &sc : spec.sources) {
 		o << sc.name << '/' << static_cast<int>(sc.type) << '/' << sc.nullable << '/' << sc.side << ';';
 	}
-	o << "|cross:" << spec.cross << "|join:" << spec.join << '/' << spec.join_key << '/' << spec.join_inline << '/' << spec.join_multi << "|chain:";
+	o << "|cross:" << spec.cross << "|join:" << spec.join << '/' << spec.join_key << '/' << spec.join_inline << '/' << spec.join_multi << '/' << spec.join_minline << "|chain:";
 	for (const PlanNode *n : spec.chain) {
 		o << static_cast<int>(n->op) << '{';
 		for (auto &e : n->expressions) {

@@ -37,6 +37,9 @@ struct PipelineSpec {
 	int join_key = -1;
 	// The lookup returns the (single, <= 4-byte) right column's value itself instead of a position.
 	bool join_inline = false;
+	// multi-match join whose right column sits inline in a dense table, one slot per match (join_multi set
+	// too): join words 0 = table, 1 = the column's smallest value bits, 3 = entries << 8 | spec byte
+	bool join_minline = false;
 	// Right keys repeat: the lookup returns the run of equal keys in the sorted right side (start and
 	// length), and every left row expands into one pipeline item per match, in sorted right order.
 	// Consumers that support it: materialization, key statistics, the one-pass group-by.

@@ -353,10 +353,14 @@ std::string GenerateSourceText(const PlanNode &plan, const std::vector<vgpu_colu
 		PipelineSpec multi = spec;
 		multi.join_multi = true;
 		PipelineCodegen cgm(multi);
+		PipelineSpec minline = multi;  // ... with the right column inline, one slot per match
+		minline.join_minline = true;
+		PipelineCodegen cgi(minline);
 		std::vector<int> outs;
 		for (size_t i = 0; i < cg.visible().size(); i++) outs.push_back(static_cast<int>(i));
 		std::string text = cg.EmitMaterialize(outs, g) + "\n//@@VGPU_TU@@\n" + cgm.EmitMaterialize(outs, g) +
-		                   "\n//@@VGPU_TU@@\n" + cgm.EmitStats(outs, g);
+		                   "\n//@@VGPU_TU@@\n" + cgm.EmitStats(outs, g) + "\n//@@VGPU_TU@@\n" +
+		                   cgi.EmitMaterialize(outs, g);
 		if (!gb) return text;
 		PipelineCodegen::GroupBySpec spec_gb;
 		int shift = 0;
@@ -385,7 +389,7 @@ std::string GenerateSourceText(const PlanNode &plan, const std::vector<vgpu_colu
 		gj.block = 512;
 		gj.items = 8;
 		return text + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_gb, false, gj) + "\n//@@VGPU_TU@@\n" +
-		       cgm.EmitGroupBy(spec_gb, false, gj);
+		       cgm.EmitGroupBy(spec_gb, false, gj) + "\n//@@VGPU_TU@@\n" + cgi.EmitGroupBy(spec_gb, false, gj);
 	}
 	if (!gb) {
 		std::vector<int> outs;

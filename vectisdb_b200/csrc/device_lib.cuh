@@ -418,6 +418,25 @@ __device__ __forceinline__ long long vgpu_join_run(u64 k, const u64 *__restrict_
 	return up > lo ? (long long)lo : -1ll;
 }
 
+// A probe key's entry in the dense multi-match inline table (the join words: table, vmin, entries and
+// the spec byte (wide << 7) | (vbits << 2) | (cbits - 1)): the entry, with *count = its match count (0
+// for a key outside the table or without matches). Match j's value bits are vmin plus the vbits-bit
+// slot at bit cbits + j * vbits.
+__device__ __forceinline__ u64 vgpu_join_minline(u64 k, const void *__restrict__ table, u64 entries, u32 spec,
+                                                 u32 *count) {
+	*count = 0u;
+	if (k >= entries) return 0ull;
+	const u32 cbits = (spec & 3u) + 1u;
+	const u64 e = (spec & 0x80u) ? ((const u64 *)table)[k] : (u64)((const u32 *)table)[k];
+	*count = (u32)(e & ((1ull << cbits) - 1ull));
+	return e;
+}
+
+__device__ __forceinline__ u32 vgpu_join_minline_value(u64 e, u32 j, u32 spec, u32 vmin) {
+	const u32 cbits = (spec & 3u) + 1u, vbits = (spec >> 2) & 31u;
+	return vmin + (u32)((e >> (cbits + j * vbits)) & ((1ull << vbits) - 1ull));
+}
+
 // ---------------------------------------------------------------------------------------------
 // Hashing of packed group keys
 

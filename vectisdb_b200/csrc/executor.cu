@@ -120,6 +120,7 @@ struct CachedJoinTable {
 	uint64_t words[4] = {0, 0, 0, 0};  // join words; [2] (the key bias) is `bias`
 	uint64_t bias = 0;
 	bool inline_value = false;
+	bool multi_inline = false;  // the multi-match inline table (one value slot per match)
 	bool cached = false;  // held by the cache (guarded by the cache's mutex)
 	//! Marks left by the executions that read the table: the free waits for all of them, wherever the
 	//! last reference is dropped (an eviction by another query, a cache clear, or the reader itself).
@@ -205,8 +206,11 @@ private:
 	};
 
 	Relation Scan(const PlanNode &node);
-	//! `multi_ok`: the consumer accepts a join source whose right keys repeat (join_multi).
-	PipelineInput BuildPipeline(const PlanNode &top, std::vector<const PlanNode *> chain_top_down, bool multi_ok = false);
+	//! `multi_ok`: the consumer accepts a join source whose right keys repeat (join_multi). `any_order`:
+	//! it also takes a row's matches in any order (an aggregation), so they may come from the dense
+	//! multi-match inline table, whose slots are filled in no particular order.
+	PipelineInput BuildPipeline(const PlanNode &top, std::vector<const PlanNode *> chain_top_down, bool multi_ok = false,
+	                            bool any_order = false);
 	//! A pipeline with no chain over the columns of a relation.
 	PipelineInput PipelineOver(const Relation &rel);
 	Relation Materialize(PipelineInput &pin, const std::vector<int> &out_cols, const std::vector<std::string> &names);
@@ -214,7 +218,7 @@ private:
 	Relation GroupBy(const PlanNode &node);
 	Relation Join(const PlanNode &node);
 	Relation JoinMaterialize(const PlanNode &node, Relation &left, Relation &right);
-	Relation JoinForPipeline(const PlanNode &node, PipelineInput &pin, bool *fused, bool multi_ok);
+	Relation JoinForPipeline(const PlanNode &node, PipelineInput &pin, bool *fused, bool multi_ok, bool any_order);
 	Relation GroupByPipeline(const PlanNode &node, PipelineInput &pin);
 	Relation CrossProduct(const PlanNode &node);
 	void ComputeStats(PipelineInput &pin, const PipelineCodegen &cg, const std::vector<int> &cols,
@@ -375,7 +379,8 @@ void Executor::FillArgs(const PipelineInput &pin, KArgsHost &args) {
 	}
 }
 
-Executor::PipelineInput Executor::BuildPipeline(const PlanNode &top, std::vector<const PlanNode *> chain, bool multi_ok) {
+Executor::PipelineInput Executor::BuildPipeline(const PlanNode &top, std::vector<const PlanNode *> chain, bool multi_ok,
+                                                bool any_order) {
 	// `top` is the first non-FILTER/PROJECTION node below the chain.
 	PipelineInput pin;
 	std::reverse(chain.begin(), chain.end()); // bottom-up
@@ -434,7 +439,7 @@ Executor::PipelineInput Executor::BuildPipeline(const PlanNode &top, std::vector
 	Relation rel;
 	if (top.op == OpType::HASH_JOIN) {
 		bool fused = false;
-		rel = JoinForPipeline(top, pin, &fused, multi_ok);
+		rel = JoinForPipeline(top, pin, &fused, multi_ok, any_order);
 		if (fused) return pin;
 	} else {
 		rel = top.op == OpType::SCAN ? Scan(top) : Exec(top);
@@ -718,7 +723,7 @@ Relation Executor::GroupBy(const PlanNode &node) {
 		chain.push_back(cur);
 		cur = cur->children[0].get();
 	}
-	PipelineInput pin = BuildPipeline(*cur, chain, true);
+	PipelineInput pin = BuildPipeline(*cur, chain, true, true);
 	return GroupByPipeline(node, pin);
 }
 
@@ -1338,7 +1343,8 @@ Relation Executor::Join(const PlanNode &node) {
 // match in the sorted right side (a radix directory over the sorted keys, then a short binary search;
 // right columns gathered into sorted order once), and rows without a match are filtered out. The
 // match pairs are never materialized. Otherwise the join output is materialized as usual.
-Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, bool *fused, bool multi_ok) {
+Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, bool *fused, bool multi_ok,
+                                   bool any_order) {
 	*fused = false;
 	if (node.children.size() != 2) {
 		Fail(VGPU_ERR_INVALID_ARGUMENT, "gpu_executor: HASH_JOIN expects exactly two children");
@@ -1426,23 +1432,26 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 	}
 	uint64_t bias = 0;
 	std::shared_ptr<CachedJoinTable> hit = cache_key.empty() ? nullptr : JoinTableCache::Get().Find(cache_key);
+	if (hit && hit->multi_inline && !(multi_ok && any_order)) hit = nullptr;  // built again in right-side order
 	if (hit) {
 		holds_.push_back(hit);
 		add_sources(false, nullptr);
 		pin.spec.join_inline = hit->inline_value;
+		pin.spec.join_multi = pin.spec.join_minline = hit->multi_inline;
 		pin.join_words[0] = hit->words[0];
 		pin.join_words[1] = hit->words[1];
 		pin.join_words[3] = hit->words[3];
 		bias = hit->bias;
 	} else {
 		// a dense table just built: handed from the execution's arena to the cache
-		auto keep = [&](void *table, uint64_t bytes, bool inline_value) {
+		auto keep = [&](void *table, uint64_t bytes, bool inline_value, bool multi_inline = false) {
 			if (cache_key.empty()) return;
 			arena_.Release(table);
 			auto t = std::make_shared<CachedJoinTable>();
 			t->table = table;
 			t->bytes = bytes;
 			t->inline_value = inline_value;
+			t->multi_inline = multi_inline;
 			t->bias = bias;
 			t->words[0] = pin.join_words[0];
 			t->words[1] = pin.join_words[1];
@@ -1511,6 +1520,36 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 					pin.join_words[3] = 0xffu | ((range + 1) << 8);
 					built = true;
 					keep(table, (range + 1) * 4, false);
+				}
+			}
+		}
+		// Repeated right keys with few matches each and one narrow right column: the dense table holds every
+		// match's value inline (a count, then one slot per match), still filled without sorting -- 4-byte
+		// entries when two matches fit, else 8-byte ones; a key with more matches than fit falls back to the
+		// sorted form.
+		const uint64_t mspan = static_cast<uint64_t>(vmax) - vmin;
+		if (!built && multi_ok && any_order && inline_col && range < (1ull << 28) && range < 4 * rn &&
+		    mspan < (1ull << 30)) {
+			const uint32_t vbits = std::max(1, BitsFor(mspan));
+			uint32_t *overflow = arena_.AllocT<uint32_t>(1);
+			for (int wide = 0; wide < 2 && !built; wide++) {
+				const uint32_t ebits = wide ? 64 : 32, cbits = wide ? 3 : 2;
+				const uint32_t rmax = std::min<uint32_t>((1u << cbits) - 1, (ebits - cbits) / vbits);
+				if (rmax < 2) continue;
+				const uint64_t bytes = (range + 1) * (wide ? 8 : 4);
+				void *table = arena_.Alloc(bytes);
+				kern::JoinDenseMulti(rw, inline_col->data, TypeSize(inline_col->type), rn, range, vmin, vbits, cbits, rmax,
+				                     table, wide != 0, overflow, stream_);
+				if (ReadU32(overflow) == 0) {
+					add_sources(false, nullptr);
+					pin.spec.join_multi = pin.spec.join_minline = true;
+					pin.join_words[0] = reinterpret_cast<uint64_t>(table);
+					pin.join_words[1] = vmin;
+					pin.join_words[3] = ((range + 1) << 8) | (wide ? 0x80u : 0u) | (vbits << 2) | (cbits - 1);
+					built = true;
+					keep(table, bytes, false, true);
+				} else {
+					arena_.FreeNow(table);
 				}
 			}
 		}

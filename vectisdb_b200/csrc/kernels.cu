@@ -712,6 +712,30 @@ void ValueBits(const void *values, size_t width, uint64_t n, uint32_t *bounds, c
 	VGPU_CUDA(cudaGetLastError());
 }
 
+// Multi-match inline table: entry[k] = the key's match count in the low `cbits` bits, then one
+// `vbits`-bit slot per match holding value bits - vmin (the matches of a key in no particular order).
+// A match reserves its slot by adding 1 to the count and then ORs its value into that slot; a key
+// with more than rmax matches (rmax < 2^cbits, so the count never wraps before it is seen) counts in
+// *overflow and the table is not valid.
+template <typename T, typename E>
+__global__ void JoinDenseMultiKernel(const uint64_t *keys, const T *values, uint64_t n, uint32_t vmin, uint32_t vbits,
+                                     uint32_t cbits, uint32_t rmax, E *table, uint32_t *overflow) {
+	const E cmask = (E(1) << cbits) - 1;
+	uint32_t local = 0;
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+		E *slot = table + keys[i];
+		const E old = atomicAdd(slot, E(1));
+		const uint32_t j = static_cast<uint32_t>(old & cmask);
+		if (j >= rmax) {
+			local++;
+			continue;
+		}
+		const E v = static_cast<E>(static_cast<uint32_t>(values[i]) - vmin);
+		atomicOr(slot, v << (cbits + j * vbits));
+	}
+	if (local) atomicAdd(overflow, local);
+}
+
 namespace {
 template <typename E>
 void LaunchDenseCompact(const uint64_t *keys, const void *values, size_t vwidth, uint64_t n, uint32_t vmin, E *table,
@@ -746,6 +770,44 @@ void JoinDenseCompact(const uint64_t *keys, const void *values, size_t vwidth, u
 	case 2: LaunchDenseCompact(keys, values, vwidth, n, vmin, static_cast<uint16_t *>(table), dups, stream); break;
 	case 4: LaunchDenseCompact(keys, values, vwidth, n, vmin, static_cast<uint32_t *>(table), dups, stream); break;
 	default: Fail(VGPU_ERR_INTERNAL, "compact join table: width must be 1, 2 or 4 bytes");
+	}
+	VGPU_CUDA(cudaGetLastError());
+}
+
+void JoinDenseMulti(const uint64_t *keys, const void *values, size_t vwidth, uint64_t n, uint64_t range, uint32_t vmin,
+                    uint32_t vbits, uint32_t cbits, uint32_t rmax, void *table, bool wide, uint32_t *overflow,
+                    cudaStream_t stream) {
+	const size_t ew = wide ? 8 : 4;
+	if (cbits < 1 || cbits > 3 || rmax >= (1u << cbits) || cbits + rmax * vbits > ew * 8) {
+		Fail(VGPU_ERR_INTERNAL, "multi-match join table: slots do not fit the entry");
+	}
+	LaunchScope scope("join_dense_multi", stream, n * (8 + vwidth) + (range + 1) * ew, n);
+	VGPU_CUDA(cudaMemsetAsync(table, 0, (range + 1) * ew, stream));
+	VGPU_CUDA(cudaMemsetAsync(overflow, 0, 4, stream));
+	const unsigned grid = GridFor(n, 256);
+	auto launch = [&](auto *tab) {
+		using E = std::remove_pointer_t<decltype(tab)>;
+		switch (vwidth) {
+		case 1:
+			JoinDenseMultiKernel<uint8_t, E><<<grid, 256, 0, stream>>>(keys, static_cast<const uint8_t *>(values), n, vmin,
+			                                                           vbits, cbits, rmax, tab, overflow);
+			break;
+		case 2:
+			JoinDenseMultiKernel<uint16_t, E><<<grid, 256, 0, stream>>>(keys, static_cast<const uint16_t *>(values), n,
+			                                                            vmin, vbits, cbits, rmax, tab, overflow);
+			break;
+		case 4:
+			JoinDenseMultiKernel<uint32_t, E><<<grid, 256, 0, stream>>>(keys, static_cast<const uint32_t *>(values), n,
+			                                                            vmin, vbits, cbits, rmax, tab, overflow);
+			break;
+		default:
+			Fail(VGPU_ERR_INTERNAL, "multi-match join table: value width must be 1, 2 or 4 bytes");
+		}
+	};
+	if (wide) {
+		launch(static_cast<unsigned long long *>(table));
+	} else {
+		launch(static_cast<unsigned int *>(table));
 	}
 	VGPU_CUDA(cudaGetLastError());
 }

@@ -72,6 +72,14 @@ void ValueBits(const void *values, size_t width, uint64_t n, uint32_t *bounds, c
 //! key (every value's offset must stay below that marker). *dups = keys met more than once.
 void JoinDenseCompact(const uint64_t *keys, const void *values, size_t vwidth, uint64_t n, uint64_t range,
                       uint32_t vmin, void *table, size_t width, uint32_t *dups, cudaStream_t stream);
+//! Dense multi-match table over (biased) keys <= range, built without sorting, for a join that contributes
+//! one right column of at most 4 bytes: entry[k] (4 bytes, or 8 when `wide`) holds k's match count in its
+//! low `cbits` bits (1..3) and one `vbits`-bit slot per match above them, each the value bits - vmin. A key
+//! with more than `rmax` matches (rmax < 2^cbits, cbits + rmax * vbits within the entry) counts in
+//! *overflow, and the table is then not valid.
+void JoinDenseMulti(const uint64_t *keys, const void *values, size_t vwidth, uint64_t n, uint64_t range, uint32_t vmin,
+                    uint32_t vbits, uint32_t cbits, uint32_t rmax, void *table, bool wide, uint32_t *overflow,
+                    cudaStream_t stream);
 //! *out = number of positions i > 0 with sorted[i] == sorted[i - 1].
 void CountAdjacentEqual(const uint64_t *sorted, uint64_t n, uint32_t *out, cudaStream_t stream);
 //! *out = the length of the longest run of equal keys in `sorted` (saturating at 2^32 - 1).
