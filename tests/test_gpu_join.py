@@ -254,12 +254,13 @@ def test_join_group_by_over_repeated_keys_every_table_form(repeat, card, path):
     """A join + group-by whose right keys each repeat `repeat` times, with right values of `card`
     distinct values: the dense multi-match table in 4- or 8-byte entries while the matches fit its
     slots, the sorted runs when a key has more; exact HUGEINT sums and counts per group against a
-    Python hash join, misses and negative keys included."""
+    Python hash join, misses and negative probe keys included (the dense forms index the right keys'
+    zero-extended range, so the right keys here are non-negative)."""
     rng = np.random.default_rng(40 + repeat)
-    base = rng.permutation(np.arange(-20_000, 20_000, dtype=np.int64))[:30_000]
+    base = rng.permutation(np.arange(0, 40_000, dtype=np.int64))[:30_000]
     rk = np.repeat(base, repeat)[rng.permutation(30_000 * repeat)]
     rg = rng.integers(0, card, len(rk)).astype(np.int32)
-    lk = rng.integers(-25_000, 25_000, 400_000).astype(np.int64)
+    lk = rng.integers(-5_000, 45_000, 400_000).astype(np.int64)
     lv = rng.integers(-(1 << 40), 1 << 40, len(lk)).astype(np.int64)
     cols, names = _launched(lambda: _run(_join_group_plan(T.INT64), [
         make_column("lk", T.INT64, lk), make_column("lv", T.INT64, lv),

@@ -1,7 +1,9 @@
 // server.cpp -- see server.hpp.
 #include "server.hpp"
 
+#include <algorithm>
 #include <chrono>
+#include <cstdlib>
 
 #include "batch.hpp"
 #include "column_cache.hpp"
@@ -83,7 +85,16 @@ uint64_t Server::Submit(std::shared_ptr<PlanNode> plan, std::vector<vgpu_column>
 	req->submitted = Clock::now();
 	req->est = Estimate(*req->plan, req->inputs, req->options);
 	req->info.estimated_bytes = req->est;
-	if (options_.batch_max > 1 && options.cache_chunk_index < 0) {
+	// Only small requests batch: the batch launch pays off by sharing one launch among queries that are
+	// each too small to fill the GPU; a large request's own kernels fill it at least as well and run
+	// beside the other slots' work (VGPU_SERVE_BATCH_ROWS: the largest input that still batches).
+	uint64_t rows = 0;
+	for (auto &c : req->inputs) rows = std::max<uint64_t>(rows, c.row_count);
+	static const uint64_t batch_rows = [] {
+		const char *env = std::getenv("VGPU_SERVE_BATCH_ROWS");
+		return env ? std::strtoull(env, nullptr, 10) : (1ull << 21);
+	}();
+	if (options_.batch_max > 1 && options.cache_chunk_index < 0 && rows <= batch_rows) {
 		auto pb = PrepareBatch({req->plan});
 		if (pb->plans[0].scan) req->tmpl = pb->plans[0].sig_base;
 	}
