@@ -827,9 +827,7 @@ int PipelineCodegen::HeavySlotBytes(const GroupBySpec &gb) {
 	for (auto &a : gb.aggs) {
 		if (a.column < 0 || a.kind == AggKind::COUNT || a.kind == AggKind::COUNT_STAR) continue;
 		const bool int_sum = (a.kind == AggKind::SUM || a.kind == AggKind::AVG) && !IsFloatType(a.input_type);
-		const size_t i = static_cast<size_t>(&a - gb.aggs.data());
-		const bool narrow = i < 32 && ((gb.narrow_sums >> i) & 1u);
-		bytes += int_sum && !narrow ? 16 : 8;
+		bytes += int_sum ? 16 : 8;
 	}
 	return bytes;
 }
@@ -1167,11 +1165,6 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			} else if (IsFloatType(ag.input_type)) {
 				hkind[i] = "f64";
 				harr.push_back({"HF" + is, "double", 8});
-			} else if (i < 32 && ((gb.narrow_sums >> i) & 1u)) {
-				// a sum that provably fits 63 bits: one 64-bit word, native 64-bit atomic adds, no
-				// overflow check at the flush
-				hkind[i] = "int64";
-				harr.push_back({"HL" + is, "unsigned long long", 8});
 			} else {
 				hkind[i] = "int";
 			}
@@ -1264,9 +1257,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			if (hkind[i].empty()) continue;
 			const std::string is = std::to_string(i);
 			const std::string v = visible_[gb.aggs[i].column].value;
-			if (hkind[i] == "int64") {
-				hupd << "\t\t\t\tatomicAdd(&HL" << is << "[h], (unsigned long long)(i64)(" << v << "));\n";
-			} else if (hkind[i] == "int") {
+			if (hkind[i] == "int") {
 				hupd << "\t\t\t\t{ const i64 x_ = (i64)(" << v << "); atomic_add_i128_u32x4(&HW" << is << "_0[h], &HW" << is
 				     << "_1[h], &HW" << is << "_2[h], &HW" << is << "_3[h], (u64)x_, x_ < 0 ? -1 : 0); }\n";
 			} else if (hkind[i] == "f64") {
@@ -1286,9 +1277,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			if (hkind[i].empty()) continue;
 			const std::string is = std::to_string(i);
 			const std::string v = visible_[gb.aggs[i].column].value;
-			if (hkind[i] == "int64") {
-				hgrp << "\t\t\tu64 glo" << is << " = (u64)(i64)(" << v << ");\n";
-			} else if (hkind[i] == "int") {
+			if (hkind[i] == "int") {
 				hgrp << "\t\t\tu64 glo" << is << " = (u64)(i64)(" << v << "); i64 ghi" << is << " = ((i64)(" << v
 				     << ") < 0) ? -1 : 0;\n";
 			} else if (hkind[i] == "f64") {
@@ -1304,9 +1293,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		for (size_t i = 0; i < gb.aggs.size(); i++) {
 			if (hkind[i].empty()) continue;
 			const std::string is = std::to_string(i);
-			if (hkind[i] == "int64") {
-				hgrp << "\t\t\t\t{ const u64 ol_ = __shfl_sync(hpeers_, glo" << is << ", src_); if (me_) glo" << is << " += ol_; }\n";
-			} else if (hkind[i] == "int") {
+			if (hkind[i] == "int") {
 				hgrp << "\t\t\t\t{ const u64 ol_ = __shfl_sync(hpeers_, glo" << is << ", src_); const i64 oh_ = __shfl_sync(hpeers_, ghi"
 				     << is << ", src_);\n\t\t\t\t  if (me_) { const u64 nl_ = glo" << is << " + ol_; ghi" << is
 				     << " += oh_ + (nl_ < glo" << is << " ? 1 : 0); glo" << is << " = nl_; } }\n";
@@ -1322,9 +1309,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		for (size_t i = 0; i < gb.aggs.size(); i++) {
 			if (hkind[i].empty()) continue;
 			const std::string is = std::to_string(i);
-			if (hkind[i] == "int64") {
-				hgrp << "\t\t\t\tatomicAdd(&HL" << is << "[h], (unsigned long long)glo" << is << ");\n";
-			} else if (hkind[i] == "int") {
+			if (hkind[i] == "int") {
 				hgrp << "\t\t\t\tatomic_add_i128_u32x4(&HW" << is << "_0[h], &HW" << is << "_1[h], &HW" << is << "_2[h], &HW" << is
 				     << "_3[h], glo" << is << ", ghi" << is << ");\n";
 			} else if (hkind[i] == "f64") {
@@ -1347,9 +1332,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			const std::string is = std::to_string(ai);
 			const int wi = sl.offset / 4;
 			std::string bits;
-			if (hkind[ai] == "int64") {
-				bits = "(u64)HL" + is + "[h]";
-			} else if (hkind[ai] == "int") {
+			if (hkind[ai] == "int") {
 				bits = "((u64)HW" + is + "_0[h] | ((u64)HW" + is + "_1[h] << 32))";
 				// the partial travels as a 64-bit value: a sum outside that range flags the launch,
 				// whose caller then runs the query without pre-aggregation

@@ -437,8 +437,6 @@ std::string GenerateSourceText(const PlanNode &plan, const std::vector<vgpu_colu
 	PipelineCodegen::GroupBySpec spec_plain = spec_dp;
 	spec_plain.bucket_plain = true;
 	spec_plain.narrow_sums = ~0u;  // ... with integer sums in one 64-bit word
-	PipelineCodegen::GroupBySpec spec_hvn = spec_hv;  // heavy keys with 64-bit partial sums (staged TU)
-	spec_hvn.narrow_sums = ~0u;
 	spec_hv.f64_l2 = PipelineCodegen::F64Fields(spec_hv) > 0;  // FP64 sums of its bucket pass in L2
 	PipelineCodegen::GroupBySpec spec_nc = spec_gb;
 	spec_nc.narrow_count = true;  // one-pass tables whose counts take no carries
@@ -454,7 +452,7 @@ std::string GenerateSourceText(const PlanNode &plan, const std::vector<vgpu_colu
 	       "\n//@@VGPU_TU@@\n" + cg.EmitStats(key_columns, gs) + "\n//@@VGPU_TU@@\n" +
 	       cg.EmitGroupBy(spec_dp, true, g) + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_hv, true, g) +
 	       "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_dp, true, gst) + "\n//@@VGPU_TU@@\n" +
-	       cg.EmitGroupBy(spec_hvn, true, gst) + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_plain, true, g) +
+	       cg.EmitGroupBy(spec_hv, true, gst) + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_plain, true, g) +
 	       "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_nc, false, g);
 }
 
