@@ -75,22 +75,19 @@ def test_c1_heavy_keys_chosen_on_skewed_input():
     _check_c1(wl, r.columns)
 
 
-def _generic_plan(table=None):
+def _generic_plan():
     return make_group_by(["k"], [
         make_aggregate(A.SUM, "v", T.HUGEINT), make_aggregate(A.MIN, "w", T.INT64),
         make_aggregate(A.MAX, "u", T.INT64), make_aggregate(A.SUM, "x", T.FLOAT64),
         make_aggregate(A.AVG, "y", T.FLOAT64), make_aggregate(A.COUNT, "z", T.INT64),
-        make_aggregate(A.COUNT_STAR, "", T.INT64)], make_scan(["k", "v", "w", "u", "x", "y", "z"], table))
+        make_aggregate(A.COUNT_STAR, "", T.INT64)], make_scan(["k", "v", "w", "u", "x", "y", "z"]))
 
 
-@pytest.mark.parametrize("resident", [False, True])
 @pytest.mark.parametrize("big", [False, True])
-def test_heavy_partials_of_every_aggregate_kind(big, resident, monkeypatch):
+def test_heavy_partials_of_every_aggregate_kind(big, monkeypatch):
     """SUM/MIN/MAX/AVG over BIGINT, SUM over DOUBLE, COUNT(col), COUNT(*) with one very heavy key and
     negative values. With values near 2^62 a CTA's partial sum leaves 64 bits: the launch is flagged
-    and the query reruns without pre-aggregation, exact all the same. With the columns resident in the
-    column cache their ranges are known, and integer sums that provably fit 63 bits (|v| < 2^40 and
-    |y| < 1000 over 300 000 rows) accumulate in one 64-bit word in the bucket pass -- exact too."""
+    and the query reruns without pre-aggregation, exact all the same."""
     monkeypatch.setenv("VGPU_GB_STRATEGY", "direct")
     monkeypatch.setenv("VGPU_GB_DIRECT_BITS", "6")
     monkeypatch.setenv("VGPU_GB_HEAVY", "2")
@@ -111,17 +108,7 @@ def test_heavy_partials_of_every_aggregate_kind(big, resident, monkeypatch):
     cols = [make_column("k", T.INT32, k), make_column("v", T.INT64, v), make_column("w", T.INT64, w),
             make_column("u", T.INT64, u), make_column("x", T.FLOAT64, x), make_column("y", T.INT64, y),
             make_column("z", T.INT64, z)]
-    if resident:
-        from vectisdb_b200 import ColumnCache, ExecuteOptions, GpuTableRef
-        ref = GpuTableRef("memory", "main", f"heavy_generic_{int(big)}")
-        ColumnCache.put_table(ref, cols)
-        try:
-            r, names = _launched(lambda: GpuEngine.instance().execute_plan(
-                _generic_plan(ref), [], ExecuteOptions(serve_whole_scan_from_cache=True)))
-        finally:
-            ColumnCache.invalidate_table(ref)
-    else:
-        r, names = _launched(lambda: GpuEngine.instance().execute_plan(_generic_plan(), cols))
+    r, names = _launched(lambda: GpuEngine.instance().execute_plan(_generic_plan(), cols))
     assert r.success, r.error_message
     assert "vgpu_gb_sample" in names
     if big:

@@ -811,7 +811,7 @@ int PipelineCodegen::DirectSlotBytes(const GroupBySpec &gb) {
 	for (auto &f : StateFields(gb)) {
 		if (f.kind == "cnt") bytes += 4;
 		if ((f.kind == "f64" && !gb.f64_l2) || f.kind == "min" || f.kind == "max") bytes += 8;
-		if (f.kind == "lo") bytes += (f.agg < 32 && ((gb.narrow_sums >> f.agg) & 1u)) ? 8 : 16;
+		if (f.kind == "lo") bytes += 16;
 	}
 	return bytes;
 }
@@ -1557,17 +1557,15 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			int bytes;
 		};
 		std::vector<DArr> arrs;
-		auto narrow = [&](const Field &fd) { return fd.kind == "lo" && fd.agg < 32 && ((gb.narrow_sums >> fd.agg) & 1u); };
 		for (int f = 0; f < F; f++) {
 			const auto &fd = fields[f];
 			if (fd.kind == "f64" && !gb.f64_l2) arrs.push_back({"DF" + std::to_string(f), "double", 8});
 			if (fd.kind == "min" || fd.kind == "max") arrs.push_back({"DM" + std::to_string(f), "i64", 8});
-			if (narrow(fd)) arrs.push_back({"DL" + std::to_string(f), "unsigned long long", 8});
 		}
 		for (int f = 0; f < F; f++) {
 			const auto &fd = fields[f];
 			if (fd.kind == "cnt") arrs.push_back({"DC", "u32", 4});
-			if (fd.kind == "lo" && !narrow(fd)) {
+			if (fd.kind == "lo") {
 				for (int w = 0; w < 4; w++) arrs.push_back({"DW" + std::to_string(f) + "_" + std::to_string(w), "u32", 4});
 			}
 		}
@@ -1603,9 +1601,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 				if (fd.kind == "min" || fd.kind == "max") {
 					r << "\t\t\tDM" << f << "[" << sv << "] = (i64)" << InitValue(fd) << ";\n";
 				}
-				if (narrow(fd)) {
-					r << "\t\t\tDL" << f << "[" << sv << "] = 0ull;\n";
-				} else if (fd.kind == "lo") {
+				if (fd.kind == "lo") {
 					for (int w = 0; w < 4; w++) r << "\t\t\tDW" << f << "_" << w << "[" << sv << "] = 0u;\n";
 				}
 			}
@@ -1619,10 +1615,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 				if (fd.kind == "cnt") r << "\t\t\tS" << f << "[0] = (u64)DC[" << sv << "];\n";
 				if (fd.kind == "f64") r << "\t\t\tS" << f << "[0] = (u64)__double_as_longlong(" << f64_load(f, sv) << ");\n";
 				if (fd.kind == "min" || fd.kind == "max") r << "\t\t\tS" << f << "[0] = (u64)DM" << f << "[" << sv << "];\n";
-				if (narrow(fd)) {  // the 64-bit two's-complement total, sign-extended to 128 bits
-					r << "\t\t\tS" << f << "[0] = DL" << f << "[" << sv << "];\n"
-					  << "\t\t\tS" << f + 1 << "[0] = (u64)((i64)DL" << f << "[" << sv << "] >> 63);\n";
-				} else if (fd.kind == "lo") {
+				if (fd.kind == "lo") {
 					r << "\t\t\tS" << f << "[0] = (u64)DW" << f << "_0[" << sv << "] | ((u64)DW" << f << "_1[" << sv
 					  << "] << 32);\n"
 					  << "\t\t\tS" << f + 1 << "[0] = (u64)DW" << f << "_2[" << sv << "] | ((u64)DW" << f << "_3[" << sv
@@ -1642,9 +1635,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 				if (fd.kind == "min" || fd.kind == "max") {
 					r << "\t\t\t\tatomic_" << fd.kind << "_i64(&DM" << fs << "[" << sv << "], " << pre << "m" << fs << ");\n";
 				}
-				if (narrow(fd)) {  // every partial fits the word's 63 bits: added mod 2^64, exact
-					r << "\t\t\t\tatomicAdd(&DL" << fs << "[" << sv << "], (unsigned long long)" << pre << "lo" << fs << ");\n";
-				} else if (fd.kind == "lo") {
+				if (fd.kind == "lo") {
 					r << "\t\t\t\tatomic_add_i128_u32x4(&DW" << fs << "_0[" << sv << "], &DW" << fs << "_1[" << sv << "], &DW" << fs
 					  << "_2[" << sv << "], &DW" << fs << "_3[" << sv << "], " << pre << "lo" << fs << ", " << pre << "hi" << fs
 					  << ");\n";
@@ -2208,7 +2199,7 @@ std::string GroupByKey(const PipelineCodegen::GroupBySpec &gb, bool partitioned)
 		o << static_cast<int>(a.kind) << '/' << a.column << '/' << static_cast<int>(a.input_type) << '/'
 		  << static_cast<int>(a.output_type) << ';';
 	}
-	o << "|db:" << gb.direct_bits << "|bt:" << gb.bucket_threads << "|hv:" << gb.heavy_slots << "|f64l2:" << gb.f64_l2 << "|hw:" << gb.heavy_warp << "|bp:" << gb.bucket_plain << "|nc:" << gb.narrow_count << "|ns:" << gb.narrow_sums;
+	o << "|db:" << gb.direct_bits << "|bt:" << gb.bucket_threads << "|hv:" << gb.heavy_slots << "|f64l2:" << gb.f64_l2 << "|hw:" << gb.heavy_warp << "|bp:" << gb.bucket_plain << "|nc:" << gb.narrow_count;
 	return o.str();
 }
 

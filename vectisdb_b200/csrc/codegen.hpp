@@ -153,10 +153,6 @@ public:
 		// One-pass group-by: fewer than 2^32 items feed it (a multi-match join source counts its matches
 		// too), so shared counts add without carries.
 		bool narrow_count = false;
-		// Bit i: integer SUM/AVG aggregate i provably fits 63 bits (rows x the input's largest magnitude,
-		// from the input column's range): the direct-partitioned bucket pass keeps it in one 64-bit word
-		// added by native 64-bit shared atomics instead of four 32-bit words with carries.
-		uint32_t narrow_sums = 0;
 	};
 
 	//! Group-by kernels (see executor for the argument layout), all in one translation unit:

@@ -780,21 +780,6 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 		Fail(VGPU_ERR_UNSUPPORTED, "gpu_groupby: the group key ranges need " + std::to_string(shift) +
 		                               " bits packed, more than the 63 this path supports");
 	}
-	// Integer sums that provably fit 63 bits -- the rows times the largest magnitude of a pass-through
-	// input column's range (column statistics) -- accumulate in one 64-bit word in the bucket pass.
-	if (!pin.spec.join_multi) {
-		for (size_t i = 0; i < gb.aggs.size() && i < 32; i++) {
-			const auto &ag = gb.aggs[i];
-			if ((ag.kind != AggKind::SUM && ag.kind != AggKind::AVG) || ag.column < 0 || IsFloatType(ag.input_type)) continue;
-			const int src = cg.visible()[ag.column].source;
-			if (src < 0 || src >= static_cast<int>(pin.sources.size()) || !pin.sources[src].has_stats) continue;
-			const DevColumn &c = pin.sources[src];
-			if (c.min == INT64_MIN) continue;
-			const uint64_t mag = std::max<uint64_t>(static_cast<uint64_t>(c.min < 0 ? -c.min : c.min),
-			                                        static_cast<uint64_t>(c.max < 0 ? -c.max : c.max));
-			if (mag == 0 || n <= (1ull << 62) / mag) gb.narrow_sums |= 1u << i;
-		}
-	}
 	const auto &props = Runtime::Get().props();
 	const int F = PipelineCodegen::StateWords(gb);
 	const uint64_t domain = 1ull << shift;
