@@ -75,19 +75,21 @@ def test_c1_heavy_keys_chosen_on_skewed_input():
     _check_c1(wl, r.columns)
 
 
-def _generic_plan():
+def _generic_plan(table=None):
     return make_group_by(["k"], [
         make_aggregate(A.SUM, "v", T.HUGEINT), make_aggregate(A.MIN, "w", T.INT64),
         make_aggregate(A.MAX, "u", T.INT64), make_aggregate(A.SUM, "x", T.FLOAT64),
         make_aggregate(A.AVG, "y", T.FLOAT64), make_aggregate(A.COUNT, "z", T.INT64),
-        make_aggregate(A.COUNT_STAR, "", T.INT64)], make_scan(["k", "v", "w", "u", "x", "y", "z"]))
+        make_aggregate(A.COUNT_STAR, "", T.INT64)], make_scan(["k", "v", "w", "u", "x", "y", "z"], table))
 
 
+@pytest.mark.parametrize("resident", [False, True])
 @pytest.mark.parametrize("big", [False, True])
-def test_heavy_partials_of_every_aggregate_kind(big, monkeypatch):
+def test_heavy_partials_of_every_aggregate_kind(big, resident, monkeypatch):
     """SUM/MIN/MAX/AVG over BIGINT, SUM over DOUBLE, COUNT(col), COUNT(*) with one very heavy key and
     negative values. With values near 2^62 a CTA's partial sum leaves 64 bits: the launch is flagged
-    and the query reruns without pre-aggregation, exact all the same."""
+    and the query reruns without pre-aggregation, exact all the same. Also with the columns served from
+    the column cache (ranges known, no host copy)."""
     monkeypatch.setenv("VGPU_GB_STRATEGY", "direct")
     monkeypatch.setenv("VGPU_GB_DIRECT_BITS", "6")
     monkeypatch.setenv("VGPU_GB_HEAVY", "2")
@@ -108,7 +110,17 @@ def test_heavy_partials_of_every_aggregate_kind(big, monkeypatch):
     cols = [make_column("k", T.INT32, k), make_column("v", T.INT64, v), make_column("w", T.INT64, w),
             make_column("u", T.INT64, u), make_column("x", T.FLOAT64, x), make_column("y", T.INT64, y),
             make_column("z", T.INT64, z)]
-    r, names = _launched(lambda: GpuEngine.instance().execute_plan(_generic_plan(), cols))
+    if resident:
+        from vectisdb_b200 import ColumnCache, ExecuteOptions, GpuTableRef
+        ref = GpuTableRef("memory", "main", f"heavy_generic_{int(big)}")
+        ColumnCache.put_table(ref, cols)
+        try:
+            r, names = _launched(lambda: GpuEngine.instance().execute_plan(
+                _generic_plan(ref), [], ExecuteOptions(serve_whole_scan_from_cache=True)))
+        finally:
+            ColumnCache.invalidate_table(ref)
+    else:
+        r, names = _launched(lambda: GpuEngine.instance().execute_plan(_generic_plan(), cols))
     assert r.success, r.error_message
     assert "vgpu_gb_sample" in names
     if big:
