@@ -1583,8 +1583,8 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			const int nf = F64Fields(gb);
 			for (int f = 0; f < F; f++) {
 				if (fields[f].kind != "f64") continue;
-				decl << "\tdouble *DF" << f << " = (double*)a.w[" << SCR << "] + (((u64)blockIdx.x * 2u + vgpu_par) * " << nf
-				     << "u + " << fi << "u) * " << D << "ull;\n";
+				decl << "\tdouble *DF" << f << " = (double*)a.w[" << SCR << "] + ((u64)blockIdx.x * " << nf << "u + " << fi
+				     << "u) * " << D << "ull;\n";
 				fi++;
 			}
 		}
@@ -1710,13 +1710,9 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			}
 		}
 
-		// With FP64 sums in L2 a CTA alternates between two tables (vgpu_par): a table reset at the end of
-		// one item is next updated two items later, after the intervening item's fences, so the work loop
-		// needs no fence of its own between the resets and the next item's reductions.
-		o << "__device__ __forceinline__ void vgpu_dslot_reset(const KArgs &a, char *sm, u32 s, u32 vgpu_par) {\n"
-		  << "\t(void)a; (void)vgpu_par;\n" << decl.str() << reset_slot("s") << "}\n\n";
-		o << "__device__ __forceinline__ void vgpu_ditem(const KArgs &a, const uint4 it, char *sm, u32 vgpu_par) {\n"
-		  << "\t(void)vgpu_par;\n"
+		o << "__device__ __forceinline__ void vgpu_dslot_reset(const KArgs &a, char *sm, u32 s) {\n\t(void)a;\n" << decl.str() << reset_slot("s")
+		  << "}\n\n";
+		o << "__device__ __forceinline__ void vgpu_ditem(const KArgs &a, const uint4 it, char *sm) {\n"
 		  << "\t__shared__ u32 warp_live[32];\n\t__shared__ u64 out_base;\n\t__shared__ bool last_chunk;\n"
 		  << "\tconst u32 p = it.x, sidx = it.w;\n"
 		  << "\tconst u64 start = it.y, end = it.z;\n"
@@ -1819,22 +1815,17 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		o << "extern \"C\" __global__ void __launch_bounds__(" << gb.bucket_threads << ") vgpu_gb_dbucket(KArgs a) {\n"
 		  << "\textern __shared__ __align__(16) char vgpu_dsm[];\n"
 		  << "\t__shared__ u32 cur;\n"
-		  << "\tfor (u32 s = threadIdx.x; s < " << D << "u; s += blockDim.x) {\n"
-		  << "\t\tvgpu_dslot_reset(a, vgpu_dsm, s, 0u);\n"
-		  << (gb.f64_l2 ? "\t\tvgpu_dslot_reset(a, vgpu_dsm, s, 1u);\n" : "")
-		  << "\t}\n"
-		  << (gb.f64_l2 ? "\t__threadfence();  // the cleared tables are in place before any reduction\n" : "")
+		  << "\tfor (u32 s = threadIdx.x; s < " << D << "u; s += blockDim.x) vgpu_dslot_reset(a, vgpu_dsm, s);\n"
 		  << "\tconst u32 n_items = *(const u32*)a.w[" << cb + 1 << "];\n"
 		  << "\tconst uint4 *items = (const uint4*)a.w[" << cb << "];\n"
-		  << "\tu32 par = 0u;\n"
 		  << "\twhile (true) {\n"
 		  << "\t\tif (threadIdx.x == 0) cur = atomicAdd((u32*)a.w[" << cb + 5 << "], 1u);\n"
+		  << (gb.f64_l2 ? "\t\t__threadfence();  // resets of the global sums land before the next reductions\n" : "")
 		  << "\t\t__syncthreads();\n"
 		  << "\t\tconst u32 i = cur;\n"
 		  << "\t\t__syncthreads();\n"
 		  << "\t\tif (i >= n_items) break;\n"
-		  << "\t\tvgpu_ditem(a, items[i], vgpu_dsm, par);\n"
-		  << "\t\tpar ^= 1u;\n"
+		  << "\t\tvgpu_ditem(a, items[i], vgpu_dsm);\n"
 		  << "\t}\n}\n";
 		return o.str();
 	}

@@ -1297,10 +1297,9 @@ uint64_t Executor::DirectBuckets(Module &module, const PipelineCodegen::GroupByS
 	b.SetPtr(cb + 6, out_count);
 	b.SetPtr(cb + 7, control + 1);
 	for (int w = 0; w < out_words; w++) b.SetPtr(cb + 8 + w, out[w].data);
-	if (gb.f64_l2) {  // per-CTA FP64 sum tables, two per CTA used by alternate work items (the kernel
-		              // clears its own on entry and leaves them clear)
+	if (gb.f64_l2) {  // per-CTA FP64 sum tables (the kernel clears its own on entry and leaves them clear)
 		const uint64_t nf = static_cast<uint64_t>(PipelineCodegen::F64Fields(gb));
-		b.SetPtr(cb + 8 + out_words, arena_.Alloc(static_cast<uint64_t>(ctas) * 2 * nf * D * 8));
+		b.SetPtr(cb + 8 + out_words, arena_.Alloc(static_cast<uint64_t>(ctas) * nf * D * 8));
 	}
 	{
 		// initializes the tables of the splits the plan made (a count it reads on the device)
