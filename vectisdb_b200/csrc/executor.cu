@@ -1480,7 +1480,9 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 		// read; the value is stored as its offset from the smallest value in the fewest bytes that hold every
 		// offset (all ones marks a missing key), so the table of a small-valued column stays in L2. A key met
 		// twice (many-to-many) falls back to the sorted form below.
-		if (range < (1ull << 28) && range < 4 * rn) {
+		// More right rows than key values: some key repeats for sure, so no unique-key table is tried.
+		const bool surely_repeated = rn > range + 1;
+		if (range < (1ull << 28) && range < 4 * rn && !surely_repeated) {
 			const uint64_t span = static_cast<uint64_t>(vmax) - vmin;
 			const size_t width = !inline_col ? 0 : span < 0xffull ? 1 : span < 0xffffull ? 2 : span < 0xffffffffull ? 4 : 8;
 			const char *env_c = std::getenv("VGPU_JOIN_COMPACT");  // "0": 8-byte inline entries (testing)
