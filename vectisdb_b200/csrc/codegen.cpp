@@ -1221,7 +1221,9 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		  << LoadBlock(g, needed, true) << item_head << chain_code_ << "\t\tif (keep) {\n"
 		  << "\t\t\tconst u64 k = " << mixed << ";\n"
 		  << "\t\t\tu32 s = (u32)mix64(k) & (SC - 1);\n"
-		  << "\t\t\t#pragma unroll 1\n\t\t\tfor (int i = 0; i < 32; ++i) {\n"
+		  // a short probe: a key that finds no slot within 8 is a rare one in a table that filled up
+		  // (many distinct keys), which no heavy-key selection would pick
+		  << "\t\t\t#pragma unroll 1\n\t\t\tfor (int i = 0; i < 8; ++i) {\n"
 		  << "\t\t\t\tconst u64 prev = atomicCAS((unsigned long long*)&skeys[s], ~0ull, k);\n"
 		  << "\t\t\t\tif (prev == ~0ull || prev == k) { atomicAdd(&scount[s], 1u); break; }\n"
 		  << "\t\t\t\ts = (s + 1) & (SC - 1);\n\t\t\t}\n"
