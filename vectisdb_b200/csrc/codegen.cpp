@@ -810,7 +810,7 @@ int PipelineCodegen::DirectSlotBytes(const GroupBySpec &gb) {
 	int bytes = 0;
 	for (auto &f : StateFields(gb)) {
 		if (f.kind == "cnt") bytes += 4;
-		if ((f.kind == "f64" || f.kind == "min" || f.kind == "max") && !gb.f64_l2) bytes += 8;
+		if ((f.kind == "f64" && !gb.f64_l2) || f.kind == "min" || f.kind == "max") bytes += 8;
 		if (f.kind == "lo") bytes += 16;
 	}
 	return bytes;
@@ -819,12 +819,6 @@ int PipelineCodegen::DirectSlotBytes(const GroupBySpec &gb) {
 int PipelineCodegen::F64Fields(const GroupBySpec &gb) {
 	int n = 0;
 	for (auto &f : StateFields(gb)) n += f.kind == "f64" ? 1 : 0;
-	return n;
-}
-
-int PipelineCodegen::L2Fields(const GroupBySpec &gb) {
-	int n = 0;
-	for (auto &f : StateFields(gb)) n += (f.kind == "f64" || f.kind == "min" || f.kind == "max") ? 1 : 0;
 	return n;
 }
 
@@ -1568,7 +1562,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		for (int f = 0; f < F; f++) {
 			const auto &fd = fields[f];
 			if (fd.kind == "f64" && !gb.f64_l2) arrs.push_back({"DF" + std::to_string(f), "double", 8});
-			if ((fd.kind == "min" || fd.kind == "max") && !gb.f64_l2) arrs.push_back({"DM" + std::to_string(f), "i64", 8});
+			if (fd.kind == "min" || fd.kind == "max") arrs.push_back({"DM" + std::to_string(f), "i64", 8});
 		}
 		for (int f = 0; f < F; f++) {
 			const auto &fd = fields[f];
@@ -1583,27 +1577,22 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			decl << "\t" << ar.type << " *" << ar.name << " = (" << ar.type << "*)(sm + " << off << ");\n";
 			off += D * ar.bytes;
 		}
-		// FP64 sums and 64-bit MIN/MAX in the CTA's own tables of the global region (L2-resident: native
-		// reductions there, where the same operations on shared memory are compare-and-swap loops)
+		// FP64 sums in the CTA's own tables of the global region (L2-resident: reductions, no CAS loops)
 		const int OUTD_ = cb + 8;
 		const int SCR = OUTD_ + static_cast<int>(gb.keys.size() + gb.aggs.size());
 		if (gb.f64_l2) {
 			int fi = 0;
-			const int nf = L2Fields(gb);
+			const int nf = F64Fields(gb);
 			for (int f = 0; f < F; f++) {
-				const bool mm = fields[f].kind == "min" || fields[f].kind == "max";
-				if (fields[f].kind != "f64" && !mm) continue;
-				decl << "\t" << (mm ? "i64 *DM" : "double *DF") << f << " = (" << (mm ? "i64" : "double") << "*)a.w[" << SCR
-				     << "] + ((u64)blockIdx.x * " << nf << "u + " << fi << "u) * " << D << "ull;\n";
+				if (fields[f].kind != "f64") continue;
+				decl << "\tdouble *DF" << f << " = (double*)a.w[" << SCR << "] + ((u64)blockIdx.x * " << nf << "u + " << fi
+				     << "u) * " << D << "ull;\n";
 				fi++;
 			}
 		}
 		// a sum field's current value (the global tables are read past L1: reductions land in L2)
 		auto f64_load = [&](int f, const std::string &sv) {
 			return gb.f64_l2 ? "__ldcg(&DF" + std::to_string(f) + "[" + sv + "])" : "DF" + std::to_string(f) + "[" + sv + "]";
-		};
-		auto mm_load = [&](int f, const std::string &sv) {
-			return gb.f64_l2 ? "__ldcg(&DM" + std::to_string(f) + "[" + sv + "])" : "DM" + std::to_string(f) + "[" + sv + "]";
 		};
 		auto reset_slot = [&](const std::string &sv) {
 			std::ostringstream r;
@@ -1627,7 +1616,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 				const auto &fd = fields[f];
 				if (fd.kind == "cnt") r << "\t\t\tS" << f << "[0] = (u64)DC[" << sv << "];\n";
 				if (fd.kind == "f64") r << "\t\t\tS" << f << "[0] = (u64)__double_as_longlong(" << f64_load(f, sv) << ");\n";
-				if (fd.kind == "min" || fd.kind == "max") r << "\t\t\tS" << f << "[0] = (u64)" << mm_load(f, sv) << ";\n";
+				if (fd.kind == "min" || fd.kind == "max") r << "\t\t\tS" << f << "[0] = (u64)DM" << f << "[" << sv << "];\n";
 				if (fd.kind == "lo") {
 					r << "\t\t\tS" << f << "[0] = (u64)DW" << f << "_0[" << sv << "] | ((u64)DW" << f << "_1[" << sv
 					  << "] << 32);\n"

@@ -141,8 +141,8 @@ public:
 		int heavy_slots = 0;
 		// FP64 sums accumulate in a per-CTA table in global memory (it stays in L2) with fire-and-forget
 		// reductions, instead of shared-memory compare-and-swap loops. Direct-partitioned bucket pass:
-		// 64-bit MIN/MAX move there too (CTAs x L2Fields x slots words, set by each CTA on entry). One-pass
-		// group-by: FP64 sums only, argument word cb+2+F+outputs, CTAs x FP64 fields x D doubles.
+		// the region (CTAs x FP64 fields x slots doubles) is zero on entry and left zero. One-pass
+		// group-by: argument word cb+2+F+outputs, CTAs x FP64 fields x D doubles, set by each CTA.
 		bool f64_l2 = false;
 		// Heavy-key partition scatter: lanes of a warp step with the same heavy key combine their rows by
 		// shuffles and one lane updates the CTA's partial state (fewer, uncontended shared atomics).
@@ -179,8 +179,6 @@ public:
 	static int DirectSlotBytes(const GroupBySpec &gb);
 	//! FP64 sum fields of a group-by's state (the per-CTA region of f64_l2 holds one table each).
 	static int F64Fields(const GroupBySpec &gb);
-	//! State fields the direct-partitioned bucket pass keeps in L2 with f64_l2: FP64 sums, MIN, MAX.
-	static int L2Fields(const GroupBySpec &gb);
 	//! Shared-memory bytes of one heavy key's partial state in the heavy partition passes (row count,
 	//! partial state of every aggregate).
 	static int HeavySlotBytes(const GroupBySpec &gb);

@@ -914,7 +914,7 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 			gb.key_bits = shift;
 			// FP64 sums of the bucket pass in L2 through reductions (VGPU_GB_F64_L2=0: shared CAS loops)
 			const char *env_l2 = std::getenv("VGPU_GB_F64_L2");
-			gb.f64_l2 = PipelineCodegen::L2Fields(gb) > 0 && !(env_l2 && std::strcmp(env_l2, "0") == 0);
+			gb.f64_l2 = PipelineCodegen::F64Fields(gb) > 0 && !(env_l2 && std::strcmp(env_l2, "0") == 0);
 			// without heavy-key pre-aggregation the bucket pass groups equal slots per warp step (hot keys);
 			// VGPU_GB_BUCKET_PLAIN=1 makes every record update its slot itself
 			const char *env_plain = std::getenv("VGPU_GB_BUCKET_PLAIN");
@@ -1297,8 +1297,8 @@ uint64_t Executor::DirectBuckets(Module &module, const PipelineCodegen::GroupByS
 	b.SetPtr(cb + 6, out_count);
 	b.SetPtr(cb + 7, control + 1);
 	for (int w = 0; w < out_words; w++) b.SetPtr(cb + 8 + w, out[w].data);
-	if (gb.f64_l2) {  // per-CTA FP64 sum and MIN/MAX tables (the kernel sets its own on entry)
-		const uint64_t nf = static_cast<uint64_t>(PipelineCodegen::L2Fields(gb));
+	if (gb.f64_l2) {  // per-CTA FP64 sum tables (the kernel clears its own on entry and leaves them clear)
+		const uint64_t nf = static_cast<uint64_t>(PipelineCodegen::F64Fields(gb));
 		b.SetPtr(cb + 8 + out_words, arena_.Alloc(static_cast<uint64_t>(ctas) * nf * D * 8));
 	}
 	{
