@@ -38,7 +38,7 @@ sys.path.insert(0, str(ROOT))
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 CPU_BASELINE_LABEL = "C++ restatement of the query (OpenMP, oracle/oracle.cpp), not DuckDB: DuckDB is not installed"
 PLAIN_CONFIGS = ("c0", "c1", "c2", "c2b", "cp", "c2dup")
-PER_CONFIG_ORDER = ("c0", "cp", "c2", "c2dup", "c2b", "c3", "c4")
+PER_CONFIG_ORDER = ("c0", "cp", "c2", "c2dup", "c2b", "c3", "c4", "c1_sharded")
 
 
 def hbm_peak():
@@ -1038,7 +1038,9 @@ def main():
                 continue
             t0 = time.time()
             try:
-                if other == "c3":
+                if other == "c1_sharded":
+                    per[other] = measure_sharded(args, world, rank, local, 10, 3, False)
+                elif other == "c3":
                     per[other] = measure_c3(args, world, rank, local, 10, 3, 64 if cpu_reps else 0, False)
                 elif other == "c4":
                     per[other] = measure_c4(args, world, rank, local, [200.0, 1600.0, 25600.0], 160, False)
