@@ -822,28 +822,14 @@ int PipelineCodegen::F64Fields(const GroupBySpec &gb) {
 	return n;
 }
 
-int PipelineCodegen::HeavySlotBytes(const GroupBySpec &gb, bool f64_in_l2) {
+int PipelineCodegen::HeavySlotBytes(const GroupBySpec &gb) {
 	int bytes = 4;
 	for (auto &a : gb.aggs) {
 		if (a.column < 0 || a.kind == AggKind::COUNT || a.kind == AggKind::COUNT_STAR) continue;
 		const bool int_sum = (a.kind == AggKind::SUM || a.kind == AggKind::AVG) && !IsFloatType(a.input_type);
-		const bool f64_sum = (a.kind == AggKind::SUM || a.kind == AggKind::AVG) && IsFloatType(a.input_type);
-		if (f64_sum && f64_in_l2) continue;
 		bytes += int_sum ? 16 : 8;
 	}
 	return bytes;
-}
-
-bool PipelineCodegen::HeavyF64InL2(const GroupBySpec &gb, int consumer_base) {
-	return gb.f64_l2 && gb.heavy_slots > 0 && consumer_base + 15 < kKeyWord;
-}
-
-int PipelineCodegen::HeavyF64Fields(const GroupBySpec &gb) {
-	int n = 0;
-	for (auto &a : gb.aggs) {
-		if (a.column >= 0 && (a.kind == AggKind::SUM || a.kind == AggKind::AVG) && IsFloatType(a.input_type)) n++;
-	}
-	return n;
 }
 
 int PipelineCodegen::StageRowBytes(const GroupBySpec &gb, bool scatter) const {
@@ -1169,10 +1155,6 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		};
 		std::vector<HArr> harr;
 		std::vector<std::string> hkind(gb.aggs.size());
-		// FP64 partial sums of heavy keys in the CTA's own L2-resident table (argument cb+15) instead of
-		// shared memory, where an FP64 add is a compare-and-swap loop that the hottest keys contend on
-		const bool hl2 = HeavyF64InL2(gb, cb);
-		std::vector<int> hl2_aggs;
 		for (size_t i = 0; i < gb.aggs.size(); i++) {
 			const auto &ag = gb.aggs[i];
 			if (ag.column < 0 || ag.kind == AggKind::COUNT || ag.kind == AggKind::COUNT_STAR) continue;
@@ -1182,11 +1164,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 				harr.push_back({"HM" + is, "i64", 8});
 			} else if (IsFloatType(ag.input_type)) {
 				hkind[i] = "f64";
-				if (hl2) {
-					hl2_aggs.push_back(static_cast<int>(i));
-				} else {
-					harr.push_back({"HF" + is, "double", 8});
-				}
+				harr.push_back({"HF" + is, "double", 8});
 			} else {
 				hkind[i] = "int";
 			}
@@ -1209,10 +1187,6 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			hdecl << "\t" << ar.type << " *" << ar.name << " = (" << ar.type << "*)(vgpu_hstate + " << hbytes << ");\n";
 			hbytes += static_cast<uint64_t>(K) * ar.bytes;
 		}
-		for (size_t j = 0; j < hl2_aggs.size(); j++) {
-			hdecl << "\tdouble *HF" << hl2_aggs[j] << " = (double*)a.w[" << cb + 15 << "] + ((u64)blockIdx.x * "
-			      << hl2_aggs.size() << "u + " << j << "u) * " << K << "ull;\n";
-		}
 		auto heavy_load = [&](bool with_state) {
 			std::ostringstream r;
 			r << "\tfor (u32 p = threadIdx.x; p < P; p += blockDim.x) vgpu_hmap[p] = ((const u32*)a.w[" << cb + 5
@@ -1228,10 +1202,8 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 					}
 					r << "\t\t" << ar.name << "[h] = (" << ar.type << ")" << init << ";\n";
 				}
-				for (int ai : hl2_aggs) r << "\t\tHF" << ai << "[h] = 0.0;\n";
 			}
 			r << "\t}\n";
-			if (with_state && hl2) r << "\t__threadfence();  // the cleared L2 sums are in place before any reduction\n";
 			return r.str();
 		};
 		const std::string mixed = "vgpu_dmix(a, " + pack.str() + ")";
@@ -1369,7 +1341,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 				hflush << "\t\t\tif (HW" << is << "_2[h] != ((HW" << is << "_1[h] & 0x80000000u) ? 0xffffffffu : 0u) || HW"
 				       << is << "_3[h] != HW" << is << "_2[h]) atomicOr((u32*)a.w[" << cb + 10 << "], 1u);\n";
 			} else if (hkind[ai] == "f64") {
-				bits = hl2 ? "(u64)__double_as_longlong(__ldcg(&HF" + is + "[h]))" : "(u64)__double_as_longlong(HF" + is + "[h])";
+				bits = "(u64)__double_as_longlong(HF" + is + "[h])";
 			} else {
 				bits = "(u64)HM" + is + "[h]";
 			}
@@ -1431,9 +1403,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		}
 		o << "\t\t\tstore_record<" << RW << ">(rec_out + (u64)pos * " << RS << ", rw);\n"
 		  << "\t\t\t}\n\t\t}\n\t\t}\n\t}\n"
-		  << stage_epilogue()
-		  << (hl2 ? "\t__threadfence();  // this thread's reductions are performed before the sums are read\n" : "")
-		  << "\t__syncthreads();\n"
+		  << stage_epilogue() << "\t__syncthreads();\n"
 		  << "\tfor (u32 h = threadIdx.x; h < nheavy; h += blockDim.x) {\n"
 		  << "\t\tconst u32 k = vgpu_hkeys[h];\n"
 		  << "\t\tconst u32 pos = atomicAdd(&vgpu_cursor[k >> " << dbits << "], 1u);\n"

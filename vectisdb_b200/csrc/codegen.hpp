@@ -181,12 +181,7 @@ public:
 	static int F64Fields(const GroupBySpec &gb);
 	//! Shared-memory bytes of one heavy key's partial state in the heavy partition passes (row count,
 	//! partial state of every aggregate).
-	static int HeavySlotBytes(const GroupBySpec &gb, bool f64_in_l2 = false);
-	//! Heavy keys' FP64 partial sums of the direct-partitioned scatter live in an L2-resident per-CTA
-	//! table (argument consumer_base + 15: CTAs x HeavyF64Fields x heavy_slots doubles) instead of
-	//! shared memory: with f64_l2, heavy keys, and that argument word free.
-	static bool HeavyF64InL2(const GroupBySpec &gb, int consumer_base);
-	static int HeavyF64Fields(const GroupBySpec &gb);
+	static int HeavySlotBytes(const GroupBySpec &gb);
 	//! Bytes per row of one staged tile of the partition count (`scatter` false) or scatter pass: the
 	//! source columns that pass reads.
 	int StageRowBytes(const GroupBySpec &gb, bool scatter) const;

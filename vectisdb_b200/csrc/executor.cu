@@ -239,7 +239,6 @@ private:
 		uint32_t *count = nullptr;       // selected keys (<= max_keys)
 		uint32_t *overflow = nullptr;    // set when an integer partial sum leaves 64 bits (status word)
 		uint32_t max_keys = 0;
-		int f64_in_l2 = 0;               // FP64 partial sums per key kept in L2 instead of shared memory
 		uint64_t state_bytes = 0;        // per heavy key
 		size_t smem(uint64_t P) const {
 			const uint64_t hoff = ((P + 32) * 4 + 15) & ~uint64_t(15);
@@ -974,7 +973,7 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 			// pre-aggregation saves more than staging, so staging yields when both do not fit
 			HeavyPlan room;
 			room.max_keys = HeavyKeyCap();
-			room.state_bytes = static_cast<uint64_t>(PipelineCodegen::HeavySlotBytes(gb, gb.f64_l2 && cb + 15 < kKeyWord));
+			room.state_bytes = static_cast<uint64_t>(PipelineCodegen::HeavySlotBytes(gb));
 			if (room.smem(P) + 128 + stage2_scatter + 1024 > static_cast<uint64_t>(props.smem_optin)) {
 				staged = false;
 				stage2_count = stage2_scatter = 0;
@@ -1039,9 +1038,6 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 				a.SetPtr(cb + 10, heavy.overflow);
 				a.SetPtr(cb + 11, heavy.keys);
 				a.SetPtr(cb + 12, heavy.count);
-				if (heavy.f64_in_l2) {  // the CTAs' L2-resident FP64 partial sums (each CTA clears its own)
-					a.SetPtr(cb + 15, arena_.AllocT<double>(G * static_cast<uint64_t>(heavy.f64_in_l2) * heavy.max_keys));
-				}
 			}
 			if (staged) {
 				a.Set(cb + 13, stage_off);
@@ -1220,8 +1216,7 @@ Executor::HeavyPlan Executor::PlanHeavy(const PipelineCodegen::GroupBySpec &gb, 
 	}
 	HeavyPlan hp;
 	hp.max_keys = K;
-	hp.state_bytes = static_cast<uint64_t>(PipelineCodegen::HeavySlotBytes(gbh, PipelineCodegen::HeavyF64InL2(gbh, cb)));
-	hp.f64_in_l2 = PipelineCodegen::HeavyF64InL2(gbh, cb) ? PipelineCodegen::HeavyF64Fields(gbh) : 0;
+	hp.state_bytes = static_cast<uint64_t>(PipelineCodegen::HeavySlotBytes(gbh));
 	if (hp.smem(P) + extra_smem + 1024 > static_cast<size_t>(props.smem_optin)) return none;
 	hp.module = compile(gbh);
 	const uint32_t SC = 1u << 16;
