@@ -1728,19 +1728,8 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		  << "\t\tu32 rw[4][" << RW << "];\n"
 		  << "\t\t#pragma unroll\n\t\tfor (int q = 0; q < 4; ++q) {\n"
 		  << "\t\t\tconst u64 i = base + 32ull * q + lane;\n"
-		  << "\t\t\tload_record<" << RW << ">(recs + (i < end ? i : end - 1) * " << RS << ", rw[q]);\n\t\t}\n";
-		// Batched carries (bucket_batched, with bucket_plain): the four records' first sum-word atomics
-		// are all issued before any of their carries is looked at, so the four round trips overlap
-		const bool batched = gb.bucket_plain && gb.bucket_batched;
-		std::vector<int> lo_fields;
-		for (int f = 0; f < F; f++) {
-			if (fields[f].kind == "lo") lo_fields.push_back(f);
-		}
-		if (batched) {
-			o << "\t\tu32 bs_[4]; bool bv_[4];\n";
-			for (int f : lo_fields) o << "\t\tu32 bo" << f << "_[4]; u64 bl" << f << "_[4]; i64 bh" << f << "_[4];\n";
-		}
-		o << "\t\t#pragma unroll\n\t\tfor (int q = 0; q < 4; ++q) {\n";
+		  << "\t\t\tload_record<" << RW << ">(recs + (i < end ? i : end - 1) * " << RS << ", rw[q]);\n\t\t}\n"
+		  << "\t\t#pragma unroll\n\t\tfor (int q = 0; q < 4; ++q) {\n";
 		if (gb.heavy_slots > 0) {
 			// partial records of heavy keys: bit 31 of the key word, row count in the next word (0: the
 			// key had no rows in that CTA, the record holds identities and is skipped)
@@ -1763,24 +1752,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			gd.replace(gd.find(one), one.size(), "u32 gc = valid ? (part_rec ? rw[q][1] : 1u) : 0u;");
 		}
 		o << gd;
-		if (batched) {
-			std::ostringstream first;  // every field's update but the sums' upper words
-			for (int f = 0; f < F; f++) {
-				const auto &fd = fields[f];
-				const std::string fs = std::to_string(f);
-				if (fd.kind == "cnt") first << "\t\t\t\tatomicAdd(&DC[slot], (u32)gc);\n";
-				if (fd.kind == "f64") first << "\t\t\t\tatomicAdd(&DF" << fs << "[slot], gf" << fs << ");\n";
-				if (fd.kind == "min" || fd.kind == "max") {
-					first << "\t\t\t\tatomic_" << fd.kind << "_i64(&DM" << fs << "[slot], gm" << fs << ");\n";
-				}
-				if (fd.kind == "lo") {
-					first << "\t\t\t\tbo" << fs << "_[q] = atomicAdd(&DW" << fs << "_0[slot], (u32)glo" << fs << ");\n"
-					      << "\t\t\t\tbl" << fs << "_[q] = glo" << fs << "; bh" << fs << "_[q] = ghi" << fs << ";\n";
-				}
-			}
-			o << "\t\t\tbv_[q] = valid; bs_[q] = slot;\n"
-			  << "\t\t\tif (valid) {\n" << first.str() << "\t\t\t}\n";
-		} else if (gb.bucket_plain) {  // every record updates its slot itself: no warp grouping, no hot run
+		if (gb.bucket_plain) {  // every record updates its slot itself: no warp grouping, no hot run
 			o << "\t\t\tif (valid) {\n" << update("g", "slot") << "\t\t\t}\n";
 		} else {
 		o << "\t\t\tconst u32 peers = __match_any_sync(0xffffffffu, slot);\n"
@@ -1809,22 +1781,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		  << "\t\t\t\t}\n\t\t\t}\n"
 		  << "\t\t\tif (valid && leader) {\n" << update("g", "slot") << "\t\t\t}\n";
 		}
-		o << "\t\t}\n";
-		if (batched) {  // the sums' carries into their upper words, now that the first words' old values are back
-			o << "\t\t#pragma unroll\n\t\tfor (int q = 0; q < 4; ++q) {\n\t\t\tif (!bv_[q]) continue;\n"
-			  << "\t\t\tconst u32 s_ = bs_[q];\n";
-			for (int f : lo_fields) {
-				const std::string fs = std::to_string(f);
-				o << "\t\t\t{ const u32 x_ = (u32)bl" << fs << "_[q]; u32 c_ = (u32)(bo" << fs << "_[q] + x_) < bo" << fs
-				  << "_[q] ? 1u : 0u;\n"
-				  << "\t\t\t  c_ = add_word_carry(&DW" << fs << "_1[s_], (u64)(u32)(bl" << fs << "_[q] >> 32) + c_);\n"
-				  << "\t\t\t  c_ = add_word_carry(&DW" << fs << "_2[s_], (u64)(u32)(u64)bh" << fs << "_[q] + c_);\n"
-				  << "\t\t\t  const u32 top_ = (u32)((u64)bh" << fs << "_[q] >> 32) + c_; if (top_) atomicAdd(&DW" << fs
-				  << "_3[s_], top_); }\n";
-			}
-			o << "\t\t}\n";
-		}
-		o << "\t}\n"
+		o << "\t\t}\n\t}\n"
 		  << "\tif (hot != ~0u && lane == 0) {\n" << update("w", "hot") << "\t}\n"
 		  << (gb.f64_l2 ? "\t__threadfence();  // this thread's reductions are performed before the tables are read\n" : "")
 		  << "\t__syncthreads();\n"
@@ -2235,7 +2192,7 @@ std::string GroupByKey(const PipelineCodegen::GroupBySpec &gb, bool partitioned)
 		o << static_cast<int>(a.kind) << '/' << a.column << '/' << static_cast<int>(a.input_type) << '/'
 		  << static_cast<int>(a.output_type) << ';';
 	}
-	o << "|db:" << gb.direct_bits << "|bt:" << gb.bucket_threads << "|hv:" << gb.heavy_slots << "|f64l2:" << gb.f64_l2 << "|hw:" << gb.heavy_warp << "|bp:" << gb.bucket_plain << "|bb:" << gb.bucket_batched << "|nc:" << gb.narrow_count;
+	o << "|db:" << gb.direct_bits << "|bt:" << gb.bucket_threads << "|hv:" << gb.heavy_slots << "|f64l2:" << gb.f64_l2 << "|hw:" << gb.heavy_warp << "|bp:" << gb.bucket_plain << "|nc:" << gb.narrow_count;
 	return o.str();
 }
 

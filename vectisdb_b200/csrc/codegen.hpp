@@ -150,9 +150,6 @@ public:
 		// Direct-partitioned bucket pass without the warp's equal-slot grouping and hot-key register run:
 		// every record updates its slot with shared atomics (cheaper once heavy keys are pre-aggregated).
 		bool bucket_plain = false;
-		// With bucket_plain: the records of a warp step issue their sums' first-word atomics together and
-		// propagate the carries afterwards (the atomics' round trips overlap).
-		bool bucket_batched = false;
 		// One-pass group-by: fewer than 2^32 items feed it (a multi-match join source counts its matches
 		// too), so shared counts add without carries.
 		bool narrow_count = false;

@@ -436,7 +436,6 @@ std::string GenerateSourceText(const PlanNode &plan, const std::vector<vgpu_colu
 	spec_hv.heavy_warp = true;
 	PipelineCodegen::GroupBySpec spec_plain = spec_dp;
 	spec_plain.bucket_plain = true;
-	spec_plain.bucket_batched = true;
 	spec_hv.f64_l2 = PipelineCodegen::F64Fields(spec_hv) > 0;  // FP64 sums of its bucket pass in L2
 	PipelineCodegen::GroupBySpec spec_nc = spec_gb;
 	spec_nc.narrow_count = true;  // one-pass tables whose counts take no carries

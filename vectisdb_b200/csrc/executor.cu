@@ -1213,8 +1213,6 @@ Executor::HeavyPlan Executor::PlanHeavy(const PipelineCodegen::GroupBySpec &gb, 
 		// VGPU_GB_BUCKET_PLAIN=0 keeps the grouping
 		const char *env_plain = std::getenv("VGPU_GB_BUCKET_PLAIN");
 		gbh.bucket_plain = !(env_plain && std::strcmp(env_plain, "0") == 0);
-		const char *env_batched = std::getenv("VGPU_GB_BUCKET_BATCHED");  // measurement knob
-		gbh.bucket_batched = env_batched && std::strcmp(env_batched, "1") == 0;
 	}
 	HeavyPlan hp;
 	hp.max_keys = K;
