@@ -729,6 +729,8 @@ CUfunction Runtime::ModuleFunction(CUmodule m, const char *name) {
 void Runtime::UnloadModule(CUmodule m) {
 	if (m && cuModuleUnload_) {
 		cuModuleUnload_(m);
+		std::lock_guard<std::mutex> lock(occ_mu_);
+		occ_.clear();  // a later module's functions may reuse these handles
 	}
 }
 
@@ -743,12 +745,21 @@ void Runtime::LaunchModuleKernel(CUfunction f, dim3 grid, dim3 block, size_t sme
 }
 
 int Runtime::MaxActiveBlocks(CUfunction f, int block, size_t smem) {
+	const auto key = std::make_tuple(f, block, smem);
+	{
+		std::lock_guard<std::mutex> lock(occ_mu_);
+		auto it = occ_.find(key);
+		if (it != occ_.end()) return it->second;
+	}
 	if (smem > 32 * 1024) {
 		DriverCheck(cuFuncSetAttribute_(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, static_cast<int>(smem)),
 		            "cuFuncSetAttribute(max dynamic smem)");
 	}
 	int n = 0;
 	DriverCheck(cuOccupancyMaxActiveBlocksPerMultiprocessor_(&n, f, block, smem), "cuOccupancyMaxActiveBlocks");
+	std::lock_guard<std::mutex> lock(occ_mu_);
+	if (occ_.size() >= 4096) occ_.clear();  // bounded: functions of unloaded modules leave stale keys
+	occ_[key] = n;
 	return n;
 }
 

@@ -9,6 +9,7 @@
 #include <memory>
 #include <functional>
 #include <map>
+#include <tuple>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -292,6 +293,10 @@ private:
 	CUresult (*cuGetErrorString_)(CUresult, const char **) = nullptr;
 	CUresult (*cuOccupancyMaxActiveBlocksPerMultiprocessor_)(int *, CUfunction, int, size_t) = nullptr;
 	void DriverCheck(CUresult r, const char *what);
+	// occupancy answers (and the shared-memory attribute set) per (function, block, dynamic shared
+	// bytes): the driver queries cost tens of microseconds per query otherwise
+	std::mutex occ_mu_;
+	std::map<std::tuple<CUfunction, int, size_t>, int> occ_;
 };
 
 } // namespace vgpu
