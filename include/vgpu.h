@@ -194,7 +194,9 @@ vgpu_status vgpu_execute_plan(const vgpu_plan *plan, const vgpu_column *inputs, 
                               const vgpu_exec_options *options, vgpu_result **out);
 
 /* GpuExecutionResult::columns (gpu_engine.hpp:215-222). Column pointers stay valid until
- * vgpu_result_free; their memory space is vgpu_exec_options.output_memory. */
+ * vgpu_result_free; their memory space is vgpu_exec_options.output_memory. Device results keep the
+ * buffers the execution wrote its outputs into (no copy), which a GROUP BY sizes for the largest
+ * group count its key ranges allow: free a device result once it has been read. */
 size_t vgpu_result_column_count(const vgpu_result *result);
 vgpu_status vgpu_result_get_column(const vgpu_result *result, size_t index, vgpu_column *out);
 /* Rows [offset, offset + count) of result column `index` as borrowed pointers into the result (no copy):

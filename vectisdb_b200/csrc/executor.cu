@@ -1749,10 +1749,17 @@ ExecResult ExecutePlan(const PlanNode &plan, const std::vector<vgpu_column> &inp
 		o.rows = c.rows;
 		const size_t bytes = c.rows * TypeSize(c.type);
 		if (options.output_on_device) {
-			// Copy into buffers the result owns, so borrowed inputs/cache entries are never aliased.
-			void *d = Runtime::Get().allocator().Alloc(bytes, stream);
+			// A buffer the execution allocated itself passes to the result as it is; anything else (borrowed
+			// inputs, cache entries, a buffer already handed to another column) is copied, so the result
+			// never aliases memory it does not own.
+			void *d = nullptr;
+			if (bytes && ex.arena().Take(c.data)) {
+				d = c.data;
+			} else {
+				d = Runtime::Get().allocator().Alloc(bytes, stream);
+				if (bytes) VGPU_CUDA(cudaMemcpyAsync(d, c.data, bytes, cudaMemcpyDeviceToDevice, stream));
+			}
 			result.device_buffers.push_back(d);
-			if (bytes) VGPU_CUDA(cudaMemcpyAsync(d, c.data, bytes, cudaMemcpyDeviceToDevice, stream));
 			o.device_data = d;
 			if (c.valid) {
 				const size_t vb = (c.rows + 7) / 8;

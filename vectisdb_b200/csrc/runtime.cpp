@@ -248,6 +248,13 @@ void Arena::Release(void *ptr) {
 	}
 }
 
+bool Arena::Take(void *ptr) {
+	auto it = std::find(owned_.begin(), owned_.end(), ptr);
+	if (it == owned_.end()) return false;
+	owned_.erase(it);
+	return true;
+}
+
 void Arena::FreeNow(void *ptr) {
 	auto it = std::find(owned_.begin(), owned_.end(), ptr);
 	if (it != owned_.end()) {

@@ -146,6 +146,9 @@ public:
 	}
 	//! Stops tracking `ptr`: it survives the arena (used for results left on the device).
 	void Release(void *ptr);
+	//! Hands `ptr` to the caller when the arena owns it (true); false for memory it does not own or
+	//! has already handed over.
+	bool Take(void *ptr);
 	void FreeNow(void *ptr);
 	cudaStream_t stream() const {
 		return stream_;
