@@ -738,14 +738,25 @@ void Runtime::UnloadModule(CUmodule m) {
 		cuModuleUnload_(m);
 		std::lock_guard<std::mutex> lock(occ_mu_);
 		occ_.clear();  // a later module's functions may reuse these handles
+		smem_attr_.clear();
 	}
 }
 
-void Runtime::LaunchModuleKernel(CUfunction f, dim3 grid, dim3 block, size_t smem, cudaStream_t stream, void **args) {
-	if (smem > 32 * 1024) {
-		DriverCheck(cuFuncSetAttribute_(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, static_cast<int>(smem)),
-		            "cuFuncSetAttribute(max dynamic smem)");
+void Runtime::EnsureSmemAttribute(CUfunction f, size_t smem) {
+	if (smem <= 32 * 1024) return;
+	{
+		std::lock_guard<std::mutex> lock(occ_mu_);
+		auto it = smem_attr_.find(f);
+		if (it != smem_attr_.end() && it->second >= smem) return;
 	}
+	DriverCheck(cuFuncSetAttribute_(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, static_cast<int>(smem)),
+	            "cuFuncSetAttribute(max dynamic smem)");
+	std::lock_guard<std::mutex> lock(occ_mu_);
+	smem_attr_[f] = smem;
+}
+
+void Runtime::LaunchModuleKernel(CUfunction f, dim3 grid, dim3 block, size_t smem, cudaStream_t stream, void **args) {
+	EnsureSmemAttribute(f, smem);
 	DriverCheck(cuLaunchKernel_(f, grid.x, grid.y, grid.z, block.x, block.y, block.z, static_cast<unsigned>(smem),
 	                            reinterpret_cast<CUstream>(stream), args, nullptr),
 	            "cuLaunchKernel");
@@ -758,10 +769,7 @@ int Runtime::MaxActiveBlocks(CUfunction f, int block, size_t smem) {
 		auto it = occ_.find(key);
 		if (it != occ_.end()) return it->second;
 	}
-	if (smem > 32 * 1024) {
-		DriverCheck(cuFuncSetAttribute_(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, static_cast<int>(smem)),
-		            "cuFuncSetAttribute(max dynamic smem)");
-	}
+	EnsureSmemAttribute(f, smem);
 	int n = 0;
 	DriverCheck(cuOccupancyMaxActiveBlocksPerMultiprocessor_(&n, f, block, smem), "cuOccupancyMaxActiveBlocks");
 	std::lock_guard<std::mutex> lock(occ_mu_);

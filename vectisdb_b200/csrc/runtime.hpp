@@ -300,6 +300,8 @@ private:
 	// bytes): the driver queries cost tens of microseconds per query otherwise
 	std::mutex occ_mu_;
 	std::map<std::tuple<CUfunction, int, size_t>, int> occ_;
+	std::map<CUfunction, size_t> smem_attr_;  // the dynamic shared-memory limit set per function
+	void EnsureSmemAttribute(CUfunction f, size_t smem);
 };
 
 } // namespace vgpu
