@@ -442,7 +442,10 @@ std::shared_ptr<Module> ModuleCache::GetOrCompileMemo(const std::string &memo_ke
 std::shared_ptr<Module> ModuleCache::GetOrCompile(const std::string &source) {
 	auto &rt = Runtime::Get();
 	const std::string arch = rt.arch();
-	const std::string keyed = source + "\n//arch=" + arch + " fmad=false";
+	// the generated source includes the device library by name: its text is part of the key too, so a
+	// cached CUBIN built against another version of it is never reused
+	static const std::string lib_hash = Sha256Hex(kDeviceLibSource, sizeof(kDeviceLibSource) - 1);
+	const std::string keyed = source + "\n//arch=" + arch + " fmad=false lib=" + lib_hash;
 	const std::string key = Sha256Hex(keyed.data(), keyed.size());
 	{
 		std::lock_guard<std::mutex> lock(mu_);
