@@ -363,14 +363,15 @@ __device__ __forceinline__ long long vgpu_join_find(u64 k, const u64 *__restrict
 	if (shift >= 0xfbu) {
 		if (k >= nb) return -1ll;
 		u32 e;
+		// random reads of an L2-resident table: loaded through L2 only (nothing to reuse in L1)
 		if (shift == 0xfdu) {
-			e = ((const u8 *)sorted)[k];
+			e = __ldcg((const unsigned char *)sorted + k);
 			if (e == 0xffu) return -1ll;
 		} else if (shift == 0xfcu) {
-			e = ((const unsigned short *)sorted)[k];
+			e = __ldcg((const unsigned short *)sorted + k);
 			if (e == 0xffffu) return -1ll;
 		} else {
-			e = ((const u32 *)sorted)[k];
+			e = __ldcg((const unsigned int *)sorted + k);
 			if (e == 0xffffffffu) return -1ll;
 		}
 		return (long long)((1ull << 32) | (u64)(u32)(e + (u32)aux));
@@ -427,7 +428,7 @@ __device__ __forceinline__ u64 vgpu_join_minline(u64 k, const void *__restrict__
 	*count = 0u;
 	if (k >= entries) return 0ull;
 	const u32 cbits = (spec & 3u) + 1u;
-	const u64 e = (spec & 0x80u) ? ((const u64 *)table)[k] : (u64)((const u32 *)table)[k];
+	const u64 e = (spec & 0x80u) ? __ldcg((const unsigned long long *)table + k) : (u64)__ldcg((const unsigned int *)table + k);
 	*count = (u32)(e & ((1ull << cbits) - 1ull));
 	return e;
 }
