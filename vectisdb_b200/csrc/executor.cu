@@ -1459,9 +1459,8 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 			JoinTableCache::Get().Insert(cache_key, t);
 		};
 		uint64_t *rw = arena_.AllocT<uint64_t>(rn);
-		kern::WidenKeys(rk->data, kw, rn, rw, stream_);
 		uint64_t *mm = arena_.AllocT<uint64_t>(3);  // key min, key max, value bits (min, max)
-		kern::MinMaxU64(rw, rn, mm, stream_);
+		kern::WidenKeysMinMax(rk->data, kw, rn, rw, mm, stream_);
 		if (inline_col) kern::ValueBits(inline_col->data, TypeSize(inline_col->type), rn, reinterpret_cast<uint32_t *>(mm + 2), stream_);
 		uint64_t host_mm[3] = {0, 0, 0};
 		VGPU_CUDA(cudaMemcpyAsync(host_mm, mm, inline_col ? 24 : 16, cudaMemcpyDeviceToHost, stream_));
@@ -1470,7 +1469,7 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 		const uint64_t range = host_mm[1] - host_mm[0];
 		const uint32_t vmin = static_cast<uint32_t>(host_mm[2]), vmax = static_cast<uint32_t>(host_mm[2] >> 32);
 		const int bits = BitsFor(range);
-		kern::SubtractBias(rw, rn, bias, stream_);
+		// the dense tables subtract the bias as they index; the sorted form below works on biased keys
 		uint32_t *dups = arena_.AllocT<uint32_t>(1);
 		bool built = false;
 		// Dense keys (range within 4x the key count, at most 2^28): a table indexed by the key over the whole
@@ -1489,7 +1488,7 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 			if (compact) {
 				void *table = arena_.Alloc((range + 1) * width);
 				kern::JoinDenseCompact(rw, inline_col->data, TypeSize(inline_col->type), rn, range, vmin, table, width, dups,
-				                       stream_);
+				                       stream_, bias);
 				if (ReadU32(dups) == 0) {
 					add_sources(false, nullptr);
 					pin.spec.join_inline = true;
@@ -1501,7 +1500,7 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 				}
 			} else if (inline_col) {
 				uint64_t *table = arena_.AllocT<uint64_t>(range + 1);
-				kern::JoinDenseInline(rw, inline_col->data, TypeSize(inline_col->type), rn, range, table, dups, stream_);
+				kern::JoinDenseInline(rw, inline_col->data, TypeSize(inline_col->type), rn, range, table, dups, stream_, bias);
 				if (ReadU32(dups) == 0) {
 					add_sources(false, nullptr);
 					pin.spec.join_inline = true;
@@ -1513,7 +1512,7 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 				}
 			} else {
 				uint32_t *table = arena_.AllocT<uint32_t>(range + 1);
-				kern::JoinDenseRows(rw, rn, range, table, dups, stream_);
+				kern::JoinDenseRows(rw, rn, range, table, dups, stream_, bias);
 				if (ReadU32(dups) == 0) {
 					add_sources(false, nullptr);
 					pin.join_words[0] = 0;
@@ -1540,7 +1539,7 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 				const uint64_t bytes = (range + 1) * (wide ? 8 : 4);
 				void *table = arena_.Alloc(bytes);
 				kern::JoinDenseMulti(rw, inline_col->data, TypeSize(inline_col->type), rn, range, vmin, vbits, cbits, rmax,
-				                     table, wide != 0, overflow, stream_);
+				                     table, wide != 0, overflow, stream_, bias);
 				if (ReadU32(overflow) == 0) {
 					add_sources(false, nullptr);
 					pin.spec.join_multi = pin.spec.join_minline = true;
@@ -1557,6 +1556,7 @@ Relation Executor::JoinForPipeline(const PlanNode &node, PipelineInput &pin, boo
 		if (!built) {
 			// Sorted form: LSD radix sort of the right keys, uniqueness check, radix directory over the sorted
 			// keys (at most 2^22 buckets), right columns gathered into sorted order once.
+			kern::SubtractBias(rw, rn, bias, stream_);
 			uint32_t *perm = arena_.AllocT<uint32_t>(rn);
 			kern::Iota(perm, rn, stream_);
 			uint64_t *rw_alt = arena_.AllocT<uint64_t>(rn);
@@ -1661,9 +1661,8 @@ Relation Executor::JoinMaterialize(const PlanNode &node, Relation &left, Relatio
 	uint64_t *lw = arena_.AllocT<uint64_t>(ln);
 	uint64_t *rw = arena_.AllocT<uint64_t>(rn);
 	kern::WidenKeys(lk.data, kw, ln, lw, stream_);
-	kern::WidenKeys(rk.data, kw, rn, rw, stream_);
 	uint64_t *mm = arena_.AllocT<uint64_t>(2);
-	kern::MinMaxU64(rw, rn, mm, stream_);
+	kern::WidenKeysMinMax(rk.data, kw, rn, rw, mm, stream_);
 	uint64_t host_mm[2];
 	VGPU_CUDA(cudaMemcpyAsync(host_mm, mm, 16, cudaMemcpyDeviceToHost, stream_));
 	VGPU_CUDA(cudaStreamSynchronize(stream_));

@@ -156,23 +156,61 @@ template <typename T> __global__ void WidenKernel(const T *src, uint64_t n, uint
 	}
 }
 
-__global__ void MinMaxKernel(const uint64_t *keys, uint64_t n, uint64_t *minmax) {
-	uint64_t mn = ~0ull, mx = 0;
-	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-		uint64_t k = keys[i];
-		mn = k < mn ? k : mn;
-		mx = k > mx ? k : mx;
-	}
+// The CTA's smallest and largest value (unsigned) folded into out[0] / out[1] with one atomic pair per
+// CTA: per-warp atomics on two words serialize at L2 once thousands of warps reach them.
+template <typename U>
+__device__ __forceinline__ void BlockMinMaxToGlobal(U mn, U mx, U *out) {
+	__shared__ U smn[32], smx[32];
 	for (int o = 16; o > 0; o >>= 1) {
-		uint64_t a = __shfl_xor_sync(0xffffffffu, mn, o);
-		uint64_t b = __shfl_xor_sync(0xffffffffu, mx, o);
+		const U a = __shfl_xor_sync(0xffffffffu, mn, o);
+		const U b = __shfl_xor_sync(0xffffffffu, mx, o);
 		mn = a < mn ? a : mn;
 		mx = b > mx ? b : mx;
 	}
-	if ((threadIdx.x & 31) == 0) {
-		atomicMin(reinterpret_cast<unsigned long long *>(&minmax[0]), mn);
-		atomicMax(reinterpret_cast<unsigned long long *>(&minmax[1]), mx);
+	const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	if (lane == 0) {
+		smn[warp] = mn;
+		smx[warp] = mx;
 	}
+	__syncthreads();
+	if (warp == 0) {
+		const unsigned nw = (blockDim.x + 31) >> 5;
+		mn = lane < nw ? smn[lane] : smn[0];
+		mx = lane < nw ? smx[lane] : smx[0];
+		for (int o = 16; o > 0; o >>= 1) {
+			const U a = __shfl_xor_sync(0xffffffffu, mn, o);
+			const U b = __shfl_xor_sync(0xffffffffu, mx, o);
+			mn = a < mn ? a : mn;
+			mx = b > mx ? b : mx;
+		}
+		if (lane == 0) {
+			atomicMin(&out[0], mn);
+			atomicMax(&out[1], mx);
+		}
+	}
+}
+
+__global__ void MinMaxKernel(const uint64_t *keys, uint64_t n, uint64_t *minmax) {
+	unsigned long long mn = ~0ull, mx = 0;
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+		const unsigned long long k = keys[i];
+		mn = k < mn ? k : mn;
+		mx = k > mx ? k : mx;
+	}
+	BlockMinMaxToGlobal<unsigned long long>(mn, mx, reinterpret_cast<unsigned long long *>(minmax));
+}
+
+// Keys zero-extended to 64 bits and their range in one pass (the widening and the range the dense join
+// tables need).
+template <typename T> __global__ void WidenMinMaxKernel(const T *src, uint64_t n, uint64_t *dst, uint64_t *minmax) {
+	unsigned long long mn = ~0ull, mx = 0;
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+		const unsigned long long k = static_cast<uint64_t>(src[i]);
+		dst[i] = k;
+		mn = k < mn ? k : mn;
+		mx = k > mx ? k : mx;
+	}
+	BlockMinMaxToGlobal<unsigned long long>(mn, mx, reinterpret_cast<unsigned long long *>(minmax));
 }
 
 template <typename T> __global__ void MinMaxSignedKernel(const T *data, uint64_t n, int64_t *out) {
@@ -469,52 +507,45 @@ __global__ void JoinDirectoryKernel(const uint64_t *sorted, uint64_t n, uint32_t
 
 // Dense key tables: entry of (biased) key k = row index + 1, or (1 << 32 | value) with the row's
 // value inlined; a key met twice counts as a duplicate (compare-and-swap from empty).
-__global__ void JoinDenseRowsKernel(const uint64_t *keys, uint64_t n, uint32_t *table, uint32_t *dups) {
+__global__ void JoinDenseRowsKernel(const uint64_t *keys, uint64_t n, uint64_t bias, uint32_t *table, uint32_t *dups) {
 	uint32_t local = 0;
 	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-		if (atomicCAS(&table[keys[i]], 0u, static_cast<uint32_t>(i + 1)) != 0u) local++;
+		if (atomicCAS(&table[keys[i] - bias], 0u, static_cast<uint32_t>(i + 1)) != 0u) local++;
 	}
 	if (local) atomicAdd(dups, local);
 }
 
 template <typename T>
-__global__ void JoinDenseInlineKernel(const uint64_t *keys, const T *values, uint64_t n, unsigned long long *table,
-                                      uint32_t *dups) {
+__global__ void JoinDenseInlineKernel(const uint64_t *keys, const T *values, uint64_t n, uint64_t bias,
+                                      unsigned long long *table, uint32_t *dups) {
 	uint32_t local = 0;
 	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
 		const unsigned long long e = (1ull << 32) | static_cast<unsigned long long>(values[i]);
-		if (atomicCAS(&table[keys[i]], 0ull, e) != 0ull) local++;
+		if (atomicCAS(&table[keys[i] - bias], 0ull, e) != 0ull) local++;
 	}
 	if (local) atomicAdd(dups, local);
 }
 
 template <typename T> __global__ void ValueBitsKernel(const T *values, uint64_t n, uint32_t *bounds) {
-	uint32_t lo = 0xffffffffu, hi = 0;
+	unsigned int lo = 0xffffffffu, hi = 0;
 	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-		const uint32_t bits = static_cast<uint32_t>(values[i]);
+		const unsigned int bits = static_cast<uint32_t>(values[i]);
 		lo = bits < lo ? bits : lo;
 		hi = bits > hi ? bits : hi;
 	}
-	for (int d = 16; d > 0; d >>= 1) {
-		lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, d));
-		hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, d));
-	}
-	if ((threadIdx.x & 31) == 0) {
-		atomicMin(bounds, lo);
-		atomicMax(bounds + 1, hi);
-	}
+	BlockMinMaxToGlobal<unsigned int>(lo, hi, bounds);
 }
 
 // Compact inline table: entry = value bits - vmin in E (all ones = no key), filled by compare-and-swap
 // from the marker; a key met twice counts in *dups. One-byte entries swap their 32-bit word (bounded
 // retries while neighbours change it; running out counts as a duplicate, so the caller falls back).
 template <typename T, typename E>
-__global__ void JoinDenseCompactKernel(const uint64_t *keys, const T *values, uint64_t n, uint32_t vmin, E *table,
-                                       uint32_t *dups) {
+__global__ void JoinDenseCompactKernel(const uint64_t *keys, const T *values, uint64_t n, uint64_t bias, uint32_t vmin,
+                                       E *table, uint32_t *dups) {
 	uint32_t local = 0;
 	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
 		const uint32_t entry = static_cast<uint32_t>(values[i]) - vmin;
-		E *slot = table + keys[i];
+		E *slot = table + (keys[i] - bias);
 		if constexpr (sizeof(E) == 4) {
 			if (atomicCAS(reinterpret_cast<unsigned int *>(slot), 0xffffffffu, entry) != 0xffffffffu) local++;
 		} else if constexpr (sizeof(E) == 2) {
@@ -666,16 +697,16 @@ void JoinDirectory(const uint64_t *sorted, uint64_t n, uint32_t shift, uint64_t 
 }
 
 void JoinDenseRows(const uint64_t *keys, uint64_t n, uint64_t range, uint32_t *table, uint32_t *dups,
-                   cudaStream_t stream) {
+                   cudaStream_t stream, uint64_t bias) {
 	LaunchScope scope("join_dense_table", stream, n * 12 + (range + 1) * 4, n);
 	VGPU_CUDA(cudaMemsetAsync(table, 0, (range + 1) * 4, stream));
 	VGPU_CUDA(cudaMemsetAsync(dups, 0, 4, stream));
-	JoinDenseRowsKernel<<<GridFor(n, 256), 256, 0, stream>>>(keys, n, table, dups);
+	JoinDenseRowsKernel<<<GridFor(n, 256), 256, 0, stream>>>(keys, n, bias, table, dups);
 	VGPU_CUDA(cudaGetLastError());
 }
 
 void JoinDenseInline(const uint64_t *keys, const void *values, size_t width, uint64_t n, uint64_t range,
-                     uint64_t *table, uint32_t *dups, cudaStream_t stream) {
+                     uint64_t *table, uint32_t *dups, cudaStream_t stream, uint64_t bias) {
 	LaunchScope scope("join_dense_table", stream, n * (8 + width) + (range + 1) * 8, n);
 	VGPU_CUDA(cudaMemsetAsync(table, 0, (range + 1) * 8, stream));
 	VGPU_CUDA(cudaMemsetAsync(dups, 0, 4, stream));
@@ -683,13 +714,13 @@ void JoinDenseInline(const uint64_t *keys, const void *values, size_t width, uin
 	const unsigned grid = GridFor(n, 256);
 	switch (width) {
 	case 1:
-		JoinDenseInlineKernel<uint8_t><<<grid, 256, 0, stream>>>(keys, static_cast<const uint8_t *>(values), n, t, dups);
+		JoinDenseInlineKernel<uint8_t><<<grid, 256, 0, stream>>>(keys, static_cast<const uint8_t *>(values), n, bias, t, dups);
 		break;
 	case 2:
-		JoinDenseInlineKernel<uint16_t><<<grid, 256, 0, stream>>>(keys, static_cast<const uint16_t *>(values), n, t, dups);
+		JoinDenseInlineKernel<uint16_t><<<grid, 256, 0, stream>>>(keys, static_cast<const uint16_t *>(values), n, bias, t, dups);
 		break;
 	case 4:
-		JoinDenseInlineKernel<uint32_t><<<grid, 256, 0, stream>>>(keys, static_cast<const uint32_t *>(values), n, t, dups);
+		JoinDenseInlineKernel<uint32_t><<<grid, 256, 0, stream>>>(keys, static_cast<const uint32_t *>(values), n, bias, t, dups);
 		break;
 	default:
 		Fail(VGPU_ERR_INTERNAL, "dense inline join table: value width must be 1, 2 or 4 bytes");
@@ -718,12 +749,12 @@ void ValueBits(const void *values, size_t width, uint64_t n, uint32_t *bounds, c
 // with more than rmax matches (rmax < 2^cbits, so the count never wraps before it is seen) counts in
 // *overflow and the table is not valid.
 template <typename T, typename E>
-__global__ void JoinDenseMultiKernel(const uint64_t *keys, const T *values, uint64_t n, uint32_t vmin, uint32_t vbits,
-                                     uint32_t cbits, uint32_t rmax, E *table, uint32_t *overflow) {
+__global__ void JoinDenseMultiKernel(const uint64_t *keys, const T *values, uint64_t n, uint64_t bias, uint32_t vmin,
+                                     uint32_t vbits, uint32_t cbits, uint32_t rmax, E *table, uint32_t *overflow) {
 	const E cmask = (E(1) << cbits) - 1;
 	uint32_t local = 0;
 	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-		E *slot = table + keys[i];
+		E *slot = table + (keys[i] - bias);
 		const E old = atomicAdd(slot, E(1));
 		const uint32_t j = static_cast<uint32_t>(old & cmask);
 		if (j >= rmax) {
@@ -738,21 +769,21 @@ __global__ void JoinDenseMultiKernel(const uint64_t *keys, const T *values, uint
 
 namespace {
 template <typename E>
-void LaunchDenseCompact(const uint64_t *keys, const void *values, size_t vwidth, uint64_t n, uint32_t vmin, E *table,
-                        uint32_t *dups, cudaStream_t stream) {
+void LaunchDenseCompact(const uint64_t *keys, const void *values, size_t vwidth, uint64_t n, uint64_t bias, uint32_t vmin,
+                        E *table, uint32_t *dups, cudaStream_t stream) {
 	const unsigned grid = GridFor(n, 256);
 	switch (vwidth) {
 	case 1:
-		JoinDenseCompactKernel<uint8_t, E><<<grid, 256, 0, stream>>>(keys, static_cast<const uint8_t *>(values), n, vmin,
-		                                                             table, dups);
+		JoinDenseCompactKernel<uint8_t, E><<<grid, 256, 0, stream>>>(keys, static_cast<const uint8_t *>(values), n, bias,
+		                                                             vmin, table, dups);
 		break;
 	case 2:
 		JoinDenseCompactKernel<uint16_t, E><<<grid, 256, 0, stream>>>(keys, static_cast<const uint16_t *>(values), n,
-		                                                              vmin, table, dups);
+		                                                              bias, vmin, table, dups);
 		break;
 	case 4:
 		JoinDenseCompactKernel<uint32_t, E><<<grid, 256, 0, stream>>>(keys, static_cast<const uint32_t *>(values), n,
-		                                                              vmin, table, dups);
+		                                                              bias, vmin, table, dups);
 		break;
 	default:
 		Fail(VGPU_ERR_INTERNAL, "compact join table: value width must be 1, 2 or 4 bytes");
@@ -761,14 +792,14 @@ void LaunchDenseCompact(const uint64_t *keys, const void *values, size_t vwidth,
 } // namespace
 
 void JoinDenseCompact(const uint64_t *keys, const void *values, size_t vwidth, uint64_t n, uint64_t range,
-                      uint32_t vmin, void *table, size_t width, uint32_t *dups, cudaStream_t stream) {
+                      uint32_t vmin, void *table, size_t width, uint32_t *dups, cudaStream_t stream, uint64_t bias) {
 	LaunchScope scope("join_dense_table", stream, n * (8 + vwidth) + (range + 1) * width, n);
 	VGPU_CUDA(cudaMemsetAsync(table, 0xff, (range + 1) * width, stream));
 	VGPU_CUDA(cudaMemsetAsync(dups, 0, 4, stream));
 	switch (width) {
-	case 1: LaunchDenseCompact(keys, values, vwidth, n, vmin, static_cast<uint8_t *>(table), dups, stream); break;
-	case 2: LaunchDenseCompact(keys, values, vwidth, n, vmin, static_cast<uint16_t *>(table), dups, stream); break;
-	case 4: LaunchDenseCompact(keys, values, vwidth, n, vmin, static_cast<uint32_t *>(table), dups, stream); break;
+	case 1: LaunchDenseCompact(keys, values, vwidth, n, bias, vmin, static_cast<uint8_t *>(table), dups, stream); break;
+	case 2: LaunchDenseCompact(keys, values, vwidth, n, bias, vmin, static_cast<uint16_t *>(table), dups, stream); break;
+	case 4: LaunchDenseCompact(keys, values, vwidth, n, bias, vmin, static_cast<uint32_t *>(table), dups, stream); break;
 	default: Fail(VGPU_ERR_INTERNAL, "compact join table: width must be 1, 2 or 4 bytes");
 	}
 	VGPU_CUDA(cudaGetLastError());
@@ -776,7 +807,7 @@ void JoinDenseCompact(const uint64_t *keys, const void *values, size_t vwidth, u
 
 void JoinDenseMulti(const uint64_t *keys, const void *values, size_t vwidth, uint64_t n, uint64_t range, uint32_t vmin,
                     uint32_t vbits, uint32_t cbits, uint32_t rmax, void *table, bool wide, uint32_t *overflow,
-                    cudaStream_t stream) {
+                    cudaStream_t stream, uint64_t bias) {
 	const size_t ew = wide ? 8 : 4;
 	if (cbits < 1 || cbits > 3 || rmax >= (1u << cbits) || cbits + rmax * vbits > ew * 8) {
 		Fail(VGPU_ERR_INTERNAL, "multi-match join table: slots do not fit the entry");
@@ -789,16 +820,16 @@ void JoinDenseMulti(const uint64_t *keys, const void *values, size_t vwidth, uin
 		using E = std::remove_pointer_t<decltype(tab)>;
 		switch (vwidth) {
 		case 1:
-			JoinDenseMultiKernel<uint8_t, E><<<grid, 256, 0, stream>>>(keys, static_cast<const uint8_t *>(values), n, vmin,
-			                                                           vbits, cbits, rmax, tab, overflow);
+			JoinDenseMultiKernel<uint8_t, E><<<grid, 256, 0, stream>>>(keys, static_cast<const uint8_t *>(values), n, bias,
+			                                                           vmin, vbits, cbits, rmax, tab, overflow);
 			break;
 		case 2:
 			JoinDenseMultiKernel<uint16_t, E><<<grid, 256, 0, stream>>>(keys, static_cast<const uint16_t *>(values), n,
-			                                                            vmin, vbits, cbits, rmax, tab, overflow);
+			                                                            bias, vmin, vbits, cbits, rmax, tab, overflow);
 			break;
 		case 4:
 			JoinDenseMultiKernel<uint32_t, E><<<grid, 256, 0, stream>>>(keys, static_cast<const uint32_t *>(values), n,
-			                                                            vmin, vbits, cbits, rmax, tab, overflow);
+			                                                            bias, vmin, vbits, cbits, rmax, tab, overflow);
 			break;
 		default:
 			Fail(VGPU_ERR_INTERNAL, "multi-match join table: value width must be 1, 2 or 4 bytes");
@@ -1041,7 +1072,35 @@ void MinMaxU64(const uint64_t *keys, uint64_t n, uint64_t *minmax, cudaStream_t 
 	LaunchScope scope("minmax", stream, n * 8, n);
 	InitMinMaxKernel<<<1, 1, 0, stream>>>(minmax);
 	if (n > 0) {
-		MinMaxKernel<<<GridFor(n, 256), 256, 0, stream>>>(keys, n, minmax);
+		const unsigned grid = std::min<unsigned>(GridFor(n, 256), Runtime::Get().props().sm_count * 8);
+		MinMaxKernel<<<grid, 256, 0, stream>>>(keys, n, minmax);
+	}
+	VGPU_CUDA(cudaGetLastError());
+}
+
+void WidenKeysMinMax(const void *src, size_t width, uint64_t n, uint64_t *dst, uint64_t *minmax, cudaStream_t stream) {
+	InitMinMaxKernel<<<1, 1, 0, stream>>>(minmax);
+	if (n == 0) {
+		VGPU_CUDA(cudaGetLastError());
+		return;
+	}
+	LaunchScope scope("widen_keys", stream, n * (width + 8), n);
+	const unsigned grid = std::min<unsigned>(GridFor(n, 256), Runtime::Get().props().sm_count * 8);
+	switch (width) {
+	case 1:
+		WidenMinMaxKernel<uint8_t><<<grid, 256, 0, stream>>>(static_cast<const uint8_t *>(src), n, dst, minmax);
+		break;
+	case 2:
+		WidenMinMaxKernel<uint16_t><<<grid, 256, 0, stream>>>(static_cast<const uint16_t *>(src), n, dst, minmax);
+		break;
+	case 4:
+		WidenMinMaxKernel<uint32_t><<<grid, 256, 0, stream>>>(static_cast<const uint32_t *>(src), n, dst, minmax);
+		break;
+	case 8:
+		WidenMinMaxKernel<uint64_t><<<grid, 256, 0, stream>>>(static_cast<const uint64_t *>(src), n, dst, minmax);
+		break;
+	default:
+		Fail(VGPU_ERR_INTERNAL, "widen: unsupported width");
 	}
 	VGPU_CUDA(cudaGetLastError());
 }

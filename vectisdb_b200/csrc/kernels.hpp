@@ -33,6 +33,8 @@ void Gather(const void *src, size_t width, const uint32_t *idx, uint64_t n, void
 //! cuda_engine/src/operators/gpu_groupby.cu:76-94), plus the range of the widened values.
 void WidenKeys(const void *src, size_t width, uint64_t n, uint64_t *dst, cudaStream_t stream);
 void MinMaxU64(const uint64_t *keys, uint64_t n, uint64_t *minmax /* device [2] */, cudaStream_t stream);
+//! WidenKeys and MinMaxU64 of the widened keys in one pass.
+void WidenKeysMinMax(const void *src, size_t width, uint64_t n, uint64_t *dst, uint64_t *minmax, cudaStream_t stream);
 
 //! Signed range of an integer/boolean column: out[0] = min, out[1] = max (device i64[2]).
 void MinMaxSigned(const void *data, int type /* ValueType */, uint64_t n, int64_t *out, cudaStream_t stream);
@@ -59,19 +61,21 @@ void JoinRuns(const uint64_t *probe, uint64_t n_probe, const uint64_t *sorted, c
 //! Radix directory of a sorted (biased) key array: dir[b] = first position whose key >> shift >= b,
 //! for b in [0, nb]; dir needs nb + 1 entries and nb must exceed every key >> shift.
 void JoinDirectory(const uint64_t *sorted, uint64_t n, uint32_t shift, uint64_t nb, uint32_t *dir, cudaStream_t stream);
-//! Dense join tables over (biased) keys all <= range, range + 1 entries, built without sorting:
+//! Dense join tables over keys - bias all <= range (`bias`: the keys' minimum, subtracted on the fly;
+//! 0 for keys already biased), range + 1 entries, built without sorting:
 //! table[k] = row index + 1 of key k (0 = none), or (1 << 32 | value) with a <= 4-byte value of that
 //! row inlined. *dups = keys met more than once (then the table is not a valid lookup).
 void JoinDenseRows(const uint64_t *keys, uint64_t n, uint64_t range, uint32_t *table, uint32_t *dups,
-                   cudaStream_t stream);
+                   cudaStream_t stream, uint64_t bias = 0);
 void JoinDenseInline(const uint64_t *keys, const void *values, size_t width, uint64_t n, uint64_t range,
-                     uint64_t *table, uint32_t *dups, cudaStream_t stream);
+                     uint64_t *table, uint32_t *dups, cudaStream_t stream, uint64_t bias = 0);
 //! Smallest and largest raw bits (zero-extended to 32) of a 1-, 2- or 4-byte column: bounds[0], bounds[1].
 void ValueBits(const void *values, size_t width, uint64_t n, uint32_t *bounds, cudaStream_t stream);
 //! The inline table in `width` (1, 2 or 4) bytes per key: table[k] = value bits - vmin, all ones = no
 //! key (every value's offset must stay below that marker). *dups = keys met more than once.
 void JoinDenseCompact(const uint64_t *keys, const void *values, size_t vwidth, uint64_t n, uint64_t range,
-                      uint32_t vmin, void *table, size_t width, uint32_t *dups, cudaStream_t stream);
+                      uint32_t vmin, void *table, size_t width, uint32_t *dups, cudaStream_t stream,
+                      uint64_t bias = 0);
 //! Dense multi-match table over (biased) keys <= range, built without sorting, for a join that contributes
 //! one right column of at most 4 bytes: entry[k] (4 bytes, or 8 when `wide`) holds k's match count in its
 //! low `cbits` bits (1..3) and one `vbits`-bit slot per match above them, each the value bits - vmin. A key
@@ -79,7 +83,7 @@ void JoinDenseCompact(const uint64_t *keys, const void *values, size_t vwidth, u
 //! *overflow, and the table is then not valid.
 void JoinDenseMulti(const uint64_t *keys, const void *values, size_t vwidth, uint64_t n, uint64_t range, uint32_t vmin,
                     uint32_t vbits, uint32_t cbits, uint32_t rmax, void *table, bool wide, uint32_t *overflow,
-                    cudaStream_t stream);
+                    cudaStream_t stream, uint64_t bias = 0);
 //! *out = number of positions i > 0 with sorted[i] == sorted[i - 1].
 void CountAdjacentEqual(const uint64_t *sorted, uint64_t n, uint32_t *out, cudaStream_t stream);
 //! *out = the length of the longest run of equal keys in `sorted` (saturating at 2^32 - 1).
