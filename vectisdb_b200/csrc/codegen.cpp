@@ -679,12 +679,15 @@ std::string InitValue(const Field &f) {
 // `narrow_count`: fewer than 2^32 rows reach the table, so the low word never carries and the count
 // is a plain 32-bit add whose result nothing waits for.
 std::string UpdateCode(const std::vector<Field> &fields, const std::string &tab, const std::string &slot,
-                       const std::vector<std::string> &agg_values, bool shared, bool narrow_count = false) {
+                       const std::vector<std::string> &agg_values, bool shared, bool narrow_count = false,
+                       bool count_as_flag = false) {
 	std::ostringstream o;
 	for (size_t i = 0; i < fields.size(); i++) {
 		auto &f = fields[i];
 		std::string p = tab + std::to_string(i) + " + " + slot;
-		if (f.kind == "cnt" && shared && narrow_count) {
+		if (f.kind == "cnt" && shared && count_as_flag) {
+			o << "\t\t\t*(u32*)(" << p << ") = 1u;\n";
+		} else if (f.kind == "cnt" && shared && narrow_count) {
 			o << "\t\t\tatomicAdd((u32*)(" << p << "), 1u);\n";
 		} else if (f.kind == "cnt" && shared) {
 			o << "\t\t\t{ u32 *w_ = (u32*)(" << p << "); if (atomicAdd(w_, 1u) == 0xffffffffu) atomicAdd(w_ + 1, 1u); }\n";
@@ -955,7 +958,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		  << "\tfor (u64 tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n"
 		  << LoadBlock(g, needed, false) << ItemOpen(g, needed) << chain_code_ << "\t\tif (keep) {\n"
 		  << "\t\t\tconst u64 slot = " << pack.str() << ";\n"
-		  << UpdateCode(fields, "T", "slot", pipe_values, true, gb.narrow_count) << "\t\t}\n" << ItemClose()
+		  << UpdateCode(fields, "T", "slot", pipe_values, true, gb.narrow_count, gb.count_as_flag) << "\t\t}\n" << ItemClose()
 		  << "\t}\n"
 		  << (l2 ? "\t__threadfence();  // this thread's reductions are performed before the sums are read\n" : "")
 		  << "\t__syncthreads();\n";
@@ -2192,7 +2195,7 @@ std::string GroupByKey(const PipelineCodegen::GroupBySpec &gb, bool partitioned)
 		o << static_cast<int>(a.kind) << '/' << a.column << '/' << static_cast<int>(a.input_type) << '/'
 		  << static_cast<int>(a.output_type) << ';';
 	}
-	o << "|db:" << gb.direct_bits << "|bt:" << gb.bucket_threads << "|hv:" << gb.heavy_slots << "|f64l2:" << gb.f64_l2 << "|hw:" << gb.heavy_warp << "|bp:" << gb.bucket_plain << "|nc:" << gb.narrow_count;
+	o << "|db:" << gb.direct_bits << "|bt:" << gb.bucket_threads << "|hv:" << gb.heavy_slots << "|f64l2:" << gb.f64_l2 << "|hw:" << gb.heavy_warp << "|bp:" << gb.bucket_plain << "|nc:" << gb.narrow_count << "|cf:" << gb.count_as_flag;
 	return o.str();
 }
 

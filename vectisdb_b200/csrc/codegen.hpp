@@ -153,6 +153,9 @@ public:
 		// One-pass group-by: fewer than 2^32 items feed it (a multi-match join source counts its matches
 		// too), so shared counts add without carries.
 		bool narrow_count = false;
+		// One-pass group-by: no aggregate reads the row count (no COUNT, no AVG), so the count word only
+		// marks a group as present -- a plain store of 1, not an atomic add.
+		bool count_as_flag = false;
 	};
 
 	//! Group-by kernels (see executor for the argument layout), all in one translation unit:

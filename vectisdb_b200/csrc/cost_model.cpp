@@ -439,6 +439,7 @@ std::string GenerateSourceText(const PlanNode &plan, const std::vector<vgpu_colu
 	spec_hv.f64_l2 = PipelineCodegen::F64Fields(spec_hv) > 0;  // FP64 sums of its bucket pass in L2
 	PipelineCodegen::GroupBySpec spec_nc = spec_gb;
 	spec_nc.narrow_count = true;  // one-pass tables whose counts take no carries
+	spec_nc.count_as_flag = true;  // ... or are presence flags
 	spec_nc.f64_l2 = PipelineCodegen::F64Fields(spec_nc) > 0;  // ... and FP64 sums in L2
 	// ... and both with tiles staged through shared memory by bulk copies
 	Geometry gst = g;

@@ -835,6 +835,10 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 	if (direct) {
 		// a CTA's table sees at most n items (a multi-match join source can expand past n: keep carries)
 		gb.narrow_count = !pin.spec.join_multi && n < (1ull << 32);
+		gb.count_as_flag = true;  // unless an aggregate reads the count
+		for (auto &ag : gb.aggs) {
+			if (ag.kind == AggKind::COUNT || ag.kind == AggKind::COUNT_STAR || ag.kind == AggKind::AVG) gb.count_as_flag = false;
+		}
 		gb.f64_l2 = direct_l2;
 		Geometry g;
 		g.block = 512;
