@@ -819,6 +819,13 @@ int PipelineCodegen::DirectSlotBytes(const GroupBySpec &gb) {
 	return bytes;
 }
 
+uint64_t PipelineCodegen::DirectSmemBytes(const GroupBySpec &gb, uint64_t domain) {
+	const int F = static_cast<int>(StateFields(gb).size());
+	const int shared64 = F - 1 - (gb.f64_l2 ? F64Fields(gb) : 0);
+	const bool c32 = gb.narrow_count || gb.count_as_flag;
+	return domain * (static_cast<uint64_t>(shared64) * 8 + (c32 ? 4 : 8));
+}
+
 int PipelineCodegen::F64Fields(const GroupBySpec &gb) {
 	int n = 0;
 	for (auto &f : StateFields(gb)) n += f.kind == "f64" ? 1 : 0;
@@ -942,14 +949,19 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_gb_direct(KArgs a) {\n"
 		  << kKernelHead << "\textern __shared__ __align__(16) u64 vgpu_smem[];\n"
 		  << "\tconst u64 D = a.w[" << cb << "];\n";
-		for (int f = 0, sh = 0, gl = 0; f < F; f++) {
+		// A count that never carries (fewer than 2^32 rows) or only marks presence needs 32 bits: its array
+		// goes after the 64-bit ones, in 4 bytes per slot (DirectSmemBytes sizes the launch alike).
+		const bool c32 = gb.narrow_count || gb.count_as_flag;
+		int sh = 0;
+		for (int f = 0, gl = 0; f < F; f++) {
 			if (l2 && fields[f].kind == "f64") {
 				o << "\tu64 *T" << f << " = (u64*)a.w[" << cb + 2 + F + out_words << "] + ((u64)blockIdx.x * " << nl2
 				  << " + " << gl++ << ") * D;\n";
-			} else {
+			} else if (!(c32 && f == 0)) {
 				o << "\tu64 *T" << f << " = vgpu_smem + " << sh++ << " * D;\n";
 			}
 		}
+		if (c32) o << "\tu32 *T0 = (u32*)(vgpu_smem + " << sh << " * D);\n";
 		o << "\tfor (u64 s = threadIdx.x; s < D; s += " << g.block << ") {\n";
 		for (int f = 0; f < F; f++) {
 			o << "\t\tT" << f << "[s] = " << InitValue(fields[f]) << ";\n";

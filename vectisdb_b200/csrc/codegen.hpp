@@ -182,6 +182,8 @@ public:
 	static int DirectSlotBytes(const GroupBySpec &gb);
 	//! FP64 sum fields of a group-by's state (the per-CTA region of f64_l2 holds one table each).
 	static int F64Fields(const GroupBySpec &gb);
+	//! Dynamic shared memory of the one-pass group-by's tables over `domain` slots.
+	static uint64_t DirectSmemBytes(const GroupBySpec &gb, uint64_t domain);
 	//! Shared-memory bytes of one heavy key's partial state in the heavy partition passes (row count,
 	//! partial state of every aggregate).
 	static int HeavySlotBytes(const GroupBySpec &gb);

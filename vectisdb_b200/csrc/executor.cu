@@ -783,13 +783,11 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 	const auto &props = Runtime::Get().props();
 	const int F = PipelineCodegen::StateWords(gb);
 	const uint64_t domain = 1ull << shift;
-	uint64_t direct_smem = domain * static_cast<uint64_t>(F) * 8;
-	const bool direct = direct_smem <= 96 * 1024;
+	const bool direct = domain * static_cast<uint64_t>(F) * 8 <= 96 * 1024;  // 8-byte words per slot bound the choice
 	// FP64 sums of the one-pass group-by in L2-resident per-CTA tables (VGPU_GB_DIRECT_F64_L2=1)
 	const char *env_dl2 = std::getenv("VGPU_GB_DIRECT_F64_L2");
 	const int direct_f64 = PipelineCodegen::F64Fields(gb);
 	const bool direct_l2 = direct && direct_f64 > 0 && env_dl2 && std::strcmp(env_dl2, "1") == 0;
-	if (direct_l2) direct_smem = domain * static_cast<uint64_t>(F - direct_f64) * 8;
 	if (!direct && pin.spec.join_multi) {
 		// the partitioned strategies take one item per input row: expand the join's matches into a
 		// relation first, then group that
@@ -863,7 +861,7 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 		a.SetPtr(cb + 1 + F + out_words, count);
 		const unsigned init_grid = static_cast<unsigned>(std::min<uint64_t>((domain + 255) / 256, 1024));
 		LaunchGenerated(*module, "vgpu_gb_direct_init", init_grid, 256, 0, stream_, a, domain * F * 8, domain);
-		const size_t smem = static_cast<size_t>(direct_smem);
+		const size_t smem = static_cast<size_t>(PipelineCodegen::DirectSmemBytes(gb, domain));
 		CUfunction f = module->Get("vgpu_gb_direct");
 		int occ = std::max(1, Runtime::Get().MaxActiveBlocks(f, g.block, smem));
 		const uint64_t ntiles = (n + g.tile() - 1) / g.tile();
