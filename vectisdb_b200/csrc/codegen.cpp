@@ -822,7 +822,7 @@ int PipelineCodegen::DirectSlotBytes(const GroupBySpec &gb) {
 uint64_t PipelineCodegen::DirectSmemBytes(const GroupBySpec &gb, uint64_t domain) {
 	const int F = static_cast<int>(StateFields(gb).size());
 	const int shared64 = F - 1 - (gb.f64_l2 ? F64Fields(gb) : 0);
-	const bool c32 = gb.narrow_count || gb.count_as_flag;
+	const bool c32 = gb.count32 && (gb.narrow_count || gb.count_as_flag);
 	return domain * (static_cast<uint64_t>(shared64) * 8 + (c32 ? 4 : 8));
 }
 
@@ -949,9 +949,10 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		o << "extern \"C\" __global__ void __launch_bounds__(" << g.block << ") vgpu_gb_direct(KArgs a) {\n"
 		  << kKernelHead << "\textern __shared__ __align__(16) u64 vgpu_smem[];\n"
 		  << "\tconst u64 D = a.w[" << cb << "];\n";
-		// A count that never carries (fewer than 2^32 rows) or only marks presence needs 32 bits: its array
-		// goes after the 64-bit ones, in 4 bytes per slot (DirectSmemBytes sizes the launch alike).
-		const bool c32 = gb.narrow_count || gb.count_as_flag;
+		// A count that never carries (fewer than 2^32 rows) or only marks presence needs 32 bits: with
+		// count32 its array goes after the 64-bit ones, in 4 bytes per slot (DirectSmemBytes sizes the
+		// launch alike).
+		const bool c32 = gb.count32 && (gb.narrow_count || gb.count_as_flag);
 		int sh = 0;
 		for (int f = 0, gl = 0; f < F; f++) {
 			if (l2 && fields[f].kind == "f64") {
@@ -2207,7 +2208,7 @@ std::string GroupByKey(const PipelineCodegen::GroupBySpec &gb, bool partitioned)
 		o << static_cast<int>(a.kind) << '/' << a.column << '/' << static_cast<int>(a.input_type) << '/'
 		  << static_cast<int>(a.output_type) << ';';
 	}
-	o << "|db:" << gb.direct_bits << "|bt:" << gb.bucket_threads << "|hv:" << gb.heavy_slots << "|f64l2:" << gb.f64_l2 << "|hw:" << gb.heavy_warp << "|bp:" << gb.bucket_plain << "|nc:" << gb.narrow_count << "|cf:" << gb.count_as_flag;
+	o << "|db:" << gb.direct_bits << "|bt:" << gb.bucket_threads << "|hv:" << gb.heavy_slots << "|f64l2:" << gb.f64_l2 << "|hw:" << gb.heavy_warp << "|bp:" << gb.bucket_plain << "|nc:" << gb.narrow_count << "|cf:" << gb.count_as_flag << "|c32:" << gb.count32;
 	return o.str();
 }
 

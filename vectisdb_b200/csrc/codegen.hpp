@@ -156,6 +156,9 @@ public:
 		// One-pass group-by: no aggregate reads the row count (no COUNT, no AVG), so the count word only
 		// marks a group as present -- a plain store of 1, not an atomic add.
 		bool count_as_flag = false;
+		// One-pass group-by: the count (narrow or a flag) takes 4 bytes per slot in shared memory instead
+		// of 8 (the tables shrink, more CTAs fit on an SM).
+		bool count32 = false;
 	};
 
 	//! Group-by kernels (see executor for the argument layout), all in one translation unit:

@@ -837,6 +837,10 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 		for (auto &ag : gb.aggs) {
 			if (ag.kind == AggKind::COUNT || ag.kind == AggKind::COUNT_STAR || ag.kind == AggKind::AVG) gb.count_as_flag = false;
 		}
+		// 4-byte count slots pay where each probe row expands into several updates (the multi-match join
+		// source: the fourth CTA per SM hides their latency); over single rows the extra CTAs' table merges
+		// cost more than they hide (C2's probe 1.45 -> 1.51 ms, C0 slower too)
+		gb.count32 = pin.spec.join_multi;
 		gb.f64_l2 = direct_l2;
 		Geometry g;
 		g.block = 512;
