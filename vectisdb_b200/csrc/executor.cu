@@ -259,6 +259,15 @@ private:
 	//! execution dropping a table's last reference) frees it only after those kernels.
 	void ReleaseHolds() {
 		if (holds_.empty() && cache_reads_.empty()) return;
+		// A stream with nothing left to run has finished every read (the usual case: the execution read
+		// a group or row count back), so no mark is needed for the readers.
+		const cudaError_t idle = cudaStreamQuery(stream_);
+		if (idle == cudaSuccess) {
+			holds_.clear();
+			cache_reads_.clear();
+			return;
+		}
+		if (idle == cudaErrorNotReady) cudaGetLastError();  // a status, not an error: leave none behind
 		auto mark = StreamMark::After(stream_);
 		for (auto &h : holds_) h->readers.Add(mark);
 		holds_.clear();
@@ -274,17 +283,23 @@ private:
 	bool nulls_supported_;
 };
 
+// Counts are read through a pooled page-locked word: a copy into pageable memory takes the driver's
+// staged path, slower for a few bytes than a direct write into pinned memory.
 uint64_t Executor::ReadU64(const void *dev) {
-	uint64_t v = 0;
-	VGPU_CUDA(cudaMemcpyAsync(&v, dev, sizeof(v), cudaMemcpyDeviceToHost, stream_));
+	auto word = PinnedPool::Get().Acquire(sizeof(uint64_t));
+	VGPU_CUDA(cudaMemcpyAsync(word.get(), dev, sizeof(uint64_t), cudaMemcpyDeviceToHost, stream_));
 	VGPU_CUDA(cudaStreamSynchronize(stream_));
+	uint64_t v;
+	std::memcpy(&v, word.get(), sizeof(v));
 	return v;
 }
 
 uint32_t Executor::ReadU32(const void *dev) {
-	uint32_t v = 0;
-	VGPU_CUDA(cudaMemcpyAsync(&v, dev, sizeof(v), cudaMemcpyDeviceToHost, stream_));
+	auto word = PinnedPool::Get().Acquire(sizeof(uint32_t));
+	VGPU_CUDA(cudaMemcpyAsync(word.get(), dev, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
 	VGPU_CUDA(cudaStreamSynchronize(stream_));
+	uint32_t v;
+	std::memcpy(&v, word.get(), sizeof(v));
 	return v;
 }
 

@@ -281,13 +281,15 @@ def serialize_plan(plan: GpuPlanNode, keep: _Keep) -> abi.vgpu_plan:
 
 
 def _plan_snapshot(node: GpuPlanNode) -> tuple:
-    """Every field serialize_plan reads, as nested tuples (equal snapshots serialize identically)."""
-    return (int(node.op_type), node.table.catalog, node.table.schema, node.table.table, tuple(node.column_names),
-            tuple((e.generated_cuda_source, tuple(e.input_columns), int(e.output_type), float(e.estimated_ops_per_row),
-                   int(e.window_primitive)) for e in node.expressions),
+    """Every field serialize_plan reads, as nested tuples (equal snapshots serialize identically: the
+    enum and number fields are kept as they are, since equal values convert alike)."""
+    t = node.table
+    return (node.op_type, t.catalog, t.schema, t.table, tuple(node.column_names),
+            tuple([(e.generated_cuda_source, tuple(e.input_columns), e.output_type, e.estimated_ops_per_row,
+                    e.window_primitive) for e in node.expressions]),
             tuple(node.build_keys), tuple(node.probe_keys), tuple(node.output_columns), tuple(node.group_keys),
-            tuple((int(a.kind), int(a.output_type), a.input_column) for a in node.aggregates), tuple(node.aggregate_exprs),
-            node.estimated_rows, node.estimated_row_width_bytes, tuple(_plan_snapshot(c) for c in node.children))
+            tuple([(a.kind, a.output_type, a.input_column) for a in node.aggregates]), tuple(node.aggregate_exprs),
+            node.estimated_rows, node.estimated_row_width_bytes, tuple([_plan_snapshot(c) for c in node.children]))
 
 
 _PLAN_MEMO: "collections.OrderedDict[int, tuple]" = collections.OrderedDict()
@@ -357,20 +359,24 @@ class _ResultOwner:
             pass
 
 
+_VALUE_TYPES = {int(v): v for v in GpuValueType}
+
+
 def _read_result(handle, owner: "_ResultOwner | None" = None) -> list[GpuColumn]:
     """Columns of a result. With `owner`, host columns are views of the result's own (page-locked)
     memory that keep it alive; without, they are copies."""
     L = abi.lib()
     cols = []
+    c = abi.vgpu_column()
+    ref = C.byref(c)
     for i in range(L.vgpu_result_column_count(handle)):
-        c = abi.vgpu_column()
-        abi.check(L.vgpu_result_get_column(handle, i, C.byref(c)))
-        t = GpuValueType(c.type)
-        dt = NUMPY_DTYPE[t]
-        n = int(c.row_count)
+        abi.check(L.vgpu_result_get_column(handle, i, ref))
+        t = _VALUE_TYPES[c.type]
+        n = c.row_count
         if c.memory == abi.MEM_DEVICE:
-            cols.append(GpuColumn(c.name.decode(), t, None, None, n, int(c.data or 0)))
+            cols.append(GpuColumn(c.name.decode(), t, None, None, n, c.data or 0))
             continue
+        dt = NUMPY_DTYPE[t]
         if n and c.data and owner is not None:
             buf = (C.c_uint8 * (n * dt.itemsize)).from_address(c.data)
             buf._vgpu_owner = owner
