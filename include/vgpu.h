@@ -181,7 +181,11 @@ typedef struct vgpu_exec_options {
 	void *stream;                        /* cudaStream_t to run on; NULL = the engine's own stream */
 } vgpu_exec_options;
 
-#define VGPU_EXEC_NO_SYNC 1u /* device output only: return without synchronizing the stream */
+/* Device output only: return without synchronizing the stream. A root GROUP BY on the one-pass path,
+ * or a root FILTER/PROJECTION chain whose outputs have no NULL masks, then leaves its row count on the
+ * device too: until vgpu_result_get_column (or _column_range) first reads the result, which waits for
+ * the stream, the columns are sized for every key value (every input row). */
+#define VGPU_EXEC_NO_SYNC 1u
 
 void vgpu_exec_options_init(vgpu_exec_options *options);
 

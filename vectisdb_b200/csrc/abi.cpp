@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -30,6 +31,7 @@ using namespace vgpu;
 struct vgpu_result {
 	ExecResult exec;
 	std::vector<std::string> names;
+	std::mutex rows_mu;  // guards the first read of a row count left on the device
 };
 
 namespace {
@@ -541,9 +543,36 @@ size_t vgpu_result_column_count(const vgpu_result *result) {
 	return result ? result->exec.columns.size() : 0;
 }
 
+namespace {
+
+// A result whose execution left its row count on the device (device output without a sync) reads it
+// now, once: the stream's work up to the count is waited for here instead of in the execution.
+void ResolveRows(const vgpu_result *result) {
+	auto *r = const_cast<vgpu_result *>(result);  // results are created mutable; the API hands out const views
+	std::lock_guard<std::mutex> lock(r->rows_mu);
+	if (!r->exec.pending_rows) return;
+	const size_t width = r->exec.pending_rows_bytes == 4 ? 4 : 8;
+	auto word = PinnedPool::Get().Acquire(sizeof(uint64_t));
+	VGPU_CUDA(cudaMemcpyAsync(word.get(), r->exec.pending_rows, width, cudaMemcpyDeviceToHost, r->exec.stream));
+	VGPU_CUDA(cudaStreamSynchronize(r->exec.stream));
+	uint64_t rows = 0;
+	if (width == 4) {
+		uint32_t v;
+		std::memcpy(&v, word.get(), sizeof(v));
+		rows = v;
+	} else {
+		std::memcpy(&rows, word.get(), sizeof(rows));
+	}
+	for (auto &c : r->exec.columns) c.rows = rows;
+	r->exec.pending_rows = nullptr;  // its buffer is freed with the result
+}
+
+} // namespace
+
 vgpu_status vgpu_result_get_column(const vgpu_result *result, size_t index, vgpu_column *out) {
 	return Guard([&] {
 		if (!result || !out) Fail(VGPU_ERR_INVALID_ARGUMENT, "null argument");
+		ResolveRows(result);
 		if (index >= result->exec.columns.size()) Fail(VGPU_ERR_INVALID_ARGUMENT, "column index out of range");
 		const HostColumnOut &c = result->exec.columns[index];
 		out->name = c.name.c_str();

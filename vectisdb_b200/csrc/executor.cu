@@ -195,6 +195,18 @@ public:
 	Arena &arena() {
 		return arena_;
 	}
+	//! The plan's root: the node whose outputs become the result.
+	void SetRoot(const PlanNode *root) {
+		root_ = root;
+	}
+	//! Device word holding the row count of every result column when the execution left it there
+	//! (taken from the arena: the result owns it), else nullptr.
+	void *deferred_rows() const {
+		return deferred_rows_;
+	}
+	int deferred_rows_bytes() const {
+		return deferred_rows_bytes_;
+	}
 
 private:
 	struct PipelineInput {
@@ -213,7 +225,9 @@ private:
 	                            bool any_order = false);
 	//! A pipeline with no chain over the columns of a relation.
 	PipelineInput PipelineOver(const Relation &rel);
-	Relation Materialize(PipelineInput &pin, const std::vector<int> &out_cols, const std::vector<std::string> &names);
+	//! `at_root`: the outputs are the plan's result (their row count may stay on the device).
+	Relation Materialize(PipelineInput &pin, const std::vector<int> &out_cols, const std::vector<std::string> &names,
+	                     bool at_root = false);
 	Relation RunChain(const PlanNode &node);
 	Relation GroupBy(const PlanNode &node);
 	Relation Join(const PlanNode &node);
@@ -281,6 +295,21 @@ private:
 	Arena arena_;
 	size_t cursor_ = 0;
 	bool nulls_supported_;
+	const PlanNode *root_ = nullptr;
+	void *deferred_rows_ = nullptr;
+	int deferred_rows_bytes_ = 8;
+	//! The root's outputs stay on the device and the caller does not wait (device output, no sync): a
+	//! row count nothing after the root needs stays on the device too, read when the result's columns
+	//! are first asked for, the columns sized for `capacity_bytes` meanwhile. False when the count must
+	//! be read now.
+	bool DeferRows(void *count, int bytes, uint64_t capacity_bytes) {
+		if (!(options_.output_on_device && options_.no_sync) || deferred_rows_) return false;
+		if (!Runtime::Get().allocator().HasHeadroom(capacity_bytes)) return false;
+		if (!arena_.Take(count)) return false;
+		deferred_rows_ = count;
+		deferred_rows_bytes_ = bytes;
+		return true;
+	}
 };
 
 // Counts are read through a pooled page-locked word: a copy into pageable memory takes the driver's
@@ -483,7 +512,7 @@ Executor::PipelineInput Executor::PipelineOver(const Relation &rel) {
 }
 
 Relation Executor::Materialize(PipelineInput &pin, const std::vector<int> &out_cols,
-                               const std::vector<std::string> &names) {
+                               const std::vector<std::string> &names, bool at_root) {
 	auto cgp = CodegenFor(pin.spec);
 	const PipelineCodegen &cg = *cgp;
 	Geometry g;
@@ -523,7 +552,19 @@ Relation Executor::Materialize(PipelineInput &pin, const std::vector<int> &out_c
 			a.SetPtr(cb, tile_counts);
 			LaunchGenerated(*module, "vgpu_mat_count", grid, g.block, 0, stream_, a, in_bytes, n);
 			kern::ExclusiveScanU32(tile_counts, tile_counts, ntiles, total, arena_);
-			out_rows = ReadU32(total);
+			// at the root, outputs without NULL masks may take a row per input row and leave the count
+			// on the device
+			bool defer = at_root;
+			uint64_t row_bytes = 0;
+			for (int c : out_cols) {
+				defer = defer && !cg.visible()[c].nullable;
+				row_bytes += TypeSize(cg.visible()[c].type);
+			}
+			if (defer && DeferRows(total, 4, n * row_bytes)) {
+				out_rows = n;
+			} else {
+				out_rows = ReadU32(total);
+			}
 			tile_offsets = tile_counts;
 		}
 	}
@@ -577,7 +618,7 @@ Relation Executor::RunChain(const PlanNode &node) {
 		outs.push_back(static_cast<int>(i));
 		names.push_back(probe.visible()[i].name);
 	}
-	return Materialize(pin, outs, names);
+	return Materialize(pin, outs, names, &node == root_);
 }
 
 Relation Executor::CrossProduct(const PlanNode &node) {
@@ -889,7 +930,11 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 		if (direct_l2) a.SetPtr(cb + 2 + F + out_words, arena_.AllocT<uint64_t>(uint64_t(grid) * direct_f64 * domain));
 		LaunchGenerated(*module, "vgpu_gb_direct", grid, g.block, smem, stream_, a, in_bytes, n);
 		LaunchGenerated(*module, "vgpu_gb_direct_final", 1, 1024, 0, stream_, a, domain * F * 8, domain);
-		groups = ReadU64(count);
+		if (&node == root_ && !node.group_keys.empty() && DeferRows(count, 8, 0)) {
+			groups = domain;  // the columns already hold a slot per key value
+		} else {
+			groups = ReadU64(count);
+		}
 	} else {
 		// Partitioned. Tier-1 bucket tables are small (about 48 KB, 128 threads per CTA, several CTAs per
 		// SM): few warps share a table, so same-slot atomics of moderately heavy keys queue behind at most
@@ -1758,9 +1803,15 @@ ExecResult ExecutePlan(const PlanNode &plan, const std::vector<vgpu_column> &inp
 	RefuseWindowPrimitives(plan);
 	Runtime::Get().EnsureDevice();
 	Executor ex(inputs, options, stream, IsRowIndependent(plan));
+	ex.SetRoot(&plan);
 	Relation rel = ex.Exec(plan);
 	ExecResult result;
 	result.stream = stream;
+	if (void *rows = ex.deferred_rows()) {
+		result.pending_rows = rows;
+		result.pending_rows_bytes = ex.deferred_rows_bytes();
+		result.device_buffers.push_back(rows);
+	}
 	for (auto &c : rel) {
 		HostColumnOut o;
 		o.name = c.name;

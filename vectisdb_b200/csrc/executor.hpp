@@ -49,6 +49,10 @@ struct ExecResult {
 	std::vector<void *> device_buffers; // owned device memory (device output mode)
 	std::vector<std::shared_ptr<void>> keepalive; // device memory shared with other results (batches)
 	cudaStream_t stream = nullptr;
+	// Device u64 with the row count of every column, not read yet (device output without a sync): the
+	// columns' `rows` are their capacity until it is. It is also listed in device_buffers.
+	void *pending_rows = nullptr;
+	int pending_rows_bytes = 8;  // its width: 8 (u64) or 4 (u32)
 };
 
 //! Validates a GROUP_BY_AGGREGATE node against its input pipeline and returns its aggregate spec;

@@ -405,11 +405,22 @@ class ExecuteOptions:  # GpuExecuteOptions (gpu_engine.hpp:357-385) + placement
 
 
 class DeviceResult:
-    """A result left on the device (output_on_device=True). Free it (or use `with`) when done."""
+    """A result left on the device (output_on_device=True). Free it (or use `with`) when done.
 
-    def __init__(self, handle, columns: list[GpuColumn]):
+    `columns` is read from the result on first access when it is not given: a result executed with
+    no_sync may still hold its row count on the device, and reading the columns is what waits for it."""
+
+    def __init__(self, handle, columns: list[GpuColumn] | None = None):
         self._handle = handle
-        self.columns = columns
+        self._columns = columns
+
+    @property
+    def columns(self) -> list[GpuColumn]:
+        if self._columns is None:
+            if not self._handle:
+                raise RuntimeError("the device result was freed before its columns were read")
+            self._columns = _read_result(self._handle)
+        return self._columns
 
     def free(self):
         if self._handle:
@@ -462,6 +473,8 @@ class GpuEngine:
         if status != abi.OK:
             return GpuExecutionResult(False, abi.last_error(), status, [])
         if o.output_on_device:
+            if o.no_sync:
+                return DeviceResult(handle)  # columns read on first use (the row count may be pending)
             try:
                 columns = _read_result(handle)
             except Exception:
