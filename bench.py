@@ -1004,6 +1004,10 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
+    # One dedicated stream for the engine and the timing events alike: torch's default stream has the
+    # handle 0, which the engine takes as "its own stream", and events on another stream than the
+    # kernels' would time only the host's enqueueing of calls that return without a sync.
+    torch.cuda.set_stream(torch.cuda.Stream())
     if world > 1:
         import datetime
         import torch.distributed as dist
