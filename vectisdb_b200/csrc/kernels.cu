@@ -107,8 +107,47 @@ __global__ void __launch_bounds__(kScanBlock) ScanApply(const T *in, T *out, uin
 	}
 }
 
+// Values one CTA scans in one launch (16 per thread): the tile counts of a materialization of up to
+// 2^24 rows. The three-launch form costs more in launches than in work at these sizes.
+constexpr int kSmallScanItems = 16;
+constexpr uint64_t kSmallScanMax = 1024 * kSmallScanItems;
+
+// Single CTA, in place allowed: each thread loads a run of up to 16 consecutive values at once (all
+// loads issued before any is used), the block scans the run sums, then each thread writes its run's
+// exclusive prefixes from registers (every read precedes the block scan's barrier, every write follows).
+template <typename T> __global__ void __launch_bounds__(1024) ScanSmall(const T *in, T *out, uint64_t n, T *total) {
+	__shared__ T scratch[33];
+	const uint64_t per = (n + blockDim.x - 1) / blockDim.x;
+	const uint64_t b = static_cast<uint64_t>(threadIdx.x) * per;
+	T vals[kSmallScanItems];
+	T local = 0;
+#pragma unroll
+	for (int k = 0; k < kSmallScanItems; k++) {
+		const uint64_t i = b + k;
+		vals[k] = (static_cast<uint64_t>(k) < per && i < n) ? in[i] : T(0);
+		local += vals[k];
+	}
+	T all;
+	T run = BlockScanExclusive<T>(local, scratch, &all);
+#pragma unroll
+	for (int k = 0; k < kSmallScanItems; k++) {
+		const uint64_t i = b + k;
+		if (static_cast<uint64_t>(k) < per && i < n) {
+			out[i] = run;
+			run += vals[k];
+		}
+	}
+	if (threadIdx.x == 0 && total) *total = all;
+}
+
 template <typename T> void ExclusiveScan(const T *in, T *out, uint64_t n, T *total, Arena &arena) {
 	cudaStream_t s = arena.stream();
+	if (n <= kSmallScanMax) {
+		LaunchScope scope("scan_small", s, 2 * n * sizeof(T), n);
+		ScanSmall<T><<<1, 1024, 0, s>>>(in, out, n, total);
+		VGPU_CUDA(cudaGetLastError());
+		return;
+	}
 	const uint64_t tiles = n == 0 ? 1 : (n + kScanTile - 1) / kScanTile;
 	T *sums = arena.AllocT<T>(tiles);
 	{
