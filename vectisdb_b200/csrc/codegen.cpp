@@ -934,9 +934,12 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 	if (!partitioned) {
 		// ---- direct: packed key is the slot of a dense table of `domain` groups ----
 		// args: cb+0 = D, cb+1+f = global field arrays, then (final) outputs, then count ptr.
+		const bool fused = DirectFinalFused(gb);
+		const int ticket = cb + 3 + F + out_words;
 		o << "extern \"C\" __global__ void vgpu_gb_direct_init(KArgs a) {\n"
-		  << "\tconst u64 D = a.w[" << cb << "];\n"
-		  << "\tfor (u64 s = blockIdx.x * (u64)blockDim.x + threadIdx.x; s < D; s += (u64)gridDim.x * blockDim.x) {\n";
+		  << "\tconst u64 D = a.w[" << cb << "];\n";
+		if (fused) o << "\tif (blockIdx.x == 0 && threadIdx.x == 0) *(u32*)a.w[" << ticket << "] = 0u;\n";
+		o << "\tfor (u64 s = blockIdx.x * (u64)blockDim.x + threadIdx.x; s < D; s += (u64)gridDim.x * blockDim.x) {\n";
 		for (int f = 0; f < F; f++) {
 			o << "\t\t((u64*)a.w[" << cb + 1 + f << "])[s] = " << InitValue(fields[f]) << ";\n";
 		}
@@ -979,13 +982,25 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			o << "\tu64 *G" << f << " = (u64*)a.w[" << cb + 1 + f << "];\n";
 		}
 		o << "\tfor (u64 s = threadIdx.x; s < D; s += " << g.block << ") {\n\t\tif (T0[s] != 0) {\n"
-		  << MergeCode(fields, "T", "s", "G", "s", l2) << "\t\t}\n\t}\n}\n\n";
-		// final: one CTA compacts the non-empty groups in key order
-		o << "extern \"C\" __global__ void vgpu_gb_direct_final(KArgs a) {\n"
-		  << "\t__shared__ u32 scan_scratch[33];\n"
-		  << "\tconst u64 D = a.w[" << cb << "];\n";
-		for (int f = 0; f < F; f++) {
-			o << "\tconst u64 *G" << f << " = (const u64*)a.w[" << cb + 1 + f << "];\n";
+		  << MergeCode(fields, "T", "s", "G", "s", l2) << "\t\t}\n\t}\n";
+		// final: one CTA compacts the non-empty groups in key order. Fused, it is the CTA whose merge
+		// finished last: every thread fences its merge atomics before the CTA takes a ticket, and the
+		// last CTA fences again before reading the global tables (which no CTA has loaded through L1:
+		// the merges are atomics).
+		if (fused) {
+			o << "\t__threadfence();\n\t__syncthreads();\n\t__shared__ u32 vgpu_last;\n"
+			  << "\tif (threadIdx.x == 0) vgpu_last = atomicAdd((u32*)a.w[" << ticket
+			  << "], 1u) == gridDim.x - 1 ? 1u : 0u;\n"
+			  << "\t__syncthreads();\n\tif (vgpu_last == 0u) return;\n\t__threadfence();\n"
+			  << "\t__shared__ u32 scan_scratch[33];\n";
+		} else {
+			o << "}\n\n";
+			o << "extern \"C\" __global__ void vgpu_gb_direct_final(KArgs a) {\n"
+			  << "\t__shared__ u32 scan_scratch[33];\n"
+			  << "\tconst u64 D = a.w[" << cb << "];\n";
+			for (int f = 0; f < F; f++) {
+				o << "\tconst u64 *G" << f << " = (const u64*)a.w[" << cb + 1 + f << "];\n";
+			}
 		}
 		o << "\tu64 base = 0;\n"
 		  << "\tfor (u64 c0 = 0; c0 < D; c0 += blockDim.x) {\n"

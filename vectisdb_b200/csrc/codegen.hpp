@@ -162,7 +162,7 @@ public:
 	};
 
 	//! Group-by kernels (see executor for the argument layout), all in one translation unit:
-	//!  direct: vgpu_gb_direct_init, vgpu_gb_direct, vgpu_gb_direct_final
+	//!  direct: vgpu_gb_direct_init, vgpu_gb_direct (+ vgpu_gb_direct_final unless DirectFinalFused)
 	//!  partitioned: vgpu_gb_part_count, vgpu_gb_part_scatter, vgpu_gb_bucket (+ _retry, _global)
 	//!  direct-partitioned: vgpu_gb_part_count, vgpu_gb_part_scatter, vgpu_gb_dtab_init, vgpu_gb_dbucket
 	std::string EmitGroupBy(const GroupBySpec &gb, bool partitioned, const Geometry &g) const;
@@ -187,6 +187,12 @@ public:
 	static int F64Fields(const GroupBySpec &gb);
 	//! Dynamic shared memory of the one-pass group-by's tables over `domain` slots.
 	static uint64_t DirectSmemBytes(const GroupBySpec &gb, uint64_t domain);
+	//! One-pass group-by: the last CTA to finish its merge compacts the groups (no separate final
+	//! launch), counting finished CTAs in a u32 ticket at argument word cb + 3 + F + outputs, which
+	//! vgpu_gb_direct_init zeroes. Only while that word lies below the reserved key words.
+	bool DirectFinalFused(const GroupBySpec &gb) const {
+		return ConsumerBase() + 3 + StateWords(gb) + static_cast<int>(gb.keys.size() + gb.aggs.size()) < kKeyWord;
+	}
 	//! Shared-memory bytes of one heavy key's partial state in the heavy partition passes (row count,
 	//! partial state of every aggregate).
 	static int HeavySlotBytes(const GroupBySpec &gb);

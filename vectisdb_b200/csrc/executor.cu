@@ -904,8 +904,8 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 		if (const char *env = std::getenv("VGPU_GB_DIRECT_ITEMS")) {  // tuning override
 			g.items = std::max(1, std::min(32, std::atoi(env)));
 		}
-		if (const char *env = std::getenv("VGPU_GB_DIRECT_BLOCK")) {  // tuning override
-			g.block = std::max(64, std::min(1024, std::atoi(env)));
+		if (const char *env = std::getenv("VGPU_GB_DIRECT_BLOCK")) {  // tuning override (whole warps)
+			g.block = std::max(64, std::min(1024, std::atoi(env))) / 32 * 32;
 		}
 		const std::string gkey = SpecKey(pin.spec) + "|" + GroupByKey(gb, false) + "|g:" + std::to_string(g.block) + "x" +
 		                         std::to_string(g.items);
@@ -919,6 +919,8 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 		for (int f = 0; f < F; f++) a.SetPtr(cb + 1 + f, fields + domain * f);
 		for (int w = 0; w < out_words; w++) a.SetPtr(cb + 1 + F + w, out[w].data);
 		a.SetPtr(cb + 1 + F + out_words, count);
+		const bool fused_final = cg.DirectFinalFused(gb);
+		if (fused_final) a.SetPtr(cb + 3 + F + out_words, arena_.AllocT<uint32_t>(1));  // finished-CTA ticket
 		const unsigned init_grid = static_cast<unsigned>(std::min<uint64_t>((domain + 255) / 256, 1024));
 		LaunchGenerated(*module, "vgpu_gb_direct_init", init_grid, 256, 0, stream_, a, domain * F * 8, domain);
 		const size_t smem = static_cast<size_t>(PipelineCodegen::DirectSmemBytes(gb, domain));
@@ -929,7 +931,7 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 		    static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ntiles, uint64_t(props.sm_count) * occ)));
 		if (direct_l2) a.SetPtr(cb + 2 + F + out_words, arena_.AllocT<uint64_t>(uint64_t(grid) * direct_f64 * domain));
 		LaunchGenerated(*module, "vgpu_gb_direct", grid, g.block, smem, stream_, a, in_bytes, n);
-		LaunchGenerated(*module, "vgpu_gb_direct_final", 1, 1024, 0, stream_, a, domain * F * 8, domain);
+		if (!fused_final) LaunchGenerated(*module, "vgpu_gb_direct_final", 1, 1024, 0, stream_, a, domain * F * 8, domain);
 		if (&node == root_ && !node.group_keys.empty() && DeferRows(count, 8, 0)) {
 			groups = domain;  // the columns already hold a slot per key value
 		} else {
