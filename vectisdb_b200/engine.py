@@ -579,18 +579,18 @@ class GpuEngine:
             plan_arr = (PlanPtr * max(1, n))(*[C.pointer(pc) for pc in plan_cs])
             abi.check(self.lib.vgpu_execute_batch(plan_arr, col_arr, counts, n, C.byref(opts), C.byref(bo), handles,
                                                   C.byref(st)))
-        results = []
-        for i in range(n):
-            h = C.c_void_p(handles[i])
-            try:
-                columns = _read_result(h)
-            except Exception:
-                for j in range(i, n):
-                    self.lib.vgpu_result_free(C.c_void_p(handles[j]))
-                raise
-            if o.output_on_device:
-                results.append(DeviceResult(h, columns))
-            else:
+        if o.output_on_device:  # each result's columns are read on first use
+            results = [DeviceResult(C.c_void_p(handles[i])) for i in range(n)]
+        else:
+            results = []
+            for i in range(n):
+                h = C.c_void_p(handles[i])
+                try:
+                    columns = _read_result(h, None)
+                except Exception:
+                    for j in range(i, n):
+                        self.lib.vgpu_result_free(C.c_void_p(handles[j]))
+                    raise
                 self.lib.vgpu_result_free(h)
                 results.append(GpuExecutionResult(True, "", abi.OK, columns))
         stats = {k: getattr(st, k) for k, _ in abi.vgpu_batch_stats._fields_}
@@ -745,7 +745,7 @@ class Server:
         if not h.value:
             return None, d
         if on_device:
-            return DeviceResult(h, _read_result(h)), d
+            return DeviceResult(h), d  # columns read on first use
         # host results: zero-copy views of the result's page-locked buffers, freed with the last view
         return GpuExecutionResult(True, "", abi.OK, _read_result(h, _ResultOwner(h))), d
 
