@@ -559,14 +559,14 @@ std::string PipelineCodegen::EmitMaterialize(const std::vector<int> &outs, const
 	if (has_filter_ && stage_bytes <= 32 * 1024) {
 		for (size_t c = 0; c < out_cols.size(); c++) {
 			const auto &col = visible_[out_cols[c]];
-			o << "\t\t__shared__ __align__(16) " << CudaTypeName(col.type) << " st" << c << "[" << g.tile() << "];\n";
-			if (col.nullable) o << "\t\t__shared__ u8 sv" << c << "[" << g.tile() << "];\n";
+			o << "\t\t__shared__ __align__(16) " << CudaTypeName(col.type) << " vgpu_st" << c << "[" << g.tile() << "];\n";
+			if (col.nullable) o << "\t\t__shared__ u8 vgpu_sv" << c << "[" << g.tile() << "];\n";
 		}
 		o << "\t\tu32 total; u32 rank = block_exclusive_scan(cnt, scan_scratch, &total);\n"
 		  << "\t\t#pragma unroll\n\t\tfor (int r = 0; r < " << g.items << "; ++r) {\n\t\t\tif (kv[r]) {\n";
 		for (size_t c = 0; c < out_cols.size(); c++) {
-			o << "\t\t\t\tst" << c << "[rank] = o" << c << "[r];\n";
-			if (visible_[out_cols[c]].nullable) o << "\t\t\t\tsv" << c << "[rank] = ov" << c << "[r] ? 1 : 0;\n";
+			o << "\t\t\t\tvgpu_st" << c << "[rank] = o" << c << "[r];\n";
+			if (visible_[out_cols[c]].nullable) o << "\t\t\t\tvgpu_sv" << c << "[rank] = ov" << c << "[r] ? 1 : 0;\n";
 		}
 		o << "\t\t\t\t++rank;\n\t\t\t}\n\t\t}\n\t\t__syncthreads();\n"
 		  << "\t\tconst u64 base = tile_offsets[tile];\n"
@@ -574,9 +574,9 @@ std::string PipelineCodegen::EmitMaterialize(const std::vector<int> &outs, const
 		for (size_t c = 0; c < out_cols.size(); c++) {
 			const auto &col = visible_[out_cols[c]];
 			int w = cb + 1 + 2 * static_cast<int>(c);
-			o << "\t\t\t((" << CudaTypeName(col.type) << "*)a.w[" << w << "])[base + i] = st" << c << "[i];\n";
+			o << "\t\t\t((" << CudaTypeName(col.type) << "*)a.w[" << w << "])[base + i] = vgpu_st" << c << "[i];\n";
 			if (col.nullable) {
-				o << "\t\t\tif (a.w[" << w + 1 << "]) ((u8*)a.w[" << w + 1 << "])[base + i] = sv" << c << "[i];\n";
+				o << "\t\t\tif (a.w[" << w + 1 << "]) ((u8*)a.w[" << w + 1 << "])[base + i] = vgpu_sv" << c << "[i];\n";
 			}
 		}
 		o << "\t\t}\n\t\t__syncthreads();  // the next tile reuses the staging\n\t}\n}\n";
