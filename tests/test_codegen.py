@@ -129,3 +129,40 @@ def test_join_source_kernels_compile_single_and_multi_match():
     for t in tus[4:]:
         assert "load_rows<int, 8>((const int*)a.w[2]" not in t
     assert all(s > 1000 for s in _compile_all(src))
+
+
+def _min_per_column_plan(m):
+    """GROUP BY k with MIN over each of m INT64 columns: every MIN adds a state word and an output word."""
+    import numpy as np
+    from vectisdb_b200.engine import GpuAggregateKind as A, GpuTableRef, make_aggregate, make_group_by
+    cols = [make_column("k", T.INT32, np.arange(64, dtype=np.int32))]
+    cols += [make_column(f"x{i}", T.INT64, np.arange(64, dtype=np.int64)) for i in range(m)]
+    plan = make_group_by(["k"], [make_aggregate(A.MIN, f"x{i}", T.INT64) for i in range(m)],
+                         make_scan([c.name for c in cols], GpuTableRef("memory", "main", "wide")))
+    return plan, cols
+
+
+def test_one_pass_group_by_compacts_in_its_last_cta_while_argument_words_allow():
+    """The one-pass group-by's compaction runs in the CTA that finishes its merge last (a ticket the init
+    kernel zeroes), with no separate final kernel -- unless the ticket's argument word would reach the
+    reserved key words: then the single-CTA final kernel runs as its own launch. Both forms compile."""
+    wl = W.c0(n=4096)
+    src = generate_source(wl.plan, wl.inputs)
+    assert "vgpu_last" in src and "vgpu_gb_direct_final" not in src
+    for m, fused in ((21, True), (22, False)):
+        plan, cols = _min_per_column_plan(m)
+        src = generate_source(plan, cols)
+        assert ("vgpu_last" in src) == fused and ("vgpu_gb_direct_final" in src) == (not fused), m
+        assert all(s > 1000 for s in _compile_all(src))
+
+
+def test_filtered_materialization_stages_kept_rows_for_coalesced_writes():
+    """A filter + projection writes each tile's kept rows from shared memory as one run per column, the
+    NULL masks included when an output is nullable."""
+    wl = W.cp(n=4096)
+    src = generate_source(wl.plan, wl.inputs)
+    write = src[src.index("vgpu_mat_write("):]
+    assert "vgpu_st0[rank] = o0[r];" in write and "[base + i] = vgpu_st0[i];" in write
+    plan, inputs, _ = CASES["nullable_column_excluded_by_filter_predicate"][1]()
+    src = generate_source(plan, inputs)
+    assert "vgpu_sv" in src[src.index("vgpu_mat_write("):]
