@@ -659,6 +659,9 @@ namespace {
 struct Field {
 	std::string kind; // "cnt", "f64", "lo", "hi", "min", "max"
 	int agg = -1;
+	// One-pass group-by, MIN/MAX in shared memory: >= 0 keeps the value as a 32-bit offset from the
+	// minimum in argument word `narrow_word` (the low word of the slot, updated by native 32-bit atomics).
+	int narrow_word = -1;
 };
 
 std::vector<Field> StateFields(const PipelineCodegen::GroupBySpec &gb) {
@@ -701,6 +704,9 @@ int FieldIndex(const std::vector<Field> &fields, const std::string &kind, int ag
 }
 
 std::string InitValue(const Field &f) {
+	if (f.narrow_word >= 0) {
+		return f.kind == "min" ? "0xffffffffull" : "0ull";
+	}
 	if (f.kind == "min") {
 		return "0x7fffffffffffffffull";
 	}
@@ -722,7 +728,10 @@ std::string UpdateCode(const std::vector<Field> &fields, const std::string &tab,
 	for (size_t i = 0; i < fields.size(); i++) {
 		auto &f = fields[i];
 		std::string p = tab + std::to_string(i) + " + " + slot;
-		if (f.kind == "cnt" && shared && count_as_flag) {
+		if ((f.kind == "min" || f.kind == "max") && shared && f.narrow_word >= 0) {
+			o << "\t\t\tatomic" << (f.kind == "min" ? "Min" : "Max") << "((u32*)(" << p << "), (u32)((i64)("
+			  << agg_values[f.agg] << ") - (i64)a.w[" << f.narrow_word << "]));\n";
+		} else if (f.kind == "cnt" && shared && count_as_flag) {
 			o << "\t\t\t*(u32*)(" << p << ") = 1u;\n";
 		} else if (f.kind == "cnt" && shared && narrow_count) {
 			o << "\t\t\tatomicAdd((u32*)(" << p << "), 1u);\n";
@@ -764,10 +773,11 @@ std::string MergeCode(const std::vector<Field> &fields, const std::string &src, 
 			std::string pd_hi = dst + std::to_string(i + 1) + " + " + ds;
 			o << "\t\t\tatomic_add_i128_pair(" << pd << ", (i64*)(" << pd_hi << "), " << ps << ", (i64)" << ps_hi
 			  << ");\n";
-		} else if (f.kind == "min") {
-			o << "\t\t\tatomic_min_i64((i64*)(" << pd << "), (i64)" << ps << ");\n";
-		} else if (f.kind == "max") {
-			o << "\t\t\tatomic_max_i64((i64*)(" << pd << "), (i64)" << ps << ");\n";
+		} else if (f.kind == "min" || f.kind == "max") {
+			const std::string v = f.narrow_word >= 0
+			                          ? "(i64)(u32)" + ps + " + (i64)a.w[" + std::to_string(f.narrow_word) + "]"
+			                          : "(i64)" + ps;
+			o << "\t\t\tatomic_" << f.kind << "_i64((i64*)(" << pd << "), " << v << ");\n";
 		}
 	}
 	return o.str();
@@ -973,6 +983,11 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		// args: cb+0 = D, cb+1+f = global field arrays, then (final) outputs, then count ptr.
 		const bool fused = DirectFinalFused(gb);
 		const int ticket = cb + 3 + F + out_words;
+		// the shared tables' view of the fields: MIN/MAX the executor narrowed to 32-bit offsets
+		std::vector<Field> dfields = fields;
+		for (auto &f : dfields) {
+			if (f.kind == "min" || f.kind == "max") f.narrow_word = gb.aggs[f.agg].narrow_word;
+		}
 		o << "extern \"C\" __global__ void vgpu_gb_direct_init(KArgs a) {\n"
 		  << "\tconst u64 D = a.w[" << cb << "];\n";
 		if (fused) o << "\tif (blockIdx.x == 0 && threadIdx.x == 0) *(u32*)a.w[" << ticket << "] = 0u;\n";
@@ -1005,13 +1020,13 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 		if (c32) o << "\tu32 *T0 = (u32*)(vgpu_smem + " << sh << " * D);\n";
 		o << "\tfor (u64 s = threadIdx.x; s < D; s += " << g.block << ") {\n";
 		for (int f = 0; f < F; f++) {
-			o << "\t\tT" << f << "[s] = " << InitValue(fields[f]) << ";\n";
+			o << "\t\tT" << f << "[s] = " << InitValue(dfields[f]) << ";\n";
 		}
 		o << "\t}\n\t__syncthreads();\n" << tile_loop_head
 		  << "\tfor (u64 tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n"
 		  << LoadBlock(g, needed, false) << ItemOpen(g, needed) << chain_code_ << "\t\tif (keep) {\n"
 		  << "\t\t\tconst u64 slot = " << pack.str() << ";\n"
-		  << UpdateCode(fields, "T", "slot", pipe_values, true, gb.narrow_count, gb.count_as_flag) << "\t\t}\n" << ItemClose()
+		  << UpdateCode(dfields, "T", "slot", pipe_values, true, gb.narrow_count, gb.count_as_flag) << "\t\t}\n" << ItemClose()
 		  << "\t}\n"
 		  << (l2 ? "\t__threadfence();  // this thread's reductions are performed before the sums are read\n" : "")
 		  << "\t__syncthreads();\n";
@@ -1019,7 +1034,7 @@ std::string PipelineCodegen::EmitGroupBy(const GroupBySpec &gb, bool partitioned
 			o << "\tu64 *G" << f << " = (u64*)a.w[" << cb + 1 + f << "];\n";
 		}
 		o << "\tfor (u64 s = threadIdx.x; s < D; s += " << g.block << ") {\n\t\tif (T0[s] != 0) {\n"
-		  << MergeCode(fields, "T", "s", "G", "s", l2) << "\t\t}\n\t}\n";
+		  << MergeCode(dfields, "T", "s", "G", "s", l2) << "\t\t}\n\t}\n";
 		// final: one CTA compacts the non-empty groups in key order. Fused, it is the CTA whose merge
 		// finished last: every thread fences its merge atomics before the CTA takes a ticket, and the
 		// last CTA fences again before reading the global tables (which no CTA has loaded through L1:
@@ -2258,7 +2273,7 @@ std::string GroupByKey(const PipelineCodegen::GroupBySpec &gb, bool partitioned)
 	o << "|aggs:";
 	for (auto &a : gb.aggs) {
 		o << static_cast<int>(a.kind) << '/' << a.column << '/' << static_cast<int>(a.input_type) << '/'
-		  << static_cast<int>(a.output_type) << ';';
+		  << static_cast<int>(a.output_type) << '/' << a.narrow_word << ';';
 	}
 	o << "|db:" << gb.direct_bits << "|bt:" << gb.bucket_threads << "|hv:" << gb.heavy_slots << "|f64l2:" << gb.f64_l2 << "|hw:" << gb.heavy_warp << "|bp:" << gb.bucket_plain << "|nc:" << gb.narrow_count << "|cf:" << gb.count_as_flag << "|c32:" << gb.count32;
 	return o.str();

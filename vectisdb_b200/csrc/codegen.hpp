@@ -120,6 +120,9 @@ public:
 		int column = -1; // visible column (-1 for COUNT_STAR)
 		ValueType input_type = ValueType::INT64;
 		ValueType output_type = ValueType::INT64;
+		// One-pass group-by, MIN/MAX: >= 0 keeps the shared-memory state as a 32-bit offset from the
+		// value in this argument word (the input's minimum; its range spans less than 2^32).
+		int narrow_word = -1;
 	};
 	struct GroupBySpec {
 		std::vector<GroupKey> keys;

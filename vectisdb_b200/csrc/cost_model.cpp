@@ -441,13 +441,23 @@ std::string GenerateSourceText(const PlanNode &plan, const std::vector<vgpu_colu
 	spec_nc.narrow_count = true;  // one-pass tables whose counts take no carries
 	spec_nc.count_as_flag = true;  // ... or are presence flags
 	spec_nc.f64_l2 = PipelineCodegen::F64Fields(spec_nc) > 0;  // ... and FP64 sums in L2
+	if (cg.DirectFinalFused(spec_nc)) {  // ... and integer MIN/MAX as 32-bit offsets
+		int word = cg.ConsumerBase() + 4 + PipelineCodegen::StateWords(spec_nc) +
+		           static_cast<int>(spec_nc.keys.size() + spec_nc.aggs.size());
+		for (auto &a : spec_nc.aggs) {
+			const bool narrowable = (a.kind == AggKind::MIN || a.kind == AggKind::MAX) &&
+			                        (a.input_type == ValueType::INT16 || a.input_type == ValueType::INT32 ||
+			                         a.input_type == ValueType::INT64);
+			if (narrowable && word < kKeyWord) a.narrow_word = word++;
+		}
+	}
 	// ... and both with tiles staged through shared memory by bulk copies
 	Geometry gst = g;
 	gst.items = 4;
 	gst.staged = true;
 	// Separate translation units, separated by a marker line: direct, partitioned, key statistics,
 	// direct-partitioned, direct-partitioned with heavy keys, the last two staged, the plain bucket pass,
-	// and the direct one with narrow counts.
+	// and the direct one with narrow counts and MIN/MAX.
 	return cg.EmitGroupBy(spec_gb, false, g) + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_gb, true, g) +
 	       "\n//@@VGPU_TU@@\n" + cg.EmitStats(key_columns, gs) + "\n//@@VGPU_TU@@\n" +
 	       cg.EmitGroupBy(spec_dp, true, g) + "\n//@@VGPU_TU@@\n" + cg.EmitGroupBy(spec_hv, true, g) +
