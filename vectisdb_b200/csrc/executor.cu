@@ -895,7 +895,7 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 		}
 		// 4-byte count slots pay where each probe row expands into several updates (the multi-match join
 		// source: the fourth CTA per SM hides their latency); over single rows the extra CTAs' table merges
-		// cost more than they hide (C2's probe 1.45 -> 1.51 ms, C0 slower too)
+		// cost more than they hide (a 2^28-row probe into 4096 groups: 1.45 -> 1.51 ms)
 		gb.count32 = pin.spec.join_multi;
 		gb.f64_l2 = direct_l2;
 		// MIN/MAX over a cached integer column whose values span less than 2^32: the shared tables hold
@@ -924,7 +924,7 @@ Relation Executor::GroupByPipeline(const PlanNode &node, PipelineInput &pin) {
 		}
 		Geometry g;
 		g.block = 512;
-		g.items = 4;  // also for a join source (measured on the fused C2 probe: 4 rows per thread 1.68 ms, 8 1.71 ms)
+		g.items = 4;  // also for a join source (a fused 2^28-row probe: 4 rows per thread 1.68 ms, 8 1.71 ms)
 		if (const char *env = std::getenv("VGPU_GB_DIRECT_ITEMS")) {  // tuning override
 			g.items = std::max(1, std::min(32, std::atoi(env)));
 		}
